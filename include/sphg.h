@@ -1,0 +1,203 @@
+/*
+ * sphg.h — C ABI of libsphg, a B200 (sm_100a) implementation of the
+ * weakly-compressible two-phase (water/soil) SPH time step of
+ * cwang2015/sources.
+ *
+ * The reference exposes its step as argument-less Fortran module procedures
+ * acting on module globals (declarations_sph.f90:13,44-56):
+ *     single_step                 declarations_sph.f90:1131  (two-phase RHS)
+ *     single_step_for_water       declarations_sph.f90:1439  (water-only RHS)
+ *     single_step_for_soil        declarations_sph.f90:1530  (soil-only RHS)
+ *     time_integration            declarations_sph.f90:525   (two-phase leapfrog)
+ *     time_integration_for_water  declarations_sph.f90:794
+ *     time_integration_for_soil   declarations_sph.f90:978
+ * called from sph.f90:51-57.  This header replaces those calls with explicit
+ * entry points: the Fortran host keeps its arrays and passes plain pointers
+ * (ISO_C_BINDING `c_loc`), the library keeps the particle state resident on
+ * the GPU between calls.  No torch or CUDA types appear in any signature.
+ *
+ * Conventions
+ *   - Every entry point returns an sphg_status (0 = OK).  The reference's
+ *     `stop` statements become status codes; nothing inside the library
+ *     aborts the process.
+ *   - Host arrays follow the Fortran layouts of the reference's `particles`
+ *     type (m_particles.f90:223-300): vectors are x(2,n) interleaved
+ *     (x1,y1,x2,y2,...), scalars are (n); index k of a host array is Fortran
+ *     particle k+1.  Real particles come first (1..ntotal), virtual (boundary)
+ *     particles follow (ntotal+1..ntotal+nvirt), as take_real / take_virtual
+ *     build them (m_particles.f90:808-893).
+ *   - A context is single-threaded and not re-entrant; several contexts may
+ *     coexist (each owns one CUDA stream).
+ */
+#ifndef SPHG_H
+#define SPHG_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SPHG_ABI_VERSION 1
+
+/* Status codes.  The reference stops the program where these are returned:
+ * pair overflow m_particles.f90:992-993,1053-1054; particle outside the grid
+ * :1131-1136; bad kernel id :932. */
+typedef enum sphg_status {
+    SPHG_OK = 0,
+    SPHG_ERR_PAIR_OVERFLOW = 1,   /* a pair list exceeded max_interaction      */
+    SPHG_ERR_OUT_OF_DOMAIN = 2,   /* a particle left [x_min,x_max]x[y_min,y_max]*/
+    SPHG_ERR_BAD_KERNEL = 3,      /* skf not in 1..4 (get_scale_k)              */
+    SPHG_ERR_BAD_ARG = 4,         /* null pointer, bad phase, bad size          */
+    SPHG_ERR_CUDA = 5,            /* a CUDA runtime call failed                 */
+    SPHG_ERR_TIMEOUT = 6,         /* a bounded device wait gave up              */
+    SPHG_ERR_NONFINITE = 7,       /* a NaN/Inf position was met                 */
+    SPHG_ERR_UNSUPPORTED = 8,     /* option outside the implemented scope       */
+    SPHG_ERR_STATE = 9,           /* call order violated (e.g. step before upload) */
+    SPHG_ERR_NO_DEVICE = 10       /* no CUDA device / driver                     */
+} sphg_status;
+
+/* Phase materials: `imaterial` of the particles type (m_particles.f90:213). */
+enum { SPHG_WATER = 1, SPHG_SOIL = 2 };
+
+/* Arithmetic of the pair kernels.  FP64: every field and sum in double, as
+ * the reference.  FP32: pair arithmetic, derivatives and neighbour sums in
+ * float; positions, time and the leapfrog-integrated state (x, v, rho, vof,
+ * stress, p) stay double. */
+enum { SPHG_FP64 = 0, SPHG_FP32 = 1 };
+
+/* Pair lists for sphg_export_pairs. */
+enum { SPHG_PAIRS_FIRST = 0,   /* same-phase pairs of phase 1 (direct_find)   */
+       SPHG_PAIRS_SECOND = 1,  /* same-phase pairs of phase 2 (direct_find)   */
+       SPHG_PAIRS_CROSS = 2 }; /* phase-1 i x phase-2 j (direct_find_2)       */
+
+/* type(material), m_particles.f90:19-29.  Water uses rho0,b,gamma,c,
+ * viscosity; soil uses rho0,k,E,niu,c,cohesion,phi,porosity,permeability
+ * (case file keys WATER PROPERTY, SOIL PROPERTY, DARCY PARAMETER, SOIL FAILURE
+ * CRITERIA, declarations_sph.f90:288-314).  phi is in radians. */
+typedef struct sphg_material {
+    double rho0, b, gamma, c, viscosity;
+    double k, porosity, permeability, G, E, niu, cohesion, phi;
+} sphg_material;
+
+/* The three configuration layers of the reference in one POD:
+ * param.f90:10-133 module flags, type(numerical) m_particles.f90:31-55, and
+ * the case-file values.  sphg_default_params() fills the reference defaults. */
+typedef struct sphg_params {
+    int32_t abi_version;            /* = SPHG_ABI_VERSION                         */
+    int32_t dim;                    /* param.f90:10; only 2 is supported          */
+    int32_t skf;                    /* m_particles.f90:141 (1 cubic,2 Gauss,3 quintic,4 Wendland) */
+    int32_t single_phase;           /* case file SINGLE PHASE                     */
+    int32_t first_material;         /* case file FIRST PHASE (single-phase runs)  */
+    int32_t summation_density;      /* param.f90:79                               */
+    int32_t average_velocity;       /* param.f90:80                               */
+    int32_t visc_artificial;        /* param.f90:86                               */
+    int32_t artificial_density;     /* param.f90:95                               */
+    int32_t soil_artificial_stress; /* param.f90:96                               */
+    int32_t volume_fraction;        /* param.f90:98                               */
+    int32_t water_artificial_volume;/* param.f90:99                               */
+    int32_t volume_fraction_renorm; /* param.f90:100                              */
+    int32_t stress_integration;     /* param.f90:92 (1 Euler, 2 leapfrog)         */
+    int32_t yield_criterion;        /* param.f90:93 (2 Drucker-Prager)            */
+    int32_t plasticity;             /* param.f90:94 (0 none, 3 flow rule 3)       */
+    int32_t integrate_scheme;       /* param.f90:78 (1 leapfrog)                  */
+    int32_t precision;              /* SPHG_FP64 / SPHG_FP32                      */
+    int32_t reorder_interval;       /* steps between spatial reorders of the device state (0: only at upload) */
+    int32_t renorm_interval;        /* vof renormalisation period, 40 in declarations_sph.f90:1415 */
+    double gravity;                 /* declarations_sph.f90:13, added to dvx(2)   */
+    double numeric_gravity;         /* numerical%gravity m_particles.f90:40, used by darcy_law */
+    double alpha, beta, etq;        /* m_particles.f90:44                         */
+    double dd, p1, p2;              /* m_particles.f90:47                         */
+    double delta;                   /* m_particles.f90:50                         */
+    double epsilon;                 /* m_particles.f90:53                         */
+    double dt;                      /* case file TIME STEP SIZE                   */
+    double x_min, x_max, y_min, y_max; /* x_mingeom.. (m_particles.f90:89-91): neighbour grid extent */
+    int64_t max_interaction;        /* param.f90:14: capacity of each pair list   */
+    sphg_material water, soil;      /* H2O, SiO2 (declarations_sph.f90:44)        */
+} sphg_params;
+
+/* Host view of one phase: pointers into the Fortran arrays of a `particles`
+ * object.  Vectors are (2,n) interleaved, n = ntotal + nvirt.  On upload,
+ * x, vx, rho, p, c, mass, hsml, itype are required; a NULL optional field is
+ * taken as zero.  On download, NULL fields are skipped.  txx/tyy/txy return
+ * the shared working arrays (declarations_sph.f90:52,371-377,414-415) as the
+ * reference leaves them, including the cross-phase aliasing. */
+typedef struct sphg_phase_host {
+    int32_t ntotal;          /* real particles                                    */
+    int32_t nvirt;           /* virtual particles (stored after the real ones)    */
+    int32_t material;        /* SPHG_WATER / SPHG_SOIL                            */
+    int32_t nfail;           /* download only: soil points on the yield surface   */
+    double dspp;             /* initial spacing; r0 of repulsive_force            */
+    double *x, *vx, *dvx, *av, *v_min;                 /* (2,n)                   */
+    double *rho, *rho_min, *drho, *p, *c, *mass, *hsml; /* (n)                    */
+    double *vof, *vof_min, *dvof, *vof2;                /* (n) volume fractions   */
+    double *sxx, *sxy, *syy, *dsxx, *dsxy, *dsyy, *dp;  /* (n) soil stress        */
+    double *sxx_min, *sxy_min, *syy_min, *p_min;        /* (n) stress_integration=2 */
+    double *epsilon_p, *vcc;                            /* (n)                    */
+    double *txx, *tyy, *txy;                            /* (n) working arrays     */
+    int32_t *itype;          /* >0 real, <0 virtual (setup_itype m_particles.f90:896) */
+    int32_t *fail;           /* download only: soil failure flag                  */
+} sphg_phase_host;
+
+/* Counters (interaction_statistics m_particles.f90:555-597 and nfail). */
+typedef struct sphg_stats_t {
+    int64_t niac[3];         /* pairs: phase 1, phase 2, cross (last step)        */
+    int32_t maxiac[2], miniac[2], noiac[2]; /* per-particle interaction stats     */
+    int32_t nfail;           /* soil points on the yield surface                  */
+    int32_t n_out_of_domain; /* particles clamped into the edge cells             */
+    int32_t itimestep;
+    int32_t _pad;
+    double time;
+    double last_step_ms;     /* device time of the last sphg_time_integration call */
+} sphg_stats_t;
+
+typedef struct sphg_ctx sphg_ctx;
+
+/* Fill *p with the reference defaults (param.f90, m_particles.f90:31-55). */
+void sphg_default_params(sphg_params* p);
+
+/* Create a context for n_phase phases (1 single-phase, 2 water+soil) on the
+ * current CUDA device.  Replaces allocate_sph (declarations_sph.f90:338). */
+int sphg_create(const sphg_params* p, int n_phase, sphg_ctx** out);
+
+/* Copy one phase (1-based: 1 = `parts`, 2 = `soil`) to the device. */
+int sphg_upload_phase(sphg_ctx* ctx, int phase, const sphg_phase_host* v);
+
+/* Right-hand side only: single_step (declarations_sph.f90:1131), or
+ * single_step_for_water (:1439) / single_step_for_soil (:1530) in
+ * single-phase runs.  itimestep drives the renormalisation period. */
+int sphg_single_step(sphg_ctx* ctx, int itimestep);
+
+/* maxtimestep leapfrog steps on the device: time_integration (:525),
+ * time_integration_for_water (:794) or time_integration_for_soil (:978).
+ * *itimestep and *time are advanced as the module globals are. */
+int sphg_time_integration(sphg_ctx* ctx, int maxtimestep, int* itimestep, double* time);
+
+/* Copy one phase back into the Fortran arrays (original particle order). */
+int sphg_download_phase(sphg_ctx* ctx, int phase, sphg_phase_host* v);
+
+/* Pair list of the last step as 1-based (i,j), sorted by i then j, as
+ * direct_find (m_particles.f90:938) / direct_find_2 (:1004) define it.
+ * Writes min(n, cap) pairs and the total count to *n. */
+int sphg_export_pairs(sphg_ctx* ctx, int which, int32_t* pair_i, int32_t* pair_j,
+                      int64_t cap, int64_t* n);
+
+/* Counters of the last step. */
+int sphg_stats(sphg_ctx* ctx, sphg_stats_t* out);
+
+/* Run the context's work on a caller-owned cudaStream_t (passed as void*);
+ * NULL restores the context's own stream. */
+int sphg_set_stream(sphg_ctx* ctx, void* cuda_stream);
+
+/* Per-kernel CUDA-event timing: enable=1 starts recording, 0 stops.
+ * sphg_kernel_report writes a JSON object {name: [launches, total_ms], ...}. */
+int sphg_kernel_profile(sphg_ctx* ctx, int enable);
+int sphg_kernel_report(sphg_ctx* ctx, char* buf, int64_t cap);
+
+void sphg_destroy(sphg_ctx* ctx);
+const char* sphg_strerror(int code);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SPHG_H */

@@ -1,0 +1,158 @@
+"""sources_b200 — B200 (sm_100a) two-phase SPH step of cwang2015/sources.
+
+The product is libsphg.so (C ABI, include/sphg.h).  This package is the
+Python host mirror of the reference's interface for the step: `Solver` owns
+one libsphg context and exposes the reference's entry points by name:
+
+    Solver.single_step(itimestep)         single_step / single_step_for_water /
+                                          single_step_for_soil (declarations_sph.f90:1131,1439,1530)
+    Solver.time_integration(maxtimestep)  time_integration / _for_water / _for_soil (:525,794,978)
+
+There is no CPU fallback: constructing a Solver without the built library or
+without a CUDA device raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+from .abi import (PhaseArrays, PhaseHost, Params, Stats, SPHG_FP32, SPHG_FP64, SPHG_PAIRS_CROSS,
+                  SPHG_PAIRS_FIRST, SPHG_PAIRS_SECOND, SPHG_SOIL, SPHG_WATER, default_params)
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsphg.so")
+
+# every entry point of include/sphg.h
+EXPORTS = ("sphg_default_params", "sphg_create", "sphg_upload_phase", "sphg_single_step",
+           "sphg_time_integration", "sphg_download_phase", "sphg_export_pairs", "sphg_stats",
+           "sphg_set_stream", "sphg_kernel_profile", "sphg_kernel_report", "sphg_destroy",
+           "sphg_strerror")
+
+_lib = None
+
+
+class SPHError(RuntimeError):
+    def __init__(self, code: int, where: str):
+        self.code = code
+        msg = load().sphg_strerror(code).decode() if _lib is not None else str(code)
+        super().__init__(f"{where}: {msg} (status {code})")
+
+
+def load(path: str = LIB_PATH):
+    """Load libsphg.so (built in-tree by sources_b200.build)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"libsphg.so not built ({path}); run python -m sources_b200.build")
+    L = C.CDLL(path)
+    P = C.c_void_p
+    L.sphg_default_params.argtypes = [C.POINTER(Params)]
+    L.sphg_default_params.restype = None
+    L.sphg_create.argtypes = [C.POINTER(Params), C.c_int, C.POINTER(P)]
+    L.sphg_upload_phase.argtypes = [P, C.c_int, C.POINTER(PhaseHost)]
+    L.sphg_single_step.argtypes = [P, C.c_int]
+    L.sphg_time_integration.argtypes = [P, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double)]
+    L.sphg_download_phase.argtypes = [P, C.c_int, C.POINTER(PhaseHost)]
+    L.sphg_export_pairs.argtypes = [P, C.c_int, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_int64,
+                                    C.POINTER(C.c_int64)]
+    L.sphg_stats.argtypes = [P, C.POINTER(Stats)]
+    L.sphg_set_stream.argtypes = [P, P]
+    L.sphg_kernel_profile.argtypes = [P, C.c_int]
+    L.sphg_kernel_report.argtypes = [P, C.c_char_p, C.c_int64]
+    L.sphg_destroy.argtypes = [P]
+    L.sphg_destroy.restype = None
+    L.sphg_strerror.argtypes = [C.c_int]
+    L.sphg_strerror.restype = C.c_char_p
+    _lib = L
+    return L
+
+
+def _check(rc: int, where: str):
+    if rc != 0:
+        raise SPHError(rc, where)
+
+
+class Solver:
+    """One libsphg context holding a Scene's phases on the GPU."""
+
+    def __init__(self, scene, params: Params | None = None):
+        self.L = load()
+        self.params = params if params is not None else scene.params
+        self.nphase = len(scene.phases)
+        self.meta = [(p.n, p.ntotal, p.material, p.dspp) for p in scene.phases]
+        h = C.c_void_p()
+        _check(self.L.sphg_create(C.byref(self.params), self.nphase, C.byref(h)), "sphg_create")
+        self.h = h
+        for k, P in enumerate(scene.phases):
+            self.upload(k + 1, P)
+        self.itimestep = 0
+        self.time = 0.0
+
+    def upload(self, phase: int, P: PhaseArrays):
+        _check(self.L.sphg_upload_phase(self.h, phase, C.byref(P.host_struct())), "sphg_upload_phase")
+
+    def single_step(self, itimestep: int):
+        _check(self.L.sphg_single_step(self.h, itimestep), "sphg_single_step")
+
+    def time_integration(self, maxtimestep: int):
+        it = C.c_int(self.itimestep)
+        t = C.c_double(self.time)
+        rc = self.L.sphg_time_integration(self.h, maxtimestep, C.byref(it), C.byref(t))
+        self.itimestep, self.time = it.value, t.value
+        _check(rc, "sphg_time_integration")
+
+    def download(self, phase: int, into: PhaseArrays | None = None, fields=None) -> PhaseArrays:
+        n, nt, mat, dspp = self.meta[phase - 1]
+        out = into if into is not None else PhaseArrays(n, nt, mat, dspp)
+        h = out.host_struct(fields)
+        _check(self.L.sphg_download_phase(self.h, phase, C.byref(h)), "sphg_download_phase")
+        out.nfail = h.nfail
+        return out
+
+    def pairs(self, which: int):
+        n = C.c_int64()
+        _check(self.L.sphg_export_pairs(self.h, which, None, None, 0, C.byref(n)), "sphg_export_pairs")
+        pi = np.zeros(max(n.value, 1), dtype=np.int32)
+        pj = np.zeros(max(n.value, 1), dtype=np.int32)
+        _check(self.L.sphg_export_pairs(self.h, which, pi.ctypes.data_as(C.POINTER(C.c_int32)),
+                                        pj.ctypes.data_as(C.POINTER(C.c_int32)), n.value, C.byref(n)),
+               "sphg_export_pairs")
+        return pi[:n.value], pj[:n.value]
+
+    def stats(self) -> Stats:
+        s = Stats()
+        _check(self.L.sphg_stats(self.h, C.byref(s)), "sphg_stats")
+        return s
+
+    def set_stream(self, stream_handle: int | None):
+        _check(self.L.sphg_set_stream(self.h, C.c_void_p(stream_handle or 0)), "sphg_set_stream")
+
+    def profile(self, enable: bool):
+        _check(self.L.sphg_kernel_profile(self.h, 1 if enable else 0), "sphg_kernel_profile")
+
+    def kernel_report(self) -> dict:
+        import json
+        buf = C.create_string_buffer(1 << 16)
+        _check(self.L.sphg_kernel_report(self.h, buf, len(buf)), "sphg_kernel_report")
+        return json.loads(buf.value.decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.sphg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

@@ -1,0 +1,839 @@
+// sphg_api.cu — context management, step orchestration and the C ABI of
+// libsphg (include/sphg.h).
+//
+// The engine is templated on the pair arithmetic T (double for SPHG_FP64,
+// float for SPHG_FP32).  One context owns one CUDA stream; every launch and
+// copy goes to that stream (or to a stream the caller sets).
+#include <cub/device/device_scan.cuh>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/sphg.h"
+#include "sphg_kernels.cuh"
+
+namespace {
+
+inline int blocks(long long n, int tpb) { return (int)((n + tpb - 1) / tpb); }
+
+struct Profiler {
+    bool on = false;
+    long long launches = 0;
+    struct Pending { const char* name; cudaEvent_t a, b; };
+    std::vector<Pending> pending;
+    std::map<std::string, std::pair<long long, double>> acc;
+    void resolve() {
+        for (auto& p : pending) {
+            float ms = 0.f;
+            cudaEventSynchronize(p.b);
+            cudaEventElapsedTime(&ms, p.a, p.b);
+            auto& e = acc[p.name];
+            e.first += 1;
+            e.second += ms;
+            cudaEventDestroy(p.a);
+            cudaEventDestroy(p.b);
+        }
+        pending.clear();
+    }
+};
+
+}  // namespace
+
+struct EngineBase {
+    virtual ~EngineBase() {}
+    virtual int upload(int phase, const sphg_phase_host* v) = 0;
+    virtual int download(int phase, sphg_phase_host* v) = 0;
+    virtual int rhs(int itimestep) = 0;
+    virtual int step(int itimestep) = 0;
+    virtual int begin_batch() = 0;
+    virtual int finish_batch() = 0;
+    virtual int export_pairs(int which, int32_t* pi, int32_t* pj, int64_t cap, int64_t* n) = 0;
+    virtual int stats(sphg_stats_t* out) = 0;
+};
+
+struct sphg_ctx {
+    sphg_params prm;
+    int nphase = 1;
+    int device = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    EngineBase* eng = nullptr;
+    Profiler prof;
+    int itimestep = 0;
+    double time = 0.0;
+    double last_step_ms = 0.0;
+};
+
+#define CUDA_TRY(x)                                        \
+    do {                                                   \
+        cudaError_t e_ = (x);                              \
+        if (e_ != cudaSuccess) {                           \
+            fprintf(stderr, "libsphg: %s failed: %s\n", #x, cudaGetErrorString(e_)); \
+            return SPHG_ERR_CUDA;                          \
+        }                                                  \
+    } while (0)
+
+template <typename T>
+struct Engine : EngineBase {
+    typedef typename V2<T>::t T2;
+    sphg_ctx* ctx;
+    PhaseDev<T> P[2];
+    bool have[2] = {false, false};
+    bool prepared = false;
+    bool aliased = false;        // a two-phase step overwrote the shared working arrays
+    GridGeom grid{};
+    SearchConst sc_same{}, sc_cross{};
+    int ncell = 0;
+    int* counts[2] = {nullptr, nullptr};
+    void* cub_tmp = nullptr;
+    size_t cub_bytes = 0;
+    DevCounters* cnt = nullptr;     // device
+    DevCounters hcnt{};             // host copy
+    int* sticky = nullptr;          // device: [overflow, nonfinite]
+    double* stage = nullptr;        // transfer staging, 2*nmax doubles
+    int* stage_i = nullptr;
+    long long* stage_l = nullptr;
+    void* spare[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};  // reorder scratch per phase: 4, 8, 16-byte elements
+    int nmax = 0;
+    std::vector<void*> allocs;
+    SimConst sim{};
+
+    explicit Engine(sphg_ctx* c) : ctx(c) { memset(P, 0, sizeof(P)); }
+    ~Engine() override {
+        for (void* p : allocs) cudaFree(p);
+    }
+
+    template <typename S>
+    int alloc(S** p, size_t count) {
+        void* q = nullptr;
+        CUDA_TRY(cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(S)));
+        CUDA_TRY(cudaMemsetAsync(q, 0, std::max<size_t>(count, 1) * sizeof(S), ctx->stream));
+        allocs.push_back(q);
+        *p = (S*)q;
+        return 0;
+    }
+    void release(void* p) {
+        if (!p) return;
+        auto it = std::find(allocs.begin(), allocs.end(), p);
+        if (it != allocs.end()) { cudaFree(p); allocs.erase(it); }
+    }
+
+    // ---------------------------------------------------------------- launch
+    template <typename K, typename... A>
+    int launch(const char* name, K kern, int grid_, int block, A... args) {
+        if (grid_ <= 0) return 0;
+        cudaEvent_t a = nullptr, b = nullptr;
+        if (ctx->prof.on) {
+            cudaEventCreate(&a); cudaEventCreate(&b);
+            cudaEventRecord(a, ctx->stream);
+        }
+        kern<<<grid_, block, 0, ctx->stream>>>(args...);
+        ctx->prof.launches++;
+        cudaError_t e = cudaGetLastError();
+        if (ctx->prof.on) {
+            cudaEventRecord(b, ctx->stream);
+            ctx->prof.pending.push_back({name, a, b});
+        }
+        if (e != cudaSuccess) {
+            fprintf(stderr, "libsphg: launch %s failed: %s\n", name, cudaGetErrorString(e));
+            return SPHG_ERR_CUDA;
+        }
+        return 0;
+    }
+
+    // ------------------------------------------------------------ constants
+    void make_sim(int itimestep) {
+        const sphg_params& p = ctx->prm;
+        SimConst& s = sim;
+        s.skf = p.skf; s.single_phase = p.single_phase; s.summation_density = p.summation_density;
+        s.average_velocity = p.average_velocity; s.visc_artificial = p.visc_artificial;
+        s.artificial_density = p.artificial_density; s.soil_artificial_stress = p.soil_artificial_stress;
+        s.volume_fraction = p.volume_fraction; s.water_artificial_volume = p.water_artificial_volume;
+        s.volume_fraction_renorm = p.volume_fraction_renorm; s.stress_integration = p.stress_integration;
+        s.plasticity = p.plasticity; s.yield_dp = p.yield_criterion == 2;
+        s.renorm_now = p.volume_fraction_renorm && p.renorm_interval > 0 && (itimestep % p.renorm_interval) == 0;
+        s.gravity = p.gravity; s.numeric_gravity = p.numeric_gravity;
+        s.alpha = p.alpha; s.beta = p.beta; s.etq = p.etq; s.dd = p.dd; s.p1 = p.p1; s.p2 = p.p2;
+        s.delta = p.delta; s.epsilon = p.epsilon; s.dt = p.dt;
+        s.w_rho0 = p.water.rho0; s.w_b = p.water.b; s.w_gamma = p.water.gamma; s.w_c = p.water.c; s.w_mu = p.water.viscosity;
+        s.s_rho0 = p.soil.rho0; s.s_k = p.soil.k; s.s_E = p.soil.E; s.s_niu = p.soil.niu; s.s_c = p.soil.c;
+        s.s_perm = p.soil.permeability; s.s_G = p.soil.G;
+        double t = tan(p.soil.phi);
+        s.s_alpha1 = t / sqrt(9.0 + 12.0 * (t * t));   // m_particles.f90:3338
+    }
+
+    static int scale_k(int skf) {
+        switch (skf) { case 1: return 2; case 2: return 3; case 3: return 3; case 4: return 2; }
+        return -1;
+    }
+
+    // smallest double t with sqrt(t) >= K: then sqrt(r2) < K  <=>  r2 < t
+    static double exact_threshold(double K) {
+        double t = K * K;
+        while (t > 0 && std::sqrt(t) >= K) t = std::nextafter(t, 0.0);
+        while (std::sqrt(t) < K) t = std::nextafter(t, INFINITY);
+        return t;
+    }
+
+    // ------------------------------------------------------------ allocation
+    int alloc_phase(int ph, int n) {
+        PhaseDev<T>& D = P[ph];
+        // a re-upload replaces the arrays
+        void* old[] = {D.x, D.v, D.v_min, D.rho, D.rho_min, D.vof, D.vof_min, D.p, D.c, D.mass, D.hsml, D.sxx, D.sxy,
+                       D.syy, D.sxx_min, D.sxy_min, D.syy_min, D.p_min, D.eps_p, D.itype, D.orig, D.fail, D.drho,
+                       D.dvof, D.dsxx, D.dsxy, D.dsyy, D.dp, D.txx, D.txy, D.tyy, D.vcc, D.wxy, D.vof2, D.dv, D.av,
+                       D.countiac, D.cell_id, D.cell_fill, D.perm, D.xs, D.hs, D.recA, D.recA2, D.recB};
+        for (void* p : old) release(p);
+        for (int t = 0; t < 3; ++t) { release(spare[ph][t]); spare[ph][t] = nullptr; }
+        memset(&D, 0, sizeof(D));
+        D.n = n;
+        size_t N = (size_t)n;
+        int rc = 0;
+        rc |= alloc(&D.x, N); rc |= alloc(&D.v, N); rc |= alloc(&D.v_min, N);
+        rc |= alloc(&D.rho, N); rc |= alloc(&D.rho_min, N); rc |= alloc(&D.vof, N); rc |= alloc(&D.vof_min, N);
+        rc |= alloc(&D.p, N); rc |= alloc(&D.c, N); rc |= alloc(&D.mass, N); rc |= alloc(&D.hsml, N);
+        rc |= alloc(&D.sxx, N); rc |= alloc(&D.sxy, N); rc |= alloc(&D.syy, N);
+        rc |= alloc(&D.sxx_min, N); rc |= alloc(&D.sxy_min, N); rc |= alloc(&D.syy_min, N); rc |= alloc(&D.p_min, N);
+        rc |= alloc(&D.eps_p, N);
+        rc |= alloc(&D.itype, N); rc |= alloc(&D.orig, N); rc |= alloc(&D.fail, N);
+        rc |= alloc(&D.drho, N); rc |= alloc(&D.dvof, N); rc |= alloc(&D.dsxx, N); rc |= alloc(&D.dsxy, N);
+        rc |= alloc(&D.dsyy, N); rc |= alloc(&D.dp, N); rc |= alloc(&D.txx, N); rc |= alloc(&D.txy, N);
+        rc |= alloc(&D.tyy, N); rc |= alloc(&D.vcc, N); rc |= alloc(&D.wxy, N); rc |= alloc(&D.vof2, N);
+        rc |= alloc(&D.dv, N); rc |= alloc(&D.av, N);
+        rc |= alloc(&D.countiac, N); rc |= alloc(&D.cell_id, N); rc |= alloc(&D.cell_fill, N); rc |= alloc(&D.perm, N);
+        rc |= alloc(&D.xs, N); rc |= alloc(&D.hs, N);
+        rc |= alloc(&D.recA, N); rc |= alloc(&D.recA2, N); rc |= alloc(&D.recB, N);
+        rc |= alloc((char**)&spare[ph][0], 4 * N); rc |= alloc((char**)&spare[ph][1], 8 * N);
+        rc |= alloc((char**)&spare[ph][2], 16 * N);
+        if (rc) return SPHG_ERR_CUDA;
+        if (n > nmax) {
+            release(stage); release(stage_i); release(stage_l);
+            nmax = n;
+            if (alloc(&stage, 2 * (size_t)n) || alloc(&stage_i, (size_t)n) || alloc(&stage_l, (size_t)n + 1))
+                return SPHG_ERR_CUDA;
+        }
+        if (!cnt) {
+            if (alloc(&cnt, 1) || alloc(&sticky, 4)) return SPHG_ERR_CUDA;
+        }
+        return 0;
+    }
+
+    int upload(int phase, const sphg_phase_host* h) override {
+        if (phase < 1 || phase > ctx->nphase || !h) return SPHG_ERR_BAD_ARG;
+        if (!h->x || !h->vx || !h->rho || !h->p || !h->c || !h->mass || !h->hsml || !h->itype) return SPHG_ERR_BAD_ARG;
+        int n = h->ntotal + h->nvirt;
+        if (n <= 0 || h->ntotal < 0 || h->nvirt < 0) return SPHG_ERR_BAD_ARG;
+        int ph = phase - 1;
+        int rc = alloc_phase(ph, n);
+        if (rc) return rc;
+        PhaseDev<T>& D = P[ph];
+        D.ntotal = h->ntotal; D.material = h->material; D.dspp = h->dspp;
+        // original order == state order until the first reorder
+        if ((rc = launch("iota", k_iota, blocks(n, 256), 256, n, D.orig))) return rc;
+        rc |= put_state(n, h->x, (double*)D.x, 2); rc |= put_state(n, h->vx, (double*)D.v, 2);
+        rc |= put_state(n, h->v_min, (double*)D.v_min, 2);
+        rc |= put_state(n, h->rho, D.rho, 1); rc |= put_state(n, h->rho_min, D.rho_min, 1);
+        rc |= put_state(n, h->vof, D.vof, 1); rc |= put_state(n, h->vof_min, D.vof_min, 1);
+        rc |= put_state(n, h->p, D.p, 1); rc |= put_state(n, h->c, D.c, 1); rc |= put_state(n, h->mass, D.mass, 1);
+        rc |= put_state(n, h->hsml, D.hsml, 1);
+        rc |= put_state(n, h->sxx, D.sxx, 1); rc |= put_state(n, h->sxy, D.sxy, 1); rc |= put_state(n, h->syy, D.syy, 1);
+        rc |= put_state(n, h->sxx_min, D.sxx_min, 1); rc |= put_state(n, h->sxy_min, D.sxy_min, 1);
+        rc |= put_state(n, h->syy_min, D.syy_min, 1); rc |= put_state(n, h->p_min, D.p_min, 1);
+        rc |= put_state(n, h->epsilon_p, D.eps_p, 1);
+        rc |= put_rate(n, h->drho, D.drho, 1); rc |= put_rate(n, h->dvof, D.dvof, 1);
+        rc |= put_rate(n, h->dsxx, D.dsxx, 1); rc |= put_rate(n, h->dsxy, D.dsxy, 1); rc |= put_rate(n, h->dsyy, D.dsyy, 1);
+        rc |= put_rate(n, h->dp, D.dp, 1); rc |= put_rate(n, h->dvx, (T*)D.dv, 2); rc |= put_rate(n, h->av, (T*)D.av, 2);
+        rc |= put_rate(n, h->vof2, D.vof2, 1); rc |= put_rate(n, h->vcc, D.vcc, 1);
+        rc |= put_rate(n, h->txx, D.txx, 1); rc |= put_rate(n, h->tyy, D.tyy, 1); rc |= put_rate(n, h->txy, D.txy, 1);
+        if (rc) return SPHG_ERR_CUDA;
+        CUDA_TRY(cudaMemcpyAsync(D.itype, h->itype, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, ctx->stream));
+        have[ph] = true;
+        prepared = false;
+        aliased = false;
+        CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        return 0;
+    }
+
+    int put_state(int n, const double* src, double* dst, int comps) {
+        if (!src) { CUDA_TRY(cudaMemsetAsync(dst, 0, sizeof(double) * (size_t)n * comps, ctx->stream)); return 0; }
+        CUDA_TRY(cudaMemcpyAsync(dst, src, sizeof(double) * (size_t)n * comps, cudaMemcpyHostToDevice, ctx->stream));
+        return 0;
+    }
+    int put_rate(int n, const double* src, T* dst, int comps) {
+        if (!src) { CUDA_TRY(cudaMemsetAsync(dst, 0, sizeof(T) * (size_t)n * comps, ctx->stream)); return 0; }
+        if (sizeof(T) == sizeof(double)) {
+            CUDA_TRY(cudaMemcpyAsync(dst, src, sizeof(double) * (size_t)n * comps, cudaMemcpyHostToDevice, ctx->stream));
+            return 0;
+        }
+        CUDA_TRY(cudaMemcpyAsync(stage, src, sizeof(double) * (size_t)n * comps, cudaMemcpyHostToDevice, ctx->stream));
+        // identity order: the phase was just uploaded, orig == iota
+        return launch("upload_convert", k_from_original<T>, blocks(n, 256), 256, n, (const int*)P_orig_identity(n),
+                      (const double*)stage, dst, comps);
+    }
+    const int* P_orig_identity(int n) {
+        // stage_i holds an identity map, rebuilt on demand
+        launch("iota", k_iota, blocks(n, 256), 256, n, stage_i);
+        return stage_i;
+    }
+
+    // -------------------------------------------------------------- prepare
+    // Grid and search constants, once every phase is on the device.
+    int prepare() {
+        if (prepared) return 0;
+        for (int ph = 0; ph < ctx->nphase; ++ph) if (!have[ph]) return SPHG_ERR_STATE;
+        const sphg_params& p = ctx->prm;
+        int sk = scale_k(p.skf);
+        if (sk < 0) return SPHG_ERR_BAD_KERNEL;
+        // h range over all phases (read back once)
+        double hmin = INFINITY, hmax = 0.0;
+        for (int ph = 0; ph < ctx->nphase; ++ph) {
+            std::vector<double> h((size_t)P[ph].n);
+            CUDA_TRY(cudaMemcpyAsync(h.data(), P[ph].hsml, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, ctx->stream));
+            CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+            for (double v : h) {
+                if (!(v > 0.0) || !std::isfinite(v)) return SPHG_ERR_BAD_ARG;
+                hmin = std::min(hmin, v); hmax = std::max(hmax, v);
+            }
+        }
+        double cell = sk * hmax * (1.0 + 1e-6);
+        if (!(p.x_max > p.x_min) || !(p.y_max > p.y_min)) return SPHG_ERR_BAD_ARG;
+        double ncx = std::ceil((p.x_max - p.x_min) / cell) + 1, ncy = std::ceil((p.y_max - p.y_min) / cell) + 1;
+        if (ncx * ncy > 2.0e8) return SPHG_ERR_BAD_ARG;
+        grid.ncx = (int)ncx; grid.ncy = (int)ncy; grid.x0 = p.x_min; grid.y0 = p.y_min; grid.inv = 1.0 / cell;
+        int nc = grid.ncx * grid.ncy;
+        if (nc != ncell) {
+            for (int ph = 0; ph < 2; ++ph) { release(counts[ph]); counts[ph] = nullptr; }
+            release(cub_tmp); cub_tmp = nullptr;
+            ncell = nc;
+        }
+        for (int ph = 0; ph < ctx->nphase; ++ph) {
+            if (!counts[ph] && alloc(&counts[ph], (size_t)nc + 1)) return SPHG_ERR_CUDA;
+            release(P[ph].cell_start);
+            if (alloc(&P[ph].cell_start, (size_t)nc + 1)) return SPHG_ERR_CUDA;
+        }
+        if (!cub_tmp) {
+            size_t bytes = 0;
+            cub::DeviceScan::ExclusiveSum(nullptr, bytes, counts[0], P[0].cell_start, nc + 1, ctx->stream);
+            size_t b2 = 0;
+            cub::DeviceScan::ExclusiveSum(nullptr, b2, (long long*)nullptr, (long long*)nullptr, nmax + 1, ctx->stream);
+            cub_bytes = std::max(bytes, b2);
+            if (alloc((char**)&cub_tmp, cub_bytes)) return SPHG_ERR_CUDA;
+        }
+        bool uniform = hmin == hmax;
+        double K = sk * hmax;
+        sc_same.scale_k = sk; sc_same.uniform = uniform; sc_same.r2_uniform = uniform ? exact_threshold(K) : 0.0;
+        sc_cross = sc_same;
+        prepared = true;
+        // spatial order from the start
+        for (int ph = 0; ph < ctx->nphase; ++ph) {
+            int rc = build_cells(ph);
+            if (rc) return rc;
+            if ((rc = reorder(ph))) return rc;
+        }
+        return 0;
+    }
+
+    int build_cells(int ph) {
+        PhaseDev<T>& D = P[ph];
+        CUDA_TRY(cudaMemsetAsync(counts[ph], 0, sizeof(int) * ((size_t)ncell + 1), ctx->stream));
+        int rc = launch("cell_count", k_cell_count, blocks(D.n, 256), 256, (const double2*)D.x, D.n, grid, D.cell_id,
+                        D.cell_fill, counts[ph], cnt);
+        if (rc) return rc;
+        size_t bytes = cub_bytes;
+        CUDA_TRY(cub::DeviceScan::ExclusiveSum(cub_tmp, bytes, counts[ph], D.cell_start, ncell + 1, ctx->stream));
+        if ((rc = launch("cell_scatter", k_cell_scatter, blocks(D.n, 256), 256, D.n, (const int*)D.cell_id,
+                         (const int*)D.cell_fill, (const int*)D.cell_start, D.perm)))
+            return rc;
+        return launch("cell_sort", k_cell_sort, blocks(ncell, 256), 256, ncell, (const int*)D.cell_start,
+                      (const int*)D.orig, D.perm);
+    }
+
+    // Gather field f into the phase's spare buffer of the same element size,
+    // then swap the two: the old field buffer becomes the spare.
+    template <typename S>
+    int permute_field(int ph, const int* perm, S*& f) {
+        static_assert(sizeof(S) == 4 || sizeof(S) == 8 || sizeof(S) == 16, "element size");
+        const int slot = sizeof(S) == 4 ? 0 : (sizeof(S) == 8 ? 1 : 2);
+        S* dst = (S*)spare[ph][slot];
+        int rc = launch("reorder", k_permute<S>, blocks(P[ph].n, 256), 256, P[ph].n, perm, (const S*)f, dst);
+        if (rc) return rc;
+        spare[ph][slot] = (void*)f;
+        f = dst;
+        return 0;
+    }
+
+    // Permute the persistent state into the current cell order.
+    int reorder(int ph) {
+        PhaseDev<T>& D = P[ph];
+        const int* perm = D.perm;
+        int n = D.n, rc = 0;
+        rc |= permute_field(ph, perm, D.x); rc |= permute_field(ph, perm, D.v); rc |= permute_field(ph, perm, D.v_min);
+        rc |= permute_field(ph, perm, D.rho); rc |= permute_field(ph, perm, D.rho_min);
+        rc |= permute_field(ph, perm, D.vof); rc |= permute_field(ph, perm, D.vof_min);
+        rc |= permute_field(ph, perm, D.p); rc |= permute_field(ph, perm, D.c); rc |= permute_field(ph, perm, D.mass);
+        rc |= permute_field(ph, perm, D.hsml);
+        rc |= permute_field(ph, perm, D.sxx); rc |= permute_field(ph, perm, D.sxy); rc |= permute_field(ph, perm, D.syy);
+        rc |= permute_field(ph, perm, D.sxx_min); rc |= permute_field(ph, perm, D.sxy_min);
+        rc |= permute_field(ph, perm, D.syy_min); rc |= permute_field(ph, perm, D.p_min);
+        rc |= permute_field(ph, perm, D.eps_p);
+        rc |= permute_field(ph, perm, D.itype); rc |= permute_field(ph, perm, D.orig); rc |= permute_field(ph, perm, D.fail);
+        rc |= permute_field(ph, perm, D.drho); rc |= permute_field(ph, perm, D.dvof);
+        rc |= permute_field(ph, perm, D.dsxx); rc |= permute_field(ph, perm, D.dsxy); rc |= permute_field(ph, perm, D.dsyy);
+        rc |= permute_field(ph, perm, D.dp); rc |= permute_field(ph, perm, D.dv); rc |= permute_field(ph, perm, D.av);
+        rc |= permute_field(ph, perm, D.txx); rc |= permute_field(ph, perm, D.txy); rc |= permute_field(ph, perm, D.tyy);
+        rc |= permute_field(ph, perm, D.vcc); rc |= permute_field(ph, perm, D.wxy); rc |= permute_field(ph, perm, D.vof2);
+        rc |= permute_field(ph, perm, D.countiac);
+        if (rc) return rc;
+        return launch("iota", k_iota, blocks(n, 256), 256, n, D.perm);
+    }
+
+    // -------------------------------------------------------------- the step
+    int reset_counters() {
+        DevCounters z;
+        memset(&z, 0, sizeof(z));
+        for (int i = 0; i < 2; ++i) { z.miniac[i] = 0x7fffffff; }
+        CUDA_TRY(cudaMemcpyAsync(cnt, &z, sizeof(z), cudaMemcpyHostToDevice, ctx->stream));
+        return 0;
+    }
+
+    // single_step / single_step_for_water / single_step_for_soil
+    int rhs(int itimestep) override {
+        int rc = prepare();
+        if (rc) return rc;
+        make_sim(itimestep);
+        if ((rc = reset_counters())) return rc;
+        const sphg_params& p = ctx->prm;
+        bool reorder_now = p.reorder_interval > 0 && itimestep > 0 && itimestep % p.reorder_interval == 0;
+        for (int ph = 0; ph < ctx->nphase; ++ph) {
+            if ((rc = build_cells(ph))) return rc;
+            if (reorder_now && (rc = reorder(ph))) return rc;
+        }
+        const int tpb = SPHG_TPB;
+        if (p.single_phase) {
+            PhaseDev<T>& D = P[0];
+            if (D.material == SPHG_WATER) {
+                if ((rc = launch("gather", k_gather<T>, blocks(D.n, 256), 256, D, sim, 0, 0, cnt))) return rc;
+                if ((rc = launch("water_sum", k_water_sum<T>, blocks(D.n, tpb), tpb, D, grid, sc_same, sim, cnt))) return rc;
+                if ((rc = launch("water_pass_a", k_water_pass_a<T, true>, blocks(D.n, tpb), tpb, D, grid, sc_same, sim, cnt))) return rc;
+                if ((rc = launch("water_pass_b", k_water_pass_b<T, true>, blocks(D.n, tpb), tpb, D, grid, sc_same, sim))) return rc;
+            } else {
+                if ((rc = launch("gather", k_gather<T>, blocks(D.n, 256), 256, D, sim, 1, sim.yield_dp, cnt))) return rc;
+                if (sim.plasticity == 3) CUDA_TRY(cudaMemsetAsync(&cnt->nfail, 0, sizeof(int), ctx->stream));
+                if ((rc = launch("soil_pass", k_soil_pass<T, true>, blocks(D.n, tpb), tpb, D, grid, sc_same, sim, cnt, 0))) return rc;
+            }
+        } else {
+            PhaseDev<T>& W = P[0];
+            PhaseDev<T>& S = P[1];
+            if ((rc = launch("gather", k_gather<T>, blocks(W.n, 256), 256, W, sim, 0, 0, cnt))) return rc;
+            if ((rc = launch("gather", k_gather<T>, blocks(S.n, 256), 256, S, sim, 1, sim.yield_dp, cnt))) return rc;
+            if ((rc = launch("water_pass_a", k_water_pass_a<T, false>, blocks(W.n, tpb), tpb, W, grid, sc_same, sim, cnt))) return rc;
+            if ((rc = launch("water_pass_b", k_water_pass_b<T, false>, blocks(W.n, tpb), tpb, W, grid, sc_same, sim))) return rc;
+            if (sim.plasticity == 3) CUDA_TRY(cudaMemsetAsync(&cnt->nfail, 0, sizeof(int), ctx->stream));
+            if ((rc = launch("soil_pass", k_soil_pass<T, false>, blocks(S.n, tpb), tpb, S, grid, sc_same, sim, cnt, 1))) return rc;
+            if ((rc = launch("cross_soil", k_cross_soil<T>, blocks(S.n, tpb), tpb, S, W, grid, sc_cross, sim))) return rc;
+            if ((rc = launch("cross_water", k_cross_water<T>, blocks(W.n, tpb), tpb, W, S, grid, sc_cross, sim, cnt))) return rc;
+            aliased = true;
+        }
+        return launch("check", k_check, 1, 32, (const DevCounters*)cnt, sticky, (unsigned long long)p.max_interaction);
+    }
+
+    // one leapfrog step of time_integration / _for_water / _for_soil
+    int step(int itimestep) override {
+        int rc = prepare();
+        if (rc) return rc;
+        make_sim(itimestep);
+        const bool two = !ctx->prm.single_phase;
+        const int first = itimestep == 1;
+        if (!first) {
+            for (int ph = 0; ph < ctx->nphase; ++ph) {
+                PhaseDev<T>& D = P[ph];
+                int dp = D.material == SPHG_SOIL && sim.yield_dp;
+                if (dp) CUDA_TRY(cudaMemsetAsync(&cnt->nfail, 0, sizeof(int), ctx->stream));
+                if ((rc = launch("first_half", k_first_half<T>, blocks(D.n, 256), 256, D, sim, two ? 1 : 0, dp, cnt))) return rc;
+            }
+        }
+        if ((rc = rhs(itimestep))) return rc;
+        for (int ph = 0; ph < ctx->nphase; ++ph) {
+            PhaseDev<T>& D = P[ph];
+            int dp = D.material == SPHG_SOIL && sim.yield_dp;
+            if (dp) CUDA_TRY(cudaMemsetAsync(&cnt->nfail, 0, sizeof(int), ctx->stream));
+            if ((rc = launch("update", k_update<T>, blocks(D.n, 256), 256, D, sim, first, two ? 1 : 0, dp, cnt))) return rc;
+        }
+        return 0;
+    }
+
+    int begin_batch() override {
+        if (!sticky) return 0;
+        CUDA_TRY(cudaMemsetAsync(sticky, 0, 4 * sizeof(int), ctx->stream));
+        return 0;
+    }
+
+    // read counters and the sticky flags after a batch
+    int finish_batch() override {
+        int hs[4];
+        CUDA_TRY(cudaMemcpyAsync(&hcnt, cnt, sizeof(hcnt), cudaMemcpyDeviceToHost, ctx->stream));
+        CUDA_TRY(cudaMemcpyAsync(hs, sticky, sizeof(hs), cudaMemcpyDeviceToHost, ctx->stream));
+        CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        if (hs[1]) return SPHG_ERR_NONFINITE;
+        if (hs[0]) return SPHG_ERR_PAIR_OVERFLOW;
+        return 0;
+    }
+
+    // ------------------------------------------------------------- download
+    template <typename S>
+    int get(int n, const int* orig, const S* src, double* dst, int comps) {
+        if (!dst) return 0;
+        int rc = launch("download", k_to_original<S>, blocks(n, 256), 256, n, orig, src, stage, comps);
+        if (rc) return rc;
+        CUDA_TRY(cudaMemcpyAsync(dst, stage, sizeof(double) * (size_t)n * comps, cudaMemcpyDeviceToHost, ctx->stream));
+        return 0;
+    }
+
+    int download(int phase, sphg_phase_host* h) override {
+        if (phase < 1 || phase > ctx->nphase || !h) return SPHG_ERR_BAD_ARG;
+        int ph = phase - 1;
+        if (!have[ph]) return SPHG_ERR_STATE;
+        PhaseDev<T>& D = P[ph];
+        int n = D.n, rc = 0;
+        const int* o = D.orig;
+        h->ntotal = D.ntotal; h->nvirt = n - D.ntotal; h->material = D.material; h->dspp = D.dspp;
+        rc |= get(n, o, (const double*)D.x, h->x, 2); rc |= get(n, o, (const double*)D.v, h->vx, 2);
+        rc |= get(n, o, (const double*)D.v_min, h->v_min, 2);
+        rc |= get(n, o, (const T*)D.dv, h->dvx, 2); rc |= get(n, o, (const T*)D.av, h->av, 2);
+        rc |= get(n, o, (const double*)D.rho, h->rho, 1); rc |= get(n, o, (const double*)D.rho_min, h->rho_min, 1);
+        rc |= get(n, o, (const T*)D.drho, h->drho, 1); rc |= get(n, o, (const double*)D.p, h->p, 1);
+        rc |= get(n, o, (const double*)D.c, h->c, 1); rc |= get(n, o, (const double*)D.mass, h->mass, 1);
+        rc |= get(n, o, (const double*)D.hsml, h->hsml, 1);
+        rc |= get(n, o, (const double*)D.vof, h->vof, 1); rc |= get(n, o, (const double*)D.vof_min, h->vof_min, 1);
+        rc |= get(n, o, (const T*)D.dvof, h->dvof, 1); rc |= get(n, o, (const T*)D.vof2, h->vof2, 1);
+        rc |= get(n, o, (const T*)D.dsxx, h->dsxx, 1); rc |= get(n, o, (const T*)D.dsxy, h->dsxy, 1);
+        rc |= get(n, o, (const T*)D.dsyy, h->dsyy, 1); rc |= get(n, o, (const T*)D.dp, h->dp, 1);
+        rc |= get(n, o, (const double*)D.sxx_min, h->sxx_min, 1); rc |= get(n, o, (const double*)D.sxy_min, h->sxy_min, 1);
+        rc |= get(n, o, (const double*)D.syy_min, h->syy_min, 1); rc |= get(n, o, (const double*)D.p_min, h->p_min, 1);
+        rc |= get(n, o, (const double*)D.eps_p, h->epsilon_p, 1); rc |= get(n, o, (const T*)D.vcc, h->vcc, 1);
+        if (D.material == SPHG_SOIL) {
+            rc |= get(n, o, (const double*)D.sxx, h->sxx, 1); rc |= get(n, o, (const double*)D.sxy, h->sxy, 1);
+            rc |= get(n, o, (const double*)D.syy, h->syy, 1);
+            rc |= get(n, o, (const T*)D.txx, h->txx, 1); rc |= get(n, o, (const T*)D.tyy, h->tyy, 1);
+            rc |= get(n, o, (const T*)D.txy, h->txy, 1);
+        } else {
+            // water stress lives in the shared working arrays (sxx => txx, ...)
+            double* xx[2] = {h->sxx, h->txx};
+            double* yy[2] = {h->syy, h->tyy};
+            double* xy[2] = {h->sxy, h->txy};
+            for (int t = 0; t < 2; ++t) {
+                rc |= get(n, o, (const double*)D.sxx, xx[t], 1);
+                rc |= get(n, o, (const double*)D.syy, yy[t], 1);
+                rc |= get(n, o, (const double*)D.sxy, xy[t], 1);
+            }
+        }
+        if (h->itype) {
+            rc |= launch("download", k_to_original_i, blocks(n, 256), 256, n, o, (const int*)D.itype, stage_i);
+            CUDA_TRY(cudaMemcpyAsync(h->itype, stage_i, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
+        }
+        if (h->fail) {
+            rc |= launch("download", k_to_original_i, blocks(n, 256), 256, n, o, (const int*)D.fail, stage_i);
+            CUDA_TRY(cudaMemcpyAsync(h->fail, stage_i, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
+        }
+        CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        if (rc) return SPHG_ERR_CUDA;
+        // Cross-phase aliasing of the working arrays (declarations_sph.f90:371-377,
+        // 414-415): after a two-phase step the soil pass has overwritten the first
+        // n_soil entries of txx/tyy with soil strain rates and all of txy with
+        // the soil spin (zero beyond n_soil, Jaumann_rate m_particles.f90:3077).
+        if (D.material == SPHG_WATER && ctx->nphase == 2 && aliased) {
+            PhaseDev<T>& S = P[1];
+            int ns = S.n;
+            std::vector<double> t((size_t)ns);
+            const T* src[3] = {S.txx, S.tyy, S.txy};
+            double* dxx[3][2] = {{h->sxx, h->txx}, {h->syy, h->tyy}, {h->sxy, h->txy}};
+            for (int f = 0; f < 3; ++f) {
+                bool want = dxx[f][0] || dxx[f][1];
+                if (!want) continue;
+                if (get(ns, S.orig, src[f], t.data(), 1)) return SPHG_ERR_CUDA;
+                CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+                for (int s = 0; s < 2; ++s) {
+                    double* d = dxx[f][s];
+                    if (!d) continue;
+                    for (int i = 0; i < n; ++i) d[i] = i < ns ? t[(size_t)i] : (f == 2 ? 0.0 : d[i]);
+                }
+            }
+        }
+        h->nfail = hcnt.nfail;
+        return 0;
+    }
+
+    // ----------------------------------------------------------- pair export
+    int export_pairs(int which, int32_t* pi, int32_t* pj, int64_t cap, int64_t* nout) override {
+        if (which < 0 || which > 2 || !nout) return SPHG_ERR_BAD_ARG;
+        if (which == 1 && ctx->nphase < 2) return SPHG_ERR_BAD_ARG;
+        if (which == 2 && ctx->nphase < 2) return SPHG_ERR_BAD_ARG;
+        int rc = prepare();
+        if (rc) return rc;
+        int a = which == 1 ? 1 : 0;
+        int b = which == 2 ? 1 : a;
+        PhaseDev<T>& A = P[a];
+        PhaseDev<T>& B = P[b];
+        // the lists of the current positions (the last step's pair search if no
+        // step ran since): rebuild sorted positions for both phases
+        for (int ph = 0; ph < ctx->nphase; ++ph) {
+            if ((rc = build_cells(ph))) return rc;
+            if ((rc = launch("gather", k_gather<T>, blocks(P[ph].n, 256), 256, P[ph], sim, 0, 0, cnt))) return rc;
+        }
+        int n = A.n;
+        int* count = stage_i;
+        long long* off = stage_l;
+        if ((rc = launch("pairs_count", k_pairs_count, blocks(n, SPHG_TPB), SPHG_TPB, n, (const int*)A.perm, (const int*)A.orig,
+                         (const double2*)A.xs, (const double*)A.hs, grid, which == 2 ? sc_cross : sc_same,
+                         (const int*)B.cell_start, (const double2*)B.xs, (const double*)B.hs, (const int*)B.perm,
+                         (const int*)B.orig, which == 2 ? 1 : 0, count, 0, (const long long*)nullptr, (int*)nullptr,
+                         (int*)nullptr, 0LL)))
+            return rc;
+        // exclusive scan of counts (as long long) in original-index order
+        std::vector<int> hc((size_t)n);
+        CUDA_TRY(cudaMemcpyAsync(hc.data(), count, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
+        CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        std::vector<long long> ho((size_t)n + 1, 0);
+        for (int i = 0; i < n; ++i) ho[(size_t)i + 1] = ho[(size_t)i] + hc[(size_t)i];
+        long long total = ho[(size_t)n];
+        *nout = total;
+        long long ncopy = std::min<long long>(total, cap);
+        if (ncopy <= 0 || !pi || !pj) return 0;
+        CUDA_TRY(cudaMemcpyAsync(off, ho.data(), sizeof(long long) * ((size_t)n + 1), cudaMemcpyHostToDevice, ctx->stream));
+        int *di = nullptr, *dj = nullptr;
+        CUDA_TRY(cudaMalloc(&di, sizeof(int) * (size_t)ncopy));
+        CUDA_TRY(cudaMalloc(&dj, sizeof(int) * (size_t)ncopy));
+        rc = launch("pairs_write", k_pairs_count, blocks(n, SPHG_TPB), SPHG_TPB, n, (const int*)A.perm, (const int*)A.orig,
+                    (const double2*)A.xs, (const double*)A.hs, grid, which == 2 ? sc_cross : sc_same,
+                    (const int*)B.cell_start, (const double2*)B.xs, (const double*)B.hs, (const int*)B.perm,
+                    (const int*)B.orig, which == 2 ? 1 : 0, count, 1, (const long long*)off, di, dj, ncopy);
+        cudaError_t e1 = cudaMemcpyAsync(pi, di, sizeof(int) * (size_t)ncopy, cudaMemcpyDeviceToHost, ctx->stream);
+        cudaError_t e2 = cudaMemcpyAsync(pj, dj, sizeof(int) * (size_t)ncopy, cudaMemcpyDeviceToHost, ctx->stream);
+        cudaError_t e3 = cudaStreamSynchronize(ctx->stream);
+        cudaFree(di);
+        cudaFree(dj);
+        if (rc) return rc;
+        if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) return SPHG_ERR_CUDA;
+        return 0;
+    }
+
+    int stats(sphg_stats_t* out) override {
+        int rc = finish_batch();
+        memset(out, 0, sizeof(*out));
+        out->niac[0] = (int64_t)(hcnt.pairs[0] / 2);
+        out->niac[1] = (int64_t)(hcnt.pairs[1] / 2);
+        out->niac[2] = (int64_t)hcnt.pairs[2];
+        for (int i = 0; i < 2; ++i) {
+            out->maxiac[i] = hcnt.maxiac[i];
+            out->miniac[i] = hcnt.miniac[i] == 0x7fffffff ? 0 : hcnt.miniac[i];
+            out->noiac[i] = hcnt.noiac[i];
+        }
+        out->nfail = hcnt.nfail;
+        out->n_out_of_domain = hcnt.n_out;
+        out->itimestep = ctx->itimestep;
+        out->time = ctx->time;
+        out->last_step_ms = ctx->last_step_ms;
+        return rc == SPHG_ERR_CUDA ? rc : 0;
+    }
+};
+
+// ============================================================== C ABI
+extern "C" {
+
+void sphg_default_params(sphg_params* p) {
+    if (!p) return;
+    memset(p, 0, sizeof(*p));
+    p->abi_version = SPHG_ABI_VERSION;
+    p->dim = 2;
+    p->skf = 4;                      // m_particles.f90:141
+    p->first_material = SPHG_WATER;
+    p->average_velocity = 1;         // param.f90:80
+    p->visc_artificial = 1;          // :86
+    p->artificial_density = 1;       // :95
+    p->soil_artificial_stress = 1;   // :96
+    p->volume_fraction = 1;          // :98
+    p->water_artificial_volume = 1;  // :99
+    p->volume_fraction_renorm = 1;   // :100
+    p->stress_integration = 1;       // :92
+    p->yield_criterion = 2;          // :93
+    p->plasticity = 3;               // :94
+    p->integrate_scheme = 1;         // :78
+    p->precision = SPHG_FP64;
+    p->reorder_interval = 10;
+    p->renorm_interval = 40;         // declarations_sph.f90:1415
+    p->gravity = (double)-9.8f;      // declarations_sph.f90:13 (default-real literal)
+    p->numeric_gravity = (double)-9.8f;  // m_particles.f90:40
+    p->alpha = 0.1; p->beta = 0.0; p->etq = 0.1;  // :44
+    p->dd = 0.1; p->p1 = 12; p->p2 = 4;          // :47
+    p->delta = 0.1;                              // :50
+    p->epsilon = (double)0.001f;                 // :53
+    p->x_min = -10.0; p->x_max = 10.0; p->y_min = -10.0; p->y_max = 10.0;  // param.f90:23-25
+    p->max_interaction = 10 * 2000;              // param.f90:14
+}
+
+static int validate(const sphg_params* p, int n_phase) {
+    if (!p || (n_phase != 1 && n_phase != 2)) return SPHG_ERR_BAD_ARG;
+    if (p->abi_version != SPHG_ABI_VERSION || p->dim != 2) return SPHG_ERR_BAD_ARG;
+    if (p->skf < 1 || p->skf > 4) return SPHG_ERR_BAD_KERNEL;
+    if ((p->single_phase != 0) != (n_phase == 1)) return SPHG_ERR_BAD_ARG;
+    if (p->single_phase && p->first_material != SPHG_WATER && p->first_material != SPHG_SOIL) return SPHG_ERR_BAD_ARG;
+    if (p->precision != SPHG_FP64 && p->precision != SPHG_FP32) return SPHG_ERR_BAD_ARG;
+    // outside the implemented scope: Verlet (param.f90:78 = 2), Mohr-Coulomb
+    // (yield_criterion = 1), flow rules 1 and 2, summation density for soil
+    if (p->integrate_scheme != 1) return SPHG_ERR_UNSUPPORTED;
+    if (p->yield_criterion != 2 && p->yield_criterion != 0) return SPHG_ERR_UNSUPPORTED;
+    if (p->plasticity != 3 && p->plasticity != 0) return SPHG_ERR_UNSUPPORTED;
+    if (p->stress_integration != 1 && p->stress_integration != 2) return SPHG_ERR_UNSUPPORTED;
+    if (p->summation_density && !(p->single_phase && p->first_material == SPHG_WATER)) return SPHG_ERR_UNSUPPORTED;
+    if (!(p->dt > 0.0) || p->max_interaction <= 0) return SPHG_ERR_BAD_ARG;
+    return SPHG_OK;
+}
+
+int sphg_create(const sphg_params* p, int n_phase, sphg_ctx** out) {
+    if (!out) return SPHG_ERR_BAD_ARG;
+    *out = nullptr;
+    int rc = validate(p, n_phase);
+    if (rc) return rc;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) { cudaGetLastError(); return SPHG_ERR_NO_DEVICE; }
+    sphg_ctx* c = new sphg_ctx();
+    c->prm = *p;
+    c->nphase = n_phase;
+    cudaGetDevice(&c->device);
+    if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) { delete c; return SPHG_ERR_CUDA; }
+    c->stream = c->own_stream;
+    if (p->precision == SPHG_FP64) c->eng = new Engine<double>(c);
+    else c->eng = new Engine<float>(c);
+    *out = c;
+    return SPHG_OK;
+}
+
+int sphg_upload_phase(sphg_ctx* c, int phase, const sphg_phase_host* v) {
+    if (!c) return SPHG_ERR_BAD_ARG;
+    if (!v) return SPHG_ERR_BAD_ARG;
+    if (c->prm.single_phase && v->material != c->prm.first_material) return SPHG_ERR_BAD_ARG;
+    if (c->nphase == 2 && v->material != (phase == 1 ? SPHG_WATER : SPHG_SOIL)) return SPHG_ERR_BAD_ARG;
+    cudaSetDevice(c->device);
+    return c->eng->upload(phase, v);
+}
+
+int sphg_single_step(sphg_ctx* c, int itimestep) {
+    if (!c) return SPHG_ERR_BAD_ARG;
+    cudaSetDevice(c->device);
+    int rc = c->eng->begin_batch();
+    if (rc) return rc;
+    rc = c->eng->rhs(itimestep);
+    if (rc) return rc;
+    return c->eng->finish_batch();
+}
+
+int sphg_time_integration(sphg_ctx* c, int maxtimestep, int* itimestep, double* time) {
+    if (!c || !itimestep || !time || maxtimestep < 0) return SPHG_ERR_BAD_ARG;
+    cudaSetDevice(c->device);
+    cudaEvent_t a, b;
+    cudaEventCreate(&a); cudaEventCreate(&b);
+    cudaEventRecord(a, c->stream);
+    int rc = c->eng->begin_batch();
+    for (int it = 0; it < maxtimestep && rc == 0; ++it) {
+        int ts = *itimestep + 1;
+        rc = c->eng->step(ts);
+        if (rc) break;
+        *itimestep = ts;
+        *time = *time + c->prm.dt;
+    }
+    cudaEventRecord(b, c->stream);
+    int rc2 = c->eng->finish_batch();
+    float ms = 0.f;
+    cudaEventSynchronize(b);
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a); cudaEventDestroy(b);
+    c->last_step_ms = maxtimestep > 0 ? ms / maxtimestep : 0.0;
+    c->itimestep = *itimestep;
+    c->time = *time;
+    return rc ? rc : rc2;
+}
+
+int sphg_download_phase(sphg_ctx* c, int phase, sphg_phase_host* v) {
+    if (!c) return SPHG_ERR_BAD_ARG;
+    cudaSetDevice(c->device);
+    return c->eng->download(phase, v);
+}
+
+int sphg_export_pairs(sphg_ctx* c, int which, int32_t* pi, int32_t* pj, int64_t cap, int64_t* n) {
+    if (!c) return SPHG_ERR_BAD_ARG;
+    cudaSetDevice(c->device);
+    return c->eng->export_pairs(which, pi, pj, cap, n);
+}
+
+int sphg_stats(sphg_ctx* c, sphg_stats_t* out) {
+    if (!c || !out) return SPHG_ERR_BAD_ARG;
+    cudaSetDevice(c->device);
+    return c->eng->stats(out);
+}
+
+int sphg_set_stream(sphg_ctx* c, void* s) {
+    if (!c) return SPHG_ERR_BAD_ARG;
+    c->stream = s ? (cudaStream_t)s : c->own_stream;
+    return SPHG_OK;
+}
+
+int sphg_kernel_profile(sphg_ctx* c, int enable) {
+    if (!c) return SPHG_ERR_BAD_ARG;
+    c->prof.resolve();
+    if (enable) { c->prof.acc.clear(); c->prof.launches = 0; }
+    c->prof.on = enable != 0;
+    return SPHG_OK;
+}
+
+int sphg_kernel_report(sphg_ctx* c, char* buf, int64_t cap) {
+    if (!c || !buf || cap <= 0) return SPHG_ERR_BAD_ARG;
+    c->prof.resolve();
+    std::string s = "{\"launches\": " + std::to_string(c->prof.launches) + ", \"kernels\": {";
+    bool first = true;
+    for (auto& kv : c->prof.acc) {
+        char tmp[256];
+        snprintf(tmp, sizeof(tmp), "%s\"%s\": [%lld, %.6f]", first ? "" : ", ", kv.first.c_str(),
+                 kv.second.first, kv.second.second);
+        s += tmp;
+        first = false;
+    }
+    s += "}}";
+    if ((int64_t)s.size() + 1 > cap) return SPHG_ERR_BAD_ARG;
+    memcpy(buf, s.c_str(), s.size() + 1);
+    return SPHG_OK;
+}
+
+void sphg_destroy(sphg_ctx* c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    c->prof.resolve();
+    delete c->eng;
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    delete c;
+}
+
+const char* sphg_strerror(int code) {
+    switch (code) {
+        case SPHG_OK: return "ok";
+        case SPHG_ERR_PAIR_OVERFLOW: return "too many interactions (pair list exceeds max_interaction)";
+        case SPHG_ERR_OUT_OF_DOMAIN: return "particle out of range";
+        case SPHG_ERR_BAD_KERNEL: return "no such kernel function (skf)";
+        case SPHG_ERR_BAD_ARG: return "bad argument";
+        case SPHG_ERR_CUDA: return "CUDA runtime error";
+        case SPHG_ERR_TIMEOUT: return "device wait timed out";
+        case SPHG_ERR_NONFINITE: return "non-finite particle position";
+        case SPHG_ERR_UNSUPPORTED: return "option outside the implemented scope";
+        case SPHG_ERR_STATE: return "call out of order (upload every phase first)";
+        case SPHG_ERR_NO_DEVICE: return "no CUDA device";
+    }
+    return "unknown status";
+}
+
+}  // extern "C"

@@ -1,0 +1,222 @@
+// sphg_device.cuh — device data layout and inline device helpers of libsphg.
+//
+// Layout in HBM (one `PhaseDev` per phase):
+//   * state order: the integrated state (x, v, rho, vof, p, stress, ...) in
+//     FP64, one array per field (SoA).  State order is a spatial cell order:
+//     the state is permuted into cell order at upload and every
+//     `reorder_interval` steps, so elementwise kernels stay coalesced and the
+//     per-step permutation stays close to the identity.
+//   * rates and per-step sums (drho, dv, av, ds, dp, dvof, txx, ...) in T
+//     (double in FP64 mode, float in FP32 mode), state order.
+//   * sorted order (rebuilt every step by a counting sort over cells): the
+//     positions/h of each particle and the per-neighbour records `recA`
+//     (vx, vy, m, rho) and `recB` (p, c, vof, sxx, sxy, syy, itype, -) the pair
+//     passes gather.  A pass reads neighbours only from these sorted copies,
+//     so it may overwrite the state of its own particle while other threads
+//     still read that particle's previous values.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define SPHG_F32LIT(v) ((double)(float)(v))
+
+// pi of m_particles.f90:1483 (a double parameter set from a default-real literal)
+#define SPHG_PI_REF 3.1415927410125732
+
+template <typename T> struct V2;
+template <> struct V2<double> { typedef double2 t; };
+template <> struct V2<float> { typedef float2 t; };
+template <typename T> struct V4;
+template <> struct V4<double> { typedef double4 t; };
+template <> struct V4<float> { typedef float4 t; };
+
+// Sorted-order neighbour records.  Fields are named for what the pair passes
+// read; `itype` is stored in T (values +-2, +-3 are exact).
+template <typename T> struct __align__(4 * sizeof(T)) RecA { T vx, vy, m, rho; };
+template <typename T> struct __align__(4 * sizeof(T)) RecB { T p, c, vof, sxx, sxy, syy, itype, aux; };
+
+struct GridGeom {
+    int ncx, ncy;
+    double x0, y0, inv;   // origin and 1 / cell size
+};
+
+// Neighbour-search constants of one pair list.
+struct SearchConst {
+    double scale_k;       // get_scale_k (m_particles.f90:916)
+    double r2_uniform;    // exact squared-radius threshold when every h is equal
+    int uniform;          // all particles of both lists share one h
+};
+
+// Counters the host reads after a batch of steps.
+struct DevCounters {
+    unsigned long long pairs[3];     // phase 1, phase 2, cross (last step)
+    int maxiac[2], miniac[2], noiac[2];
+    int nfail;
+    int n_out;                       // particles clamped into edge cells
+    int nonfinite;                   // NaN/Inf positions met
+    int overflow;                    // a pair list exceeded max_interaction
+};
+
+template <typename T>
+struct PhaseDev {
+    typedef typename V2<T>::t T2;
+    int n, ntotal, material;
+    double dspp;
+    // state order, FP64
+    double2 *x, *v, *v_min;
+    double *rho, *rho_min, *vof, *vof_min, *p, *c, *mass, *hsml;
+    double *sxx, *sxy, *syy, *sxx_min, *sxy_min, *syy_min, *p_min, *eps_p;
+    int *itype, *orig, *fail;
+    // state order, T
+    T *drho, *dvof, *dsxx, *dsxy, *dsyy, *dp, *txx, *txy, *tyy, *vcc, *wxy, *vof2;
+    T2 *dv, *av;
+    int *countiac;
+    // cell list and sorted copies
+    int *cell_id, *cell_fill, *cell_start, *perm;
+    double2 *xs;
+    double *hs;
+    RecA<T> *recA, *recA2;
+    RecB<T> *recB;
+};
+
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void cell_coords(const GridGeom& g, double x, double y, int& cx, int& cy, bool& clamped) {
+    double fx = floor((x - g.x0) * g.inv), fy = floor((y - g.y0) * g.inv);
+    clamped = false;
+    if (!(fx >= 0.0)) { fx = 0.0; clamped = true; }       // also catches NaN
+    if (fx > g.ncx - 1) { fx = g.ncx - 1; clamped = true; }
+    if (!(fy >= 0.0)) { fy = 0.0; clamped = true; }
+    if (fy > g.ncy - 1) { fy = g.ncy - 1; clamped = true; }
+    cx = (int)fx; cy = (int)fy;
+}
+
+// kernel, m_particles.f90:1469-1602, dim = 2, gradient with respect to the
+// first particle of dx = x_a - x_b.  Evaluated in T in the reference's
+// operation order.
+template <typename T>
+__device__ __forceinline__ void sph_kernel(int skf, T r, T dx, T dy, T h, T& w, T& gx, T& gy) {
+    const T pi = (T)SPHG_PI_REF;
+    T q = r / h;
+    w = T(0); gx = T(0); gy = T(0);
+    if (skf == 1) {
+        T factor = T(15) / (T(7) * pi * h * h);
+        if (q >= T(0) && q <= T(1)) {
+            w = factor * ((T)SPHG_F32LIT(2.0f / 3.0f) - q * q + q * q * q / T(2));
+            T s = factor * (T(-2) + T(1.5) * q) / (h * h);
+            gx = s * dx; gy = s * dy;
+        } else if (q > T(1) && q <= T(2)) {
+            T u = T(2) - q;
+            w = factor * T(1) / T(6) * (u * u * u);
+            T s = -(factor * T(1) / T(6) * T(3) * (u * u) / h);
+            gx = s * (dx / r); gy = s * (dy / r);
+        }
+    } else if (skf == 2) {
+        T factor = T(1) / ((h * h) * pi);
+        if (q >= T(0) && q <= T(3)) {
+            w = factor * exp(-q * q);
+            gx = w * (T(-2) * dx / h / h); gy = w * (T(-2) * dy / h / h);
+        }
+    } else if (skf == 3) {
+        T factor = T(7) / (T(478) * pi * h * h);
+        T a = T(3) - q, b = T(2) - q, c = T(1) - q;
+        T a4 = a * a * a * a, b4 = b * b * b * b, c4 = c * c * c * c;
+        if (q >= T(0) && q <= T(1)) {
+            w = factor * (a4 * a - T(6) * (b4 * b) + T(15) * (c4 * c));
+            T s = factor * ((T(-120) + T(120) * q - T(50) * (q * q)) / (h * h));
+            gx = s * dx; gy = s * dy;
+        } else if (q > T(1) && q <= T(2)) {
+            w = factor * (a4 * a - T(6) * (b4 * b));
+            T s = factor * (T(-5) * a4 + T(30) * b4) / h;
+            gx = s * (dx / r); gy = s * (dy / r);
+        } else if (q > T(2) && q <= T(3)) {
+            w = factor * (a4 * a);
+            T s = factor * (T(-5) * a4) / h;
+            gx = s * (dx / r); gy = s * (dy / r);
+        }
+    } else if (skf == 4) {
+        T factor = T(7) / (T(4) * pi * h * h);
+        if (q >= T(0) && q <= T(2)) {
+            T u = T(1) - q / T(2);
+            w = factor * ((u * u * u * u) * (T(1) + T(2) * q));
+            T s = factor * (T(-5) + T(15) * q / T(2) - T(15) * (q * q) / T(4) + T(5) * (q * q * q) / T(8)) / (h * h);
+            gx = s * dx; gy = s * dy;
+        }
+    }
+}
+
+// Visit every particle of a sorted list whose distance to (xa, ha) passes
+// the reference's pair test sqrt(dx^2 + dy^2) < scale_k * (ha + hb)/2
+// (m_particles.f90:966-973, 1027-1034) evaluated bit-exactly: unfused
+// double products and sum, IEEE sqrt (or its exact squared threshold when
+// every h is equal).  `self` (a sorted index) is skipped.
+// f(m, dx, dy, r2, mhsml) gets dx = xa - xb.
+template <class F>
+__device__ __forceinline__ int visit_neighbours(const GridGeom& g, const SearchConst& sc,
+                                                const int* __restrict__ cstart,
+                                                const double2* __restrict__ xs,
+                                                const double* __restrict__ hs,
+                                                double2 xa, double ha, int self, F&& f) {
+    int cx, cy; bool clamped;
+    cell_coords(g, xa.x, xa.y, cx, cy, clamped);
+    const int x0 = cx > 0 ? cx - 1 : 0;
+    const int x1 = cx < g.ncx - 1 ? cx + 1 : g.ncx - 1;
+    const int y0 = cy > 0 ? cy - 1 : 0;
+    const int y1 = cy < g.ncy - 1 ? cy + 1 : g.ncy - 1;
+    int hits = 0;
+#pragma unroll 1
+    for (int yy = y0; yy <= y1; ++yy) {
+        const int beg = __ldg(cstart + yy * g.ncx + x0);
+        const int end = __ldg(cstart + yy * g.ncx + x1 + 1);
+#pragma unroll 1
+        for (int m = beg; m < end; ++m) {
+            if (m == self) continue;
+            const double2 xb = xs[m];
+            const double dx = xa.x - xb.x;
+            const double dy = xa.y - xb.y;
+            const double r2 = __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));
+            double mh;
+            bool hit;
+            if (sc.uniform) {
+                mh = ha;
+                hit = r2 < sc.r2_uniform;
+            } else {
+                mh = (ha + hs[m]) / 2.0;
+                hit = __dsqrt_rn(r2) < sc.scale_k * mh;
+            }
+            if (hit) { ++hits; f(m, dx, dy, r2, mh); }
+        }
+    }
+    return hits;
+}
+
+// Drucker-Prager return, drucker_prager_failure_criterion
+// (m_particles.f90:3323-3381).  Returns the fail flag.
+__device__ __forceinline__ int dp_return(double& p, double& sxx, double& sxy, double& syy, double alpha1) {
+    if (p < 0.0) p = 0.0;
+    const double I1 = 3.0 * p;
+    double J2 = sxx * sxx + 2.0 * (sxy * sxy) + syy * syy + (sxx + syy) * (sxx + syy);
+    J2 = sqrt(J2 / 2.0) + 1.0e-6;
+    if (J2 > alpha1 * I1) {
+        const double skale = alpha1 * I1 / J2;
+        sxx = skale * sxx; sxy = skale * sxy; syy = skale * syy;
+        return 1;
+    }
+    return 0;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ int warp_max(int v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ int warp_min(int v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}

@@ -1,0 +1,797 @@
+// sphg_kernels.cuh — the sm_100a kernels of libsphg.
+//
+// Per step (two-phase, declarations_sph.f90:525-791 with single_step :1131):
+//   k_first_half      leapfrog predictor (+ Drucker-Prager on soil)      elementwise
+//   k_cell_count      cell key per particle, rank inside its cell         elementwise
+//   k_cell_scatter    counting-sort scatter into cell order              elementwise
+//   k_cell_sort       order each cell by state index (determinism)       per cell
+//   k_gather          sorted copies: x, h, (v, m, rho); soil: DP + stress pair pass inputs
+//   k_water_sum       summation density (water-only step)                pair pass
+//   k_water_pass_a    continuity / df2, delta-SPH(rho), strain rate, EOS  pair pass
+//   k_water_pass_b    momentum, art. viscosity, delta-SPH(vof), wall force, XSPH  pair pass
+//   k_soil_pass       every same-phase soil term + flow rule + Jaumann   pair pass
+//   k_cross_soil      Darcy drag + pore pressure on soil, vof_s           pair pass
+//   k_cross_water     Darcy drag, dvof, vof2 on water, vof renorm        pair pass
+//   k_update          leapfrog corrector / first step (+ DP on soil)     elementwise
+// Every pair pass is a gather: one thread per particle in cell order visits
+// the 3 x 3 neighbouring cells (three contiguous row segments of the sorted
+// list), evaluates the reference's pair test bit-exactly in FP64 and sums the
+// particle's own side of each pair term.  The reference scatters each pair
+// to both ends (e.g. m_particles.f90:2427-2428); the gather evaluates the pair
+// once from each end, with the algebraically identical term, so the sums
+// match the reference to rounding, and the pair set matches exactly.
+#pragma once
+#include "sphg_device.cuh"
+
+struct SimConst {
+    int skf, single_phase, summation_density, average_velocity, visc_artificial;
+    int artificial_density, soil_artificial_stress, volume_fraction, water_artificial_volume;
+    int volume_fraction_renorm, stress_integration, plasticity, yield_dp;
+    int renorm_now;        // this step renormalises vof (itimestep % interval == 0)
+    double gravity, numeric_gravity, alpha, beta, etq, dd, p1, p2, delta, epsilon, dt;
+    double w_rho0, w_b, w_gamma, w_c, w_mu;
+    double s_rho0, s_k, s_E, s_niu, s_c, s_perm, s_G, s_alpha1;
+};
+
+#define SPHG_TPB 128
+
+__device__ __forceinline__ int gtid() { return blockIdx.x * blockDim.x + threadIdx.x; }
+
+// ----------------------------------------------------------------- cell list
+// cell key (row-major) and the particle's rank inside its cell.
+__global__ void __launch_bounds__(256) k_cell_count(const double2* __restrict__ x, int n, GridGeom g,
+                                                    int* __restrict__ cell_id, int* __restrict__ rank,
+                                                    int* __restrict__ counts, DevCounters* cnt) {
+    int a = gtid();
+    if (a >= n) return;
+    double2 p = x[a];
+    int cx, cy; bool clamped;
+    cell_coords(g, p.x, p.y, cx, cy, clamped);
+    if (clamped) atomicAdd(&cnt->n_out, 1);
+    if (!(isfinite(p.x) && isfinite(p.y))) atomicAdd(&cnt->nonfinite, 1);
+    int c = cy * g.ncx + cx;
+    cell_id[a] = c;
+    rank[a] = atomicAdd(counts + c, 1);
+}
+
+__global__ void __launch_bounds__(256) k_cell_scatter(int n, const int* __restrict__ cell_id, const int* __restrict__ rank,
+                                                      const int* __restrict__ cell_start, int* __restrict__ perm) {
+    int a = gtid();
+    if (a >= n) return;
+    perm[cell_start[cell_id[a]] + rank[a]] = a;
+}
+
+// Insertion sort of each cell's (few) entries by original particle index, so
+// the visiting order, and with it every sum, depends neither on atomic timing
+// nor on the current state order (a download/upload restart is bit-identical).
+__global__ void __launch_bounds__(256) k_cell_sort(int ncell, const int* __restrict__ cell_start,
+                                                   const int* __restrict__ orig, int* __restrict__ perm) {
+    int c = gtid();
+    if (c >= ncell) return;
+    int b = cell_start[c], e = cell_start[c + 1];
+    for (int i = b + 1; i < e; ++i) {
+        int v = perm[i], ov = orig[v], j = i - 1;
+        while (j >= b && orig[perm[j]] > ov) { perm[j + 1] = perm[j]; --j; }
+        perm[j + 1] = v;
+    }
+}
+
+// ------------------------------------------------------------------ gathers
+// Sorted copies of position, h and (v, m, rho).  For soil also the in-step
+// Drucker-Prager return (declarations_sph.f90:1242-1247) on the state and the
+// stress/pressure record of the soil pass.
+template <typename T>
+__global__ void __launch_bounds__(256) k_gather(PhaseDev<T> P, SimConst c, int soil, int do_dp, DevCounters* cnt) {
+    int k = gtid();
+    int fail = 0;
+    if (k < P.n) {
+        int a = P.perm[k];
+        P.xs[k] = P.x[a];
+        P.hs[k] = P.hsml[a];
+        double2 v = P.v[a];
+        RecA<T> ra;
+        ra.vx = (T)v.x; ra.vy = (T)v.y; ra.m = (T)P.mass[a]; ra.rho = (T)P.rho[a];
+        P.recA[k] = ra;
+        if (soil) {
+            double p = P.p[a], sxx = P.sxx[a], sxy = P.sxy[a], syy = P.syy[a];
+            if (do_dp) {
+                fail = dp_return(p, sxx, sxy, syy, c.s_alpha1);
+                P.p[a] = p; P.sxx[a] = sxx; P.sxy[a] = sxy; P.syy[a] = syy;
+                P.fail[a] = fail;
+            }
+            RecB<T> rb;
+            rb.p = (T)p; rb.c = (T)P.c[a]; rb.vof = (T)P.vof[a];
+            rb.sxx = (T)sxx; rb.sxy = (T)sxy; rb.syy = (T)syy;
+            rb.itype = (T)P.itype[a]; rb.aux = T(0);
+            P.recB[k] = rb;
+        }
+    }
+    if (soil && do_dp) {
+        int s = __syncthreads_count(fail);
+        if (threadIdx.x == 0 && s) atomicAdd(&cnt->nfail, s);
+    }
+}
+
+// Per-particle interaction statistics (interaction_statistics,
+// m_particles.f90:555-597) and the pair count of the list.
+__device__ __forceinline__ void count_stats(DevCounters* cnt, int list, int phase_slot, int hits, bool valid) {
+    unsigned long long h = valid ? (unsigned long long)hits : 0ull;
+    int hmax = valid ? hits : 0, hmin = valid ? hits : 0x7fffffff, hz = (valid && hits == 0) ? 1 : 0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        h += __shfl_xor_sync(0xffffffffu, h, o);
+        hmax = max(hmax, __shfl_xor_sync(0xffffffffu, hmax, o));
+        hmin = min(hmin, __shfl_xor_sync(0xffffffffu, hmin, o));
+        hz += __shfl_xor_sync(0xffffffffu, hz, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&cnt->pairs[list], h);
+        if (phase_slot >= 0) {
+            atomicMax(&cnt->maxiac[phase_slot], hmax);
+            atomicMin(&cnt->miniac[phase_slot], hmin);
+            if (hz) atomicAdd(&cnt->noiac[phase_slot], hz);
+        }
+    }
+}
+
+// ------------------------------------------------------ water: summation rho
+// sum_density (m_particles.f90:2243-2298) and the df2 divergence of the
+// water-only step, drho = -rho*(df2(vx,'x') + df2(vy,'y'))
+// (declarations_sph.f90:1465-1466, df2 m_particles.f90:1802-1831).
+template <typename T>
+__global__ void __launch_bounds__(SPHG_TPB) k_water_sum(PhaseDev<T> P, GridGeom g, SearchConst sc, SimConst c, DevCounters* cnt) {
+    int k = gtid();
+    bool valid = k < P.n;
+    int hits = 0;
+    if (valid) {
+        const int a = P.perm[k];
+        const double2 xa = P.xs[k];
+        const double ha = P.hs[k];
+        const RecA<T> ra = P.recA[k];
+        T w0, g0x, g0y;
+        sph_kernel<T>(c.skf, T(0), T(0), T(0), (T)ha, w0, g0x, g0y);
+        T wi = w0 * ra.m / ra.rho;
+        T num = w0 * ra.m;
+        T sx = T(0), sy = T(0);
+        const RecA<T>* __restrict__ rec = P.recA;
+        hits = visit_neighbours(g, sc, P.cell_start, P.xs, P.hs, xa, ha, k,
+            [&](int m, double dx, double dy, double r2, double mh) {
+                const RecA<T> rb = rec[m];
+                T w, gx, gy;
+                sph_kernel<T>(c.skf, (T)sqrt(r2), (T)dx, (T)dy, (T)mh, w, gx, gy);
+                wi += rb.m / rb.rho * w;
+                num += rb.m * w;
+                sx += rb.m * ((rb.vx - ra.vx) * gx);
+                sy += rb.m * ((rb.vy - ra.vy) * gy);
+            });
+        const T rho = num / wi;
+        P.rho[a] = (double)rho;
+        P.drho[a] = -rho * (sx / rho + sy / rho);
+        RecA<T> r2;
+        r2.vx = ra.vx; r2.vy = ra.vy; r2.m = ra.m; r2.rho = rho;
+        P.recA2[k] = r2;
+        P.countiac[a] = hits;
+    }
+    count_stats(cnt, 0, 0, hits, valid);
+}
+
+// ----------------------------------------------------------- water: pass A
+// Two-phase (SINGLE = false), declarations_sph.f90:1195-1233:
+//   con_density :2402, delta_sph(rho) :2658, shear_strain_rate :2855,
+//   pressure :2133 (Tait with vof, c ~ (rho/rho0 vof)^3), newtonian_fluid :2484.
+// Water-only (SINGLE = true), declarations_sph.f90:1471-1490:
+//   delta_sph on the summation density, Tait without vof, t = df(v) form.
+template <typename T, bool SINGLE>
+__global__ void __launch_bounds__(SPHG_TPB) k_water_pass_a(PhaseDev<T> P, GridGeom g, SearchConst sc, SimConst c, DevCounters* cnt) {
+    int k = gtid();
+    bool valid = k < P.n;
+    int hits = 0;
+    if (valid) {
+        const int a = P.perm[k];
+        const double2 xa = P.xs[k];
+        const double ha = P.hs[k];
+        const RecA<T>* __restrict__ rec = SINGLE ? P.recA2 : P.recA;
+        const RecA<T> ra = rec[k];
+        const T pref = (T)(c.delta * ha * P.c[a]);   // delta*hsml(i)*c(i), c of the previous EOS call
+        const T c23 = (T)SPHG_F32LIT(2.0f / 3.0f);
+        T con = 0, dl = 0, t0 = 0, t1 = 0, t2 = 0, t3 = 0;
+        hits = visit_neighbours(g, sc, P.cell_start, P.xs, P.hs, xa, ha, k,
+            [&](int m, double dx, double dy, double r2, double mh) {
+                const RecA<T> rb = rec[m];
+                T w, gx, gy;
+                const T tdx = (T)dx, tdy = (T)dy, rr = (T)r2;
+                sph_kernel<T>(c.skf, (T)sqrt(r2), tdx, tdy, (T)mh, w, gx, gy);
+                if (!SINGLE) con += rb.m * ((ra.vx - rb.vx) * gx + (ra.vy - rb.vy) * gy);
+                if (c.artificial_density) {
+                    const T muv = T(2) * (ra.rho - rb.rho) / rr;
+                    const T h = tdx * muv * gx + tdy * muv * gy;
+                    dl += pref * rb.m * h / rb.rho;
+                }
+                if (SINGLE) {   // df(vx,'x'), df(vy,'y'), df(vx,'y'), df(vy,'x')
+                    const T vb = rb.m / rb.rho;
+                    t0 += vb * ((ra.vx + rb.vx) * gx);
+                    t1 += vb * ((ra.vy + rb.vy) * gy);
+                    t2 += vb * ((ra.vx + rb.vx) * gy);
+                    t3 += vb * ((ra.vy + rb.vy) * gx);
+                } else {        // shear_strain_rate, dv = v_b - v_a
+                    const T du = rb.vx - ra.vx, dv = rb.vy - ra.vy;
+                    const T hxx = c23 * (T(2) * du * gx - dv * gy);
+                    const T hxy = du * gy + dv * gx;
+                    const T hyy = c23 * (T(2) * dv * gy - du * gx);
+                    t0 += rb.m * hxx / rb.rho;
+                    t1 += rb.m * hxy / rb.rho;
+                    t2 += rb.m * hyy / rb.rho;
+                }
+            });
+        T txx, txy, tyy, drho;
+        double p, cnew, vof;
+        const double rho = P.rho[a];
+        if (SINGLE) {
+            drho = P.drho[a] + dl;
+            txx = c23 * (T(2) * t0 - t1);
+            txy = t2 + t3;
+            tyy = c23 * (T(2) * t1 - t0);
+            p = P.p[a];
+            if (rho > 0.0) p = c.w_b * (pow(rho / c.w_rho0, c.w_gamma) - 1);
+            cnew = P.c[a];
+            vof = 1.0;
+        } else {
+            drho = con + dl;
+            txx = t0; txy = t1; tyy = t2;
+            vof = P.vof[a];
+            const double ratio = rho / (c.w_rho0 * vof);
+            p = c.w_b * (pow(ratio, c.w_gamma) - 1);
+            cnew = c.w_c * pow(ratio, 3.0);
+            P.c[a] = cnew;
+        }
+        P.drho[a] = drho;
+        P.p[a] = p;
+        // newtonian_fluid: sxx = mu*txx in place (sxx and txx are one array)
+        const double sxx = c.w_mu * (double)txx, sxy = c.w_mu * (double)txy, syy = c.w_mu * (double)tyy;
+        P.sxx[a] = sxx; P.sxy[a] = sxy; P.syy[a] = syy;
+        RecB<T> rb;
+        rb.p = (T)p; rb.c = (T)cnew; rb.vof = (T)vof;
+        rb.sxx = (T)sxx; rb.sxy = (T)sxy; rb.syy = (T)syy;
+        rb.itype = (T)P.itype[a]; rb.aux = T(0);
+        P.recB[k] = rb;
+        P.countiac[a] = hits;
+    }
+    if (!SINGLE) count_stats(cnt, 0, 0, hits, valid);
+}
+
+// ----------------------------------------------------------- water: pass B
+// Momentum dv = (-vof*df(p) + df(vof*sxx) + df(vof*sxy)) / rho
+// (declarations_sph.f90:1257-1265; df m_particles.f90:1711), art_visc :2504,
+// delta_sph(vof) :2658, repulsive_force :1605, gravity, av_vel :2761.
+// The water-only step (declarations_sph.f90:1494-1518) is the same with
+// vof = 1 and neither wall force nor delta-SPH on vof.
+template <typename T, bool SINGLE>
+__global__ void __launch_bounds__(SPHG_TPB) k_water_pass_b(PhaseDev<T> P, GridGeom g, SearchConst sc, SimConst c) {
+    typedef typename V2<T>::t T2;
+    int k = gtid();
+    if (k >= P.n) return;
+    const int a = P.perm[k];
+    const double2 xa = P.xs[k];
+    const double ha = P.hs[k];
+    const RecA<T>* __restrict__ rec = SINGLE ? P.recA2 : P.recA;
+    const RecA<T> ra = rec[k];
+    const RecB<T> qa = P.recB[k];
+    const bool real_a = P.itype[a] > 0;
+    const T phia = qa.vof;
+    const T fa_xx = phia * qa.sxx, fa_xy = phia * qa.sxy, fa_yy = phia * qa.syy;
+    const T pref = (T)(c.delta * ha) * qa.c;
+    const T alpha = (T)c.alpha, beta = (T)c.beta, etq = (T)c.etq;
+    const T r0 = (T)P.dspp, dd = (T)c.dd, p1 = (T)c.p1, p2 = (T)c.p2;
+    const bool do_rep = !SINGLE;
+    const bool do_dvof = !SINGLE && c.water_artificial_volume;
+    T d1x = 0, d1y = 0, d2x = 0, d3x = 0, d2y = 0, d3y = 0;
+    T avx = 0, avy = 0, rpx = 0, rpy = 0, dvf = 0, xsx = 0, xsy = 0;
+    visit_neighbours(g, sc, P.cell_start, P.xs, P.hs, xa, ha, k,
+        [&](int m, double dx, double dy, double r2, double mh) {
+            const RecA<T> rb = rec[m];
+            const RecB<T> qb = P.recB[m];
+            T w, gx, gy;
+            const T tdx = (T)dx, tdy = (T)dy, rr = (T)r2;
+            sph_kernel<T>(c.skf, (T)sqrt(r2), tdx, tdy, (T)mh, w, gx, gy);
+            const T vb = rb.m / rb.rho;
+            const T pp = qa.p + qb.p;
+            d1x += vb * (pp * gx);
+            d1y += vb * (pp * gy);
+            const T sxx = fa_xx + qb.vof * qb.sxx, sxy = fa_xy + qb.vof * qb.sxy, syy = fa_yy + qb.vof * qb.syy;
+            d2x += vb * (sxx * gx);
+            d3x += vb * (sxy * gy);
+            d2y += vb * (sxy * gx);
+            d3y += vb * (syy * gy);
+            const T dvx = ra.vx - rb.vx, dvy = ra.vy - rb.vy;
+            if (c.visc_artificial) {
+                const T vr = dvx * tdx + dvy * tdy;
+                if (vr < T(0)) {
+                    const T tmh = (T)mh;
+                    const T muv = tmh * vr / (rr + tmh * tmh * etq * etq);
+                    const T mc = T(0.5) * (qa.c + qb.c);
+                    const T mrho = T(0.5) * (ra.rho + rb.rho);
+                    const T piv = (beta * muv - alpha * mc) * muv / mrho;
+                    avx += rb.m * (-piv * gx);
+                    avy += rb.m * (-piv * gy);
+                }
+            }
+            if (do_dvof) {
+                const T muv = T(2) * (phia - qb.vof) / rr;
+                const T h = tdx * muv * gx + tdy * muv * gy;
+                dvf += pref * rb.m * h / rb.rho;
+            }
+            if (do_rep && real_a && qb.itype < T(0)) {
+                const T r = (T)sqrt(r2);
+                if (!(r > r0)) {
+                    const T f = (pow(r0 / r, p1) - pow(r0 / r, p2)) / (r * r);
+                    rpx += dd * tdx * f;
+                    rpy += dd * tdy * f;
+                }
+            }
+            if (c.average_velocity) {
+                const T mrho = (ra.rho + rb.rho) / T(2);
+                xsx -= rb.m * dvx / mrho * w;
+                xsy -= rb.m * dvy / mrho * w;
+            }
+        });
+    T dvx = -(phia * d1x) + d2x + d3x;
+    T dvy = -(phia * d1y) + d2y + d3y;
+    if (ra.rho > T(0)) { dvx = dvx / ra.rho; dvy = dvy / ra.rho; }
+    dvx = dvx + avx + rpx;
+    dvy = dvy + avy + rpy + (T)c.gravity;
+    T2 o; o.x = dvx; o.y = dvy;
+    P.dv[a] = o;
+    if (c.average_velocity) {
+        const T eps = (T)c.epsilon;
+        T2 av; av.x = real_a ? eps * xsx : xsx; av.y = real_a ? eps * xsy : xsy;
+        P.av[a] = av;
+    }
+    if (!SINGLE) P.dvof[a] = dvf;
+}
+
+// ------------------------------------------------------------------ soil
+// Same-phase soil terms in one pass (declarations_sph.f90:1195-1373 for the
+// two-phase step, :1546-1645 for the soil-only step): con_density,
+// delta_sph(rho), shear_strain_rate, velocity_divergence, momentum (df3 of
+// vof-weighted p and s two-phase, df soil-only), art_visc, delta_sph on p and
+// s, repulsive_force (two-phase only), gravity, av_vel; then per particle
+// plastic_or_not :3447, plastic_flow_rule3 :3700 and Jaumann_rate :3047,
+// whose spin sum wxy comes from the same pass.
+template <typename T, bool SINGLE>
+__global__ void __launch_bounds__(SPHG_TPB) k_soil_pass(PhaseDev<T> P, GridGeom g, SearchConst sc, SimConst c,
+                                                       DevCounters* cnt, int slot) {
+    typedef typename V2<T>::t T2;
+    int k = gtid();
+    bool valid = k < P.n;
+    int hits = 0, fail = 0;
+    if (valid) {
+        const int a = P.perm[k];
+        const double2 xa = P.xs[k];
+        const double ha = P.hs[k];
+        const RecA<T> ra = P.recA[k];
+        const RecB<T> qa = P.recB[k];
+        const bool real_a = P.itype[a] > 0;
+        const T cs = (T)c.s_c;                          // pressure(): c = soil%c
+        const T pref_old = (T)(c.delta * ha) * qa.c;    // delta_sph(rho) runs before pressure()
+        const T pref = (T)(c.delta * ha) * cs;
+        const T c23 = (T)SPHG_F32LIT(2.0f / 3.0f);
+        const T alpha = (T)c.alpha, beta = (T)c.beta, etq = (T)c.etq;
+        const T r0 = (T)P.dspp, dd = (T)c.dd, p1 = (T)c.p1, p2 = (T)c.p2;
+        const T phia = SINGLE ? T(1) : qa.vof;
+        const T fap = phia * qa.p, faxx = phia * qa.sxx, faxy = phia * qa.sxy, fayy = phia * qa.syy;
+        const T ira2 = T(1) / (ra.rho * ra.rho);
+        T con = 0, dl = 0, txx = 0, txy = 0, tyy = 0, vcc = 0, wxy = 0;
+        T s1x = 0, s1y = 0, s2x = 0, s3x = 0, s2y = 0, s3y = 0;
+        T avx = 0, avy = 0, rpx = 0, rpy = 0, xsx = 0, xsy = 0;
+        T dpp = 0, dsx = 0, dsxy = 0, dsy = 0;
+        hits = visit_neighbours(g, sc, P.cell_start, P.xs, P.hs, xa, ha, k,
+            [&](int m, double dx, double dy, double r2, double mh) {
+                const RecA<T> rb = P.recA[m];
+                const RecB<T> qb = P.recB[m];
+                T w, gx, gy;
+                const T tdx = (T)dx, tdy = (T)dy, rr = (T)r2;
+                sph_kernel<T>(c.skf, (T)sqrt(r2), tdx, tdy, (T)mh, w, gx, gy);
+                const T du = rb.vx - ra.vx, dv = rb.vy - ra.vy;   // v_b - v_a
+                con += rb.m * ((-du) * gx + (-dv) * gy);
+                const T e = T(2) * (tdx * gx + tdy * gy) / rr;     // 2 (dx.gradW) / r^2
+                if (c.artificial_density) dl += pref_old * rb.m * ((ra.rho - rb.rho) * e) / rb.rho;
+                const T hxx = c23 * (T(2) * du * gx - dv * gy);
+                const T hxy = du * gy + dv * gx;
+                const T hyy = c23 * (T(2) * dv * gy - du * gx);
+                txx += rb.m * hxx / rb.rho;
+                txy += rb.m * hxy / rb.rho;
+                tyy += rb.m * hyy / rb.rho;
+                vcc += rb.m * (du * gx + dv * gy) / rb.rho;
+                wxy += rb.m * (T(0.5) * (du * gy - dv * gx)) / rb.rho;
+                const T phib = SINGLE ? T(1) : qb.vof;
+                if (SINGLE) {       // df: m_b/rho_b (f_a + f_b) gradW
+                    const T vb = rb.m / rb.rho;
+                    const T pp = fap + qb.p;
+                    s1x += vb * (pp * gx); s1y += vb * (pp * gy);
+                    s2x += vb * ((faxx + qb.sxx) * gx);
+                    s3x += vb * ((faxy + qb.sxy) * gy);
+                    s2y += vb * ((faxy + qb.sxy) * gx);
+                    s3y += vb * ((fayy + qb.syy) * gy);
+                } else {            // df3: m_b (f_a/rho_a^2 + f_b/rho_b^2) gradW
+                    const T irb2 = T(1) / (rb.rho * rb.rho);
+                    const T pp = fap * ira2 + phib * qb.p * irb2;
+                    s1x += rb.m * (pp * gx); s1y += rb.m * (pp * gy);
+                    const T xx = faxx * ira2 + phib * qb.sxx * irb2;
+                    const T xy = faxy * ira2 + phib * qb.sxy * irb2;
+                    const T yy = fayy * ira2 + phib * qb.syy * irb2;
+                    s2x += rb.m * (xx * gx);
+                    s3x += rb.m * (xy * gy);
+                    s2y += rb.m * (xy * gx);
+                    s3y += rb.m * (yy * gy);
+                }
+                if (c.visc_artificial) {
+                    const T vr = (-du) * tdx + (-dv) * tdy;
+                    if (vr < T(0)) {
+                        const T tmh = (T)mh;
+                        const T muv = tmh * vr / (rr + tmh * tmh * etq * etq);
+                        const T mrho = T(0.5) * (ra.rho + rb.rho);
+                        const T piv = (beta * muv - alpha * cs) * muv / mrho;
+                        avx += rb.m * (-piv * gx);
+                        avy += rb.m * (-piv * gy);
+                    }
+                }
+                if (c.soil_artificial_stress) {
+                    const T q = pref * rb.m / rb.rho;
+                    dpp += q * ((qa.p - qb.p) * e);
+                    dsx += q * ((qa.sxx - qb.sxx) * e);
+                    dsxy += q * ((qa.sxy - qb.sxy) * e);
+                    dsy += q * ((qa.syy - qb.syy) * e);
+                }
+                if (!SINGLE && real_a && qb.itype < T(0)) {
+                    const T r = (T)sqrt(r2);
+                    if (!(r > r0)) {
+                        const T f = (pow(r0 / r, p1) - pow(r0 / r, p2)) / (r * r);
+                        rpx += dd * tdx * f;
+                        rpy += dd * tdy * f;
+                    }
+                }
+                if (c.average_velocity) {
+                    const T mrho = (ra.rho + rb.rho) / T(2);
+                    xsx += rb.m * du / mrho * w;
+                    xsy += rb.m * dv / mrho * w;
+                }
+            });
+        T dvx, dvy;
+        if (SINGLE) { dvx = -s1x + s2x + s3x; dvy = -s1y + s2y + s3y; }
+        else {
+            dvx = -(s1x * ra.rho) + s2x * ra.rho + s3x * ra.rho;
+            dvy = -(s1y * ra.rho) + s2y * ra.rho + s3y * ra.rho;
+        }
+        if (ra.rho > T(0)) { dvx = dvx / ra.rho; dvy = dvy / ra.rho; }
+        dvx = dvx + avx + rpx;
+        dvy = dvy + avy + rpy + (T)c.gravity;
+        T2 o; o.x = dvx; o.y = dvy;
+        P.dv[a] = o;
+        if (c.average_velocity) {
+            const T eps = (T)c.epsilon;
+            T2 av; av.x = real_a ? eps * xsx : xsx; av.y = real_a ? eps * xsy : xsy;
+            P.av[a] = av;
+        }
+        P.drho[a] = con + dl;
+        // plastic_or_not + plastic_flow_rule3 + Jaumann_rate on the post-DP state
+        const double p = P.p[a], sxx = P.sxx[a], sxy = P.sxy[a], syy = P.syy[a];
+        const double dtxx = (double)txx, dtxy = (double)txy, dtyy = (double)tyy, dvcc = (double)vcc;
+        const double G = c.s_E / (2.0 * (1 + c.s_niu));
+        double ds0 = 0.0, ds1 = 0.0, ds2 = 0.0, dp = 0.0;
+        if (c.plasticity == 3) {
+            fail = 0;
+            const double J2a = sqrt((sxx * sxx + 2.0 * (sxy * sxy) + syy * syy + (sxx + syy) * (sxx + syy)) / 2.0) + 1.0e-6;
+            if (fabs(J2a - c.s_alpha1 * (3.0 * p)) < SPHG_F32LIT(1.0e-5f)) fail = 1;
+            P.fail[a] = fail;
+            if (fail) {
+                const double exx = dtxx / 2.0 + dvcc / 3.0, exy = dtxy / 2.0, eyy = dtyy / 2.0 + dvcc / 3.0;
+                const double sde = sxx * exx + 2.0 * sxy * exy + syy * eyy;
+                double J2 = (sxx * sxx + 2.0 * (sxy * sxy) + syy * syy + (sxx + syy) * (sxx + syy)) / 2.0;
+                J2 = J2 + 1.0e-10;
+                const double al = c.s_alpha1, K = c.s_k;
+                const double dlambda = (3.0 * al * K * dvcc + G / sqrt(J2) * sde) / (9.0 * (al * al) * K + G);
+                if (!(dlambda < 0)) {
+                    ds0 = ds0 - dlambda * (G / sqrt(J2) * sxx);
+                    ds1 = ds1 - dlambda * (G / sqrt(J2) * sxy);
+                    ds2 = ds2 - dlambda * (G / sqrt(J2) * syy);
+                    dp = dp + 3.0 * K * al * dlambda;
+                    P.eps_p[a] = P.eps_p[a] + dlambda * sxy / (2 * sqrt(J2)) * SPHG_F32LIT(0.000005f);
+                }
+            }
+        } else {
+            fail = P.fail[a];
+        }
+        const double dwxy = (double)wxy;
+        ds0 = ds0 + G * dtxx; ds1 = ds1 + G * dtxy; ds2 = ds2 + G * dtyy;
+        dp = dp - c.s_k * dvcc;
+        ds0 = ds0 + 2.0 * sxy * dwxy;
+        ds1 = ds1 - (sxx - syy) * dwxy;
+        ds2 = ds2 - 2.0 * sxy * dwxy;
+        P.dsxx[a] = (T)(ds0 + (double)dsx);
+        P.dsxy[a] = (T)(ds1 + (double)dsxy);
+        P.dsyy[a] = (T)(ds2 + (double)dsy);
+        P.dp[a] = (T)(dp + (double)dpp);
+        P.c[a] = c.s_c;
+        P.txx[a] = txx; P.tyy[a] = tyy; P.txy[a] = wxy;   // wxy is txy (alias)
+        P.vcc[a] = vcc;
+        P.countiac[a] = hits;
+    }
+    count_stats(cnt, slot, slot, hits, valid);
+    if (c.plasticity == 3) {
+        int s = __syncthreads_count(valid ? fail : 0);
+        if (threadIdx.x == 0 && s) atomicAdd(&cnt->nfail, s);
+    }
+}
+
+// ------------------------------------------------------------- cross phase
+// Soil side of the water x soil pairs (direct_find_2 m_particles.f90:1004):
+// darcy_law :3832 and pore_water_pressure :3877, then volume_fraction_soil
+// :3970.  Neighbour data comes from the water records of this step; the
+// gradient is taken, as the reference does, with dx = x_water - x_soil.
+template <typename T>
+__global__ void __launch_bounds__(SPHG_TPB) k_cross_soil(PhaseDev<T> S, PhaseDev<T> W, GridGeom g, SearchConst sc, SimConst c) {
+    typedef typename V2<T>::t T2;
+    int k = gtid();
+    if (k >= S.n) return;
+    const int a = S.perm[k];
+    const double2 xa = S.xs[k];
+    const double ha = S.hs[k];
+    const RecA<T> ra = S.recA[k];
+    const T phis = S.recB[k].vof;
+    const T negg_ks = (T)(-c.numeric_gravity / c.s_perm);
+    T dx_ = 0, dy_ = 0;
+    visit_neighbours(g, sc, W.cell_start, W.xs, W.hs, xa, ha, -1,
+        [&](int m, double dx, double dy, double r2, double mh) {
+            const RecA<T> rb = W.recA[m];
+            const RecB<T> qb = W.recB[m];
+            T w, gx, gy;
+            const T wdx = -(T)dx, wdy = -(T)dy;   // x_water - x_soil
+            sph_kernel<T>(c.skf, (T)sqrt(r2), wdx, wdy, (T)mh, w, gx, gy);
+            const T rrw = w / (rb.rho * ra.rho);
+            const T cf = qb.vof * phis * rb.rho * negg_ks;
+            dx_ += rb.m * (cf * (rb.vx - ra.vx) * rrw);
+            dy_ += rb.m * (cf * (rb.vy - ra.vy) * rrw);
+            const T mprr = rb.m * qb.p / (rb.rho * ra.rho);
+            dx_ += mprr * gx * phis;
+            dy_ += mprr * gy * phis;
+        });
+    T2 d = S.dv[a];
+    d.x += dx_; d.y += dy_;
+    S.dv[a] = d;
+    if (c.volume_fraction) S.vof[a] = S.rho[a] / c.s_rho0;
+}
+
+// Water side: darcy_law :3832, volume_fraction_water2 :3940 (dvof),
+// volume_fraction_water :3912 (vof2), and every renorm_interval steps the
+// renormalisation rho <- rho/vof*vof2, vof <- vof2 (declarations_sph.f90:1414-1421).
+template <typename T>
+__global__ void __launch_bounds__(SPHG_TPB) k_cross_water(PhaseDev<T> W, PhaseDev<T> S, GridGeom g, SearchConst sc, SimConst c,
+                                                         DevCounters* cnt) {
+    typedef typename V2<T>::t T2;
+    int k = gtid();
+    bool valid = k < W.n;
+    int hits = 0;
+    if (valid) {
+        const int a = W.perm[k];
+        const double2 xa = W.xs[k];
+        const double ha = W.hs[k];
+        const RecA<T> ra = W.recA[k];
+        const T phiw = W.recB[k].vof;
+        const T negg_ks = (T)(-c.numeric_gravity / c.s_perm);
+        const T irho0 = (T)c.s_rho0;
+        T dvx = 0, dvy = 0, dvof = 0, v2 = 0;
+        hits = visit_neighbours(g, sc, S.cell_start, S.xs, S.hs, xa, ha, -1,
+            [&](int m, double dx, double dy, double r2, double mh) {
+                const RecA<T> rb = S.recA[m];
+                const T phis = S.recB[m].vof;
+                T w, gx, gy;
+                sph_kernel<T>(c.skf, (T)sqrt(r2), (T)dx, (T)dy, (T)mh, w, gx, gy);
+                const T rrw = w / (ra.rho * rb.rho);
+                const T cf = phiw * phis * ra.rho * negg_ks;
+                const T ux = ra.vx - rb.vx, uy = ra.vy - rb.vy;
+                dvx -= rb.m * (cf * ux * rrw);
+                dvy -= rb.m * (cf * uy * rrw);
+                dvof -= rb.m * (ux * gx + uy * gy) / irho0;
+                v2 += rb.m * w;
+            });
+        T2 d = W.dv[a];
+        d.x += dvx; d.y += dvy;
+        W.dv[a] = d;
+        if (c.volume_fraction) {
+            W.dvof[a] = W.dvof[a] + dvof;
+            const T vof2 = T(1) - v2 / irho0;
+            W.vof2[a] = vof2;
+            if (c.renorm_now) {
+                double rho = W.rho[a] / W.vof[a];
+                W.vof[a] = (double)vof2;
+                W.rho[a] = rho * (double)vof2;
+            }
+        }
+        W.countiac[a] = hits;
+    }
+    count_stats(cnt, 2, -1, hits, valid);
+}
+
+// ------------------------------------------------------------- integrators
+// first_half, declarations_sph.f90:643-684 (and :812-825, :998-1025), plus the
+// Drucker-Prager call that follows it on soil (:559, :1027).
+template <typename T>
+__global__ void __launch_bounds__(256) k_first_half(PhaseDev<T> P, SimConst c, int with_vof, int do_dp, DevCounters* cnt) {
+    int a = gtid();
+    int fail = 0;
+    if (a < P.n) {
+        const double dt = c.dt;
+        if (!c.summation_density) { double r = P.rho[a]; P.rho_min[a] = r; P.rho[a] = r + (dt / 2.0) * (double)P.drho[a]; }
+        if (with_vof && P.material == 1 && c.volume_fraction) {
+            double f = P.vof[a]; P.vof_min[a] = f; P.vof[a] = f + (dt / 2.0) * (double)P.dvof[a];
+        }
+        const bool soil = P.material == 2;
+        double p = 0, sxx = 0, sxy = 0, syy = 0;
+        if (soil) {
+            p = P.p[a]; sxx = P.sxx[a]; sxy = P.sxy[a]; syy = P.syy[a];
+            if (c.stress_integration == 2) {
+                P.sxx_min[a] = sxx; P.sxy_min[a] = sxy; P.syy_min[a] = syy; P.p_min[a] = p;
+                sxx = sxx + (dt / 2.0) * (double)P.dsxx[a];
+                sxy = sxy + (dt / 2.0) * (double)P.dsxy[a];
+                syy = syy + (dt / 2.0) * (double)P.dsyy[a];
+                p = p + (dt / 2.0) * (double)P.dp[a];
+            }
+        }
+        if (P.itype[a] >= 0) {
+            double2 v = P.v[a];
+            P.v_min[a] = v;
+            typename V2<T>::t d = P.dv[a];
+            v.x = v.x + (dt / 2.0) * (double)d.x;
+            v.y = v.y + (dt / 2.0) * (double)d.y;
+            P.v[a] = v;
+        }
+        if (soil) {
+            if (do_dp) { fail = dp_return(p, sxx, sxy, syy, c.s_alpha1); P.fail[a] = fail; }
+            P.p[a] = p; P.sxx[a] = sxx; P.sxy[a] = sxy; P.syy[a] = syy;
+        }
+    }
+    if (do_dp) {
+        int s = __syncthreads_count(fail);
+        if (threadIdx.x == 0 && s) atomicAdd(&cnt->nfail, s);
+    }
+}
+
+// first_step (:686-723) when first != 0, else second_half (:725-762), plus the
+// Drucker-Prager call after it on soil (:583, :601, :1069, :1107).
+template <typename T>
+__global__ void __launch_bounds__(256) k_update(PhaseDev<T> P, SimConst c, int first, int with_vof, int do_dp, DevCounters* cnt) {
+    int a = gtid();
+    int fail = 0;
+    if (a < P.n) {
+        const double dt = c.dt;
+        if (!c.summation_density) {
+            P.rho[a] = first ? P.rho[a] + (dt / 2.0) * (double)P.drho[a] : P.rho_min[a] + dt * (double)P.drho[a];
+        }
+        if (with_vof && P.material == 1 && c.volume_fraction) {
+            P.vof[a] = first ? P.vof[a] + (dt / 2.0) * (double)P.dvof[a] : P.vof_min[a] + dt * (double)P.dvof[a];
+        }
+        const bool soil = P.material == 2;
+        if (soil) {
+            double p = P.p[a], sxx = P.sxx[a], sxy = P.sxy[a], syy = P.syy[a];
+            const double d0 = P.dsxx[a], d1 = P.dsxy[a], d2 = P.dsyy[a], d3 = P.dp[a];
+            if (c.stress_integration == 1) {
+                sxx = sxx + dt * d0; sxy = sxy + dt * d1; syy = syy + dt * d2; p = p + dt * d3;
+            } else if (c.stress_integration == 2) {
+                if (first) {
+                    sxx = sxx + (dt / 2.0) * d0; sxy = sxy + (dt / 2.0) * d1;
+                    syy = syy + (dt / 2.0) * d2; p = p + (dt / 2.0) * d3;
+                } else {
+                    sxx = P.sxx_min[a] + dt * d0; sxy = P.sxy_min[a] + dt * d1;
+                    syy = P.syy_min[a] + dt * d2; p = P.p_min[a] + dt * d3;
+                }
+            }
+            if (do_dp) { fail = dp_return(p, sxx, sxy, syy, c.s_alpha1); P.fail[a] = fail; }
+            P.p[a] = p; P.sxx[a] = sxx; P.sxy[a] = sxy; P.syy[a] = syy;
+        }
+        if (P.itype[a] >= 0) {
+            double2 v = first ? P.v[a] : P.v_min[a];
+            const typename V2<T>::t d = P.dv[a];
+            const typename V2<T>::t av = P.av[a];
+            double2 x = P.x[a];
+            const double h = first ? dt / 2.0 : dt;
+            v.x = v.x + h * (double)d.x + (double)av.x;
+            x.x = x.x + dt * v.x;
+            v.y = v.y + h * (double)d.y + (double)av.y;
+            x.y = x.y + dt * v.y;
+            P.v[a] = v;
+            P.x[a] = x;
+        }
+    }
+    if (do_dp) {
+        int s = __syncthreads_count(fail);
+        if (threadIdx.x == 0 && s) atomicAdd(&cnt->nfail, s);
+    }
+}
+
+// Sticky per-batch flags: a pair list above max_interaction (the reference
+// stops there, m_particles.f90:992-993) and non-finite positions.
+__global__ void k_check(const DevCounters* __restrict__ c, int* __restrict__ sticky, unsigned long long cap) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        if (c->pairs[0] / 2 > cap || c->pairs[1] / 2 > cap || c->pairs[2] > cap) sticky[0] = 1;
+        if (c->nonfinite) sticky[1] = 1;
+    }
+}
+
+// ------------------------------------------------------- layout transforms
+template <typename S>
+__global__ void __launch_bounds__(256) k_permute(int n, const int* __restrict__ perm, const S* __restrict__ src, S* __restrict__ dst) {
+    int k = gtid();
+    if (k < n) dst[k] = src[perm[k]];
+}
+__global__ void __launch_bounds__(256) k_iota(int n, int* __restrict__ v) {
+    int k = gtid();
+    if (k < n) v[k] = k;
+}
+// state order -> original (Fortran) order, widening to double
+template <typename S>
+__global__ void __launch_bounds__(256) k_to_original(int n, const int* __restrict__ orig, const S* __restrict__ src,
+                                                     double* __restrict__ dst, int comps) {
+    int a = gtid();
+    if (a >= n) return;
+    const S* s = src + (size_t)a * comps;
+    double* d = dst + (size_t)orig[a] * comps;
+    for (int t = 0; t < comps; ++t) d[t] = (double)s[t];
+}
+// original order -> state order, narrowing from double
+template <typename S>
+__global__ void __launch_bounds__(256) k_from_original(int n, const int* __restrict__ orig, const double* __restrict__ src,
+                                                       S* __restrict__ dst, int comps) {
+    int a = gtid();
+    if (a >= n) return;
+    const double* s = src + (size_t)orig[a] * comps;
+    S* d = dst + (size_t)a * comps;
+    for (int t = 0; t < comps; ++t) d[t] = (S)s[t];
+}
+__global__ void __launch_bounds__(256) k_to_original_i(int n, const int* __restrict__ orig, const int* __restrict__ src,
+                                                       int* __restrict__ dst) {
+    int a = gtid();
+    if (a < n) dst[orig[a]] = src[a];
+}
+__global__ void __launch_bounds__(256) k_from_original_i(int n, const int* __restrict__ orig, const int* __restrict__ src,
+                                                         int* __restrict__ dst) {
+    int a = gtid();
+    if (a < n) dst[a] = src[orig[a]];
+}
+
+// Pair export: per particle (original index i), the neighbours j > i (or, for
+// the cross list, every neighbour), sorted, written at offset[i].
+__global__ void __launch_bounds__(SPHG_TPB) k_pairs_count(int n, const int* __restrict__ perm, const int* __restrict__ orig,
+                                                          const double2* __restrict__ xs, const double* __restrict__ hs,
+                                                          GridGeom g, SearchConst sc, const int* __restrict__ cstart_o,
+                                                          const double2* __restrict__ xs_o, const double* __restrict__ hs_o,
+                                                          const int* __restrict__ perm_o, const int* __restrict__ orig_o,
+                                                          int cross, int* __restrict__ count, int pass, const long long* __restrict__ offset,
+                                                          int* __restrict__ out_i, int* __restrict__ out_j, long long cap) {
+    int k = gtid();
+    if (k >= n) return;
+    const int oi = orig[perm[k]];
+    const double2 xa = xs[k];
+    const double ha = hs[k];
+    int cnt = 0;
+    long long base = pass ? offset[oi] : 0;
+    visit_neighbours(g, sc, cstart_o, xs_o, hs_o, xa, ha, cross ? -1 : k,
+        [&](int m, double, double, double, double) {
+            const int oj = orig_o[perm_o[m]];
+            if (!cross && oj <= oi) return;
+            if (pass) {
+                long long pos = base + cnt;
+                if (pos < cap) { out_i[pos] = oi + 1; out_j[pos] = oj + 1; }
+            }
+            ++cnt;
+        });
+    if (!pass) { count[oi] = cnt; return; }
+    // sort this particle's j's (few) in place
+    long long b = base, e = base + cnt;
+    if (e > cap) e = cap;
+    for (long long i = b + 1; i < e; ++i) {
+        int v = out_j[i];
+        long long j = i - 1;
+        while (j >= b && out_j[j] > v) { out_j[j + 1] = out_j[j]; --j; }
+        out_j[j + 1] = v;
+    }
+}

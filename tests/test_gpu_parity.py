@@ -1,0 +1,217 @@
+"""Parity of libsphg (through its C ABI) with the CPU oracle, on a GPU.
+
+* Pair sets: bit-exact, compared as sorted 1-based (i, j) lists from the same
+  positions (direct_find m_particles.f90:938, direct_find_2 :1004).
+* Fields in FP64 mode: the GPU sums each particle's neighbours in cell order
+  where the reference scatters pairs in list order, so fields agree to
+  rounding: field-scale relative error max|gpu - ref| / max|ref| <= 1e-9 after
+  one step and <= 1e-7 after 30 steps.
+* FP32 mode (float pair arithmetic, FP64 positions/time/leapfrog state):
+  errors against the FP64 oracle within the per-field budget FP32_BUDGET.
+"""
+import numpy as np
+import pytest
+
+from oracle import Oracle
+from sources_b200 import SPHError, Solver, scenes
+from sources_b200.abi import (SPHG_ERR_NONFINITE, SPHG_ERR_PAIR_OVERFLOW, SPHG_FP32, SPHG_FP64,
+                              SPHG_PAIRS_CROSS, SPHG_PAIRS_FIRST, SPHG_PAIRS_SECOND)
+
+pytestmark = pytest.mark.gpu
+
+NAMES = ["dam_break", "granular_column", "two_phase"]
+RHS_FIELDS = ["drho", "dvx", "av", "p", "c", "rho", "dvof", "vof2", "vof", "dsxx", "dsxy", "dsyy", "dp",
+              "sxx", "sxy", "syy", "txx", "tyy", "txy", "vcc", "epsilon_p"]
+STATE_FIELDS = ["x", "vx", "rho", "p", "vof", "sxx", "sxy", "syy", "drho", "dvx", "c"]
+
+# FP32 mode, field-scale relative error vs the FP64 oracle
+FP32_BUDGET_1 = {"x": 1e-12, "vx": 1e-4, "rho": 1e-6, "p": 1e-4, "drho": 1e-3, "dvx": 1e-3, "sxx": 1e-4,
+                 "sxy": 1e-3, "syy": 1e-4, "vof": 1e-6, "c": 1e-5}
+FP32_BUDGET_30 = {"x": 1e-9, "vx": 1e-3, "rho": 1e-5, "p": 1e-3, "drho": 1e-2, "dvx": 1e-2, "sxx": 1e-3,
+                  "sxy": 1e-2, "syy": 1e-3, "vof": 1e-5, "c": 1e-4}
+
+
+def ferr(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    scale = np.abs(b).max()
+    if scale == 0.0:
+        return float(np.abs(a).max())
+    return float(np.abs(a - b).max() / scale)
+
+
+def lists_for(scene):
+    return [SPHG_PAIRS_FIRST] if len(scene.phases) == 1 else [SPHG_PAIRS_FIRST, SPHG_PAIRS_SECOND, SPHG_PAIRS_CROSS]
+
+
+def compare_pairs(scene, gpu, positions_from_gpu=False):
+    """GPU pair lists of the current positions against the oracle's from the
+    same positions."""
+    if positions_from_gpu:
+        s = scene.copy()
+        s.phases = [gpu.download(k + 1) for k in range(len(scene.phases))]
+    else:
+        s = scene
+    o = Oracle(s)
+    assert o.single_step(1) == 0
+    for w in lists_for(scene):
+        gi, gj = gpu.pairs(w)
+        oi, oj = o.pairs(w)
+        assert len(gi) == len(oi), (w, len(gi), len(oi))
+        assert np.array_equal(gi, oi) and np.array_equal(gj, oj), w
+
+
+@pytest.mark.parametrize("skf", [1, 2, 3, 4])
+@pytest.mark.parametrize("name", NAMES)
+def test_pairs_bit_exact(cuda_ok, name, skf):
+    s = scenes.jitter(scenes.small(name, precision=SPHG_FP64, skf=skf), 0.0003, seed=skf)
+    with Solver(s) as g:
+        compare_pairs(s, g)
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_pairs_bit_exact_after_steps(cuda_ok, name):
+    s = scenes.small(name, precision=SPHG_FP64)
+    with Solver(s) as g:
+        g.time_integration(25)
+        compare_pairs(s, g, positions_from_gpu=True)
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_rhs_parity_fp64(cuda_ok, name):
+    s = scenes.jitter(scenes.small(name, precision=SPHG_FP64), 0.0002, seed=21)
+    for P in s.phases:   # some motion so every term is exercised
+        P.vx[:P.ntotal] = np.random.default_rng(3).normal(0, 0.02, size=(P.ntotal, 2))
+    o = Oracle(s)
+    assert o.single_step(1) == 0
+    with Solver(s) as g:
+        g.single_step(1)
+        for k in range(len(s.phases)):
+            a, b = g.download(k + 1), o.download(k + 1)
+            for f in RHS_FIELDS:
+                e = ferr(getattr(a, f), getattr(b, f))
+                assert e <= 1e-9, (name, k + 1, f, e)
+            assert np.mean(a.fail == b.fail) > 0.99
+        st = g.stats()
+        for w in lists_for(s):
+            assert st.niac[w] == len(o.pairs(w)[0])
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_steps_parity_fp64(cuda_ok, name):
+    s = scenes.small(name, precision=SPHG_FP64)
+    o = Oracle(s)
+    assert o.time_integration(30) == 0
+    with Solver(s) as g:
+        g.time_integration(30)
+        assert g.itimestep == 30 and abs(g.time - o.time) < 1e-15
+        for k in range(len(s.phases)):
+            a, b = g.download(k + 1), o.download(k + 1)
+            for f in STATE_FIELDS:
+                e = ferr(getattr(a, f), getattr(b, f))
+                assert e <= 1e-7, (name, k + 1, f, e)
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_fp32_error_budget(cuda_ok, name):
+    s64 = scenes.small(name, precision=SPHG_FP64)
+    s32 = scenes.small(name, precision=SPHG_FP32)
+    for steps, budget in ((1, FP32_BUDGET_1), (30, FP32_BUDGET_30)):
+        o = Oracle(s64)
+        assert o.time_integration(steps) == 0
+        with Solver(s32) as g:
+            g.time_integration(steps)
+            for k in range(len(s64.phases)):
+                a, b = g.download(k + 1), o.download(k + 1)
+                for f, tol in budget.items():
+                    if np.abs(getattr(b, f)).max() == 0:
+                        continue
+                    e = ferr(getattr(a, f), getattr(b, f))
+                    assert e <= tol, (name, steps, k + 1, f, e)
+
+
+@pytest.mark.parametrize("precision", [SPHG_FP64, SPHG_FP32])
+@pytest.mark.parametrize("name", NAMES)
+def test_restart_and_determinism(cuda_ok, name, precision):
+    s = scenes.small(name, precision=precision)
+    with Solver(s) as full, Solver(s) as twin:
+        full.time_integration(14)
+        twin.time_integration(14)
+        s2 = s.copy()
+        with Solver(s) as half:
+            half.time_integration(7)
+            s2.phases = [half.download(k + 1) for k in range(len(s.phases))]
+            it, t = half.itimestep, half.time
+        with Solver(s2) as rest:
+            rest.itimestep, rest.time = it, t
+            rest.time_integration(7)
+            for k in range(len(s.phases)):
+                a, b, c = full.download(k + 1), twin.download(k + 1), rest.download(k + 1)
+                for f in ("x", "vx", "rho", "p", "sxx", "vof", "drho", "dvx"):
+                    assert np.array_equal(getattr(a, f), getattr(b, f)), ("determinism", f)
+                    assert np.array_equal(getattr(a, f), getattr(c, f)), ("restart", f)
+
+
+def test_working_array_aliasing_after_two_phase_step(cuda_ok):
+    """Water sxx/syy/sxy are the shared txx/tyy/txy arrays, which the soil
+    pass overwrites (declarations_sph.f90:371-377,414-415)."""
+    s = scenes.small("two_phase", precision=SPHG_FP64)
+    o = Oracle(s)
+    assert o.time_integration(3) == 0
+    with Solver(s) as g:
+        g.time_integration(3)
+        a, b = g.download(1), o.download(1)
+        for f in ("sxx", "syy", "sxy", "txx", "tyy", "txy"):
+            assert ferr(getattr(a, f), getattr(b, f)) <= 1e-7, f
+        ns = s.phases[1].n
+        assert np.all(a.sxy[ns:] == 0.0)
+
+
+def test_pair_overflow_is_reported(cuda_ok):
+    s = scenes.small("dam_break", precision=SPHG_FP64)
+    s.params.max_interaction = 100
+    with Solver(s) as g:
+        with pytest.raises(SPHError) as e:
+            g.time_integration(1)
+        assert e.value.code == SPHG_ERR_PAIR_OVERFLOW
+
+
+def test_nonfinite_position_is_reported(cuda_ok):
+    s = scenes.small("granular_column", precision=SPHG_FP64)
+    s.phases[0].x[5, 0] = np.nan
+    with Solver(s) as g:
+        with pytest.raises(SPHError) as e:
+            g.time_integration(2)
+        assert e.value.code == SPHG_ERR_NONFINITE
+
+
+@pytest.mark.parametrize("name", ["dam_break", "granular_column"])
+def test_full_size_single_phase_pairs(cuda_ok, name):
+    s = getattr(scenes, name)(precision=SPHG_FP64)
+    assert s.n_particles == {"dam_break": 4008, "granular_column": 6608}[name]
+    with Solver(s) as g:
+        compare_pairs(s, g)
+        g.time_integration(5)
+        compare_pairs(s, g, positions_from_gpu=True)
+
+
+def test_full_size_two_phase_pairs_and_fp32_vs_fp64(cuda_ok):
+    """The 912,016-particle two-phase workload: pair sets bit-exact against
+    the oracle, one FP32 step within the FP32 budget of the FP64 step."""
+    s64 = scenes.two_phase(precision=SPHG_FP64)
+    assert s64.n_particles == 912016
+    with Solver(s64) as g:
+        compare_pairs(s64, g)
+        g.time_integration(1)
+        a64 = [g.download(k + 1) for k in range(2)]
+    s32 = scenes.two_phase(precision=SPHG_FP32)
+    with Solver(s32) as g:
+        g.time_integration(1)
+        a32 = [g.download(k + 1) for k in range(2)]
+    for k in range(2):
+        for f, tol in FP32_BUDGET_1.items():
+            ref = getattr(a64[k], f)
+            if np.abs(ref).max() == 0:
+                continue
+            assert np.all(np.isfinite(getattr(a32[k], f))), f
+            assert ferr(getattr(a32[k], f), ref) <= tol, (k + 1, f)

@@ -1,0 +1,315 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 SPH step: particle-steps/s on the two-phase
+submerged-soil workload (912,016 particles: 4.0 m x 1.0 m domain, dx 0.002 m,
+soil block 1.0 m x 0.4 m under 0.8 m of water, FP32 pair arithmetic with FP64
+positions/time/leapfrog state).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = one full leapfrog step of time_integration (declarations_sph.f90:525)
+over both phases, neighbour search included.  Prints one JSON line (rank 0).
+
+Under torchrun (N > 1) every rank steps its own replica of the workload on
+its own GPU (the step has no exchange between replicas: weak scaling, no
+collective on the data path); the timed region is bracketed by a barrier
+and device synchronisation on every rank and the time is the max over ranks.
+
+--impl reference times the reference's CPU path on the host cores: the C
+restatement of the serial Fortran step (the reference itself has no C/CUDA
+code and no Fortran compiler exists here), on a bounded sub-domain sample of
+the same workload at the same spacing.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s at 1M particles (two-phase water/soil SPH step, 1 B200)"
+UNIT = "particle-steps/s"
+WORKLOAD = "two_phase_912k"
+
+# Algorithmic HBM bytes per particle of each pair pass in FP32 mode: the
+# particle's own sorted record, position and index read once and its results
+# written once (neighbour records are re-read from L1/L2 and not counted).
+ALG_BYTES = {
+    "water_pass_a": 4 + 16 + 8 + 16 + 8 + 8 + 4 + 4 + 4 + 8 + 3 * 8 + 32 + 4,  # perm,xs,hs,recA,rho,c,vof,itype,drho,p,c,s(3),recB,count
+    "water_pass_b": 4 + 16 + 8 + 16 + 32 + 4 + 8 + 8 + 4,                     # perm,xs,hs,recA,recB,itype -> dv,av,dvof
+    "soil_pass": 4 + 16 + 8 + 16 + 32 + 4 + 4 * 8 + 8 + 8 + 4 + 16 + 4 * 4 + 8 + 4 * 4 + 4,
+    "cross_water": 4 + 16 + 8 + 16 + 4 + 8 + 8 + 4 + 4 + 4 + 16,
+    "cross_soil": 4 + 16 + 8 + 16 + 4 + 8 + 8 + 8 + 8,
+}
+# Whole-step algorithmic bytes per particle-step (FP32 pair data, FP64 state):
+# the compulsory state read + write once per step plus the cell key.
+STEP_BYTES = {"water": 112, "soil": 168}
+
+
+def clocks_sampler(stop, out):
+    cmd = ["nvidia-smi", "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+           "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+           "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+           "--format=csv,noheader,nounits", "-lms", "200"]
+    try:
+        p = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+    except OSError:
+        return
+    def reader():
+        for line in p.stdout:
+            out.append(line.strip())
+    t = threading.Thread(target=reader, daemon=True)
+    t.start()
+    stop.wait()
+    p.terminate()
+    try:
+        p.wait(timeout=5)
+    except Exception:
+        p.kill()
+    t.join(timeout=2)
+
+
+def summarize_clocks(lines, device_index):
+    sm, mx, reasons = [], [], set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    for l in lines:
+        f = [x.strip() for x in l.split(",")]
+        if len(f) < 9 or f[0] != str(device_index):
+            continue
+        try:
+            sm.append(float(f[1])); mx.append(float(f[2]))
+        except ValueError:
+            continue
+        for n, v in zip(names, f[5:9]):
+            if v.lower().startswith("active"):
+                reasons.add(n)
+    if not sm:
+        return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+    return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak_hbm():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    try:
+        with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def cpu_baseline(steps: int):
+    """The oracle port of the serial reference step on a sub-domain sample of
+    the workload (same spacing and physics, 1.0 m wide, 0.2 m of water)."""
+    from oracle import Oracle
+    from sources_b200 import scenes
+    s = scenes.two_phase(width=1.0, height=1.0, block_w=0.25, block_h=0.1, water_h=0.2)
+    o = Oracle(s)
+    o.time_integration(1)
+    t0 = time.perf_counter()
+    rc = o.time_integration(steps)
+    dt = time.perf_counter() - t0
+    if rc:
+        raise RuntimeError(f"oracle step failed: {rc}")
+    n = s.n_particles
+    return {"value": n * steps / dt, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"serial C restatement of the Fortran step, {steps} leapfrog steps of a {n}-particle "
+                      f"sub-domain of the workload (1.0 m x 0.2 m water, 0.25 m x 0.1 m soil block, dx 0.002 m)",
+            "seconds": dt}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    from oracle import Oracle
+    from sources_b200 import scenes
+    s = scenes.two_phase(width=1.0, height=1.0, block_w=0.25, block_h=0.1, water_h=0.2)
+    o = Oracle(s)
+    o.time_integration(args.warmup)
+    t0 = time.perf_counter()
+    rc = o.time_integration(args.steps)
+    dt = time.perf_counter() - t0
+    if rc:
+        print(json.dumps({"impl": "reference", "unavailable": f"oracle step failed with status {rc}"}))
+        return 0
+    n = s.n_particles
+    v = n * args.steps / dt
+    sample = (f"serial C restatement of the Fortran step (the reference has no compilable C/CUDA and no Fortran "
+              f"compiler is present); each step is one leapfrog step of a {n}-particle sub-domain of the workload")
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * dt / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (deterministic lattice scene)",
+            "config": {"workload": WORKLOAD, "particles": 912016, "sample_particles": n,
+                       "precision": "fp64 (reference)", "l2": "state larger than L2"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--cpu-steps", type=int, default=60)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload", default=WORKLOAD, choices=[WORKLOAD, "two_phase_456k"],
+                    help="two_phase_456k: the same scene 2.0 m wide (for profiler captures)")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device")
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+
+    from sources_b200 import Solver, build, scenes
+    from sources_b200.abi import SPHG_FP32
+
+    build.build()
+    if args.workload == WORKLOAD:
+        scene = scenes.two_phase(precision=SPHG_FP32)
+    else:
+        scene = scenes.two_phase(width=2.0, precision=SPHG_FP32)
+    n = scene.n_particles
+    stream = torch.cuda.current_stream()
+    solver = Solver(scene)
+    solver.set_stream(stream.cuda_stream)
+
+    solver.time_integration(args.warmup)
+    torch.cuda.synchronize()
+
+    # ---- device-resident timed region
+    samples, stop = [], threading.Event()
+    th = threading.Thread(target=clocks_sampler, args=(stop, samples), daemon=True)
+    th.start()
+    time.sleep(0.3)
+    launches0 = solver.kernel_report()["launches"]
+    solver.profile(True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    solver.time_integration(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ms = e0.elapsed_time(e1)
+    rep = solver.kernel_report()
+    solver.profile(False)
+    launches = rep["launches"] - launches0
+    stop.set()
+    th.join(timeout=10)
+    clocks = summarize_clocks(samples, local)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * n * args.steps / (ms / 1000.0)
+
+    # ---- dominant kernel and its roofline
+    kern = rep["kernels"]
+    top = max(kern.items(), key=lambda kv: kv[1][1])
+    top_name, (top_launches, top_ms) = top[0], top[1]
+    avg_ms = top_ms / max(top_launches, 1)
+    units = scene.phases[0].n if top_name in ("water_pass_a", "water_pass_b", "cross_water", "water_sum") \
+        else scene.phases[1].n
+    alg = ALG_BYTES.get(top_name, 0) * units
+    peak, peak_kind = measured_peak_hbm()
+    achieved = alg / (avg_ms / 1000.0) / 1e9
+    tr = ncu_traffic().get(top_name)
+    step_bytes = STEP_BYTES["water"] * scene.phases[0].n + STEP_BYTES["soil"] * scene.phases[1].n
+    step_ms = ms / args.steps
+    roofline = {"bound": "hbm", "kernel": top_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind, "traffic": tr,
+                "alg_bytes_per_launch": alg, "avg_launch_ms": avg_ms,
+                "step": {"alg_bytes": step_bytes, "achieved_gbs": step_bytes / (step_ms / 1000.0) / 1e9,
+                         "frac": step_bytes / (step_ms / 1000.0) / 1e9 / peak},
+                "kernels_ms_per_step": {k: v[1] / args.steps for k, v in kern.items()}}
+
+    # ---- end to end through the C ABI with pinned host buffers
+    def pinned(shape, dtype):
+        t = torch.zeros(shape, dtype=torch.float64 if dtype == np.float64 else torch.int32, pin_memory=True)
+        return t.numpy()
+    host = [P.copy(alloc=pinned) for P in scene.phases]
+    for k in range(len(host)):
+        solver.download(k + 1, into=host[k])
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        for k, P in enumerate(host):
+            solver.upload(k + 1, P)
+        solver.time_integration(1)
+        for k in range(len(host)):
+            solver.download(k + 1, into=host[k])
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    bytes_per_step = sum(P.nbytes() for P in host)
+    e2e = {"value": world * n * args.e2e_steps / e2e_s, "unit": UNIT,
+           "h2d_bytes_per_step": bytes_per_step, "d2h_bytes_per_step": bytes_per_step,
+           "steps": args.e2e_steps,
+           "mode": "every step: upload the full phase state from pinned host arrays, one leapfrog step, "
+                   "download the full state (the Fortran host owns its arrays)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(args.cpu_steps)
+
+    solver.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (deterministic lattice scene, no dataset)",
+                "config": {"workload": args.workload, "particles": n, "water": scene.phases[0].n,
+                           "soil": scene.phases[1].n, "dx": 0.002, "precision": "fp32 pairs / fp64 state",
+                           "skf": int(scene.params.skf), "parallelism": f"replicas{world}",
+                           "l2": "inputs larger than L2 (state ~%.0f MB)" % (n * 250 / 1e6)},
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+                "clocks": clocks}
+        print(json.dumps(line))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -190,7 +190,9 @@ int sphg_stats(sphg_ctx* ctx, sphg_stats_t* out);
 int sphg_set_stream(sphg_ctx* ctx, void* cuda_stream);
 
 /* Per-kernel CUDA-event timing: enable=1 starts recording, 0 stops.
- * sphg_kernel_report writes a JSON object {name: [launches, total_ms], ...}. */
+ * sphg_kernel_report writes a JSON object
+ *   {"launches": L, "kernels": {name: [launches, total_ms], ...}}
+ * where L counts every kernel the context launched since its creation. */
 int sphg_kernel_profile(sphg_ctx* ctx, int enable);
 int sphg_kernel_report(sphg_ctx* ctx, char* buf, int64_t cap);
 

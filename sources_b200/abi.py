@@ -130,22 +130,31 @@ def default_params() -> Params:
 class PhaseArrays:
     """Host arrays of one phase, in the reference's particle order."""
 
-    def __init__(self, n: int, ntotal: int, material: int, dspp: float = 0.0):
+    def __init__(self, n: int, ntotal: int, material: int, dspp: float = 0.0, alloc=None):
+        """alloc(shape, dtype) -> zeroed array; e.g. pinned host memory."""
         self.n = int(n)
         self.ntotal = int(ntotal)
         self.nvirt = int(n - ntotal)
         self.material = int(material)
         self.dspp = float(dspp)
         self.nfail = 0
+        mk = alloc or (lambda shape, dtype: np.zeros(shape, dtype=dtype))
         for f in VEC_FIELDS:
-            setattr(self, f, np.zeros((self.n, 2), dtype=np.float64))
+            setattr(self, f, mk((self.n, 2), np.float64))
         for f in SCALAR_FIELDS:
-            setattr(self, f, np.zeros(self.n, dtype=np.float64))
+            setattr(self, f, mk((self.n,), np.float64))
         for f in INT_FIELDS:
-            setattr(self, f, np.zeros(self.n, dtype=np.int32))
+            setattr(self, f, mk((self.n,), np.int32))
 
-    def copy(self) -> "PhaseArrays":
-        o = PhaseArrays(self.n, self.ntotal, self.material, self.dspp)
+    def nbytes(self, fields=None) -> int:
+        tot = 0
+        for f in VEC_FIELDS + SCALAR_FIELDS + INT_FIELDS:
+            if fields is None or f in fields:
+                tot += getattr(self, f).nbytes
+        return tot
+
+    def copy(self, alloc=None) -> "PhaseArrays":
+        o = PhaseArrays(self.n, self.ntotal, self.material, self.dspp, alloc=alloc)
         for f in VEC_FIELDS + SCALAR_FIELDS + INT_FIELDS:
             getattr(o, f)[...] = getattr(self, f)
         o.nfail = self.nfail

@@ -22,12 +22,19 @@ namespace {
 
 inline int blocks(long long n, int tpb) { return (int)((n + tpb - 1) / tpb); }
 
+// Per-kernel CUDA-event timing on the launching stream.  Events come from a
+// pool so that timing a long run adds no event creation to the step.
 struct Profiler {
     bool on = false;
-    long long launches = 0;
+    long long launches = 0;   // kernels launched since the context was created
     struct Pending { const char* name; cudaEvent_t a, b; };
     std::vector<Pending> pending;
+    std::vector<cudaEvent_t> pool;
     std::map<std::string, std::pair<long long, double>> acc;
+    cudaEvent_t get() {
+        if (pool.empty()) { cudaEvent_t e; cudaEventCreate(&e); return e; }
+        cudaEvent_t e = pool.back(); pool.pop_back(); return e;
+    }
     void resolve() {
         for (auto& p : pending) {
             float ms = 0.f;
@@ -36,11 +43,12 @@ struct Profiler {
             auto& e = acc[p.name];
             e.first += 1;
             e.second += ms;
-            cudaEventDestroy(p.a);
-            cudaEventDestroy(p.b);
+            pool.push_back(p.a);
+            pool.push_back(p.b);
         }
         pending.clear();
     }
+    ~Profiler() { for (auto e : pool) cudaEventDestroy(e); }
 };
 
 }  // namespace
@@ -91,6 +99,7 @@ struct Engine : EngineBase {
     SearchConst sc_same{}, sc_cross{};
     int ncell = 0;
     int* counts[2] = {nullptr, nullptr};
+    int* cell_start_buf[2] = {nullptr, nullptr};
     void* cub_tmp = nullptr;
     size_t cub_bytes = 0;
     DevCounters* cnt = nullptr;     // device
@@ -101,6 +110,7 @@ struct Engine : EngineBase {
     long long* stage_l = nullptr;
     void* spare[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};  // reorder scratch per phase: 4, 8, 16-byte elements
     int nmax = 0;
+    double hrange[2][2] = {{0, 0}, {0, 0}};
     std::vector<void*> allocs;
     SimConst sim{};
 
@@ -130,7 +140,7 @@ struct Engine : EngineBase {
         if (grid_ <= 0) return 0;
         cudaEvent_t a = nullptr, b = nullptr;
         if (ctx->prof.on) {
-            cudaEventCreate(&a); cudaEventCreate(&b);
+            a = ctx->prof.get(); b = ctx->prof.get();
             cudaEventRecord(a, ctx->stream);
         }
         kern<<<grid_, block, 0, ctx->stream>>>(args...);
@@ -184,6 +194,7 @@ struct Engine : EngineBase {
     // ------------------------------------------------------------ allocation
     int alloc_phase(int ph, int n) {
         PhaseDev<T>& D = P[ph];
+        if (have[ph] && D.n == n) return 0;   // same size: reuse every buffer
         // a re-upload replaces the arrays
         void* old[] = {D.x, D.v, D.v_min, D.rho, D.rho_min, D.vof, D.vof_min, D.p, D.c, D.mass, D.hsml, D.sxx, D.sxy,
                        D.syy, D.sxx_min, D.sxy_min, D.syy_min, D.p_min, D.eps_p, D.itype, D.orig, D.fail, D.drho,
@@ -234,6 +245,13 @@ struct Engine : EngineBase {
         if (rc) return rc;
         PhaseDev<T>& D = P[ph];
         D.ntotal = h->ntotal; D.material = h->material; D.dspp = h->dspp;
+        double lo = INFINITY, hi = 0.0;
+        for (int i = 0; i < n; ++i) {
+            double v = h->hsml[i];
+            if (!(v > 0.0) || !std::isfinite(v)) return SPHG_ERR_BAD_ARG;
+            lo = std::min(lo, v); hi = std::max(hi, v);
+        }
+        hrange[ph][0] = lo; hrange[ph][1] = hi;
         // original order == state order until the first reorder
         if ((rc = launch("iota", k_iota, blocks(n, 256), 256, n, D.orig))) return rc;
         rc |= put_state(n, h->x, (double*)D.x, 2); rc |= put_state(n, h->vx, (double*)D.v, 2);
@@ -290,16 +308,11 @@ struct Engine : EngineBase {
         const sphg_params& p = ctx->prm;
         int sk = scale_k(p.skf);
         if (sk < 0) return SPHG_ERR_BAD_KERNEL;
-        // h range over all phases (read back once)
+        // h range over all phases (from the uploaded host arrays)
         double hmin = INFINITY, hmax = 0.0;
         for (int ph = 0; ph < ctx->nphase; ++ph) {
-            std::vector<double> h((size_t)P[ph].n);
-            CUDA_TRY(cudaMemcpyAsync(h.data(), P[ph].hsml, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, ctx->stream));
-            CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-            for (double v : h) {
-                if (!(v > 0.0) || !std::isfinite(v)) return SPHG_ERR_BAD_ARG;
-                hmin = std::min(hmin, v); hmax = std::max(hmax, v);
-            }
+            hmin = std::min(hmin, hrange[ph][0]);
+            hmax = std::max(hmax, hrange[ph][1]);
         }
         double cell = sk * hmax * (1.0 + 1e-6);
         if (!(p.x_max > p.x_min) || !(p.y_max > p.y_min)) return SPHG_ERR_BAD_ARG;
@@ -308,14 +321,17 @@ struct Engine : EngineBase {
         grid.ncx = (int)ncx; grid.ncy = (int)ncy; grid.x0 = p.x_min; grid.y0 = p.y_min; grid.inv = 1.0 / cell;
         int nc = grid.ncx * grid.ncy;
         if (nc != ncell) {
-            for (int ph = 0; ph < 2; ++ph) { release(counts[ph]); counts[ph] = nullptr; }
+            for (int ph = 0; ph < 2; ++ph) {
+                release(counts[ph]); counts[ph] = nullptr;
+                release(cell_start_buf[ph]); cell_start_buf[ph] = nullptr;
+            }
             release(cub_tmp); cub_tmp = nullptr;
             ncell = nc;
         }
         for (int ph = 0; ph < ctx->nphase; ++ph) {
             if (!counts[ph] && alloc(&counts[ph], (size_t)nc + 1)) return SPHG_ERR_CUDA;
-            release(P[ph].cell_start);
-            if (alloc(&P[ph].cell_start, (size_t)nc + 1)) return SPHG_ERR_CUDA;
+            if (!cell_start_buf[ph] && alloc(&cell_start_buf[ph], (size_t)nc + 1)) return SPHG_ERR_CUDA;
+            P[ph].cell_start = cell_start_buf[ph];
         }
         if (!cub_tmp) {
             size_t bytes = 0;
@@ -786,7 +802,7 @@ int sphg_set_stream(sphg_ctx* c, void* s) {
 int sphg_kernel_profile(sphg_ctx* c, int enable) {
     if (!c) return SPHG_ERR_BAD_ARG;
     c->prof.resolve();
-    if (enable) { c->prof.acc.clear(); c->prof.launches = 0; }
+    if (enable) c->prof.acc.clear();
     c->prof.on = enable != 0;
     return SPHG_OK;
 }

@@ -129,7 +129,10 @@ def _finish(p: Params, phases, width, height, dx, skf, precision):
     margin = 8 * dx
     p.x_min, p.x_max = -2 * dx - margin, width + 2 * dx + margin
     p.y_min, p.y_max = -2 * dx - margin, 2.0 * height + margin
-    p.max_interaction = int(16 * max(ph.n for ph in phases)) + 1024
+    # capacity of each pair list: ~12 pairs per particle at support 2h, scaled
+    # with the support area for the 3h kernels
+    sk = 3 if skf in (2, 3) else 2
+    p.max_interaction = int(3 * sk * sk * max(ph.n for ph in phases)) + 4096
 
 
 def dam_break(width=0.2, height=0.4, tank_w=0.8, tank_h=0.6, dx=0.005, skf=1,

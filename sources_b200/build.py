@@ -43,7 +43,10 @@ def build(force: bool = False, verbose: bool = False) -> str:
         return OUT
     os.makedirs(os.path.join(HERE, "_build"), exist_ok=True)
     tmp = OUT + ".tmp"
-    cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
+    # -prec-div/-prec-sqrt=false only affect float arithmetic (the FP32 pair
+    # mode); double division and sqrt stay IEEE.
+    cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-prec-div=false", "-prec-sqrt=false",
+           "-shared", "-Xcompiler", "-fPIC",
            "-Xptxas", "-v", "-o", tmp, SRC, "-lcudart"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     with open(os.path.join(HERE, "_build", "ptxas.log"), "w") as f:

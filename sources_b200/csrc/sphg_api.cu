@@ -418,6 +418,40 @@ struct Engine : EngineBase {
         return 0;
     }
 
+    // the pair passes of one right-hand side, for kernel function SKF
+    template <int SKF>
+    int passes() {
+        const sphg_params& p = ctx->prm;
+        const int tpb = SPHG_TPB;
+        int rc;
+        if (p.single_phase) {
+            PhaseDev<T>& D = P[0];
+            if (D.material == SPHG_WATER) {
+                if ((rc = launch("gather", k_gather<T>, blocks(D.n, 256), 256, D, sim, 0, 0, cnt))) return rc;
+                if ((rc = launch("water_sum", k_water_sum<T, SKF>, blocks(D.n, tpb), tpb, D, grid, sc_same, sim, cnt))) return rc;
+                if ((rc = launch("water_pass_a", k_water_pass_a<T, SKF, true>, blocks(D.n, tpb), tpb, D, grid, sc_same, sim, cnt))) return rc;
+                if ((rc = launch("water_pass_b", k_water_pass_b<T, SKF, true>, blocks(D.n, tpb), tpb, D, grid, sc_same, sim))) return rc;
+            } else {
+                if ((rc = launch("gather", k_gather<T>, blocks(D.n, 256), 256, D, sim, 1, sim.yield_dp, cnt))) return rc;
+                if (sim.plasticity == 3) CUDA_TRY(cudaMemsetAsync(&cnt->nfail, 0, sizeof(int), ctx->stream));
+                if ((rc = launch("soil_pass", k_soil_pass<T, SKF, true>, blocks(D.n, tpb), tpb, D, grid, sc_same, sim, cnt, 0))) return rc;
+            }
+        } else {
+            PhaseDev<T>& W = P[0];
+            PhaseDev<T>& S = P[1];
+            if ((rc = launch("gather", k_gather<T>, blocks(W.n, 256), 256, W, sim, 0, 0, cnt))) return rc;
+            if ((rc = launch("gather", k_gather<T>, blocks(S.n, 256), 256, S, sim, 1, sim.yield_dp, cnt))) return rc;
+            if ((rc = launch("water_pass_a", k_water_pass_a<T, SKF, false>, blocks(W.n, tpb), tpb, W, grid, sc_same, sim, cnt))) return rc;
+            if ((rc = launch("water_pass_b", k_water_pass_b<T, SKF, false>, blocks(W.n, tpb), tpb, W, grid, sc_same, sim))) return rc;
+            if (sim.plasticity == 3) CUDA_TRY(cudaMemsetAsync(&cnt->nfail, 0, sizeof(int), ctx->stream));
+            if ((rc = launch("soil_pass", k_soil_pass<T, SKF, false>, blocks(S.n, tpb), tpb, S, grid, sc_same, sim, cnt, 1))) return rc;
+            if ((rc = launch("cross_soil", k_cross_soil<T, SKF>, blocks(S.n, tpb), tpb, S, W, grid, sc_cross, sim))) return rc;
+            if ((rc = launch("cross_water", k_cross_water<T, SKF>, blocks(W.n, tpb), tpb, W, S, grid, sc_cross, sim, cnt))) return rc;
+            aliased = true;
+        }
+        return 0;
+    }
+
     // single_step / single_step_for_water / single_step_for_soil
     int rhs(int itimestep) override {
         int rc = prepare();
@@ -430,32 +464,13 @@ struct Engine : EngineBase {
             if ((rc = build_cells(ph))) return rc;
             if (reorder_now && (rc = reorder(ph))) return rc;
         }
-        const int tpb = SPHG_TPB;
-        if (p.single_phase) {
-            PhaseDev<T>& D = P[0];
-            if (D.material == SPHG_WATER) {
-                if ((rc = launch("gather", k_gather<T>, blocks(D.n, 256), 256, D, sim, 0, 0, cnt))) return rc;
-                if ((rc = launch("water_sum", k_water_sum<T>, blocks(D.n, tpb), tpb, D, grid, sc_same, sim, cnt))) return rc;
-                if ((rc = launch("water_pass_a", k_water_pass_a<T, true>, blocks(D.n, tpb), tpb, D, grid, sc_same, sim, cnt))) return rc;
-                if ((rc = launch("water_pass_b", k_water_pass_b<T, true>, blocks(D.n, tpb), tpb, D, grid, sc_same, sim))) return rc;
-            } else {
-                if ((rc = launch("gather", k_gather<T>, blocks(D.n, 256), 256, D, sim, 1, sim.yield_dp, cnt))) return rc;
-                if (sim.plasticity == 3) CUDA_TRY(cudaMemsetAsync(&cnt->nfail, 0, sizeof(int), ctx->stream));
-                if ((rc = launch("soil_pass", k_soil_pass<T, true>, blocks(D.n, tpb), tpb, D, grid, sc_same, sim, cnt, 0))) return rc;
-            }
-        } else {
-            PhaseDev<T>& W = P[0];
-            PhaseDev<T>& S = P[1];
-            if ((rc = launch("gather", k_gather<T>, blocks(W.n, 256), 256, W, sim, 0, 0, cnt))) return rc;
-            if ((rc = launch("gather", k_gather<T>, blocks(S.n, 256), 256, S, sim, 1, sim.yield_dp, cnt))) return rc;
-            if ((rc = launch("water_pass_a", k_water_pass_a<T, false>, blocks(W.n, tpb), tpb, W, grid, sc_same, sim, cnt))) return rc;
-            if ((rc = launch("water_pass_b", k_water_pass_b<T, false>, blocks(W.n, tpb), tpb, W, grid, sc_same, sim))) return rc;
-            if (sim.plasticity == 3) CUDA_TRY(cudaMemsetAsync(&cnt->nfail, 0, sizeof(int), ctx->stream));
-            if ((rc = launch("soil_pass", k_soil_pass<T, false>, blocks(S.n, tpb), tpb, S, grid, sc_same, sim, cnt, 1))) return rc;
-            if ((rc = launch("cross_soil", k_cross_soil<T>, blocks(S.n, tpb), tpb, S, W, grid, sc_cross, sim))) return rc;
-            if ((rc = launch("cross_water", k_cross_water<T>, blocks(W.n, tpb), tpb, W, S, grid, sc_cross, sim, cnt))) return rc;
-            aliased = true;
+        switch (p.skf) {
+            case 1: rc = passes<1>(); break;
+            case 2: rc = passes<2>(); break;
+            case 3: rc = passes<3>(); break;
+            default: rc = passes<4>(); break;
         }
+        if (rc) return rc;
         return launch("check", k_check, 1, 32, (const DevCounters*)cnt, sticky, (unsigned long long)p.max_interaction);
     }
 

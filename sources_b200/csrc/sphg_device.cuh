@@ -31,8 +31,9 @@ template <> struct V4<double> { typedef double4 t; };
 template <> struct V4<float> { typedef float4 t; };
 
 // Sorted-order neighbour records.  Fields are named for what the pair passes
-// read; `itype` is stored in T (values +-2, +-3 are exact).
-template <typename T> struct __align__(4 * sizeof(T)) RecA { T vx, vy, m, rho; };
+// read: vol = m/rho, so the particle mass is vol*rho; `itype` is stored in T
+// (values +-2, +-3 are exact).
+template <typename T> struct __align__(4 * sizeof(T)) RecA { T vx, vy, vol, rho; };
 template <typename T> struct __align__(4 * sizeof(T)) RecB { T p, c, vof, sxx, sxy, syy, itype, aux; };
 
 struct GridGeom {
@@ -219,4 +220,149 @@ __device__ __forceinline__ int warp_min(int v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(0xffffffffu, v, o));
     return v;
+}
+
+
+// ---------------------------------------------------------------------------
+// Smoothing kernel with the per-particle constants hoisted out of the pair
+// loop (every pair of a particle shares one h when all h are equal).
+// eval() returns W and the radial factor s with grad W = s * dx, so that
+// dx . grad W = s * r^2.  T = double keeps the IEEE sqrt and divisions of
+// the reference's expression; T = float uses rsqrt/reciprocal.
+template <typename T> __device__ __forceinline__ T rcp_(T x) { return T(1) / x; }
+template <> __device__ __forceinline__ float rcp_<float>(float x) { return __frcp_rn(x); }
+template <typename T> __device__ __forceinline__ T div_(T a, T b) { return a / b; }
+template <> __device__ __forceinline__ float div_<float>(float a, float b) { return __fdividef(a, b); }
+
+template <typename T> __device__ __forceinline__ T sqsum(T dx, T dy) { return dx * dx + dy * dy; }
+template <> __device__ __forceinline__ double sqsum<double>(double dx, double dy) {
+    return __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));
+}
+
+template <typename T, int SKF>
+struct KernelConst {
+    T h, inv_h, inv_h2, fac;
+    __device__ __forceinline__ void init(T hh) {
+        const T pi = (T)SPHG_PI_REF;
+        h = hh;
+        inv_h = T(1) / hh;
+        inv_h2 = inv_h * inv_h;
+        if (SKF == 1) fac = T(15) / (T(7) * pi * hh * hh);
+        else if (SKF == 2) fac = T(1) / ((hh * hh) * pi);
+        else if (SKF == 3) fac = T(7) / (T(478) * pi * hh * hh);
+        else fac = T(7) / (T(4) * pi * hh * hh);
+    }
+    // r2 = dx^2 + dy^2 of the pair
+    __device__ __forceinline__ void eval(T r2, T& w, T& s) const {
+        T r, rinv;
+        if (sizeof(T) == 8) { r = sqrt(r2); rinv = T(1) / r; }
+        else {
+            rinv = (T)rsqrtf((float)fmaxf((float)r2, 1e-30f));
+            r = r2 * rinv;
+        }
+        const T q = sizeof(T) == 8 ? r / h : r * inv_h;
+        w = T(0); s = T(0);
+        if (SKF == 1) {
+            if (q <= T(1)) {
+                w = fac * ((T)SPHG_F32LIT(2.0f / 3.0f) - q * q + q * q * q / T(2));
+                s = fac * (T(-2) + T(1.5) * q) * inv_h2;
+            } else if (q <= T(2)) {
+                const T u = T(2) - q;
+                w = fac / T(6) * (u * u * u);
+                s = -(fac / T(6) * T(3) * (u * u) * inv_h) * rinv;
+            }
+        } else if (SKF == 2) {
+            if (q <= T(3)) {
+                w = fac * exp(-q * q);
+                s = w * T(-2) * inv_h2;
+            }
+        } else if (SKF == 3) {
+            const T a = T(3) - q, b = T(2) - q, c = T(1) - q;
+            const T a4 = a * a * a * a, b4 = b * b * b * b, c4 = c * c * c * c;
+            if (q <= T(1)) {
+                w = fac * (a4 * a - T(6) * (b4 * b) + T(15) * (c4 * c));
+                s = fac * (T(-120) + T(120) * q - T(50) * (q * q)) * inv_h2;   // as m_particles.f90:1554
+            } else if (q <= T(2)) {
+                w = fac * (a4 * a - T(6) * (b4 * b));
+                s = fac * (T(-5) * a4 + T(30) * b4) * inv_h * rinv;
+            } else if (q <= T(3)) {
+                w = fac * (a4 * a);
+                s = fac * (T(-5) * a4) * inv_h * rinv;
+            }
+        } else {
+            if (q <= T(2)) {
+                const T u = T(1) - q / T(2);
+                w = fac * ((u * u * u * u) * (T(1) + T(2) * q));
+                s = fac * (T(-5) + T(15) * q / T(2) - T(15) * (q * q) / T(4) + T(5) * (q * q * q) / T(8)) * inv_h2;
+            }
+        }
+    }
+};
+
+// Per-thread hit buffer in shared memory: entry i of thread t at [i*TPB + t],
+// so a warp's accesses are conflict-free.
+template <typename T, int TPB, int CH>
+struct HitBuf {
+    int m[CH * TPB];
+    T dx[CH * TPB];
+    T dy[CH * TPB];
+};
+
+// Warp-synchronous neighbour visitor.  Each lane scans the candidates of its
+// particle (three row segments of the sorted list) with the exact FP64 pair
+// test and appends hits to its buffer; as soon as any lane's buffer is full,
+// or every lane has finished scanning, the whole warp drains the buffers
+// through body(m, dx, dy) together.  Scanning (cheap, divergent) and pair
+// physics (expensive) thus run with full lanes instead of the body executing
+// under the hit/miss divergence of the scan.  All 32 lanes must call it;
+// `active` marks lanes that own a particle.
+template <typename T, int TPB, int CH, class F>
+__device__ __forceinline__ int visit_batched(HitBuf<T, TPB, CH>& buf, const GridGeom& g, const SearchConst& sc,
+                                             const int* __restrict__ cstart, const double2* __restrict__ xs,
+                                             const double* __restrict__ hs, double2 xa, double ha, int self,
+                                             bool active, F&& body) {
+    const unsigned FULL = 0xffffffffu;
+    const int tid = threadIdx.x;
+    int b0 = 0, b1 = 0, b2 = 0, L0 = 0, L1 = 0, L2 = 0;
+    if (active) {
+        int cx, cy; bool clamped;
+        cell_coords(g, xa.x, xa.y, cx, cy, clamped);
+        const int x0 = cx > 0 ? cx - 1 : 0;
+        const int x1 = cx < g.ncx - 1 ? cx + 1 : g.ncx - 1;
+        if (cy - 1 >= 0) { b0 = __ldg(cstart + (cy - 1) * g.ncx + x0); L0 = __ldg(cstart + (cy - 1) * g.ncx + x1 + 1) - b0; }
+        b1 = __ldg(cstart + cy * g.ncx + x0); L1 = __ldg(cstart + cy * g.ncx + x1 + 1) - b1;
+        if (cy + 1 < g.ncy) { b2 = __ldg(cstart + (cy + 1) * g.ncx + x0); L2 = __ldg(cstart + (cy + 1) * g.ncx + x1 + 1) - b2; }
+    }
+    const int tot = L0 + L1 + L2;
+    int t = 0, cnt = 0, hits = 0;
+    bool more = true;
+    while (more) {
+        while (true) {
+            more = __any_sync(FULL, t < tot);
+            if (!more || __any_sync(FULL, cnt == CH)) break;
+            if (t < tot) {
+                const int m = t < L0 ? b0 + t : (t < L0 + L1 ? b1 + (t - L0) : b2 + (t - L0 - L1));
+                ++t;
+                if (m != self) {
+                    const double2 xb = xs[m];
+                    const double dx = xa.x - xb.x;
+                    const double dy = xa.y - xb.y;
+                    const double r2 = __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));
+                    const bool hit = sc.uniform ? (r2 < sc.r2_uniform)
+                                                : (__dsqrt_rn(r2) < sc.scale_k * ((ha + hs[m]) / 2.0));
+                    if (hit) {
+                        buf.m[cnt * TPB + tid] = m;
+                        buf.dx[cnt * TPB + tid] = (T)dx;
+                        buf.dy[cnt * TPB + tid] = (T)dy;
+                        ++cnt;
+                        ++hits;
+                    }
+                }
+            }
+        }
+        for (int i = 0; __any_sync(FULL, i < cnt); ++i)
+            if (i < cnt) body(buf.m[i * TPB + tid], buf.dx[i * TPB + tid], buf.dy[i * TPB + tid]);
+        cnt = 0;
+    }
+    return hits;
 }

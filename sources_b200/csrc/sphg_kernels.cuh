@@ -90,7 +90,8 @@ __global__ void __launch_bounds__(256) k_gather(PhaseDev<T> P, SimConst c, int s
         P.hs[k] = P.hsml[a];
         double2 v = P.v[a];
         RecA<T> ra;
-        ra.vx = (T)v.x; ra.vy = (T)v.y; ra.m = (T)P.mass[a]; ra.rho = (T)P.rho[a];
+        const double rho = P.rho[a];
+        ra.vx = (T)v.x; ra.vy = (T)v.y; ra.vol = (T)(P.mass[a] / rho); ra.rho = (T)rho;
         P.recA[k] = ra;
         if (soil) {
             double p = P.p[a], sxx = P.sxx[a], sxy = P.sxy[a], syy = P.syy[a];
@@ -134,41 +135,69 @@ __device__ __forceinline__ void count_stats(DevCounters* cnt, int list, int phas
     }
 }
 
+// hit-buffer depth per thread: 24 covers the ~20 neighbours of a particle at
+// support 2h = 2.4 dx in one drain (FP32); FP64 entries are larger.
+template <typename T> struct Chunk { static const int value = sizeof(T) == 4 ? 24 : 16; };
+#define SPHG_HITBUF(T) __shared__ HitBuf<T, SPHG_TPB, Chunk<T>::value> hb
+
+// Kernel constants for particle a: per particle when every h is equal, else
+// per pair (mhsml = (h_a + h_b)/2).
+template <typename T, int SKF>
+__device__ __forceinline__ void pair_kernel(const KernelConst<T, SKF>& ka, const SearchConst& sc, double ha,
+                                            const double* __restrict__ hs, int m, T dx, T dy, T& w, T& s, T& r2,
+                                            T& mh) {
+    r2 = sqsum<T>(dx, dy);
+    if (sc.uniform) {
+        ka.eval(r2, w, s);
+        mh = ka.h;
+    } else {
+        KernelConst<T, SKF> kb;
+        const double mhd = (ha + hs[m]) / 2.0;
+        kb.init((T)mhd);
+        kb.eval(r2, w, s);
+        mh = (T)mhd;
+    }
+}
+
 // ------------------------------------------------------ water: summation rho
 // sum_density (m_particles.f90:2243-2298) and the df2 divergence of the
 // water-only step, drho = -rho*(df2(vx,'x') + df2(vy,'y'))
 // (declarations_sph.f90:1465-1466, df2 m_particles.f90:1802-1831).
-template <typename T>
+template <typename T, int SKF>
 __global__ void __launch_bounds__(SPHG_TPB) k_water_sum(PhaseDev<T> P, GridGeom g, SearchConst sc, SimConst c, DevCounters* cnt) {
-    int k = gtid();
-    bool valid = k < P.n;
-    int hits = 0;
+    SPHG_HITBUF(T);
+    const int k = gtid();
+    const bool valid = k < P.n;
+    const int kk = valid ? k : 0;
+    const double2 xa = P.xs[kk];
+    const double ha = P.hs[kk];
+    const RecA<T> ra = P.recA[kk];
+    KernelConst<T, SKF> ka;
+    ka.init((T)ha);
+    T w0, s0;
+    ka.eval(T(0), w0, s0);
+    const T ma = ra.vol * ra.rho;
+    T wi = w0 * ma / ra.rho;
+    T num = w0 * ma;
+    T sx = T(0), sy = T(0);
+    const RecA<T>* __restrict__ rec = P.recA;
+    const int hits = visit_batched(hb, g, sc, P.cell_start, P.xs, P.hs, xa, ha, k, valid, [&](int m, T dx, T dy) {
+        const RecA<T> rb = rec[m];
+        T w, sr, r2, mh;
+        pair_kernel<T, SKF>(ka, sc, ha, P.hs, m, dx, dy, w, sr, r2, mh);
+        const T mb = rb.vol * rb.rho;
+        wi += rb.vol * w;
+        num += mb * w;
+        sx += mb * ((rb.vx - ra.vx) * (sr * dx));
+        sy += mb * ((rb.vy - ra.vy) * (sr * dy));
+    });
     if (valid) {
         const int a = P.perm[k];
-        const double2 xa = P.xs[k];
-        const double ha = P.hs[k];
-        const RecA<T> ra = P.recA[k];
-        T w0, g0x, g0y;
-        sph_kernel<T>(c.skf, T(0), T(0), T(0), (T)ha, w0, g0x, g0y);
-        T wi = w0 * ra.m / ra.rho;
-        T num = w0 * ra.m;
-        T sx = T(0), sy = T(0);
-        const RecA<T>* __restrict__ rec = P.recA;
-        hits = visit_neighbours(g, sc, P.cell_start, P.xs, P.hs, xa, ha, k,
-            [&](int m, double dx, double dy, double r2, double mh) {
-                const RecA<T> rb = rec[m];
-                T w, gx, gy;
-                sph_kernel<T>(c.skf, (T)sqrt(r2), (T)dx, (T)dy, (T)mh, w, gx, gy);
-                wi += rb.m / rb.rho * w;
-                num += rb.m * w;
-                sx += rb.m * ((rb.vx - ra.vx) * gx);
-                sy += rb.m * ((rb.vy - ra.vy) * gy);
-            });
         const T rho = num / wi;
         P.rho[a] = (double)rho;
         P.drho[a] = -rho * (sx / rho + sy / rho);
         RecA<T> r2;
-        r2.vx = ra.vx; r2.vy = ra.vy; r2.m = ra.m; r2.rho = rho;
+        r2.vx = ra.vx; r2.vy = ra.vy; r2.vol = (T)(P.mass[a] / (double)rho); r2.rho = rho;
         P.recA2[k] = r2;
         P.countiac[a] = hits;
     }
@@ -181,48 +210,46 @@ __global__ void __launch_bounds__(SPHG_TPB) k_water_sum(PhaseDev<T> P, GridGeom 
 //   pressure :2133 (Tait with vof, c ~ (rho/rho0 vof)^3), newtonian_fluid :2484.
 // Water-only (SINGLE = true), declarations_sph.f90:1471-1490:
 //   delta_sph on the summation density, Tait without vof, t = df(v) form.
-template <typename T, bool SINGLE>
+// delta_sph's (dx . grad W) 2 (f_a - f_b) / r^2 is evaluated as 2 s (f_a - f_b)
+// since grad W = s dx.
+template <typename T, int SKF, bool SINGLE>
 __global__ void __launch_bounds__(SPHG_TPB) k_water_pass_a(PhaseDev<T> P, GridGeom g, SearchConst sc, SimConst c, DevCounters* cnt) {
-    int k = gtid();
-    bool valid = k < P.n;
-    int hits = 0;
+    SPHG_HITBUF(T);
+    const int k = gtid();
+    const bool valid = k < P.n;
+    const int kk = valid ? k : 0;
+    const int a = P.perm[kk];
+    const double2 xa = P.xs[kk];
+    const double ha = P.hs[kk];
+    const RecA<T>* __restrict__ rec = SINGLE ? P.recA2 : P.recA;
+    const RecA<T> ra = rec[kk];
+    const T pref = (T)(c.delta * ha * P.c[a]);   // delta*hsml(i)*c(i), c of the previous EOS call
+    const T c23 = (T)SPHG_F32LIT(2.0f / 3.0f);
+    const bool dens = c.artificial_density;
+    KernelConst<T, SKF> ka;
+    ka.init((T)ha);
+    T con = 0, dl = 0, t0 = 0, t1 = 0, t2 = 0, t3 = 0;
+    const int hits = visit_batched(hb, g, sc, P.cell_start, P.xs, P.hs, xa, ha, k, valid, [&](int m, T dx, T dy) {
+        const RecA<T> rb = rec[m];
+        T w, sr, r2, mh;
+        pair_kernel<T, SKF>(ka, sc, ha, P.hs, m, dx, dy, w, sr, r2, mh);
+        const T gx = sr * dx, gy = sr * dy;
+        if (!SINGLE) con += (rb.vol * rb.rho) * ((ra.vx - rb.vx) * gx + (ra.vy - rb.vy) * gy);
+        if (dens) dl += pref * rb.vol * ((ra.rho - rb.rho) * (T(2) * sr));
+        if (SINGLE) {   // df(vx,'x'), df(vy,'y'), df(vx,'y'), df(vy,'x')
+            const T su = ra.vx + rb.vx, sv = ra.vy + rb.vy;
+            t0 += rb.vol * (su * gx);
+            t1 += rb.vol * (sv * gy);
+            t2 += rb.vol * (su * gy);
+            t3 += rb.vol * (sv * gx);
+        } else {        // shear_strain_rate, dv = v_b - v_a
+            const T du = rb.vx - ra.vx, dv = rb.vy - ra.vy;
+            t0 += rb.vol * (c23 * (T(2) * du * gx - dv * gy));
+            t1 += rb.vol * (du * gy + dv * gx);
+            t2 += rb.vol * (c23 * (T(2) * dv * gy - du * gx));
+        }
+    });
     if (valid) {
-        const int a = P.perm[k];
-        const double2 xa = P.xs[k];
-        const double ha = P.hs[k];
-        const RecA<T>* __restrict__ rec = SINGLE ? P.recA2 : P.recA;
-        const RecA<T> ra = rec[k];
-        const T pref = (T)(c.delta * ha * P.c[a]);   // delta*hsml(i)*c(i), c of the previous EOS call
-        const T c23 = (T)SPHG_F32LIT(2.0f / 3.0f);
-        T con = 0, dl = 0, t0 = 0, t1 = 0, t2 = 0, t3 = 0;
-        hits = visit_neighbours(g, sc, P.cell_start, P.xs, P.hs, xa, ha, k,
-            [&](int m, double dx, double dy, double r2, double mh) {
-                const RecA<T> rb = rec[m];
-                T w, gx, gy;
-                const T tdx = (T)dx, tdy = (T)dy, rr = (T)r2;
-                sph_kernel<T>(c.skf, (T)sqrt(r2), tdx, tdy, (T)mh, w, gx, gy);
-                if (!SINGLE) con += rb.m * ((ra.vx - rb.vx) * gx + (ra.vy - rb.vy) * gy);
-                if (c.artificial_density) {
-                    const T muv = T(2) * (ra.rho - rb.rho) / rr;
-                    const T h = tdx * muv * gx + tdy * muv * gy;
-                    dl += pref * rb.m * h / rb.rho;
-                }
-                if (SINGLE) {   // df(vx,'x'), df(vy,'y'), df(vx,'y'), df(vy,'x')
-                    const T vb = rb.m / rb.rho;
-                    t0 += vb * ((ra.vx + rb.vx) * gx);
-                    t1 += vb * ((ra.vy + rb.vy) * gy);
-                    t2 += vb * ((ra.vx + rb.vx) * gy);
-                    t3 += vb * ((ra.vy + rb.vy) * gx);
-                } else {        // shear_strain_rate, dv = v_b - v_a
-                    const T du = rb.vx - ra.vx, dv = rb.vy - ra.vy;
-                    const T hxx = c23 * (T(2) * du * gx - dv * gy);
-                    const T hxy = du * gy + dv * gx;
-                    const T hyy = c23 * (T(2) * dv * gy - du * gx);
-                    t0 += rb.m * hxx / rb.rho;
-                    t1 += rb.m * hxy / rb.rho;
-                    t2 += rb.m * hyy / rb.rho;
-                }
-            });
         T txx, txy, tyy, drho;
         double p, cnew, vof;
         const double rho = P.rho[a];
@@ -264,89 +291,93 @@ __global__ void __launch_bounds__(SPHG_TPB) k_water_pass_a(PhaseDev<T> P, GridGe
 // (declarations_sph.f90:1257-1265; df m_particles.f90:1711), art_visc :2504,
 // delta_sph(vof) :2658, repulsive_force :1605, gravity, av_vel :2761.
 // The water-only step (declarations_sph.f90:1494-1518) is the same with
-// vof = 1 and neither wall force nor delta-SPH on vof.
-template <typename T, bool SINGLE>
+// vof = 1 and neither wall force nor delta-SPH on vof.  The wall force takes
+// dx = x_real - x_virtual, as the reference does with real particles
+// numbered before virtual ones.
+template <typename T, int SKF, bool SINGLE>
 __global__ void __launch_bounds__(SPHG_TPB) k_water_pass_b(PhaseDev<T> P, GridGeom g, SearchConst sc, SimConst c) {
     typedef typename V2<T>::t T2;
-    int k = gtid();
-    if (k >= P.n) return;
-    const int a = P.perm[k];
-    const double2 xa = P.xs[k];
-    const double ha = P.hs[k];
+    SPHG_HITBUF(T);
+    const int k = gtid();
+    const bool valid = k < P.n;
+    const int kk = valid ? k : 0;
+    const int a = P.perm[kk];
+    const double2 xa = P.xs[kk];
+    const double ha = P.hs[kk];
     const RecA<T>* __restrict__ rec = SINGLE ? P.recA2 : P.recA;
-    const RecA<T> ra = rec[k];
-    const RecB<T> qa = P.recB[k];
+    const RecA<T> ra = rec[kk];
+    const RecB<T> qa = P.recB[kk];
     const bool real_a = P.itype[a] > 0;
     const T phia = qa.vof;
     const T fa_xx = phia * qa.sxx, fa_xy = phia * qa.sxy, fa_yy = phia * qa.syy;
     const T pref = (T)(c.delta * ha) * qa.c;
-    const T alpha = (T)c.alpha, beta = (T)c.beta, etq = (T)c.etq;
+    const T alpha = (T)c.alpha, beta = (T)c.beta, etq2 = (T)(c.etq * c.etq);
     const T r0 = (T)P.dspp, dd = (T)c.dd, p1 = (T)c.p1, p2 = (T)c.p2;
-    const bool do_rep = !SINGLE;
+    const bool do_rep = !SINGLE && real_a;
     const bool do_dvof = !SINGLE && c.water_artificial_volume;
+    const bool visc = c.visc_artificial, xsph = c.average_velocity;
+    KernelConst<T, SKF> ka;
+    ka.init((T)ha);
     T d1x = 0, d1y = 0, d2x = 0, d3x = 0, d2y = 0, d3y = 0;
     T avx = 0, avy = 0, rpx = 0, rpy = 0, dvf = 0, xsx = 0, xsy = 0;
-    visit_neighbours(g, sc, P.cell_start, P.xs, P.hs, xa, ha, k,
-        [&](int m, double dx, double dy, double r2, double mh) {
-            const RecA<T> rb = rec[m];
-            const RecB<T> qb = P.recB[m];
-            T w, gx, gy;
-            const T tdx = (T)dx, tdy = (T)dy, rr = (T)r2;
-            sph_kernel<T>(c.skf, (T)sqrt(r2), tdx, tdy, (T)mh, w, gx, gy);
-            const T vb = rb.m / rb.rho;
-            const T pp = qa.p + qb.p;
-            d1x += vb * (pp * gx);
-            d1y += vb * (pp * gy);
-            const T sxx = fa_xx + qb.vof * qb.sxx, sxy = fa_xy + qb.vof * qb.sxy, syy = fa_yy + qb.vof * qb.syy;
-            d2x += vb * (sxx * gx);
-            d3x += vb * (sxy * gy);
-            d2y += vb * (sxy * gx);
-            d3y += vb * (syy * gy);
-            const T dvx = ra.vx - rb.vx, dvy = ra.vy - rb.vy;
-            if (c.visc_artificial) {
-                const T vr = dvx * tdx + dvy * tdy;
-                if (vr < T(0)) {
-                    const T tmh = (T)mh;
-                    const T muv = tmh * vr / (rr + tmh * tmh * etq * etq);
-                    const T mc = T(0.5) * (qa.c + qb.c);
-                    const T mrho = T(0.5) * (ra.rho + rb.rho);
-                    const T piv = (beta * muv - alpha * mc) * muv / mrho;
-                    avx += rb.m * (-piv * gx);
-                    avy += rb.m * (-piv * gy);
-                }
+    visit_batched(hb, g, sc, P.cell_start, P.xs, P.hs, xa, ha, k, valid, [&](int m, T dx, T dy) {
+        const RecA<T> rb = rec[m];
+        const RecB<T> qb = P.recB[m];
+        T w, sr, rr, mh;
+        pair_kernel<T, SKF>(ka, sc, ha, P.hs, m, dx, dy, w, sr, rr, mh);
+        const T gx = sr * dx, gy = sr * dy;
+        const T vb = rb.vol;
+        const T pp = qa.p + qb.p;
+        d1x += vb * (pp * gx);
+        d1y += vb * (pp * gy);
+        const T sxx = fa_xx + qb.vof * qb.sxx, sxy = fa_xy + qb.vof * qb.sxy, syy = fa_yy + qb.vof * qb.syy;
+        d2x += vb * (sxx * gx);
+        d3x += vb * (sxy * gy);
+        d2y += vb * (sxy * gx);
+        d3y += vb * (syy * gy);
+        const T dvx = ra.vx - rb.vx, dvy = ra.vy - rb.vy;
+        const T mb = vb * rb.rho;
+        if (visc) {
+            const T vr = dvx * dx + dvy * dy;
+            if (vr < T(0)) {
+                const T muv = div_<T>(mh * vr, rr + mh * mh * etq2);
+                const T mc = T(0.5) * (qa.c + qb.c);
+                const T mrho = T(0.5) * (ra.rho + rb.rho);
+                const T piv = div_<T>((beta * muv - alpha * mc) * muv, mrho);
+                avx -= mb * (piv * gx);
+                avy -= mb * (piv * gy);
             }
-            if (do_dvof) {
-                const T muv = T(2) * (phia - qb.vof) / rr;
-                const T h = tdx * muv * gx + tdy * muv * gy;
-                dvf += pref * rb.m * h / rb.rho;
+        }
+        if (do_dvof) dvf += pref * vb * ((phia - qb.vof) * (T(2) * sr));
+        if (do_rep && qb.itype < T(0)) {
+            const T r = sqrt(rr);
+            if (!(r > r0)) {
+                const T f = (pow(r0 / r, p1) - pow(r0 / r, p2)) / (r * r);
+                rpx += dd * dx * f;
+                rpy += dd * dy * f;
             }
-            if (do_rep && real_a && qb.itype < T(0)) {
-                const T r = (T)sqrt(r2);
-                if (!(r > r0)) {
-                    const T f = (pow(r0 / r, p1) - pow(r0 / r, p2)) / (r * r);
-                    rpx += dd * tdx * f;
-                    rpy += dd * tdy * f;
-                }
-            }
-            if (c.average_velocity) {
-                const T mrho = (ra.rho + rb.rho) / T(2);
-                xsx -= rb.m * dvx / mrho * w;
-                xsy -= rb.m * dvy / mrho * w;
-            }
-        });
-    T dvx = -(phia * d1x) + d2x + d3x;
-    T dvy = -(phia * d1y) + d2y + d3y;
-    if (ra.rho > T(0)) { dvx = dvx / ra.rho; dvy = dvy / ra.rho; }
-    dvx = dvx + avx + rpx;
-    dvy = dvy + avy + rpy + (T)c.gravity;
-    T2 o; o.x = dvx; o.y = dvy;
-    P.dv[a] = o;
-    if (c.average_velocity) {
-        const T eps = (T)c.epsilon;
-        T2 av; av.x = real_a ? eps * xsx : xsx; av.y = real_a ? eps * xsy : xsy;
-        P.av[a] = av;
+        }
+        if (xsph) {
+            const T q = div_<T>(mb * w, (ra.rho + rb.rho) / T(2));
+            xsx -= q * dvx;
+            xsy -= q * dvy;
+        }
+    });
+    if (valid) {
+        T dvx = -(phia * d1x) + d2x + d3x;
+        T dvy = -(phia * d1y) + d2y + d3y;
+        if (ra.rho > T(0)) { dvx = dvx / ra.rho; dvy = dvy / ra.rho; }
+        dvx = dvx + avx + rpx;
+        dvy = dvy + avy + rpy + (T)c.gravity;
+        T2 o; o.x = dvx; o.y = dvy;
+        P.dv[a] = o;
+        if (xsph) {
+            const T eps = (T)c.epsilon;
+            T2 av; av.x = real_a ? eps * xsx : xsx; av.y = real_a ? eps * xsy : xsy;
+            P.av[a] = av;
+        }
+        if (!SINGLE) P.dvof[a] = dvf;
     }
-    if (!SINGLE) P.dvof[a] = dvf;
 }
 
 // ------------------------------------------------------------------ soil
@@ -357,105 +388,106 @@ __global__ void __launch_bounds__(SPHG_TPB) k_water_pass_b(PhaseDev<T> P, GridGe
 // s, repulsive_force (two-phase only), gravity, av_vel; then per particle
 // plastic_or_not :3447, plastic_flow_rule3 :3700 and Jaumann_rate :3047,
 // whose spin sum wxy comes from the same pass.
-template <typename T, bool SINGLE>
+template <typename T, int SKF, bool SINGLE>
 __global__ void __launch_bounds__(SPHG_TPB) k_soil_pass(PhaseDev<T> P, GridGeom g, SearchConst sc, SimConst c,
                                                        DevCounters* cnt, int slot) {
     typedef typename V2<T>::t T2;
-    int k = gtid();
-    bool valid = k < P.n;
-    int hits = 0, fail = 0;
+    SPHG_HITBUF(T);
+    const int k = gtid();
+    const bool valid = k < P.n;
+    const int kk = valid ? k : 0;
+    const int a = P.perm[kk];
+    const double2 xa = P.xs[kk];
+    const double ha = P.hs[kk];
+    const RecA<T> ra = P.recA[kk];
+    const RecB<T> qa = P.recB[kk];
+    const bool real_a = P.itype[a] > 0;
+    const T cs = (T)c.s_c;                          // pressure(): c = soil%c
+    const T pref_old = (T)(c.delta * ha) * qa.c;    // delta_sph(rho) runs before pressure()
+    const T pref = (T)(c.delta * ha) * cs;
+    const T c23 = (T)SPHG_F32LIT(2.0f / 3.0f);
+    const T alpha = (T)c.alpha, beta = (T)c.beta, etq2 = (T)(c.etq * c.etq);
+    const T r0 = (T)P.dspp, dd = (T)c.dd, p1 = (T)c.p1, p2 = (T)c.p2;
+    const T phia = SINGLE ? T(1) : qa.vof;
+    const T fap = phia * qa.p, faxx = phia * qa.sxx, faxy = phia * qa.sxy, fayy = phia * qa.syy;
+    const T ira2 = T(1) / (ra.rho * ra.rho);
+    const bool dens = c.artificial_density, visc = c.visc_artificial, xsph = c.average_velocity;
+    const bool dstress = c.soil_artificial_stress, do_rep = !SINGLE && real_a;
+    KernelConst<T, SKF> ka;
+    ka.init((T)ha);
+    T con = 0, dl = 0, txx = 0, txy = 0, tyy = 0, vcc = 0, wxy = 0;
+    T s1x = 0, s1y = 0, s2x = 0, s3x = 0, s2y = 0, s3y = 0;
+    T avx = 0, avy = 0, rpx = 0, rpy = 0, xsx = 0, xsy = 0;
+    T dpp = 0, dsx = 0, dsxy = 0, dsy = 0;
+    const int hits = visit_batched(hb, g, sc, P.cell_start, P.xs, P.hs, xa, ha, k, valid, [&](int m, T dx, T dy) {
+        const RecA<T> rb = P.recA[m];
+        const RecB<T> qb = P.recB[m];
+        T w, sr, rr, mh;
+        pair_kernel<T, SKF>(ka, sc, ha, P.hs, m, dx, dy, w, sr, rr, mh);
+        const T gx = sr * dx, gy = sr * dy;
+        const T du = rb.vx - ra.vx, dv = rb.vy - ra.vy;   // v_b - v_a
+        const T vb = rb.vol, mb = vb * rb.rho;
+        const T e = T(2) * sr;                            // 2 (dx . grad W) / r^2
+        con -= mb * (du * gx + dv * gy);
+        if (dens) dl += pref_old * vb * ((ra.rho - rb.rho) * e);
+        txx += vb * (c23 * (T(2) * du * gx - dv * gy));
+        txy += vb * (du * gy + dv * gx);
+        tyy += vb * (c23 * (T(2) * dv * gy - du * gx));
+        vcc += vb * (du * gx + dv * gy);
+        wxy += vb * (T(0.5) * (du * gy - dv * gx));
+        if (SINGLE) {       // df: m_b/rho_b (f_a + f_b) gradW
+            const T pp = fap + qb.p;
+            s1x += vb * (pp * gx); s1y += vb * (pp * gy);
+            s2x += vb * ((faxx + qb.sxx) * gx);
+            s3x += vb * ((faxy + qb.sxy) * gy);
+            s2y += vb * ((faxy + qb.sxy) * gx);
+            s3y += vb * ((fayy + qb.syy) * gy);
+        } else {            // df3: m_b (f_a/rho_a^2 + f_b/rho_b^2) gradW
+            const T irb = rcp_<T>(rb.rho);
+            const T ib = qb.vof * irb * irb;
+            const T pp = fap * ira2 + qb.p * ib;
+            s1x += mb * (pp * gx); s1y += mb * (pp * gy);
+            const T xx = faxx * ira2 + qb.sxx * ib;
+            const T xy = faxy * ira2 + qb.sxy * ib;
+            const T yy = fayy * ira2 + qb.syy * ib;
+            s2x += mb * (xx * gx);
+            s3x += mb * (xy * gy);
+            s2y += mb * (xy * gx);
+            s3y += mb * (yy * gy);
+        }
+        if (visc) {
+            const T vr = -(du * dx + dv * dy);
+            if (vr < T(0)) {
+                const T muv = div_<T>(mh * vr, rr + mh * mh * etq2);
+                const T mrho = T(0.5) * (ra.rho + rb.rho);
+                const T piv = div_<T>((beta * muv - alpha * cs) * muv, mrho);
+                avx -= mb * (piv * gx);
+                avy -= mb * (piv * gy);
+            }
+        }
+        if (dstress) {
+            const T q = pref * vb * e;
+            dpp += q * (qa.p - qb.p);
+            dsx += q * (qa.sxx - qb.sxx);
+            dsxy += q * (qa.sxy - qb.sxy);
+            dsy += q * (qa.syy - qb.syy);
+        }
+        if (do_rep && qb.itype < T(0)) {
+            const T r = sqrt(rr);
+            if (!(r > r0)) {
+                const T f = (pow(r0 / r, p1) - pow(r0 / r, p2)) / (r * r);
+                rpx += dd * dx * f;
+                rpy += dd * dy * f;
+            }
+        }
+        if (xsph) {
+            const T q = div_<T>(mb * w, (ra.rho + rb.rho) / T(2));
+            xsx += q * du;
+            xsy += q * dv;
+        }
+    });
+    int fail = 0;
     if (valid) {
-        const int a = P.perm[k];
-        const double2 xa = P.xs[k];
-        const double ha = P.hs[k];
-        const RecA<T> ra = P.recA[k];
-        const RecB<T> qa = P.recB[k];
-        const bool real_a = P.itype[a] > 0;
-        const T cs = (T)c.s_c;                          // pressure(): c = soil%c
-        const T pref_old = (T)(c.delta * ha) * qa.c;    // delta_sph(rho) runs before pressure()
-        const T pref = (T)(c.delta * ha) * cs;
-        const T c23 = (T)SPHG_F32LIT(2.0f / 3.0f);
-        const T alpha = (T)c.alpha, beta = (T)c.beta, etq = (T)c.etq;
-        const T r0 = (T)P.dspp, dd = (T)c.dd, p1 = (T)c.p1, p2 = (T)c.p2;
-        const T phia = SINGLE ? T(1) : qa.vof;
-        const T fap = phia * qa.p, faxx = phia * qa.sxx, faxy = phia * qa.sxy, fayy = phia * qa.syy;
-        const T ira2 = T(1) / (ra.rho * ra.rho);
-        T con = 0, dl = 0, txx = 0, txy = 0, tyy = 0, vcc = 0, wxy = 0;
-        T s1x = 0, s1y = 0, s2x = 0, s3x = 0, s2y = 0, s3y = 0;
-        T avx = 0, avy = 0, rpx = 0, rpy = 0, xsx = 0, xsy = 0;
-        T dpp = 0, dsx = 0, dsxy = 0, dsy = 0;
-        hits = visit_neighbours(g, sc, P.cell_start, P.xs, P.hs, xa, ha, k,
-            [&](int m, double dx, double dy, double r2, double mh) {
-                const RecA<T> rb = P.recA[m];
-                const RecB<T> qb = P.recB[m];
-                T w, gx, gy;
-                const T tdx = (T)dx, tdy = (T)dy, rr = (T)r2;
-                sph_kernel<T>(c.skf, (T)sqrt(r2), tdx, tdy, (T)mh, w, gx, gy);
-                const T du = rb.vx - ra.vx, dv = rb.vy - ra.vy;   // v_b - v_a
-                con += rb.m * ((-du) * gx + (-dv) * gy);
-                const T e = T(2) * (tdx * gx + tdy * gy) / rr;     // 2 (dx.gradW) / r^2
-                if (c.artificial_density) dl += pref_old * rb.m * ((ra.rho - rb.rho) * e) / rb.rho;
-                const T hxx = c23 * (T(2) * du * gx - dv * gy);
-                const T hxy = du * gy + dv * gx;
-                const T hyy = c23 * (T(2) * dv * gy - du * gx);
-                txx += rb.m * hxx / rb.rho;
-                txy += rb.m * hxy / rb.rho;
-                tyy += rb.m * hyy / rb.rho;
-                vcc += rb.m * (du * gx + dv * gy) / rb.rho;
-                wxy += rb.m * (T(0.5) * (du * gy - dv * gx)) / rb.rho;
-                const T phib = SINGLE ? T(1) : qb.vof;
-                if (SINGLE) {       // df: m_b/rho_b (f_a + f_b) gradW
-                    const T vb = rb.m / rb.rho;
-                    const T pp = fap + qb.p;
-                    s1x += vb * (pp * gx); s1y += vb * (pp * gy);
-                    s2x += vb * ((faxx + qb.sxx) * gx);
-                    s3x += vb * ((faxy + qb.sxy) * gy);
-                    s2y += vb * ((faxy + qb.sxy) * gx);
-                    s3y += vb * ((fayy + qb.syy) * gy);
-                } else {            // df3: m_b (f_a/rho_a^2 + f_b/rho_b^2) gradW
-                    const T irb2 = T(1) / (rb.rho * rb.rho);
-                    const T pp = fap * ira2 + phib * qb.p * irb2;
-                    s1x += rb.m * (pp * gx); s1y += rb.m * (pp * gy);
-                    const T xx = faxx * ira2 + phib * qb.sxx * irb2;
-                    const T xy = faxy * ira2 + phib * qb.sxy * irb2;
-                    const T yy = fayy * ira2 + phib * qb.syy * irb2;
-                    s2x += rb.m * (xx * gx);
-                    s3x += rb.m * (xy * gy);
-                    s2y += rb.m * (xy * gx);
-                    s3y += rb.m * (yy * gy);
-                }
-                if (c.visc_artificial) {
-                    const T vr = (-du) * tdx + (-dv) * tdy;
-                    if (vr < T(0)) {
-                        const T tmh = (T)mh;
-                        const T muv = tmh * vr / (rr + tmh * tmh * etq * etq);
-                        const T mrho = T(0.5) * (ra.rho + rb.rho);
-                        const T piv = (beta * muv - alpha * cs) * muv / mrho;
-                        avx += rb.m * (-piv * gx);
-                        avy += rb.m * (-piv * gy);
-                    }
-                }
-                if (c.soil_artificial_stress) {
-                    const T q = pref * rb.m / rb.rho;
-                    dpp += q * ((qa.p - qb.p) * e);
-                    dsx += q * ((qa.sxx - qb.sxx) * e);
-                    dsxy += q * ((qa.sxy - qb.sxy) * e);
-                    dsy += q * ((qa.syy - qb.syy) * e);
-                }
-                if (!SINGLE && real_a && qb.itype < T(0)) {
-                    const T r = (T)sqrt(r2);
-                    if (!(r > r0)) {
-                        const T f = (pow(r0 / r, p1) - pow(r0 / r, p2)) / (r * r);
-                        rpx += dd * tdx * f;
-                        rpy += dd * tdy * f;
-                    }
-                }
-                if (c.average_velocity) {
-                    const T mrho = (ra.rho + rb.rho) / T(2);
-                    xsx += rb.m * du / mrho * w;
-                    xsy += rb.m * dv / mrho * w;
-                }
-            });
         T dvx, dvy;
         if (SINGLE) { dvx = -s1x + s2x + s3x; dvy = -s1y + s2y + s3y; }
         else {
@@ -467,7 +499,7 @@ __global__ void __launch_bounds__(SPHG_TPB) k_soil_pass(PhaseDev<T> P, GridGeom 
         dvy = dvy + avy + rpy + (T)c.gravity;
         T2 o; o.x = dvx; o.y = dvy;
         P.dv[a] = o;
-        if (c.average_velocity) {
+        if (xsph) {
             const T eps = (T)c.epsilon;
             T2 av; av.x = real_a ? eps * xsx : xsx; av.y = real_a ? eps * xsy : xsy;
             P.av[a] = av;
@@ -479,7 +511,6 @@ __global__ void __launch_bounds__(SPHG_TPB) k_soil_pass(PhaseDev<T> P, GridGeom 
         const double G = c.s_E / (2.0 * (1 + c.s_niu));
         double ds0 = 0.0, ds1 = 0.0, ds2 = 0.0, dp = 0.0;
         if (c.plasticity == 3) {
-            fail = 0;
             const double J2a = sqrt((sxx * sxx + 2.0 * (sxy * sxy) + syy * syy + (sxx + syy) * (sxx + syy)) / 2.0) + 1.0e-6;
             if (fabs(J2a - c.s_alpha1 * (3.0 * p)) < SPHG_F32LIT(1.0e-5f)) fail = 1;
             P.fail[a] = fail;
@@ -498,8 +529,6 @@ __global__ void __launch_bounds__(SPHG_TPB) k_soil_pass(PhaseDev<T> P, GridGeom 
                     P.eps_p[a] = P.eps_p[a] + dlambda * sxy / (2 * sqrt(J2)) * SPHG_F32LIT(0.000005f);
                 }
             }
-        } else {
-            fail = P.fail[a];
         }
         const double dwxy = (double)wxy;
         ds0 = ds0 + G * dtxx; ds1 = ds1 + G * dtxy; ds2 = ds2 + G * dtyy;
@@ -518,7 +547,7 @@ __global__ void __launch_bounds__(SPHG_TPB) k_soil_pass(PhaseDev<T> P, GridGeom 
     }
     count_stats(cnt, slot, slot, hits, valid);
     if (c.plasticity == 3) {
-        int s = __syncthreads_count(valid ? fail : 0);
+        int s = __syncthreads_count(fail);
         if (threadIdx.x == 0 && s) atomicAdd(&cnt->nfail, s);
     }
 }
@@ -528,78 +557,93 @@ __global__ void __launch_bounds__(SPHG_TPB) k_soil_pass(PhaseDev<T> P, GridGeom 
 // darcy_law :3832 and pore_water_pressure :3877, then volume_fraction_soil
 // :3970.  Neighbour data comes from the water records of this step; the
 // gradient is taken, as the reference does, with dx = x_water - x_soil.
-template <typename T>
+// With m = vol*rho, Darcy's m_w*cf*(v_w - v_s)*W/(rho_w rho_s) becomes
+// vol_w*rho_w*vof_w*vof_s*(-g/k)*(v_w - v_s)*W/rho_s and the pore pressure
+// m_w p_w/(rho_w rho_s) becomes vol_w p_w / rho_s.
+template <typename T, int SKF>
 __global__ void __launch_bounds__(SPHG_TPB) k_cross_soil(PhaseDev<T> S, PhaseDev<T> W, GridGeom g, SearchConst sc, SimConst c) {
     typedef typename V2<T>::t T2;
-    int k = gtid();
-    if (k >= S.n) return;
-    const int a = S.perm[k];
-    const double2 xa = S.xs[k];
-    const double ha = S.hs[k];
-    const RecA<T> ra = S.recA[k];
-    const T phis = S.recB[k].vof;
+    SPHG_HITBUF(T);
+    const int k = gtid();
+    const bool valid = k < S.n;
+    const int kk = valid ? k : 0;
+    const double2 xa = S.xs[kk];
+    const double ha = S.hs[kk];
+    const RecA<T> ra = S.recA[kk];
+    const T phis = S.recB[kk].vof;
     const T negg_ks = (T)(-c.numeric_gravity / c.s_perm);
-    T dx_ = 0, dy_ = 0;
-    visit_neighbours(g, sc, W.cell_start, W.xs, W.hs, xa, ha, -1,
-        [&](int m, double dx, double dy, double r2, double mh) {
-            const RecA<T> rb = W.recA[m];
-            const RecB<T> qb = W.recB[m];
-            T w, gx, gy;
-            const T wdx = -(T)dx, wdy = -(T)dy;   // x_water - x_soil
-            sph_kernel<T>(c.skf, (T)sqrt(r2), wdx, wdy, (T)mh, w, gx, gy);
-            const T rrw = w / (rb.rho * ra.rho);
-            const T cf = qb.vof * phis * rb.rho * negg_ks;
-            dx_ += rb.m * (cf * (rb.vx - ra.vx) * rrw);
-            dy_ += rb.m * (cf * (rb.vy - ra.vy) * rrw);
-            const T mprr = rb.m * qb.p / (rb.rho * ra.rho);
-            dx_ += mprr * gx * phis;
-            dy_ += mprr * gy * phis;
-        });
-    T2 d = S.dv[a];
-    d.x += dx_; d.y += dy_;
-    S.dv[a] = d;
-    if (c.volume_fraction) S.vof[a] = S.rho[a] / c.s_rho0;
+    const T irs = T(1) / ra.rho;
+    KernelConst<T, SKF> ka;
+    ka.init((T)ha);
+    T ddx = 0, ddy = 0, dpx = 0, dpy = 0;
+    visit_batched(hb, g, sc, W.cell_start, W.xs, W.hs, xa, ha, -1, valid, [&](int m, T dx, T dy) {
+        const RecA<T> rb = W.recA[m];
+        const RecB<T> qb = W.recB[m];
+        T w, sr, rr, mh;
+        pair_kernel<T, SKF>(ka, sc, ha, W.hs, m, dx, dy, w, sr, rr, mh);
+        // x_water - x_soil = -(x_a - x_b)
+        const T gx = -sr * dx, gy = -sr * dy;
+        const T q = rb.vol * rb.rho * qb.vof * w;
+        ddx += q * (rb.vx - ra.vx);
+        ddy += q * (rb.vy - ra.vy);
+        const T mp = rb.vol * qb.p;
+        dpx += mp * gx;
+        dpy += mp * gy;
+    });
+    if (valid) {
+        const int a = S.perm[k];
+        const T fd = phis * negg_ks * irs, fp = irs * phis;
+        T2 d = S.dv[a];
+        d.x += fd * ddx + fp * dpx;
+        d.y += fd * ddy + fp * dpy;
+        S.dv[a] = d;
+        if (c.volume_fraction) S.vof[a] = S.rho[a] / c.s_rho0;
+    }
 }
 
 // Water side: darcy_law :3832, volume_fraction_water2 :3940 (dvof),
 // volume_fraction_water :3912 (vof2), and every renorm_interval steps the
 // renormalisation rho <- rho/vof*vof2, vof <- vof2 (declarations_sph.f90:1414-1421).
-template <typename T>
+template <typename T, int SKF>
 __global__ void __launch_bounds__(SPHG_TPB) k_cross_water(PhaseDev<T> W, PhaseDev<T> S, GridGeom g, SearchConst sc, SimConst c,
                                                          DevCounters* cnt) {
     typedef typename V2<T>::t T2;
-    int k = gtid();
-    bool valid = k < W.n;
-    int hits = 0;
+    SPHG_HITBUF(T);
+    const int k = gtid();
+    const bool valid = k < W.n;
+    const int kk = valid ? k : 0;
+    const double2 xa = W.xs[kk];
+    const double ha = W.hs[kk];
+    const RecA<T> ra = W.recA[kk];
+    const T phiw = W.recB[kk].vof;
+    const T negg_ks = (T)(-c.numeric_gravity / c.s_perm);
+    const T irho0 = (T)(1.0 / c.s_rho0);
+    KernelConst<T, SKF> ka;
+    ka.init((T)ha);
+    T ddx = 0, ddy = 0, dvof = 0, v2 = 0;
+    const int hits = visit_batched(hb, g, sc, S.cell_start, S.xs, S.hs, xa, ha, -1, valid, [&](int m, T dx, T dy) {
+        const RecA<T> rb = S.recA[m];
+        const T phis = S.recB[m].vof;
+        T w, sr, rr, mh;
+        pair_kernel<T, SKF>(ka, sc, ha, S.hs, m, dx, dy, w, sr, rr, mh);
+        const T mb = rb.vol * rb.rho;
+        const T ux = ra.vx - rb.vx, uy = ra.vy - rb.vy;
+        const T q = rb.vol * phis * w;
+        ddx -= q * ux;
+        ddy -= q * uy;
+        dvof -= mb * (sr * (ux * dx + uy * dy));
+        v2 += mb * w;
+    });
     if (valid) {
         const int a = W.perm[k];
-        const double2 xa = W.xs[k];
-        const double ha = W.hs[k];
-        const RecA<T> ra = W.recA[k];
-        const T phiw = W.recB[k].vof;
-        const T negg_ks = (T)(-c.numeric_gravity / c.s_perm);
-        const T irho0 = (T)c.s_rho0;
-        T dvx = 0, dvy = 0, dvof = 0, v2 = 0;
-        hits = visit_neighbours(g, sc, S.cell_start, S.xs, S.hs, xa, ha, -1,
-            [&](int m, double dx, double dy, double r2, double mh) {
-                const RecA<T> rb = S.recA[m];
-                const T phis = S.recB[m].vof;
-                T w, gx, gy;
-                sph_kernel<T>(c.skf, (T)sqrt(r2), (T)dx, (T)dy, (T)mh, w, gx, gy);
-                const T rrw = w / (ra.rho * rb.rho);
-                const T cf = phiw * phis * ra.rho * negg_ks;
-                const T ux = ra.vx - rb.vx, uy = ra.vy - rb.vy;
-                dvx -= rb.m * (cf * ux * rrw);
-                dvy -= rb.m * (cf * uy * rrw);
-                dvof -= rb.m * (ux * gx + uy * gy) / irho0;
-                v2 += rb.m * w;
-            });
+        const T fd = phiw * negg_ks;
         T2 d = W.dv[a];
-        d.x += dvx; d.y += dvy;
+        d.x += fd * ddx;
+        d.y += fd * ddy;
         W.dv[a] = d;
         if (c.volume_fraction) {
-            W.dvof[a] = W.dvof[a] + dvof;
-            const T vof2 = T(1) - v2 / irho0;
+            W.dvof[a] = W.dvof[a] + dvof * irho0;
+            const T vof2 = T(1) - v2 * irho0;
             W.vof2[a] = vof2;
             if (c.renorm_now) {
                 double rho = W.rho[a] / W.vof[a];

@@ -24,11 +24,15 @@ RHS_FIELDS = ["drho", "dvx", "av", "p", "c", "rho", "dvof", "vof2", "vof", "dsxx
               "sxx", "sxy", "syy", "txx", "tyy", "txy", "vcc", "epsilon_p"]
 STATE_FIELDS = ["x", "vx", "rho", "p", "vof", "sxx", "sxy", "syy", "drho", "dvx", "c"]
 
-# FP32 mode, field-scale relative error vs the FP64 oracle
-FP32_BUDGET_1 = {"x": 1e-12, "vx": 1e-4, "rho": 1e-6, "p": 1e-4, "drho": 1e-3, "dvx": 1e-3, "sxx": 1e-4,
-                 "sxy": 1e-3, "syy": 1e-4, "vof": 1e-6, "c": 1e-5}
-FP32_BUDGET_30 = {"x": 1e-9, "vx": 1e-3, "rho": 1e-5, "p": 1e-3, "drho": 1e-2, "dvx": 1e-2, "sxx": 1e-3,
-                  "sxy": 1e-2, "syy": 1e-3, "vof": 1e-5, "c": 1e-4}
+# FP32 mode, field-scale relative error vs the FP64 oracle (max |a-b| / max |b|
+# over the phase), about 5-10x above the errors measured on a B200.  After one
+# step the velocity is a few dt*g, so its field scale is tiny and the FP32
+# force noise (the (p_a + p_b) pressure sum cancels to ~1e-3 of its terms)
+# shows most there.
+FP32_BUDGET_1 = {"x": 1e-9, "vx": 5e-3, "rho": 2e-6, "p": 5e-4, "drho": 2e-3, "dvx": 5e-4, "sxx": 1e-5,
+                 "sxy": 1e-4, "syy": 1e-5, "vof": 1e-7, "c": 1e-6}
+FP32_BUDGET_30 = {"x": 5e-7, "vx": 5e-4, "rho": 5e-6, "p": 5e-4, "drho": 1e-2, "dvx": 5e-4, "sxx": 5e-4,
+                  "sxy": 1e-3, "syy": 5e-4, "vof": 1e-6, "c": 1e-6}
 
 
 def ferr(a, b):

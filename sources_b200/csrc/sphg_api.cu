@@ -108,11 +108,12 @@ struct Engine : EngineBase {
     double* stage = nullptr;        // transfer staging, 2*nmax doubles
     int* stage_i = nullptr;
     long long* stage_l = nullptr;
-    void* spare[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};  // reorder scratch per phase: 4, 8, 16-byte elements
+    std::vector<void*> shadow[2];   // one reorder target per persistent field
     int nmax = 0;
     double hrange[2][2] = {{0, 0}, {0, 0}};
     std::vector<void*> allocs;
     SimConst sim{};
+    int nfail_slot = 3;             // which DP site the reported nfail comes from
 
     explicit Engine(sphg_ctx* c) : ctx(c) { memset(P, 0, sizeof(P)); }
     ~Engine() override {
@@ -201,7 +202,8 @@ struct Engine : EngineBase {
                        D.dvof, D.dsxx, D.dsxy, D.dsyy, D.dp, D.txx, D.txy, D.tyy, D.vcc, D.wxy, D.vof2, D.dv, D.av,
                        D.countiac, D.cell_id, D.cell_fill, D.perm, D.xs, D.hs, D.recA, D.recA2, D.recB};
         for (void* p : old) release(p);
-        for (int t = 0; t < 3; ++t) { release(spare[ph][t]); spare[ph][t] = nullptr; }
+        for (void* p : shadow[ph]) release(p);
+        shadow[ph].clear();
         memset(&D, 0, sizeof(D));
         D.n = n;
         size_t N = (size_t)n;
@@ -220,9 +222,12 @@ struct Engine : EngineBase {
         rc |= alloc(&D.countiac, N); rc |= alloc(&D.cell_id, N); rc |= alloc(&D.cell_fill, N); rc |= alloc(&D.perm, N);
         rc |= alloc(&D.xs, N); rc |= alloc(&D.hs, N);
         rc |= alloc(&D.recA, N); rc |= alloc(&D.recA2, N); rc |= alloc(&D.recB, N);
-        rc |= alloc((char**)&spare[ph][0], 4 * N); rc |= alloc((char**)&spare[ph][1], 8 * N);
-        rc |= alloc((char**)&spare[ph][2], 16 * N);
         if (rc) return SPHG_ERR_CUDA;
+        for (auto& f : field_refs(ph)) {
+            char* q = nullptr;
+            if (alloc(&q, (size_t)f.second * N)) return SPHG_ERR_CUDA;
+            shadow[ph].push_back(q);
+        }
         if (n > nmax) {
             release(stage); release(stage_i); release(stage_l);
             nmax = n;
@@ -370,43 +375,40 @@ struct Engine : EngineBase {
                       (const int*)D.orig, D.perm);
     }
 
-    // Gather field f into the phase's spare buffer of the same element size,
-    // then swap the two: the old field buffer becomes the spare.
-    template <typename S>
-    int permute_field(int ph, const int* perm, S*& f) {
-        static_assert(sizeof(S) == 4 || sizeof(S) == 8 || sizeof(S) == 16, "element size");
-        const int slot = sizeof(S) == 4 ? 0 : (sizeof(S) == 8 ? 1 : 2);
-        S* dst = (S*)spare[ph][slot];
-        int rc = launch("reorder", k_permute<S>, blocks(P[ph].n, 256), 256, P[ph].n, perm, (const S*)f, dst);
-        if (rc) return rc;
-        spare[ph][slot] = (void*)f;
-        f = dst;
-        return 0;
+    // The persistent per-particle fields of a phase and their element sizes.
+    std::vector<std::pair<void**, int>> field_refs(int ph) {
+        PhaseDev<T>& D = P[ph];
+        std::vector<std::pair<void**, int>> f;
+        auto add = [&](void** p, int b) { f.push_back({p, b}); };
+        add((void**)&D.x, 16); add((void**)&D.v, 16); add((void**)&D.v_min, 16);
+        for (double** q : {&D.rho, &D.rho_min, &D.vof, &D.vof_min, &D.p, &D.c, &D.mass, &D.hsml, &D.sxx, &D.sxy,
+                           &D.syy, &D.sxx_min, &D.sxy_min, &D.syy_min, &D.p_min, &D.eps_p})
+            add((void**)q, 8);
+        for (int** q : {&D.itype, &D.orig, &D.fail, &D.countiac}) add((void**)q, 4);
+        for (T** q : {&D.drho, &D.dvof, &D.dsxx, &D.dsxy, &D.dsyy, &D.dp, &D.txx, &D.txy, &D.tyy, &D.vcc, &D.wxy, &D.vof2})
+            add((void**)q, (int)sizeof(T));
+        add((void**)&D.dv, (int)sizeof(T2)); add((void**)&D.av, (int)sizeof(T2));
+        return f;
     }
 
-    // Permute the persistent state into the current cell order.
+    // Permute every persistent field into the current cell order in one launch
+    // (each into its shadow buffer), then swap fields and shadows.
     int reorder(int ph) {
         PhaseDev<T>& D = P[ph];
-        const int* perm = D.perm;
-        int n = D.n, rc = 0;
-        rc |= permute_field(ph, perm, D.x); rc |= permute_field(ph, perm, D.v); rc |= permute_field(ph, perm, D.v_min);
-        rc |= permute_field(ph, perm, D.rho); rc |= permute_field(ph, perm, D.rho_min);
-        rc |= permute_field(ph, perm, D.vof); rc |= permute_field(ph, perm, D.vof_min);
-        rc |= permute_field(ph, perm, D.p); rc |= permute_field(ph, perm, D.c); rc |= permute_field(ph, perm, D.mass);
-        rc |= permute_field(ph, perm, D.hsml);
-        rc |= permute_field(ph, perm, D.sxx); rc |= permute_field(ph, perm, D.sxy); rc |= permute_field(ph, perm, D.syy);
-        rc |= permute_field(ph, perm, D.sxx_min); rc |= permute_field(ph, perm, D.sxy_min);
-        rc |= permute_field(ph, perm, D.syy_min); rc |= permute_field(ph, perm, D.p_min);
-        rc |= permute_field(ph, perm, D.eps_p);
-        rc |= permute_field(ph, perm, D.itype); rc |= permute_field(ph, perm, D.orig); rc |= permute_field(ph, perm, D.fail);
-        rc |= permute_field(ph, perm, D.drho); rc |= permute_field(ph, perm, D.dvof);
-        rc |= permute_field(ph, perm, D.dsxx); rc |= permute_field(ph, perm, D.dsxy); rc |= permute_field(ph, perm, D.dsyy);
-        rc |= permute_field(ph, perm, D.dp); rc |= permute_field(ph, perm, D.dv); rc |= permute_field(ph, perm, D.av);
-        rc |= permute_field(ph, perm, D.txx); rc |= permute_field(ph, perm, D.txy); rc |= permute_field(ph, perm, D.tyy);
-        rc |= permute_field(ph, perm, D.vcc); rc |= permute_field(ph, perm, D.wxy); rc |= permute_field(ph, perm, D.vof2);
-        rc |= permute_field(ph, perm, D.countiac);
+        auto refs = field_refs(ph);
+        PermList L;
+        memset(&L, 0, sizeof(L));
+        if (refs.size() > sizeof(L.f) / sizeof(L.f[0]) || refs.size() != shadow[ph].size()) return SPHG_ERR_STATE;
+        L.count = (int)refs.size();
+        for (size_t i = 0; i < refs.size(); ++i) {
+            L.f[i].src = *refs[i].first;
+            L.f[i].dst = shadow[ph][i];
+            L.f[i].bytes = refs[i].second;
+        }
+        int rc = launch("reorder", k_permute_all, blocks(D.n, 256), 256, D.n, (const int*)D.perm, L);
         if (rc) return rc;
-        return launch("iota", k_iota, blocks(n, 256), 256, n, D.perm);
+        for (size_t i = 0; i < refs.size(); ++i) std::swap(*refs[i].first, shadow[ph][i]);
+        return launch("iota", k_iota, blocks(D.n, 256), 256, D.n, D.perm);
     }
 
     // -------------------------------------------------------------- the step
@@ -418,42 +420,46 @@ struct Engine : EngineBase {
         return 0;
     }
 
-    // the pair passes of one right-hand side, for kernel function SKF
+    // The pair passes of one step for kernel function SKF.  fh: run the
+    // leapfrog predictor inside the gathers; u: what the last pass of each
+    // phase does after its sums (nothing, or the corrector).
     template <int SKF>
-    int passes() {
+    int passes(int fh, StepCtl u) {
         const sphg_params& p = ctx->prm;
         const int tpb = SPHG_TPB;
+        const int dp = sim.yield_dp;
         int rc;
         if (p.single_phase) {
             PhaseDev<T>& D = P[0];
             if (D.material == SPHG_WATER) {
-                if ((rc = launch("gather", k_gather<T>, blocks(D.n, 256), 256, D, sim, 0, 0, cnt))) return rc;
+                if ((rc = launch("gather", k_gather<T>, blocks(D.n, 256), 256, D, sim, 0, 0, fh, 0, 0, cnt))) return rc;
                 if ((rc = launch("water_sum", k_water_sum<T, SKF>, blocks(D.n, tpb), tpb, D, grid, sc_same, sim, cnt))) return rc;
                 if ((rc = launch("water_pass_a", k_water_pass_a<T, SKF, true>, blocks(D.n, tpb), tpb, D, grid, sc_same, sim, cnt))) return rc;
-                if ((rc = launch("water_pass_b", k_water_pass_b<T, SKF, true>, blocks(D.n, tpb), tpb, D, grid, sc_same, sim))) return rc;
+                if ((rc = launch("water_pass_b", k_water_pass_b<T, SKF, true>, blocks(D.n, tpb), tpb, D, grid, sc_same, sim, u))) return rc;
             } else {
-                if ((rc = launch("gather", k_gather<T>, blocks(D.n, 256), 256, D, sim, 1, sim.yield_dp, cnt))) return rc;
-                if (sim.plasticity == 3) CUDA_TRY(cudaMemsetAsync(&cnt->nfail, 0, sizeof(int), ctx->stream));
-                if ((rc = launch("soil_pass", k_soil_pass<T, SKF, true>, blocks(D.n, tpb), tpb, D, grid, sc_same, sim, cnt, 0))) return rc;
+                if ((rc = launch("gather", k_gather<T>, blocks(D.n, 256), 256, D, sim, 1, dp, fh, 0, dp, cnt))) return rc;
+                StepCtl us = u; us.with_vof = 0; us.do_dp = dp;
+                if ((rc = launch("soil_pass", k_soil_pass<T, SKF, true>, blocks(D.n, tpb), tpb, D, grid, sc_same, sim, cnt, 0, us))) return rc;
             }
         } else {
             PhaseDev<T>& W = P[0];
             PhaseDev<T>& S = P[1];
-            if ((rc = launch("gather", k_gather<T>, blocks(W.n, 256), 256, W, sim, 0, 0, cnt))) return rc;
-            if ((rc = launch("gather", k_gather<T>, blocks(S.n, 256), 256, S, sim, 1, sim.yield_dp, cnt))) return rc;
+            StepCtl uw = u; uw.with_vof = 1; uw.do_dp = 0;
+            StepCtl us = u; us.with_vof = 1; us.do_dp = dp;
+            StepCtl none{}; 
+            if ((rc = launch("gather", k_gather<T>, blocks(W.n, 256), 256, W, sim, 0, 0, fh, 1, 0, cnt))) return rc;
+            if ((rc = launch("gather", k_gather<T>, blocks(S.n, 256), 256, S, sim, 1, dp, fh, 1, dp, cnt))) return rc;
             if ((rc = launch("water_pass_a", k_water_pass_a<T, SKF, false>, blocks(W.n, tpb), tpb, W, grid, sc_same, sim, cnt))) return rc;
-            if ((rc = launch("water_pass_b", k_water_pass_b<T, SKF, false>, blocks(W.n, tpb), tpb, W, grid, sc_same, sim))) return rc;
-            if (sim.plasticity == 3) CUDA_TRY(cudaMemsetAsync(&cnt->nfail, 0, sizeof(int), ctx->stream));
-            if ((rc = launch("soil_pass", k_soil_pass<T, SKF, false>, blocks(S.n, tpb), tpb, S, grid, sc_same, sim, cnt, 1))) return rc;
-            if ((rc = launch("cross_soil", k_cross_soil<T, SKF>, blocks(S.n, tpb), tpb, S, W, grid, sc_cross, sim))) return rc;
-            if ((rc = launch("cross_water", k_cross_water<T, SKF>, blocks(W.n, tpb), tpb, W, S, grid, sc_cross, sim, cnt))) return rc;
+            if ((rc = launch("water_pass_b", k_water_pass_b<T, SKF, false>, blocks(W.n, tpb), tpb, W, grid, sc_same, sim, none))) return rc;
+            if ((rc = launch("soil_pass", k_soil_pass<T, SKF, false>, blocks(S.n, tpb), tpb, S, grid, sc_same, sim, cnt, 1, none))) return rc;
+            if ((rc = launch("cross_soil", k_cross_soil<T, SKF>, blocks(S.n, tpb), tpb, S, W, grid, sc_cross, sim, us, cnt))) return rc;
+            if ((rc = launch("cross_water", k_cross_water<T, SKF>, blocks(W.n, tpb), tpb, W, S, grid, sc_cross, sim, cnt, uw))) return rc;
             aliased = true;
         }
         return 0;
     }
 
-    // single_step / single_step_for_water / single_step_for_soil
-    int rhs(int itimestep) override {
+    int run(int itimestep, int fh, StepCtl u) {
         int rc = prepare();
         if (rc) return rc;
         make_sim(itimestep);
@@ -465,38 +471,31 @@ struct Engine : EngineBase {
             if (reorder_now && (rc = reorder(ph))) return rc;
         }
         switch (p.skf) {
-            case 1: rc = passes<1>(); break;
-            case 2: rc = passes<2>(); break;
-            case 3: rc = passes<3>(); break;
-            default: rc = passes<4>(); break;
+            case 1: rc = passes<1>(fh, u); break;
+            case 2: rc = passes<2>(fh, u); break;
+            case 3: rc = passes<3>(fh, u); break;
+            default: rc = passes<4>(fh, u); break;
         }
         if (rc) return rc;
         return launch("check", k_check, 1, 32, (const DevCounters*)cnt, sticky, (unsigned long long)p.max_interaction);
     }
 
-    // one leapfrog step of time_integration / _for_water / _for_soil
+    // single_step / single_step_for_water / single_step_for_soil
+    int rhs(int itimestep) override {
+        StepCtl none{};
+        nfail_slot = ctx->prm.plasticity == 3 ? 2 : 1;
+        return run(itimestep, 0, none);
+    }
+
+    // one leapfrog step of time_integration / _for_water / _for_soil: the
+    // predictor runs inside the gathers (not on the first step), the
+    // corrector inside the last pass of each phase
     int step(int itimestep) override {
-        int rc = prepare();
-        if (rc) return rc;
-        make_sim(itimestep);
-        const bool two = !ctx->prm.single_phase;
-        const int first = itimestep == 1;
-        if (!first) {
-            for (int ph = 0; ph < ctx->nphase; ++ph) {
-                PhaseDev<T>& D = P[ph];
-                int dp = D.material == SPHG_SOIL && sim.yield_dp;
-                if (dp) CUDA_TRY(cudaMemsetAsync(&cnt->nfail, 0, sizeof(int), ctx->stream));
-                if ((rc = launch("first_half", k_first_half<T>, blocks(D.n, 256), 256, D, sim, two ? 1 : 0, dp, cnt))) return rc;
-            }
-        }
-        if ((rc = rhs(itimestep))) return rc;
-        for (int ph = 0; ph < ctx->nphase; ++ph) {
-            PhaseDev<T>& D = P[ph];
-            int dp = D.material == SPHG_SOIL && sim.yield_dp;
-            if (dp) CUDA_TRY(cudaMemsetAsync(&cnt->nfail, 0, sizeof(int), ctx->stream));
-            if ((rc = launch("update", k_update<T>, blocks(D.n, 256), 256, D, sim, first, two ? 1 : 0, dp, cnt))) return rc;
-        }
-        return 0;
+        StepCtl u{};
+        u.update = 1;
+        u.first = itimestep == 1;
+        nfail_slot = 3;
+        return run(itimestep, itimestep != 1, u);
     }
 
     int begin_batch() override {
@@ -596,7 +595,7 @@ struct Engine : EngineBase {
                 }
             }
         }
-        h->nfail = hcnt.nfail;
+        h->nfail = hcnt.nfail[nfail_slot];
         return 0;
     }
 
@@ -615,7 +614,7 @@ struct Engine : EngineBase {
         // step ran since): rebuild sorted positions for both phases
         for (int ph = 0; ph < ctx->nphase; ++ph) {
             if ((rc = build_cells(ph))) return rc;
-            if ((rc = launch("gather", k_gather<T>, blocks(P[ph].n, 256), 256, P[ph], sim, 0, 0, cnt))) return rc;
+            if ((rc = launch("gather", k_gather<T>, blocks(P[ph].n, 256), 256, P[ph], sim, 0, 0, 0, 0, 0, cnt))) return rc;
         }
         int n = A.n;
         int* count = stage_i;
@@ -665,7 +664,7 @@ struct Engine : EngineBase {
             out->miniac[i] = hcnt.miniac[i] == 0x7fffffff ? 0 : hcnt.miniac[i];
             out->noiac[i] = hcnt.noiac[i];
         }
-        out->nfail = hcnt.nfail;
+        out->nfail = hcnt.nfail[nfail_slot];
         out->n_out_of_domain = hcnt.n_out;
         out->itimestep = ctx->itimestep;
         out->time = ctx->time;

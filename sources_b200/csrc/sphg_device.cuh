@@ -52,7 +52,8 @@ struct SearchConst {
 struct DevCounters {
     unsigned long long pairs[3];     // phase 1, phase 2, cross (last step)
     int maxiac[2], miniac[2], noiac[2];
-    int nfail;
+    int nfail[4];                    // soil points flagged by: DP after the predictor,
+                                     // in-step DP, plastic_or_not, DP after the corrector
     int n_out;                       // particles clamped into edge cells
     int nonfinite;                   // NaN/Inf positions met
     int overflow;                    // a pair list exceeded max_interaction

@@ -76,16 +76,116 @@ __global__ void __launch_bounds__(256) k_cell_sort(int ncell, const int* __restr
     }
 }
 
-// ------------------------------------------------------------------ gathers
-// Sorted copies of position, h and (v, m, rho).  For soil also the in-step
-// Drucker-Prager return (declarations_sph.f90:1242-1247) on the state and the
-// stress/pressure record of the soil pass.
+// ------------------------------------------------------------- integrators
+// What the last pass of a phase does after its sums: nothing (right-hand side
+// only, sphg_single_step) or the leapfrog corrector of this step.
+struct StepCtl {
+    int update;      // run the corrector (first_step or second_half)
+    int first;       // itimestep == 1: first_step
+    int with_vof;    // integrate the water volume fraction (two-phase)
+    int do_dp;       // Drucker-Prager after the corrector (soil)
+};
+
+// first_half, declarations_sph.f90:643-684 (and :812-825, :998-1025), plus the
+// Drucker-Prager call that follows it on soil (:559, :1027).  Returns the
+// particle's fail flag of that DP call.
 template <typename T>
-__global__ void __launch_bounds__(256) k_gather(PhaseDev<T> P, SimConst c, int soil, int do_dp, DevCounters* cnt) {
-    int k = gtid();
+__device__ __forceinline__ int first_half_one(const PhaseDev<T>& P, int a, const SimConst& c, int with_vof, int do_dp) {
+    const double dt = c.dt;
+    if (!c.summation_density) { double r = P.rho[a]; P.rho_min[a] = r; P.rho[a] = r + (dt / 2.0) * (double)P.drho[a]; }
+    if (with_vof && P.material == 1 && c.volume_fraction) {
+        double f = P.vof[a]; P.vof_min[a] = f; P.vof[a] = f + (dt / 2.0) * (double)P.dvof[a];
+    }
     int fail = 0;
+    const bool soil = P.material == 2;
+    double p = 0, sxx = 0, sxy = 0, syy = 0;
+    if (soil) {
+        p = P.p[a]; sxx = P.sxx[a]; sxy = P.sxy[a]; syy = P.syy[a];
+        if (c.stress_integration == 2) {
+            P.sxx_min[a] = sxx; P.sxy_min[a] = sxy; P.syy_min[a] = syy; P.p_min[a] = p;
+            sxx = sxx + (dt / 2.0) * (double)P.dsxx[a];
+            sxy = sxy + (dt / 2.0) * (double)P.dsxy[a];
+            syy = syy + (dt / 2.0) * (double)P.dsyy[a];
+            p = p + (dt / 2.0) * (double)P.dp[a];
+        }
+    }
+    if (P.itype[a] >= 0) {
+        double2 v = P.v[a];
+        P.v_min[a] = v;
+        const typename V2<T>::t d = P.dv[a];
+        v.x = v.x + (dt / 2.0) * (double)d.x;
+        v.y = v.y + (dt / 2.0) * (double)d.y;
+        P.v[a] = v;
+    }
+    if (soil) {
+        if (do_dp) { fail = dp_return(p, sxx, sxy, syy, c.s_alpha1); P.fail[a] = fail; }
+        P.p[a] = p; P.sxx[a] = sxx; P.sxy[a] = sxy; P.syy[a] = syy;
+    }
+    return fail;
+}
+
+// first_step (:686-723) when first != 0, else second_half (:725-762), plus the
+// Drucker-Prager call after it on soil (:583, :601, :1069, :1107).
+template <typename T>
+__device__ __forceinline__ int update_one(const PhaseDev<T>& P, int a, const SimConst& c, int first, int with_vof, int do_dp) {
+    const double dt = c.dt;
+    int fail = 0;
+    if (!c.summation_density)
+        P.rho[a] = first ? P.rho[a] + (dt / 2.0) * (double)P.drho[a] : P.rho_min[a] + dt * (double)P.drho[a];
+    if (with_vof && P.material == 1 && c.volume_fraction)
+        P.vof[a] = first ? P.vof[a] + (dt / 2.0) * (double)P.dvof[a] : P.vof_min[a] + dt * (double)P.dvof[a];
+    if (P.material == 2) {
+        double p = P.p[a], sxx = P.sxx[a], sxy = P.sxy[a], syy = P.syy[a];
+        const double d0 = P.dsxx[a], d1 = P.dsxy[a], d2 = P.dsyy[a], d3 = P.dp[a];
+        if (c.stress_integration == 1) {
+            sxx = sxx + dt * d0; sxy = sxy + dt * d1; syy = syy + dt * d2; p = p + dt * d3;
+        } else if (c.stress_integration == 2) {
+            if (first) {
+                sxx = sxx + (dt / 2.0) * d0; sxy = sxy + (dt / 2.0) * d1;
+                syy = syy + (dt / 2.0) * d2; p = p + (dt / 2.0) * d3;
+            } else {
+                sxx = P.sxx_min[a] + dt * d0; sxy = P.sxy_min[a] + dt * d1;
+                syy = P.syy_min[a] + dt * d2; p = P.p_min[a] + dt * d3;
+            }
+        }
+        if (do_dp) { fail = dp_return(p, sxx, sxy, syy, c.s_alpha1); P.fail[a] = fail; }
+        P.p[a] = p; P.sxx[a] = sxx; P.sxy[a] = sxy; P.syy[a] = syy;
+    }
+    if (P.itype[a] >= 0) {
+        double2 v = first ? P.v[a] : P.v_min[a];
+        const typename V2<T>::t d = P.dv[a];
+        const typename V2<T>::t av = P.av[a];
+        double2 x = P.x[a];
+        const double h = first ? dt / 2.0 : dt;
+        v.x = v.x + h * (double)d.x + (double)av.x;
+        x.x = x.x + dt * v.x;
+        v.y = v.y + h * (double)d.y + (double)av.y;
+        x.y = x.y + dt * v.y;
+        P.v[a] = v;
+        P.x[a] = x;
+    }
+    return fail;
+}
+
+__device__ __forceinline__ void count_fail(DevCounters* cnt, int slot, int fail) {
+    int s = __syncthreads_count(fail);
+    if (threadIdx.x == 0 && s) atomicAdd(&cnt->nfail[slot], s);
+}
+
+// ------------------------------------------------------------------ gathers
+// Sorted copies of position, h and (v, vol, rho).  With fh != 0 the particle's
+// leapfrog predictor (first_half, + DP on soil) runs first, so the records
+// carry the half-step state.  For soil also the in-step Drucker-Prager return
+// (declarations_sph.f90:1242-1247) on the state and the stress/pressure
+// record of the soil pass.
+template <typename T>
+__global__ void __launch_bounds__(256) k_gather(PhaseDev<T> P, SimConst c, int soil, int do_dp, int fh, int with_vof,
+                                                int fh_dp, DevCounters* cnt) {
+    int k = gtid();
+    int fail0 = 0, fail = 0;
     if (k < P.n) {
         int a = P.perm[k];
+        if (fh) fail0 = first_half_one(P, a, c, with_vof, fh_dp);
         P.xs[k] = P.x[a];
         P.hs[k] = P.hsml[a];
         double2 v = P.v[a];
@@ -107,10 +207,8 @@ __global__ void __launch_bounds__(256) k_gather(PhaseDev<T> P, SimConst c, int s
             P.recB[k] = rb;
         }
     }
-    if (soil && do_dp) {
-        int s = __syncthreads_count(fail);
-        if (threadIdx.x == 0 && s) atomicAdd(&cnt->nfail, s);
-    }
+    if (fh && fh_dp) count_fail(cnt, 0, fail0);
+    if (soil && do_dp) count_fail(cnt, 1, fail);
 }
 
 // Per-particle interaction statistics (interaction_statistics,
@@ -295,7 +393,7 @@ __global__ void __launch_bounds__(SPHG_TPB) k_water_pass_a(PhaseDev<T> P, GridGe
 // dx = x_real - x_virtual, as the reference does with real particles
 // numbered before virtual ones.
 template <typename T, int SKF, bool SINGLE>
-__global__ void __launch_bounds__(SPHG_TPB) k_water_pass_b(PhaseDev<T> P, GridGeom g, SearchConst sc, SimConst c) {
+__global__ void __launch_bounds__(SPHG_TPB) k_water_pass_b(PhaseDev<T> P, GridGeom g, SearchConst sc, SimConst c, StepCtl u) {
     typedef typename V2<T>::t T2;
     SPHG_HITBUF(T);
     const int k = gtid();
@@ -377,6 +475,7 @@ __global__ void __launch_bounds__(SPHG_TPB) k_water_pass_b(PhaseDev<T> P, GridGe
             P.av[a] = av;
         }
         if (!SINGLE) P.dvof[a] = dvf;
+        if (SINGLE && u.update) update_one(P, a, c, u.first, 0, 0);   // last pass of the water-only step
     }
 }
 
@@ -390,7 +489,7 @@ __global__ void __launch_bounds__(SPHG_TPB) k_water_pass_b(PhaseDev<T> P, GridGe
 // whose spin sum wxy comes from the same pass.
 template <typename T, int SKF, bool SINGLE>
 __global__ void __launch_bounds__(SPHG_TPB) k_soil_pass(PhaseDev<T> P, GridGeom g, SearchConst sc, SimConst c,
-                                                       DevCounters* cnt, int slot) {
+                                                       DevCounters* cnt, int slot, StepCtl u) {
     typedef typename V2<T>::t T2;
     SPHG_HITBUF(T);
     const int k = gtid();
@@ -486,7 +585,7 @@ __global__ void __launch_bounds__(SPHG_TPB) k_soil_pass(PhaseDev<T> P, GridGeom 
             xsy += q * dv;
         }
     });
-    int fail = 0;
+    int fail = 0, fail3 = 0;
     if (valid) {
         T dvx, dvy;
         if (SINGLE) { dvx = -s1x + s2x + s3x; dvy = -s1y + s2y + s3y; }
@@ -544,12 +643,11 @@ __global__ void __launch_bounds__(SPHG_TPB) k_soil_pass(PhaseDev<T> P, GridGeom 
         P.txx[a] = txx; P.tyy[a] = tyy; P.txy[a] = wxy;   // wxy is txy (alias)
         P.vcc[a] = vcc;
         P.countiac[a] = hits;
+        if (SINGLE && u.update) fail3 = update_one(P, a, c, u.first, 0, u.do_dp);   // last pass of the soil-only step
     }
     count_stats(cnt, slot, slot, hits, valid);
-    if (c.plasticity == 3) {
-        int s = __syncthreads_count(fail);
-        if (threadIdx.x == 0 && s) atomicAdd(&cnt->nfail, s);
-    }
+    if (c.plasticity == 3) count_fail(cnt, 2, fail);
+    if (SINGLE && u.update && u.do_dp) count_fail(cnt, 3, fail3);
 }
 
 // ------------------------------------------------------------- cross phase
@@ -561,7 +659,8 @@ __global__ void __launch_bounds__(SPHG_TPB) k_soil_pass(PhaseDev<T> P, GridGeom 
 // vol_w*rho_w*vof_w*vof_s*(-g/k)*(v_w - v_s)*W/rho_s and the pore pressure
 // m_w p_w/(rho_w rho_s) becomes vol_w p_w / rho_s.
 template <typename T, int SKF>
-__global__ void __launch_bounds__(SPHG_TPB) k_cross_soil(PhaseDev<T> S, PhaseDev<T> W, GridGeom g, SearchConst sc, SimConst c) {
+__global__ void __launch_bounds__(SPHG_TPB) k_cross_soil(PhaseDev<T> S, PhaseDev<T> W, GridGeom g, SearchConst sc, SimConst c,
+                                                        StepCtl u, DevCounters* cnt) {
     typedef typename V2<T>::t T2;
     SPHG_HITBUF(T);
     const int k = gtid();
@@ -590,6 +689,7 @@ __global__ void __launch_bounds__(SPHG_TPB) k_cross_soil(PhaseDev<T> S, PhaseDev
         dpx += mp * gx;
         dpy += mp * gy;
     });
+    int fail3 = 0;
     if (valid) {
         const int a = S.perm[k];
         const T fd = phis * negg_ks * irs, fp = irs * phis;
@@ -598,7 +698,9 @@ __global__ void __launch_bounds__(SPHG_TPB) k_cross_soil(PhaseDev<T> S, PhaseDev
         d.y += fd * ddy + fp * dpy;
         S.dv[a] = d;
         if (c.volume_fraction) S.vof[a] = S.rho[a] / c.s_rho0;
+        if (u.update) fail3 = update_one(S, a, c, u.first, u.with_vof, u.do_dp);   // last pass of the soil phase
     }
+    if (u.update && u.do_dp) count_fail(cnt, 3, fail3);
 }
 
 // Water side: darcy_law :3832, volume_fraction_water2 :3940 (dvof),
@@ -606,7 +708,7 @@ __global__ void __launch_bounds__(SPHG_TPB) k_cross_soil(PhaseDev<T> S, PhaseDev
 // renormalisation rho <- rho/vof*vof2, vof <- vof2 (declarations_sph.f90:1414-1421).
 template <typename T, int SKF>
 __global__ void __launch_bounds__(SPHG_TPB) k_cross_water(PhaseDev<T> W, PhaseDev<T> S, GridGeom g, SearchConst sc, SimConst c,
-                                                         DevCounters* cnt) {
+                                                         DevCounters* cnt, StepCtl u) {
     typedef typename V2<T>::t T2;
     SPHG_HITBUF(T);
     const int k = gtid();
@@ -652,104 +754,9 @@ __global__ void __launch_bounds__(SPHG_TPB) k_cross_water(PhaseDev<T> W, PhaseDe
             }
         }
         W.countiac[a] = hits;
+        if (u.update) update_one(W, a, c, u.first, u.with_vof, 0);   // last pass of the water phase
     }
     count_stats(cnt, 2, -1, hits, valid);
-}
-
-// ------------------------------------------------------------- integrators
-// first_half, declarations_sph.f90:643-684 (and :812-825, :998-1025), plus the
-// Drucker-Prager call that follows it on soil (:559, :1027).
-template <typename T>
-__global__ void __launch_bounds__(256) k_first_half(PhaseDev<T> P, SimConst c, int with_vof, int do_dp, DevCounters* cnt) {
-    int a = gtid();
-    int fail = 0;
-    if (a < P.n) {
-        const double dt = c.dt;
-        if (!c.summation_density) { double r = P.rho[a]; P.rho_min[a] = r; P.rho[a] = r + (dt / 2.0) * (double)P.drho[a]; }
-        if (with_vof && P.material == 1 && c.volume_fraction) {
-            double f = P.vof[a]; P.vof_min[a] = f; P.vof[a] = f + (dt / 2.0) * (double)P.dvof[a];
-        }
-        const bool soil = P.material == 2;
-        double p = 0, sxx = 0, sxy = 0, syy = 0;
-        if (soil) {
-            p = P.p[a]; sxx = P.sxx[a]; sxy = P.sxy[a]; syy = P.syy[a];
-            if (c.stress_integration == 2) {
-                P.sxx_min[a] = sxx; P.sxy_min[a] = sxy; P.syy_min[a] = syy; P.p_min[a] = p;
-                sxx = sxx + (dt / 2.0) * (double)P.dsxx[a];
-                sxy = sxy + (dt / 2.0) * (double)P.dsxy[a];
-                syy = syy + (dt / 2.0) * (double)P.dsyy[a];
-                p = p + (dt / 2.0) * (double)P.dp[a];
-            }
-        }
-        if (P.itype[a] >= 0) {
-            double2 v = P.v[a];
-            P.v_min[a] = v;
-            typename V2<T>::t d = P.dv[a];
-            v.x = v.x + (dt / 2.0) * (double)d.x;
-            v.y = v.y + (dt / 2.0) * (double)d.y;
-            P.v[a] = v;
-        }
-        if (soil) {
-            if (do_dp) { fail = dp_return(p, sxx, sxy, syy, c.s_alpha1); P.fail[a] = fail; }
-            P.p[a] = p; P.sxx[a] = sxx; P.sxy[a] = sxy; P.syy[a] = syy;
-        }
-    }
-    if (do_dp) {
-        int s = __syncthreads_count(fail);
-        if (threadIdx.x == 0 && s) atomicAdd(&cnt->nfail, s);
-    }
-}
-
-// first_step (:686-723) when first != 0, else second_half (:725-762), plus the
-// Drucker-Prager call after it on soil (:583, :601, :1069, :1107).
-template <typename T>
-__global__ void __launch_bounds__(256) k_update(PhaseDev<T> P, SimConst c, int first, int with_vof, int do_dp, DevCounters* cnt) {
-    int a = gtid();
-    int fail = 0;
-    if (a < P.n) {
-        const double dt = c.dt;
-        if (!c.summation_density) {
-            P.rho[a] = first ? P.rho[a] + (dt / 2.0) * (double)P.drho[a] : P.rho_min[a] + dt * (double)P.drho[a];
-        }
-        if (with_vof && P.material == 1 && c.volume_fraction) {
-            P.vof[a] = first ? P.vof[a] + (dt / 2.0) * (double)P.dvof[a] : P.vof_min[a] + dt * (double)P.dvof[a];
-        }
-        const bool soil = P.material == 2;
-        if (soil) {
-            double p = P.p[a], sxx = P.sxx[a], sxy = P.sxy[a], syy = P.syy[a];
-            const double d0 = P.dsxx[a], d1 = P.dsxy[a], d2 = P.dsyy[a], d3 = P.dp[a];
-            if (c.stress_integration == 1) {
-                sxx = sxx + dt * d0; sxy = sxy + dt * d1; syy = syy + dt * d2; p = p + dt * d3;
-            } else if (c.stress_integration == 2) {
-                if (first) {
-                    sxx = sxx + (dt / 2.0) * d0; sxy = sxy + (dt / 2.0) * d1;
-                    syy = syy + (dt / 2.0) * d2; p = p + (dt / 2.0) * d3;
-                } else {
-                    sxx = P.sxx_min[a] + dt * d0; sxy = P.sxy_min[a] + dt * d1;
-                    syy = P.syy_min[a] + dt * d2; p = P.p_min[a] + dt * d3;
-                }
-            }
-            if (do_dp) { fail = dp_return(p, sxx, sxy, syy, c.s_alpha1); P.fail[a] = fail; }
-            P.p[a] = p; P.sxx[a] = sxx; P.sxy[a] = sxy; P.syy[a] = syy;
-        }
-        if (P.itype[a] >= 0) {
-            double2 v = first ? P.v[a] : P.v_min[a];
-            const typename V2<T>::t d = P.dv[a];
-            const typename V2<T>::t av = P.av[a];
-            double2 x = P.x[a];
-            const double h = first ? dt / 2.0 : dt;
-            v.x = v.x + h * (double)d.x + (double)av.x;
-            x.x = x.x + dt * v.x;
-            v.y = v.y + h * (double)d.y + (double)av.y;
-            x.y = x.y + dt * v.y;
-            P.v[a] = v;
-            P.x[a] = x;
-        }
-    }
-    if (do_dp) {
-        int s = __syncthreads_count(fail);
-        if (threadIdx.x == 0 && s) atomicAdd(&cnt->nfail, s);
-    }
 }
 
 // Sticky per-batch flags: a pair list above max_interaction (the reference
@@ -762,6 +769,22 @@ __global__ void k_check(const DevCounters* __restrict__ c, int* __restrict__ sti
 }
 
 // ------------------------------------------------------- layout transforms
+// Every persistent field of a phase permuted into the current cell order in
+// one launch: dst_i[k] = src_i[perm[k]].
+struct PermField { const void* src; void* dst; int bytes; int pad; };
+struct PermList { int count; int pad; PermField f[44]; };
+__global__ void __launch_bounds__(256) k_permute_all(int n, const int* __restrict__ perm, PermList L) {
+    int k = gtid();
+    if (k >= n) return;
+    const int a = perm[k];
+    for (int i = 0; i < L.count; ++i) {
+        const PermField& f = L.f[i];
+        if (f.bytes == 4) ((int*)f.dst)[k] = ((const int*)f.src)[a];
+        else if (f.bytes == 8) ((long long*)f.dst)[k] = ((const long long*)f.src)[a];
+        else ((int4*)f.dst)[k] = ((const int4*)f.src)[a];
+    }
+}
+
 template <typename S>
 __global__ void __launch_bounds__(256) k_permute(int n, const int* __restrict__ perm, const S* __restrict__ src, S* __restrict__ dst) {
     int k = gtid();

@@ -214,7 +214,6 @@ def main():
     th.start()
     time.sleep(0.3)
     launches0 = solver.kernel_report()["launches"]
-    solver.profile(True)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
@@ -226,9 +225,13 @@ def main():
     if world > 1:
         dist.barrier()
     ms = e0.elapsed_time(e1)
+    launches = solver.kernel_report()["launches"] - launches0
+    # per-kernel CUDA-event times on the library's stream over a second window
+    # of the same K steps (events between launches would slow the headline one)
+    solver.profile(True)
+    solver.time_integration(args.steps)
     rep = solver.kernel_report()
     solver.profile(False)
-    launches = rep["launches"] - launches0
     stop.set()
     th.join(timeout=10)
     clocks = summarize_clocks(samples, local)

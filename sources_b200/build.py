@@ -38,16 +38,16 @@ def up_to_date() -> bool:
     return all(os.path.getmtime(s) <= t for s in sources())
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    if not force and up_to_date():
+def build(force: bool = False, verbose: bool = False, defines=(), out: str = OUT) -> str:
+    if not force and out == OUT and up_to_date():
         return OUT
     os.makedirs(os.path.join(HERE, "_build"), exist_ok=True)
-    tmp = OUT + ".tmp"
+    tmp = out + ".tmp"
     # -prec-div/-prec-sqrt=false only affect float arithmetic (the FP32 pair
     # mode); double division and sqrt stay IEEE.
     cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-prec-div=false", "-prec-sqrt=false",
            "-shared", "-Xcompiler", "-fPIC",
-           "-Xptxas", "-v", "-o", tmp, SRC, "-lcudart"]
+           "-Xptxas", "-v", *["-D" + d for d in defines], "-o", tmp, SRC, "-lcudart"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     with open(os.path.join(HERE, "_build", "ptxas.log"), "w") as f:
         f.write(r.stdout + r.stderr)
@@ -56,8 +56,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
         raise RuntimeError("nvcc failed building libsphg.so")
     if verbose:
         sys.stderr.write(r.stderr)
-    os.replace(tmp, OUT)
-    return OUT
+    os.replace(tmp, out)
+    return out
 
 
 if __name__ == "__main__":

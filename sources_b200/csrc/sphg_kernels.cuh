@@ -288,7 +288,7 @@ __global__ void __launch_bounds__(SPHG_TPB) k_water_sum(PhaseDev<T> P, GridGeom 
         num += mb * w;
         sx += mb * ((rb.vx - ra.vx) * (sr * dx));
         sy += mb * ((rb.vy - ra.vy) * (sr * dy));
-    });
+    }, [&](int m) { prefetch_l1(rec + m); });
     if (valid) {
         const int a = P.perm[k];
         const T rho = num / wi;
@@ -346,7 +346,7 @@ __global__ void __launch_bounds__(SPHG_TPB) k_water_pass_a(PhaseDev<T> P, GridGe
             t1 += rb.vol * (du * gy + dv * gx);
             t2 += rb.vol * (c23 * (T(2) * dv * gy - du * gx));
         }
-    });
+    }, [&](int m) { prefetch_l1(rec + m); });
     if (valid) {
         T txx, txy, tyy, drho;
         double p, cnew, vof;
@@ -460,7 +460,7 @@ __global__ void __launch_bounds__(SPHG_TPB) k_water_pass_b(PhaseDev<T> P, GridGe
             xsx -= q * dvx;
             xsy -= q * dvy;
         }
-    });
+    }, [&](int m) { prefetch_l1(rec + m); prefetch_l1(P.recB + m); });
     if (valid) {
         T dvx = -(phia * d1x) + d2x + d3x;
         T dvy = -(phia * d1y) + d2y + d3y;
@@ -584,7 +584,7 @@ __global__ void __launch_bounds__(SPHG_TPB) k_soil_pass(PhaseDev<T> P, GridGeom 
             xsx += q * du;
             xsy += q * dv;
         }
-    });
+    }, [&](int m) { prefetch_l1(P.recA + m); prefetch_l1(P.recB + m); });
     int fail = 0, fail3 = 0;
     if (valid) {
         T dvx, dvy;
@@ -688,7 +688,7 @@ __global__ void __launch_bounds__(SPHG_TPB) k_cross_soil(PhaseDev<T> S, PhaseDev
         const T mp = rb.vol * qb.p;
         dpx += mp * gx;
         dpy += mp * gy;
-    });
+    }, [&](int m) { prefetch_l1(W.recA + m); prefetch_l1(W.recB + m); });
     int fail3 = 0;
     if (valid) {
         const int a = S.perm[k];
@@ -735,7 +735,7 @@ __global__ void __launch_bounds__(SPHG_TPB) k_cross_water(PhaseDev<T> W, PhaseDe
         ddy -= q * uy;
         dvof -= mb * (sr * (ux * dx + uy * dy));
         v2 += mb * w;
-    });
+    }, [&](int m) { prefetch_l1(S.recA + m); prefetch_l1(S.recB + m); });
     if (valid) {
         const int a = W.perm[k];
         const T fd = phiw * negg_ks;

@@ -192,7 +192,7 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
 
-    from sources_b200 import Solver, build, scenes
+    from sources_b200 import Solver, build, replicas, scenes
     from sources_b200.abi import SPHG_FP32
 
     build.build()
@@ -235,11 +235,8 @@ def main():
     stop.set()
     th.join(timeout=10)
     clocks = summarize_clocks(samples, local)
-    if world > 1:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * n * args.steps / (ms / 1000.0)
+    ms = replicas.max_over_ranks(ms, dist if world > 1 else None, device="cuda")
+    value = replicas.weak_scaling_value(world, n, args.steps, ms)
 
     # ---- dominant kernel and its roofline
     kern = rep["kernels"]
@@ -280,10 +277,7 @@ def main():
             solver.download(k + 1, into=host[k])
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = replicas.max_over_ranks(e2e_s, dist if world > 1 else None, device="cuda")
     bytes_per_step = sum(P.nbytes() for P in host)
     e2e = {"value": world * n * args.e2e_steps / e2e_s, "unit": UNIT,
            "h2d_bytes_per_step": bytes_per_step, "d2h_bytes_per_step": bytes_per_step,

@@ -199,6 +199,30 @@ int sphg_kernel_report(sphg_ctx* ctx, char* buf, int64_t cap);
 void sphg_destroy(sphg_ctx* ctx);
 const char* sphg_strerror(int code);
 
+/* Size limits of sphg_sum_density_noalloc. */
+#define SPHG_NOALLOC_MAX_PARTICLES 32768
+#define SPHG_NOALLOC_MAX_CELLS 65536
+
+/* No counterpart in the reference: an allocation-free summation density
+ * (the Shepard-normalised kernel sum that starts the water-only step) for
+ * callers that cannot allocate device memory, e.g. a host whose GPU memory
+ * is owned by another runtime's pool allocator, or a solver loop that runs on
+ * a fixed memory budget and may not allocate during its time steps.
+ * Inputs and the output are DEVICE pointers in the Fortran layout (x is
+ * (2,n)); rho_out may alias rho.  Only p->skf, p->dim and the grid extent
+ * p->x_min..y_max are read.  Its working memory is one static array of about
+ * 4.3 MB that every GPU loading the library keeps until exit: n above
+ * SPHG_NOALLOC_MAX_PARTICLES, or a neighbour grid above
+ * SPHG_NOALLOC_MAX_CELLS cells, returns SPHG_ERR_BAD_ARG.  All calls share
+ * that array, so calls whose GPU work overlaps race and must be serialised.
+ * The first call on a device looks up the array's address and should come
+ * before any stream capture.  The call waits on `cuda_stream` once (for the
+ * h range); the result is complete when the stream reaches the end of the
+ * call's work. */
+int sphg_sum_density_noalloc(const sphg_params* p, int32_t n, const double* x_dev, const double* hsml_dev,
+                             const double* mass_dev, const double* rho_dev, double* rho_out_dev,
+                             void* cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif

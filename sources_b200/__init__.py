@@ -29,7 +29,7 @@ LIB_PATH = os.path.join(HERE, "libsphg.so")
 EXPORTS = ("sphg_default_params", "sphg_create", "sphg_upload_phase", "sphg_single_step",
            "sphg_time_integration", "sphg_download_phase", "sphg_export_pairs", "sphg_stats",
            "sphg_set_stream", "sphg_kernel_profile", "sphg_kernel_report", "sphg_destroy",
-           "sphg_strerror")
+           "sphg_strerror", "sphg_sum_density_noalloc")
 
 _lib = None
 
@@ -67,6 +67,8 @@ def load(path: str = LIB_PATH):
     L.sphg_destroy.restype = None
     L.sphg_strerror.argtypes = [C.c_int]
     L.sphg_strerror.restype = C.c_char_p
+    L.sphg_sum_density_noalloc.argtypes = [C.POINTER(Params), C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                           C.c_void_p, C.c_void_p, C.c_void_p]
     _lib = L
     return L
 

@@ -14,7 +14,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-SRC = os.path.join(HERE, "csrc", "sphg_api.cu")
+SRC = [os.path.join(HERE, "csrc", "sphg_api.cu"), os.path.join(HERE, "csrc", "sphg_noalloc.cu")]
 OUT = os.path.join(HERE, "libsphg.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -47,7 +47,7 @@ def build(force: bool = False, verbose: bool = False, defines=(), out: str = OUT
     # mode); double division and sqrt stay IEEE.
     cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-prec-div=false", "-prec-sqrt=false",
            "-shared", "-Xcompiler", "-fPIC",
-           "-Xptxas", "-v", *["-D" + d for d in defines], "-o", tmp, SRC, "-lcudart"]
+           "-Xptxas", "-v", *["-D" + d for d in defines], "-o", tmp, *SRC, "-lcudart"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     with open(os.path.join(HERE, "_build", "ptxas.log"), "w") as f:
         f.write(r.stdout + r.stderr)

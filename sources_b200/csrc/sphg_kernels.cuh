@@ -39,7 +39,7 @@ __device__ __forceinline__ int gtid() { return blockIdx.x * blockDim.x + threadI
 
 // ----------------------------------------------------------------- cell list
 // cell key (row-major) and the particle's rank inside its cell.
-__global__ void __launch_bounds__(256) k_cell_count(const double2* __restrict__ x, int n, GridGeom g,
+static __global__ void __launch_bounds__(256) k_cell_count(const double2* __restrict__ x, int n, GridGeom g,
                                                     int* __restrict__ cell_id, int* __restrict__ rank,
                                                     int* __restrict__ counts, DevCounters* cnt) {
     int a = gtid();
@@ -54,7 +54,7 @@ __global__ void __launch_bounds__(256) k_cell_count(const double2* __restrict__ 
     rank[a] = atomicAdd(counts + c, 1);
 }
 
-__global__ void __launch_bounds__(256) k_cell_scatter(int n, const int* __restrict__ cell_id, const int* __restrict__ rank,
+static __global__ void __launch_bounds__(256) k_cell_scatter(int n, const int* __restrict__ cell_id, const int* __restrict__ rank,
                                                       const int* __restrict__ cell_start, int* __restrict__ perm) {
     int a = gtid();
     if (a >= n) return;
@@ -64,7 +64,7 @@ __global__ void __launch_bounds__(256) k_cell_scatter(int n, const int* __restri
 // Insertion sort of each cell's (few) entries by original particle index, so
 // the visiting order, and with it every sum, depends neither on atomic timing
 // nor on the current state order (a download/upload restart is bit-identical).
-__global__ void __launch_bounds__(256) k_cell_sort(int ncell, const int* __restrict__ cell_start,
+static __global__ void __launch_bounds__(256) k_cell_sort(int ncell, const int* __restrict__ cell_start,
                                                    const int* __restrict__ orig, int* __restrict__ perm) {
     int c = gtid();
     if (c >= ncell) return;
@@ -761,7 +761,7 @@ __global__ void __launch_bounds__(SPHG_TPB) k_cross_water(PhaseDev<T> W, PhaseDe
 
 // Sticky per-batch flags: a pair list above max_interaction (the reference
 // stops there, m_particles.f90:992-993) and non-finite positions.
-__global__ void k_check(const DevCounters* __restrict__ c, int* __restrict__ sticky, unsigned long long cap) {
+static __global__ void k_check(const DevCounters* __restrict__ c, int* __restrict__ sticky, unsigned long long cap) {
     if (threadIdx.x == 0 && blockIdx.x == 0) {
         if (c->pairs[0] / 2 > cap || c->pairs[1] / 2 > cap || c->pairs[2] > cap) sticky[0] = 1;
         if (c->nonfinite) sticky[1] = 1;
@@ -773,7 +773,7 @@ __global__ void k_check(const DevCounters* __restrict__ c, int* __restrict__ sti
 // one launch: dst_i[k] = src_i[perm[k]].
 struct PermField { const void* src; void* dst; int bytes; int pad; };
 struct PermList { int count; int pad; PermField f[44]; };
-__global__ void __launch_bounds__(256) k_permute_all(int n, const int* __restrict__ perm, PermList L) {
+static __global__ void __launch_bounds__(256) k_permute_all(int n, const int* __restrict__ perm, PermList L) {
     int k = gtid();
     if (k >= n) return;
     const int a = perm[k];
@@ -790,7 +790,7 @@ __global__ void __launch_bounds__(256) k_permute(int n, const int* __restrict__ 
     int k = gtid();
     if (k < n) dst[k] = src[perm[k]];
 }
-__global__ void __launch_bounds__(256) k_iota(int n, int* __restrict__ v) {
+static __global__ void __launch_bounds__(256) k_iota(int n, int* __restrict__ v) {
     int k = gtid();
     if (k < n) v[k] = k;
 }
@@ -814,12 +814,12 @@ __global__ void __launch_bounds__(256) k_from_original(int n, const int* __restr
     S* d = dst + (size_t)a * comps;
     for (int t = 0; t < comps; ++t) d[t] = (S)s[t];
 }
-__global__ void __launch_bounds__(256) k_to_original_i(int n, const int* __restrict__ orig, const int* __restrict__ src,
+static __global__ void __launch_bounds__(256) k_to_original_i(int n, const int* __restrict__ orig, const int* __restrict__ src,
                                                        int* __restrict__ dst) {
     int a = gtid();
     if (a < n) dst[orig[a]] = src[a];
 }
-__global__ void __launch_bounds__(256) k_from_original_i(int n, const int* __restrict__ orig, const int* __restrict__ src,
+static __global__ void __launch_bounds__(256) k_from_original_i(int n, const int* __restrict__ orig, const int* __restrict__ src,
                                                          int* __restrict__ dst) {
     int a = gtid();
     if (a < n) dst[a] = src[orig[a]];
@@ -827,7 +827,7 @@ __global__ void __launch_bounds__(256) k_from_original_i(int n, const int* __res
 
 // Pair export: per particle (original index i), the neighbours j > i (or, for
 // the cross list, every neighbour), sorted, written at offset[i].
-__global__ void __launch_bounds__(SPHG_TPB) k_pairs_count(int n, const int* __restrict__ perm, const int* __restrict__ orig,
+static __global__ void __launch_bounds__(SPHG_TPB) k_pairs_count(int n, const int* __restrict__ perm, const int* __restrict__ orig,
                                                           const double2* __restrict__ xs, const double* __restrict__ hs,
                                                           GridGeom g, SearchConst sc, const int* __restrict__ cstart_o,
                                                           const double2* __restrict__ xs_o, const double* __restrict__ hs_o,

@@ -37,15 +37,24 @@ METRIC = "particle-steps/s at 1M particles (two-phase water/soil SPH step, 1 B20
 UNIT = "particle-steps/s"
 WORKLOAD = "two_phase_912k"
 
-# Algorithmic HBM bytes per particle of each pair pass in FP32 mode: the
-# particle's own sorted record, position and index read once and its results
-# written once (neighbour records are re-read from L1/L2 and not counted).
+# Algorithmic HBM bytes per particle of each kernel in FP32 mode: the
+# particle's own data read once and its results written once (neighbour
+# records are re-read from L1/L2 and not counted).  The leapfrog predictor
+# runs inside `gather`, the corrector inside the last pass of each phase
+# (`cross_water`, `cross_soil`), so their state traffic is counted there.
 ALG_BYTES = {
-    "water_pass_a": 4 + 16 + 8 + 16 + 8 + 8 + 4 + 4 + 4 + 8 + 3 * 8 + 32 + 4,  # perm,xs,hs,recA,rho,c,vof,itype,drho,p,c,s(3),recB,count
-    "water_pass_b": 4 + 16 + 8 + 16 + 32 + 4 + 8 + 8 + 4,                     # perm,xs,hs,recA,recB,itype -> dv,av,dvof
-    "soil_pass": 4 + 16 + 8 + 16 + 32 + 4 + 4 * 8 + 8 + 8 + 4 + 16 + 4 * 4 + 8 + 4 * 4 + 4,
-    "cross_water": 4 + 16 + 8 + 16 + 4 + 8 + 8 + 4 + 4 + 4 + 16,
-    "cross_soil": 4 + 16 + 8 + 16 + 4 + 8 + 8 + 8 + 8,
+    # perm, xs, hs, recA, c, rho, vof, itype -> c, drho, p, s(3), recB, countiac
+    "water_pass_a": 4 + 16 + 8 + 16 + 8 + 8 + 8 + 4 + 8 + 4 + 8 + 24 + 32 + 4,
+    # perm, xs, hs, recA, recB, itype -> dv, av, dvof
+    "water_pass_b": 4 + 16 + 8 + 16 + 32 + 4 + 8 + 8 + 4,
+    # perm, xs, hs, recA, recB, itype, p, s(3), eps_p rw, fail -> dv, av, drho, ds(3), dp, c, t(3), vcc, countiac
+    "soil_pass": 4 + 16 + 8 + 16 + 32 + 4 + 8 + 24 + 16 + 4 + 8 + 8 + 4 + 12 + 4 + 8 + 12 + 4 + 4,
+    # perm, xs, hs, recA, vof, dv rw, dvof rw, vof2, countiac + corrector (rho, rho_min, drho, vof, vof_min,
+    # v_min, av, x rw, v, itype)
+    "cross_water": 4 + 16 + 8 + 16 + 4 + 16 + 8 + 4 + 4 + 16 + 8 + 4 + 16 + 8 + 16 + 8 + 32 + 16 + 4,
+    # perm, xs, hs, recA, vof, dv rw, rho, vof w + corrector (rho, rho_min, drho, p/s rw, ds, dp, v_min, av,
+    # x rw, v, itype, fail)
+    "cross_soil": 4 + 16 + 8 + 16 + 4 + 16 + 8 + 8 + 16 + 4 + 64 + 16 + 16 + 8 + 32 + 16 + 4 + 4,
 }
 # Whole-step algorithmic bytes per particle-step (FP32 pair data, FP64 state):
 # the compulsory state read + write once per step plus the cell key.
@@ -256,7 +265,15 @@ def main():
                 "alg_bytes_per_launch": alg, "avg_launch_ms": avg_ms,
                 "step": {"alg_bytes": step_bytes, "achieved_gbs": step_bytes / (step_ms / 1000.0) / 1e9,
                          "frac": step_bytes / (step_ms / 1000.0) / 1e9 / peak},
-                "kernels_ms_per_step": {k: v[1] / args.steps for k, v in kern.items()}}
+                "kernels_ms_per_step": {k: v[1] / args.steps for k, v in kern.items()},
+                "passes": {k: {"alg_bytes": ALG_BYTES[k] * (scene.phases[1].n if k in ("soil_pass", "cross_soil")
+                                                            else scene.phases[0].n),
+                               "avg_ms": kern[k][1] / max(kern[k][0], 1),
+                               "achieved_gbs": ALG_BYTES[k] * (scene.phases[1].n if k in ("soil_pass", "cross_soil")
+                                                               else scene.phases[0].n)
+                               / (kern[k][1] / max(kern[k][0], 1) / 1000.0) / 1e9,
+                               "traffic": ncu_traffic().get(k)}
+                           for k in ALG_BYTES if k in kern}}
 
     # ---- end to end through the C ABI with pinned host buffers
     def pinned(shape, dtype):

@@ -117,6 +117,7 @@ struct Engine : EngineBase {
 
     explicit Engine(sphg_ctx* c) : ctx(c) { memset(P, 0, sizeof(P)); }
     ~Engine() override {
+        drop_graphs();
         for (void* p : allocs) cudaFree(p);
     }
 
@@ -279,6 +280,7 @@ struct Engine : EngineBase {
         have[ph] = true;
         prepared = false;
         aliased = false;
+        drop_graphs();
         CUDA_TRY(cudaStreamSynchronize(ctx->stream));
         return 0;
     }
@@ -407,18 +409,12 @@ struct Engine : EngineBase {
         }
         int rc = launch("reorder", k_permute_all, blocks(D.n, 256), 256, D.n, (const int*)D.perm, L);
         if (rc) return rc;
-        for (size_t i = 0; i < refs.size(); ++i) std::swap(*refs[i].first, shadow[ph][i]);
+        if ((rc = launch("reorder", k_copy_back_all, blocks(D.n, 256), 256, D.n, L))) return rc;
         return launch("iota", k_iota, blocks(D.n, 256), 256, D.n, D.perm);
     }
 
     // -------------------------------------------------------------- the step
-    int reset_counters() {
-        DevCounters z;
-        memset(&z, 0, sizeof(z));
-        for (int i = 0; i < 2; ++i) { z.miniac[i] = 0x7fffffff; }
-        CUDA_TRY(cudaMemcpyAsync(cnt, &z, sizeof(z), cudaMemcpyHostToDevice, ctx->stream));
-        return 0;
-    }
+    int reset_counters() { return launch("reset", k_reset_counters, 1, 32, cnt); }
 
     // The pair passes of one step for kernel function SKF.  fh: run the
     // leapfrog predictor inside the gathers; u: what the last pass of each
@@ -459,6 +455,62 @@ struct Engine : EngineBase {
         return 0;
     }
 
+    // One captured CUDA graph per kind of regular step (itimestep >= 2):
+    // bit 0 = reorder step, bit 1 = renormalisation step.  Every buffer keeps
+    // its address for the life of a phase, so a graph stays valid until the
+    // next upload.
+    cudaGraphExec_t graphs[4] = {nullptr, nullptr, nullptr, nullptr};
+    bool use_graphs = true;
+
+    void drop_graphs() {
+        for (auto& g : graphs) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    }
+
+    int step_kind(int itimestep) const {
+        const sphg_params& p = ctx->prm;
+        return ((p.reorder_interval > 0 && itimestep % p.reorder_interval == 0) ? 1 : 0) |
+               ((p.volume_fraction_renorm && p.renorm_interval > 0 && itimestep % p.renorm_interval == 0) ? 2 : 0);
+    }
+
+    // Launch the captured graph of this kind of step, capturing it first if
+    // needed.  If capture is not possible, graphs are switched off and the
+    // caller launches the step directly.
+    int step_graphed(int itimestep) {
+        const int kind = step_kind(itimestep);
+        int rc = prepare();
+        if (rc) return rc;
+        if (!graphs[kind]) {
+            cudaGraph_t g = nullptr;
+            const long long before = ctx->prof.launches;
+            if (cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+                cudaGetLastError();
+                use_graphs = false;
+                return 0;
+            }
+            StepCtl u{};
+            u.update = 1;
+            rc = run(itimestep, 1, u);
+            cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+            if (rc || e != cudaSuccess || !g) {
+                if (g) cudaGraphDestroy(g);
+                cudaGetLastError();
+                use_graphs = false;
+                return rc;
+            }
+            cudaError_t ei = cudaGraphInstantiate(&graphs[kind], g, 0);
+            cudaGraphDestroy(g);
+            if (ei != cudaSuccess) { graphs[kind] = nullptr; cudaGetLastError(); use_graphs = false; return 0; }
+            launches_per_graph[kind] = ctx->prof.launches - before;
+            ctx->prof.launches = before;
+        }
+        nfail_slot = 3;
+        if (!ctx->prm.single_phase) aliased = true;
+        CUDA_TRY(cudaGraphLaunch(graphs[kind], ctx->stream));
+        ctx->prof.launches += launches_per_graph[kind];
+        return 0;
+    }
+    long long launches_per_graph[4] = {0, 0, 0, 0};
+
     int run(int itimestep, int fh, StepCtl u) {
         int rc = prepare();
         if (rc) return rc;
@@ -491,6 +543,11 @@ struct Engine : EngineBase {
     // predictor runs inside the gathers (not on the first step), the
     // corrector inside the last pass of each phase
     int step(int itimestep) override {
+        // regular steps replay a captured graph (not while per-kernel timing is on)
+        if (itimestep >= 2 && use_graphs && !ctx->prof.on) {
+            int rc = step_graphed(itimestep);
+            if (rc || use_graphs) return rc;
+        }
         StepCtl u{};
         u.update = 1;
         u.first = itimestep == 1;

@@ -773,6 +773,30 @@ static __global__ void k_check(const DevCounters* __restrict__ c, int* __restric
 // one launch: dst_i[k] = src_i[perm[k]].
 struct PermField { const void* src; void* dst; int bytes; int pad; };
 struct PermList { int count; int pad; PermField f[44]; };
+// Copy every field of the list back (identity order): after k_permute_all
+// has written the cell-ordered fields into their shadows, the state returns
+// to the same buffers, so buffer addresses never change and a captured CUDA
+// graph stays valid across reorders.
+static __global__ void __launch_bounds__(256) k_copy_back_all(int n, PermList L) {
+    int k = gtid();
+    if (k >= n) return;
+    for (int i = 0; i < L.count; ++i) {
+        const PermField& f = L.f[i];
+        if (f.bytes == 4) ((int*)f.src)[k] = ((const int*)f.dst)[k];
+        else if (f.bytes == 8) ((long long*)f.src)[k] = ((const long long*)f.dst)[k];
+        else ((int4*)f.src)[k] = ((const int4*)f.dst)[k];
+    }
+}
+
+// Per-step counters to their initial values (a kernel, so that it can live in a graph).
+static __global__ void k_reset_counters(DevCounters* c) {
+    int i = threadIdx.x;
+    if (i < 3) c->pairs[i] = 0ull;
+    if (i < 2) { c->maxiac[i] = 0; c->miniac[i] = 0x7fffffff; c->noiac[i] = 0; }
+    if (i < 4) c->nfail[i] = 0;
+    if (i == 0) { c->n_out = 0; c->nonfinite = 0; c->overflow = 0; }
+}
+
 static __global__ void __launch_bounds__(256) k_permute_all(int n, const int* __restrict__ perm, PermList L) {
     int k = gtid();
     if (k >= n) return;

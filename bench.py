@@ -169,6 +169,40 @@ def run_reference(args, rank, world):
     return 0
 
 
+def run_ensemble(args, rank, world, torch, dist):
+    """256 scenes (Philox-keyed seeds 0..255: dam-breaks, dry and submerged
+    collapses of 2k-60k particles at dx 0.004 m), each kind packed into one
+    context, cell factor and reorder interval autotuned per group."""
+    from sources_b200 import ensemble, replicas
+    t0 = time.perf_counter()
+    ens = ensemble.Ensemble(ensemble.specs(256))
+    setup_s = time.perf_counter() - t0
+    stream = torch.cuda.current_stream()
+    ens.set_stream(stream.cuda_stream)
+    ens.time_integration(args.warmup)
+    torch.cuda.synchronize()
+    replicas.barrier(dist if world > 1 else None)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ens.time_integration(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = replicas.max_over_ranks(e0.elapsed_time(e1), dist if world > 1 else None, device="cuda")
+    n = ens.n_particles
+    groups = {g.kind: {"scenes": len(g.members), "particles": g.scene.n_particles, "tuning": list(g.tuning),
+                       "autotune_ms_per_step": {"%s,%s" % k: v for k, v in ens.tuning_table.get(g.kind, {}).items()}}
+              for g in ens.groups}
+    ens.close()
+    if rank == 0:
+        print(json.dumps({"metric": "particle-steps/s, 256-scene batched ensemble", "value":
+                          replicas.weak_scaling_value(world, n, args.steps, ms), "unit": UNIT, "n_gpus": world,
+                          "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+                          "higher_is_better": True, "scaling": "weak", "dtype": "f32",
+                          "config": {"workload": "ensemble_256", "scenes": 256, "particles": n, "groups": groups,
+                                     "setup_s": setup_s}}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -178,8 +212,9 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--cpu-steps", type=int, default=60)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default=WORKLOAD, choices=[WORKLOAD, "two_phase_456k"],
-                    help="two_phase_456k: the same scene 2.0 m wide (for profiler captures)")
+    ap.add_argument("--workload", default=WORKLOAD, choices=[WORKLOAD, "two_phase_456k", "ensemble_256"],
+                    help="two_phase_456k: the same scene 2.0 m wide (for profiler captures); "
+                         "ensemble_256: 256 uneven scenes stepped as three batched groups")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -205,6 +240,8 @@ def main():
     from sources_b200.abi import SPHG_FP32
 
     build.build()
+    if args.workload == "ensemble_256":
+        return run_ensemble(args, rank, world, torch, dist)
     if args.workload == WORKLOAD:
         scene = scenes.two_phase(precision=SPHG_FP32)
     else:

@@ -185,6 +185,35 @@ int sphg_export_pairs(sphg_ctx* ctx, int which, int32_t* pair_i, int32_t* pair_j
 /* Counters of the last step. */
 int sphg_stats(sphg_ctx* ctx, sphg_stats_t* out);
 
+/* Batched ensembles (no counterpart in the reference, whose program holds one
+ * scene).  A context may hold several independent scenes side by side: the
+ * host places them far enough apart that no pair crosses scenes, uploads
+ * them as one phase, and gives each particle the index of its scene.  The
+ * parameters that differ between scenes are per-scene; everything else in
+ * sphg_params is shared.  soil_phi is the friction angle in radians.  With a
+ * scene table, scene s advances by its own dt every step (its time is
+ * itimestep * dt_s); *time of sphg_time_integration advances by p->dt. */
+typedef struct sphg_scene {
+    double dt;        /* TIME STEP SIZE of the scene                        */
+    double water_b;   /* WATER PROPERTY b (Tait) of the scene               */
+    double water_c;   /* WATER PROPERTY c (reference sound speed)           */
+    double soil_phi;  /* SOIL FAILURE CRITERIA phi [rad]                    */
+} sphg_scene;
+int sphg_set_scenes(sphg_ctx* ctx, int nscenes, const sphg_scene* scenes);
+/* scene index (0..nscenes-1) of every particle of a phase, original order */
+int sphg_upload_scene_ids(sphg_ctx* ctx, int phase, const int32_t* scene_id);
+
+/* Tuning knobs (no counterpart in the reference): the neighbour-cell edge as
+ * a multiple (>= 1) of the support radius, and the steps between spatial
+ * reorders of the device state.  They change the order in which neighbours
+ * are summed, so results agree to rounding, and the pair sets not at all. */
+typedef struct sphg_tuning {
+    double cell_factor;
+    int32_t reorder_interval;
+    int32_t _pad;
+} sphg_tuning;
+int sphg_set_tuning(sphg_ctx* ctx, const sphg_tuning* t);
+
 /* Run the context's work on a caller-owned cudaStream_t (passed as void*);
  * NULL restores the context's own stream. */
 int sphg_set_stream(sphg_ctx* ctx, void* cuda_stream);

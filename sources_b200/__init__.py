@@ -29,7 +29,8 @@ LIB_PATH = os.path.join(HERE, "libsphg.so")
 EXPORTS = ("sphg_default_params", "sphg_create", "sphg_upload_phase", "sphg_single_step",
            "sphg_time_integration", "sphg_download_phase", "sphg_export_pairs", "sphg_stats",
            "sphg_set_stream", "sphg_kernel_profile", "sphg_kernel_report", "sphg_destroy",
-           "sphg_strerror", "sphg_sum_density_noalloc")
+           "sphg_strerror", "sphg_sum_density_noalloc", "sphg_set_scenes", "sphg_upload_scene_ids",
+           "sphg_set_tuning")
 
 _lib = None
 
@@ -67,6 +68,9 @@ def load(path: str = LIB_PATH):
     L.sphg_destroy.restype = None
     L.sphg_strerror.argtypes = [C.c_int]
     L.sphg_strerror.restype = C.c_char_p
+    L.sphg_set_scenes.argtypes = [P, C.c_int, C.POINTER(abi.SceneRow)]
+    L.sphg_upload_scene_ids.argtypes = [P, C.c_int, C.POINTER(C.c_int32)]
+    L.sphg_set_tuning.argtypes = [P, C.POINTER(abi.Tuning)]
     L.sphg_sum_density_noalloc.argtypes = [C.POINTER(Params), C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
                                            C.c_void_p, C.c_void_p, C.c_void_p]
     _lib = L
@@ -129,6 +133,20 @@ class Solver:
         s = Stats()
         _check(self.L.sphg_stats(self.h, C.byref(s)), "sphg_stats")
         return s
+
+    def set_scenes(self, rows):
+        """rows: [(dt, water_b, water_c, soil_phi), ...] per scene."""
+        arr = (abi.SceneRow * len(rows))(*[abi.SceneRow(*r) for r in rows])
+        _check(self.L.sphg_set_scenes(self.h, len(rows), arr), "sphg_set_scenes")
+
+    def upload_scene_ids(self, phase: int, ids):
+        a = np.ascontiguousarray(ids, dtype=np.int32)
+        _check(self.L.sphg_upload_scene_ids(self.h, phase, a.ctypes.data_as(C.POINTER(C.c_int32))),
+               "sphg_upload_scene_ids")
+
+    def set_tuning(self, cell_factor: float = 1.0, reorder_interval: int = 10):
+        t = abi.Tuning(cell_factor, reorder_interval, 0)
+        _check(self.L.sphg_set_tuning(self.h, C.byref(t)), "sphg_set_tuning")
 
     def set_stream(self, stream_handle: int | None):
         _check(self.L.sphg_set_stream(self.h, C.c_void_p(stream_handle or 0)), "sphg_set_stream")

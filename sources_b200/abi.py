@@ -83,6 +83,14 @@ class PhaseHost(C.Structure):
                 + [(n, _IP) for n in INT_FIELDS])
 
 
+class SceneRow(C.Structure):
+    _fields_ = [("dt", C.c_double), ("water_b", C.c_double), ("water_c", C.c_double), ("soil_phi", C.c_double)]
+
+
+class Tuning(C.Structure):
+    _fields_ = [("cell_factor", C.c_double), ("reorder_interval", C.c_int32), ("_pad", C.c_int32)]
+
+
 class Stats(C.Structure):
     _fields_ = [("niac", C.c_int64 * 3), ("maxiac", C.c_int32 * 2), ("miniac", C.c_int32 * 2),
                 ("noiac", C.c_int32 * 2), ("nfail", C.c_int32), ("n_out_of_domain", C.c_int32),

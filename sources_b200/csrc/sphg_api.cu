@@ -63,6 +63,9 @@ struct EngineBase {
     virtual int finish_batch() = 0;
     virtual int export_pairs(int which, int32_t* pi, int32_t* pj, int64_t cap, int64_t* n) = 0;
     virtual int stats(sphg_stats_t* out) = 0;
+    virtual int set_scenes(int nscenes, const sphg_scene* sc) = 0;
+    virtual int upload_scene_ids(int phase, const int32_t* ids) = 0;
+    virtual int set_tuning(const sphg_tuning* t) = 0;
 };
 
 struct sphg_ctx {
@@ -111,6 +114,12 @@ struct Engine : EngineBase {
     std::vector<void*> shadow[2];   // one reorder target per persistent field
     int nmax = 0;
     double hrange[2][2] = {{0, 0}, {0, 0}};
+    // per-scene parameters (entry 0 = the context's own parameters)
+    std::vector<SceneTab> tab_host;
+    SceneTab* tab_dev = nullptr;
+    int tab_cap = 0;
+    bool tab_custom = false;
+    double cell_factor = 1.0;       // neighbour cell = factor * support radius (autotuned)
     std::vector<void*> allocs;
     SimConst sim{};
     int nfail_slot = 3;             // which DP site the reported nfail comes from
@@ -176,8 +185,68 @@ struct Engine : EngineBase {
         s.w_rho0 = p.water.rho0; s.w_b = p.water.b; s.w_gamma = p.water.gamma; s.w_c = p.water.c; s.w_mu = p.water.viscosity;
         s.s_rho0 = p.soil.rho0; s.s_k = p.soil.k; s.s_E = p.soil.E; s.s_niu = p.soil.niu; s.s_c = p.soil.c;
         s.s_perm = p.soil.permeability; s.s_G = p.soil.G;
-        double t = tan(p.soil.phi);
-        s.s_alpha1 = t / sqrt(9.0 + 12.0 * (t * t));   // m_particles.f90:3338
+        s.s_alpha1 = alpha1_of(p.soil.phi);
+        s.tab = tab_dev;
+    }
+
+    static double alpha1_of(double phi) {   // m_particles.f90:3338
+        double t = tan(phi);
+        return t / sqrt(9.0 + 12.0 * (t * t));
+    }
+
+    // Copy the scene table to the device; entry 0 follows the context's
+    // parameters unless the host set its own table.
+    int sync_table() {
+        const sphg_params& p = ctx->prm;
+        if (!tab_custom) {
+            tab_host.assign(1, SceneTab{p.dt, p.water.b, p.water.c, alpha1_of(p.soil.phi)});
+        }
+        if ((int)tab_host.size() > tab_cap) {
+            release(tab_dev);
+            tab_dev = nullptr;
+            tab_cap = (int)tab_host.size();
+            if (alloc(&tab_dev, (size_t)tab_cap)) return SPHG_ERR_CUDA;
+        }
+        CUDA_TRY(cudaMemcpyAsync(tab_dev, tab_host.data(), sizeof(SceneTab) * tab_host.size(), cudaMemcpyHostToDevice,
+                                 ctx->stream));
+        CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        return 0;
+    }
+
+    int set_scenes(int nscenes, const sphg_scene* sc) override {
+        if (nscenes < 1 || !sc) return SPHG_ERR_BAD_ARG;
+        std::vector<SceneTab> t((size_t)nscenes);
+        for (int i = 0; i < nscenes; ++i) {
+            if (!(sc[i].dt > 0.0)) return SPHG_ERR_BAD_ARG;
+            t[(size_t)i] = SceneTab{sc[i].dt, sc[i].water_b, sc[i].water_c, alpha1_of(sc[i].soil_phi)};
+        }
+        tab_host.swap(t);
+        tab_custom = true;
+        return sync_table();
+    }
+
+    int upload_scene_ids(int phase, const int32_t* ids) override {
+        if (phase < 1 || phase > ctx->nphase || !ids) return SPHG_ERR_BAD_ARG;
+        const int ph = phase - 1;
+        if (!have[ph]) return SPHG_ERR_STATE;
+        PhaseDev<T>& D = P[ph];
+        for (int i = 0; i < D.n; ++i)
+            if (ids[i] < 0 || ids[i] >= (int)std::max<size_t>(tab_host.size(), 1)) return SPHG_ERR_BAD_ARG;
+        CUDA_TRY(cudaMemcpyAsync(stage_i, ids, sizeof(int) * (size_t)D.n, cudaMemcpyHostToDevice, ctx->stream));
+        int rc = launch("upload", k_from_original_i, blocks(D.n, 256), 256, D.n, (const int*)D.orig,
+                        (const int*)stage_i, D.sid);
+        if (rc) return rc;
+        CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        return 0;
+    }
+
+    int set_tuning(const sphg_tuning* t) override {
+        if (!t || !(t->cell_factor >= 1.0) || t->cell_factor > 4.0 || t->reorder_interval < 0) return SPHG_ERR_BAD_ARG;
+        cell_factor = t->cell_factor;
+        ctx->prm.reorder_interval = t->reorder_interval;
+        prepared = false;
+        drop_graphs();
+        return 0;
     }
 
     static int scale_k(int skf) {
@@ -199,7 +268,7 @@ struct Engine : EngineBase {
         if (have[ph] && D.n == n) return 0;   // same size: reuse every buffer
         // a re-upload replaces the arrays
         void* old[] = {D.x, D.v, D.v_min, D.rho, D.rho_min, D.vof, D.vof_min, D.p, D.c, D.mass, D.hsml, D.sxx, D.sxy,
-                       D.syy, D.sxx_min, D.sxy_min, D.syy_min, D.p_min, D.eps_p, D.itype, D.orig, D.fail, D.drho,
+                       D.syy, D.sxx_min, D.sxy_min, D.syy_min, D.p_min, D.eps_p, D.itype, D.orig, D.fail, D.sid, D.drho,
                        D.dvof, D.dsxx, D.dsxy, D.dsyy, D.dp, D.txx, D.txy, D.tyy, D.vcc, D.wxy, D.vof2, D.dv, D.av,
                        D.countiac, D.cell_id, D.cell_fill, D.perm, D.xs, D.hs, D.recA, D.recA2, D.recB};
         for (void* p : old) release(p);
@@ -215,7 +284,7 @@ struct Engine : EngineBase {
         rc |= alloc(&D.sxx, N); rc |= alloc(&D.sxy, N); rc |= alloc(&D.syy, N);
         rc |= alloc(&D.sxx_min, N); rc |= alloc(&D.sxy_min, N); rc |= alloc(&D.syy_min, N); rc |= alloc(&D.p_min, N);
         rc |= alloc(&D.eps_p, N);
-        rc |= alloc(&D.itype, N); rc |= alloc(&D.orig, N); rc |= alloc(&D.fail, N);
+        rc |= alloc(&D.itype, N); rc |= alloc(&D.orig, N); rc |= alloc(&D.fail, N); rc |= alloc(&D.sid, N);
         rc |= alloc(&D.drho, N); rc |= alloc(&D.dvof, N); rc |= alloc(&D.dsxx, N); rc |= alloc(&D.dsxy, N);
         rc |= alloc(&D.dsyy, N); rc |= alloc(&D.dp, N); rc |= alloc(&D.txx, N); rc |= alloc(&D.txy, N);
         rc |= alloc(&D.tyy, N); rc |= alloc(&D.vcc, N); rc |= alloc(&D.wxy, N); rc |= alloc(&D.vof2, N);
@@ -277,6 +346,7 @@ struct Engine : EngineBase {
         rc |= put_rate(n, h->txx, D.txx, 1); rc |= put_rate(n, h->tyy, D.tyy, 1); rc |= put_rate(n, h->txy, D.txy, 1);
         if (rc) return SPHG_ERR_CUDA;
         CUDA_TRY(cudaMemcpyAsync(D.itype, h->itype, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, ctx->stream));
+        CUDA_TRY(cudaMemsetAsync(D.sid, 0, sizeof(int) * (size_t)n, ctx->stream));
         have[ph] = true;
         prepared = false;
         aliased = false;
@@ -311,6 +381,7 @@ struct Engine : EngineBase {
     // Grid and search constants, once every phase is on the device.
     int prepare() {
         if (prepared) return 0;
+        int rc0;
         for (int ph = 0; ph < ctx->nphase; ++ph) if (!have[ph]) return SPHG_ERR_STATE;
         const sphg_params& p = ctx->prm;
         int sk = scale_k(p.skf);
@@ -321,7 +392,8 @@ struct Engine : EngineBase {
             hmin = std::min(hmin, hrange[ph][0]);
             hmax = std::max(hmax, hrange[ph][1]);
         }
-        double cell = sk * hmax * (1.0 + 1e-6);
+        if ((rc0 = sync_table())) return rc0;
+        double cell = sk * hmax * cell_factor * (1.0 + 1e-6);
         if (!(p.x_max > p.x_min) || !(p.y_max > p.y_min)) return SPHG_ERR_BAD_ARG;
         double ncx = std::ceil((p.x_max - p.x_min) / cell) + 1, ncy = std::ceil((p.y_max - p.y_min) / cell) + 1;
         if (ncx * ncy > 2.0e8) return SPHG_ERR_BAD_ARG;
@@ -386,7 +458,7 @@ struct Engine : EngineBase {
         for (double** q : {&D.rho, &D.rho_min, &D.vof, &D.vof_min, &D.p, &D.c, &D.mass, &D.hsml, &D.sxx, &D.sxy,
                            &D.syy, &D.sxx_min, &D.sxy_min, &D.syy_min, &D.p_min, &D.eps_p})
             add((void**)q, 8);
-        for (int** q : {&D.itype, &D.orig, &D.fail, &D.countiac}) add((void**)q, 4);
+        for (int** q : {&D.itype, &D.orig, &D.fail, &D.countiac, &D.sid}) add((void**)q, 4);
         for (T** q : {&D.drho, &D.dvof, &D.dsxx, &D.dsxy, &D.dsyy, &D.dp, &D.txx, &D.txy, &D.tyy, &D.vcc, &D.wxy, &D.vof2})
             add((void**)q, (int)sizeof(T));
         add((void**)&D.dv, (int)sizeof(T2)); add((void**)&D.av, (int)sizeof(T2));
@@ -862,6 +934,24 @@ int sphg_stats(sphg_ctx* c, sphg_stats_t* out) {
     if (!c || !out) return SPHG_ERR_BAD_ARG;
     cudaSetDevice(c->device);
     return c->eng->stats(out);
+}
+
+int sphg_set_scenes(sphg_ctx* c, int nscenes, const sphg_scene* scenes) {
+    if (!c) return SPHG_ERR_BAD_ARG;
+    cudaSetDevice(c->device);
+    return c->eng->set_scenes(nscenes, scenes);
+}
+
+int sphg_upload_scene_ids(sphg_ctx* c, int phase, const int32_t* scene_id) {
+    if (!c) return SPHG_ERR_BAD_ARG;
+    cudaSetDevice(c->device);
+    return c->eng->upload_scene_ids(phase, scene_id);
+}
+
+int sphg_set_tuning(sphg_ctx* c, const sphg_tuning* t) {
+    if (!c) return SPHG_ERR_BAD_ARG;
+    cudaSetDevice(c->device);
+    return c->eng->set_tuning(t);
 }
 
 int sphg_set_stream(sphg_ctx* c, void* s) {

@@ -48,6 +48,16 @@ struct SearchConst {
     int uniform;          // all particles of both lists share one h
 };
 
+// The parameters that differ between the scenes of a batched context
+// (several independent scenes side by side in one set of arrays); every
+// particle carries the index of its scene.  A single scene is entry 0.
+struct SceneTab {
+    double dt;        // time step
+    double w_b;       // water Tait b
+    double w_c;       // water reference sound speed
+    double s_alpha1;  // Drucker-Prager alpha1 = tan(phi)/sqrt(9+12 tan^2(phi))
+};
+
 // Counters the host reads after a batch of steps.
 struct DevCounters {
     unsigned long long pairs[3];     // phase 1, phase 2, cross (last step)
@@ -68,7 +78,7 @@ struct PhaseDev {
     double2 *x, *v, *v_min;
     double *rho, *rho_min, *vof, *vof_min, *p, *c, *mass, *hsml;
     double *sxx, *sxy, *syy, *sxx_min, *sxy_min, *syy_min, *p_min, *eps_p;
-    int *itype, *orig, *fail;
+    int *itype, *orig, *fail, *sid;
     // state order, T
     T *drho, *dvof, *dsxx, *dsxy, *dsyy, *dp, *txx, *txy, *tyy, *vcc, *wxy, *vof2;
     T2 *dv, *av;

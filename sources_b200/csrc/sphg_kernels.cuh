@@ -31,6 +31,7 @@ struct SimConst {
     double gravity, numeric_gravity, alpha, beta, etq, dd, p1, p2, delta, epsilon, dt;
     double w_rho0, w_b, w_gamma, w_c, w_mu;
     double s_rho0, s_k, s_E, s_niu, s_c, s_perm, s_G, s_alpha1;
+    const SceneTab* tab;   // per-scene dt, water b and c, soil alpha1 (indexed by PhaseDev::sid)
 };
 
 #define SPHG_TPB 128
@@ -91,7 +92,8 @@ struct StepCtl {
 // particle's fail flag of that DP call.
 template <typename T>
 __device__ __forceinline__ int first_half_one(const PhaseDev<T>& P, int a, const SimConst& c, int with_vof, int do_dp) {
-    const double dt = c.dt;
+    const SceneTab& st = c.tab[P.sid[a]];
+    const double dt = st.dt;
     if (!c.summation_density) { double r = P.rho[a]; P.rho_min[a] = r; P.rho[a] = r + (dt / 2.0) * (double)P.drho[a]; }
     if (with_vof && P.material == 1 && c.volume_fraction) {
         double f = P.vof[a]; P.vof_min[a] = f; P.vof[a] = f + (dt / 2.0) * (double)P.dvof[a];
@@ -118,7 +120,7 @@ __device__ __forceinline__ int first_half_one(const PhaseDev<T>& P, int a, const
         P.v[a] = v;
     }
     if (soil) {
-        if (do_dp) { fail = dp_return(p, sxx, sxy, syy, c.s_alpha1); P.fail[a] = fail; }
+        if (do_dp) { fail = dp_return(p, sxx, sxy, syy, st.s_alpha1); P.fail[a] = fail; }
         P.p[a] = p; P.sxx[a] = sxx; P.sxy[a] = sxy; P.syy[a] = syy;
     }
     return fail;
@@ -128,7 +130,8 @@ __device__ __forceinline__ int first_half_one(const PhaseDev<T>& P, int a, const
 // Drucker-Prager call after it on soil (:583, :601, :1069, :1107).
 template <typename T>
 __device__ __forceinline__ int update_one(const PhaseDev<T>& P, int a, const SimConst& c, int first, int with_vof, int do_dp) {
-    const double dt = c.dt;
+    const SceneTab& st = c.tab[P.sid[a]];
+    const double dt = st.dt;
     int fail = 0;
     if (!c.summation_density)
         P.rho[a] = first ? P.rho[a] + (dt / 2.0) * (double)P.drho[a] : P.rho_min[a] + dt * (double)P.drho[a];
@@ -148,7 +151,7 @@ __device__ __forceinline__ int update_one(const PhaseDev<T>& P, int a, const Sim
                 syy = P.syy_min[a] + dt * d2; p = P.p_min[a] + dt * d3;
             }
         }
-        if (do_dp) { fail = dp_return(p, sxx, sxy, syy, c.s_alpha1); P.fail[a] = fail; }
+        if (do_dp) { fail = dp_return(p, sxx, sxy, syy, st.s_alpha1); P.fail[a] = fail; }
         P.p[a] = p; P.sxx[a] = sxx; P.sxy[a] = sxy; P.syy[a] = syy;
     }
     if (P.itype[a] >= 0) {
@@ -196,7 +199,7 @@ __global__ void __launch_bounds__(256) k_gather(PhaseDev<T> P, SimConst c, int s
         if (soil) {
             double p = P.p[a], sxx = P.sxx[a], sxy = P.sxy[a], syy = P.syy[a];
             if (do_dp) {
-                fail = dp_return(p, sxx, sxy, syy, c.s_alpha1);
+                fail = dp_return(p, sxx, sxy, syy, c.tab[P.sid[a]].s_alpha1);
                 P.p[a] = p; P.sxx[a] = sxx; P.sxy[a] = sxy; P.syy[a] = syy;
                 P.fail[a] = fail;
             }
@@ -357,7 +360,7 @@ __global__ void __launch_bounds__(SPHG_TPB) k_water_pass_a(PhaseDev<T> P, GridGe
             txy = t2 + t3;
             tyy = c23 * (T(2) * t1 - t0);
             p = P.p[a];
-            if (rho > 0.0) p = c.w_b * (pow(rho / c.w_rho0, c.w_gamma) - 1);
+            if (rho > 0.0) p = c.tab[P.sid[a]].w_b * (pow(rho / c.w_rho0, c.w_gamma) - 1);
             cnew = P.c[a];
             vof = 1.0;
         } else {
@@ -365,8 +368,9 @@ __global__ void __launch_bounds__(SPHG_TPB) k_water_pass_a(PhaseDev<T> P, GridGe
             txx = t0; txy = t1; tyy = t2;
             vof = P.vof[a];
             const double ratio = rho / (c.w_rho0 * vof);
-            p = c.w_b * (pow(ratio, c.w_gamma) - 1);
-            cnew = c.w_c * pow(ratio, 3.0);
+            const SceneTab& st = c.tab[P.sid[a]];
+            p = st.w_b * (pow(ratio, c.w_gamma) - 1);
+            cnew = st.w_c * pow(ratio, 3.0);
             P.c[a] = cnew;
         }
         P.drho[a] = drho;
@@ -611,14 +615,15 @@ __global__ void __launch_bounds__(SPHG_TPB) k_soil_pass(PhaseDev<T> P, GridGeom 
         double ds0 = 0.0, ds1 = 0.0, ds2 = 0.0, dp = 0.0;
         if (c.plasticity == 3) {
             const double J2a = sqrt((sxx * sxx + 2.0 * (sxy * sxy) + syy * syy + (sxx + syy) * (sxx + syy)) / 2.0) + 1.0e-6;
-            if (fabs(J2a - c.s_alpha1 * (3.0 * p)) < SPHG_F32LIT(1.0e-5f)) fail = 1;
+            const double alpha1 = c.tab[P.sid[a]].s_alpha1;
+            if (fabs(J2a - alpha1 * (3.0 * p)) < SPHG_F32LIT(1.0e-5f)) fail = 1;
             P.fail[a] = fail;
             if (fail) {
                 const double exx = dtxx / 2.0 + dvcc / 3.0, exy = dtxy / 2.0, eyy = dtyy / 2.0 + dvcc / 3.0;
                 const double sde = sxx * exx + 2.0 * sxy * exy + syy * eyy;
                 double J2 = (sxx * sxx + 2.0 * (sxy * sxy) + syy * syy + (sxx + syy) * (sxx + syy)) / 2.0;
                 J2 = J2 + 1.0e-10;
-                const double al = c.s_alpha1, K = c.s_k;
+                const double al = alpha1, K = c.s_k;
                 const double dlambda = (3.0 * al * K * dvcc + G / sqrt(J2) * sde) / (9.0 * (al * al) * K + G);
                 if (!(dlambda < 0)) {
                     ds0 = ds0 - dlambda * (G / sqrt(J2) * sxx);

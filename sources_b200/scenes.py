@@ -186,7 +186,7 @@ def granular_column(width=0.2, height=0.1, box_w=1.0, box_h=0.3, dx=0.002, skf=1
 
 
 def two_phase(width=4.0, height=1.0, block_w=1.0, block_h=0.4, water_h=0.8, dx=0.002,
-              porosity=0.4, permeability=1.0e-3, skf=1, precision=SPHG_FP32) -> Scene:
+              porosity=0.4, permeability=1.0e-3, skf=1, phi_deg=19.8, precision=SPHG_FP32) -> Scene:
     """Submerged soil block under a water layer (two-phase step,
     declarations_sph.f90:1131), laid out as input_mix_Savage.f90 does: the
     water lattice fills the block too, as the pore-water phase."""
@@ -197,7 +197,7 @@ def two_phase(width=4.0, height=1.0, block_w=1.0, block_h=0.4, water_h=0.8, dx=0
     S = _phase(x, y, inside & in_block, virt, SPHG_SOIL, dx)
     p = default_params()
     wm = _water_material(water_h)
-    sm = _soil_material(porosity=porosity, permeability=permeability)
+    sm = _soil_material(porosity=porosity, permeability=permeability, phi_deg=phi_deg)
     _set_material(p.water, wm)
     _set_material(p.soil, sm)
     g = p.gravity

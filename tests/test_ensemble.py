@@ -1,0 +1,93 @@
+"""Batched ensembles (sources_b200.ensemble): the scene generator and packing
+on CPU; on a GPU, every scene of a packed group evolves as the same scene
+stepped alone, no pair crosses scenes, and the autotuner picks a candidate."""
+import math
+
+import numpy as np
+import pytest
+
+from sources_b200 import ensemble
+from sources_b200.abi import SPHG_FP64, SPHG_PAIRS_CROSS, SPHG_PAIRS_FIRST, SPHG_PAIRS_SECOND
+
+
+def test_specs_are_keyed_by_seed_and_in_range():
+    a = ensemble.specs(64)
+    b = ensemble.specs(8, first_seed=5)
+    assert a[5:13] == b                       # scene s does not depend on the ensemble size
+    assert {s.kind for s in a} == set(ensemble.KINDS)
+    for s in a:
+        assert 2000 <= s.n_target <= 60000
+        assert 0.5 <= s.aspect <= 4.0 and 20.0 <= s.phi_deg <= 40.0 and 0.1 <= s.depth <= 0.5
+
+
+def small_specs():
+    out = []
+    for seed in range(40):
+        s = ensemble.spec(seed)
+        s.n_target = 1500 + 97 * seed % 900
+        out.append(s)
+    by_kind = {k: [s for s in out if s.kind == k][:2] for k in ensemble.KINDS}
+    return [s for k in ensemble.KINDS for s in by_kind[k]]
+
+
+def test_packing_keeps_scenes_apart():
+    sp = small_specs()
+    built = [ensemble.build_scene(s) for s in sp]
+    for kind in ensemble.KINDS:
+        members = [i for i, s in enumerate(sp) if s.kind == kind]
+        g = ensemble.pack(members, built)
+        h = max(float(built[m].phases[0].hsml.max()) for m in members)
+        for k, P in enumerate(g.scene.phases):
+            spans = []
+            for local, m in enumerate(members):
+                a, b = g.ranges[k][local]
+                assert np.all(g.sids[k][a:b] == local)
+                x = P.x[a:b, 0]
+                spans.append((x.min(), x.max()))
+                assert np.allclose(x - g.offsets[local], built[m].phases[k].x[:, 0])
+            for (l0, r0), (l1, r1) in zip(spans, spans[1:]):
+                assert l1 - r0 > 3 * h * 2          # wider than two support radii
+        assert len(g.rows) == len(members)
+
+
+@pytest.mark.gpu
+def test_packed_scenes_evolve_as_alone(cuda_ok):
+    from sources_b200 import Solver
+    sp = small_specs()
+    ens = ensemble.Ensemble(sp, precision=SPHG_FP64, tune=False)
+    try:
+        ens.time_integration(15)
+        for i, s in enumerate(sp):
+            alone = ensemble.build_scene(s, precision=SPHG_FP64)
+            with Solver(alone) as g:
+                g.time_integration(15)
+                for k in range(len(alone.phases)):
+                    a = g.download(k + 1)
+                    b = ens.scene(i)[k]
+                    for f in ("x", "vx", "rho", "p", "sxx", "vof", "dvx"):
+                        ref = getattr(a, f)
+                        scale = max(float(np.abs(ref).max()), 1e-300)
+                        err = float(np.abs(getattr(b, f) - ref).max()) / scale
+                        assert err <= 1e-7, (s.kind, i, k, f, err)
+    finally:
+        ens.close()
+
+
+@pytest.mark.gpu
+def test_no_pair_crosses_scenes_and_autotuner_picks(cuda_ok):
+    sp = small_specs()
+    ens = ensemble.Ensemble(sp, tune=True)
+    try:
+        for g, sv in zip(ens.groups, ens.solvers):
+            lists = [SPHG_PAIRS_FIRST] if len(g.scene.phases) == 1 else [SPHG_PAIRS_FIRST, SPHG_PAIRS_SECOND,
+                                                                        SPHG_PAIRS_CROSS]
+            for w in lists:
+                pi, pj = sv.pairs(w)
+                si = g.sids[1 if w == SPHG_PAIRS_SECOND else 0][pi - 1]
+                sj = g.sids[0 if w == SPHG_PAIRS_FIRST else 1][pj - 1]
+                assert len(pi) > 0 and np.all(si == sj), (g.kind, w)
+            assert g.tuning in ensemble.CANDIDATES
+            assert all(math.isfinite(v) and v > 0 for v in ens.tuning_table[g.kind].values())
+        ens.time_integration(5)
+    finally:
+        ens.close()

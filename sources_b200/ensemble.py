@@ -187,6 +187,7 @@ class Ensemble:
             if not members:
                 continue
             g = pack(members, self.built)
+            g.kind = kind
             if tune:
                 g.tuning, self.tuning_table[kind] = autotune(g)
             self.groups.append(g)

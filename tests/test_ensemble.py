@@ -64,7 +64,12 @@ def test_packed_scenes_evolve_as_alone(cuda_ok):
                 for k in range(len(alone.phases)):
                     a = g.download(k + 1)
                     b = ens.scene(i)[k]
-                    for f in ("x", "vx", "rho", "p", "sxx", "vof", "dvx"):
+                    # water stress of a two-phase context is the shared working
+                    # array the soil pass overwrites (a view over the whole
+                    # context, not a per-scene field), so it is not compared
+                    fields = ("x", "vx", "rho", "p", "vof", "dvx") + (
+                        ("sxx", "syy", "sxy") if not (len(alone.phases) == 2 and k == 0) else ())
+                    for f in fields:
                         ref = getattr(a, f)
                         scale = max(float(np.abs(ref).max()), 1e-300)
                         err = float(np.abs(getattr(b, f) - ref).max()) / scale

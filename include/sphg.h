@@ -214,6 +214,36 @@ typedef struct sphg_tuning {
 } sphg_tuning;
 int sphg_set_tuning(sphg_ctx* ctx, const sphg_tuning* t);
 
+/* The case (steering) file of the reference, read_cas / treat_cmd /
+ * usr_def_parameter (declarations_sph.f90:61-335): "NAME = value" commands,
+ * '#' comment lines, a trailing ',' continues a command on the next line,
+ * a line starting with '&' ends the file.  sphg_read_case fills the
+ * matching fields of *p (WATER PROPERTY, SOIL PROPERTY, DARCY PARAMETER,
+ * SOIL FAILURE CRITERIA, TIME STEP SIZE, INTEGRATION SCHEME, SINGLE PHASE,
+ * FIRST PHASE) and the rest into *c.  Unknown keywords are counted, as the
+ * reference reports and skips them; a value that does not parse makes the
+ * call return SPHG_ERR_BAD_ARG after reading the whole file. */
+typedef struct sphg_case {
+    int32_t print_step, save_step, nnps, single_phase, dry_soil, with_nozzle;
+    int32_t first_material, second_material;   /* SPHG_WATER / SPHG_SOIL     */
+    int32_t unknown_keywords, bad_values;
+    double inlet_velocity, dt;
+    char results[3][256];                       /* RESULTS FILE: three names  */
+    char particle_size[32], operating_mode[32];
+} sphg_case;
+int sphg_read_case(const char* path, sphg_params* p, sphg_case* c);
+
+/* Tecplot ASCII output of output (declarations_sph.f90:1703-1810): one zone
+ * in BLOCK format with the reference's variable list (water: X, Y, Pressure,
+ * VoF, vx, vy, rho, zone, VoF2, mass; soil: X, Y, Pressure, VoF, ep, sxy,
+ * sxx, syy, vx, vy, rho, mass, sigma_yy = -p + syy, zone).  zone may be NULL
+ * (written as 0).  The _phase form writes host arrays (no GPU involved); the
+ * context form downloads phase 1 to path_first and, for two-phase contexts,
+ * phase 2 to path_second, appending when `append` is set. */
+int sphg_write_tecplot_phase(const char* path, int append, const sphg_phase_host* v, const int32_t* zone);
+int sphg_write_tecplot(sphg_ctx* ctx, const char* path_first, const char* path_second, int append,
+                       const int32_t* zone_first, const int32_t* zone_second);
+
 /* Run the context's work on a caller-owned cudaStream_t (passed as void*);
  * NULL restores the context's own stream. */
 int sphg_set_stream(sphg_ctx* ctx, void* cuda_stream);

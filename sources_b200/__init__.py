@@ -30,7 +30,7 @@ EXPORTS = ("sphg_default_params", "sphg_create", "sphg_upload_phase", "sphg_sing
            "sphg_time_integration", "sphg_download_phase", "sphg_export_pairs", "sphg_stats",
            "sphg_set_stream", "sphg_kernel_profile", "sphg_kernel_report", "sphg_destroy",
            "sphg_strerror", "sphg_sum_density_noalloc", "sphg_set_scenes", "sphg_upload_scene_ids",
-           "sphg_set_tuning")
+           "sphg_set_tuning", "sphg_read_case", "sphg_write_tecplot_phase", "sphg_write_tecplot")
 
 _lib = None
 
@@ -71,10 +71,36 @@ def load(path: str = LIB_PATH):
     L.sphg_set_scenes.argtypes = [P, C.c_int, C.POINTER(abi.SceneRow)]
     L.sphg_upload_scene_ids.argtypes = [P, C.c_int, C.POINTER(C.c_int32)]
     L.sphg_set_tuning.argtypes = [P, C.POINTER(abi.Tuning)]
+    L.sphg_read_case.argtypes = [C.c_char_p, C.POINTER(Params), C.POINTER(abi.Case)]
+    L.sphg_write_tecplot_phase.argtypes = [C.c_char_p, C.c_int, C.POINTER(PhaseHost), C.POINTER(C.c_int32)]
+    L.sphg_write_tecplot.argtypes = [P, C.c_char_p, C.c_char_p, C.c_int, C.POINTER(C.c_int32),
+                                     C.POINTER(C.c_int32)]
     L.sphg_sum_density_noalloc.argtypes = [C.POINTER(Params), C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
                                            C.c_void_p, C.c_void_p, C.c_void_p]
     _lib = L
     return L
+
+
+def read_case(path: str, params: Params | None = None):
+    """Read a reference case file (read_cas, declarations_sph.f90:61).
+    Returns (params, case) with the file's values applied to `params`
+    (reference defaults if None)."""
+    L = load()
+    p = params if params is not None else default_params()
+    c = abi.Case()
+    rc = L.sphg_read_case(path.encode(), C.byref(p), C.byref(c))
+    if rc:
+        raise SPHError(rc, f"sphg_read_case({path}): {c.bad_values} bad value(s)")
+    return p, c
+
+
+def write_tecplot_phase(path: str, P: PhaseArrays, zone=None, append: bool = False):
+    """Tecplot ASCII zone of one phase from host arrays."""
+    L = load()
+    z = None if zone is None else np.ascontiguousarray(zone, dtype=np.int32)
+    _check(L.sphg_write_tecplot_phase(path.encode(), 1 if append else 0, C.byref(P.host_struct()),
+                                      None if z is None else z.ctypes.data_as(C.POINTER(C.c_int32))),
+           "sphg_write_tecplot_phase")
 
 
 def _check(rc: int, where: str):
@@ -147,6 +173,15 @@ class Solver:
     def set_tuning(self, cell_factor: float = 1.0, reorder_interval: int = 10):
         t = abi.Tuning(cell_factor, reorder_interval, 0)
         _check(self.L.sphg_set_tuning(self.h, C.byref(t)), "sphg_set_tuning")
+
+    def write_tecplot(self, path_first: str, path_second: str | None = None, append: bool = False,
+                      zone_first=None, zone_second=None):
+        """Tecplot ASCII output of every phase (output, declarations_sph.f90:1703)."""
+        z = [None if a is None else np.ascontiguousarray(a, dtype=np.int32) for a in (zone_first, zone_second)]
+        zp = [None if a is None else a.ctypes.data_as(C.POINTER(C.c_int32)) for a in z]
+        _check(self.L.sphg_write_tecplot(self.h, path_first.encode(), None if path_second is None else
+                                         path_second.encode(), 1 if append else 0, zp[0], zp[1]),
+               "sphg_write_tecplot")
 
     def set_stream(self, stream_handle: int | None):
         _check(self.L.sphg_set_stream(self.h, C.c_void_p(stream_handle or 0)), "sphg_set_stream")

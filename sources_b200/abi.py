@@ -91,6 +91,14 @@ class Tuning(C.Structure):
     _fields_ = [("cell_factor", C.c_double), ("reorder_interval", C.c_int32), ("_pad", C.c_int32)]
 
 
+class Case(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in ("print_step", "save_step", "nnps", "single_phase", "dry_soil",
+                                         "with_nozzle", "first_material", "second_material",
+                                         "unknown_keywords", "bad_values")] + [
+        ("inlet_velocity", C.c_double), ("dt", C.c_double), ("results", (C.c_char * 256) * 3),
+        ("particle_size", C.c_char * 32), ("operating_mode", C.c_char * 32)]
+
+
 class Stats(C.Structure):
     _fields_ = [("niac", C.c_int64 * 3), ("maxiac", C.c_int32 * 2), ("miniac", C.c_int32 * 2),
                 ("noiac", C.c_int32 * 2), ("nfail", C.c_int32), ("n_out_of_domain", C.c_int32),

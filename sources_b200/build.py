@@ -14,7 +14,8 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-SRC = [os.path.join(HERE, "csrc", "sphg_api.cu"), os.path.join(HERE, "csrc", "sphg_noalloc.cu")]
+SRC = [os.path.join(HERE, "csrc", "sphg_api.cu"), os.path.join(HERE, "csrc", "sphg_noalloc.cu"),
+       os.path.join(HERE, "csrc", "sphg_io.cpp")]
 OUT = os.path.join(HERE, "libsphg.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -954,6 +954,27 @@ int sphg_set_tuning(sphg_ctx* c, const sphg_tuning* t) {
     return c->eng->set_tuning(t);
 }
 
+int sphg_write_tecplot(sphg_ctx* c, const char* path_first, const char* path_second, int append,
+                       const int32_t* zone_first, const int32_t* zone_second) {
+    if (!c || !path_first || (c->nphase == 2 && !path_second)) return SPHG_ERR_BAD_ARG;
+    for (int ph = 1; ph <= c->nphase; ++ph) {
+        sphg_phase_host h;
+        memset(&h, 0, sizeof(h));
+        // sizes first
+        int rc = c->eng->download(ph, &h);
+        if (rc) return rc;
+        const size_t n = (size_t)(h.ntotal + h.nvirt);
+        std::vector<double> x(2 * n), vx(2 * n), p(n), rho(n), mass(n), vof(n), vof2(n), eps(n), sxx(n), sxy(n), syy(n);
+        h.x = x.data(); h.vx = vx.data(); h.p = p.data(); h.rho = rho.data(); h.mass = mass.data();
+        h.vof = vof.data(); h.vof2 = vof2.data(); h.epsilon_p = eps.data();
+        h.sxx = sxx.data(); h.sxy = sxy.data(); h.syy = syy.data();
+        if ((rc = c->eng->download(ph, &h))) return rc;
+        rc = sphg_write_tecplot_phase(ph == 1 ? path_first : path_second, append, &h, ph == 1 ? zone_first : zone_second);
+        if (rc) return rc;
+    }
+    return SPHG_OK;
+}
+
 int sphg_set_stream(sphg_ctx* c, void* s) {
     if (!c) return SPHG_ERR_BAD_ARG;
     c->stream = s ? (cudaStream_t)s : c->own_stream;

@@ -46,6 +46,8 @@ int main(void) {
   printf("%zu %zu %zu %zu\n", offsetof(sphg_phase_host, x), offsetof(sphg_phase_host, txy),
          offsetof(sphg_phase_host, fail), offsetof(sphg_params, max_interaction));
   printf("%zu %zu\n", offsetof(sphg_stats_t, time), offsetof(sphg_stats_t, last_step_ms));
+  printf("%zu %zu %zu %zu %zu\n", sizeof(sphg_case), offsetof(sphg_case, results), offsetof(sphg_case, operating_mode),
+         sizeof(sphg_scene), sizeof(sphg_tuning));
   return 0;
 }
 '''
@@ -67,6 +69,9 @@ def test_struct_layout_matches_ctypes():
     assert v[5] == PhaseHost.x.offset and v[6] == PhaseHost.txy.offset and v[7] == PhaseHost.fail.offset
     assert v[8] == Params.max_interaction.offset
     assert v[9] == Stats.time.offset and v[10] == Stats.last_step_ms.offset
+    assert v[11] == C.sizeof(abi.Case) and v[12] == abi.Case.results.offset
+    assert v[13] == abi.Case.operating_mode.offset
+    assert v[14] == C.sizeof(abi.SceneRow) and v[15] == C.sizeof(abi.Tuning)
 
 
 def test_default_params_match_reference_defaults(lib):

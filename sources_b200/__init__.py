@@ -30,7 +30,8 @@ EXPORTS = ("sphg_default_params", "sphg_create", "sphg_upload_phase", "sphg_sing
            "sphg_time_integration", "sphg_download_phase", "sphg_export_pairs", "sphg_stats",
            "sphg_set_stream", "sphg_kernel_profile", "sphg_kernel_report", "sphg_destroy",
            "sphg_strerror", "sphg_sum_density_noalloc", "sphg_set_scenes", "sphg_upload_scene_ids",
-           "sphg_set_tuning", "sphg_read_case", "sphg_write_tecplot_phase", "sphg_write_tecplot")
+           "sphg_set_tuning", "sphg_read_case", "sphg_write_tecplot_phase", "sphg_write_tecplot",
+           "sphg_gemm_bf16_tn")
 
 _lib = None
 
@@ -71,6 +72,7 @@ def load(path: str = LIB_PATH):
     L.sphg_set_scenes.argtypes = [P, C.c_int, C.POINTER(abi.SceneRow)]
     L.sphg_upload_scene_ids.argtypes = [P, C.c_int, C.POINTER(C.c_int32)]
     L.sphg_set_tuning.argtypes = [P, C.POINTER(abi.Tuning)]
+    L.sphg_gemm_bf16_tn.argtypes = [P, P, P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, P, P]
     L.sphg_read_case.argtypes = [C.c_char_p, C.POINTER(Params), C.POINTER(abi.Case)]
     L.sphg_write_tecplot_phase.argtypes = [C.c_char_p, C.c_int, C.POINTER(PhaseHost), C.POINTER(C.c_int32)]
     L.sphg_write_tecplot.argtypes = [P, C.c_char_p, C.c_char_p, C.c_int, C.POINTER(C.c_int32),

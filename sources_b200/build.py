@@ -15,7 +15,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 SRC = [os.path.join(HERE, "csrc", "sphg_api.cu"), os.path.join(HERE, "csrc", "sphg_noalloc.cu"),
-       os.path.join(HERE, "csrc", "sphg_io.cpp")]
+       os.path.join(HERE, "csrc", "sphg_io.cpp"), os.path.join(HERE, "csrc", "sphg_umma.cu")]
 OUT = os.path.join(HERE, "libsphg.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -29,7 +29,8 @@ def nvcc() -> str:
 
 def sources():
     d = os.path.join(HERE, "csrc")
-    return [os.path.join(d, f) for f in sorted(os.listdir(d))] + [os.path.join(ROOT, "include", "sphg.h")]
+    inc = os.path.join(ROOT, "include")
+    return [os.path.join(d, f) for f in sorted(os.listdir(d))] + [os.path.join(inc, f) for f in sorted(os.listdir(inc))]
 
 
 def up_to_date() -> bool:

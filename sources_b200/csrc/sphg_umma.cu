@@ -1,0 +1,208 @@
+// sphg_umma.cu — BF16 GEMM on the 5th-generation tensor cores (tcgen05) for
+// the learned particle stepper: C[M x N] (+)= A[M x K] * B[N x K]^T, A and B
+// row-major bf16 (K contiguous), C row-major fp32.
+//
+// One CTA of 128 threads computes a 128 x BN tile with UMMA M = 128:
+//   * warp 0 allocates BN (>= 32) TMEM columns for the fp32 accumulator;
+//   * every K block of 64 the CTA stages A (128 x 64) and B (BN x 64) in
+//     shared memory in the canonical no-swizzle K-major layout (8-row x
+//     16-byte core matrices; K halves LBO apart, 8-row groups SBO = 128 B
+//     apart), fences the generic->async proxy, and one thread issues four
+//     K = 16 tcgen05.mma instructions followed by tcgen05.commit to an
+//     mbarrier;
+//   * every wait on that mbarrier is bounded: on timeout the kernel sets
+//     *err, waits (bounded again) for its MMAs, frees TMEM and returns;
+//   * the epilogue reads the accumulator with tcgen05.ld (warp w owns TMEM
+//     lanes 32w..32w+31 = tile rows) and stores, adds to, or atomically adds
+//     into C (split-K over gridDim.z).
+// Shapes: M % 128 == 0, N % BN == 0 with BN in {16, 32, 64, 128, 256},
+// K % 64 == 0, 16-byte aligned rows.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/sphg.h"
+#include "../../include/sphg_learn.h"
+
+namespace {
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// shared-memory matrix descriptor, no swizzle, K-major (version 1 = sm_100)
+__device__ __forceinline__ uint64_t make_desc(uint32_t saddr, uint32_t lbo_bytes, uint32_t sbo_bytes) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+    d |= (uint64_t)((lbo_bytes >> 4) & 0x3FFF) << 16;
+    d |= (uint64_t)((sbo_bytes >> 4) & 0x3FFF) << 32;
+    d |= (uint64_t)1 << 46;          // version
+    // base offset 0, lbo mode 0, layout type 0 (SWIZZLE_NONE)
+    return d;
+}
+
+// instruction descriptor: D fp32, A and B bf16, both K-major, M = 128, N = BN
+__host__ __device__ constexpr uint32_t make_idesc(int n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t parity, long long limit) {
+    for (long long i = 0; i < limit; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred P1;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, P1;\n\t}"
+            : "=r"(done)
+            : "r"(addr), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+constexpr long long kWaitLimit = 1LL << 22;
+
+template <int BN>
+__global__ void __launch_bounds__(128, 1) k_gemm_bf16_tn(const __nv_bfloat16* __restrict__ A,
+                                                         const __nv_bfloat16* __restrict__ B, float* __restrict__ C,
+                                                         int M, int N, int K, int k_per_split, int accumulate,
+                                                         int atomic_out, int* __restrict__ err) {
+    constexpr int TCOLS = BN < 32 ? 32 : BN;
+    constexpr uint32_t A_KC = 128 * 16;     // bytes between K chunks of the A stage
+    constexpr uint32_t B_KC = BN * 16;      // bytes between K chunks of the B stage
+    extern __shared__ __align__(128) uint8_t smem[];
+    uint8_t* sA = smem;
+    uint8_t* sB = smem + 8 * A_KC;
+    uint64_t* mbar = (uint64_t*)(sB + 8 * B_KC);
+    uint32_t* tslot = (uint32_t*)(mbar + 1);
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m0 = blockIdx.x * 128, n0 = blockIdx.y * BN;
+    const int kbeg = blockIdx.z * k_per_split;
+    const int kend = min(K, kbeg + k_per_split);
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                     "r"(TCOLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mbar)), "r"(1));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::);
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::);
+    const uint32_t tmem = *tslot;
+    const uint32_t mbar_a = smem_u32(mbar);
+    const uint32_t idesc = make_idesc(BN);
+
+    bool ok = true;
+    uint32_t parity = 0;
+    int issued = 0;
+    for (int k0 = kbeg; k0 < kend && ok; k0 += 64) {
+        // stage A and B in the canonical K-major layout
+        for (int c = tid; c < 128 * 8; c += 128) {
+            const int r = c >> 3, kc = c & 7;
+            const uint4 v = *reinterpret_cast<const uint4*>(A + (size_t)(m0 + r) * K + k0 + kc * 8);
+            *reinterpret_cast<uint4*>(sA + kc * A_KC + (r >> 3) * 128 + (r & 7) * 16) = v;
+        }
+        for (int c = tid; c < BN * 8; c += 128) {
+            const int r = c >> 3, kc = c & 7;
+            const uint4 v = *reinterpret_cast<const uint4*>(B + (size_t)(n0 + r) * K + k0 + kc * 8);
+            *reinterpret_cast<uint4*>(sB + kc * B_KC + (r >> 3) * 128 + (r & 7) * 16) = v;
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::);
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk) {
+                const uint64_t da = make_desc(smem_u32(sA + kk * 2 * A_KC), A_KC, 128);
+                const uint64_t db = make_desc(smem_u32(sB + kk * 2 * B_KC), B_KC, 128);
+                const uint32_t en = (k0 > kbeg || kk > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+                    ::"r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(en), "r"(0), "r"(0), "r"(0), "r"(0));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                         ::"r"(mbar_a) : "memory");
+        }
+        ++issued;
+        const bool done = mbar_wait(mbar_a, parity, kWaitLimit);
+        parity ^= 1u;
+        ok = __syncthreads_and(done ? 1 : 0) != 0;   // block-uniform: every thread leaves the loop together
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::);
+
+    if (ok && issued > 0) {
+        const int row = m0 + warp * 32 + lane;
+        const uint32_t tbase = tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll 1
+        for (int c = 0; c < BN; c += 8) {
+            uint32_t r[8];
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                           "=r"(r[7])
+                         : "r"(tbase + (uint32_t)c));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            float* out = C + (size_t)row * N + n0 + c;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const float v = __uint_as_float(r[j]);
+                if (atomic_out) atomicAdd(out + j, v);
+                else if (accumulate) out[j] += v;
+                else out[j] = v;
+            }
+        }
+    } else if (!ok) {
+        if (tid == 0) atomicExch(err, 1);
+        // a bounded second wait for MMAs that may still be in flight
+        if (issued > 0) mbar_wait(mbar_a, parity ^ 1u, kWaitLimit);
+    } else if (!accumulate && !atomic_out) {
+        // empty K range: C = 0
+        const int row = m0 + warp * 32 + lane;
+        for (int c = 0; c < BN; ++c) C[(size_t)row * N + n0 + c] = 0.f;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::);
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TCOLS));
+}
+
+template <int BN>
+int launch_gemm(const __nv_bfloat16* A, const __nv_bfloat16* B, float* C, int M, int N, int K, int accumulate,
+                int split, int* err, cudaStream_t s) {
+    const size_t smem = 8 * (128 * 16) + 8 * (BN * 16) + 16 + 16;
+    static bool configured = false;
+    if (!configured) {
+        if (cudaFuncSetAttribute(k_gemm_bf16_tn<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess)
+            return SPHG_ERR_CUDA;
+        configured = true;
+    }
+    const int kblocks = K / 64;
+    const int per = (kblocks + split - 1) / split;
+    dim3 grid(M / 128, N / BN, split);
+    k_gemm_bf16_tn<BN><<<grid, 128, smem, s>>>(A, B, C, M, N, K, per * 64, accumulate, split > 1 ? 1 : 0, err);
+    return cudaGetLastError() == cudaSuccess ? SPHG_OK : SPHG_ERR_CUDA;
+}
+
+}  // namespace
+
+extern "C" int sphg_gemm_bf16_tn(const void* A, const void* B, float* C, int M, int N, int K, int accumulate,
+                                 int split_k, int* err_dev, void* stream) {
+    if (!A || !B || !C || !err_dev) return SPHG_ERR_BAD_ARG;
+    if (M <= 0 || N <= 0 || K <= 0 || M % 128 || N % 16 || K % 64) return SPHG_ERR_BAD_ARG;
+    if ((((uintptr_t)A) | ((uintptr_t)B)) & 15) return SPHG_ERR_BAD_ARG;
+    if (split_k < 1) split_k = 1;
+    if (split_k > K / 64) split_k = K / 64;
+    const __nv_bfloat16* a = (const __nv_bfloat16*)A;
+    const __nv_bfloat16* b = (const __nv_bfloat16*)B;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (N % 128 == 0) return launch_gemm<128>(a, b, C, M, N, K, accumulate, split_k, err_dev, s);
+    if (N % 64 == 0) return launch_gemm<64>(a, b, C, M, N, K, accumulate, split_k, err_dev, s);
+    if (N % 32 == 0) return launch_gemm<32>(a, b, C, M, N, K, accumulate, split_k, err_dev, s);
+    return launch_gemm<16>(a, b, C, M, N, K, accumulate, split_k, err_dev, s);
+}

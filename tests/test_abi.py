@@ -18,9 +18,10 @@ HEADER = os.path.join(ROOT, "include", "sphg.h")
 
 
 def header_functions():
-    txt = open(HEADER).read()
+    inc = os.path.dirname(HEADER)
+    txt = "".join(open(os.path.join(inc, f)).read() for f in sorted(os.listdir(inc)) if f.endswith(".h"))
     txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
-    return sorted(set(re.findall(r"\b(sphg_[a-z_]+)\s*\(", txt)))
+    return sorted(set(re.findall(r"\b(sphg_[a-z0-9_]+)\s*\(", txt)))
 
 
 def test_header_and_python_agree_on_exports():

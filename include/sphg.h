@@ -176,6 +176,15 @@ int sphg_time_integration(sphg_ctx* ctx, int maxtimestep, int* itimestep, double
 /* Copy one phase back into the Fortran arrays (original particle order). */
 int sphg_download_phase(sphg_ctx* ctx, int phase, sphg_phase_host* v);
 
+/* Positions and velocities of one phase (2n doubles each, original particle
+ * order) copied to (export) or from (import) caller DEVICE arrays on the
+ * context's stream, without a host copy or a synchronisation; either
+ * pointer may be NULL.  No counterpart in the reference, whose state lives in
+ * module arrays the host reads directly: the learned stepper uses these to
+ * take rollout snapshots and to hand a stride back to the solver. */
+int sphg_export_xv_device(sphg_ctx* ctx, int phase, double* x_dev, double* v_dev);
+int sphg_import_xv_device(sphg_ctx* ctx, int phase, const double* x_dev, const double* v_dev);
+
 /* Pair list of the last step as 1-based (i,j), sorted by i then j, as
  * direct_find (m_particles.f90:938) / direct_find_2 (:1004) define it.
  * Writes min(n, cap) pairs and the total count to *n. */

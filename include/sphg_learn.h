@@ -7,6 +7,7 @@
 #ifndef SPHG_LEARN_H
 #define SPHG_LEARN_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -20,6 +21,99 @@ extern "C" {
  * device wait that gives up sets *err_dev to 1 (the call still returns). */
 int sphg_gemm_bf16_tn(const void* A, const void* B, float* C, int M, int N, int K, int accumulate, int split_k,
                       int* err_dev, void* cuda_stream);
+
+/* ---------------------------------------------------------------------
+ * Message-passing network kernels.  Feature matrices are row-major bf16 or
+ * fp32 with the row count padded to a multiple of 128; L is the latent
+ * width.  Graphs are CSR by receiver: off[n + 1] (int64), src[e] and dst[e]
+ * (int32), receivers in node order.
+ * ------------------------------------------------------------------- */
+
+#define SPHG_GNN_FEATURES 64 /* padded input width of node and edge rows */
+#define SPHG_GNN_HISTORY 5   /* velocities kept per node */
+
+enum { SPHG_GNN_WATER = 0, SPHG_GNN_SOIL = 1, SPHG_GNN_BOUNDARY = 2 };
+
+/* per-node constants of the learned stepper (32 bytes) */
+typedef struct {
+    float xl, xr, yf;   /* left wall, right wall, floor of the node's scene */
+    float dts;          /* stride length: k solver steps of the scene's dt  */
+    float porosity;     /* scene porosity (0 without a soil-water mixture)  */
+    float phi;          /* scene friction angle (rad), 0 for water scenes   */
+    float mass;
+    int32_t type;       /* SPHG_GNN_WATER / SOIL / BOUNDARY                 */
+} sphg_gnn_node;
+
+/* cell grid of the radius-graph search: cells of side `radius` from
+ * (xmin, ymin), nx * ny of them; positions outside are clamped in */
+typedef struct {
+    double xmin, ymin, radius;
+    int32_t nx, ny;
+} sphg_gnn_grid;
+
+/* scratch bytes of the scans for up to n items (cells or nodes) */
+int sphg_gnn_scan_bytes(int n, size_t* bytes);
+/* radius graph, pass 1: cell list (order[n]: nodes by cell, by index
+ * within a cell; cell_count and cell_start hold nx * ny + 1), degrees
+ * (deg[n + 1]) and off[n + 1] = exclusive scan of the degrees; off[n] is the
+ * edge count, read by the caller to size src and dst */
+int sphg_gnn_graph_count(const sphg_gnn_grid* grid, const double* x, int n, int* order, int* cell_count,
+                         int* cell_start, int* deg, int64_t* off, void* scan_tmp, size_t scan_tmp_bytes,
+                         void* cuda_stream);
+/* radius graph, pass 2: every pair closer than the radius, both
+ * directions, no self edges */
+int sphg_gnn_graph_fill(const sphg_gnn_grid* grid, const double* x, int n, const int* order, const int* cell_start,
+                        const int64_t* off, int* src, int* dst, void* cuda_stream);
+
+/* node rows: 5 velocities (newest first, / vscale), type one-hot, wall
+ * distances / 2h clipped to [0, 1], porosity, friction angle, stride (ms) */
+int sphg_gnn_node_features(const double* x, const float* vhist, int head, const sphg_gnn_node* nodes, int n,
+                           int n_pad, float inv2h, float inv_vscale, void* out_bf16, void* cuda_stream);
+/* edge rows: (x_dst - x_src) / 2h, distance / 2h, same-type flag */
+int sphg_gnn_edge_features(const double* x, const sphg_gnn_node* nodes, const int* src, const int* dst,
+                           long long nedge, long long nedge_pad, double inv2h, void* out_bf16, void* cuda_stream);
+
+int sphg_gnn_f32_to_bf16(const float* x, void* y_bf16, long long n, void* cuda_stream);
+/* z += b (broadcast over rows); h = relu(z) (relu != 0) or z, in bf16 */
+int sphg_gnn_bias_act(float* z, const float* b, void* h_bf16, long long rows, int cols, int relu, void* cuda_stream);
+/* fused edge first layer: z += P[src, :L] + P[dst, L:] + b, a = relu(z) */
+int sphg_gnn_edge_gather_act(float* z, const float* P, const int* src, const int* dst, const float* b, void* a_bf16,
+                             long long nedge, long long nedge_pad, int L, void* cuda_stream);
+int sphg_gnn_relu_bwd(const float* dh, const float* z, float* dz, void* dz_bf16, long long n, void* cuda_stream);
+/* out[c] += sum_r x[r, c] */
+int sphg_gnn_colsum(const float* x, long long rows, int cols, float* out, void* cuda_stream);
+/* out[c, r] = in[r, c] as bf16; in is fp32 (in_is_f32) or bf16 */
+int sphg_gnn_transpose(const void* in, int in_is_f32, void* out_bf16, long long rows, int cols, void* cuda_stream);
+/* agg[n] = scale * sum of e over the edges n receives */
+int sphg_gnn_segsum(const float* e, const int64_t* off, float* agg, int nnode, int L, float scale, void* cuda_stream);
+int sphg_gnn_segsum_bwd(const float* dagg, const int* dst, float* de, long long nedge, int L, float scale,
+                        void* cuda_stream);
+/* dP [nnode x 2L] (sender half zero on entry) from dz of the fused layer */
+int sphg_gnn_gather_bwd(const float* dz, const int* src, const int64_t* off, float* dP, int nnode, long long nedge,
+                        int L, void* cuda_stream);
+/* [h | agg] as bf16 rows of 2L, and its backward (dh += ..., dagg = ...) */
+int sphg_gnn_node_concat(const void* h_bf16, const float* agg, void* out_bf16, long long nnode, int L,
+                         void* cuda_stream);
+int sphg_gnn_node_concat_bwd(const float* d, float* dh, float* dagg, long long nnode, int L, void* cuda_stream);
+/* mean squared error over masked rows, first nout columns; loss += ... */
+int sphg_gnn_mse(const float* pred, int ld, const float* target, int nout, const float* mask, long long rows,
+                 float inv_count, float* dpred, float* loss, void* cuda_stream);
+/* Adam on w [rows x cols]; rows >= row_limit held at zero; refreshes the
+ * bf16 copy w_bf16 and its transpose wt_bf16 [cols x rows] when non-null */
+int sphg_gnn_adam(float* w, const float* g, float* m, float* v, void* w_bf16, void* wt_bf16, int rows, int cols,
+                  float lr, float beta1, float beta2, float eps, int step, int row_limit, void* cuda_stream);
+
+/* learned stride: a = pred[:, :2] * norm[2:4] + norm[0:2]; v' = v + a dts;
+ * x += dts (v + v') / 2 clamped to the walls (margin); v' -> slot head_new */
+int sphg_gnn_stride_update(const float* pred, int ld, const float* norm, const sphg_gnn_node* nodes, double* x,
+                           float* vhist, int head_old, int head_new, int n, double margin, void* cuda_stream);
+/* sigma_i = 1 + sum over received edges of the cubic-spline shape W(r/h) */
+int sphg_gnn_number_density(const double* x, const int64_t* off, const int* src, int n, double h, double* sigma,
+                            void* cuda_stream);
+/* out[4] = {sum (sigma_new/sigma_old - 1)^2, count, kinetic, potential
+ * energy} over the non-boundary nodes */
+int sphg_gnn_gate_sums(const double* sigma_new, const double* sigma_old, const double* x, const float* v_new,
+                       const sphg_gnn_node* nodes, int n, double g, double* out, void* cuda_stream);
 
 #ifdef __cplusplus
 }

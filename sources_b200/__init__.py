@@ -31,7 +31,31 @@ EXPORTS = ("sphg_default_params", "sphg_create", "sphg_upload_phase", "sphg_sing
            "sphg_set_stream", "sphg_kernel_profile", "sphg_kernel_report", "sphg_destroy",
            "sphg_strerror", "sphg_sum_density_noalloc", "sphg_set_scenes", "sphg_upload_scene_ids",
            "sphg_set_tuning", "sphg_read_case", "sphg_write_tecplot_phase", "sphg_write_tecplot",
-           "sphg_gemm_bf16_tn")
+           "sphg_gemm_bf16_tn", "sphg_export_xv_device", "sphg_import_xv_device", *sorted(_GNN_SIGNATURES := {
+               # message-passing network kernels (include/sphg_learn.h); P pointer,
+               # I int, L 64-bit count, F float, D double, S size_t pointer
+               "sphg_gnn_scan_bytes": "IP",
+               "sphg_gnn_graph_count": "PPIPPPPPPLP",
+               "sphg_gnn_graph_fill": "PPIPPPPPP",
+               "sphg_gnn_node_features": "PPIPIIFFPP",
+               "sphg_gnn_edge_features": "PPPPLLDPP",
+               "sphg_gnn_f32_to_bf16": "PPLP",
+               "sphg_gnn_bias_act": "PPPLIIP",
+               "sphg_gnn_edge_gather_act": "PPPPPPLLIP",
+               "sphg_gnn_relu_bwd": "PPPPLP",
+               "sphg_gnn_colsum": "PLIPP",
+               "sphg_gnn_transpose": "PIPLIP",
+               "sphg_gnn_segsum": "PPPIIFP",
+               "sphg_gnn_segsum_bwd": "PPPLIFP",
+               "sphg_gnn_gather_bwd": "PPPPILIP",
+               "sphg_gnn_node_concat": "PPPLIP",
+               "sphg_gnn_node_concat_bwd": "PPPLIP",
+               "sphg_gnn_mse": "PIPIPLFPPP",
+               "sphg_gnn_adam": "PPPPPPIIFFFFIIP",
+               "sphg_gnn_stride_update": "PIPPPPIIIDP",
+               "sphg_gnn_number_density": "PPPIDPP",
+               "sphg_gnn_gate_sums": "PPPPPIDPP",
+           }))
 
 _lib = None
 
@@ -79,6 +103,11 @@ def load(path: str = LIB_PATH):
                                      C.POINTER(C.c_int32)]
     L.sphg_sum_density_noalloc.argtypes = [C.POINTER(Params), C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
                                            C.c_void_p, C.c_void_p, C.c_void_p]
+    L.sphg_export_xv_device.argtypes = [P, C.c_int, P, P]
+    L.sphg_import_xv_device.argtypes = [P, C.c_int, P, P]
+    codes = {"P": C.c_void_p, "I": C.c_int, "L": C.c_longlong, "F": C.c_float, "D": C.c_double}
+    for name, sig in _GNN_SIGNATURES.items():
+        getattr(L, name).argtypes = [codes[c] for c in sig]
     _lib = L
     return L
 
@@ -146,6 +175,16 @@ class Solver:
         _check(self.L.sphg_download_phase(self.h, phase, C.byref(h)), "sphg_download_phase")
         out.nfail = h.nfail
         return out
+
+    def export_xv(self, phase: int, x_dev: int | None, v_dev: int | None):
+        """Positions / velocities (original order) into device arrays given
+        by address, on the context's stream."""
+        _check(self.L.sphg_export_xv_device(self.h, phase, C.c_void_p(x_dev or 0), C.c_void_p(v_dev or 0)),
+               "sphg_export_xv_device")
+
+    def import_xv(self, phase: int, x_dev: int | None, v_dev: int | None):
+        _check(self.L.sphg_import_xv_device(self.h, phase, C.c_void_p(x_dev or 0), C.c_void_p(v_dev or 0)),
+               "sphg_import_xv_device")
 
     def pairs(self, which: int):
         n = C.c_int64()

@@ -66,6 +66,7 @@ struct EngineBase {
     virtual int set_scenes(int nscenes, const sphg_scene* sc) = 0;
     virtual int upload_scene_ids(int phase, const int32_t* ids) = 0;
     virtual int set_tuning(const sphg_tuning* t) = 0;
+    virtual int xv_device(int phase, double* x, double* v, int to_caller) = 0;
 };
 
 struct sphg_ctx {
@@ -654,6 +655,29 @@ struct Engine : EngineBase {
         return 0;
     }
 
+    // positions and velocities between the state and caller device arrays in
+    // original order, on the context's stream (no host copy, no sync)
+    int xv_device(int phase, double* x, double* v, int to_caller) override {
+        if (phase < 1 || phase > ctx->nphase) return SPHG_ERR_BAD_ARG;
+        int ph = phase - 1;
+        if (!have[ph]) return SPHG_ERR_STATE;
+        PhaseDev<T>& D = P[ph];
+        const int n = D.n;
+        double* state[2] = {(double*)D.x, (double*)D.v};
+        double* user[2] = {x, v};
+        int rc = 0;
+        for (int f = 0; f < 2; ++f) {
+            if (!user[f]) continue;
+            if (to_caller)
+                rc |= launch("xv_device", k_to_original<double>, blocks(n, 256), 256, n, (const int*)D.orig,
+                             (const double*)state[f], user[f], 2);
+            else
+                rc |= launch("xv_device", k_from_original<double>, blocks(n, 256), 256, n, (const int*)D.orig,
+                             (const double*)user[f], state[f], 2);
+        }
+        return rc ? SPHG_ERR_CUDA : SPHG_OK;
+    }
+
     int download(int phase, sphg_phase_host* h) override {
         if (phase < 1 || phase > ctx->nphase || !h) return SPHG_ERR_BAD_ARG;
         int ph = phase - 1;
@@ -922,6 +946,18 @@ int sphg_download_phase(sphg_ctx* c, int phase, sphg_phase_host* v) {
     if (!c) return SPHG_ERR_BAD_ARG;
     cudaSetDevice(c->device);
     return c->eng->download(phase, v);
+}
+
+int sphg_export_xv_device(sphg_ctx* c, int phase, double* x_dev, double* v_dev) {
+    if (!c) return SPHG_ERR_BAD_ARG;
+    cudaSetDevice(c->device);
+    return c->eng->xv_device(phase, x_dev, v_dev, 1);
+}
+
+int sphg_import_xv_device(sphg_ctx* c, int phase, const double* x_dev, const double* v_dev) {
+    if (!c) return SPHG_ERR_BAD_ARG;
+    cudaSetDevice(c->device);
+    return c->eng->xv_device(phase, (double*)x_dev, (double*)v_dev, 0);
 }
 
 int sphg_export_pairs(sphg_ctx* c, int which, int32_t* pi, int32_t* pj, int64_t cap, int64_t* n) {

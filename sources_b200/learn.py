@@ -1,0 +1,832 @@
+"""Learned particle stepper: a message-passing network over the particles
+that predicts each particle's mean acceleration over a stride of k solver
+steps, trained on rollouts of the batched SPH solver, with the plain SPH
+step as its fallback and as the judge of its error.  The reference has no
+counterpart: its step is the SPH solver alone.
+
+Everything numeric runs in libsphg's own CUDA kernels (include/sphg_learn.h):
+the dense layers on the tcgen05 BF16 GEMM (fp32 accumulation in TMEM), the
+graph search, features, gathers, scatters, segment sums, loss, Adam and the
+stride update in sphg_gnn.cu.  PyTorch only allocates device memory, copies
+buffers and assembles training batches (indexing and noise).
+
+Network (latent width L = 128, 4 message-passing layers, 2-layer MLPs):
+    node inputs  5 velocities (newest first), type one-hot (water, soil,
+                 boundary), wall distances / 2h clipped to [0, 1], porosity,
+                 friction angle, stride length   (19 of 64 padded columns)
+    edge inputs  (x_receiver - x_sender) / 2h, distance / 2h, same-type flag
+    edges        every pair closer than 2h, both directions
+    encoder      2-layer MLPs to L for nodes and edges
+    layer        z = e We^T + h[src] Ws^T + h[dst] Wd^T + be   (the [e, h_src,
+                 h_dst] input of the edge MLP, with the node projections
+                 computed once per node and gathered per edge);
+                 e += relu(z) W2^T + b2;  agg = sum of e over received edges / 16;
+                 h += relu([h, agg] V1^T + c1) V2^T + c2
+    decoder      2-layer MLP to the 2 acceleration components (normalised)
+Stride update (k = 10 solver steps of the scene's dt): v' = v + a k dt,
+x' = x + k dt (v + v') / 2, clamped inside the walls.  Fallback gates: the
+RMS relative change of the SPH number density over real particles above
+1 %, or a rise of kinetic + potential energy above 5 % of (kinetic energy +
+one dx of potential energy per particle); a failed stride is redone by k
+plain SPH steps.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import SPHError, load
+from .abi import SPHG_SOIL, SPHG_WATER
+
+L_WIDTH = 128
+F_IN = 64
+LAYERS = 4
+AGG_SCALE = 1.0 / 16.0
+NOUT = 2
+K_STRIDE = 10
+HIST = 5
+GRAVITY = -9.800000190734863     # the solver's default gravity (single-precision -9.8)
+GATE_DENSITY = 0.01
+GATE_ENERGY = 0.05
+
+GNN_WATER, GNN_SOIL, GNN_BOUNDARY = 0, 1, 2
+NODE_DTYPE = np.dtype([("xl", "<f4"), ("xr", "<f4"), ("yf", "<f4"), ("dts", "<f4"), ("porosity", "<f4"),
+                       ("phi", "<f4"), ("mass", "<f4"), ("type", "<i4")])
+
+
+class Grid(C.Structure):
+    _fields_ = [("xmin", C.c_double), ("ymin", C.c_double), ("radius", C.c_double), ("nx", C.c_int32),
+                ("ny", C.c_int32)]
+
+
+def pad128(n: int) -> int:
+    return max(128, (n + 127) // 128 * 128)
+
+
+def weight_specs():
+    """[(name, rows, cols, row_limit)] of the weights, [(name, size, limit)] of the biases."""
+    L, F = L_WIDTH, F_IN
+    W = [("enc_n.w1", L, F), ("enc_n.w2", L, L), ("enc_e.w1", L, F), ("enc_e.w2", L, L)]
+    B = ["enc_n.b1", "enc_n.b2", "enc_e.b1", "enc_e.b2"]
+    for l in range(LAYERS):
+        W += [(f"p{l}.we", L, L), (f"p{l}.wsd", 2 * L, L), (f"p{l}.w2", L, L), (f"p{l}.v1", L, 2 * L),
+              (f"p{l}.v2", L, L)]
+        B += [f"p{l}.be", f"p{l}.b2", f"p{l}.c1", f"p{l}.c2"]
+    W += [("dec.w1", L, L), ("dec.w2", L, L)]
+    B += ["dec.b1", "dec.b2"]
+    lim = {"dec.w2": NOUT, "dec.b2": NOUT}
+    return ([(n, r, c, lim.get(n, r)) for n, r, c in W], [(n, L, lim.get(n, L)) for n in B])
+
+
+def init_weights(seed: int = 0) -> dict:
+    """Uniform(-1/sqrt(fan_in), 1/sqrt(fan_in)) weights, zero biases (PCG64 seed)."""
+    g = np.random.Generator(np.random.PCG64(seed))
+    out = {}
+    Ws, Bs = weight_specs()
+    for name, r, c, lim in Ws:
+        a = 1.0 / math.sqrt(c)
+        w = g.uniform(-a, a, size=(r, c)).astype(np.float32)
+        w[lim:] = 0.0
+        out[name] = w
+    for name, r, lim in Bs:
+        out[name] = np.zeros(r, np.float32)
+    return out
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _ptr(t) -> int:
+    return 0 if t is None else t.data_ptr()
+
+
+def _call(rc: int, what: str):
+    if rc != 0:
+        raise SPHError(rc, what)
+
+
+class _Buffers:
+    """Grow-only named device buffers; new memory is zeroed, so every view
+    holds finite values."""
+
+    def __init__(self, device):
+        self.torch = _torch()
+        self.device = device
+        self.buf = {}
+
+    def get(self, name, shape, dtype, zero=False):
+        numel = int(np.prod(shape))
+        t = self.buf.get(name)
+        if t is None or t.numel() < numel:
+            t = self.torch.zeros(max(numel, 1), dtype=dtype, device=self.device)
+            self.buf[name] = t
+        v = t[:numel].view(*shape)
+        if zero:
+            v.zero_()
+        return v
+
+
+@dataclass
+class Batch:
+    """One graph on the device: n nodes (rows padded to n_pad), E edges."""
+    n: int
+    n_pad: int
+    E: int
+    E_pad: int
+    x: object            # [n, 2] f64
+    nodes: object        # [n, 32] uint8 (NODE_DTYPE rows)
+    off: object          # [n + 1] int64
+    src: object          # [E] int32
+    dst: object
+    fn: object           # [n_pad, 64] bf16
+    fe: object           # [E_pad, 64] bf16
+    target: object = None
+    mask: object = None
+    n_real: int = 0
+
+
+class GraphBuilder:
+    """Radius graph of the particles on the device (sphg_gnn_graph_count /
+    _fill): the edge count is read back once to size the edge arrays."""
+
+    def __init__(self, lib, bufs: _Buffers, prefix="g"):
+        self.L, self.b, self.p = lib, bufs, prefix
+        self.torch = bufs.torch
+
+    def build(self, x, n: int, grid: Grid, stream: int):
+        t = self.torch
+        ncell = grid.nx * grid.ny
+        nbytes = C.c_size_t()
+        _call(self.L.sphg_gnn_scan_bytes(max(ncell, n), C.byref(nbytes)), "sphg_gnn_scan_bytes")
+        tmp = self.b.get(self.p + ".tmp", (nbytes.value + 16,), t.uint8)
+        order = self.b.get(self.p + ".order", (n,), t.int32)
+        cc = self.b.get(self.p + ".cc", (ncell + 1,), t.int32)
+        cs = self.b.get(self.p + ".cs", (ncell + 1,), t.int32)
+        deg = self.b.get(self.p + ".deg", (n + 1,), t.int32)
+        off = self.b.get(self.p + ".off", (n + 1,), t.int64)
+        _call(self.L.sphg_gnn_graph_count(C.byref(grid), _ptr(x), n, _ptr(order), _ptr(cc), _ptr(cs), _ptr(deg),
+                                          _ptr(off), _ptr(tmp), nbytes.value, stream), "sphg_gnn_graph_count")
+        E = int(off[n].item())
+        if E < 0 or E >= 2 ** 31 - 1:
+            raise SPHError(4, "graph edge count out of range")
+        src = self.b.get(self.p + ".src", (max(E, 1),), t.int32)
+        dst = self.b.get(self.p + ".dst", (max(E, 1),), t.int32)
+        _call(self.L.sphg_gnn_graph_fill(C.byref(grid), _ptr(x), n, _ptr(order), _ptr(cs), _ptr(off), _ptr(src),
+                                         _ptr(dst), stream), "sphg_gnn_graph_fill")
+        return off, src, dst, E
+
+
+class MPNet:
+    """The message-passing network with its device weights, Adam state and
+    activation buffers; forward/backward call libsphg kernels only."""
+
+    def __init__(self, weights: dict | None = None, seed: int = 0, device="cuda"):
+        self.torch = t = _torch()
+        self.L = load()
+        self.device = t.device(device)
+        self.bufs = _Buffers(self.device)
+        self.graph = GraphBuilder(self.L, self.bufs)
+        w = weights if weights is not None else init_weights(seed)
+        self.W, self.B = {}, {}
+        Ws, Bs = weight_specs()
+        for name, r, c, lim in Ws:
+            m = t.from_numpy(np.ascontiguousarray(w[name], dtype=np.float32)).to(self.device)
+            self.W[name] = dict(w=m, wb=m.to(t.bfloat16), wt=m.t().contiguous().to(t.bfloat16), g=t.zeros_like(m),
+                                m=t.zeros_like(m), v=t.zeros_like(m), rows=r, cols=c, lim=lim)
+        for name, r, lim in Bs:
+            m = t.from_numpy(np.ascontiguousarray(w[name], dtype=np.float32)).to(self.device)
+            self.B[name] = dict(w=m, g=t.zeros_like(m), m=t.zeros_like(m), v=t.zeros_like(m), rows=r, lim=lim)
+        self.err = t.zeros(1, dtype=t.int32, device=self.device)
+        self.loss_buf = t.zeros(1, dtype=t.float32, device=self.device)
+        self.adam_step = 0
+        # normalisation: velocity scale, acceleration mean (2) and std (2)
+        self.vscale = 1.0
+        self.norm = t.tensor([0.0, 0.0, 1.0, 1.0], dtype=t.float32, device=self.device)
+        self.launches = 0
+
+    # ------------------------------------------------------------ plumbing
+    @property
+    def stream(self) -> int:
+        return self.torch.cuda.current_stream(self.device).cuda_stream
+
+    def weights(self) -> dict:
+        out = {k: v["w"].cpu().numpy().copy() for k, v in self.W.items()}
+        out.update({k: v["w"].cpu().numpy().copy() for k, v in self.B.items()})
+        return out
+
+    def state(self) -> dict:
+        d = self.weights()
+        d["_vscale"] = np.array([self.vscale], np.float64)
+        d["_norm"] = self.norm.cpu().numpy()
+        return d
+
+    @classmethod
+    def from_state(cls, d: dict, device="cuda"):
+        net = cls({k: v for k, v in d.items() if not k.startswith("_")}, device=device)
+        net.vscale = float(d["_vscale"][0])
+        net.norm.copy_(net.torch.from_numpy(np.asarray(d["_norm"], np.float32)))
+        return net
+
+    def _gemm(self, A, B, Cm, M, N, K, acc=0, split=1):
+        self.launches += 1
+        _call(self.L.sphg_gemm_bf16_tn(_ptr(A), _ptr(B), _ptr(Cm), M, N, K, acc, split, _ptr(self.err), self.stream),
+              "sphg_gemm_bf16_tn")
+
+    @staticmethod
+    def _split(M, N, K):
+        bn = 128 if N % 128 == 0 else 64 if N % 64 == 0 else 32 if N % 32 == 0 else 16
+        tiles = (M // 128) * (N // bn)
+        return max(1, min(K // 64 // 2, (2 * 148) // max(tiles, 1)))
+
+    def _lin(self, X, name, Y, rows):
+        w = self.W[name]
+        self._gemm(X, w["wb"], Y, rows, w["rows"], w["cols"])
+
+    def _k(self, fn, *args):
+        self.launches += 1
+        _call(getattr(self.L, fn)(*args), fn)
+
+    def _bias_act(self, z, bname, hb, rows, relu):
+        self._k("sphg_gnn_bias_act", _ptr(z), _ptr(self.B[bname]["w"]), _ptr(hb), rows, z.shape[1], relu,
+                self.stream)
+
+    def _wgrad(self, dY, X, name, rows):
+        """W.g += dY^T X through two transposes and one split-K GEMM."""
+        t = self.torch
+        w = self.W[name]
+        out, inn = w["rows"], w["cols"]
+        tA = self.bufs.get("tA", (out, rows), t.bfloat16)
+        tB = self.bufs.get("tB", (inn, rows), t.bfloat16)
+        self._k("sphg_gnn_transpose", _ptr(dY), 1 if dY.dtype == t.float32 else 0, _ptr(tA), rows, out, self.stream)
+        self._k("sphg_gnn_transpose", _ptr(X), 1 if X.dtype == t.float32 else 0, _ptr(tB), rows, inn, self.stream)
+        self._gemm(tA, tB, w["g"], out, inn, rows, acc=1, split=self._split(out, inn, rows))
+
+    def _bgrad(self, dY, bname, rows):
+        self._k("sphg_gnn_colsum", _ptr(dY), rows, dY.shape[1], _ptr(self.B[bname]["g"]), self.stream)
+
+    def _bf16(self, x, name):
+        t = self.torch
+        y = self.bufs.get(name, tuple(x.shape), t.bfloat16)
+        self._k("sphg_gnn_f32_to_bf16", _ptr(x), _ptr(y), x.numel(), self.stream)
+        return y
+
+    # ------------------------------------------------------------- forward
+    def forward(self, b: Batch, keep: bool):
+        """Network output [n_pad, L] (columns 0, 1 = normalised acceleration)."""
+        t, L, G = self.torch, L_WIDTH, self.bufs.get
+        f32, bf = t.float32, t.bfloat16
+        Np, Ep = b.n_pad, b.E_pad
+        s = self.stream
+        tag = (lambda l: str(l)) if keep else (lambda l: "0")
+        nz = G("nz", (Np, L), f32)
+        na = G("na", (Np, L), bf)
+        self._lin(b.fn, "enc_n.w1", nz, Np)
+        self._bias_act(nz, "enc_n.b1", na, Np, 1)
+        hf = G("hf", (Np, L), f32)
+        hb = G("hb" + tag(0), (Np, L), bf)
+        self._lin(na, "enc_n.w2", hf, Np)
+        self._bias_act(hf, "enc_n.b2", hb, Np, 0)
+        ez = G("ez", (Ep, L), f32)
+        ea = G("ea", (Ep, L), bf)
+        self._lin(b.fe, "enc_e.w1", ez, Ep)
+        self._bias_act(ez, "enc_e.b1", ea, Ep, 1)
+        ef = G("ef", (Ep, L), f32)
+        eb = G("eb" + tag(0), (Ep, L), bf)
+        self._lin(ea, "enc_e.w2", ef, Ep)
+        self._bias_act(ef, "enc_e.b2", eb, Ep, 0)
+        P = G("P", (Np, 2 * L), f32)
+        agg = G("agg", (Np, L), f32)
+        for l in range(LAYERS):
+            p = f"p{l}."
+            z = G("z" + tag(l), (Ep, L), f32)
+            a = G("a" + tag(l), (Ep, L), bf)
+            self._lin(hb, p + "wsd", P, Np)
+            self._lin(eb, p + "we", z, Ep)
+            self._k("sphg_gnn_edge_gather_act", _ptr(z), _ptr(P), _ptr(b.src), _ptr(b.dst),
+                    _ptr(self.B[p + "be"]["w"]), _ptr(a), b.E, Ep, L, s)
+            self._gemm(a, self.W[p + "w2"]["wb"], ef, Ep, L, L, acc=1)         # residual: e += relu(z) W2^T
+            eb = G("eb" + tag(l + 1), (Ep, L), bf)
+            self._bias_act(ef, p + "b2", eb, Ep, 0)
+            self._k("sphg_gnn_segsum", _ptr(ef), _ptr(b.off), _ptr(agg), b.n, L, AGG_SCALE, s)
+            cat = G("cat" + tag(l), (Np, 2 * L), bf)
+            self._k("sphg_gnn_node_concat", _ptr(hb), _ptr(agg), _ptr(cat), Np, L, s)
+            y = G("y" + tag(l), (Np, L), f32)
+            ya = G("ya" + tag(l), (Np, L), bf)
+            self._lin(cat, p + "v1", y, Np)
+            self._bias_act(y, p + "c1", ya, Np, 1)
+            self._gemm(ya, self.W[p + "v2"]["wb"], hf, Np, L, L, acc=1)        # residual: h += relu(y) V2^T
+            hb = G("hb" + tag(l + 1), (Np, L), bf)
+            self._bias_act(hf, p + "c2", hb, Np, 0)
+        du = G("du", (Np, L), f32)
+        dua = G("dua", (Np, L), bf)
+        self._lin(hb, "dec.w1", du, Np)
+        self._bias_act(du, "dec.b1", dua, Np, 1)
+        out = G("out", (Np, L), f32)
+        outb = G("outb", (Np, L), bf)
+        self._lin(dua, "dec.w2", out, Np)
+        self._bias_act(out, "dec.b2", outb, Np, 0)
+        return out
+
+    # ------------------------------------------------------------ backward
+    def zero_grad(self):
+        for d in list(self.W.values()) + list(self.B.values()):
+            d["g"].zero_()
+
+    def loss(self, b: Batch, out):
+        """Masked MSE over the 2 acceleration columns; returns d loss / d out."""
+        t = self.torch
+        dout = self.bufs.get("dout", (b.n_pad, L_WIDTH), t.float32)
+        self.loss_buf.zero_()
+        self._k("sphg_gnn_mse", _ptr(out), L_WIDTH, _ptr(b.target), NOUT, _ptr(b.mask), b.n_pad,
+                1.0 / (NOUT * max(b.n_real, 1)), _ptr(dout), _ptr(self.loss_buf), self.stream)
+        return dout
+
+    def backward(self, b: Batch, dout, trace: dict | None = None):
+        """Gradients into W[.]["g"] / B[.]["g"]; with a trace dict, copies of the
+        incoming node and edge gradients of every layer (and of the encoders)
+        are kept for a stage-by-stage check."""
+        t, L, G = self.torch, L_WIDTH, self.bufs.get
+        f32, bf = t.float32, t.bfloat16
+        Np, Ep = b.n_pad, b.E_pad
+        s = self.stream
+        # decoder
+        self._bgrad(dout, "dec.b2", Np)
+        self._wgrad(dout, G("dua", (Np, L), bf), "dec.w2", Np)
+        tmpN = G("tmpN", (Np, L), f32)
+        self._gemm(self._bf16(dout, "doutb"), self.W["dec.w2"]["wt"], tmpN, Np, L, L)
+        dy = G("dy", (Np, L), f32)
+        dyb = G("dyb", (Np, L), bf)
+        self._k("sphg_gnn_relu_bwd", _ptr(tmpN), _ptr(G("du", (Np, L), f32)), _ptr(dy), _ptr(dyb), Np * L, s)
+        self._bgrad(dy, "dec.b1", Np)
+        self._wgrad(dy, G(f"hb{LAYERS}", (Np, L), bf), "dec.w1", Np)
+        dh = G("dh", (Np, L), f32)
+        self._gemm(dyb, self.W["dec.w1"]["wt"], dh, Np, L, L)
+        de = G("de", (Ep, L), f32, zero=True)
+        dcat = G("dcat", (Np, 2 * L), f32)
+        dagg = G("dagg", (Np, L), f32)
+        da = G("da", (Ep, L), f32)
+        dz = G("dz", (Ep, L), f32)
+        dzb = G("dzb", (Ep, L), bf)
+        dP = G("dP", (Np, 2 * L), f32)
+        for l in reversed(range(LAYERS)):
+            p = f"p{l}."
+            if trace is not None:
+                trace[l] = (dh.clone(), de.clone())
+            hb, eb = G(f"hb{l}", (Np, L), bf), G(f"eb{l}", (Ep, L), bf)
+            z, a = G(f"z{l}", (Ep, L), f32), G(f"a{l}", (Ep, L), bf)
+            y, ya, cat = G(f"y{l}", (Np, L), f32), G(f"ya{l}", (Np, L), bf), G(f"cat{l}", (Np, 2 * L), bf)
+            # node update h' = h + relu(y) V2^T + c2
+            self._bgrad(dh, p + "c2", Np)
+            self._wgrad(dh, ya, p + "v2", Np)
+            self._gemm(self._bf16(dh, "dhb"), self.W[p + "v2"]["wt"], tmpN, Np, L, L)
+            self._k("sphg_gnn_relu_bwd", _ptr(tmpN), _ptr(y), _ptr(dy), _ptr(dyb), Np * L, s)
+            self._bgrad(dy, p + "c1", Np)
+            self._wgrad(dy, cat, p + "v1", Np)
+            self._gemm(dyb, self.W[p + "v1"]["wt"], dcat, Np, 2 * L, L)
+            self._k("sphg_gnn_node_concat_bwd", _ptr(dcat), _ptr(dh), _ptr(dagg), b.n, L, s)
+            self._k("sphg_gnn_segsum_bwd", _ptr(dagg), _ptr(b.dst), _ptr(de), b.E, L, AGG_SCALE, s)
+            # edge update e' = e + relu(z) W2^T + b2
+            self._bgrad(de, p + "b2", Ep)
+            self._wgrad(de, a, p + "w2", Ep)
+            self._gemm(self._bf16(de, "deb"), self.W[p + "w2"]["wt"], da, Ep, L, L)
+            self._k("sphg_gnn_relu_bwd", _ptr(da), _ptr(z), _ptr(dz), _ptr(dzb), Ep * L, s)
+            self._bgrad(dz, p + "be", Ep)
+            self._wgrad(dz, eb, p + "we", Ep)
+            self._gemm(dzb, self.W[p + "we"]["wt"], de, Ep, L, L, acc=1)
+            dP.zero_()
+            self._k("sphg_gnn_gather_bwd", _ptr(dz), _ptr(b.src), _ptr(b.off), _ptr(dP), b.n, b.E, L, s)
+            self._wgrad(dP, hb, p + "wsd", Np)
+            self._gemm(self._bf16(dP, "dPb"), self.W[p + "wsd"]["wt"], dh, Np, L, 2 * L, acc=1)
+        if trace is not None:
+            trace["enc"] = (dh.clone(), de.clone())
+        # encoders
+        for side, d, rows, feat in (("n", dh, Np, b.fn), ("e", de, Ep, b.fe)):
+            enc = "enc_" + side
+            zbuf = G(side + "z", (rows, L), f32)
+            abuf = G(side + "a", (rows, L), bf)
+            tmp = G("tmp" + side, (rows, L), f32)
+            self._bgrad(d, enc + ".b2", rows)
+            self._wgrad(d, abuf, enc + ".w2", rows)
+            self._gemm(self._bf16(d, "d" + side + "b"), self.W[enc + ".w2"]["wt"], tmp, rows, L, L)
+            dzz = G("dzz" + side, (rows, L), f32)
+            dzzb = G("dzzb" + side, (rows, L), bf)
+            self._k("sphg_gnn_relu_bwd", _ptr(tmp), _ptr(zbuf), _ptr(dzz), _ptr(dzzb), rows * L, s)
+            self._bgrad(dzz, enc + ".b1", rows)
+            self._wgrad(dzz, feat, enc + ".w1", rows)
+
+    def adam(self, lr: float, b1=0.9, b2=0.999, eps=1e-8):
+        self.adam_step += 1
+        s = self.stream
+        for d in self.W.values():
+            self._k("sphg_gnn_adam", _ptr(d["w"]), _ptr(d["g"]), _ptr(d["m"]), _ptr(d["v"]), _ptr(d["wb"]),
+                    _ptr(d["wt"]), d["rows"], d["cols"], lr, b1, b2, eps, self.adam_step, d["lim"], s)
+        for d in self.B.values():
+            self._k("sphg_gnn_adam", _ptr(d["w"]), _ptr(d["g"]), _ptr(d["m"]), _ptr(d["v"]), None, None,
+                    d["rows"], 1, lr, b1, b2, eps, self.adam_step, d["lim"], s)
+
+    def check_device_errors(self):
+        if int(self.err.item()) != 0:
+            raise SPHError(6, "tcgen05 GEMM wait timed out")
+
+    # --------------------------------------------------------------- batch
+    def make_batch(self, x, nodes, vhist, head: int, grid: Grid, inv2h: float, target=None) -> Batch:
+        """Graph, node and edge features of the particles x [n, 2] (f64,
+        device) with velocity history vhist [5, n, 2] (f32) at ring slot head."""
+        t = self.torch
+        n = x.shape[0]
+        off, src, dst, E = self.graph.build(x, n, grid, self.stream)
+        Np, Ep = pad128(n), pad128(E)
+        fn = self.bufs.get("fn", (Np, F_IN), t.bfloat16)
+        fe = self.bufs.get("fe", (Ep, F_IN), t.bfloat16)
+        self._k("sphg_gnn_node_features", _ptr(x), _ptr(vhist), head, _ptr(nodes), n, Np, inv2h,
+                1.0 / self.vscale, _ptr(fn), self.stream)
+        self._k("sphg_gnn_edge_features", _ptr(x), _ptr(nodes), _ptr(src), _ptr(dst), E, Ep, float(inv2h),
+                _ptr(fe), self.stream)
+        b = Batch(n, Np, E, Ep, x, nodes, off, src, dst, fn, fe)
+        if target is not None:
+            b.target = self.bufs.get("target", (Np, NOUT), t.float32)
+            b.target[:n] = target
+            b.mask = self.bufs.get("mask", (Np,), t.float32, zero=True)
+            typ = nodes.view(t.int32)[:, 7]
+            b.mask[:n] = (typ != GNN_BOUNDARY).to(t.float32)
+            b.n_real = int((typ != GNN_BOUNDARY).sum().item())
+        return b
+
+    def train_step(self, b: Batch, lr: float) -> float:
+        self.zero_grad()
+        out = self.forward(b, keep=True)
+        dout = self.loss(b, out)
+        self.backward(b, dout)
+        self.adam(lr)
+        return float(self.loss_buf.item())
+
+
+# ---------------------------------------------------------------- rollouts
+
+def node_table(scene, offset: float, dts: float, kind: str) -> np.ndarray:
+    """Per-particle constants of one scene (all phases, in phase order)."""
+    rows = []
+    xl, xr, yf = scene.box
+    p = scene.params
+    porosity = p.soil.porosity if kind == "submerged" else 0.0
+    phi = p.soil.phi if kind in ("dry", "submerged") else 0.0
+    for P in scene.phases:
+        a = np.zeros(P.n, NODE_DTYPE)
+        a["xl"], a["xr"], a["yf"] = xl + offset, xr + offset, yf
+        a["dts"], a["porosity"], a["phi"] = dts, porosity, phi
+        a["mass"] = P.mass
+        real = np.asarray(P.itype) > 0
+        a["type"] = np.where(real, GNN_WATER if P.material == SPHG_WATER else GNN_SOIL, GNN_BOUNDARY)
+        rows.append(a)
+    return np.concatenate(rows)
+
+
+@dataclass
+class GroupRollout:
+    """Snapshots every k steps of one ensemble group (all phases, phase order)."""
+    kind: str
+    nodes: np.ndarray            # NODE_DTYPE [n]
+    X: object                    # [T, n, 2] f64 device
+    V: object                    # [T, n, 2] f32 device
+    scene_idx: list              # per member: int64 device index of its nodes
+    members: list                # ensemble scene indices
+    grid: Grid
+    inv2h: float
+    h: float
+    dx: float
+    plain_ms: float = 0.0        # device time of the plain solver per step
+    boxes: list = field(default_factory=list)
+    scene_idx_np: list = field(default_factory=list)
+    nodes_dev: object = None     # [n, 32] uint8
+    typ_dev: object = None       # [n] int32
+    dts_dev: object = None       # [n] f32
+
+    def finish(self, torch, device):
+        self.scene_idx_np = [i.cpu().numpy() for i in self.scene_idx]
+        self.nodes_dev = torch.from_numpy(self.nodes.view(np.uint8).reshape(-1, 32).copy()).to(device)
+        self.typ_dev = torch.from_numpy(self.nodes["type"].copy()).to(device)
+        self.dts_dev = torch.from_numpy(self.nodes["dts"].copy()).to(device)
+        return self
+
+
+def _group_grid(g, radius: float) -> Grid:
+    p = g.scene.params
+    xmin, ymin = p.x_min - 4 * radius, p.y_min - 4 * radius
+    nx = int(math.ceil((p.x_max + 4 * radius - xmin) / radius)) + 1
+    ny = int(math.ceil((p.y_max + 4 * radius - ymin) / radius)) + 1
+    return Grid(xmin, ymin, radius, nx, ny)
+
+
+def _group_nodes(ens, g):
+    parts = [[] for _ in g.scene.phases]
+    for local, m in enumerate(g.members):
+        sc = ens.built[m]
+        dts = K_STRIDE * g.rows[local][0]
+        tab = node_table(sc, g.offsets[local], dts, g.kind)
+        a = 0
+        for k, P in enumerate(sc.phases):
+            parts[k].append(tab[a:a + P.n])
+            a += P.n
+    return np.concatenate([np.concatenate(p) for p in parts])
+
+
+def _scene_index(g, torch, device):
+    idx = []
+    base = np.cumsum([0] + [P.n for P in g.scene.phases])
+    for local in range(len(g.members)):
+        parts = [np.arange(base[k] + a, base[k] + b) for k, (a, b) in
+                 ((k, g.ranges[k][local]) for k in range(len(g.scene.phases)))]
+        idx.append(torch.from_numpy(np.concatenate(parts).astype(np.int64)).to(device))
+    return idx
+
+
+def rollout_ensemble(ens, strides: int, device="cuda"):
+    """Run every group of an Ensemble for `strides` strides of k steps and
+    keep x (f64) and v (f32) of every particle after each stride (T =
+    strides + 1 snapshots, the first the initial state)."""
+    torch = _torch()
+    dev = torch.device(device)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    ens.set_stream(stream)
+    out = []
+    for g, sv in zip(ens.groups, ens.solvers):
+        n_ph = [P.n for P in g.scene.phases]
+        n = sum(n_ph)
+        X = torch.empty((strides + 1, n, 2), dtype=torch.float64, device=dev)
+        V = torch.empty((strides + 1, n, 2), dtype=torch.float32, device=dev)
+        vtmp = torch.empty((n, 2), dtype=torch.float64, device=dev)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        steps_ms = 0.0
+        for t in range(strides + 1):
+            if t:
+                ev0.record()
+                sv.time_integration(K_STRIDE)
+                ev1.record()
+                ev1.synchronize()
+                steps_ms += ev0.elapsed_time(ev1)
+            a = 0
+            for k, nk in enumerate(n_ph):
+                sv.export_xv(k + 1, X[t, a:a + nk].data_ptr(), vtmp[a:a + nk].data_ptr())
+                a += nk
+            V[t].copy_(vtmp)
+        h = float(g.scene.phases[0].hsml[0])
+        dx = float(g.scene.phases[0].dspp)
+        r = GroupRollout(g.kind, _group_nodes(ens, g), X, V, _scene_index(g, torch, dev), list(g.members),
+                         _group_grid(g, 2.0 * h), 1.0 / (2.0 * h), h, dx,
+                         steps_ms / max(strides * K_STRIDE, 1))
+        r.boxes = [ens.built[m].box for m in g.members]
+        out.append(r.finish(torch, dev))
+    torch.cuda.synchronize(dev)
+    return out
+
+
+def normalisation(rollouts, t0: int = HIST - 1):
+    """Velocity scale and per-component acceleration mean / std over real
+    particles of the training rollouts."""
+    torch = _torch()
+    vs, acc = [], []
+    for r in rollouts:
+        typ = torch.from_numpy(r.nodes["type"].copy()).to(r.V.device)
+        real = typ != GNN_BOUNDARY
+        dts = torch.from_numpy(r.nodes["dts"].copy()).to(r.V.device)[real]
+        V = r.V[:, real]
+        vs.append(V[t0:].reshape(-1, 2).double())
+        acc.append(((V[t0 + 1:] - V[t0:-1]) / dts[None, :, None]).reshape(-1, 2).double())
+    v = torch.cat(vs)
+    a = torch.cat(acc)
+    vscale = float(v.std().item()) or 1.0
+    return vscale, [float(a[:, 0].mean()), float(a[:, 1].mean()), float(a[:, 0].std()) or 1.0,
+                    float(a[:, 1].std()) or 1.0]
+
+
+def sample_batch(net: MPNet, r: GroupRollout, t: int, members: list, noise: float, gen=None) -> Batch:
+    """Training batch: the chosen member scenes of a group at snapshot t
+    (HIST - 1 <= t < T - 1); input velocities carry Gaussian noise of
+    std noise * vscale (the target is taken relative to the noisy current
+    velocity, so the network learns to correct it)."""
+    torch = net.torch
+    idx = torch.cat([r.scene_idx[m] for m in members])
+    x = r.X[t].index_select(0, idx).contiguous()
+    vh = torch.stack([r.V[t - j].index_select(0, idx) for j in range(HIST)]).contiguous()
+    nodes = r.nodes_dev.index_select(0, idx).contiguous()
+    typ = r.typ_dev.index_select(0, idx)
+    dts = r.dts_dev.index_select(0, idx)
+    if noise > 0:
+        nz = torch.randn(vh.shape, device=x.device, generator=gen) * (noise * net.vscale)
+        nz[:, typ == GNN_BOUNDARY] = 0
+        vh = vh + nz
+    vnext = r.V[t + 1].index_select(0, idx)
+    acc = (vnext - vh[0]) / dts[:, None]
+    nrm = net.norm
+    target = ((acc - nrm[:2]) / nrm[2:]).float()
+    return net.make_batch(x, nodes, vh, 0, r.grid, r.inv2h, target=target)
+
+
+def train(net: MPNet, rollouts, iters: int, lr0=3e-4, lr1=3e-5, batch_nodes=120_000, noise=0.03, seed=0,
+          log_every=0):
+    """Adam on random (group, snapshot, member subset) batches; learning rate
+    decays exponentially from lr0 to lr1.  Returns the loss history."""
+    torch = net.torch
+    rng = np.random.Generator(np.random.PCG64(seed))
+    gen = torch.Generator(device=net.device)
+    gen.manual_seed(seed)
+    sizes = np.array([sum(int(r.scene_idx[m].numel()) for m in range(len(r.members))) for r in rollouts], float)
+    losses = []
+    for it in range(iters):
+        r = rollouts[rng.choice(len(rollouts), p=sizes / sizes.sum())]
+        T = r.X.shape[0]
+        t = int(rng.integers(HIST - 1, T - 1))
+        order = rng.permutation(len(r.members))
+        chosen, total = [], 0
+        for m in order:
+            k = int(r.scene_idx[m].numel())
+            if chosen and total + k > batch_nodes:
+                continue
+            chosen.append(int(m))
+            total += k
+        b = sample_batch(net, r, t, chosen, noise, gen)
+        lr = lr0 * (lr1 / lr0) ** (it / max(iters - 1, 1))
+        losses.append(net.train_step(b, lr))
+        if log_every and it % log_every == 0:
+            print(f"iter {it} loss {losses[-1]:.4f} nodes {b.n} edges {b.E}", flush=True)
+    net.check_device_errors()
+    return losses
+
+
+# ------------------------------------------------------------ the stepper
+
+class LearnedStepper:
+    """Learned strides over one group's particles, starting from snapshot
+    t0 of a rollout (positions and the HIST velocities up to t0).  mode
+    'net' uses the network, 'gravity' the stepper with a = g (the method
+    without the network), both with the same stride update and walls."""
+
+    def __init__(self, net: MPNet, r: GroupRollout, t0: int = HIST - 1, mode: str = "net", solver=None,
+                 phase_sizes=None):
+        torch = net.torch
+        self.net, self.r, self.mode = net, r, mode
+        dev = net.device
+        self.n = r.X.shape[1]
+        self.x = r.X[t0].clone()
+        self.vh = torch.stack([r.V[t0 - j] for j in range(HIST)]).contiguous()
+        self.head = 0
+        self.nodes = r.nodes_dev
+        self.solver, self.phase_sizes = solver, phase_sizes
+        self.sig = [torch.zeros(self.n, dtype=torch.float64, device=dev) for _ in range(2)]
+        self.gate = torch.zeros(4, dtype=torch.float64, device=dev)
+        typ = r.nodes["type"]
+        self.e_floor = float((r.nodes["mass"][typ != GNN_BOUNDARY].astype(np.float64) * (-GRAVITY) * r.dx).sum())
+        self.fallbacks = 0
+        self.strides = 0
+        self.batch = None
+        self._graph()
+        self._density(self.sig[0])
+        self.energy, self.energy_ke = self._energy(self.sig[0])
+
+    def _energy(self, sig_new):
+        """(kinetic + potential, kinetic) energy of the current state; the
+        density sums of the gate against sig[0] land in self.gate."""
+        net = self.net
+        _call(net.L.sphg_gnn_gate_sums(_ptr(sig_new), _ptr(self.sig[0]), _ptr(self.x), _ptr(self.vh[self.head]),
+                                       _ptr(self.nodes), self.n, -GRAVITY, _ptr(self.gate), net.stream),
+              "sphg_gnn_gate_sums")
+        g = self.gate.cpu().numpy()
+        self.last_gate = g
+        return float(g[2] + g[3]), float(g[2])
+
+    def _graph(self):
+        self.batch = self.net.make_batch(self.x, self.nodes, self.vh, self.head, self.r.grid, self.r.inv2h)
+
+    def _density(self, out):
+        b = self.batch
+        _call(self.net.L.sphg_gnn_number_density(_ptr(self.x), _ptr(b.off), _ptr(b.src), self.n, self.r.h,
+                                                 _ptr(out), self.net.stream), "sphg_gnn_number_density")
+
+    def _pred(self):
+        net, torch = self.net, self.net.torch
+        if self.mode == "net":
+            return net.forward(self.batch, keep=False)
+        out = net.bufs.get("gravity_pred", (self.batch.n_pad, L_WIDTH), torch.float32, zero=True)
+        out[:, 1] = (GRAVITY - float(net.norm[1])) / float(net.norm[3])
+        out[:, 0] = -float(net.norm[0]) / float(net.norm[2])
+        return out
+
+    def step(self):
+        """One stride: network, update, gates; a failed stride is redone by
+        the solver.  Returns True when the learned stride was kept."""
+        net = self.net
+        x0, vh0, head0 = self.x.clone(), self.vh.clone(), self.head
+        pred = self._pred()
+        new = (self.head + HIST - 1) % HIST
+        _call(net.L.sphg_gnn_stride_update(_ptr(pred), L_WIDTH, _ptr(net.norm), _ptr(self.nodes), _ptr(self.x),
+                                           _ptr(self.vh), self.head, new, self.n, 1e-9, net.stream),
+              "sphg_gnn_stride_update")
+        self.head = new
+        self._graph()
+        self._density(self.sig[1])
+        energy, ke = self._energy(self.sig[1])
+        g = self.last_gate
+        rms = math.sqrt(g[0] / max(g[1], 1.0))
+        rise = (energy - self.energy) / (max(self.energy_ke, 0.0) + self.e_floor)
+        self.last_rms, self.last_rise = rms, rise
+        failed = self.solver is not None and (rms > GATE_DENSITY or rise > GATE_ENERGY)
+        if failed:
+            self.fallbacks += 1
+            self.x.copy_(x0)
+            self.vh.copy_(vh0)
+            self.head = head0
+            self._solver_stride()
+            self._graph()
+            self._density(self.sig[1])
+            energy, ke = self._energy(self.sig[1])
+        self.energy, self.energy_ke = energy, ke
+        self.sig.reverse()
+        self.strides += 1
+        return not failed
+
+    def _solver_stride(self):
+        """k plain SPH steps from the current positions and velocities."""
+        torch = self.net.torch
+        v = self.vh[self.head].double()
+        a = 0
+        for k, nk in enumerate(self.phase_sizes):
+            self.solver.import_xv(k + 1, self.x[a:a + nk].data_ptr(), v[a:a + nk].contiguous().data_ptr())
+            a += nk
+        self.solver.time_integration(K_STRIDE)
+        new = (self.head + HIST - 1) % HIST
+        vt = torch.empty((self.n, 2), dtype=torch.float64, device=self.net.device)
+        a = 0
+        for k, nk in enumerate(self.phase_sizes):
+            self.solver.export_xv(k + 1, self.x[a:a + nk].data_ptr(), vt[a:a + nk].data_ptr())
+            a += nk
+        self.vh[new].copy_(vt)
+        self.head = new
+
+
+# -------------------------------------------------------------- evaluation
+
+def front_and_surface(x, typ, material, box, dx, bin_w=None):
+    """Runout (furthest x of the column material from the left wall) and the
+    free-surface profile (highest y per x bin of width 2 dx, -inf where empty)."""
+    p = x[typ == material]
+    if p.size == 0:
+        return 0.0, np.full(0, -np.inf)
+    bin_w = bin_w or 2.0 * dx
+    runout = float(p[:, 0].max() - box[0])
+    bins = np.clip(np.floor((p[:, 0] - box[0]) / bin_w).astype(np.int64), 0, None)
+    prof = np.full(int(bins.max()) + 1, -np.inf)
+    np.maximum.at(prof, bins, p[:, 1])
+    return runout, prof
+
+
+def scene_errors(x_pred, x_ref, nodes, kind, box, dx):
+    """Runout and mean free-surface errors in units of dx."""
+    typ = nodes["type"]
+    mat = GNN_WATER if kind == "dam_break" else GNN_SOIL
+    r_p, s_p = front_and_surface(x_pred, typ, mat, box, dx)
+    r_r, s_r = front_and_surface(x_ref, typ, mat, box, dx)
+    m = min(s_p.size, s_r.size)
+    both = np.isfinite(s_p[:m]) & np.isfinite(s_r[:m])
+    surf = float(np.abs(s_p[:m][both] - s_r[:m][both]).mean() / dx) if both.any() else float("nan")
+    return abs(r_p - r_r) / dx, surf
+
+
+def evaluate(net: MPNet, rollouts, t0: int = HIST - 1, strides: int | None = None, mode="net", solvers=None):
+    """Roll every group out from snapshot t0 for `strides` learned strides and
+    compare each scene with the plain solver's snapshot at the same time.
+    Returns per-scene errors, timing and fallback counts."""
+    torch = net.torch
+    rows = []
+    wall = 0.0
+    psteps = 0
+    plain_ms = 0.0
+    fallbacks = 0
+    for gi, r in enumerate(rollouts):
+        T = r.X.shape[0]
+        ns = strides if strides is not None else T - 1 - t0
+        solver, sizes = (solvers[gi] if solvers else (None, None))
+        st = LearnedStepper(net, r, t0, mode, solver, sizes)
+        torch.cuda.synchronize(net.device)
+        c0 = time.perf_counter()
+        for _ in range(ns):
+            st.step()
+        torch.cuda.synchronize(net.device)
+        wall += time.perf_counter() - c0
+        psteps += r.X.shape[1] * ns * K_STRIDE
+        plain_ms += r.plain_ms * ns * K_STRIDE
+        fallbacks += st.fallbacks
+        xp = st.x.cpu().numpy()
+        xr = r.X[t0 + ns].cpu().numpy()
+        for local, m in enumerate(r.members):
+            idx = r.scene_idx_np[local]
+            ro, sf = scene_errors(xp[idx], xr[idx], r.nodes[idx], r.kind, r.boxes[local], r.dx)
+            rows.append(dict(scene=m, kind=r.kind, n=int(idx.size), runout_dx=ro, surface_dx=sf))
+    return dict(scenes=rows, learned_particle_steps_per_s=psteps / max(wall, 1e-12),
+                plain_particle_steps_per_s=psteps / max(plain_ms * 1e-3, 1e-12), fallbacks=fallbacks,
+                wall_s=wall)

@@ -42,13 +42,14 @@ class Scene:
     name: str
     params: Params
     phases: list = field(default_factory=list)   # [PhaseArrays] (1 or 2)
+    box: tuple = (0.0, 0.0, 0.0)                  # (left wall, right wall, floor)
 
     @property
     def n_particles(self) -> int:
         return sum(p.n for p in self.phases)
 
     def copy(self) -> "Scene":
-        return Scene(self.name, _copy_params(self.params), [p.copy() for p in self.phases])
+        return Scene(self.name, _copy_params(self.params), [p.copy() for p in self.phases], self.box)
 
 
 def _copy_params(p: Params) -> Params:
@@ -157,7 +158,7 @@ def dam_break(width=0.2, height=0.4, tank_w=0.8, tank_h=0.6, dx=0.005, skf=1,
     p.alpha, p.beta, p.delta = 0.1, 0.0, 0.1
     p.dt = 0.25 * float(P.hsml[0]) / wm["c"]
     _finish(p, [P], tank_w, tank_h, dx, skf, precision)
-    return Scene("dam_break", p, [P])
+    return Scene("dam_break", p, [P], (0.0, tank_w, 0.0))
 
 
 def granular_column(width=0.2, height=0.1, box_w=1.0, box_h=0.3, dx=0.002, skf=1,
@@ -182,7 +183,7 @@ def granular_column(width=0.2, height=0.1, box_w=1.0, box_h=0.3, dx=0.002, skf=1
     p.alpha = 0.1
     p.dt = 0.1 * float(P.hsml[0]) / sm["c"]
     _finish(p, [P], box_w, box_h, dx, skf, precision)
-    return Scene("granular_column", p, [P])
+    return Scene("granular_column", p, [P], (0.0, box_w, 0.0))
 
 
 def two_phase(width=4.0, height=1.0, block_w=1.0, block_h=0.4, water_h=0.8, dx=0.002,
@@ -224,7 +225,7 @@ def two_phase(width=4.0, height=1.0, block_w=1.0, block_h=0.4, water_h=0.8, dx=0
     h = float(W.hsml[0])
     p.dt = min(0.25 * h / wm["c"], 0.1 * h / sm["c"])
     _finish(p, [W, S], width, height, dx, skf, precision)
-    return Scene("two_phase", p, [W, S])
+    return Scene("two_phase", p, [W, S], (0.0, width, 0.0))
 
 
 def jitter(scene: Scene, amplitude: float, seed: int = 12345) -> Scene:

@@ -1,0 +1,358 @@
+"""Learned particle stepper: the FP64 reference network (oracle/gnn_ref.py)
+pinned by finite differences on the CPU; on the GPU, the radius graph
+against brute force, the tcgen05/bf16 network's forward pass and gradients
+against the FP64 reference, training, and what the trained network gains
+over the same stepper without it on held-out scenes."""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import gnn_ref
+from sources_b200 import learn
+
+
+def _tiny(seed=0, n=14, L=8, F=6, layers=2):
+    rng = np.random.default_rng(seed)
+    x = rng.uniform(0, 1.0, size=(n, 2))
+    src, dst = gnn_ref.radius_graph(x, 0.45)
+    wn, bn = gnn_ref.weight_names(layers)
+    W = {}
+    for name in wn:
+        r = 2 * L if name.endswith("wsd") else L
+        c = F if name.endswith(".w1") and name.startswith("enc") else (2 * L if name.endswith("v1") else L)
+        W[name] = rng.normal(0, 1.0 / math.sqrt(c), size=(r, c))
+    for name in bn:
+        W[name] = rng.normal(0, 0.1, size=L)
+    fn = rng.normal(size=(n, F))
+    fe = rng.normal(size=(len(src), F))
+    target = rng.normal(size=(n, 2))
+    mask = (rng.random(n) < 0.8).astype(float)
+    return W, fn, fe, src, dst, n, layers, target, mask
+
+
+def _loss(W, fn, fe, src, dst, n, layers, target, mask, scale=0.25):
+    out, _ = gnn_ref.forward(W, fn, fe, src, dst, n, layers, scale)
+    return gnn_ref.loss_and_grad_out(out, target, mask)[0]
+
+
+def test_reference_backward_matches_finite_differences():
+    W, fn, fe, src, dst, n, layers, target, mask = _tiny()
+    assert len(src) > 2 * n
+    out, cache = gnn_ref.forward(W, fn, fe, src, dst, n, layers, 0.25)
+    _, dout = gnn_ref.loss_and_grad_out(out, target, mask)
+    G = gnn_ref.backward(W, fn, fe, src, dst, n, layers, 0.25, cache, dout)
+    rng = np.random.default_rng(1)
+    eps = 1e-6
+    for name in W:
+        flat = W[name].reshape(-1)
+        for k in rng.choice(flat.size, size=min(4, flat.size), replace=False):
+            old = flat[k]
+            flat[k] = old + eps
+            lp = _loss(W, fn, fe, src, dst, n, layers, target, mask)
+            flat[k] = old - eps
+            lm = _loss(W, fn, fe, src, dst, n, layers, target, mask)
+            flat[k] = old
+            fd = (lp - lm) / (2 * eps)
+            an = G[name].reshape(-1)[k]
+            assert abs(fd - an) <= 1e-6 + 1e-5 * abs(fd), (name, k, fd, an)
+
+
+def test_reference_radius_graph_order():
+    x = np.array([[0.0, 0.0], [0.1, 0.0], [0.0, 0.1], [0.5, 0.5], [0.0, 0.0]])
+    src, dst = gnn_ref.radius_graph(x, 0.2)
+    pairs = list(zip(dst.tolist(), src.tolist()))
+    assert pairs == sorted(pairs)
+    assert (0, 4) in pairs and (4, 0) in pairs and all(3 not in p for p in pairs)
+
+
+def test_weight_layout():
+    Ws, Bs = learn.weight_specs()
+    w = learn.init_weights(3)
+    names = [n for n, *_ in Ws] + [n for n, *_ in Bs]
+    wn, bn = gnn_ref.weight_names(learn.LAYERS)
+    assert sorted(names) == sorted(wn + bn)
+    assert w["dec.w2"].shape == (learn.L_WIDTH, learn.L_WIDTH)
+    assert not w["dec.w2"][learn.NOUT:].any()
+    assert w["p0.wsd"].shape == (2 * learn.L_WIDTH, learn.L_WIDTH) and w["p0.v1"].shape == (128, 256)
+    assert learn.NODE_DTYPE.itemsize == 32
+
+
+def test_node_table_types_and_walls():
+    from sources_b200 import scenes
+    s = scenes.small("two_phase")
+    t = learn.node_table(s, 1.5, 2e-4, "submerged")
+    assert t.size == s.n_particles
+    W, S = s.phases
+    assert (t["type"][:W.ntotal] == learn.GNN_WATER).all()
+    assert (t["type"][W.ntotal:W.n] == learn.GNN_BOUNDARY).all()
+    assert (t["type"][W.n:W.n + S.ntotal] == learn.GNN_SOIL).all()
+    assert np.allclose(t["xl"], 1.5) and np.allclose(t["xr"], 1.5 + s.box[1])
+    assert np.allclose(t["porosity"], s.params.soil.porosity) and np.allclose(t["phi"], s.params.soil.phi)
+
+
+# ------------------------------------------------------------------- GPU
+
+def _cloud(n_side=40, dx=0.004, seed=5, dup=50):
+    """Jittered lattice with a few duplicated points (zero-distance pairs)."""
+    rng = np.random.default_rng(seed)
+    i, j = np.meshgrid(np.arange(n_side), np.arange(n_side), indexing="ij")
+    x = np.stack([i.ravel(), j.ravel()], 1) * dx + dx / 2
+    x = x + rng.uniform(-0.2 * dx, 0.2 * dx, size=x.shape)
+    return np.concatenate([x, x[rng.choice(len(x), dup, replace=False)]])
+
+
+def _nodes(n, rng, boundary_frac=0.2):
+    a = np.zeros(n, learn.NODE_DTYPE)
+    a["xl"], a["xr"], a["yf"] = 0.0, 0.16, 0.0
+    a["dts"], a["porosity"], a["phi"], a["mass"] = 4e-4, 0.4, 0.5, 0.016
+    a["type"] = rng.integers(0, 2, n)
+    a["type"][rng.random(n) < boundary_frac] = learn.GNN_BOUNDARY
+    return a
+
+
+@pytest.mark.gpu
+def test_radius_graph_matches_brute_force(cuda_ok):
+    import torch
+    net = learn.MPNet(seed=0)
+    x = _cloud()
+    h = 0.0048
+    xd = torch.from_numpy(x).cuda()
+    grid = learn.Grid(-0.01, -0.01, 2 * h, 12, 12)     # too small on purpose: nodes beyond are clamped in
+    off, src, dst, E = net.graph.build(xd, len(x), grid, net.stream)
+    s_ref, d_ref = gnn_ref.radius_graph(x, 2 * h)
+    assert E == len(s_ref)
+    off, src, dst = off.cpu().numpy(), src[:E].cpu().numpy(), dst[:E].cpu().numpy()
+    assert (np.diff(off) == np.bincount(d_ref, minlength=len(x))).all()
+    assert (dst == d_ref).all()                          # receivers in node order
+    for i in range(len(x)):                              # same senders per receiver
+        a, b = off[i], off[i + 1]
+        assert sorted(src[a:b]) == sorted(s_ref[a:b].tolist())
+
+
+def _net_and_batch(seed=0, with_target=True):
+    import torch
+    net = learn.MPNet(seed=seed)
+    rng = np.random.default_rng(seed)
+    x = _cloud(n_side=24, seed=seed, dup=20)
+    n = len(x)
+    nodes = _nodes(n, rng)
+    vh = rng.normal(0, 0.3, size=(learn.HIST, n, 2)).astype(np.float32)
+    net.vscale = 0.3
+    xd = torch.from_numpy(x).cuda()
+    nd = torch.from_numpy(nodes.view(np.uint8).reshape(-1, 32).copy()).cuda()
+    vd = torch.from_numpy(vh).cuda()
+    target = torch.from_numpy(rng.normal(size=(n, 2)).astype(np.float32)).cuda() if with_target else None
+    grid = learn.Grid(-0.02, -0.02, 2 * 0.0048, 30, 30)
+    b = net.make_batch(xd, nd, vd, 2, grid, 1.0 / (2 * 0.0048), target=target)
+    return net, b
+
+
+def _ref_weights(net):
+    """The bf16-rounded weights the GPU multiplies with, in FP64."""
+    W = {k: v["wb"].float().cpu().numpy().astype(np.float64) for k, v in net.W.items()}
+    W.update({k: v["w"].cpu().numpy().astype(np.float64) for k, v in net.B.items()})
+    return W
+
+
+def _ref_inputs(b):
+    fn = b.fn[:b.n].float().cpu().numpy().astype(np.float64)
+    fe = b.fe[:b.E].float().cpu().numpy().astype(np.float64)
+    return fn, fe, b.src[:b.E].cpu().numpy(), b.dst[:b.E].cpu().numpy()
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
+
+
+@pytest.mark.gpu
+def test_features_match_definition(cuda_ok):
+    net, b = _net_and_batch()
+    fn = b.fn.float().cpu().numpy()
+    nodes = b.nodes.cpu().numpy().view(learn.NODE_DTYPE).ravel()
+    x = b.x.cpu().numpy()
+    assert not fn[b.n:].any()                                     # padded rows zero
+    assert np.allclose(fn[:b.n, 10 + 0], nodes["type"] == 0)
+    assert np.allclose(fn[:b.n, 12], nodes["type"] == learn.GNN_BOUNDARY)
+    wall = np.clip((x[:, 0] - 0.0) / (2 * 0.0048), 0, 1)
+    assert np.allclose(fn[:b.n, 13], wall, atol=1e-2)
+    fe = b.fe.float().cpu().numpy()
+    s, d = b.src[:b.E].cpu().numpy(), b.dst[:b.E].cpu().numpy()
+    dx = (x[d] - x[s]) / (2 * 0.0048)
+    assert np.allclose(fe[:b.E, 0], dx[:, 0], atol=1e-2) and np.allclose(fe[:b.E, 2], np.hypot(*dx.T), atol=1e-2)
+    assert not fe[b.E:].any() and not fe[:b.E, 4:].any()
+
+
+@pytest.mark.gpu
+def test_forward_matches_fp64_reference(cuda_ok):
+    net, b = _net_and_batch()
+    out = net.forward(b, keep=True).cpu().numpy()[:b.n]
+    net.check_device_errors()
+    W = _ref_weights(net)
+    fn, fe, src, dst = _ref_inputs(b)
+    ref, _ = gnn_ref.forward(W, fn, fe, src, dst, b.n, learn.LAYERS, learn.AGG_SCALE)
+    # bf16 operands at every GEMM input (8-bit mantissa): a few 1e-3 per layer
+    assert _rel(out, ref) < 2e-2
+    assert not out[:, learn.NOUT:].any()
+
+
+def _grad_errors(net, G):
+    errs = {}
+    for name, g_ref in G.items():
+        if name.startswith("_"):
+            continue
+        d = net.W.get(name) or net.B.get(name)
+        g = d["g"].cpu().numpy().astype(np.float64)
+        if name in ("dec.w2", "dec.b2"):
+            g_ref = g_ref.copy()
+            g_ref[learn.NOUT:] = 0.0
+            g = g.copy()
+            g[learn.NOUT:] = 0.0
+        cos = float((g * g_ref).sum() / max(np.linalg.norm(g) * np.linalg.norm(g_ref), 1e-30))
+        errs[name] = (_rel(g, g_ref), cos)
+    return errs
+
+
+@pytest.mark.gpu
+def test_gradients_match_fp64_reference(cuda_ok):
+    net, b = _net_and_batch()
+    net.zero_grad()
+    out = net.forward(b, keep=True)
+    dout = net.loss(b, out)
+    net.backward(b, dout)
+    net.check_device_errors()
+    W = _ref_weights(net)
+    fn, fe, src, dst = _ref_inputs(b)
+    target = b.target[:b.n].cpu().numpy().astype(np.float64)
+    mask = b.mask[:b.n].cpu().numpy().astype(np.float64)
+    n, E = b.n, b.E
+    dh0 = net.bufs.buf["dh"][:b.n_pad * learn.L_WIDTH].view(b.n_pad, -1)[:n].cpu().numpy().astype(np.float64)
+    de0 = net.bufs.buf["de"][:b.E_pad * learn.L_WIDTH].view(b.E_pad, -1)[:E].cpu().numpy().astype(np.float64)
+    out_gpu = out[:n].cpu().numpy().astype(np.float64)
+    for rounded in (True, False):
+        ref_out, cache = gnn_ref.forward(W, fn, fe, src, dst, n, learn.LAYERS, learn.AGG_SCALE,
+                                         round_bf16=rounded)
+        loss_ref, dref = gnn_ref.loss_and_grad_out(ref_out, target, mask)
+        G = gnn_ref.backward(W, fn, fe, src, dst, n, learn.LAYERS, learn.AGG_SCALE, cache, dref)
+        errs = _grad_errors(net, G)
+        rel = np.array([r for r, _ in errs.values()])
+        cos = np.array([c for _, c in errs.values()])
+        r_out, r_dh, r_de = _rel(out_gpu, ref_out), _rel(dh0, G["_dh0"]), _rel(de0, G["_de0"])
+        print("FP64 reference", "with" if rounded else "without", "bf16 operand rounding:",
+              f"loss {float(net.loss_buf.item()):.7g} vs {loss_ref:.7g}; output {r_out:.2e};",
+              f"d/dh0 {r_dh:.2e}; d/de0 {r_de:.2e}; weight gradients max {rel.max():.3f} mean {rel.mean():.3f}",
+              f"min cosine {cos.min():.5f}")
+        if rounded:
+            # the same bf16 operands at the same places.  What remains: fp32
+            # summation order, whose ~1e-7 differences flip an occasional bf16
+            # rounding (2^-8); the flips compound over the ~12 forward and ~20
+            # backward rounding stages of this untrained network to ~1e-3 at the
+            # output and a few percent in the gradients (sums with sign
+            # cancellation magnify it).  Each stage on its own is checked to
+            # fp32 level by test_backward_stages_match_fp64_reference.
+            assert abs(float(net.loss_buf.item()) - loss_ref) < 1e-4 * loss_ref
+            assert r_out < 1e-2 and r_dh < 6e-2 and r_de < 6e-2
+            assert cos.min() > 0.998 and rel.max() < 0.06, errs
+        else:
+            # against exact FP64 arithmetic the bf16 operands cost a few percent,
+            # evenly over every tensor; a wrong index or a missing term is O(1)
+            assert abs(float(net.loss_buf.item()) - loss_ref) < 3e-2 * loss_ref
+            assert r_out < 3e-2 and r_dh < 0.1 and r_de < 0.1
+            assert cos.min() > 0.99 and rel.max() < 0.12 and rel.mean() < 0.08, errs
+
+
+def _np(t, rows=None):
+    a = t.float().cpu().numpy().astype(np.float64)
+    return a if rows is None else a[:rows]
+
+
+@pytest.mark.gpu
+def test_backward_stages_match_fp64_reference(cuda_ok):
+    """Teacher-forced check of every backward stage: the FP64 reference runs
+    the decoder, each layer and the encoders from the GPU's own inputs of
+    that stage (incoming gradients, saved activations, bf16 operands) and
+    must reproduce the stage's weight gradients and outgoing gradients up
+    to fp32 summation order."""
+    net, b = _net_and_batch(seed=1)
+    net.zero_grad()
+    out = net.forward(b, keep=True)
+    dout = net.loss(b, out)
+    trace = {}
+    net.backward(b, dout, trace)
+    net.check_device_errors()
+    W = _ref_weights(net)
+    fn, fe, src, dst = _ref_inputs(b)
+    n, E, Np, Ep, L = b.n, b.E, b.n_pad, b.E_pad, learn.L_WIDTH
+    q = gnn_ref.bf16
+    buf = lambda name, rows, cols=L: net.bufs.buf[name][:rows * cols].view(rows, cols)
+    worst = {}
+
+    def check(G, names):
+        for name in names:
+            d = net.W.get(name) or net.B.get(name)
+            g, r = _np(d["g"]), G[name]
+            if name.startswith("dec."):
+                g, r = g.copy(), r.copy()
+                g[learn.NOUT:] = 0.0
+                r[learn.NOUT:] = 0.0
+            worst[name] = _rel(g, r)
+
+    G, dh = gnn_ref.decoder_backward(W, _np(dout, n), _np(buf("du", Np), n), _np(buf(f"hb{learn.LAYERS}", Np), n), q)
+    check(G, G)
+    worst["dh@dec"] = _rel(_np(trace[learn.LAYERS - 1][0], n), dh)
+    for l in reversed(range(learn.LAYERS)):
+        p = f"p{l}."
+        dh_in, de_in = _np(trace[l][0], n), _np(trace[l][1], E)
+        G, dh, de = gnn_ref.layer_backward(
+            W, p, dh_in, de_in, _np(buf(f"hb{l}", Np), n), _np(buf(f"eb{l}", Ep), E), _np(buf(f"z{l}", Ep), E),
+            _np(buf(f"cat{l}", Np, 2 * L), n), _np(buf(f"y{l}", Np), n), src, dst, n, learn.AGG_SCALE, q)
+        check(G, G)
+        nxt = trace[l - 1] if l > 0 else trace["enc"]
+        worst[f"dh@{l}"] = _rel(_np(nxt[0], n), dh)
+        worst[f"de@{l}"] = _rel(_np(nxt[1], E), de)
+    G = gnn_ref.encoder_backward(W, _np(trace["enc"][0], n), _np(trace["enc"][1], E), _np(buf("nz", Np), n),
+                                 _np(buf("ez", Ep), E), fn, fe, q)
+    check(G, G)
+    print("teacher-forced stage errors: max", max(worst.values()), max(worst, key=worst.get))
+    # fp32 vs fp64 summation inside one stage, and the rare bf16 rounding
+    # that difference flips; a wrong index, transpose or missing term is O(1)
+    assert max(worst.values()) < 5e-3, worst
+
+
+@pytest.mark.gpu
+def test_training_reduces_loss(cuda_ok):
+    net, b = _net_and_batch(seed=2)
+    losses = [net.train_step(b, 1e-3) for _ in range(150)]
+    net.check_device_errors()
+    assert all(math.isfinite(v) for v in losses)
+    assert min(losses[-10:]) < 0.2 * losses[0]
+
+
+@pytest.mark.gpu
+def test_trained_stepper_beats_the_stepper_without_network(cuda_ok):
+    """Small ensemble: train on rollouts of 10 scenes, evaluate on 3 held-out
+    scenes; the learned strides must track the plain solver better than the
+    same stepper with gravity-only acceleration (no network)."""
+    from sources_b200 import ensemble
+    small = [s for s in ensemble.specs(400) if s.n_target < 4000]
+    kinds = {k: [s for s in small if s.kind == k] for k in ensemble.KINDS}
+    train_specs = kinds["dam_break"][:4] + kinds["dry"][:3] + kinds["submerged"][:3]
+    test_specs = [kinds["dam_break"][4], kinds["dry"][3], kinds["submerged"][3]]
+    strides = 30
+    ens = ensemble.Ensemble(train_specs, tune=False)
+    roll = learn.rollout_ensemble(ens, strides)
+    ens.close()
+    net = learn.MPNet(seed=0)
+    net.vscale, nrm = learn.normalisation(roll)
+    net.norm.copy_(net.torch.tensor(nrm))
+    losses = learn.train(net, roll, 300, lr0=5e-4, lr1=5e-5, batch_nodes=60_000)
+    assert np.mean(losses[-20:]) < np.mean(losses[:20])
+    ens2 = ensemble.Ensemble(test_specs, tune=False)
+    held = learn.rollout_ensemble(ens2, strides)
+    ens2.close()
+    res_net = learn.evaluate(net, held, strides=20, mode="net")
+    res_grav = learn.evaluate(net, held, strides=20, mode="gravity")
+    e_net = np.nanmean([r["runout_dx"] + r["surface_dx"] for r in res_net["scenes"]])
+    e_grav = np.nanmean([r["runout_dx"] + r["surface_dx"] for r in res_grav["scenes"]])
+    print("held-out error (runout + surface, dx): net", e_net, "gravity-only", e_grav)
+    assert e_net < e_grav

@@ -22,10 +22,39 @@ extern "C" {
 int sphg_gemm_bf16_tn(const void* A, const void* B, float* C, int M, int N, int K, int accumulate, int split_k,
                       int* err_dev, void* cuda_stream);
 
+/* Epilogues of the weight-stationary GEMM (acc = the A B^T tile):
+ *   STORE     z = acc                 ACC    z += acc
+ *   BIAS_ACT  z = acc + bias (z kept when non-null), h = bf16(relu ? max(z, 0) : z)
+ *   EDGE      z = acc + bias + P[src[r], :N] + P[dst[r], N:2N] for rows r < nedge
+ *             (z kept when non-null), h = bf16(max(z, 0))
+ *   RESID     z = z + acc + bias, h = bf16(z) when h is non-null */
+enum { SPHG_EPI_STORE = 0, SPHG_EPI_ACC = 1, SPHG_EPI_BIAS_ACT = 2, SPHG_EPI_EDGE = 3, SPHG_EPI_RESID = 4 };
+
+typedef struct SphgGemmEpi {
+    int32_t mode, relu;
+    const float* bias;   /* [N] */
+    float* z;            /* [M x N] fp32 */
+    void* h;             /* [M x N] bf16 */
+    const float* P;      /* EDGE: [nodes x 2N] projections gathered per row */
+    const int* src;
+    const int* dst;
+    long long nedge;
+} SphgGemmEpi;
+
+/* Weight-stationary persistent GEMM C[M x N] = A[M x K] * B[N x K]^T with
+ * B resident in shared memory and a fused epilogue; (N, K) in {(128, 64),
+ * (128, 128), (256, 128), (128, 256)} (SPHG_ERR_UNSUPPORTED otherwise),
+ * M % 128 == 0, 16-byte aligned arrays.  A device wait that gives up sets
+ * *err_dev to 1. */
+int sphg_gemm_bf16_ws(const void* A, const void* B, int M, int N, int K, const SphgGemmEpi* epilogue, int* err_dev,
+                      void* cuda_stream);
+
 /* ---------------------------------------------------------------------
  * Message-passing network kernels.  Feature matrices are row-major bf16 or
  * fp32 with the row count padded to a multiple of 128; L is the latent
- * width.  Graphs are CSR by receiver: off[n + 1] (int64), src[e] and dst[e]
+ * width, which must be 128 (the width the kernels are compiled for; other
+ * values return SPHG_ERR_BAD_ARG); element counts n are multiples of 4 and
+ * bias_act takes 64, 128 or 256 columns.  Graphs are CSR by receiver: off[n + 1] (int64), src[e] and dst[e]
  * (int32), receivers in node order.
  * ------------------------------------------------------------------- */
 
@@ -95,9 +124,10 @@ int sphg_gnn_gather_bwd(const float* dz, const int* src, const int64_t* off, flo
 int sphg_gnn_node_concat(const void* h_bf16, const float* agg, void* out_bf16, long long nnode, int L,
                          void* cuda_stream);
 int sphg_gnn_node_concat_bwd(const float* d, float* dh, float* dagg, long long nnode, int L, void* cuda_stream);
-/* mean squared error over masked rows, first nout columns; loss += ... */
+/* squared error (Huber beyond |d| = delta when delta > 0) over masked rows
+ * and the first nout columns, times inv_count; loss += ..., dpred = d/dpred */
 int sphg_gnn_mse(const float* pred, int ld, const float* target, int nout, const float* mask, long long rows,
-                 float inv_count, float* dpred, float* loss, void* cuda_stream);
+                 float inv_count, float delta, float* dpred, float* loss, void* cuda_stream);
 /* Adam on w [rows x cols]; rows >= row_limit held at zero; refreshes the
  * bf16 copy w_bf16 and its transpose wt_bf16 [cols x rows] when non-null */
 int sphg_gnn_adam(float* w, const float* g, float* m, float* v, void* w_bf16, void* wt_bf16, int rows, int cols,

@@ -80,13 +80,20 @@ def forward(W, fn, fe, src, dst, n_nodes, layers, scale, keep=True, round_bf16=F
     return out, c
 
 
-def loss_and_grad_out(out, target, mask, nout=2):
-    """Masked mean squared error over the first nout columns."""
+def loss_and_grad_out(out, target, mask, nout=2, delta=0.0):
+    """Masked mean squared error over the first nout columns; with delta > 0
+    the Huber form (linear beyond |d| = delta)."""
     rows = mask != 0
     count = float(rows.sum() * nout)
     d = out[:, :nout] - target
     d[~rows] = 0.0
     g = np.zeros_like(out)
+    if delta > 0:
+        a = np.abs(d)
+        lin = a > delta
+        val = np.where(lin, delta * (2 * a - delta), d * d)
+        g[:, :nout] = np.where(lin, 2.0 * delta * np.sign(d), 2.0 * d) / count
+        return float(val.sum() / count), g
     g[:, :nout] = 2.0 * d / count
     return float((d * d).sum() / count), g
 

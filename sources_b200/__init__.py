@@ -34,6 +34,7 @@ EXPORTS = ("sphg_default_params", "sphg_create", "sphg_upload_phase", "sphg_sing
            "sphg_gemm_bf16_tn", "sphg_export_xv_device", "sphg_import_xv_device", *sorted(_GNN_SIGNATURES := {
                # message-passing network kernels (include/sphg_learn.h); P pointer,
                # I int, L 64-bit count, F float, D double, S size_t pointer
+               "sphg_gemm_bf16_ws": "PPIIIPPP",
                "sphg_gnn_scan_bytes": "IP",
                "sphg_gnn_graph_count": "PPIPPPPPPLP",
                "sphg_gnn_graph_fill": "PPIPPPPPP",
@@ -50,7 +51,7 @@ EXPORTS = ("sphg_default_params", "sphg_create", "sphg_upload_phase", "sphg_sing
                "sphg_gnn_gather_bwd": "PPPPILIP",
                "sphg_gnn_node_concat": "PPPLIP",
                "sphg_gnn_node_concat_bwd": "PPPLIP",
-               "sphg_gnn_mse": "PIPIPLFPPP",
+               "sphg_gnn_mse": "PIPIPLFFPPP",
                "sphg_gnn_adam": "PPPPPPIIFFFFIIP",
                "sphg_gnn_stride_update": "PIPPPPIIIDP",
                "sphg_gnn_number_density": "PPPIDPP",

@@ -52,7 +52,8 @@ def build(force: bool = False, verbose: bool = False, defines=(), out: str = OUT
            "-shared", "-Xcompiler", "-fPIC",
            "-Xptxas", "-v", *["-D" + d for d in defines], "-o", tmp, *SRC, "-lcudart"]
     r = subprocess.run(cmd, capture_output=True, text=True)
-    with open(os.path.join(HERE, "_build", "ptxas.log"), "w") as f:
+    log = os.path.join(HERE, "_build", "ptxas.log") if out == OUT else out + ".ptxas.log"
+    with open(log, "w") as f:
         f.write(r.stdout + r.stderr)
     if r.returncode != 0:
         sys.stderr.write(r.stderr[-8000:])

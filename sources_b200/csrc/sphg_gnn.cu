@@ -121,93 +121,146 @@ __global__ void k_graph_fill(const double2* __restrict__ x, int n, const int* __
 }
 
 // --------------------------------------------------------------- features
+//
+// Row kernels: a row of C values is handled by C/4 (fp32, float4) or C/8
+// (bf16, 16-byte) adjacent threads, so every access is a full-width
+// vector and no index needs a division by a run-time width.
 
+constexpr int LW = 128;              // latent width the layer kernels are compiled for
+constexpr int FW = SPHG_GNN_FEATURES;
+
+template <int TPR>
+__device__ __forceinline__ void row_lane(long long& r, int& lane) {
+    r = (long long)blockIdx.x * (256 / TPR) + threadIdx.x / TPR;
+    lane = threadIdx.x % TPR;
+}
+
+__device__ __forceinline__ uint4 pack8(const float* v) {
+    uint4 u;
+    __nv_bfloat162 t;
+    t = __floats2bfloat162_rn(v[0], v[1]); u.x = *reinterpret_cast<uint32_t*>(&t);
+    t = __floats2bfloat162_rn(v[2], v[3]); u.y = *reinterpret_cast<uint32_t*>(&t);
+    t = __floats2bfloat162_rn(v[4], v[5]); u.z = *reinterpret_cast<uint32_t*>(&t);
+    t = __floats2bfloat162_rn(v[6], v[7]); u.w = *reinterpret_cast<uint32_t*>(&t);
+    return u;
+}
+
+__device__ __forceinline__ uint2 pack4(float4 v) {
+    uint2 u;
+    __nv_bfloat162 t;
+    t = __floats2bfloat162_rn(v.x, v.y); u.x = *reinterpret_cast<uint32_t*>(&t);
+    t = __floats2bfloat162_rn(v.z, v.w); u.y = *reinterpret_cast<uint32_t*>(&t);
+    return u;
+}
+
+__device__ __forceinline__ float4 add4(float4 a, float4 b) { return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w); }
+__device__ __forceinline__ float4 relu4(float4 a) {
+    return make_float4(fmaxf(a.x, 0.f), fmaxf(a.y, 0.f), fmaxf(a.z, 0.f), fmaxf(a.w, 0.f));
+}
+
+// node rows of 64 bf16, 8 threads per row, 8 features each
 __global__ void k_node_features(const double2* __restrict__ x, const float2* __restrict__ vhist, int head,
                                 const sphg_gnn_node* __restrict__ st, int n, int n_pad, float inv2h, float inv_vscale,
                                 bf16* __restrict__ out) {
-    const long long t = gid();
-    if (t >= (long long)n_pad * SPHG_GNN_FEATURES) return;
-    const int i = (int)(t / SPHG_GNN_FEATURES), f = (int)(t % SPHG_GNN_FEATURES);
-    float v = 0.f;
-    if (i < n) {
+    long long i;
+    int lane;
+    row_lane<FW / 8>(i, lane);
+    if (i >= n_pad) return;
+    float v[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (i < n && lane < 3) {
         const sphg_gnn_node s = st[i];
-        if (f < 2 * SPHG_GNN_HISTORY) {
-            const int slot = (head + (f >> 1)) % SPHG_GNN_HISTORY;
-            const float2 u = vhist[(size_t)slot * n + i];
-            v = ((f & 1) ? u.y : u.x) * inv_vscale;
-        } else if (f < 13) {
-            v = (f - 10) == s.type ? 1.f : 0.f;
-        } else if (f < 16) {
-            const double2 p = x[i];
-            const double d = f == 13 ? p.x - s.xl : (f == 14 ? s.xr - p.x : p.y - s.yf);
-            v = fminf(fmaxf((float)d * inv2h, 0.f), 1.f);
-        } else if (f == 16) v = s.porosity;
-        else if (f == 17) v = s.phi;
-        else if (f == 18) v = s.dts * 1.0e3f;
+        for (int k = 0; k < 8; ++k) {
+            const int f = lane * 8 + k;
+            if (f < 2 * SPHG_GNN_HISTORY) {
+                const int slot = (head + (f >> 1)) % SPHG_GNN_HISTORY;
+                const float2 u = vhist[(size_t)slot * n + i];
+                v[k] = ((f & 1) ? u.y : u.x) * inv_vscale;
+            } else if (f < 13) {
+                v[k] = (f - 10) == s.type ? 1.f : 0.f;
+            } else if (f < 16) {
+                const double2 p = x[i];
+                const double d = f == 13 ? p.x - s.xl : (f == 14 ? s.xr - p.x : p.y - s.yf);
+                v[k] = fminf(fmaxf((float)d * inv2h, 0.f), 1.f);
+            } else if (f == 16) v[k] = s.porosity;
+            else if (f == 17) v[k] = s.phi;
+            else if (f == 18) v[k] = s.dts * 1.0e3f;
+        }
     }
-    out[t] = __float2bfloat16_rn(v);
+    reinterpret_cast<uint4*>(out)[i * (FW / 8) + lane] = pack8(v);
 }
 
+// edge rows of 64 bf16: (x_dst - x_src) / 2h, distance / 2h, same type
 __global__ void k_edge_features(const double2* __restrict__ x, const sphg_gnn_node* __restrict__ st,
                                 const int* __restrict__ src, const int* __restrict__ dst, long long nedge,
                                 long long nedge_pad, double inv2h, bf16* __restrict__ out) {
-    const long long t = gid();
-    if (t >= nedge_pad * SPHG_GNN_FEATURES) return;
-    const long long k = t / SPHG_GNN_FEATURES;
-    const int f = (int)(t % SPHG_GNN_FEATURES);
-    float v = 0.f;
-    if (k < nedge && f < 4) {
+    long long k;
+    int lane;
+    row_lane<FW / 8>(k, lane);
+    if (k >= nedge_pad) return;
+    float v[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (k < nedge && lane == 0) {
         const int a = dst[k], b = src[k];
         const double2 p = x[a], q = x[b];
         const double dx = (p.x - q.x) * inv2h, dy = (p.y - q.y) * inv2h;
-        if (f == 0) v = (float)dx;
-        else if (f == 1) v = (float)dy;
-        else if (f == 2) v = (float)sqrt(dx * dx + dy * dy);
-        else v = st[a].type == st[b].type ? 1.f : 0.f;
+        v[0] = (float)dx;
+        v[1] = (float)dy;
+        v[2] = (float)sqrt(dx * dx + dy * dy);
+        v[3] = st[a].type == st[b].type ? 1.f : 0.f;
     }
-    out[t] = __float2bfloat16_rn(v);
+    reinterpret_cast<uint4*>(out)[k * (FW / 8) + lane] = pack8(v);
 }
 
 // ----------------------------------------------------------------- layers
 
-__global__ void k_f32_to_bf16(const float* __restrict__ x, bf16* __restrict__ y, long long n) {
+// n % 4 == 0
+__global__ void k_f32_to_bf16(const float4* __restrict__ x, uint2* __restrict__ y, long long n4) {
     const long long i = gid();
-    if (i < n) y[i] = __float2bfloat16_rn(x[i]);
+    if (i < n4) y[i] = pack4(x[i]);
 }
 
-// z += b; h = relu(z) or z, in bf16
+// z += b; h = relu(z) or z, in bf16; rows of C
+template <int C>
 __global__ void k_bias_act(float* __restrict__ z, const float* __restrict__ b, bf16* __restrict__ h, long long rows,
-                           int cols, int relu) {
-    const long long i = gid();
-    if (i >= rows * cols) return;
-    const float v = z[i] + b[i % cols];
-    z[i] = v;
-    h[i] = __float2bfloat16_rn(relu ? fmaxf(v, 0.f) : v);
+                           int relu) {
+    long long r;
+    int lane;
+    row_lane<C / 4>(r, lane);
+    if (r >= rows) return;
+    float4* zr = reinterpret_cast<float4*>(z + r * C);
+    const float4 v = add4(zr[lane], reinterpret_cast<const float4*>(b)[lane]);
+    zr[lane] = v;
+    reinterpret_cast<uint2*>(h + r * C)[lane] = pack4(relu ? relu4(v) : v);
 }
 
 // fused edge first layer: z[k] (= e_k W_e^T from the GEMM) += P[src][:L] +
 // P[dst][L:] + b; a = relu(z)
 __global__ void k_edge_gather_act(float* __restrict__ z, const float* __restrict__ P, const int* __restrict__ src,
                                   const int* __restrict__ dst, const float* __restrict__ b, bf16* __restrict__ a,
-                                  long long nedge, long long nedge_pad, int L) {
-    const long long i = gid();
-    if (i >= nedge_pad * L) return;
-    const long long k = i / L;
-    const int f = (int)(i % L);
-    float v = z[i] + b[f];
-    if (k < nedge) v += P[(long long)src[k] * 2 * L + f] + P[(long long)dst[k] * 2 * L + L + f];
-    z[i] = v;
-    a[i] = __float2bfloat16_rn(fmaxf(v, 0.f));
+                                  long long nedge, long long nedge_pad) {
+    long long k;
+    int lane;
+    row_lane<LW / 4>(k, lane);
+    if (k >= nedge_pad) return;
+    float4* zr = reinterpret_cast<float4*>(z + k * LW);
+    float4 v = add4(zr[lane], reinterpret_cast<const float4*>(b)[lane]);
+    if (k < nedge) {
+        v = add4(v, reinterpret_cast<const float4*>(P + (long long)src[k] * 2 * LW)[lane]);
+        v = add4(v, reinterpret_cast<const float4*>(P + (long long)dst[k] * 2 * LW + LW)[lane]);
+    }
+    zr[lane] = v;
+    reinterpret_cast<uint2*>(a + k * LW)[lane] = pack4(relu4(v));
 }
 
-// dz = dh * (z > 0), fp32 and bf16
-__global__ void k_relu_bwd(const float* __restrict__ dh, const float* __restrict__ z, float* __restrict__ dz,
-                           bf16* __restrict__ dzb, long long n) {
+// dz = dh * (z > 0), fp32 and bf16; n % 4 == 0
+__global__ void k_relu_bwd(const float4* __restrict__ dh, const float4* __restrict__ z, float4* __restrict__ dz,
+                           uint2* __restrict__ dzb, long long n4) {
     const long long i = gid();
-    if (i >= n) return;
-    const float v = z[i] > 0.f ? dh[i] : 0.f;
+    if (i >= n4) return;
+    const float4 g = dh[i], m = z[i];
+    const float4 v = make_float4(m.x > 0.f ? g.x : 0.f, m.y > 0.f ? g.y : 0.f, m.z > 0.f ? g.z : 0.f,
+                                 m.w > 0.f ? g.w : 0.f);
     dz[i] = v;
-    dzb[i] = __float2bfloat16_rn(v);
+    dzb[i] = pack4(v);
 }
 
 // out[c] += sum over rows of x[r, c]; 512 rows per block
@@ -242,68 +295,97 @@ __global__ void k_transpose(const S* __restrict__ in, bf16* __restrict__ out, lo
 
 // agg[n] = scale * sum of e over the edges received by n
 __global__ void k_segsum(const float* __restrict__ e, const int64_t* __restrict__ off, float* __restrict__ agg,
-                         int nnode, int L, float scale) {
-    const long long i = gid();
-    if (i >= (long long)nnode * L) return;
-    const int n = (int)(i / L), f = (int)(i % L);
-    float s = 0.f;
-    for (long long k = off[n]; k < off[n + 1]; ++k) s += e[k * L + f];
-    agg[i] = s * scale;
+                         int nnode, float scale) {
+    long long n;
+    int lane;
+    row_lane<LW / 4>(n, lane);
+    if (n >= nnode) return;
+    float4 s = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (long long k = off[n]; k < off[n + 1]; ++k) s = add4(s, reinterpret_cast<const float4*>(e + k * LW)[lane]);
+    reinterpret_cast<float4*>(agg + n * LW)[lane] = make_float4(s.x * scale, s.y * scale, s.z * scale, s.w * scale);
 }
 
 // de[k] += scale * dagg[receiver of k]
 __global__ void k_segsum_bwd(const float* __restrict__ dagg, const int* __restrict__ dst, float* __restrict__ de,
-                             long long nedge, int L, float scale) {
-    const long long i = gid();
-    if (i >= nedge * L) return;
-    de[i] += scale * dagg[(long long)dst[i / L] * L + (i % L)];
+                             long long nedge, float scale) {
+    long long k;
+    int lane;
+    row_lane<LW / 4>(k, lane);
+    if (k >= nedge) return;
+    const float4 g = reinterpret_cast<const float4*>(dagg + (long long)dst[k] * LW)[lane];
+    float4* d = reinterpret_cast<float4*>(de + k * LW) + lane;
+    *d = add4(*d, make_float4(g.x * scale, g.y * scale, g.z * scale, g.w * scale));
 }
 
 // backward of the gathered projections: dP[n][L + f] = sum of dz over the
 // edges n receives; dP[n][f] += dz over the edges n sends (atomic; dP[n][f]
 // must be zero before)
 __global__ void k_gather_bwd_dst(const float* __restrict__ dz, const int64_t* __restrict__ off,
-                                 float* __restrict__ dP, int nnode, int L) {
-    const long long i = gid();
-    if (i >= (long long)nnode * L) return;
-    const int n = (int)(i / L), f = (int)(i % L);
-    float s = 0.f;
-    for (long long k = off[n]; k < off[n + 1]; ++k) s += dz[k * L + f];
-    dP[(long long)n * 2 * L + L + f] = s;
+                                 float* __restrict__ dP, int nnode) {
+    long long n;
+    int lane;
+    row_lane<LW / 4>(n, lane);
+    if (n >= nnode) return;
+    float4 s = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (long long k = off[n]; k < off[n + 1]; ++k) s = add4(s, reinterpret_cast<const float4*>(dz + k * LW)[lane]);
+    reinterpret_cast<float4*>(dP + n * 2 * LW + LW)[lane] = s;
 }
 
 __global__ void k_gather_bwd_src(const float* __restrict__ dz, const int* __restrict__ src, float* __restrict__ dP,
-                                 long long nedge, int L) {
-    const long long i = gid();
-    if (i >= nedge * L) return;
-    atomicAdd(dP + (long long)src[i / L] * 2 * L + (i % L), dz[i]);
+                                 long long nedge) {
+    long long k;
+    int lane;
+    row_lane<LW / 4>(k, lane);
+    if (k >= nedge) return;
+    const float4 g = reinterpret_cast<const float4*>(dz + k * LW)[lane];
+    float* d = dP + (long long)src[k] * 2 * LW + lane * 4;
+    atomicAdd(d, g.x);
+    atomicAdd(d + 1, g.y);
+    atomicAdd(d + 2, g.z);
+    atomicAdd(d + 3, g.w);
 }
 
-// [h | agg] as bf16 rows of 2L
+// [h | agg] as bf16 rows of 2L: 16 bytes (8 values) per thread
 __global__ void k_node_concat(const bf16* __restrict__ h, const float* __restrict__ agg, bf16* __restrict__ out,
-                              long long nnode, int L) {
-    const long long i = gid();
-    if (i >= nnode * 2 * L) return;
-    const long long n = i / (2 * L);
-    const int f = (int)(i % (2 * L));
-    out[i] = f < L ? h[n * L + f] : __float2bfloat16_rn(agg[n * L + f - L]);
+                              long long nnode) {
+    long long n;
+    int lane;
+    row_lane<2 * LW / 8>(n, lane);
+    if (n >= nnode) return;
+    uint4 v;
+    if (lane < LW / 8) {
+        v = reinterpret_cast<const uint4*>(h + n * LW)[lane];
+    } else {
+        const float4* a = reinterpret_cast<const float4*>(agg + n * LW) + 2 * (lane - LW / 8);
+        const float4 p = a[0], q = a[1];
+        const float t[8] = {p.x, p.y, p.z, p.w, q.x, q.y, q.z, q.w};
+        v = pack8(t);
+    }
+    reinterpret_cast<uint4*>(out + n * 2 * LW)[lane] = v;
 }
 
 __global__ void k_node_concat_bwd(const float* __restrict__ d, float* __restrict__ dh, float* __restrict__ dagg,
-                                  long long nnode, int L) {
-    const long long i = gid();
-    if (i >= nnode * 2 * L) return;
-    const long long n = i / (2 * L);
-    const int f = (int)(i % (2 * L));
-    if (f < L) dh[n * L + f] += d[i];
-    else dagg[n * L + f - L] = d[i];
+                                  long long nnode) {
+    long long n;
+    int lane;
+    row_lane<2 * LW / 4>(n, lane);
+    if (n >= nnode) return;
+    const float4 g = reinterpret_cast<const float4*>(d + n * 2 * LW)[lane];
+    if (lane < LW / 4) {
+        float4* t = reinterpret_cast<float4*>(dh + n * LW) + lane;
+        *t = add4(*t, g);
+    } else {
+        reinterpret_cast<float4*>(dagg + n * LW)[lane - LW / 4] = g;
+    }
 }
 
-// mean squared error over the rows with mask != 0, first nout columns of
-// pred (row stride ld); dpred = d loss / d pred (zero elsewhere)
+// Huber loss (squared error up to |d| = delta, linear beyond; plain squared
+// error for delta <= 0) over the rows with mask != 0, first nout columns of
+// pred (row stride ld), scaled by inv_count; dpred = d loss / d pred (zero
+// elsewhere)
 __global__ void k_mse(const float* __restrict__ pred, int ld, const float* __restrict__ target, int nout,
-                      const float* __restrict__ mask, long long rows, float inv_count, float* __restrict__ dpred,
-                      float* __restrict__ loss) {
+                      const float* __restrict__ mask, long long rows, float inv_count, float delta,
+                      float* __restrict__ dpred, float* __restrict__ loss) {
     const long long i = gid();
     if (i >= rows * ld) return;
     const long long r = i / ld;
@@ -311,8 +393,14 @@ __global__ void k_mse(const float* __restrict__ pred, int ld, const float* __res
     float g = 0.f;
     if (c < nout && mask[r] != 0.f) {
         const float d = pred[i] - target[r * nout + c];
-        g = 2.f * d * inv_count;
-        atomicAdd(loss, d * d * inv_count);
+        const float a = fabsf(d);
+        if (delta <= 0.f || a <= delta) {
+            g = 2.f * d * inv_count;
+            atomicAdd(loss, d * d * inv_count);
+        } else {
+            g = copysignf(2.f * delta, d) * inv_count;
+            atomicAdd(loss, delta * (2.f * a - delta) * inv_count);
+        }
     }
     dpred[i] = g;
 }
@@ -479,35 +567,48 @@ int sphg_gnn_graph_fill(const sphg_gnn_grid* g, const double* x, int n, const in
     return ok_or_cuda();
 }
 
+// blocks of 256 threads for `rows` rows of TPR threads each
+inline unsigned row_blocks(long long rows, int tpr) { return nb(rows, 256 / tpr); }
+#define ROWS(kern, rows, tpr, ...)                                                            \
+    do {                                                                                      \
+        if ((rows) > 0) kern<<<row_blocks((rows), (tpr)), 256, 0, (cudaStream_t)stream>>>(__VA_ARGS__); \
+        return ok_or_cuda();                                                                  \
+    } while (0)
+
 int sphg_gnn_node_features(const double* x, const float* vhist, int head, const sphg_gnn_node* st, int n, int n_pad,
                            float inv2h, float inv_vscale, void* out, void* stream) {
     if (head < 0 || head >= SPHG_GNN_HISTORY || n_pad < n) return SPHG_ERR_BAD_ARG;
-    LAUNCH1(k_node_features, (long long)n_pad * SPHG_GNN_FEATURES, (const double2*)x, (const float2*)vhist, head, st,
-            n, n_pad, inv2h, inv_vscale, (bf16*)out);
+    ROWS(k_node_features, n_pad, FW / 8, (const double2*)x, (const float2*)vhist, head, st, n, n_pad, inv2h,
+         inv_vscale, (bf16*)out);
 }
 
 int sphg_gnn_edge_features(const double* x, const sphg_gnn_node* st, const int* src, const int* dst, long long nedge,
                            long long nedge_pad, double inv2h, void* out, void* stream) {
     if (nedge_pad < nedge) return SPHG_ERR_BAD_ARG;
-    LAUNCH1(k_edge_features, nedge_pad * SPHG_GNN_FEATURES, (const double2*)x, st, src, dst, nedge, nedge_pad, inv2h,
-            (bf16*)out);
+    ROWS(k_edge_features, nedge_pad, FW / 8, (const double2*)x, st, src, dst, nedge, nedge_pad, inv2h, (bf16*)out);
 }
 
 int sphg_gnn_f32_to_bf16(const float* x, void* y, long long n, void* stream) {
-    LAUNCH1(k_f32_to_bf16, n, x, (bf16*)y, n);
+    if (n % 4) return SPHG_ERR_BAD_ARG;
+    LAUNCH1(k_f32_to_bf16, n / 4, (const float4*)x, (uint2*)y, n / 4);
 }
 
 int sphg_gnn_bias_act(float* z, const float* b, void* h, long long rows, int cols, int relu, void* stream) {
-    LAUNCH1(k_bias_act, rows * cols, z, b, (bf16*)h, rows, cols, relu);
+    if (cols == 64) ROWS(k_bias_act<64>, rows, 16, z, b, (bf16*)h, rows, relu);
+    if (cols == 128) ROWS(k_bias_act<128>, rows, 32, z, b, (bf16*)h, rows, relu);
+    if (cols == 256) ROWS(k_bias_act<256>, rows, 64, z, b, (bf16*)h, rows, relu);
+    return SPHG_ERR_BAD_ARG;
 }
 
 int sphg_gnn_edge_gather_act(float* z, const float* P, const int* src, const int* dst, const float* b, void* a,
                              long long nedge, long long nedge_pad, int L, void* stream) {
-    LAUNCH1(k_edge_gather_act, nedge_pad * L, z, P, src, dst, b, (bf16*)a, nedge, nedge_pad, L);
+    if (L != LW || nedge_pad < nedge) return SPHG_ERR_BAD_ARG;
+    ROWS(k_edge_gather_act, nedge_pad, LW / 4, z, P, src, dst, b, (bf16*)a, nedge, nedge_pad);
 }
 
 int sphg_gnn_relu_bwd(const float* dh, const float* z, float* dz, void* dzb, long long n, void* stream) {
-    LAUNCH1(k_relu_bwd, n, dh, z, dz, (bf16*)dzb, n);
+    if (n % 4) return SPHG_ERR_BAD_ARG;
+    LAUNCH1(k_relu_bwd, n / 4, (const float4*)dh, (const float4*)z, (float4*)dz, (uint2*)dzb, n / 4);
 }
 
 int sphg_gnn_colsum(const float* x, long long rows, int cols, float* out, void* stream) {
@@ -528,33 +629,38 @@ int sphg_gnn_transpose(const void* in, int in_is_f32, void* out, long long rows,
 }
 
 int sphg_gnn_segsum(const float* e, const int64_t* off, float* agg, int nnode, int L, float scale, void* stream) {
-    LAUNCH1(k_segsum, (long long)nnode * L, e, off, agg, nnode, L, scale);
+    if (L != LW) return SPHG_ERR_BAD_ARG;
+    ROWS(k_segsum, (long long)nnode, LW / 4, e, off, agg, nnode, scale);
 }
 
 int sphg_gnn_segsum_bwd(const float* dagg, const int* dst, float* de, long long nedge, int L, float scale,
                         void* stream) {
-    LAUNCH1(k_segsum_bwd, nedge * L, dagg, dst, de, nedge, L, scale);
+    if (L != LW) return SPHG_ERR_BAD_ARG;
+    ROWS(k_segsum_bwd, nedge, LW / 4, dagg, dst, de, nedge, scale);
 }
 
 int sphg_gnn_gather_bwd(const float* dz, const int* src, const int64_t* off, float* dP, int nnode,
                         long long nedge, int L, void* stream) {
+    if (L != LW) return SPHG_ERR_BAD_ARG;
     cudaStream_t s = (cudaStream_t)stream;
-    if (nnode > 0) k_gather_bwd_dst<<<nb((long long)nnode * L, 256), 256, 0, s>>>(dz, off, dP, nnode, L);
-    if (nedge > 0) k_gather_bwd_src<<<nb(nedge * L, 256), 256, 0, s>>>(dz, src, dP, nedge, L);
+    if (nnode > 0) k_gather_bwd_dst<<<row_blocks(nnode, LW / 4), 256, 0, s>>>(dz, off, dP, nnode);
+    if (nedge > 0) k_gather_bwd_src<<<row_blocks(nedge, LW / 4), 256, 0, s>>>(dz, src, dP, nedge);
     return ok_or_cuda();
 }
 
 int sphg_gnn_node_concat(const void* h, const float* agg, void* out, long long nnode, int L, void* stream) {
-    LAUNCH1(k_node_concat, nnode * 2 * L, (const bf16*)h, agg, (bf16*)out, nnode, L);
+    if (L != LW) return SPHG_ERR_BAD_ARG;
+    ROWS(k_node_concat, nnode, 2 * LW / 8, (const bf16*)h, agg, (bf16*)out, nnode);
 }
 
 int sphg_gnn_node_concat_bwd(const float* d, float* dh, float* dagg, long long nnode, int L, void* stream) {
-    LAUNCH1(k_node_concat_bwd, nnode * 2 * L, d, dh, dagg, nnode, L);
+    if (L != LW) return SPHG_ERR_BAD_ARG;
+    ROWS(k_node_concat_bwd, nnode, 2 * LW / 4, d, dh, dagg, nnode);
 }
 
 int sphg_gnn_mse(const float* pred, int ld, const float* target, int nout, const float* mask, long long rows,
-                 float inv_count, float* dpred, float* loss, void* stream) {
-    LAUNCH1(k_mse, rows * ld, pred, ld, target, nout, mask, rows, inv_count, dpred, loss);
+                 float inv_count, float delta, float* dpred, float* loss, void* stream) {
+    LAUNCH1(k_mse, rows * ld, pred, ld, target, nout, mask, rows, inv_count, delta, dpred, loss);
 }
 
 int sphg_gnn_adam(float* w, const float* g, float* m, float* v, void* wb, void* wt, int rows, int cols, float lr,

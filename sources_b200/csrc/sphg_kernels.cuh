@@ -35,6 +35,23 @@ struct SimConst {
 };
 
 #define SPHG_TPB 128
+// minimum resident blocks per SM of each pair pass (register cap for the
+// compiler: 65,536 / (SPHG_TPB * min blocks) registers per thread).  Timed on
+// a B200 at 912,016 particles: water_pass_a 172 -> 148 us at 8 blocks,
+// water_pass_b 234 -> 207 us at 6, cross_water 81 -> 69 us at 8; the soil
+// pass is fastest uncapped (8 blocks: 60 -> 84 us).
+#ifndef SPHG_MINB_A
+#define SPHG_MINB_A 8
+#endif
+#ifndef SPHG_MINB_B
+#define SPHG_MINB_B 6
+#endif
+#ifndef SPHG_MINB_SOIL
+#define SPHG_MINB_SOIL 1
+#endif
+#ifndef SPHG_MINB_CROSS
+#define SPHG_MINB_CROSS 8
+#endif
 
 __device__ __forceinline__ int gtid() { return blockIdx.x * blockDim.x + threadIdx.x; }
 
@@ -314,7 +331,7 @@ __global__ void __launch_bounds__(SPHG_TPB) k_water_sum(PhaseDev<T> P, GridGeom 
 // delta_sph's (dx . grad W) 2 (f_a - f_b) / r^2 is evaluated as 2 s (f_a - f_b)
 // since grad W = s dx.
 template <typename T, int SKF, bool SINGLE>
-__global__ void __launch_bounds__(SPHG_TPB) k_water_pass_a(PhaseDev<T> P, GridGeom g, SearchConst sc, SimConst c, DevCounters* cnt) {
+__global__ void __launch_bounds__(SPHG_TPB, SPHG_MINB_A) k_water_pass_a(PhaseDev<T> P, GridGeom g, SearchConst sc, SimConst c, DevCounters* cnt) {
     SPHG_HITBUF(T);
     const int k = gtid();
     const bool valid = k < P.n;
@@ -397,7 +414,7 @@ __global__ void __launch_bounds__(SPHG_TPB) k_water_pass_a(PhaseDev<T> P, GridGe
 // dx = x_real - x_virtual, as the reference does with real particles
 // numbered before virtual ones.
 template <typename T, int SKF, bool SINGLE>
-__global__ void __launch_bounds__(SPHG_TPB) k_water_pass_b(PhaseDev<T> P, GridGeom g, SearchConst sc, SimConst c, StepCtl u) {
+__global__ void __launch_bounds__(SPHG_TPB, SPHG_MINB_B) k_water_pass_b(PhaseDev<T> P, GridGeom g, SearchConst sc, SimConst c, StepCtl u) {
     typedef typename V2<T>::t T2;
     SPHG_HITBUF(T);
     const int k = gtid();
@@ -492,7 +509,7 @@ __global__ void __launch_bounds__(SPHG_TPB) k_water_pass_b(PhaseDev<T> P, GridGe
 // plastic_or_not :3447, plastic_flow_rule3 :3700 and Jaumann_rate :3047,
 // whose spin sum wxy comes from the same pass.
 template <typename T, int SKF, bool SINGLE>
-__global__ void __launch_bounds__(SPHG_TPB) k_soil_pass(PhaseDev<T> P, GridGeom g, SearchConst sc, SimConst c,
+__global__ void __launch_bounds__(SPHG_TPB, SPHG_MINB_SOIL) k_soil_pass(PhaseDev<T> P, GridGeom g, SearchConst sc, SimConst c,
                                                        DevCounters* cnt, int slot, StepCtl u) {
     typedef typename V2<T>::t T2;
     SPHG_HITBUF(T);
@@ -664,7 +681,7 @@ __global__ void __launch_bounds__(SPHG_TPB) k_soil_pass(PhaseDev<T> P, GridGeom 
 // vol_w*rho_w*vof_w*vof_s*(-g/k)*(v_w - v_s)*W/rho_s and the pore pressure
 // m_w p_w/(rho_w rho_s) becomes vol_w p_w / rho_s.
 template <typename T, int SKF>
-__global__ void __launch_bounds__(SPHG_TPB) k_cross_soil(PhaseDev<T> S, PhaseDev<T> W, GridGeom g, SearchConst sc, SimConst c,
+__global__ void __launch_bounds__(SPHG_TPB, SPHG_MINB_CROSS) k_cross_soil(PhaseDev<T> S, PhaseDev<T> W, GridGeom g, SearchConst sc, SimConst c,
                                                         StepCtl u, DevCounters* cnt) {
     typedef typename V2<T>::t T2;
     SPHG_HITBUF(T);
@@ -712,7 +729,7 @@ __global__ void __launch_bounds__(SPHG_TPB) k_cross_soil(PhaseDev<T> S, PhaseDev
 // volume_fraction_water :3912 (vof2), and every renorm_interval steps the
 // renormalisation rho <- rho/vof*vof2, vof <- vof2 (declarations_sph.f90:1414-1421).
 template <typename T, int SKF>
-__global__ void __launch_bounds__(SPHG_TPB) k_cross_water(PhaseDev<T> W, PhaseDev<T> S, GridGeom g, SearchConst sc, SimConst c,
+__global__ void __launch_bounds__(SPHG_TPB, SPHG_MINB_CROSS) k_cross_water(PhaseDev<T> W, PhaseDev<T> S, GridGeom g, SearchConst sc, SimConst c,
                                                          DevCounters* cnt, StepCtl u) {
     typedef typename V2<T>::t T2;
     SPHG_HITBUF(T);

@@ -189,7 +189,276 @@ int launch_gemm(const __nv_bfloat16* A, const __nv_bfloat16* B, float* C, int M,
     return cudaGetLastError() == cudaSuccess ? SPHG_OK : SPHG_ERR_CUDA;
 }
 
+// ------------------------------------------------------------------------
+// Weight-stationary persistent GEMM for tall-skinny products: C[M x N] =
+// A[M x K] * B[N x K]^T with B (the weights, N * K <= 32k elements) resident
+// in shared memory for the whole launch.  Each CTA loops over 128-row tiles
+// of A (tile = blockIdx.x + i * gridDim.x): the A tile of step i + 1 is
+// copied (cp.async, 16 bytes per request, into the canonical no-swizzle
+// K-major layout) while the MMAs of step i run on the tensor cores and the
+// epilogue of step i - 1 drains the other TMEM accumulator, so load, MMA
+// and epilogue overlap.  Every wait on an MMA is bounded; on timeout the
+// kernel sets *err, waits (bounded) for its MMAs and copies, frees TMEM and
+// returns.  Epilogues fuse what follows the product in the network:
+//   STORE     z = acc
+//   ACC       z += acc
+//   BIAS_ACT  z = acc + bias (kept when z != null), h = bf16(act(z))
+//   EDGE      z = acc + bias + P[src[row], :N] + P[dst[row], N:] (rows < nedge),
+//             h = bf16(relu(z))
+//   RESID     z = z + acc + bias, h = bf16(z) when h != null
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+__device__ __forceinline__ uint4 bf16x8(const float* v) {
+    uint4 u;
+    __nv_bfloat162 t;
+    t = __floats2bfloat162_rn(v[0], v[1]); u.x = *reinterpret_cast<uint32_t*>(&t);
+    t = __floats2bfloat162_rn(v[2], v[3]); u.y = *reinterpret_cast<uint32_t*>(&t);
+    t = __floats2bfloat162_rn(v[4], v[5]); u.z = *reinterpret_cast<uint32_t*>(&t);
+    t = __floats2bfloat162_rn(v[6], v[7]); u.w = *reinterpret_cast<uint32_t*>(&t);
+    return u;
+}
+
+template <int N, int K>
+struct WsShape {
+    static constexpr uint32_t A_KC = 128 * 16;          // bytes between K chunks of an A tile
+    static constexpr uint32_t B_KC = N * 16;            // ... of the resident B
+    static constexpr uint32_t A_BYTES = (K / 8) * A_KC;
+    static constexpr uint32_t B_BYTES = (K / 8) * B_KC;
+    static constexpr uint32_t SMEM = B_BYTES + 2 * A_BYTES + 32;
+    static constexpr int TCOLS = 2 * N;                 // two accumulators
+    // at most 2 CTAs per SM (TMEM: 2 x 256 columns), 1 when N = 256
+    static constexpr uint32_t SMEM_REQ = N == 256 ? (SMEM > 120 * 1024 ? SMEM : 120 * 1024)
+                                                  : (SMEM > 100 * 1024 ? SMEM : 100 * 1024);
+    static constexpr int PER_SM = N == 256 || SMEM > 110 * 1024 ? 1 : 2;
+};
+
+template <int N, int K>
+__device__ __forceinline__ void ws_load_a(uint8_t* sA, const __nv_bfloat16* __restrict__ A, int m0, int tid) {
+    constexpr int KC = K / 8;
+#pragma unroll 4
+    for (int c = tid; c < 128 * KC; c += 128) {
+        const int r = c / KC, kc = c % KC;
+        cp_async16(smem_u32(sA + kc * WsShape<N, K>::A_KC + (r >> 3) * 128 + (r & 7) * 16),
+                   A + (size_t)(m0 + r) * K + kc * 8);
+    }
+}
+
+template <int N, int K>
+__device__ __forceinline__ void ws_epilogue(const SphgGemmEpi& ep, uint32_t tacc, long long row) {
+#pragma unroll 1
+    for (int c = 0; c < N; c += 8) {
+        uint32_t r[8];
+        asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                     : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                       "=r"(r[7])
+                     : "r"(tacc + (uint32_t)c));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        float v[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) v[j] = __uint_as_float(r[j]);
+        float4* z4 = ep.z ? reinterpret_cast<float4*>(ep.z + row * N + c) : nullptr;
+        if (ep.mode == SPHG_EPI_STORE) {
+            z4[0] = make_float4(v[0], v[1], v[2], v[3]);
+            z4[1] = make_float4(v[4], v[5], v[6], v[7]);
+            continue;
+        }
+        if (ep.mode == SPHG_EPI_ACC || ep.mode == SPHG_EPI_RESID) {
+            const float4 a = z4[0], b = z4[1];
+            v[0] += a.x; v[1] += a.y; v[2] += a.z; v[3] += a.w;
+            v[4] += b.x; v[5] += b.y; v[6] += b.z; v[7] += b.w;
+        }
+        if (ep.mode != SPHG_EPI_ACC) {
+            const float4 b0 = reinterpret_cast<const float4*>(ep.bias + c)[0];
+            const float4 b1 = reinterpret_cast<const float4*>(ep.bias + c)[1];
+            v[0] += b0.x; v[1] += b0.y; v[2] += b0.z; v[3] += b0.w;
+            v[4] += b1.x; v[5] += b1.y; v[6] += b1.z; v[7] += b1.w;
+        }
+        if (ep.mode == SPHG_EPI_EDGE && row < ep.nedge) {
+            const float4* ps = reinterpret_cast<const float4*>(ep.P + (long long)ep.src[row] * 2 * N + c);
+            const float4* pd = reinterpret_cast<const float4*>(ep.P + (long long)ep.dst[row] * 2 * N + N + c);
+            const float4 s0 = ps[0], s1 = ps[1], d0 = pd[0], d1 = pd[1];
+            v[0] += s0.x + d0.x; v[1] += s0.y + d0.y; v[2] += s0.z + d0.z; v[3] += s0.w + d0.w;
+            v[4] += s1.x + d1.x; v[5] += s1.y + d1.y; v[6] += s1.z + d1.z; v[7] += s1.w + d1.w;
+        }
+        if (z4) {
+            z4[0] = make_float4(v[0], v[1], v[2], v[3]);
+            z4[1] = make_float4(v[4], v[5], v[6], v[7]);
+        }
+        if (ep.mode != SPHG_EPI_ACC && ep.h) {
+            const bool act = ep.mode == SPHG_EPI_EDGE || (ep.mode == SPHG_EPI_BIAS_ACT && ep.relu);
+            if (act) {
+#pragma unroll
+                for (int j = 0; j < 8; ++j) v[j] = fmaxf(v[j], 0.f);
+            }
+            *reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(ep.h) + row * N + c) = bf16x8(v);
+        }
+    }
+}
+
+template <int N, int K>
+__global__ void __launch_bounds__(128, 1) k_gemm_ws(const __nv_bfloat16* __restrict__ A,
+                                                    const __nv_bfloat16* __restrict__ B, int M, SphgGemmEpi ep,
+                                                    int* __restrict__ err) {
+    typedef WsShape<N, K> S;
+    extern __shared__ __align__(128) uint8_t smem[];
+    uint8_t* sB = smem;
+    uint8_t* sA0 = smem + S::B_BYTES;    // A buffer s at sA0 + s * A_BYTES
+    uint64_t* mbar = (uint64_t*)(smem + S::B_BYTES + 2 * S::A_BYTES);
+    uint32_t* tslot = (uint32_t*)(mbar + 2);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int ntiles = M / 128;
+    const int my = blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+    auto tile_m0 = [&](int i) { return ((int)blockIdx.x + i * (int)gridDim.x) * 128; };
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                     "r"(S::TCOLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mbar)), "r"(1));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mbar + 1)), "r"(1));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::);
+    }
+    // resident B in the canonical K-major layout
+    constexpr int KC = K / 8;
+    for (int c = tid; c < N * KC; c += 128) {
+        const int r = c / KC, kc = c % KC;
+        *reinterpret_cast<uint4*>(sB + kc * S::B_KC + (r >> 3) * 128 + (r & 7) * 16) =
+            *reinterpret_cast<const uint4*>(B + (size_t)r * K + kc * 8);
+    }
+    if (my > 0) ws_load_a<N, K>(sA0, A, tile_m0(0), tid);
+    cp_async_commit();
+    cp_async_wait_all();
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::);
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::);
+    const uint32_t tmem = *tslot;
+    const uint32_t idesc = make_idesc(N);
+    const uint32_t lane_off = (uint32_t)(warp * 32) << 16;
+    uint32_t ph = 0u;    // bit s: parity of the next completion of mbar[s]
+    bool ok = true;
+    int issued = 0, waited = 0;   // MMA steps issued, and seen complete
+
+    for (int i = 0; i < my && ok; ++i) {
+        const int s = i & 1;
+        if (i > 0) {
+            cp_async_wait_all();
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncthreads();
+        }
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::);
+#pragma unroll
+            for (int kk = 0; kk < K / 16; ++kk) {
+                const uint64_t da = make_desc(smem_u32(sA0 + s * S::A_BYTES + kk * 2 * S::A_KC), S::A_KC, 128);
+                const uint64_t db = make_desc(smem_u32(sB + kk * 2 * S::B_KC), S::B_KC, 128);
+                const uint32_t en = kk > 0 ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+                    ::"r"(tmem + (uint32_t)(s * N)), "l"(da), "l"(db), "r"(idesc), "r"(en), "r"(0), "r"(0), "r"(0),
+                      "r"(0));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                         ::"r"(smem_u32(mbar + s)) : "memory");
+        }
+        ++issued;
+        if (i == 0) {
+            if (my > 1) ws_load_a<N, K>(sA0 + S::A_BYTES, A, tile_m0(1), tid);
+            cp_async_commit();
+            continue;
+        }
+        // MMA(i - 1) done: its A buffer is free and its accumulator is ready
+        const int p = s ^ 1;
+        const bool done = mbar_wait(smem_u32(mbar + p), (ph >> p) & 1u, kWaitLimit);
+        ok = __syncthreads_and(done ? 1 : 0) != 0;
+        if (!ok) break;
+        ph ^= 1u << p;
+        ++waited;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::);
+        if (i + 1 < my) ws_load_a<N, K>(sA0 + p * S::A_BYTES, A, tile_m0(i + 1), tid);
+        cp_async_commit();
+        ws_epilogue<N, K>(ep, tmem + lane_off + (uint32_t)(p * N), (long long)tile_m0(i - 1) + warp * 32 + lane);
+        asm volatile("tcgen05.fence::before_thread_sync;" ::);
+        __syncthreads();
+    }
+    if (ok && my > 0) {
+        const int s = (my - 1) & 1;
+        const bool done = mbar_wait(smem_u32(mbar + s), (ph >> s) & 1u, kWaitLimit);
+        ok = __syncthreads_and(done ? 1 : 0) != 0;
+        if (ok) {
+            ph ^= 1u << s;
+            ++waited;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::);
+            ws_epilogue<N, K>(ep, tmem + lane_off + (uint32_t)(s * N), (long long)tile_m0(my - 1) + warp * 32 + lane);
+        }
+    }
+    if (!ok) {
+        if (tid == 0) atomicExch(err, 1);
+        // bounded waits for the MMAs issued but not yet seen complete
+        for (int j = waited; j < issued; ++j) {
+            const int s = j & 1;
+            mbar_wait(smem_u32(mbar + s), (ph >> s) & 1u, kWaitLimit);
+            ph ^= 1u << s;
+        }
+    }
+    cp_async_wait_all();
+    asm volatile("tcgen05.fence::before_thread_sync;" ::);
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(S::TCOLS));
+}
+
+template <int N, int K>
+int launch_ws(const __nv_bfloat16* A, const __nv_bfloat16* B, int M, const SphgGemmEpi& ep, int* err,
+              cudaStream_t s) {
+    typedef WsShape<N, K> S;
+    static bool configured = false;
+    if (!configured) {
+        if (cudaFuncSetAttribute(k_gemm_ws<N, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM_REQ) !=
+            cudaSuccess)
+            return SPHG_ERR_CUDA;
+        configured = true;
+    }
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int ntiles = M / 128;
+    const int grid = ntiles < sms * S::PER_SM ? ntiles : sms * S::PER_SM;
+    k_gemm_ws<N, K><<<grid, 128, S::SMEM_REQ, s>>>(A, B, M, ep, err);
+    return cudaGetLastError() == cudaSuccess ? SPHG_OK : SPHG_ERR_CUDA;
+}
+
 }  // namespace
+
+extern "C" int sphg_gemm_bf16_ws(const void* A, const void* B, int M, int N, int K, const SphgGemmEpi* epi,
+                                 int* err_dev, void* stream) {
+    if (!A || !B || !epi || !err_dev || M <= 0 || M % 128) return SPHG_ERR_BAD_ARG;
+    if ((((uintptr_t)A) | ((uintptr_t)B)) & 15) return SPHG_ERR_BAD_ARG;
+    const SphgGemmEpi& e = *epi;
+    if (e.mode < SPHG_EPI_STORE || e.mode > SPHG_EPI_RESID) return SPHG_ERR_BAD_ARG;
+    const bool need_z = e.mode == SPHG_EPI_STORE || e.mode == SPHG_EPI_ACC || e.mode == SPHG_EPI_RESID;
+    if ((need_z && !e.z) || (e.mode != SPHG_EPI_STORE && e.mode != SPHG_EPI_ACC && !e.bias)) return SPHG_ERR_BAD_ARG;
+    if (e.mode == SPHG_EPI_EDGE && (!e.P || !e.src || !e.dst || !e.h || e.nedge < 0 || e.nedge > M))
+        return SPHG_ERR_BAD_ARG;
+    if ((((uintptr_t)e.z) | ((uintptr_t)e.h) | ((uintptr_t)e.bias) | ((uintptr_t)e.P)) & 15) return SPHG_ERR_BAD_ARG;
+    const __nv_bfloat16* a = (const __nv_bfloat16*)A;
+    const __nv_bfloat16* b = (const __nv_bfloat16*)B;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (N == 128 && K == 64) return launch_ws<128, 64>(a, b, M, e, err_dev, s);
+    if (N == 128 && K == 128) return launch_ws<128, 128>(a, b, M, e, err_dev, s);
+    if (N == 256 && K == 128) return launch_ws<256, 128>(a, b, M, e, err_dev, s);
+    if (N == 128 && K == 256) return launch_ws<128, 256>(a, b, M, e, err_dev, s);
+    return SPHG_ERR_UNSUPPORTED;
+}
 
 extern "C" int sphg_gemm_bf16_tn(const void* A, const void* B, float* C, int M, int N, int K, int accumulate,
                                  int split_k, int* err_dev, void* stream) {

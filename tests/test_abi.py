@@ -41,6 +41,7 @@ def _c_layout():
 #include <stdio.h>
 #include <stddef.h>
 #include "sphg.h"
+#include "sphg_learn.h"
 int main(void) {
   printf("%zu %zu %zu %zu %zu\n", sizeof(sphg_params), sizeof(sphg_phase_host), sizeof(sphg_stats_t),
          sizeof(sphg_material), offsetof(sphg_params, soil));
@@ -49,6 +50,8 @@ int main(void) {
   printf("%zu %zu\n", offsetof(sphg_stats_t, time), offsetof(sphg_stats_t, last_step_ms));
   printf("%zu %zu %zu %zu %zu\n", sizeof(sphg_case), offsetof(sphg_case, results), offsetof(sphg_case, operating_mode),
          sizeof(sphg_scene), sizeof(sphg_tuning));
+  printf("%zu %zu %zu %zu\n", sizeof(SphgGemmEpi), offsetof(SphgGemmEpi, nedge), sizeof(sphg_gnn_node),
+         sizeof(sphg_gnn_grid));
   return 0;
 }
 '''
@@ -73,6 +76,9 @@ def test_struct_layout_matches_ctypes():
     assert v[11] == C.sizeof(abi.Case) and v[12] == abi.Case.results.offset
     assert v[13] == abi.Case.operating_mode.offset
     assert v[14] == C.sizeof(abi.SceneRow) and v[15] == C.sizeof(abi.Tuning)
+    from sources_b200 import learn
+    assert v[16] == C.sizeof(learn.GemmEpi) and v[17] == learn.GemmEpi.nedge.offset
+    assert v[18] == learn.NODE_DTYPE.itemsize and v[19] == C.sizeof(learn.Grid)
 
 
 def test_default_params_match_reference_defaults(lib):

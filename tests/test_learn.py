@@ -261,6 +261,21 @@ def test_gradients_match_fp64_reference(cuda_ok):
             assert cos.min() > 0.99 and rel.max() < 0.12 and rel.mean() < 0.08, errs
 
 
+@pytest.mark.gpu
+def test_huber_loss_kernel(cuda_ok):
+    net, b = _net_and_batch(seed=3)
+    out = net.forward(b, keep=True)
+    pred = out[:b.n].cpu().numpy().astype(np.float64)
+    target = b.target[:b.n].cpu().numpy().astype(np.float64)
+    mask = b.mask[:b.n].cpu().numpy().astype(np.float64)
+    for delta in (0.0, 0.5):
+        dout = net.loss(b, out, delta)
+        ref, g = gnn_ref.loss_and_grad_out(pred, target, mask, delta=delta)
+        assert abs(float(net.loss_buf.item()) - ref) < 1e-5 * ref
+        assert np.allclose(dout[:b.n].cpu().numpy(), g, rtol=1e-5, atol=1e-9)
+        assert not dout[b.n:].any()
+
+
 def _np(t, rows=None):
     a = t.float().cpu().numpy().astype(np.float64)
     return a if rows is None else a[:rows]

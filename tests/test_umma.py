@@ -1,5 +1,7 @@
-"""tcgen05 BF16 GEMM (sphg_gemm_bf16_tn) against an fp32 product of the same
-bf16 inputs: C = A B^T, accumulate, split-K, every N tile width."""
+"""tcgen05 BF16 GEMMs against an fp32 product of the same bf16 inputs:
+sphg_gemm_bf16_tn (C = A B^T, accumulate, split-K, every N tile width) and
+the weight-stationary persistent sphg_gemm_bf16_ws with each fused epilogue,
+from one tile to many tiles per CTA."""
 import pytest
 
 pytestmark = pytest.mark.gpu
@@ -33,3 +35,99 @@ def test_gemm_rejects_bad_shapes(lib):
     assert lib.sphg_gemm_bf16_tn(one, one, one, 100, 128, 64, 0, 1, one, None) != 0   # M % 128
     assert lib.sphg_gemm_bf16_tn(one, one, one, 128, 24, 64, 0, 1, one, None) != 0    # N % 16
     assert lib.sphg_gemm_bf16_tn(one, one, one, 128, 128, 32, 0, 1, one, None) != 0   # K % 64
+
+
+WS_SHAPES = [(128, 64), (128, 128), (256, 128), (128, 256)]
+
+
+def _ws(lib, A, B, M, N, K, epi):
+    import torch
+    from sources_b200 import learn
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    rc = lib.sphg_gemm_bf16_ws(A.data_ptr(), B.data_ptr(), M, N, K, ctypes_addr(epi), err.data_ptr(),
+                               torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    assert rc == 0 and int(err.item()) == 0
+
+
+def ctypes_addr(s):
+    import ctypes
+    return ctypes.addressof(s)
+
+
+@pytest.mark.parametrize("N,K", WS_SHAPES)
+@pytest.mark.parametrize("M", [128, 640, 128 * 701])
+def test_ws_gemm_epilogues(cuda_ok, lib, M, N, K):
+    import torch
+    from sources_b200 import learn
+    g = torch.Generator(device="cuda").manual_seed(M + 3 * N + 7 * K)
+    A = torch.randn(M, K, device="cuda", generator=g).to(torch.bfloat16)
+    B = (torch.randn(N, K, device="cuda", generator=g) / K ** 0.5).to(torch.bfloat16)
+    bias = torch.randn(N, device="cuda", generator=g)
+    prod = A.float() @ B.float().T
+    tol = 1e-4 * float(prod.abs().max()) * (K / 64) ** 0.5 + 1e-5
+    E = learn.GemmEpi()
+    # STORE
+    z = torch.full((M, N), float("nan"), device="cuda")
+    E.mode, E.z = learn.EPI_STORE, z.data_ptr()
+    _ws(lib, A, B, M, N, K, E)
+    assert float((z - prod).abs().max()) <= tol
+    # ACC
+    z0 = torch.randn(M, N, device="cuda", generator=g)
+    z = z0.clone()
+    E.mode = learn.EPI_ACC
+    E.z = z.data_ptr()
+    _ws(lib, A, B, M, N, K, E)
+    assert float((z - (z0 + prod)).abs().max()) <= tol
+    # BIAS_ACT with and without relu, z kept or not
+    for relu, keep in ((1, True), (0, False)):
+        z = torch.zeros(M, N, device="cuda")
+        h = torch.zeros(M, N, device="cuda", dtype=torch.bfloat16)
+        E = learn.GemmEpi(mode=learn.EPI_BIAS_ACT, relu=relu, bias=bias.data_ptr(), z=z.data_ptr() if keep else None,
+                          h=h.data_ptr())
+        _ws(lib, A, B, M, N, K, E)
+        ref = prod + bias
+        if keep:
+            assert float((z - ref).abs().max()) <= tol
+        else:
+            assert not z.any()
+        act = ref.clamp_min(0) if relu else ref
+        assert float((h.float() - act).abs().max()) <= 1e-2 * float(act.abs().max()) + tol
+    # EDGE: rows beyond nedge get the bias only
+    nodes = 300
+    P = torch.randn(nodes, 2 * N, device="cuda", generator=g)
+    nedge = M - 37 if M > 128 else M
+    src = torch.randint(0, nodes, (M,), device="cuda", generator=g, dtype=torch.int32)
+    dst = torch.randint(0, nodes, (M,), device="cuda", generator=g, dtype=torch.int32)
+    z = torch.zeros(M, N, device="cuda")
+    h = torch.zeros(M, N, device="cuda", dtype=torch.bfloat16)
+    E = learn.GemmEpi(mode=learn.EPI_EDGE, relu=1, bias=bias.data_ptr(), z=z.data_ptr(), h=h.data_ptr(),
+                      P=P.data_ptr(), src=src.data_ptr(), dst=dst.data_ptr(), nedge=nedge)
+    _ws(lib, A, B, M, N, K, E)
+    ref = prod + bias
+    ref[:nedge] += P[src[:nedge].long(), :N] + P[dst[:nedge].long(), N:]
+    assert float((z - ref).abs().max()) <= tol
+    assert float((h.float() - ref.clamp_min(0)).abs().max()) <= 1e-2 * float(ref.abs().max()) + tol
+    # RESID
+    z0 = torch.randn(M, N, device="cuda", generator=g)
+    z = z0.clone()
+    h = torch.zeros(M, N, device="cuda", dtype=torch.bfloat16)
+    E = learn.GemmEpi(mode=learn.EPI_RESID, bias=bias.data_ptr(), z=z.data_ptr(), h=h.data_ptr())
+    _ws(lib, A, B, M, N, K, E)
+    ref = z0 + prod + bias
+    assert float((z - ref).abs().max()) <= tol
+    assert float((h.float() - ref).abs().max()) <= 1e-2 * float(ref.abs().max()) + tol
+
+
+def test_ws_gemm_rejects_bad_arguments(lib):
+    from sources_b200 import learn
+    import ctypes
+    one = ctypes.c_void_p(256)
+    E = learn.GemmEpi(mode=learn.EPI_STORE, z=256)
+    a = ctypes.addressof(E)
+    assert lib.sphg_gemm_bf16_ws(one, one, 100, 128, 128, a, one, None) != 0      # M % 128
+    assert lib.sphg_gemm_bf16_ws(one, one, 128, 64, 128, a, one, None) != 0      # unsupported (N, K)
+    E.z = None
+    assert lib.sphg_gemm_bf16_ws(one, one, 128, 128, 128, a, one, None) != 0     # STORE without z
+    E.mode = 9
+    assert lib.sphg_gemm_bf16_ws(one, one, 128, 128, 128, a, one, None) != 0     # unknown epilogue

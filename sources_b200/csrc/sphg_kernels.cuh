@@ -34,9 +34,12 @@ struct SimConst {
     const SceneTab* tab;   // per-scene dt, water b and c, soil alpha1 (indexed by PhaseDev::sid)
 };
 
+#ifndef SPHG_TPB
 #define SPHG_TPB 128
-// minimum resident blocks per SM of each pair pass (register cap for the
-// compiler: 65,536 / (SPHG_TPB * min blocks) registers per thread).  Timed on
+#endif
+// minimum resident blocks per SM of each FP32 pair pass (register cap for
+// the compiler: 65,536 / (SPHG_TPB * min blocks) registers per thread); the
+// FP64 passes are left uncapped.  Timed on
 // a B200 at 912,016 particles: water_pass_a 172 -> 148 us at 8 blocks,
 // water_pass_b 234 -> 207 us at 6, cross_water 81 -> 69 us at 8; the soil
 // pass is fastest uncapped (8 blocks: 60 -> 84 us).
@@ -207,6 +210,9 @@ __global__ void __launch_bounds__(256) k_gather(PhaseDev<T> P, SimConst c, int s
         int a = P.perm[k];
         if (fh) fail0 = first_half_one(P, a, c, with_vof, fh_dp);
         P.xs[k] = P.x[a];
+#if SPHG_F32_SCAN
+        P.xsf[k] = make_float2((float)P.x[a].x, (float)P.x[a].y);
+#endif
         P.hs[k] = P.hsml[a];
         double2 v = P.v[a];
         RecA<T> ra;
@@ -299,7 +305,7 @@ __global__ void __launch_bounds__(SPHG_TPB) k_water_sum(PhaseDev<T> P, GridGeom 
     T num = w0 * ma;
     T sx = T(0), sy = T(0);
     const RecA<T>* __restrict__ rec = P.recA;
-    const int hits = visit_batched(hb, g, sc, P.cell_start, P.xs, P.hs, xa, ha, k, valid, [&](int m, T dx, T dy) {
+    const int hits = visit_batched(hb, g, sc, P.cell_start, P.xs, P.xsf, P.hs, xa, ha, k, valid, [&](int m, T dx, T dy) {
         const RecA<T> rb = rec[m];
         T w, sr, r2, mh;
         pair_kernel<T, SKF>(ka, sc, ha, P.hs, m, dx, dy, w, sr, r2, mh);
@@ -331,7 +337,7 @@ __global__ void __launch_bounds__(SPHG_TPB) k_water_sum(PhaseDev<T> P, GridGeom 
 // delta_sph's (dx . grad W) 2 (f_a - f_b) / r^2 is evaluated as 2 s (f_a - f_b)
 // since grad W = s dx.
 template <typename T, int SKF, bool SINGLE>
-__global__ void __launch_bounds__(SPHG_TPB, SPHG_MINB_A) k_water_pass_a(PhaseDev<T> P, GridGeom g, SearchConst sc, SimConst c, DevCounters* cnt) {
+__global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_A : 1) k_water_pass_a(PhaseDev<T> P, GridGeom g, SearchConst sc, SimConst c, DevCounters* cnt) {
     SPHG_HITBUF(T);
     const int k = gtid();
     const bool valid = k < P.n;
@@ -347,7 +353,7 @@ __global__ void __launch_bounds__(SPHG_TPB, SPHG_MINB_A) k_water_pass_a(PhaseDev
     KernelConst<T, SKF> ka;
     ka.init((T)ha);
     T con = 0, dl = 0, t0 = 0, t1 = 0, t2 = 0, t3 = 0;
-    const int hits = visit_batched(hb, g, sc, P.cell_start, P.xs, P.hs, xa, ha, k, valid, [&](int m, T dx, T dy) {
+    const int hits = visit_batched(hb, g, sc, P.cell_start, P.xs, P.xsf, P.hs, xa, ha, k, valid, [&](int m, T dx, T dy) {
         const RecA<T> rb = rec[m];
         T w, sr, r2, mh;
         pair_kernel<T, SKF>(ka, sc, ha, P.hs, m, dx, dy, w, sr, r2, mh);
@@ -414,7 +420,7 @@ __global__ void __launch_bounds__(SPHG_TPB, SPHG_MINB_A) k_water_pass_a(PhaseDev
 // dx = x_real - x_virtual, as the reference does with real particles
 // numbered before virtual ones.
 template <typename T, int SKF, bool SINGLE>
-__global__ void __launch_bounds__(SPHG_TPB, SPHG_MINB_B) k_water_pass_b(PhaseDev<T> P, GridGeom g, SearchConst sc, SimConst c, StepCtl u) {
+__global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_B : 1) k_water_pass_b(PhaseDev<T> P, GridGeom g, SearchConst sc, SimConst c, StepCtl u) {
     typedef typename V2<T>::t T2;
     SPHG_HITBUF(T);
     const int k = gtid();
@@ -439,7 +445,7 @@ __global__ void __launch_bounds__(SPHG_TPB, SPHG_MINB_B) k_water_pass_b(PhaseDev
     ka.init((T)ha);
     T d1x = 0, d1y = 0, d2x = 0, d3x = 0, d2y = 0, d3y = 0;
     T avx = 0, avy = 0, rpx = 0, rpy = 0, dvf = 0, xsx = 0, xsy = 0;
-    visit_batched(hb, g, sc, P.cell_start, P.xs, P.hs, xa, ha, k, valid, [&](int m, T dx, T dy) {
+    visit_batched(hb, g, sc, P.cell_start, P.xs, P.xsf, P.hs, xa, ha, k, valid, [&](int m, T dx, T dy) {
         const RecA<T> rb = rec[m];
         const RecB<T> qb = P.recB[m];
         T w, sr, rr, mh;
@@ -509,7 +515,7 @@ __global__ void __launch_bounds__(SPHG_TPB, SPHG_MINB_B) k_water_pass_b(PhaseDev
 // plastic_or_not :3447, plastic_flow_rule3 :3700 and Jaumann_rate :3047,
 // whose spin sum wxy comes from the same pass.
 template <typename T, int SKF, bool SINGLE>
-__global__ void __launch_bounds__(SPHG_TPB, SPHG_MINB_SOIL) k_soil_pass(PhaseDev<T> P, GridGeom g, SearchConst sc, SimConst c,
+__global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_SOIL : 1) k_soil_pass(PhaseDev<T> P, GridGeom g, SearchConst sc, SimConst c,
                                                        DevCounters* cnt, int slot, StepCtl u) {
     typedef typename V2<T>::t T2;
     SPHG_HITBUF(T);
@@ -539,7 +545,7 @@ __global__ void __launch_bounds__(SPHG_TPB, SPHG_MINB_SOIL) k_soil_pass(PhaseDev
     T s1x = 0, s1y = 0, s2x = 0, s3x = 0, s2y = 0, s3y = 0;
     T avx = 0, avy = 0, rpx = 0, rpy = 0, xsx = 0, xsy = 0;
     T dpp = 0, dsx = 0, dsxy = 0, dsy = 0;
-    const int hits = visit_batched(hb, g, sc, P.cell_start, P.xs, P.hs, xa, ha, k, valid, [&](int m, T dx, T dy) {
+    const int hits = visit_batched(hb, g, sc, P.cell_start, P.xs, P.xsf, P.hs, xa, ha, k, valid, [&](int m, T dx, T dy) {
         const RecA<T> rb = P.recA[m];
         const RecB<T> qb = P.recB[m];
         T w, sr, rr, mh;
@@ -681,7 +687,7 @@ __global__ void __launch_bounds__(SPHG_TPB, SPHG_MINB_SOIL) k_soil_pass(PhaseDev
 // vol_w*rho_w*vof_w*vof_s*(-g/k)*(v_w - v_s)*W/rho_s and the pore pressure
 // m_w p_w/(rho_w rho_s) becomes vol_w p_w / rho_s.
 template <typename T, int SKF>
-__global__ void __launch_bounds__(SPHG_TPB, SPHG_MINB_CROSS) k_cross_soil(PhaseDev<T> S, PhaseDev<T> W, GridGeom g, SearchConst sc, SimConst c,
+__global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_CROSS : 1) k_cross_soil(PhaseDev<T> S, PhaseDev<T> W, GridGeom g, SearchConst sc, SimConst c,
                                                         StepCtl u, DevCounters* cnt) {
     typedef typename V2<T>::t T2;
     SPHG_HITBUF(T);
@@ -697,7 +703,7 @@ __global__ void __launch_bounds__(SPHG_TPB, SPHG_MINB_CROSS) k_cross_soil(PhaseD
     KernelConst<T, SKF> ka;
     ka.init((T)ha);
     T ddx = 0, ddy = 0, dpx = 0, dpy = 0;
-    visit_batched(hb, g, sc, W.cell_start, W.xs, W.hs, xa, ha, -1, valid, [&](int m, T dx, T dy) {
+    visit_batched(hb, g, sc, W.cell_start, W.xs, W.xsf, W.hs, xa, ha, -1, valid, [&](int m, T dx, T dy) {
         const RecA<T> rb = W.recA[m];
         const RecB<T> qb = W.recB[m];
         T w, sr, rr, mh;
@@ -729,7 +735,7 @@ __global__ void __launch_bounds__(SPHG_TPB, SPHG_MINB_CROSS) k_cross_soil(PhaseD
 // volume_fraction_water :3912 (vof2), and every renorm_interval steps the
 // renormalisation rho <- rho/vof*vof2, vof <- vof2 (declarations_sph.f90:1414-1421).
 template <typename T, int SKF>
-__global__ void __launch_bounds__(SPHG_TPB, SPHG_MINB_CROSS) k_cross_water(PhaseDev<T> W, PhaseDev<T> S, GridGeom g, SearchConst sc, SimConst c,
+__global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_CROSS : 1) k_cross_water(PhaseDev<T> W, PhaseDev<T> S, GridGeom g, SearchConst sc, SimConst c,
                                                          DevCounters* cnt, StepCtl u) {
     typedef typename V2<T>::t T2;
     SPHG_HITBUF(T);
@@ -745,7 +751,7 @@ __global__ void __launch_bounds__(SPHG_TPB, SPHG_MINB_CROSS) k_cross_water(Phase
     KernelConst<T, SKF> ka;
     ka.init((T)ha);
     T ddx = 0, ddy = 0, dvof = 0, v2 = 0;
-    const int hits = visit_batched(hb, g, sc, S.cell_start, S.xs, S.hs, xa, ha, -1, valid, [&](int m, T dx, T dy) {
+    const int hits = visit_batched(hb, g, sc, S.cell_start, S.xs, S.xsf, S.hs, xa, ha, -1, valid, [&](int m, T dx, T dy) {
         const RecA<T> rb = S.recA[m];
         const T phis = S.recB[m].vof;
         T w, sr, rr, mh;

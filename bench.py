@@ -203,6 +203,40 @@ def run_ensemble(args, rank, world, torch, dist):
     return 0
 
 
+def learned_arm(solver, scene, torch, plain_value, strides):
+    """The learned stepper on the same scene, beside the plain solver: a
+    history of 5 strides (k = 10 steps) from the plain solver, then `strides`
+    learned strides timed end to end (graph search, network, stride update and
+    the fallback-gate sums, wall clock with a synchronisation per stride), and
+    the plain solver's own strides from the same state as the judge of the
+    position error."""
+    import numpy as np
+    from sources_b200 import learn
+    if not os.path.exists(learn.DEFAULT_WEIGHTS):
+        return {"unavailable": "no trained weights at sources_b200/data/learned_weights.npz"}
+    net = learn.MPNet.from_state(dict(np.load(learn.DEFAULT_WEIGHTS)))
+    hist = learn.scene_rollout(solver, scene, "submerged", learn.HIST)
+    learn.LearnedStepper(net, hist, learn.HIST, "net").step()        # warm-up: buffers, graph
+    st = learn.LearnedStepper(net, hist, learn.HIST, "net")
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(strides):
+        st.step()
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    n = hist.X.shape[1]
+    ref = learn.scene_rollout(solver, scene, "submerged", strides)
+    real = hist.nodes["type"] != learn.GNN_BOUNDARY
+    d = ((st.x - ref.X[-1]).norm(dim=1).cpu().numpy()[real]) / hist.dx
+    value = n * strides * learn.K_STRIDE / wall
+    return {"value": value, "unit": UNIT, "vs_plain": value / plain_value, "stride_steps": learn.K_STRIDE,
+            "strides": strides, "ms_per_stride": wall / strides * 1e3, "edges": int(st.batch.E),
+            "position_error_dx": {"mean": float(d.mean()), "p99": float(np.percentile(d, 99)),
+                                  "max": float(d.max())},
+            "weights": "sources_b200/data/learned_weights.npz (trained on the 4 mm ensemble)",
+            "network": f"message passing, {learn.LAYERS} layers, width {learn.L_WIDTH}, bf16 tcgen05"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -212,6 +246,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--cpu-steps", type=int, default=60)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-stepper arm")
+    ap.add_argument("--learned-strides", type=int, default=5)
     ap.add_argument("--workload", default=WORKLOAD, choices=[WORKLOAD, "two_phase_456k", "ensemble_256"],
                     help="two_phase_456k: the same scene 2.0 m wide (for profiler captures); "
                          "ensemble_256: 256 uneven scenes stepped as three batched groups")
@@ -339,6 +375,10 @@ def main():
            "mode": "every step: upload the full phase state from pinned host arrays, one leapfrog step, "
                    "download the full state (the Fortran host owns its arrays)"}
 
+    learned = None
+    if not args.no_learned and args.workload == WORKLOAD:
+        learned = learned_arm(solver, scene, torch, value / world, args.learned_strides)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(args.cpu_steps)
@@ -357,7 +397,7 @@ def main():
                            "skf": int(scene.params.skf), "parallelism": f"replicas{world}",
                            "l2": "inputs larger than L2 (state ~%.0f MB)" % (n * 250 / 1e6)},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-                "clocks": clocks}
+                "clocks": clocks, "learned": learned}
         print(json.dumps(line))
     return 0
 

@@ -431,8 +431,10 @@ __global__ void k_adam(float* __restrict__ w, const float* __restrict__ g, float
 // ---------------------------------------------------------------- rollout
 
 // one learned stride of length dts (per node): a = pred * std + mean,
-// v' = v + a dts, x' = x + dts (v + v') / 2, clamped inside the walls; the
-// new velocity goes to history slot head_new; boundary nodes stay put
+// v' = v + a dts, x' = x + v' dts (semi-implicit Euler: with v the stride
+// velocity (x - x_prev) / dts and a the stride acceleration, exactly the
+// next position), clamped inside the walls; v' goes to history slot
+// head_new; boundary nodes stay put
 __global__ void k_stride_update(const float* __restrict__ pred, int ld, const float* __restrict__ norm,
                                 const sphg_gnn_node* __restrict__ st, double2* __restrict__ x,
                                 float2* __restrict__ vhist, int head_old, int head_new, int n, double margin) {
@@ -446,8 +448,8 @@ __global__ void k_stride_update(const float* __restrict__ pred, int ld, const fl
         const float ay = pred[(long long)i * ld + 1] * norm[3] + norm[1];
         vn = make_float2(vo.x + ax * s.dts, vo.y + ay * s.dts);
         double2 p = x[i];
-        p.x += (double)s.dts * 0.5 * ((double)vo.x + (double)vn.x);
-        p.y += (double)s.dts * 0.5 * ((double)vo.y + (double)vn.y);
+        p.x += (double)s.dts * (double)vn.x;
+        p.y += (double)s.dts * (double)vn.y;
         p.x = fmin(fmax(p.x, (double)s.xl + margin), (double)s.xr - margin);
         p.y = fmax(p.y, (double)s.yf + margin);
         x[i] = p;

@@ -23,8 +23,13 @@ Network (latent width L = 128, 4 message-passing layers, 2-layer MLPs):
                  e += relu(z) W2^T + b2;  agg = sum of e over received edges / 16;
                  h += relu([h, agg] V1^T + c1) V2^T + c2
     decoder      2-layer MLP to the 2 acceleration components (normalised)
-Stride update (k = 10 solver steps of the scene's dt): v' = v + a k dt,
-x' = x + k dt (v + v') / 2, clamped inside the walls.  Fallback gates: the
+Velocities are finite differences over a stride, v_t = (x_t - x_{t-k}) / D
+with D = k dt (k = 10 solver steps of the scene's dt), and the target is the
+stride acceleration a_t = (x_{t+k} - 2 x_t + x_{t-k}) / D^2: position
+differences average out the acoustic oscillations that the solver's own
+velocities carry at a period of a few steps.  Stride update (semi-implicit
+Euler, exact for the exact a): v' = v + a D, x' = x + v' D, clamped inside
+the walls.  Fallback gates: the
 RMS relative change of the SPH number density over real particles above
 1 %, or a rise of kinetic + potential energy above 5 % of (kinetic energy +
 one dx of potential energy per particle); a failed stride is redone by k
@@ -56,6 +61,8 @@ TARGET_CLAMP = 20.0      # normalised acceleration targets, in std
 HUBER_DELTA = 3.0        # training loss: squared error up to 3 std, linear beyond
 
 GNN_WATER, GNN_SOIL, GNN_BOUNDARY = 0, 1, 2
+DEFAULT_WEIGHTS = __import__("os").path.join(__import__("os").path.dirname(__import__("os").path.abspath(__file__)),
+                                            "data", "learned_weights.npz")
 NODE_DTYPE = np.dtype([("xl", "<f4"), ("xr", "<f4"), ("yf", "<f4"), ("dts", "<f4"), ("porosity", "<f4"),
                        ("phi", "<f4"), ("mass", "<f4"), ("type", "<i4")])
 
@@ -504,11 +511,10 @@ def node_table(scene, offset: float, dts: float, kind: str) -> np.ndarray:
 
 @dataclass
 class GroupRollout:
-    """Snapshots every k steps of one ensemble group (all phases, phase order)."""
+    """Positions every k steps of one ensemble group (all phases, phase order)."""
     kind: str
     nodes: np.ndarray            # NODE_DTYPE [n]
     X: object                    # [T, n, 2] f64 device
-    V: object                    # [T, n, 2] f32 device
     scene_idx: list              # per member: int64 device index of its nodes
     members: list                # ensemble scene indices
     grid: Grid
@@ -563,7 +569,7 @@ def _scene_index(g, torch, device):
 
 def rollout_ensemble(ens, strides: int, device="cuda"):
     """Run every group of an Ensemble for `strides` strides of k steps and
-    keep x (f64) and v (f32) of every particle after each stride (T =
+    keep the positions (f64) of every particle after each stride (T =
     strides + 1 snapshots, the first the initial state)."""
     torch = _torch()
     dev = torch.device(device)
@@ -574,8 +580,6 @@ def rollout_ensemble(ens, strides: int, device="cuda"):
         n_ph = [P.n for P in g.scene.phases]
         n = sum(n_ph)
         X = torch.empty((strides + 1, n, 2), dtype=torch.float64, device=dev)
-        V = torch.empty((strides + 1, n, 2), dtype=torch.float32, device=dev)
-        vtmp = torch.empty((n, 2), dtype=torch.float64, device=dev)
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         steps_ms = 0.0
         for t in range(strides + 1):
@@ -587,12 +591,11 @@ def rollout_ensemble(ens, strides: int, device="cuda"):
                 steps_ms += ev0.elapsed_time(ev1)
             a = 0
             for k, nk in enumerate(n_ph):
-                sv.export_xv(k + 1, X[t, a:a + nk].data_ptr(), vtmp[a:a + nk].data_ptr())
+                sv.export_xv(k + 1, X[t, a:a + nk].data_ptr(), None)
                 a += nk
-            V[t].copy_(vtmp)
         h = float(g.scene.phases[0].hsml[0])
         dx = float(g.scene.phases[0].dspp)
-        r = GroupRollout(g.kind, _group_nodes(ens, g), X, V, _scene_index(g, torch, dev), list(g.members),
+        r = GroupRollout(g.kind, _group_nodes(ens, g), X, _scene_index(g, torch, dev), list(g.members),
                          _group_grid(g, 2.0 * h), 1.0 / (2.0 * h), h, dx,
                          steps_ms / max(strides * K_STRIDE, 1))
         r.boxes = [ens.built[m].box for m in g.members]
@@ -601,18 +604,69 @@ def rollout_ensemble(ens, strides: int, device="cuda"):
     return out
 
 
-def normalisation(rollouts, t0: int = HIST - 1):
-    """Velocity scale and per-component acceleration mean / std over real
-    particles of the training rollouts."""
+def fd_velocity(r: GroupRollout, t: int, idx=None):
+    """Stride velocity (x_t - x_{t-1}) / D of the nodes idx (all when None), f32."""
+    if idx is None:
+        d = r.X[t] - r.X[t - 1]
+        return (d / r.dts_dev.double()[:, None]).float()
+    d = r.X[t].index_select(0, idx) - r.X[t - 1].index_select(0, idx)
+    return (d / r.dts_dev.index_select(0, idx).double()[:, None]).float()
+
+
+def fd_acceleration(r: GroupRollout, t: int, idx):
+    """Stride acceleration (x_{t+1} - 2 x_t + x_{t-1}) / D^2 of the nodes idx (f64)."""
+    x0, x1, x2 = (r.X[t + j].index_select(0, idx) for j in (-1, 0, 1))
+    dts = r.dts_dev.index_select(0, idx).double()[:, None]
+    return (x2 - 2.0 * x1 + x0) / (dts * dts)
+
+
+def scene_rollout(solver, scene, kind: str, strides: int, device="cuda") -> GroupRollout:
+    """Positions of one running single-scene Solver now and after each of
+    `strides` further strides of k steps (T = strides + 1 snapshots)."""
     torch = _torch()
+    dev = torch.device(device)
+    solver.set_stream(torch.cuda.current_stream(dev).cuda_stream)
+    sizes = [P.n for P in scene.phases]
+    n = sum(sizes)
+    X = torch.empty((strides + 1, n, 2), dtype=torch.float64, device=dev)
+    for t in range(strides + 1):
+        if t:
+            solver.time_integration(K_STRIDE)
+        a = 0
+        for k, nk in enumerate(sizes):
+            solver.export_xv(k + 1, X[t, a:a + nk].data_ptr(), None)
+            a += nk
+    h = float(scene.phases[0].hsml[0])
+    p = scene.params
+    radius = 2.0 * h
+    xmin, ymin = p.x_min - 4 * radius, p.y_min - 4 * radius
+    grid = Grid(xmin, ymin, radius, int(math.ceil((p.x_max + 4 * radius - xmin) / radius)) + 1,
+                int(math.ceil((p.y_max + 4 * radius - ymin) / radius)) + 1)
+    nodes = node_table(scene, 0.0, K_STRIDE * p.dt, kind)
+    r = GroupRollout(kind, nodes, X, [torch.arange(n, device=dev)], [0], grid, 1.0 / radius, h,
+                     float(scene.phases[0].dspp))
+    r.boxes = [scene.box]
+    torch.cuda.synchronize(dev)
+    return r.finish(torch, dev)
+
+
+def normalisation(rollouts, t0: int = HIST, snapshots: int = 24, nodes: int = 100_000, seed: int = 0):
+    """Velocity scale and per-component acceleration mean / std over real
+    particles of the training rollouts (stride finite differences), from up
+    to `snapshots` evenly spaced snapshots and `nodes` random real particles
+    of each group."""
+    torch = _torch()
+    g = torch.Generator(device=rollouts[0].X.device)
+    g.manual_seed(seed)
     vs, acc = [], []
     for r in rollouts:
-        typ = torch.from_numpy(r.nodes["type"].copy()).to(r.V.device)
-        real = typ != GNN_BOUNDARY
-        dts = torch.from_numpy(r.nodes["dts"].copy()).to(r.V.device)[real]
-        V = r.V[:, real]
-        vs.append(V[t0:].reshape(-1, 2).double())
-        acc.append(((V[t0 + 1:] - V[t0:-1]) / dts[None, :, None]).reshape(-1, 2).double())
+        real = torch.nonzero(r.typ_dev != GNN_BOUNDARY).flatten()
+        if real.numel() > nodes:
+            real = real[torch.randperm(real.numel(), device=real.device, generator=g)[:nodes]]
+        T = r.X.shape[0]
+        for t in range(t0, T - 1, max(1, (T - 1 - t0) // snapshots)):
+            vs.append(fd_velocity(r, t, real).double())
+            acc.append(fd_acceleration(r, t, real))
     v = torch.cat(vs)
     a = torch.cat(acc)
     vscale = float(v.std().item()) or 1.0
@@ -622,25 +676,25 @@ def normalisation(rollouts, t0: int = HIST - 1):
 
 def sample_batch(net: MPNet, r: GroupRollout, t: int, members: list, noise: float, gen=None) -> Batch:
     """Training batch: the chosen member scenes of a group at snapshot t
-    (HIST - 1 <= t < T - 1); input velocities carry Gaussian noise of
-    std noise * vscale (the target is taken relative to the noisy current
+    (HIST <= t < T - 1); input velocities carry Gaussian noise of std
+    noise * vscale (the target is taken relative to the noisy current
     velocity, so the network learns to correct it)."""
     torch = net.torch
     idx = torch.cat([r.scene_idx[m] for m in members])
     x = r.X[t].index_select(0, idx).contiguous()
-    vh = torch.stack([r.V[t - j].index_select(0, idx) for j in range(HIST)]).contiguous()
+    vh = torch.stack([fd_velocity(r, t - j, idx) for j in range(HIST)]).contiguous()
     nodes = r.nodes_dev.index_select(0, idx).contiguous()
     typ = r.typ_dev.index_select(0, idx)
     dts = r.dts_dev.index_select(0, idx)
+    acc = fd_acceleration(r, t, idx).float()
     if noise > 0:
         nz = torch.randn(vh.shape, device=x.device, generator=gen) * (noise * net.vscale)
         nz[:, typ == GNN_BOUNDARY] = 0
         vh = vh + nz
-    vnext = r.V[t + 1].index_select(0, idx)
-    acc = (vnext - vh[0]) / dts[:, None]
+        acc = acc - nz[0] / dts[:, None]
     nrm = net.norm
-    # heavy tails (wall impacts, acoustic spikes) are clamped at 20 std
-    target = ((acc - nrm[:2]) / nrm[2:]).float().clamp_(-TARGET_CLAMP, TARGET_CLAMP)
+    # heavy tails (wall impacts, splashes) are clamped at 20 std
+    target = ((acc - nrm[:2]) / nrm[2:]).clamp_(-TARGET_CLAMP, TARGET_CLAMP)
     return net.make_batch(x, nodes, vh, 0, r.grid, r.inv2h, target=target)
 
 
@@ -660,7 +714,7 @@ def train(net: MPNet, rollouts, iters: int, lr0=3e-4, lr1=3e-5, batch_nodes=120_
     for it in range(iters):
         r = rollouts[rng.choice(len(rollouts), p=sizes / sizes.sum())]
         T = r.X.shape[0]
-        t = int(rng.integers(HIST - 1, T - 1))
+        t = int(rng.integers(HIST, T - 1))
         order = rng.permutation(len(r.members))
         chosen, total = [], 0
         for m in order:
@@ -687,21 +741,32 @@ def train(net: MPNet, rollouts, iters: int, lr0=3e-4, lr1=3e-5, batch_nodes=120_
 
 class LearnedStepper:
     """Learned strides over one group's particles, starting from snapshot
-    t0 of a rollout (positions and the HIST velocities up to t0).  mode
-    'net' uses the network, 'gravity' the stepper with a = g (the method
-    without the network), both with the same stride update and walls."""
+    t0 of a rollout (positions and the HIST stride velocities up to t0).
+    mode 'net' uses the network, 'gravity' the stepper with a = g (the
+    method without the network), both with the same stride update and walls.
 
-    def __init__(self, net: MPNet, r: GroupRollout, t0: int = HIST - 1, mode: str = "net", solver=None,
+    With a solver (holding the same group at snapshot t0, phase sizes in
+    phase_sizes) the fallback gates are live: a stride that fails them is
+    discarded and the solver, which stays authoritative, advances from the
+    last state it holds to the end of that stride; the learned strides then
+    continue from its positions and stride velocities.  The solver never
+    receives learned positions, so its density and stress fields stay its
+    own."""
+
+    def __init__(self, net: MPNet, r: GroupRollout, t0: int = HIST, mode: str = "net", solver=None,
                  phase_sizes=None):
         torch = net.torch
         self.net, self.r, self.mode = net, r, mode
         dev = net.device
         self.n = r.X.shape[1]
         self.x = r.X[t0].clone()
-        self.vh = torch.stack([r.V[t0 - j] for j in range(HIST)]).contiguous()
+        self.vh = torch.stack([fd_velocity(r, t0 - j) for j in range(HIST)]).contiguous()
         self.head = 0
         self.nodes = r.nodes_dev
         self.solver, self.phase_sizes = solver, phase_sizes
+        # the solver's own trajectory at stride boundaries (oldest first)
+        self.solver_x = [r.X[t0 - j].clone() for j in range(HIST, -1, -1)] if solver is not None else None
+        self.synced = 0            # learned strides done when the solver was last at the same time
         self.sig = [torch.zeros(self.n, dtype=torch.float64, device=dev) for _ in range(2)]
         self.gate = torch.zeros(4, dtype=torch.float64, device=dev)
         typ = r.nodes["type"]
@@ -742,10 +807,9 @@ class LearnedStepper:
         return out
 
     def step(self):
-        """One stride: network, update, gates; a failed stride is redone by
-        the solver.  Returns True when the learned stride was kept."""
+        """One stride: network, update, gates; a failed stride is replaced
+        by the solver's.  Returns True when the learned stride was kept."""
         net = self.net
-        x0, vh0, head0 = self.x.clone(), self.vh.clone(), self.head
         pred = self._pred()
         new = (self.head + HIST - 1) % HIST
         _call(net.L.sphg_gnn_stride_update(_ptr(pred), L_WIDTH, _ptr(net.norm), _ptr(self.nodes), _ptr(self.x),
@@ -759,13 +823,10 @@ class LearnedStepper:
         rms = math.sqrt(g[0] / max(g[1], 1.0))
         rise = (energy - self.energy) / (max(self.energy_ke, 0.0) + self.e_floor)
         self.last_rms, self.last_rise = rms, rise
-        failed = self.solver is not None and (rms > GATE_DENSITY or rise > GATE_ENERGY)
+        failed = self.solver is not None and (not math.isfinite(rms) or rms > GATE_DENSITY or rise > GATE_ENERGY)
         if failed:
             self.fallbacks += 1
-            self.x.copy_(x0)
-            self.vh.copy_(vh0)
-            self.head = head0
-            self._solver_stride()
+            self._catch_up(self.strides + 1)
             self._graph()
             self._density(self.sig[1])
             energy, ke = self._energy(self.sig[1])
@@ -774,23 +835,25 @@ class LearnedStepper:
         self.strides += 1
         return not failed
 
-    def _solver_stride(self):
-        """k plain SPH steps from the current positions and velocities."""
+    def _catch_up(self, upto: int):
+        """The solver advances from the last time it holds to `upto` strides
+        after t0; positions and stride velocities are taken from it."""
         torch = self.net.torch
-        v = self.vh[self.head].double()
-        a = 0
-        for k, nk in enumerate(self.phase_sizes):
-            self.solver.import_xv(k + 1, self.x[a:a + nk].data_ptr(), v[a:a + nk].contiguous().data_ptr())
-            a += nk
-        self.solver.time_integration(K_STRIDE)
-        new = (self.head + HIST - 1) % HIST
-        vt = torch.empty((self.n, 2), dtype=torch.float64, device=self.net.device)
-        a = 0
-        for k, nk in enumerate(self.phase_sizes):
-            self.solver.export_xv(k + 1, self.x[a:a + nk].data_ptr(), vt[a:a + nk].data_ptr())
-            a += nk
-        self.vh[new].copy_(vt)
-        self.head = new
+        for _ in range(upto - self.synced):
+            self.solver.time_integration(K_STRIDE)
+            x = torch.empty_like(self.x)
+            a = 0
+            for k, nk in enumerate(self.phase_sizes):
+                self.solver.export_xv(k + 1, x[a:a + nk].data_ptr(), None)
+                a += nk
+            self.solver_x.append(x)
+            self.solver_x.pop(0)
+        self.synced = upto
+        self.x.copy_(self.solver_x[-1])
+        dts = self.r.dts_dev.double()[:, None]
+        for j in range(HIST):
+            self.vh[j].copy_(((self.solver_x[-1 - j] - self.solver_x[-2 - j]) / dts).float())
+        self.head = 0
 
 
 # -------------------------------------------------------------- evaluation
@@ -821,7 +884,7 @@ def scene_errors(x_pred, x_ref, nodes, kind, box, dx):
     return abs(r_p - r_r) / dx, surf
 
 
-def evaluate(net: MPNet, rollouts, t0: int = HIST - 1, strides: int | None = None, mode="net", solvers=None):
+def evaluate(net: MPNet, rollouts, t0: int = HIST, strides: int | None = None, mode="net", solvers=None):
     """Roll every group out from snapshot t0 for `strides` learned strides and
     compare each scene with the plain solver's snapshot at the same time.
     Returns per-scene errors, timing and fallback counts."""
@@ -895,13 +958,57 @@ def summarise(res: dict) -> dict:
     sc = res["scenes"]
     ro = np.array([r["runout_dx"] for r in sc])
     sf = np.array([r["surface_dx"] for r in sc])
-    return dict(scenes=len(sc), runout_dx_mean=float(np.nanmean(ro)), runout_dx_max=float(np.nanmax(ro)),
-                surface_dx_mean=float(np.nanmean(sf)), surface_dx_max=float(np.nanmax(sf)),
-                within_1dx=float(np.mean((ro <= 1.0) & (sf <= 1.0))),
+    kinds = {}
+    for kind in sorted({r["kind"] for r in sc}):
+        k_ro = np.array([r["runout_dx"] for r in sc if r["kind"] == kind])
+        k_sf = np.array([r["surface_dx"] for r in sc if r["kind"] == kind])
+        kinds[kind] = dict(scenes=int(k_ro.size), runout_dx_mean=float(np.nanmean(k_ro)),
+                           runout_dx_median=float(np.nanmedian(k_ro)), surface_dx_mean=float(np.nanmean(k_sf)),
+                           surface_dx_median=float(np.nanmedian(k_sf)),
+                           within_1dx=float(np.mean((k_ro <= 1.0) & (k_sf <= 1.0))))
+    return dict(scenes=len(sc), runout_dx_mean=float(np.nanmean(ro)), runout_dx_median=float(np.nanmedian(ro)),
+                runout_dx_max=float(np.nanmax(ro)), surface_dx_mean=float(np.nanmean(sf)),
+                surface_dx_median=float(np.nanmedian(sf)), surface_dx_max=float(np.nanmax(sf)),
+                within_1dx=float(np.mean((ro <= 1.0) & (sf <= 1.0))), by_kind=kinds,
                 learned_particle_steps_per_s=res["learned_particle_steps_per_s"],
                 plain_particle_steps_per_s=res["plain_particle_steps_per_s"],
                 speed_vs_plain=res["learned_particle_steps_per_s"] / res["plain_particle_steps_per_s"],
                 fallbacks=res["fallbacks"])
+
+
+def stride_bench(n_scenes: int, strides: int, weights=None):
+    """Learned strides on the largest group of n_scenes held-out scenes (a
+    history of HIST strides from the plain solver first): wall time per
+    stride, forward time (CUDA events) and the graph size, as one JSON line."""
+    import json
+    import os
+    from . import ensemble
+    torch = _torch()
+    _, specs = split_specs(0, n_scenes)
+    ens = ensemble.Ensemble(specs, tune=False)
+    roll = rollout_ensemble(ens, HIST)
+    ens.close()
+    path = weights or (DEFAULT_WEIGHTS if os.path.exists(DEFAULT_WEIGHTS) else None)
+    net = MPNet.from_state(dict(np.load(path))) if path else MPNet(seed=0)
+    r = max(roll, key=lambda q: q.X.shape[1])
+    LearnedStepper(net, r, HIST, "net").step()
+    st = LearnedStepper(net, r, HIST, "net")
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(strides):
+        st.step()
+    torch.cuda.synchronize()
+    wall = (time.perf_counter() - t0) / strides
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(strides):
+        net.forward(st.batch, keep=False)
+    e1.record()
+    e1.synchronize()
+    n = r.X.shape[1]
+    print(json.dumps(dict(nodes=n, edges=int(st.batch.E), kind=r.kind, strides=strides, ms_per_stride=wall * 1e3,
+                          forward_ms=e0.elapsed_time(e1) / strides,
+                          particle_steps_per_s=n * K_STRIDE / wall, weights=path or "random")))
 
 
 def main(argv=None):
@@ -919,8 +1026,12 @@ def main(argv=None):
     ap.add_argument("--weights", default=None, help="write the trained weights (.npz)")
     ap.add_argument("--load", default=None, help="evaluate these weights instead of training")
     ap.add_argument("--report", default=None, help="write the JSON report")
+    ap.add_argument("--stride-bench", type=int, default=0, metavar="S",
+                    help="only time S learned strides on the first --test held-out scenes (no training)")
     a = ap.parse_args(argv)
     torch = _torch()
+    if a.stride_bench:
+        return stride_bench(a.test, a.stride_bench, a.load)
     strides = a.steps // K_STRIDE
     train_specs, test_specs = split_specs(a.pool, a.test)
     report = dict(config=dict(pool=a.pool, train_scenes=len(train_specs), test_scenes=len(test_specs),
@@ -953,9 +1064,9 @@ def main(argv=None):
     held = rollout_ensemble(ens_t, strides)
     ens_t.close()
     ens_f = ensemble.Ensemble(test_specs, tune=False)
-    solvers = _fallback_solvers(ens_f, HIST - 1)
-    res_net = evaluate(net, held, HIST - 1, mode="net", solvers=solvers)
-    res_grav = evaluate(net, held, HIST - 1, mode="gravity")
+    solvers = _fallback_solvers(ens_f, HIST)
+    res_net = evaluate(net, held, HIST, mode="net", solvers=solvers)
+    res_grav = evaluate(net, held, HIST, mode="gravity")
     ens_f.close()
     report["learned"] = summarise(res_net)
     report["gravity_only"] = summarise(res_grav)

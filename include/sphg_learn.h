@@ -53,8 +53,7 @@ int sphg_gemm_bf16_ws(const void* A, const void* B, int M, int N, int K, const S
  * Message-passing network kernels.  Feature matrices are row-major bf16 or
  * fp32 with the row count padded to a multiple of 128; L is the latent
  * width, which must be 128 (the width the kernels are compiled for; other
- * values return SPHG_ERR_BAD_ARG); element counts n are multiples of 4 and
- * bias_act takes 64, 128 or 256 columns.  Graphs are CSR by receiver: off[n + 1] (int64), src[e] and dst[e]
+ * values return SPHG_ERR_BAD_ARG); element counts n are multiples of 4.  Graphs are CSR by receiver: off[n + 1] (int64), src[e] and dst[e]
  * (int32), receivers in node order.
  * ------------------------------------------------------------------- */
 
@@ -103,11 +102,6 @@ int sphg_gnn_edge_features(const double* x, const sphg_gnn_node* nodes, const in
                            long long nedge, long long nedge_pad, double inv2h, void* out_bf16, void* cuda_stream);
 
 int sphg_gnn_f32_to_bf16(const float* x, void* y_bf16, long long n, void* cuda_stream);
-/* z += b (broadcast over rows); h = relu(z) (relu != 0) or z, in bf16 */
-int sphg_gnn_bias_act(float* z, const float* b, void* h_bf16, long long rows, int cols, int relu, void* cuda_stream);
-/* fused edge first layer: z += P[src, :L] + P[dst, L:] + b, a = relu(z) */
-int sphg_gnn_edge_gather_act(float* z, const float* P, const int* src, const int* dst, const float* b, void* a_bf16,
-                             long long nedge, long long nedge_pad, int L, void* cuda_stream);
 int sphg_gnn_relu_bwd(const float* dh, const float* z, float* dz, void* dz_bf16, long long n, void* cuda_stream);
 /* out[c] += sum_r x[r, c] */
 int sphg_gnn_colsum(const float* x, long long rows, int cols, float* out, void* cuda_stream);
@@ -134,7 +128,7 @@ int sphg_gnn_adam(float* w, const float* g, float* m, float* v, void* w_bf16, vo
                   float lr, float beta1, float beta2, float eps, int step, int row_limit, void* cuda_stream);
 
 /* learned stride: a = pred[:, :2] * norm[2:4] + norm[0:2]; v' = v + a dts;
- * x += dts (v + v') / 2 clamped to the walls (margin); v' -> slot head_new */
+ * x += v' dts clamped to the walls (margin); v' -> slot head_new */
 int sphg_gnn_stride_update(const float* pred, int ld, const float* norm, const sphg_gnn_node* nodes, double* x,
                            float* vhist, int head_old, int head_new, int n, double margin, void* cuda_stream);
 /* sigma_i = 1 + sum over received edges of the cubic-spline shape W(r/h) */

@@ -41,8 +41,6 @@ EXPORTS = ("sphg_default_params", "sphg_create", "sphg_upload_phase", "sphg_sing
                "sphg_gnn_node_features": "PPIPIIFFPP",
                "sphg_gnn_edge_features": "PPPPLLDPP",
                "sphg_gnn_f32_to_bf16": "PPLP",
-               "sphg_gnn_bias_act": "PPPLIIP",
-               "sphg_gnn_edge_gather_act": "PPPPPPLLIP",
                "sphg_gnn_relu_bwd": "PPPPLP",
                "sphg_gnn_colsum": "PLIPP",
                "sphg_gnn_transpose": "PIPLIP",

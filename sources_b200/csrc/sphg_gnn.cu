@@ -8,10 +8,10 @@
 //   features   node inputs (velocity history, type, wall distances, scene
 //              constants) and edge inputs (offset / radius, distance, same
 //              type) as bf16 rows of 64
-//   layers     fused edge first layer (GEMM output + gathered node
-//              projections + bias, ReLU), bias (+ReLU), segment sums,
-//              concatenations, their backward passes, transposes for the
-//              weight-gradient GEMMs, column sums, loss, Adam
+//   layers     segment sums, concatenations and their backward passes,
+//              ReLU backward, transposes for the weight-gradient GEMMs,
+//              column sums, loss, Adam (bias, activation and the edge
+//              layer's gathers are fused into the GEMM epilogues)
 //   rollout    stride update of velocity history and position, the
 //              number-density and energy sums of the fallback gates
 // Feature matrices are row-major (feature index contiguous) with the row
@@ -216,39 +216,6 @@ __global__ void k_edge_features(const double2* __restrict__ x, const sphg_gnn_no
 __global__ void k_f32_to_bf16(const float4* __restrict__ x, uint2* __restrict__ y, long long n4) {
     const long long i = gid();
     if (i < n4) y[i] = pack4(x[i]);
-}
-
-// z += b; h = relu(z) or z, in bf16; rows of C
-template <int C>
-__global__ void k_bias_act(float* __restrict__ z, const float* __restrict__ b, bf16* __restrict__ h, long long rows,
-                           int relu) {
-    long long r;
-    int lane;
-    row_lane<C / 4>(r, lane);
-    if (r >= rows) return;
-    float4* zr = reinterpret_cast<float4*>(z + r * C);
-    const float4 v = add4(zr[lane], reinterpret_cast<const float4*>(b)[lane]);
-    zr[lane] = v;
-    reinterpret_cast<uint2*>(h + r * C)[lane] = pack4(relu ? relu4(v) : v);
-}
-
-// fused edge first layer: z[k] (= e_k W_e^T from the GEMM) += P[src][:L] +
-// P[dst][L:] + b; a = relu(z)
-__global__ void k_edge_gather_act(float* __restrict__ z, const float* __restrict__ P, const int* __restrict__ src,
-                                  const int* __restrict__ dst, const float* __restrict__ b, bf16* __restrict__ a,
-                                  long long nedge, long long nedge_pad) {
-    long long k;
-    int lane;
-    row_lane<LW / 4>(k, lane);
-    if (k >= nedge_pad) return;
-    float4* zr = reinterpret_cast<float4*>(z + k * LW);
-    float4 v = add4(zr[lane], reinterpret_cast<const float4*>(b)[lane]);
-    if (k < nedge) {
-        v = add4(v, reinterpret_cast<const float4*>(P + (long long)src[k] * 2 * LW)[lane]);
-        v = add4(v, reinterpret_cast<const float4*>(P + (long long)dst[k] * 2 * LW + LW)[lane]);
-    }
-    zr[lane] = v;
-    reinterpret_cast<uint2*>(a + k * LW)[lane] = pack4(relu4(v));
 }
 
 // dz = dh * (z > 0), fp32 and bf16; n % 4 == 0
@@ -593,19 +560,6 @@ int sphg_gnn_edge_features(const double* x, const sphg_gnn_node* st, const int* 
 int sphg_gnn_f32_to_bf16(const float* x, void* y, long long n, void* stream) {
     if (n % 4) return SPHG_ERR_BAD_ARG;
     LAUNCH1(k_f32_to_bf16, n / 4, (const float4*)x, (uint2*)y, n / 4);
-}
-
-int sphg_gnn_bias_act(float* z, const float* b, void* h, long long rows, int cols, int relu, void* stream) {
-    if (cols == 64) ROWS(k_bias_act<64>, rows, 16, z, b, (bf16*)h, rows, relu);
-    if (cols == 128) ROWS(k_bias_act<128>, rows, 32, z, b, (bf16*)h, rows, relu);
-    if (cols == 256) ROWS(k_bias_act<256>, rows, 64, z, b, (bf16*)h, rows, relu);
-    return SPHG_ERR_BAD_ARG;
-}
-
-int sphg_gnn_edge_gather_act(float* z, const float* P, const int* src, const int* dst, const float* b, void* a,
-                             long long nedge, long long nedge_pad, int L, void* stream) {
-    if (L != LW || nedge_pad < nedge) return SPHG_ERR_BAD_ARG;
-    ROWS(k_edge_gather_act, nedge_pad, LW / 4, z, P, src, dst, b, (bf16*)a, nedge, nedge_pad);
 }
 
 int sphg_gnn_relu_bwd(const float* dh, const float* z, float* dz, void* dzb, long long n, void* stream) {

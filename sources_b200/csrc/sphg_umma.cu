@@ -237,71 +237,102 @@ struct WsShape {
     static constexpr int PER_SM = N == 256 || SMEM > 110 * 1024 ? 1 : 2;
 };
 
+constexpr int WS_THREADS = 256;   // 8 warps: warps w and w + 4 share TMEM lanes 32 (w % 4) ..
+
 template <int N, int K>
 __device__ __forceinline__ void ws_load_a(uint8_t* sA, const __nv_bfloat16* __restrict__ A, int m0, int tid) {
     constexpr int KC = K / 8;
 #pragma unroll 4
-    for (int c = tid; c < 128 * KC; c += 128) {
+    for (int c = tid; c < 128 * KC; c += WS_THREADS) {
         const int r = c / KC, kc = c % KC;
         cp_async16(smem_u32(sA + kc * WsShape<N, K>::A_KC + (r >> 3) * 128 + (r & 7) * 16),
                    A + (size_t)(m0 + r) * K + kc * 8);
     }
 }
 
-template <int N, int K>
-__device__ __forceinline__ void ws_epilogue(const SphgGemmEpi& ep, uint32_t tacc, long long row) {
-#pragma unroll 1
-    for (int c = 0; c < N; c += 8) {
-        uint32_t r[8];
-        asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-                     : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-                       "=r"(r[7])
-                     : "r"(tacc + (uint32_t)c));
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        float v[8];
+__device__ __forceinline__ float4 add4f(float4 a, float4 b) {
+    return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w);
+}
+
+// 16 accumulator columns of this thread's TMEM lane
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-        for (int j = 0; j < 8; ++j) v[j] = __uint_as_float(r[j]);
-        float4* z4 = ep.z ? reinterpret_cast<float4*>(ep.z + row * N + c) : nullptr;
-        if (ep.mode == SPHG_EPI_STORE) {
-            z4[0] = make_float4(v[0], v[1], v[2], v[3]);
-            z4[1] = make_float4(v[4], v[5], v[6], v[7]);
-            continue;
+    for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
+}
+
+// Epilogue of one row (this thread's TMEM lane) over columns [c0, c0 + N/2)
+// in chunks of 16: every global input of a chunk (residual row, gathered
+// projection rows, bias) is requested before the TMEM read, so a thread has
+// up to 12 16-byte loads in flight; each chunk writes 64 contiguous bytes of
+// the fp32 row and 32 of the bf16 row.
+template <int N, int K>
+__device__ __forceinline__ void ws_epilogue(const SphgGemmEpi& ep, uint32_t tacc, long long row, int c0) {
+    constexpr int CW = 16;
+    const bool edge = ep.mode == SPHG_EPI_EDGE && row < ep.nedge;
+    const float4* ps = nullptr;
+    const float4* pd = nullptr;
+    if (edge) {
+        ps = reinterpret_cast<const float4*>(ep.P + (long long)ep.src[row] * 2 * N);
+        pd = reinterpret_cast<const float4*>(ep.P + (long long)ep.dst[row] * 2 * N + N);
+    }
+    const bool readz = ep.mode == SPHG_EPI_ACC || ep.mode == SPHG_EPI_RESID;
+    const bool bias = ep.mode != SPHG_EPI_STORE && ep.mode != SPHG_EPI_ACC;
+    float4* zr = ep.z ? reinterpret_cast<float4*>(ep.z + row * N) : nullptr;
+#pragma unroll 1
+    for (int c = c0; c < c0 + N / 2; c += CW) {
+        float4 add[CW / 4];
+#pragma unroll
+        for (int j = 0; j < CW / 4; ++j) add[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (readz) {
+#pragma unroll
+            for (int j = 0; j < CW / 4; ++j) add[j] = zr[c / 4 + j];
         }
-        if (ep.mode == SPHG_EPI_ACC || ep.mode == SPHG_EPI_RESID) {
-            const float4 a = z4[0], b = z4[1];
-            v[0] += a.x; v[1] += a.y; v[2] += a.z; v[3] += a.w;
-            v[4] += b.x; v[5] += b.y; v[6] += b.z; v[7] += b.w;
+        if (edge) {
+            float4 a[CW / 4], b[CW / 4];
+#pragma unroll
+            for (int j = 0; j < CW / 4; ++j) { a[j] = ps[c / 4 + j]; b[j] = pd[c / 4 + j]; }
+#pragma unroll
+            for (int j = 0; j < CW / 4; ++j) add[j] = add4f(add[j], add4f(a[j], b[j]));
         }
-        if (ep.mode != SPHG_EPI_ACC) {
-            const float4 b0 = reinterpret_cast<const float4*>(ep.bias + c)[0];
-            const float4 b1 = reinterpret_cast<const float4*>(ep.bias + c)[1];
-            v[0] += b0.x; v[1] += b0.y; v[2] += b0.z; v[3] += b0.w;
-            v[4] += b1.x; v[5] += b1.y; v[6] += b1.z; v[7] += b1.w;
+        if (bias) {
+            const float4* b4 = reinterpret_cast<const float4*>(ep.bias + c);
+#pragma unroll
+            for (int j = 0; j < CW / 4; ++j) add[j] = add4f(add[j], b4[j]);
         }
-        if (ep.mode == SPHG_EPI_EDGE && row < ep.nedge) {
-            const float4* ps = reinterpret_cast<const float4*>(ep.P + (long long)ep.src[row] * 2 * N + c);
-            const float4* pd = reinterpret_cast<const float4*>(ep.P + (long long)ep.dst[row] * 2 * N + N + c);
-            const float4 s0 = ps[0], s1 = ps[1], d0 = pd[0], d1 = pd[1];
-            v[0] += s0.x + d0.x; v[1] += s0.y + d0.y; v[2] += s0.z + d0.z; v[3] += s0.w + d0.w;
-            v[4] += s1.x + d1.x; v[5] += s1.y + d1.y; v[6] += s1.z + d1.z; v[7] += s1.w + d1.w;
+        float v[CW];
+        tmem_ld16(tacc + (uint32_t)c, v);
+#pragma unroll
+        for (int j = 0; j < CW / 4; ++j) {
+            v[4 * j] += add[j].x; v[4 * j + 1] += add[j].y; v[4 * j + 2] += add[j].z; v[4 * j + 3] += add[j].w;
         }
-        if (z4) {
-            z4[0] = make_float4(v[0], v[1], v[2], v[3]);
-            z4[1] = make_float4(v[4], v[5], v[6], v[7]);
+        if (zr) {
+#pragma unroll
+            for (int j = 0; j < CW / 4; ++j)
+                zr[c / 4 + j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
         }
-        if (ep.mode != SPHG_EPI_ACC && ep.h) {
+        if (ep.mode != SPHG_EPI_STORE && ep.mode != SPHG_EPI_ACC && ep.h) {
             const bool act = ep.mode == SPHG_EPI_EDGE || (ep.mode == SPHG_EPI_BIAS_ACT && ep.relu);
             if (act) {
 #pragma unroll
-                for (int j = 0; j < 8; ++j) v[j] = fmaxf(v[j], 0.f);
+                for (int j = 0; j < CW; ++j) v[j] = fmaxf(v[j], 0.f);
             }
-            *reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(ep.h) + row * N + c) = bf16x8(v);
+            uint4* hr = reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(ep.h) + row * N + c);
+#pragma unroll
+            for (int j = 0; j < CW / 8; ++j) hr[j] = bf16x8(v + 8 * j);
         }
     }
 }
 
 template <int N, int K>
-__global__ void __launch_bounds__(128, 1) k_gemm_ws(const __nv_bfloat16* __restrict__ A,
+__global__ void __launch_bounds__(WS_THREADS, 2) k_gemm_ws(const __nv_bfloat16* __restrict__ A,
                                                     const __nv_bfloat16* __restrict__ B, int M, SphgGemmEpi ep,
                                                     int* __restrict__ err) {
     typedef WsShape<N, K> S;
@@ -327,7 +358,7 @@ __global__ void __launch_bounds__(128, 1) k_gemm_ws(const __nv_bfloat16* __restr
     }
     // resident B in the canonical K-major layout
     constexpr int KC = K / 8;
-    for (int c = tid; c < N * KC; c += 128) {
+    for (int c = tid; c < N * KC; c += WS_THREADS) {
         const int r = c / KC, kc = c % KC;
         *reinterpret_cast<uint4*>(sB + kc * S::B_KC + (r >> 3) * 128 + (r & 7) * 16) =
             *reinterpret_cast<const uint4*>(B + (size_t)r * K + kc * 8);
@@ -341,7 +372,8 @@ __global__ void __launch_bounds__(128, 1) k_gemm_ws(const __nv_bfloat16* __restr
     asm volatile("tcgen05.fence::after_thread_sync;" ::);
     const uint32_t tmem = *tslot;
     const uint32_t idesc = make_idesc(N);
-    const uint32_t lane_off = (uint32_t)(warp * 32) << 16;
+    const uint32_t lane_off = (uint32_t)((warp & 3) * 32) << 16;
+    const int col0 = (warp >> 2) * (N / 2);    // the column half of this warp
     uint32_t ph = 0u;    // bit s: parity of the next completion of mbar[s]
     bool ok = true;
     int issued = 0, waited = 0;   // MMA steps issued, and seen complete
@@ -386,7 +418,8 @@ __global__ void __launch_bounds__(128, 1) k_gemm_ws(const __nv_bfloat16* __restr
         asm volatile("tcgen05.fence::after_thread_sync;" ::);
         if (i + 1 < my) ws_load_a<N, K>(sA0 + p * S::A_BYTES, A, tile_m0(i + 1), tid);
         cp_async_commit();
-        ws_epilogue<N, K>(ep, tmem + lane_off + (uint32_t)(p * N), (long long)tile_m0(i - 1) + warp * 32 + lane);
+        ws_epilogue<N, K>(ep, tmem + lane_off + (uint32_t)(p * N), (long long)tile_m0(i - 1) + (warp & 3) * 32 + lane,
+                          col0);
         asm volatile("tcgen05.fence::before_thread_sync;" ::);
         __syncthreads();
     }
@@ -398,7 +431,8 @@ __global__ void __launch_bounds__(128, 1) k_gemm_ws(const __nv_bfloat16* __restr
             ph ^= 1u << s;
             ++waited;
             asm volatile("tcgen05.fence::after_thread_sync;" ::);
-            ws_epilogue<N, K>(ep, tmem + lane_off + (uint32_t)(s * N), (long long)tile_m0(my - 1) + warp * 32 + lane);
+            ws_epilogue<N, K>(ep, tmem + lane_off + (uint32_t)(s * N),
+                              (long long)tile_m0(my - 1) + (warp & 3) * 32 + lane, col0);
         }
     }
     if (!ok) {
@@ -433,7 +467,7 @@ int launch_ws(const __nv_bfloat16* A, const __nv_bfloat16* B, int M, const SphgG
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int ntiles = M / 128;
     const int grid = ntiles < sms * S::PER_SM ? ntiles : sms * S::PER_SM;
-    k_gemm_ws<N, K><<<grid, 128, S::SMEM_REQ, s>>>(A, B, M, ep, err);
+    k_gemm_ws<N, K><<<grid, WS_THREADS, S::SMEM_REQ, s>>>(A, B, M, ep, err);
     return cudaGetLastError() == cudaSuccess ? SPHG_OK : SPHG_ERR_CUDA;
 }
 

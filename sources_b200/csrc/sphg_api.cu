@@ -351,6 +351,12 @@ struct Engine : EngineBase {
             if (!(v > 0.0) || !std::isfinite(v)) return SPHG_ERR_BAD_ARG;
             lo = std::min(lo, v); hi = std::max(hi, v);
         }
+        // same particles again (size, material, h range): refill the arrays in
+        // the current state order and keep the grid, the cell order and the
+        // captured graphs
+        if (have[ph] && prepared && P[ph].n == n && P[ph].ntotal == h->ntotal && P[ph].material == h->material &&
+            hrange[ph][0] == lo && hrange[ph][1] == hi)
+            return refill(ph, h);
         hrange[ph][0] = lo; hrange[ph][1] = hi;
         // original order == state order until the first reorder
         if ((rc = launch("iota", k_iota, blocks(n, 256), 256, n, D.orig))) return rc;
@@ -376,6 +382,43 @@ struct Engine : EngineBase {
         prepared = false;
         aliased = false;
         drop_graphs();
+        CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        return 0;
+    }
+
+    // host (original order) -> state order through the current permutation
+    template <typename S>
+    int fill(int n, const int* orig, const double* src, S* dst, int comps) {
+        if (!src) { CUDA_TRY(cudaMemsetAsync(dst, 0, sizeof(S) * (size_t)n * comps, ctx->stream)); return 0; }
+        CUDA_TRY(cudaMemcpyAsync(stage, src, sizeof(double) * (size_t)n * comps, cudaMemcpyHostToDevice, ctx->stream));
+        return launch("refill", k_from_original<S>, blocks(n, 256), 256, n, orig, (const double*)stage, dst, comps);
+    }
+    int refill(int ph, const sphg_phase_host* h) {
+        PhaseDev<T>& D = P[ph];
+        const int n = D.n;
+        const int* o = D.orig;
+        D.dspp = h->dspp;
+        int rc = 0;
+        rc |= fill(n, o, h->x, (double*)D.x, 2); rc |= fill(n, o, h->vx, (double*)D.v, 2);
+        rc |= fill(n, o, h->v_min, (double*)D.v_min, 2);
+        rc |= fill(n, o, h->rho, D.rho, 1); rc |= fill(n, o, h->rho_min, D.rho_min, 1);
+        rc |= fill(n, o, h->vof, D.vof, 1); rc |= fill(n, o, h->vof_min, D.vof_min, 1);
+        rc |= fill(n, o, h->p, D.p, 1); rc |= fill(n, o, h->c, D.c, 1); rc |= fill(n, o, h->mass, D.mass, 1);
+        rc |= fill(n, o, h->hsml, D.hsml, 1);
+        rc |= fill(n, o, h->sxx, D.sxx, 1); rc |= fill(n, o, h->sxy, D.sxy, 1); rc |= fill(n, o, h->syy, D.syy, 1);
+        rc |= fill(n, o, h->sxx_min, D.sxx_min, 1); rc |= fill(n, o, h->sxy_min, D.sxy_min, 1);
+        rc |= fill(n, o, h->syy_min, D.syy_min, 1); rc |= fill(n, o, h->p_min, D.p_min, 1);
+        rc |= fill(n, o, h->epsilon_p, D.eps_p, 1);
+        rc |= fill(n, o, h->drho, D.drho, 1); rc |= fill(n, o, h->dvof, D.dvof, 1);
+        rc |= fill(n, o, h->dsxx, D.dsxx, 1); rc |= fill(n, o, h->dsxy, D.dsxy, 1); rc |= fill(n, o, h->dsyy, D.dsyy, 1);
+        rc |= fill(n, o, h->dp, D.dp, 1); rc |= fill(n, o, h->dvx, (T*)D.dv, 2); rc |= fill(n, o, h->av, (T*)D.av, 2);
+        rc |= fill(n, o, h->vof2, D.vof2, 1); rc |= fill(n, o, h->vcc, D.vcc, 1);
+        rc |= fill(n, o, h->txx, D.txx, 1); rc |= fill(n, o, h->tyy, D.tyy, 1); rc |= fill(n, o, h->txy, D.txy, 1);
+        if (rc) return SPHG_ERR_CUDA;
+        CUDA_TRY(cudaMemcpyAsync(stage_i, h->itype, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, ctx->stream));
+        if (launch("refill", k_from_original_i, blocks(n, 256), 256, n, o, (const int*)stage_i, D.itype))
+            return SPHG_ERR_CUDA;
+        aliased = false;
         CUDA_TRY(cudaStreamSynchronize(ctx->stream));
         return 0;
     }

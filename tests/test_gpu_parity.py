@@ -156,6 +156,28 @@ def test_restart_and_determinism(cuda_ok, name, precision):
                     assert np.array_equal(getattr(a, f), getattr(c, f)), ("restart", f)
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [SPHG_FP64, SPHG_FP32])
+def test_host_round_trip_keeps_the_trajectory(cuda_ok, precision):
+    """A host that downloads the state and uploads it again every step (the
+    same particles: the in-place refill path, which keeps the cell order and
+    the captured graphs) follows the uninterrupted trajectory bit for bit."""
+    s = scenes.small("two_phase", precision=precision)
+    with Solver(s) as full, Solver(s) as trip:
+        full.time_integration(23)
+        trip.time_integration(12)                   # past the first reorder
+        for _ in range(3):
+            host = [trip.download(k + 1) for k in range(len(s.phases))]
+            for k, P in enumerate(host):
+                trip.upload(k + 1, P)
+            trip.time_integration(1)
+        trip.time_integration(8)
+        for k in range(len(s.phases)):
+            a, b = full.download(k + 1), trip.download(k + 1)
+            for f in ("x", "vx", "rho", "p", "sxx", "vof", "drho", "dvx", "epsilon_p"):
+                assert np.array_equal(getattr(a, f), getattr(b, f)), f
+
+
 def test_working_array_aliasing_after_two_phase_step(cuda_ok):
     """Water sxx/syy/sxy are the shared txx/tyy/txy arrays, which the soil
     pass overwrites (declarations_sph.f90:371-377,414-415)."""

@@ -119,51 +119,88 @@ def ncu_traffic():
         return {}
 
 
-def cpu_baseline(steps: int):
-    """The oracle port of the serial reference step on a sub-domain sample of
-    the workload (same spacing and physics, 1.0 m wide, 0.2 m of water)."""
+SUBDOMAIN = dict(width=1.0, height=1.0, block_w=0.25, block_h=0.1, water_h=0.2)
+SUBDOMAIN_TEXT = "1.0 m x 0.2 m water, 0.25 m x 0.1 m soil block, dx 0.002 m"
+
+
+def _oracle_worker(args):
+    """One serial oracle on its own copy of the sub-domain; every worker
+    starts its timed steps behind the same barrier."""
+    steps, warmup, barrier = args
+    os.environ["OMP_NUM_THREADS"] = "1"
+    sys.path.insert(0, ROOT)
     from oracle import Oracle
     from sources_b200 import scenes
-    s = scenes.two_phase(width=1.0, height=1.0, block_w=0.25, block_h=0.1, water_h=0.2)
+    s = scenes.two_phase(**SUBDOMAIN)
     o = Oracle(s)
-    o.time_integration(1)
+    rc = o.time_integration(warmup)
+    barrier.wait()
     t0 = time.perf_counter()
-    rc = o.time_integration(steps)
-    dt = time.perf_counter() - t0
-    if rc:
-        raise RuntimeError(f"oracle step failed: {rc}")
-    n = s.n_particles
-    return {"value": n * steps / dt, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"serial C restatement of the Fortran step, {steps} leapfrog steps of a {n}-particle "
-                      f"sub-domain of the workload (1.0 m x 0.2 m water, 0.25 m x 0.1 m soil block, dx 0.002 m)",
+    rc = rc or o.time_integration(steps)
+    return s.n_particles, time.perf_counter() - t0, rc
+
+
+def host_cores() -> int:
+    """Host threads this process may run on (SPHG_HOST_CORES caps it)."""
+    try:
+        n = len(os.sched_getaffinity(0))
+    except AttributeError:
+        n = os.cpu_count() or 1
+    cap = int(os.environ.get("SPHG_HOST_CORES", "0") or 0)
+    return min(n, cap) if cap > 0 else n
+
+
+def oracle_throughput(steps: int, warmup: int, cores: int):
+    """The serial C restatement of the reference step (the reference's own
+    path is serial) on every host core at once: one independent instance per
+    core, each on its own copy of a 62,266-particle sub-domain of the workload.
+    Aggregate particle-steps/s = all instances' particle-steps / the slowest
+    instance's time (all start together).  Spawned processes: no fork after
+    the CUDA context exists."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    mgr = ctx.Manager()
+    barrier = mgr.Barrier(cores)
+    with ctx.Pool(cores) as pool:
+        res = pool.map(_oracle_worker, [(steps, warmup, barrier)] * cores)
+    mgr.shutdown()
+    if any(r[2] for r in res):
+        raise RuntimeError(f"oracle step failed: {[r[2] for r in res]}")
+    n = res[0][0]
+    dt = max(r[1] for r in res)
+    return n, dt, n * steps * cores / dt
+
+
+def cpu_baseline(steps: int, cores: int | None = None):
+    """The oracle port of the serial reference step, one instance per host
+    core on a sub-domain sample of the workload (same spacing and physics)."""
+    cores = cores or host_cores()
+    n, dt, v = oracle_throughput(steps, 1, cores)
+    return {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"serial C restatement of the Fortran step, one instance per core on {cores} cores, each "
+                      f"{steps} leapfrog steps of its own {n}-particle sub-domain of the workload ({SUBDOMAIN_TEXT})",
             "seconds": dt}
 
 
 def run_reference(args, rank, world):
     if rank != 0:
         return 0
-    from oracle import Oracle
-    from sources_b200 import scenes
-    s = scenes.two_phase(width=1.0, height=1.0, block_w=0.25, block_h=0.1, water_h=0.2)
-    o = Oracle(s)
-    o.time_integration(args.warmup)
-    t0 = time.perf_counter()
-    rc = o.time_integration(args.steps)
-    dt = time.perf_counter() - t0
-    if rc:
-        print(json.dumps({"impl": "reference", "unavailable": f"oracle step failed with status {rc}"}))
+    cores = host_cores()
+    try:
+        n, dt, v = oracle_throughput(args.steps, args.warmup, cores)
+    except RuntimeError as e:
+        print(json.dumps({"impl": "reference", "unavailable": str(e)}))
         return 0
-    n = s.n_particles
-    v = n * args.steps / dt
     sample = (f"serial C restatement of the Fortran step (the reference has no compilable C/CUDA and no Fortran "
-              f"compiler is present); each step is one leapfrog step of a {n}-particle sub-domain of the workload")
+              f"compiler is present), one instance per host core on {cores} cores; each step is one leapfrog step "
+              f"of every instance's own {n}-particle sub-domain of the workload ({SUBDOMAIN_TEXT})")
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * dt / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (deterministic lattice scene)",
-            "config": {"workload": WORKLOAD, "particles": 912016, "sample_particles": n,
+            "config": {"workload": WORKLOAD, "particles": 912016, "sample_particles": n, "instances": cores,
                        "precision": "fp64 (reference)", "l2": "state larger than L2"},
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0

@@ -22,6 +22,7 @@ the same workload at the same spacing.
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -280,7 +281,9 @@ def main():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--e2e-steps", type=int, default=100, help="steps of the end-to-end reference loop")
+    ap.add_argument("--full-state-steps", type=int, default=5,
+                    help="steps of the end-to-end run that copies the full state every step")
     ap.add_argument("--cpu-steps", type=int, default=60)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-stepper arm")
@@ -310,7 +313,7 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
 
     from sources_b200 import Solver, build, replicas, scenes
-    from sources_b200.abi import SPHG_FP32
+    from sources_b200.abi import SPHG_FP32, Stats
 
     build.build()
     if args.workload == "ensemble_256":
@@ -393,24 +396,52 @@ def main():
     for k in range(len(host)):
         solver.download(k + 1, into=host[k])
     torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    t0 = time.perf_counter()
-    for _ in range(args.e2e_steps):
+    state_bytes = sum(P.nbytes() for P in host)
+    stats_bytes = ctypes.sizeof(Stats)
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        t0 = time.perf_counter()
+        fn()
+        torch.cuda.synchronize()
+        return replicas.max_over_ranks(time.perf_counter() - t0, dist if world > 1 else None, device="cuda")
+
+    # The reference's own host loop (declarations_sph.f90:535-885): the input
+    # state goes in once, every step is one call whose statistics come back,
+    # the full state comes out at the output step.
+    def reference_loop():
         for k, P in enumerate(host):
             solver.upload(k + 1, P)
-        solver.time_integration(1)
+        for _ in range(args.e2e_steps):
+            solver.time_integration(1)
+            solver.stats()
         for k in range(len(host)):
             solver.download(k + 1, into=host[k])
-    torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
-    e2e_s = replicas.max_over_ranks(e2e_s, dist if world > 1 else None, device="cuda")
-    bytes_per_step = sum(P.nbytes() for P in host)
-    e2e = {"value": world * n * args.e2e_steps / e2e_s, "unit": UNIT,
-           "h2d_bytes_per_step": bytes_per_step, "d2h_bytes_per_step": bytes_per_step,
-           "steps": args.e2e_steps,
-           "mode": "every step: upload the full phase state from pinned host arrays, one leapfrog step, "
-                   "download the full state (the Fortran host owns its arrays)"}
+
+    # A host that owns every array and hands all of them over every step.
+    def full_state():
+        for _ in range(args.full_state_steps):
+            for k, P in enumerate(host):
+                solver.upload(k + 1, P)
+            solver.time_integration(1)
+            for k in range(len(host)):
+                solver.download(k + 1, into=host[k])
+
+    e2e_s = timed(reference_loop)
+    full_s = timed(full_state)
+    K = args.e2e_steps
+    e2e = {"value": world * n * K / e2e_s, "unit": UNIT,
+           "h2d_bytes_per_step": (state_bytes + K * 16) / K,
+           "d2h_bytes_per_step": (state_bytes + K * stats_bytes) / K, "steps": K,
+           "mode": "the reference's time loop through the C ABI on pinned host arrays: upload the full state, "
+                   "then every step one sphg_time_integration call (itimestep and time in, status out) and its "
+                   "statistics read back (sphg_stats), then download the full state (the output step)",
+           "full_state_every_step": {"value": world * n * args.full_state_steps / full_s, "unit": UNIT,
+                                     "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes,
+                                     "steps": args.full_state_steps,
+                                     "mode": "every step: upload the full state, one step, download the full state"}}
 
     learned = None
     if not args.no_learned and args.workload == WORKLOAD:

@@ -112,6 +112,14 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
+def ncu_issue():
+    try:
+        with open(os.path.join(ROOT, "profiles", "ncu_issue.json")) as f:
+            return json.load(f)["warp_instructions_per_particle"]
+    except Exception:
+        return {}
+
+
 def ncu_traffic():
     try:
         with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
@@ -373,9 +381,24 @@ def main():
     tr = ncu_traffic().get(top_name)
     step_bytes = STEP_BYTES["water"] * scene.phases[0].n + STEP_BYTES["soil"] * scene.phases[1].n
     step_ms = ms / args.steps
+    # issue roofline of the same kernel: warp instructions per launch (ncu count
+    # per particle x particles) over the live launch time, against 4 schedulers
+    # x 1 warp-instruction per clock per SM at the SM clock seen under load
+    ipp = ncu_issue()
+    sms = torch.cuda.get_device_properties(local).multi_processor_count
+    mhz = (clocks or {}).get("sm_mhz") or 1965.0
+    issue_peak = sms * 4 * mhz * 1e6
+
+    def issue(name, ms_launch, particles):
+        if name not in ipp:
+            return None
+        inst = ipp[name] * particles
+        return {"warp_inst_per_launch": inst, "achieved": inst / (ms_launch / 1000.0), "peak": issue_peak,
+                "unit": "warp-inst/s", "frac": inst / (ms_launch / 1000.0) / issue_peak}
     roofline = {"bound": "hbm", "kernel": top_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": peak_kind, "traffic": tr,
                 "alg_bytes_per_launch": alg, "avg_launch_ms": avg_ms,
+                "issue": issue(top_name, avg_ms, units),
                 "step": {"alg_bytes": step_bytes, "achieved_gbs": step_bytes / (step_ms / 1000.0) / 1e9,
                          "frac": step_bytes / (step_ms / 1000.0) / 1e9 / peak},
                 "kernels_ms_per_step": {k: v[1] / args.steps for k, v in kern.items()},
@@ -385,7 +408,10 @@ def main():
                                "achieved_gbs": ALG_BYTES[k] * (scene.phases[1].n if k in ("soil_pass", "cross_soil")
                                                                else scene.phases[0].n)
                                / (kern[k][1] / max(kern[k][0], 1) / 1000.0) / 1e9,
-                               "traffic": ncu_traffic().get(k)}
+                               "traffic": ncu_traffic().get(k),
+                               "issue": issue(k, kern[k][1] / max(kern[k][0], 1),
+                                              scene.phases[1].n if k in ("soil_pass", "cross_soil")
+                                              else scene.phases[0].n)}
                            for k in ALG_BYTES if k in kern}}
 
     # ---- end to end through the C ABI with pinned host buffers

@@ -39,6 +39,7 @@ from __future__ import annotations
 
 import ctypes as C
 import math
+import os
 import time
 from dataclasses import dataclass, field
 
@@ -61,8 +62,7 @@ TARGET_CLAMP = 20.0      # normalised acceleration targets, in std
 HUBER_DELTA = 3.0        # training loss: squared error up to 3 std, linear beyond
 
 GNN_WATER, GNN_SOIL, GNN_BOUNDARY = 0, 1, 2
-DEFAULT_WEIGHTS = __import__("os").path.join(__import__("os").path.dirname(__import__("os").path.abspath(__file__)),
-                                            "data", "learned_weights.npz")
+DEFAULT_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "learned_weights.npz")
 NODE_DTYPE = np.dtype([("xl", "<f4"), ("xr", "<f4"), ("yf", "<f4"), ("dts", "<f4"), ("porosity", "<f4"),
                        ("phi", "<f4"), ("mass", "<f4"), ("type", "<i4")])
 
@@ -699,7 +699,7 @@ def sample_batch(net: MPNet, r: GroupRollout, t: int, members: list, noise: floa
 
 
 def train(net: MPNet, rollouts, iters: int, lr0=3e-4, lr1=3e-5, batch_nodes=120_000, noise=0.002, seed=0,
-          log_every=0, delta=HUBER_DELTA):
+          log_every=0, delta=HUBER_DELTA, balance=False):
     """Adam on random (group, snapshot, member subset) batches with a Huber
     loss; the learning rate decays exponentially from lr0 to lr1.  The
     weights with the lowest running loss (exponential average over ~50
@@ -708,7 +708,9 @@ def train(net: MPNet, rollouts, iters: int, lr0=3e-4, lr1=3e-5, batch_nodes=120_
     rng = np.random.Generator(np.random.PCG64(seed))
     gen = torch.Generator(device=net.device)
     gen.manual_seed(seed)
-    sizes = np.array([sum(int(r.scene_idx[m].numel()) for m in range(len(r.members))) for r in rollouts], float)
+    # groups drawn by particle count, or each kind (group) equally often
+    sizes = np.array([1.0 if balance else sum(int(r.scene_idx[m].numel()) for m in range(len(r.members)))
+                      for r in rollouts], float)
     losses = []
     ema, best, best_w = None, math.inf, None
     for it in range(iters):
@@ -981,7 +983,6 @@ def stride_bench(n_scenes: int, strides: int, weights=None):
     history of HIST strides from the plain solver first): wall time per
     stride, forward time (CUDA events) and the graph size, as one JSON line."""
     import json
-    import os
     from . import ensemble
     torch = _torch()
     _, specs = split_specs(0, n_scenes)
@@ -1023,6 +1024,7 @@ def main(argv=None):
     ap.add_argument("--batch-nodes", type=int, default=120_000)
     ap.add_argument("--lr", type=float, nargs=2, default=(3e-4, 2e-5))
     ap.add_argument("--noise", type=float, default=0.002)
+    ap.add_argument("--balance", action="store_true", help="draw each scene kind equally often")
     ap.add_argument("--weights", default=None, help="write the trained weights (.npz)")
     ap.add_argument("--load", default=None, help="evaluate these weights instead of training")
     ap.add_argument("--report", default=None, help="write the JSON report")
@@ -1036,7 +1038,7 @@ def main(argv=None):
     train_specs, test_specs = split_specs(a.pool, a.test)
     report = dict(config=dict(pool=a.pool, train_scenes=len(train_specs), test_scenes=len(test_specs),
                               steps=a.steps, stride=K_STRIDE, iters=a.iters, batch_nodes=a.batch_nodes,
-                              lr=list(a.lr), noise=a.noise, width=L_WIDTH, layers=LAYERS))
+                              lr=list(a.lr), noise=a.noise, balance=a.balance, width=L_WIDTH, layers=LAYERS))
     t0 = time.perf_counter()
     if a.load:
         net = MPNet.from_state(dict(np.load(a.load)))
@@ -1050,7 +1052,8 @@ def main(argv=None):
         net.vscale, nrm = normalisation(roll)
         net.norm.copy_(torch.tensor(nrm))
         t1 = time.perf_counter()
-        losses = train(net, roll, a.iters, a.lr[0], a.lr[1], a.batch_nodes, a.noise, log_every=250)
+        losses = train(net, roll, a.iters, a.lr[0], a.lr[1], a.batch_nodes, a.noise, log_every=250,
+                       balance=a.balance)
         torch.cuda.synchronize()
         report["train_s"] = time.perf_counter() - t1
         report["loss_first_100"] = float(np.mean(losses[:100]))

@@ -261,7 +261,8 @@ def learned_arm(solver, scene, torch, plain_value, strides):
     if not os.path.exists(learn.DEFAULT_WEIGHTS):
         return {"unavailable": "no trained weights at sources_b200/data/learned_weights.npz"}
     net = learn.MPNet.from_state(dict(np.load(learn.DEFAULT_WEIGHTS)))
-    hist = learn.scene_rollout(solver, scene, "submerged", learn.HIST)
+    x0 = torch.from_numpy(np.concatenate([P.x for P in scene.phases])).to("cuda")   # the initial lattice
+    hist = learn.scene_rollout(solver, scene, "submerged", learn.HIST, x0=x0)
     learn.LearnedStepper(net, hist, learn.HIST, "net").step()        # warm-up: buffers, graph
     st = learn.LearnedStepper(net, hist, learn.HIST, "net")
     torch.cuda.synchronize()
@@ -271,7 +272,7 @@ def learned_arm(solver, scene, torch, plain_value, strides):
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0
     n = hist.X.shape[1]
-    ref = learn.scene_rollout(solver, scene, "submerged", strides)
+    ref = learn.scene_rollout(solver, scene, "submerged", strides, x0=x0)
     real = hist.nodes["type"] != learn.GNN_BOUNDARY
     d = ((st.x - ref.X[-1]).norm(dim=1).cpu().numpy()[real]) / hist.dx
     value = n * strides * learn.K_STRIDE / wall

@@ -94,12 +94,17 @@ int sphg_gnn_graph_fill(const sphg_gnn_grid* grid, const double* x, int n, const
                         const int64_t* off, int* src, int* dst, void* cuda_stream);
 
 /* node rows: 5 velocities (newest first, / vscale), type one-hot, wall
- * distances / 2h clipped to [0, 1], porosity, friction angle, stride (ms) */
-int sphg_gnn_node_features(const double* x, const float* vhist, int head, const sphg_gnn_node* nodes, int n,
-                           int n_pad, float inv2h, float inv_vscale, void* out_bf16, void* cuda_stream);
-/* edge rows: (x_dst - x_src) / 2h, distance / 2h, same-type flag */
-int sphg_gnn_edge_features(const double* x, const sphg_gnn_node* nodes, const int* src, const int* dst,
-                           long long nedge, long long nedge_pad, double inv2h, void* out_bf16, void* cuda_stream);
+ * distances / 2h clipped to [0, 1], porosity, friction angle, stride (ms),
+ * displacement (x - x0) / 2h clipped to [-16, 16] (zero when x0 is NULL) */
+int sphg_gnn_node_features(const double* x, const double* x0, const float* vhist, int head,
+                           const sphg_gnn_node* nodes, int n, int n_pad, float inv2h, float inv_vscale, void* out_bf16,
+                           void* cuda_stream);
+/* edge rows: (x_dst - x_src) / 2h, distance / 2h, same-type flag, change of
+ * that offset since the reference positions x0 (clipped to [-4, 4]; zero
+ * when x0 is NULL) */
+int sphg_gnn_edge_features(const double* x, const double* x0, const sphg_gnn_node* nodes, const int* src,
+                           const int* dst, long long nedge, long long nedge_pad, double inv2h, void* out_bf16,
+                           void* cuda_stream);
 
 int sphg_gnn_f32_to_bf16(const float* x, void* y_bf16, long long n, void* cuda_stream);
 int sphg_gnn_relu_bwd(const float* dh, const float* z, float* dz, void* dz_bf16, long long n, void* cuda_stream);

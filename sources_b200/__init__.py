@@ -38,8 +38,8 @@ EXPORTS = ("sphg_default_params", "sphg_create", "sphg_upload_phase", "sphg_sing
                "sphg_gnn_scan_bytes": "IP",
                "sphg_gnn_graph_count": "PPIPPPPPPLP",
                "sphg_gnn_graph_fill": "PPIPPPPPP",
-               "sphg_gnn_node_features": "PPIPIIFFPP",
-               "sphg_gnn_edge_features": "PPPPLLDPP",
+               "sphg_gnn_node_features": "PPPIPIIFFPP",
+               "sphg_gnn_edge_features": "PPPPPLLDPP",
                "sphg_gnn_f32_to_bf16": "PPLP",
                "sphg_gnn_relu_bwd": "PPPPLP",
                "sphg_gnn_colsum": "PLIPP",

@@ -6,8 +6,9 @@
 //              sort, per-receiver degree, CSR fill: edges grouped by
 //              receiver, receivers in node order, senders in cell-scan order
 //   features   node inputs (velocity history, type, wall distances, scene
-//              constants) and edge inputs (offset / radius, distance, same
-//              type) as bf16 rows of 64
+//              constants, displacement since a reference state) and edge
+//              inputs (offset / radius, distance, same type, change of the
+//              offset since the reference state) as bf16 rows of 64
 //   layers     segment sums, concatenations and their backward passes,
 //              ReLU backward, transposes for the weight-gradient GEMMs,
 //              column sums, loss, Adam (bias, activation and the edge
@@ -159,9 +160,9 @@ __device__ __forceinline__ float4 relu4(float4 a) {
 }
 
 // node rows of 64 bf16, 8 threads per row, 8 features each
-__global__ void k_node_features(const double2* __restrict__ x, const float2* __restrict__ vhist, int head,
-                                const sphg_gnn_node* __restrict__ st, int n, int n_pad, float inv2h, float inv_vscale,
-                                bf16* __restrict__ out) {
+__global__ void k_node_features(const double2* __restrict__ x, const double2* __restrict__ x0,
+                                const float2* __restrict__ vhist, int head, const sphg_gnn_node* __restrict__ st, int n,
+                                int n_pad, float inv2h, float inv_vscale, bf16* __restrict__ out) {
     long long i;
     int lane;
     row_lane<FW / 8>(i, lane);
@@ -184,15 +185,20 @@ __global__ void k_node_features(const double2* __restrict__ x, const float2* __r
             } else if (f == 16) v[k] = s.porosity;
             else if (f == 17) v[k] = s.phi;
             else if (f == 18) v[k] = s.dts * 1.0e3f;
+            else if (f < 21 && x0) {     // displacement since the reference state / 2h
+                const double d = f == 19 ? x[i].x - x0[i].x : x[i].y - x0[i].y;
+                v[k] = fminf(fmaxf((float)d * inv2h, -16.f), 16.f);
+            }
         }
     }
     reinterpret_cast<uint4*>(out)[i * (FW / 8) + lane] = pack8(v);
 }
 
 // edge rows of 64 bf16: (x_dst - x_src) / 2h, distance / 2h, same type
-__global__ void k_edge_features(const double2* __restrict__ x, const sphg_gnn_node* __restrict__ st,
-                                const int* __restrict__ src, const int* __restrict__ dst, long long nedge,
-                                long long nedge_pad, double inv2h, bf16* __restrict__ out) {
+__global__ void k_edge_features(const double2* __restrict__ x, const double2* __restrict__ x0,
+                                const sphg_gnn_node* __restrict__ st, const int* __restrict__ src,
+                                const int* __restrict__ dst, long long nedge, long long nedge_pad, double inv2h,
+                                bf16* __restrict__ out) {
     long long k;
     int lane;
     row_lane<FW / 8>(k, lane);
@@ -206,6 +212,11 @@ __global__ void k_edge_features(const double2* __restrict__ x, const sphg_gnn_no
         v[1] = (float)dy;
         v[2] = (float)sqrt(dx * dx + dy * dy);
         v[3] = st[a].type == st[b].type ? 1.f : 0.f;
+        if (x0) {   // change of the offset since the reference state / 2h: the local strain
+            const double2 p0 = x0[a], q0 = x0[b];
+            v[4] = fminf(fmaxf((float)(dx - (p0.x - q0.x) * inv2h), -4.f), 4.f);
+            v[5] = fminf(fmaxf((float)(dy - (p0.y - q0.y) * inv2h), -4.f), 4.f);
+        }
     }
     reinterpret_cast<uint4*>(out)[k * (FW / 8) + lane] = pack8(v);
 }
@@ -544,17 +555,18 @@ inline unsigned row_blocks(long long rows, int tpr) { return nb(rows, 256 / tpr)
         return ok_or_cuda();                                                                  \
     } while (0)
 
-int sphg_gnn_node_features(const double* x, const float* vhist, int head, const sphg_gnn_node* st, int n, int n_pad,
-                           float inv2h, float inv_vscale, void* out, void* stream) {
+int sphg_gnn_node_features(const double* x, const double* x0, const float* vhist, int head, const sphg_gnn_node* st,
+                           int n, int n_pad, float inv2h, float inv_vscale, void* out, void* stream) {
     if (head < 0 || head >= SPHG_GNN_HISTORY || n_pad < n) return SPHG_ERR_BAD_ARG;
-    ROWS(k_node_features, n_pad, FW / 8, (const double2*)x, (const float2*)vhist, head, st, n, n_pad, inv2h,
-         inv_vscale, (bf16*)out);
+    ROWS(k_node_features, n_pad, FW / 8, (const double2*)x, (const double2*)x0, (const float2*)vhist, head, st, n,
+         n_pad, inv2h, inv_vscale, (bf16*)out);
 }
 
-int sphg_gnn_edge_features(const double* x, const sphg_gnn_node* st, const int* src, const int* dst, long long nedge,
-                           long long nedge_pad, double inv2h, void* out, void* stream) {
+int sphg_gnn_edge_features(const double* x, const double* x0, const sphg_gnn_node* st, const int* src, const int* dst,
+                           long long nedge, long long nedge_pad, double inv2h, void* out, void* stream) {
     if (nedge_pad < nedge) return SPHG_ERR_BAD_ARG;
-    ROWS(k_edge_features, nedge_pad, FW / 8, (const double2*)x, st, src, dst, nedge, nedge_pad, inv2h, (bf16*)out);
+    ROWS(k_edge_features, nedge_pad, FW / 8, (const double2*)x, (const double2*)x0, st, src, dst, nedge, nedge_pad,
+         inv2h, (bf16*)out);
 }
 
 int sphg_gnn_f32_to_bf16(const float* x, void* y, long long n, void* stream) {

@@ -225,6 +225,8 @@ class MPNet:
         self.err = t.zeros(1, dtype=t.int32, device=self.device)
         self.loss_buf = t.zeros(1, dtype=t.float32, device=self.device)
         self.adam_step = 0
+        # inputs include the displacement since the reference positions
+        self.use_x0 = True
         # normalisation: velocity scale, acceleration mean (2) and std (2)
         self.vscale = 1.0
         self.norm = t.tensor([0.0, 0.0, 1.0, 1.0], dtype=t.float32, device=self.device)
@@ -243,6 +245,7 @@ class MPNet:
     def state(self) -> dict:
         d = self.weights()
         d["_vscale"] = np.array([self.vscale], np.float64)
+        d["_x0"] = np.array([1 if self.use_x0 else 0], np.int32)
         d["_norm"] = self.norm.cpu().numpy()
         return d
 
@@ -250,6 +253,7 @@ class MPNet:
     def from_state(cls, d: dict, device="cuda"):
         net = cls({k: v for k, v in d.items() if not k.startswith("_")}, device=device)
         net.vscale = float(d["_vscale"][0])
+        net.use_x0 = bool(int(np.asarray(d.get("_x0", [0]))[0]))
         net.norm.copy_(net.torch.from_numpy(np.asarray(d["_norm"], np.float32)))
         return net
 
@@ -457,19 +461,22 @@ class MPNet:
             raise SPHError(6, "tcgen05 GEMM wait timed out")
 
     # --------------------------------------------------------------- batch
-    def make_batch(self, x, nodes, vhist, head: int, grid: Grid, inv2h: float, target=None) -> Batch:
+    def make_batch(self, x, nodes, vhist, head: int, grid: Grid, inv2h: float, target=None, x0=None) -> Batch:
         """Graph, node and edge features of the particles x [n, 2] (f64,
-        device) with velocity history vhist [5, n, 2] (f32) at ring slot head."""
+        device) with velocity history vhist [5, n, 2] (f32) at ring slot head
+        and reference positions x0 [n, 2] (f64; the displacement features
+        stay zero for a network trained without them, or without x0)."""
         t = self.torch
         n = x.shape[0]
         off, src, dst, E = self.graph.build(x, n, grid, self.stream)
         Np, Ep = pad128(n), pad128(E)
         fn = self.bufs.get("fn", (Np, F_IN), t.bfloat16)
         fe = self.bufs.get("fe", (Ep, F_IN), t.bfloat16)
-        self._k("sphg_gnn_node_features", _ptr(x), _ptr(vhist), head, _ptr(nodes), n, Np, inv2h,
+        ref = x0 if self.use_x0 else None
+        self._k("sphg_gnn_node_features", _ptr(x), _ptr(ref), _ptr(vhist), head, _ptr(nodes), n, Np, inv2h,
                 1.0 / self.vscale, _ptr(fn), self.stream)
-        self._k("sphg_gnn_edge_features", _ptr(x), _ptr(nodes), _ptr(src), _ptr(dst), E, Ep, float(inv2h),
-                _ptr(fe), self.stream)
+        self._k("sphg_gnn_edge_features", _ptr(x), _ptr(ref), _ptr(nodes), _ptr(src), _ptr(dst), E, Ep,
+                float(inv2h), _ptr(fe), self.stream)
         b = Batch(n, Np, E, Ep, x, nodes, off, src, dst, fn, fe)
         if target is not None:
             b.target = self.bufs.get("target", (Np, NOUT), t.float32)
@@ -524,12 +531,15 @@ class GroupRollout:
     plain_ms: float = 0.0        # device time of the plain solver per step
     boxes: list = field(default_factory=list)
     scene_idx_np: list = field(default_factory=list)
+    x0: object = None            # [n, 2] f64 reference positions (the first snapshot)
     nodes_dev: object = None     # [n, 32] uint8
     typ_dev: object = None       # [n] int32
     dts_dev: object = None       # [n] f32
 
     def finish(self, torch, device):
         self.scene_idx_np = [i.cpu().numpy() for i in self.scene_idx]
+        if self.x0 is None:
+            self.x0 = self.X[0]
         self.nodes_dev = torch.from_numpy(self.nodes.view(np.uint8).reshape(-1, 32).copy()).to(device)
         self.typ_dev = torch.from_numpy(self.nodes["type"].copy()).to(device)
         self.dts_dev = torch.from_numpy(self.nodes["dts"].copy()).to(device)
@@ -620,9 +630,11 @@ def fd_acceleration(r: GroupRollout, t: int, idx):
     return (x2 - 2.0 * x1 + x0) / (dts * dts)
 
 
-def scene_rollout(solver, scene, kind: str, strides: int, device="cuda") -> GroupRollout:
+def scene_rollout(solver, scene, kind: str, strides: int, device="cuda", x0=None) -> GroupRollout:
     """Positions of one running single-scene Solver now and after each of
-    `strides` further strides of k steps (T = strides + 1 snapshots)."""
+    `strides` further strides of k steps (T = strides + 1 snapshots).  The
+    reference positions are x0 when given (e.g. the scene's initial
+    lattice), else the first snapshot."""
     torch = _torch()
     dev = torch.device(device)
     solver.set_stream(torch.cuda.current_stream(dev).cuda_stream)
@@ -646,6 +658,8 @@ def scene_rollout(solver, scene, kind: str, strides: int, device="cuda") -> Grou
     r = GroupRollout(kind, nodes, X, [torch.arange(n, device=dev)], [0], grid, 1.0 / radius, h,
                      float(scene.phases[0].dspp))
     r.boxes = [scene.box]
+    if x0 is not None:
+        r.x0 = x0
     torch.cuda.synchronize(dev)
     return r.finish(torch, dev)
 
@@ -695,7 +709,8 @@ def sample_batch(net: MPNet, r: GroupRollout, t: int, members: list, noise: floa
     nrm = net.norm
     # heavy tails (wall impacts, splashes) are clamped at 20 std
     target = ((acc - nrm[:2]) / nrm[2:]).clamp_(-TARGET_CLAMP, TARGET_CLAMP)
-    return net.make_batch(x, nodes, vh, 0, r.grid, r.inv2h, target=target)
+    return net.make_batch(x, nodes, vh, 0, r.grid, r.inv2h, target=target,
+                          x0=r.x0.index_select(0, idx).contiguous())
 
 
 def train(net: MPNet, rollouts, iters: int, lr0=3e-4, lr1=3e-5, batch_nodes=120_000, noise=0.002, seed=0,
@@ -792,7 +807,8 @@ class LearnedStepper:
         return float(g[2] + g[3]), float(g[2])
 
     def _graph(self):
-        self.batch = self.net.make_batch(self.x, self.nodes, self.vh, self.head, self.r.grid, self.r.inv2h)
+        self.batch = self.net.make_batch(self.x, self.nodes, self.vh, self.head, self.r.grid, self.r.inv2h,
+                                         x0=self.r.x0)
 
     def _density(self, out):
         b = self.batch

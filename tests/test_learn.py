@@ -184,6 +184,25 @@ def test_features_match_definition(cuda_ok):
 
 
 @pytest.mark.gpu
+def test_displacement_features(cuda_ok):
+    """Node columns 19-20: (x - x0) / 2h; edge columns 4-5: the change of the
+    edge offset since x0, / 2h (the local strain of the reference state)."""
+    import torch
+    net, b0 = _net_and_batch()
+    x = b0.x.clone()
+    rng = np.random.default_rng(7)
+    x0 = x - torch.from_numpy(rng.uniform(-0.003, 0.003, size=tuple(x.shape))).cuda()
+    b = net.make_batch(x, b0.nodes, torch.zeros((learn.HIST, b0.n, 2), device="cuda"), 0,
+                       learn.Grid(-0.02, -0.02, 2 * 0.0048, 30, 30), 1.0 / (2 * 0.0048), x0=x0)
+    fn, fe = b.fn.float().cpu().numpy(), b.fe.float().cpu().numpy()
+    d = ((x - x0).cpu().numpy()) / (2 * 0.0048)
+    assert np.allclose(fn[:b.n, 19:21], d, atol=1e-2, rtol=1e-2)
+    s_, t_ = b.src[:b.E].cpu().numpy(), b.dst[:b.E].cpu().numpy()
+    assert np.allclose(fe[:b.E, 4:6], d[t_] - d[s_], atol=1e-2, rtol=1e-2)
+    assert not fe[:b.E, 6:].any() and not fn[:b.n, 21:].any()
+
+
+@pytest.mark.gpu
 def test_forward_matches_fp64_reference(cuda_ok):
     net, b = _net_and_batch()
     out = net.forward(b, keep=True).cpu().numpy()[:b.n]

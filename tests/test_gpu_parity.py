@@ -241,3 +241,25 @@ def test_full_size_two_phase_pairs_and_fp32_vs_fp64(cuda_ok):
                 continue
             assert np.all(np.isfinite(getattr(a32[k], f))), f
             assert ferr(getattr(a32[k], f), ref) <= tol, (k + 1, f)
+
+
+def test_full_size_determinism_and_restart_fp32(cuda_ok):
+    """The 912,016-particle benchmark workload in FP32 mode: two runs of 14
+    steps (across the reorder at step 10) are bit-identical, and so is a run
+    restarted from a download at step 7."""
+    s = scenes.two_phase(precision=SPHG_FP32)
+    with Solver(s) as a, Solver(s) as b:
+        a.time_integration(14)
+        b.time_integration(7)
+        s2 = s.copy()
+        s2.phases = [b.download(k + 1) for k in range(2)]
+        it, t = b.itimestep, b.time
+        b.time_integration(7)
+        with Solver(s2) as c:
+            c.itimestep, c.time = it, t
+            c.time_integration(7)
+            for k in range(2):
+                da, db, dc = a.download(k + 1), b.download(k + 1), c.download(k + 1)
+                for f in ("x", "vx", "rho", "p", "sxx", "vof", "drho", "dvx"):
+                    assert np.array_equal(getattr(da, f), getattr(db, f)), ("determinism", k + 1, f)
+                    assert np.array_equal(getattr(da, f), getattr(dc, f)), ("restart", k + 1, f)

@@ -46,6 +46,13 @@ module sphg_iface
      type(c_ptr) :: itype = c_null_ptr, fail = c_null_ptr
   end type
 
+  type, bind(C) :: sphg_stats_t
+     integer(c_int64_t) :: niac(3)
+     integer(c_int32_t) :: maxiac(2), miniac(2), noiac(2)
+     integer(c_int32_t) :: nfail, n_out_of_domain, itimestep, pad
+     real(c_double) :: time, last_step_ms
+  end type
+
   interface
      subroutine sphg_default_params(p) bind(C, name="sphg_default_params")
        import :: sphg_params
@@ -90,6 +97,46 @@ module sphg_iface
        integer(c_int32_t), intent(out) :: pair_i(*), pair_j(*)
        integer(c_int64_t), value :: cap
        integer(c_int64_t), intent(out) :: n
+     end function
+     ! interaction statistics and nfail of the last step (interaction_statistics)
+     integer(c_int) function sphg_stats(ctx, out) bind(C, name="sphg_stats")
+       import :: sphg_stats_t, c_int, c_ptr
+       type(c_ptr), value :: ctx
+       type(sphg_stats_t), intent(out) :: out
+     end function
+     ! Tecplot output of every phase (output, declarations_sph.f90:1703); the
+     ! paths end with c_null_char, path_second and the zone arrays may be c_null_ptr
+     integer(c_int) function sphg_write_tecplot(ctx, path_first, path_second, append, zone_first, zone_second) &
+          bind(C, name="sphg_write_tecplot")
+       import :: c_int, c_ptr, c_char
+       type(c_ptr), value :: ctx
+       character(kind=c_char), intent(in) :: path_first(*)
+       type(c_ptr), value :: path_second
+       integer(c_int), value :: append
+       type(c_ptr), value :: zone_first, zone_second
+     end function
+     ! run the context on a caller's CUDA stream (c_null_ptr: its own stream)
+     integer(c_int) function sphg_set_stream(ctx, stream) bind(C, name="sphg_set_stream")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: ctx, stream
+     end function
+     integer(c_int) function sphg_kernel_profile(ctx, enable) bind(C, name="sphg_kernel_profile")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: ctx
+       integer(c_int), value :: enable
+     end function
+     ! positions / velocities of one phase to or from DEVICE arrays (original order)
+     integer(c_int) function sphg_export_xv_device(ctx, phase, x_dev, v_dev) bind(C, name="sphg_export_xv_device")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: ctx
+       integer(c_int), value :: phase
+       type(c_ptr), value :: x_dev, v_dev
+     end function
+     integer(c_int) function sphg_import_xv_device(ctx, phase, x_dev, v_dev) bind(C, name="sphg_import_xv_device")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: ctx
+       integer(c_int), value :: phase
+       type(c_ptr), value :: x_dev, v_dev
      end function
      subroutine sphg_destroy(ctx) bind(C, name="sphg_destroy")
        import :: c_ptr

@@ -714,7 +714,7 @@ def sample_batch(net: MPNet, r: GroupRollout, t: int, members: list, noise: floa
 
 
 def train(net: MPNet, rollouts, iters: int, lr0=3e-4, lr1=3e-5, batch_nodes=120_000, noise=0.002, seed=0,
-          log_every=0, delta=HUBER_DELTA, balance=False):
+          log_every=0, delta=HUBER_DELTA, balance=False, kind_weight=None):
     """Adam on random (group, snapshot, member subset) batches with a Huber
     loss; the learning rate decays exponentially from lr0 to lr1.  The
     weights with the lowest running loss (exponential average over ~50
@@ -726,6 +726,8 @@ def train(net: MPNet, rollouts, iters: int, lr0=3e-4, lr1=3e-5, batch_nodes=120_
     # groups drawn by particle count, or each kind (group) equally often
     sizes = np.array([1.0 if balance else sum(int(r.scene_idx[m].numel()) for m in range(len(r.members)))
                       for r in rollouts], float)
+    if kind_weight:
+        sizes *= np.array([kind_weight.get(r.kind, 1.0) for r in rollouts])
     losses = []
     ema, best, best_w = None, math.inf, None
     for it in range(iters):
@@ -1041,6 +1043,8 @@ def main(argv=None):
     ap.add_argument("--lr", type=float, nargs=2, default=(3e-4, 2e-5))
     ap.add_argument("--noise", type=float, default=0.002)
     ap.add_argument("--balance", action="store_true", help="draw each scene kind equally often")
+    ap.add_argument("--kind-weight", nargs=2, action="append", metavar=("KIND", "W"), default=[],
+                    help="multiply the draw probability of a scene kind (repeatable)")
     ap.add_argument("--weights", default=None, help="write the trained weights (.npz)")
     ap.add_argument("--load", default=None, help="evaluate these weights instead of training")
     ap.add_argument("--report", default=None, help="write the JSON report")
@@ -1054,7 +1058,8 @@ def main(argv=None):
     train_specs, test_specs = split_specs(a.pool, a.test)
     report = dict(config=dict(pool=a.pool, train_scenes=len(train_specs), test_scenes=len(test_specs),
                               steps=a.steps, stride=K_STRIDE, iters=a.iters, batch_nodes=a.batch_nodes,
-                              lr=list(a.lr), noise=a.noise, balance=a.balance, width=L_WIDTH, layers=LAYERS))
+                              lr=list(a.lr), noise=a.noise, balance=a.balance, kind_weight=a.kind_weight,
+                              width=L_WIDTH, layers=LAYERS))
     t0 = time.perf_counter()
     if a.load:
         net = MPNet.from_state(dict(np.load(a.load)))
@@ -1069,7 +1074,7 @@ def main(argv=None):
         net.norm.copy_(torch.tensor(nrm))
         t1 = time.perf_counter()
         losses = train(net, roll, a.iters, a.lr[0], a.lr[1], a.batch_nodes, a.noise, log_every=250,
-                       balance=a.balance)
+                       balance=a.balance, kind_weight={k: float(w) for k, w in a.kind_weight})
         torch.cuda.synchronize()
         report["train_s"] = time.perf_counter() - t1
         report["loss_first_100"] = float(np.mean(losses[:100]))

@@ -142,3 +142,15 @@ def test_solver_fails_loudly_without_library(tmp_path):
             sb.load(str(tmp_path / "missing.so"))
     finally:
         sb._lib = saved
+
+
+def test_fortran_bindings_name_exported_symbols(lib):
+    """Every bind(C, name=...) of the Fortran interface module names a symbol
+    the library exports (the module itself needs a Fortran compiler, which
+    this image does not have)."""
+    src = open(os.path.join(ROOT, "sources_b200", "fortran", "sphg_iface.f90")).read()
+    names = set(re.findall(r'bind\(C,\s*name="(sphg_[a-z0-9_]+)"\)', src))
+    out = subprocess.run(["nm", "-D", "--defined-only", lib._name], capture_output=True, text=True).stdout
+    syms = {l.split()[-1] for l in out.splitlines() if l.strip()}
+    assert len(names) >= 15
+    assert names <= syms, sorted(names - syms)

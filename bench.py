@@ -297,6 +297,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-stepper arm")
     ap.add_argument("--learned-strides", type=int, default=5)
+    ap.add_argument("--forchheimer-b", type=float, default=0.0,
+                    help="Forchheimer coefficient of the water-soil drag [s^2/m^2] (0: the reference's Darcy law)")
     ap.add_argument("--workload", default=WORKLOAD, choices=[WORKLOAD, "two_phase_456k", "ensemble_256"],
                     help="two_phase_456k: the same scene 2.0 m wide (for profiler captures); "
                          "ensemble_256: 256 uneven scenes stepped as three batched groups")
@@ -328,9 +330,9 @@ def main():
     if args.workload == "ensemble_256":
         return run_ensemble(args, rank, world, torch, dist)
     if args.workload == WORKLOAD:
-        scene = scenes.two_phase(precision=SPHG_FP32)
+        scene = scenes.two_phase(precision=SPHG_FP32, forchheimer_b=args.forchheimer_b)
     else:
-        scene = scenes.two_phase(width=2.0, precision=SPHG_FP32)
+        scene = scenes.two_phase(width=2.0, precision=SPHG_FP32, forchheimer_b=args.forchheimer_b)
     n = scene.n_particles
     stream = torch.cuda.current_stream()
     solver = Solver(scene)
@@ -490,6 +492,8 @@ def main():
                 "config": {"workload": args.workload, "particles": n, "water": scene.phases[0].n,
                            "soil": scene.phases[1].n, "dx": 0.002, "precision": "fp32 pairs / fp64 state",
                            "skf": int(scene.params.skf), "parallelism": f"replicas{world}",
+                           "drag": ("darcy (the reference's law)" if args.forchheimer_b == 0
+                                    else "darcy-forchheimer b=%g s^2/m^2" % args.forchheimer_b),
                            "l2": "inputs larger than L2 (state ~%.0f MB)" % (n * 250 / 1e6)},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
                 "clocks": clocks, "learned": learned}

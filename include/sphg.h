@@ -38,7 +38,7 @@
 extern "C" {
 #endif
 
-#define SPHG_ABI_VERSION 1
+#define SPHG_ABI_VERSION 2
 
 /* Status codes.  The reference stops the program where these are returned:
  * pair overflow m_particles.f90:992-993,1053-1054; particle outside the grid
@@ -114,6 +114,12 @@ typedef struct sphg_params {
     double x_min, x_max, y_min, y_max; /* x_mingeom.. (m_particles.f90:89-91): neighbour grid extent */
     int64_t max_interaction;        /* param.f90:14: capacity of each pair list   */
     sphg_material water, soil;      /* H2O, SiO2 (declarations_sph.f90:44)        */
+    /* Forchheimer coefficient b [s^2/m^2] of the water-soil drag.  The
+     * reference's darcy_law (m_particles.f90:3832-3874) is linear: hydraulic
+     * gradient i = u/k with u = v_w - v_s.  With b > 0 the drag follows
+     * i = u/k + b|u|u, i.e. each pair's Darcy term is scaled by (1 + k b |u|).
+     * 0 (the default) is the reference's law, bit for bit. */
+    double forchheimer_b;
 } sphg_params;
 
 /* Host view of one phase: pointers into the Fortran arrays of a `particles`

@@ -586,13 +586,20 @@ static void jaumann_rate(or_ctx* C, or_phase* P) {
     }
 }
 
-/* darcy_law, m_particles.f90:3832-3874 */
+/* darcy_law, m_particles.f90:3832-3874.  With forchheimer_b > 0 (not in the
+ * reference) the pair's coefficient cf is scaled by 1 + ks*b*|v_w - v_s|, the
+ * Forchheimer law i = u/ks + b|u|u in the reference's hydraulic-gradient form. */
 static void darcy_law(or_ctx* C, or_phase* W, or_phase* S) {
     double gravity = C->prm.numeric_gravity, ks = C->prm.soil.permeability;
+    double kb = ks * C->prm.forchheimer_b;
     for (int64_t k = 0; k < C->niac; ++k) {
         int i = C->pair_i[k], j = C->pair_j[k];
         double rrw = C->w[k] / (W->rho[i] * S->rho[j]);
         double cf = W->vof[i] * S->vof[j] * W->rho[i] * (-gravity) / ks;
+        if (kb != 0.0) {
+            double u0 = W->vx[2 * i] - S->vx[2 * j], u1 = W->vx[2 * i + 1] - S->vx[2 * j + 1];
+            cf = cf * (1.0 + kb * sqrt(u0 * u0 + u1 * u1));
+        }
         for (int d = 0; d < 2; ++d) {
             double sp = cf * (W->vx[2 * i + d] - S->vx[2 * j + d]) * rrw;
             W->dvx[2 * i + d] = W->dvx[2 * i + d] - S->mass[j] * sp;

@@ -12,7 +12,7 @@ import ctypes as C
 
 import numpy as np
 
-SPHG_ABI_VERSION = 1
+SPHG_ABI_VERSION = 2
 
 SPHG_OK = 0
 SPHG_ERR_PAIR_OVERFLOW = 1
@@ -60,6 +60,7 @@ class Params(C.Structure):
         ("max_interaction", C.c_int64),
         ("water", Material),
         ("soil", Material),
+        ("forchheimer_b", C.c_double),
     ]
 
 

@@ -186,6 +186,7 @@ struct Engine : EngineBase {
         s.w_rho0 = p.water.rho0; s.w_b = p.water.b; s.w_gamma = p.water.gamma; s.w_c = p.water.c; s.w_mu = p.water.viscosity;
         s.s_rho0 = p.soil.rho0; s.s_k = p.soil.k; s.s_E = p.soil.E; s.s_niu = p.soil.niu; s.s_c = p.soil.c;
         s.s_perm = p.soil.permeability; s.s_G = p.soil.G;
+        s.s_kb = p.soil.permeability * p.forchheimer_b;
         s.s_alpha1 = alpha1_of(p.soil.phi);
         s.tab = tab_dev;
     }
@@ -589,8 +590,13 @@ struct Engine : EngineBase {
             if ((rc = launch("water_pass_a", k_water_pass_a<T, SKF, false>, blocks(W.n, tpb), tpb, W, grid, sc_same, sim, cnt))) return rc;
             if ((rc = launch("water_pass_b", k_water_pass_b<T, SKF, false>, blocks(W.n, tpb), tpb, W, grid, sc_same, sim, none))) return rc;
             if ((rc = launch("soil_pass", k_soil_pass<T, SKF, false>, blocks(S.n, tpb), tpb, S, grid, sc_same, sim, cnt, 1, none))) return rc;
-            if ((rc = launch("cross_soil", k_cross_soil<T, SKF>, blocks(S.n, tpb), tpb, S, W, grid, sc_cross, sim, us, cnt))) return rc;
-            if ((rc = launch("cross_water", k_cross_water<T, SKF>, blocks(W.n, tpb), tpb, W, S, grid, sc_cross, sim, cnt, uw))) return rc;
+            if (p.forchheimer_b != 0.0) {
+                if ((rc = launch("cross_soil", k_cross_soil<T, SKF, true>, blocks(S.n, tpb), tpb, S, W, grid, sc_cross, sim, us, cnt))) return rc;
+                if ((rc = launch("cross_water", k_cross_water<T, SKF, true>, blocks(W.n, tpb), tpb, W, S, grid, sc_cross, sim, cnt, uw))) return rc;
+            } else {
+                if ((rc = launch("cross_soil", k_cross_soil<T, SKF, false>, blocks(S.n, tpb), tpb, S, W, grid, sc_cross, sim, us, cnt))) return rc;
+                if ((rc = launch("cross_water", k_cross_water<T, SKF, false>, blocks(W.n, tpb), tpb, W, S, grid, sc_cross, sim, cnt, uw))) return rc;
+            }
             aliased = true;
         }
         return 0;
@@ -935,6 +941,7 @@ static int validate(const sphg_params* p, int n_phase) {
     if ((p->single_phase != 0) != (n_phase == 1)) return SPHG_ERR_BAD_ARG;
     if (p->single_phase && p->first_material != SPHG_WATER && p->first_material != SPHG_SOIL) return SPHG_ERR_BAD_ARG;
     if (p->precision != SPHG_FP64 && p->precision != SPHG_FP32) return SPHG_ERR_BAD_ARG;
+    if (!(p->forchheimer_b >= 0.0) || !std::isfinite(p->forchheimer_b)) return SPHG_ERR_BAD_ARG;
     // outside the implemented scope: Verlet (param.f90:78 = 2), Mohr-Coulomb
     // (yield_criterion = 1), flow rules 1 and 2, summation density for soil
     if (p->integrate_scheme != 1) return SPHG_ERR_UNSUPPORTED;

@@ -31,6 +31,7 @@ struct SimConst {
     double gravity, numeric_gravity, alpha, beta, etq, dd, p1, p2, delta, epsilon, dt;
     double w_rho0, w_b, w_gamma, w_c, w_mu;
     double s_rho0, s_k, s_E, s_niu, s_c, s_perm, s_G, s_alpha1;
+    double s_kb;           // permeability x Forchheimer b (0: linear Darcy)
     const SceneTab* tab;   // per-scene dt, water b and c, soil alpha1 (indexed by PhaseDev::sid)
 };
 
@@ -685,8 +686,9 @@ __global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_SOIL : 1)
 // gradient is taken, as the reference does, with dx = x_water - x_soil.
 // With m = vol*rho, Darcy's m_w*cf*(v_w - v_s)*W/(rho_w rho_s) becomes
 // vol_w*rho_w*vof_w*vof_s*(-g/k)*(v_w - v_s)*W/rho_s and the pore pressure
-// m_w p_w/(rho_w rho_s) becomes vol_w p_w / rho_s.
-template <typename T, int SKF>
+// m_w p_w/(rho_w rho_s) becomes vol_w p_w / rho_s.  FCH: the Forchheimer
+// drag, each pair's Darcy term scaled by (1 + k b |v_w - v_s|).
+template <typename T, int SKF, bool FCH>
 __global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_CROSS : 1) k_cross_soil(PhaseDev<T> S, PhaseDev<T> W, GridGeom g, SearchConst sc, SimConst c,
                                                         StepCtl u, DevCounters* cnt) {
     typedef typename V2<T>::t T2;
@@ -710,9 +712,11 @@ __global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_CROSS : 1
         pair_kernel<T, SKF>(ka, sc, ha, W.hs, m, dx, dy, w, sr, rr, mh);
         // x_water - x_soil = -(x_a - x_b)
         const T gx = -sr * dx, gy = -sr * dy;
-        const T q = rb.vol * rb.rho * qb.vof * w;
-        ddx += q * (rb.vx - ra.vx);
-        ddy += q * (rb.vy - ra.vy);
+        T q = rb.vol * rb.rho * qb.vof * w;
+        const T ux = rb.vx - ra.vx, uy = rb.vy - ra.vy;
+        if constexpr (FCH) q *= T(1) + (T)c.s_kb * sqrt(ux * ux + uy * uy);
+        ddx += q * ux;
+        ddy += q * uy;
         const T mp = rb.vol * qb.p;
         dpx += mp * gx;
         dpy += mp * gy;
@@ -734,7 +738,8 @@ __global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_CROSS : 1
 // Water side: darcy_law :3832, volume_fraction_water2 :3940 (dvof),
 // volume_fraction_water :3912 (vof2), and every renorm_interval steps the
 // renormalisation rho <- rho/vof*vof2, vof <- vof2 (declarations_sph.f90:1414-1421).
-template <typename T, int SKF>
+// FCH as in k_cross_soil.
+template <typename T, int SKF, bool FCH>
 __global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_CROSS : 1) k_cross_water(PhaseDev<T> W, PhaseDev<T> S, GridGeom g, SearchConst sc, SimConst c,
                                                          DevCounters* cnt, StepCtl u) {
     typedef typename V2<T>::t T2;
@@ -758,7 +763,8 @@ __global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_CROSS : 1
         pair_kernel<T, SKF>(ka, sc, ha, S.hs, m, dx, dy, w, sr, rr, mh);
         const T mb = rb.vol * rb.rho;
         const T ux = ra.vx - rb.vx, uy = ra.vy - rb.vy;
-        const T q = rb.vol * phis * w;
+        T q = rb.vol * phis * w;
+        if constexpr (FCH) q *= T(1) + (T)c.s_kb * sqrt(ux * ux + uy * uy);
         ddx -= q * ux;
         ddy -= q * uy;
         dvof -= mb * (sr * (ux * dx + uy * dy));

@@ -29,6 +29,7 @@ module sphg_iface
      real(c_double) :: delta, epsilon, dt, x_min, x_max, y_min, y_max
      integer(c_int64_t) :: max_interaction
      type(sphg_material) :: water, soil
+     real(c_double) :: forchheimer_b
   end type
 
   type, bind(C) :: sphg_phase_host

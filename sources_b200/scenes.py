@@ -187,10 +187,13 @@ def granular_column(width=0.2, height=0.1, box_w=1.0, box_h=0.3, dx=0.002, skf=1
 
 
 def two_phase(width=4.0, height=1.0, block_w=1.0, block_h=0.4, water_h=0.8, dx=0.002,
-              porosity=0.4, permeability=1.0e-3, skf=1, phi_deg=19.8, precision=SPHG_FP32) -> Scene:
+              porosity=0.4, permeability=1.0e-3, skf=1, phi_deg=19.8, precision=SPHG_FP32,
+              forchheimer_b=0.0) -> Scene:
     """Submerged soil block under a water layer (two-phase step,
     declarations_sph.f90:1131), laid out as input_mix_Savage.f90 does: the
-    water lattice fills the block too, as the pore-water phase."""
+    water lattice fills the block too, as the pore-water phase.
+    forchheimer_b [s^2/m^2] > 0 adds the quadratic Forchheimer drag to the
+    reference's linear Darcy law (0: the reference's law)."""
     x, y, virt = _box(width, height, dx)
     inside = ~virt
     in_block = (x < block_w) & (y < block_h)
@@ -222,6 +225,7 @@ def two_phase(width=4.0, height=1.0, block_w=1.0, block_h=0.4, water_h=0.8, dx=0
     S.mass[:] = dx * dx * S.rho
     p.single_phase = 0
     p.alpha = 0.1
+    p.forchheimer_b = forchheimer_b
     h = float(W.hsml[0])
     p.dt = min(0.25 * h / wm["c"], 0.1 * h / sm["c"])
     _finish(p, [W, S], width, height, dx, skf, precision)

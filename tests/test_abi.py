@@ -117,6 +117,14 @@ def test_create_validates_before_touching_the_device(lib):
     assert lib.sphg_create(C.byref(p), 3, C.byref(h)) == abi.SPHG_ERR_BAD_ARG
     p.dt = 0.0
     assert lib.sphg_create(C.byref(p), 2, C.byref(h)) == abi.SPHG_ERR_BAD_ARG
+    p.dt = 1e-5
+    for b in (-1.0, float("nan"), float("inf")):   # Forchheimer coefficient
+        p.forchheimer_b = b
+        assert lib.sphg_create(C.byref(p), 2, C.byref(h)) == abi.SPHG_ERR_BAD_ARG
+    p.forchheimer_b = 0.0
+    p.abi_version = abi.SPHG_ABI_VERSION - 1   # a caller built against an older header
+    assert lib.sphg_create(C.byref(p), 2, C.byref(h)) == abi.SPHG_ERR_BAD_ARG
+    p.abi_version = abi.SPHG_ABI_VERSION
     assert lib.sphg_create(None, 2, C.byref(h)) == abi.SPHG_ERR_BAD_ARG
     assert lib.sphg_single_step(None, 1) == abi.SPHG_ERR_BAD_ARG
     assert lib.sphg_stats(None, None) == abi.SPHG_ERR_BAD_ARG

@@ -101,6 +101,59 @@ def test_rhs_parity_fp64(cuda_ok, name):
             assert st.niac[w] == len(o.pairs(w)[0])
 
 
+def forchheimer_scene(precision):
+    s = scenes.jitter(scenes.small("two_phase", precision=precision), 0.0002, seed=23)
+    s.params.forchheimer_b = 4e4     # k b |u| ~ 1 at the slip speeds below
+    rng = np.random.default_rng(4)
+    for P in s.phases:
+        P.vx[:P.ntotal] = rng.normal(0, 0.02, size=(P.ntotal, 2))
+    return s
+
+
+def test_forchheimer_rhs_and_steps_fp64(cuda_ok):
+    """The Forchheimer drag option (b > 0; not in the reference) against the
+    oracle's restatement of it, at the tolerances of the plain law: one
+    right-hand side within 1e-9 and 30 steps within 1e-7."""
+    s = forchheimer_scene(SPHG_FP64)
+    o = Oracle(s)
+    assert o.single_step(1) == 0
+    with Solver(s) as g:
+        g.single_step(1)
+        for k in range(2):
+            a, b = g.download(k + 1), o.download(k + 1)
+            for f in RHS_FIELDS:
+                e = ferr(getattr(a, f), getattr(b, f))
+                assert e <= 1e-9, (k + 1, f, e)
+    o = Oracle(s)
+    assert o.time_integration(30) == 0
+    with Solver(s) as g:
+        g.time_integration(30)
+        for k in range(2):
+            a, b = g.download(k + 1), o.download(k + 1)
+            for f in STATE_FIELDS:
+                e = ferr(getattr(a, f), getattr(b, f))
+                assert e <= 1e-7, (k + 1, f, e)
+
+
+def test_forchheimer_fp32_error_budget(cuda_ok):
+    """FP32 mode with the Forchheimer drag against the FP64 oracle, within
+    the FP32 budgets of the plain law after 1 and 30 steps."""
+    s64 = forchheimer_scene(SPHG_FP64)
+    s32 = forchheimer_scene(SPHG_FP32)
+    for steps, budget in ((1, FP32_BUDGET_1), (30, FP32_BUDGET_30)):
+        o = Oracle(s64)
+        assert o.time_integration(steps) == 0
+        with Solver(s32) as g:
+            g.time_integration(steps)
+            for k in range(2):
+                a, b = g.download(k + 1), o.download(k + 1)
+                for f, tol in budget.items():
+                    if np.abs(getattr(b, f)).max() == 0:
+                        continue
+                    e = ferr(getattr(a, f), getattr(b, f))
+                    assert e <= tol, (steps, k + 1, f, e)
+
+
 @pytest.mark.parametrize("name", NAMES)
 def test_steps_parity_fp64(cuda_ok, name):
     s = scenes.small(name, precision=SPHG_FP64)

@@ -183,3 +183,32 @@ def test_restart_is_bit_identical(name):
         pf, pb = full.download(k + 1), b.download(k + 1)
         for f in ("x", "vx", "rho", "p", "sxx", "syy", "sxy", "vof", "drho", "dvx"):
             assert np.array_equal(getattr(pf, f), getattr(pb, f)), (k, f)
+
+
+def test_forchheimer_drag_is_linear_in_b_opposes_slip_and_conserves_momentum():
+    """The Forchheimer option (not in the reference) scales each water-soil
+    pair's Darcy coefficient by 1 + k b |v_w - v_s|.  Within one step the
+    right-hand side is then affine in b, the extra drag opposes the slip and,
+    being a pair force, adds no net momentum over both phases."""
+    base = scenes.jitter(scenes.small("two_phase", precision=SPHG_FP64), 0.0002, seed=31)
+    rng = np.random.default_rng(8)
+    W, S = base.phases
+    W.vx[:W.ntotal] = rng.normal(0, 0.02, size=(W.ntotal, 2)) + (0.05, 0.0)   # water slips to +x
+    S.vx[:S.ntotal] = rng.normal(0, 0.02, size=(S.ntotal, 2))
+    dv = {}
+    for b in (0.0, 2e4, 4e4):
+        s = base.copy()
+        s.params.forchheimer_b = b
+        o = Oracle(s)
+        assert o.single_step(1) == 0
+        dv[b] = [o.download(k) for k in (1, 2)]
+    for k in range(2):
+        d0, d1, d2 = (dv[b][k].dvx for b in (0.0, 2e4, 4e4))
+        scale = np.abs(d2 - d0).max()
+        assert scale > 1e-3 * np.abs(d0).max()          # the option changes the drag
+        assert np.abs(d2 - 2 * d1 + d0).max() <= 1e-9 * scale
+    # extra momentum exchanged between the phases: equal and opposite
+    mw = (dv[0.0][0].mass[:, None] * (dv[4e4][0].dvx - dv[0.0][0].dvx)).sum(axis=0)
+    ms = (dv[0.0][1].mass[:, None] * (dv[4e4][1].dvx - dv[0.0][1].dvx)).sum(axis=0)
+    assert np.all(np.abs(mw + ms) <= 1e-9 * np.abs(mw).max())
+    assert mw[0] < 0 < ms[0]                             # water slowed, soil dragged along

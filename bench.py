@@ -236,7 +236,7 @@ def run_ensemble(args, rank, world, torch, dist):
     ms = replicas.max_over_ranks(e0.elapsed_time(e1), dist if world > 1 else None, device="cuda")
     n = ens.n_particles
     groups = {g.kind: {"scenes": len(g.members), "particles": g.scene.n_particles, "tuning": list(g.tuning),
-                       "autotune_ms_per_step": {"%s,%s" % k: v for k, v in ens.tuning_table.get(g.kind, {}).items()}}
+                       "autotune_ms_per_step": {",".join(map(str, k)): v for k, v in ens.tuning_table.get(g.kind, {}).items()}}
               for g in ens.groups}
     ens.close()
     if rank == 0:

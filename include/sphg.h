@@ -154,7 +154,7 @@ typedef struct sphg_stats_t {
     int32_t itimestep;
     int32_t _pad;
     double time;
-    double last_step_ms;     /* device time of the last sphg_time_integration call */
+    double last_step_ms;     /* device time per step of the last sphg_time_integration call */
 } sphg_stats_t;
 
 typedef struct sphg_ctx sphg_ctx;
@@ -219,13 +219,17 @@ int sphg_set_scenes(sphg_ctx* ctx, int nscenes, const sphg_scene* scenes);
 int sphg_upload_scene_ids(sphg_ctx* ctx, int phase, const int32_t* scene_id);
 
 /* Tuning knobs (no counterpart in the reference): the neighbour-cell edge as
- * a multiple (>= 1) of the support radius, and the steps between spatial
- * reorders of the device state.  They change the order in which neighbours
- * are summed, so results agree to rounding, and the pair sets not at all. */
+ * a multiple (>= 1) of the support radius, the steps between spatial
+ * reorders of the device state, and x_split, the number of cells each row of
+ * that edge is cut into along x (1..8; 0 = the library default).  A particle
+ * scans 3 rows of 2*x_split+1 cells: finer cells along x test fewer
+ * candidates while each row stays one contiguous run of the cell-sorted
+ * list.  They change the order in which neighbours are summed, so results
+ * agree to rounding, and the pair sets not at all. */
 typedef struct sphg_tuning {
     double cell_factor;
     int32_t reorder_interval;
-    int32_t _pad;
+    int32_t x_split;
 } sphg_tuning;
 int sphg_set_tuning(sphg_ctx* ctx, const sphg_tuning* t);
 

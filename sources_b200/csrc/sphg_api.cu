@@ -121,6 +121,7 @@ struct Engine : EngineBase {
     int tab_cap = 0;
     bool tab_custom = false;
     double cell_factor = 1.0;       // neighbour cell = factor * support radius (autotuned)
+    int x_split = 0;                // x cells per neighbour cell (0: SPHG_X_SPLIT)
     std::vector<void*> allocs;
     SimConst sim{};
     int nfail_slot = 3;             // which DP site the reported nfail comes from
@@ -244,7 +245,9 @@ struct Engine : EngineBase {
 
     int set_tuning(const sphg_tuning* t) override {
         if (!t || !(t->cell_factor >= 1.0) || t->cell_factor > 4.0 || t->reorder_interval < 0) return SPHG_ERR_BAD_ARG;
+        if (t->x_split < 0 || t->x_split > 8) return SPHG_ERR_BAD_ARG;
         cell_factor = t->cell_factor;
+        x_split = t->x_split;
         ctx->prm.reorder_interval = t->reorder_interval;
         prepared = false;
         drop_graphs();
@@ -464,9 +467,15 @@ struct Engine : EngineBase {
         if ((rc0 = sync_table())) return rc0;
         double cell = sk * hmax * cell_factor * (1.0 + 1e-6);
         if (!(p.x_max > p.x_min) || !(p.y_max > p.y_min)) return SPHG_ERR_BAD_ARG;
-        double ncx = std::ceil((p.x_max - p.x_min) / cell) + 1, ncy = std::ceil((p.y_max - p.y_min) / cell) + 1;
+        // rows one cell high; kx cells per cell along x (each at least
+        // support/kx wide, so the 2*kx+1 cells around a particle's own cover
+        // its support, clamped edge cells included)
+        const int kx = x_split > 0 ? x_split : SPHG_X_SPLIT;
+        const double cellx = cell / kx;
+        double ncx = std::ceil((p.x_max - p.x_min) / cellx) + 1, ncy = std::ceil((p.y_max - p.y_min) / cell) + 1;
         if (ncx * ncy > 2.0e8) return SPHG_ERR_BAD_ARG;
-        grid.ncx = (int)ncx; grid.ncy = (int)ncy; grid.x0 = p.x_min; grid.y0 = p.y_min; grid.inv = 1.0 / cell;
+        grid.ncx = (int)ncx; grid.ncy = (int)ncy; grid.kx = kx; grid.x0 = p.x_min; grid.y0 = p.y_min;
+        grid.inv = 1.0 / cell; grid.invx = 1.0 / cellx;
         int nc = grid.ncx * grid.ncy;
         if (nc != ncell) {
             for (int ph = 0; ph < 2; ++ph) {

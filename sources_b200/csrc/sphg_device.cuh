@@ -36,9 +36,15 @@ template <> struct V4<float> { typedef float4 t; };
 template <typename T> struct __align__(4 * sizeof(T)) RecA { T vx, vy, vol, rho; };
 template <typename T> struct __align__(4 * sizeof(T)) RecB { T p, c, vof, sxx, sxy, syy, itype, aux; };
 
+// Cell grid.  Rows are one support-radius-sized cell high; along x each such
+// cell is split into kx cells, so a particle's neighbours lie in 3 rows of
+// 2*kx+1 cells, each row one contiguous run of the cell-sorted list.
 struct GridGeom {
-    int ncx, ncy;
-    double x0, y0, inv;   // origin and 1 / cell size
+    int ncx, ncy;         // cells along x (kx per row cell) and rows
+    int kx;               // x cells per support-radius cell (stencil half-width)
+    double x0, y0;        // origin
+    double inv;           // 1 / row height
+    double invx;          // 1 / x cell width (= kx * inv)
 };
 
 // Neighbour-search constants of one pair list.
@@ -102,7 +108,7 @@ struct PhaseDev {
 
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void cell_coords(const GridGeom& g, double x, double y, int& cx, int& cy, bool& clamped) {
-    double fx = floor((x - g.x0) * g.inv), fy = floor((y - g.y0) * g.inv);
+    double fx = floor((x - g.x0) * g.invx), fy = floor((y - g.y0) * g.inv);
     clamped = false;
     if (!(fx >= 0.0)) { fx = 0.0; clamped = true; }       // also catches NaN
     if (fx > g.ncx - 1) { fx = g.ncx - 1; clamped = true; }
@@ -179,8 +185,8 @@ __device__ __forceinline__ int visit_neighbours(const GridGeom& g, const SearchC
                                                 double2 xa, double ha, int self, F&& f) {
     int cx, cy; bool clamped;
     cell_coords(g, xa.x, xa.y, cx, cy, clamped);
-    const int x0 = cx > 0 ? cx - 1 : 0;
-    const int x1 = cx < g.ncx - 1 ? cx + 1 : g.ncx - 1;
+    const int x0 = cx > g.kx ? cx - g.kx : 0;
+    const int x1 = cx < g.ncx - 1 - g.kx ? cx + g.kx : g.ncx - 1;
     const int y0 = cy > 0 ? cy - 1 : 0;
     const int y1 = cy < g.ncy - 1 ? cy + 1 : g.ncy - 1;
     int hits = 0;
@@ -360,7 +366,7 @@ __device__ __forceinline__ void prefetch_l1(const void* p) {
 }
 
 // Warp-synchronous neighbour visitor.  Each lane scans the candidates of its
-// particle (three row segments of the sorted list) with the exact FP64 pair
+// particle (three row runs of the sorted list) with the exact FP64 pair
 // test and appends hits to its buffer; as soon as any lane's buffer is full,
 // or every lane has finished scanning, the whole warp drains the buffers
 // through body(m, dx, dy) together.  Scanning (cheap, divergent) and pair
@@ -382,8 +388,8 @@ __device__ __forceinline__ int visit_batched(HitBuf<T, TPB, CH>& buf, const Grid
     if (active) {
         int cx, cy; bool clamped;
         cell_coords(g, xa.x, xa.y, cx, cy, clamped);
-        const int x0 = cx > 0 ? cx - 1 : 0;
-        const int x1 = cx < g.ncx - 1 ? cx + 1 : g.ncx - 1;
+        const int x0 = cx > g.kx ? cx - g.kx : 0;
+        const int x1 = cx < g.ncx - 1 - g.kx ? cx + g.kx : g.ncx - 1;
         if (cy - 1 >= 0) { b0 = __ldg(cstart + (cy - 1) * g.ncx + x0); L0 = __ldg(cstart + (cy - 1) * g.ncx + x1 + 1) - b0; }
         b1 = __ldg(cstart + cy * g.ncx + x0); L1 = __ldg(cstart + cy * g.ncx + x1 + 1) - b1;
         if (cy + 1 < g.ncy) { b2 = __ldg(cstart + (cy + 1) * g.ncx + x0); L2 = __ldg(cstart + (cy + 1) * g.ncx + x1 + 1) - b2; }

@@ -38,6 +38,13 @@ struct SimConst {
 #ifndef SPHG_TPB
 #define SPHG_TPB 128
 #endif
+// Default x cells per neighbour cell (GridGeom::kx; sphg_tuning.x_split
+// overrides it per context).  Step time on a B200 at 912,016 particles:
+// 1: 0.596-0.603 ms, 2: 0.558-0.565, 3: 0.567, 4: 0.548 (the candidate
+// strip narrows from 3 to 2.25 support radii; the pair set is the same).
+#ifndef SPHG_X_SPLIT
+#define SPHG_X_SPLIT 4
+#endif
 // minimum resident blocks per SM of each FP32 pair pass (register cap for
 // the compiler: 65,536 / (SPHG_TPB * min blocks) registers per thread); the
 // FP64 passes are left uncapped.  Timed on

@@ -185,6 +185,7 @@ extern "C" int sphg_sum_density_noalloc(const sphg_params* p, int32_t n, const d
     if (!(ncx * ncy <= (double)kMaxC)) return SPHG_ERR_BAD_ARG;
     GridGeom g;
     g.ncx = (int)ncx; g.ncy = (int)ncy; g.x0 = p->x_min; g.y0 = p->y_min; g.inv = 1.0 / cell;
+    g.kx = 1; g.invx = g.inv;
     const int ncell = g.ncx * g.ncy;
     SearchConst sc;
     sc.scale_k = sk;

@@ -18,9 +18,9 @@ column aspect H/W uniform in [0.5, 4]; friction angle uniform in [20, 40]
 degrees; water depth uniform in [0.1, 0.5] m (the water level above the
 soil of a submerged scene); spacing dx = 0.004 m.
 
-An autotuner picks the neighbour-cell factor and the reorder interval of
-each group by timing a few steps of every candidate on a throw-away copy
-of the group.
+An autotuner picks the neighbour-cell factor, the reorder interval and the
+number of x cells per neighbour cell of each group by timing a few steps of
+every candidate on a throw-away copy of the group.
 """
 from __future__ import annotations
 
@@ -100,7 +100,7 @@ class Group:
     offsets: list                # x offset of each member
     rows: list                   # per-scene table rows
     sids: list                   # per phase: scene id of every particle
-    tuning: tuple = (1.0, 10)
+    tuning: tuple = (1.0, 10, 0)
 
 
 def pack(members, built, gap_cells: float = 6.0) -> Group:
@@ -159,12 +159,14 @@ def _solver(g: Group, tuning):
     return sv
 
 
-CANDIDATES = [(1.0, 10), (1.0, 25), (1.25, 10), (1.25, 25), (1.5, 10)]
+# (cell factor, reorder interval, x cells per cell)
+CANDIDATES = [(1.0, 10, 4), (1.0, 25, 4), (1.0, 10, 2), (1.0, 10, 1), (1.25, 10, 4), (1.25, 25, 4), (1.5, 10, 4)]
 
 
 def autotune(g: Group, steps: int = 8, warmup: int = 3, candidates=CANDIDATES):
-    """Time every (cell factor, reorder interval) candidate on a copy of the
-    group and return the fastest with the table of timings (ms/step)."""
+    """Time every (cell factor, reorder interval, x split) candidate on a
+    copy of the group and return the fastest with the table of timings
+    (ms/step)."""
     table = {}
     for cand in candidates:
         sv = _solver(g, cand)

@@ -101,6 +101,41 @@ def test_rhs_parity_fp64(cuda_ok, name):
             assert st.niac[w] == len(o.pairs(w)[0])
 
 
+@pytest.mark.parametrize("x_split", [1, 2, 3, 4])
+@pytest.mark.parametrize("name", NAMES)
+def test_x_split_cells_keep_pairs_and_fields(cuda_ok, name, x_split):
+    """Cells cut along x (sphg_tuning.x_split) visit fewer candidates; the
+    pair sets stay bit-exact and FP64 fields match the oracle as with the
+    default grid, clamped particles outside the grid included."""
+    s = scenes.jitter(scenes.small(name, precision=SPHG_FP64), 0.0003, seed=40 + x_split)
+    P = s.phases[0]
+    R = 2 * float(P.hsml[0])
+    y = float(P.x[0, 1])
+    # chains of particles within R of each other beyond both ends of the grid:
+    # clamped into the first / last column of cells, next to unclamped ones
+    for k, x in enumerate((s.params.x_min - 0.01, s.params.x_min - 0.01 + 0.8 * R, s.params.x_min - 0.01 + 1.6 * R,
+                           s.params.x_max + 0.01, s.params.x_max + 0.01 - 0.8 * R, s.params.x_max + 0.01 - 1.6 * R)):
+        P.x[k] = (x, y)
+    rng = np.random.default_rng(x_split)
+    for Q in s.phases:
+        Q.vx[:Q.ntotal] = rng.normal(0, 0.02, size=(Q.ntotal, 2))
+    o = Oracle(s)
+    assert o.single_step(1) == 0
+    with Solver(s) as g:
+        g.set_tuning(1.0, 10, x_split)
+        g.single_step(1)
+        for w in lists_for(s):
+            gi, gj = g.pairs(w)
+            oi, oj = o.pairs(w)
+            assert np.array_equal(gi, oi) and np.array_equal(gj, oj), (w, len(gi), len(oi))
+        assert g.stats().n_out_of_domain >= 2
+        for k in range(len(s.phases)):
+            a, b = g.download(k + 1), o.download(k + 1)
+            for f in ("drho", "dvx", "av", "dvof", "vof2", "dsxx", "dsxy", "dp", "txx", "vcc"):
+                e = ferr(getattr(a, f), getattr(b, f))
+                assert e <= 1e-9, (name, x_split, k + 1, f, e)
+
+
 def forchheimer_scene(precision):
     s = scenes.jitter(scenes.small("two_phase", precision=precision), 0.0002, seed=23)
     s.params.forchheimer_b = 4e4     # k b |u| ~ 1 at the slip speeds below

@@ -41,21 +41,19 @@ WORKLOAD = "two_phase_912k"
 # Algorithmic HBM bytes per particle of each kernel in FP32 mode: the
 # particle's own data read once and its results written once (neighbour
 # records are re-read from L1/L2 and not counted).  The leapfrog predictor
-# runs inside `gather`, the corrector inside the last pass of each phase
-# (`cross_water`, `cross_soil`), so their state traffic is counted there.
+# runs inside `gather`; the cross pairs and the corrector run inside the last
+# pass of each phase (`water_pass_b`, `soil_pass`), so their state traffic is
+# counted there.
+CORRECTOR_WATER = 16 + 8 + 4 + 16 + 8 + 16 + 8 + 32 + 16 + 4   # rho, rho_min, drho, vof, vof_min, v_min, av, x rw, v, itype
+CORRECTOR_SOIL = 16 + 4 + 64 + 16 + 16 + 8 + 32 + 16 + 4 + 4    # rho, rho_min, drho, p/s rw, ds, dp, v_min, av, x rw, v, itype, fail
 ALG_BYTES = {
     # perm, xs, hs, recA, c, rho, vof, itype -> c, drho, p, s(3), recB, countiac
     "water_pass_a": 4 + 16 + 8 + 16 + 8 + 8 + 8 + 4 + 8 + 4 + 8 + 24 + 32 + 4,
-    # perm, xs, hs, recA, recB, itype -> dv, av, dvof
-    "water_pass_b": 4 + 16 + 8 + 16 + 32 + 4 + 8 + 8 + 4,
-    # perm, xs, hs, recA, recB, itype, p, s(3), eps_p rw, fail -> dv, av, drho, ds(3), dp, c, t(3), vcc, countiac
-    "soil_pass": 4 + 16 + 8 + 16 + 32 + 4 + 8 + 24 + 16 + 4 + 8 + 8 + 4 + 12 + 4 + 8 + 12 + 4 + 4,
-    # perm, xs, hs, recA, vof, dv rw, dvof rw, vof2, countiac + corrector (rho, rho_min, drho, vof, vof_min,
-    # v_min, av, x rw, v, itype)
-    "cross_water": 4 + 16 + 8 + 16 + 4 + 16 + 8 + 4 + 4 + 16 + 8 + 4 + 16 + 8 + 16 + 8 + 32 + 16 + 4,
-    # perm, xs, hs, recA, vof, dv rw, rho, vof w + corrector (rho, rho_min, drho, p/s rw, ds, dp, v_min, av,
-    # x rw, v, itype, fail)
-    "cross_soil": 4 + 16 + 8 + 16 + 4 + 16 + 8 + 8 + 16 + 4 + 64 + 16 + 16 + 8 + 32 + 16 + 4 + 4,
+    # perm, xs, hs, recA, recB, itype -> dv, av, dvof, vof2, countiac + corrector
+    "water_pass_b": 4 + 16 + 8 + 16 + 32 + 4 + 8 + 8 + 4 + 4 + 4 + CORRECTOR_WATER,
+    # perm, xs, hs, recA, recB, itype, p, s(3), eps_p rw, fail -> dv, av, drho, ds(3), dp, c, t(3), vcc, countiac;
+    # rho -> vof + corrector
+    "soil_pass": 4 + 16 + 8 + 16 + 32 + 4 + 8 + 24 + 16 + 4 + 8 + 8 + 4 + 12 + 4 + 8 + 12 + 4 + 4 + 8 + 8 + CORRECTOR_SOIL,
 }
 # Whole-step algorithmic bytes per particle-step (FP32 pair data, FP64 state):
 # the compulsory state read + write once per step plus the cell key.
@@ -376,7 +374,7 @@ def main():
     top = max(kern.items(), key=lambda kv: kv[1][1])
     top_name, (top_launches, top_ms) = top[0], top[1]
     avg_ms = top_ms / max(top_launches, 1)
-    units = scene.phases[0].n if top_name in ("water_pass_a", "water_pass_b", "cross_water", "water_sum") \
+    units = scene.phases[0].n if top_name in ("water_pass_a", "water_pass_b", "water_sum") \
         else scene.phases[1].n
     alg = ALG_BYTES.get(top_name, 0) * units
     peak, peak_kind = measured_peak_hbm()
@@ -405,15 +403,15 @@ def main():
                 "step": {"alg_bytes": step_bytes, "achieved_gbs": step_bytes / (step_ms / 1000.0) / 1e9,
                          "frac": step_bytes / (step_ms / 1000.0) / 1e9 / peak},
                 "kernels_ms_per_step": {k: v[1] / args.steps for k, v in kern.items()},
-                "passes": {k: {"alg_bytes": ALG_BYTES[k] * (scene.phases[1].n if k in ("soil_pass", "cross_soil")
+                "passes": {k: {"alg_bytes": ALG_BYTES[k] * (scene.phases[1].n if k == "soil_pass"
                                                             else scene.phases[0].n),
                                "avg_ms": kern[k][1] / max(kern[k][0], 1),
-                               "achieved_gbs": ALG_BYTES[k] * (scene.phases[1].n if k in ("soil_pass", "cross_soil")
+                               "achieved_gbs": ALG_BYTES[k] * (scene.phases[1].n if k == "soil_pass"
                                                                else scene.phases[0].n)
                                / (kern[k][1] / max(kern[k][0], 1) / 1000.0) / 1e9,
                                "traffic": ncu_traffic().get(k),
                                "issue": issue(k, kern[k][1] / max(kern[k][0], 1),
-                                              scene.phases[1].n if k in ("soil_pass", "cross_soil")
+                                              scene.phases[1].n if k == "soil_pass"
                                               else scene.phases[0].n)}
                            for k in ALG_BYTES if k in kern}}
 

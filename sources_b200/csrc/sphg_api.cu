@@ -582,29 +582,34 @@ struct Engine : EngineBase {
                 if ((rc = launch("gather", k_gather<T>, blocks(D.n, 256), 256, D, sim, 0, 0, fh, 0, 0, cnt))) return rc;
                 if ((rc = launch("water_sum", k_water_sum<T, SKF>, blocks(D.n, tpb), tpb, D, grid, sc_same, sim, cnt))) return rc;
                 if ((rc = launch("water_pass_a", k_water_pass_a<T, SKF, true>, blocks(D.n, tpb), tpb, D, grid, sc_same, sim, cnt))) return rc;
-                if ((rc = launch("water_pass_b", k_water_pass_b<T, SKF, true>, blocks(D.n, tpb), tpb, D, grid, sc_same, sim, u))) return rc;
+                if ((rc = launch("water_pass_b", k_water_pass_b<T, SKF, true, false>, blocks(D.n, tpb), tpb, D, D, grid, sc_same,
+                                 sc_same, sim, u, cnt))) return rc;
             } else {
                 if ((rc = launch("gather", k_gather<T>, blocks(D.n, 256), 256, D, sim, 1, dp, fh, 0, dp, cnt))) return rc;
                 StepCtl us = u; us.with_vof = 0; us.do_dp = dp;
-                if ((rc = launch("soil_pass", k_soil_pass<T, SKF, true>, blocks(D.n, tpb), tpb, D, grid, sc_same, sim, cnt, 0, us))) return rc;
+                if ((rc = launch("soil_pass", k_soil_pass<T, SKF, true, false>, blocks(D.n, tpb), tpb, D, D, grid, sc_same, sc_same,
+                                 sim, cnt, 0, us))) return rc;
             }
         } else {
             PhaseDev<T>& W = P[0];
             PhaseDev<T>& S = P[1];
             StepCtl uw = u; uw.with_vof = 1; uw.do_dp = 0;
             StepCtl us = u; us.with_vof = 1; us.do_dp = dp;
-            StepCtl none{}; 
             if ((rc = launch("gather", k_gather<T>, blocks(W.n, 256), 256, W, sim, 0, 0, fh, 1, 0, cnt))) return rc;
             if ((rc = launch("gather", k_gather<T>, blocks(S.n, 256), 256, S, sim, 1, dp, fh, 1, dp, cnt))) return rc;
             if ((rc = launch("water_pass_a", k_water_pass_a<T, SKF, false>, blocks(W.n, tpb), tpb, W, grid, sc_same, sim, cnt))) return rc;
-            if ((rc = launch("water_pass_b", k_water_pass_b<T, SKF, false>, blocks(W.n, tpb), tpb, W, grid, sc_same, sim, none))) return rc;
-            if ((rc = launch("soil_pass", k_soil_pass<T, SKF, false>, blocks(S.n, tpb), tpb, S, grid, sc_same, sim, cnt, 1, none))) return rc;
+            // the cross pairs run inside the last pass of each phase; the soil
+            // pass reads the water pressure that water_pass_a sets
             if (p.forchheimer_b != 0.0) {
-                if ((rc = launch("cross_soil", k_cross_soil<T, SKF, true>, blocks(S.n, tpb), tpb, S, W, grid, sc_cross, sim, us, cnt))) return rc;
-                if ((rc = launch("cross_water", k_cross_water<T, SKF, true>, blocks(W.n, tpb), tpb, W, S, grid, sc_cross, sim, cnt, uw))) return rc;
+                if ((rc = launch("water_pass_b", k_water_pass_b<T, SKF, false, true>, blocks(W.n, tpb), tpb, W, S, grid, sc_same,
+                                 sc_cross, sim, uw, cnt))) return rc;
+                if ((rc = launch("soil_pass", k_soil_pass<T, SKF, false, true>, blocks(S.n, tpb), tpb, S, W, grid, sc_same, sc_cross,
+                                 sim, cnt, 1, us))) return rc;
             } else {
-                if ((rc = launch("cross_soil", k_cross_soil<T, SKF, false>, blocks(S.n, tpb), tpb, S, W, grid, sc_cross, sim, us, cnt))) return rc;
-                if ((rc = launch("cross_water", k_cross_water<T, SKF, false>, blocks(W.n, tpb), tpb, W, S, grid, sc_cross, sim, cnt, uw))) return rc;
+                if ((rc = launch("water_pass_b", k_water_pass_b<T, SKF, false, false>, blocks(W.n, tpb), tpb, W, S, grid, sc_same,
+                                 sc_cross, sim, uw, cnt))) return rc;
+                if ((rc = launch("soil_pass", k_soil_pass<T, SKF, false, false>, blocks(S.n, tpb), tpb, S, W, grid, sc_same, sc_cross,
+                                 sim, cnt, 1, us))) return rc;
             }
             aliased = true;
         }

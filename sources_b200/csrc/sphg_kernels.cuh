@@ -10,8 +10,8 @@
 //   k_water_pass_a    continuity / df2, delta-SPH(rho), strain rate, EOS  pair pass
 //   k_water_pass_b    momentum, art. viscosity, delta-SPH(vof), wall force, XSPH  pair pass
 //   k_soil_pass       every same-phase soil term + flow rule + Jaumann   pair pass
-//   k_cross_soil      Darcy drag + pore pressure on soil, vof_s           pair pass
-//   k_cross_water     Darcy drag, dvof, vof2 on water, vof renorm        pair pass
+//   cross_soil_sums   Darcy drag + pore pressure on soil (in k_soil_pass) pair sums
+//   cross_water_sums  Darcy drag, dvof, vof2 on water (in k_water_pass_b) pair sums
 //   k_update          leapfrog corrector / first step (+ DP on soil)     elementwise
 // Every pair pass is a gather: one thread per particle in cell order visits
 // the 3 x 3 neighbouring cells (three contiguous row segments of the sorted
@@ -47,10 +47,10 @@ struct SimConst {
 #endif
 // minimum resident blocks per SM of each FP32 pair pass (register cap for
 // the compiler: 65,536 / (SPHG_TPB * min blocks) registers per thread); the
-// FP64 passes are left uncapped.  Timed on
-// a B200 at 912,016 particles: water_pass_a 172 -> 148 us at 8 blocks,
-// water_pass_b 234 -> 207 us at 6, cross_water 81 -> 69 us at 8; the soil
-// pass is fastest uncapped (8 blocks: 60 -> 84 us).
+// FP64 passes are left uncapped.  Timed on a B200 at 912,016 particles:
+// water_pass_a 172 -> 148 us at 8 blocks.  water_pass_b with the cross
+// pairs: 222 / 210 / 254 / 307 us at 5 / 6 / 7 / 8 blocks.  soil_pass with
+// the cross pairs: 86 us uncapped (128 registers), 91 at 5, 86 at 6.
 #ifndef SPHG_MINB_A
 #define SPHG_MINB_A 8
 #endif
@@ -59,9 +59,6 @@ struct SimConst {
 #endif
 #ifndef SPHG_MINB_SOIL
 #define SPHG_MINB_SOIL 1
-#endif
-#ifndef SPHG_MINB_CROSS
-#define SPHG_MINB_CROSS 8
 #endif
 
 __device__ __forceinline__ int gtid() { return blockIdx.x * blockDim.x + threadIdx.x; }
@@ -419,6 +416,62 @@ __global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_A : 1) k_
     if (!SINGLE) count_stats(cnt, 0, 0, hits, valid);
 }
 
+// ------------------------------------------------------------- cross phase
+// Neighbour sums over the water x soil pairs (direct_find_2
+// m_particles.f90:1004), run inside the last same-phase pass of each phase.
+// Neighbours come from the other phase's records of this step.  FCH: the
+// Forchheimer drag, each pair's Darcy term scaled by (1 + k b |v_w - v_s|).
+//
+// Soil side: darcy_law :3832 and pore_water_pressure :3877; the gradient is
+// taken, as the reference does, with dx = x_water - x_soil.  With m =
+// vol*rho, Darcy's m_w*cf*(v_w - v_s)*W/(rho_w rho_s) becomes
+// vol_w*rho_w*vof_w*vof_s*(-g/k)*(v_w - v_s)*W/rho_s; the sums here are the
+// pair parts, the particle factors are applied by the caller.  The pore
+// pressure m_w p_w/(rho_w rho_s) becomes vol_w p_w / rho_s.
+template <typename T, int SKF, bool FCH, class HB>
+__device__ __forceinline__ void cross_soil_sums(HB& hb, const PhaseDev<T>& W, const GridGeom& g, const SearchConst& sc,
+                                                const SimConst& c, const KernelConst<T, SKF>& ka, double2 xa, double ha,
+                                                const RecA<T>& ra, bool valid, T& ddx, T& ddy, T& dpx, T& dpy) {
+    visit_batched(hb, g, sc, W.cell_start, W.xs, W.xsf, W.hs, xa, ha, -1, valid, [&](int m, T dx, T dy) {
+        const RecA<T> rb = W.recA[m];
+        const RecB<T> qb = W.recB[m];
+        T w, sr, rr, mh;
+        pair_kernel<T, SKF>(ka, sc, ha, W.hs, m, dx, dy, w, sr, rr, mh);
+        // x_water - x_soil = -(x_a - x_b)
+        const T gx = -sr * dx, gy = -sr * dy;
+        T q = rb.vol * rb.rho * qb.vof * w;
+        const T ux = rb.vx - ra.vx, uy = rb.vy - ra.vy;
+        if constexpr (FCH) q *= T(1) + (T)c.s_kb * sqrt(ux * ux + uy * uy);
+        ddx += q * ux;
+        ddy += q * uy;
+        const T mp = rb.vol * qb.p;
+        dpx += mp * gx;
+        dpy += mp * gy;
+    }, [&](int m) { prefetch_l1(W.recA + m); prefetch_l1(W.recB + m); });
+}
+
+// Water side: darcy_law :3832, volume_fraction_water2 :3940 (dvof) and
+// volume_fraction_water :3912 (vof2).  Returns the number of pairs.
+template <typename T, int SKF, bool FCH, class HB>
+__device__ __forceinline__ int cross_water_sums(HB& hb, const PhaseDev<T>& S, const GridGeom& g, const SearchConst& sc,
+                                                const SimConst& c, const KernelConst<T, SKF>& ka, double2 xa, double ha,
+                                                const RecA<T>& ra, bool valid, T& ddx, T& ddy, T& dvof, T& v2) {
+    return visit_batched(hb, g, sc, S.cell_start, S.xs, S.xsf, S.hs, xa, ha, -1, valid, [&](int m, T dx, T dy) {
+        const RecA<T> rb = S.recA[m];
+        const T phis = S.recB[m].vof;
+        T w, sr, rr, mh;
+        pair_kernel<T, SKF>(ka, sc, ha, S.hs, m, dx, dy, w, sr, rr, mh);
+        const T mb = rb.vol * rb.rho;
+        const T ux = ra.vx - rb.vx, uy = ra.vy - rb.vy;
+        T q = rb.vol * phis * w;
+        if constexpr (FCH) q *= T(1) + (T)c.s_kb * sqrt(ux * ux + uy * uy);
+        ddx -= q * ux;
+        ddy -= q * uy;
+        dvof -= mb * (sr * (ux * dx + uy * dy));
+        v2 += mb * w;
+    }, [&](int m) { prefetch_l1(S.recA + m); prefetch_l1(S.recB + m); });
+}
+
 // ----------------------------------------------------------- water: pass B
 // Momentum dv = (-vof*df(p) + df(vof*sxx) + df(vof*sxy)) / rho
 // (declarations_sph.f90:1257-1265; df m_particles.f90:1711), art_visc :2504,
@@ -427,8 +480,15 @@ __global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_A : 1) k_
 // vof = 1 and neither wall force nor delta-SPH on vof.  The wall force takes
 // dx = x_real - x_virtual, as the reference does with real particles
 // numbered before virtual ones.
-template <typename T, int SKF, bool SINGLE>
-__global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_B : 1) k_water_pass_b(PhaseDev<T> P, GridGeom g, SearchConst sc, SimConst c, StepCtl u) {
+//
+// Two-phase (SINGLE = false): the water side of the cross pairs follows in
+// the same kernel (cross_water_sums), then the renormalisation rho <-
+// rho/vof*vof2, vof <- vof2 every renorm_interval steps
+// (declarations_sph.f90:1414-1421), then, as the last pass of the water
+// phase, the leapfrog corrector.  FCH as in cross_water_sums.
+template <typename T, int SKF, bool SINGLE, bool FCH>
+__global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_B : 1) k_water_pass_b(PhaseDev<T> P, PhaseDev<T> S, GridGeom g, SearchConst sc,
+                                                          SearchConst scx, SimConst c, StepCtl u, DevCounters* cnt) {
     typedef typename V2<T>::t T2;
     SPHG_HITBUF(T);
     const int k = gtid();
@@ -496,21 +556,46 @@ __global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_B : 1) k_
             xsy -= q * dvy;
         }
     }, [&](int m) { prefetch_l1(rec + m); prefetch_l1(P.recB + m); });
-    if (valid) {
-        T dvx = -(phia * d1x) + d2x + d3x;
-        T dvy = -(phia * d1y) + d2y + d3y;
-        if (ra.rho > T(0)) { dvx = dvx / ra.rho; dvy = dvy / ra.rho; }
-        dvx = dvx + avx + rpx;
-        dvy = dvy + avy + rpy + (T)c.gravity;
-        T2 o; o.x = dvx; o.y = dvy;
-        P.dv[a] = o;
-        if (xsph) {
-            const T eps = (T)c.epsilon;
-            T2 av; av.x = real_a ? eps * xsx : xsx; av.y = real_a ? eps * xsy : xsy;
-            P.av[a] = av;
+    T dvx = -(phia * d1x) + d2x + d3x;
+    T dvy = -(phia * d1y) + d2y + d3y;
+    if (ra.rho > T(0)) { dvx = dvx / ra.rho; dvy = dvy / ra.rho; }
+    dvx = dvx + avx + rpx;
+    dvy = dvy + avy + rpy + (T)c.gravity;
+    if (valid && xsph) {
+        const T eps = (T)c.epsilon;
+        T2 av; av.x = real_a ? eps * xsx : xsx; av.y = real_a ? eps * xsy : xsy;
+        P.av[a] = av;
+    }
+    if constexpr (SINGLE) {
+        if (valid) {
+            T2 o; o.x = dvx; o.y = dvy;
+            P.dv[a] = o;
+            if (u.update) update_one(P, a, c, u.first, 0, 0);   // last pass of the water-only step
         }
-        if (!SINGLE) P.dvof[a] = dvf;
-        if (SINGLE && u.update) update_one(P, a, c, u.first, 0, 0);   // last pass of the water-only step
+    } else {
+        T cdx = 0, cdy = 0, cdvof = 0, cv2 = 0;
+        const int chits = cross_water_sums<T, SKF, FCH>(hb, S, g, scx, c, ka, xa, ha, ra, valid, cdx, cdy, cdvof, cv2);
+        if (valid) {
+            const T fd = phia * (T)(-c.numeric_gravity / c.s_perm);
+            T2 o; o.x = dvx + fd * cdx; o.y = dvy + fd * cdy;
+            P.dv[a] = o;
+            if (c.volume_fraction) {
+                const T irho0 = (T)(1.0 / c.s_rho0);
+                P.dvof[a] = dvf + cdvof * irho0;
+                const T vof2 = T(1) - cv2 * irho0;
+                P.vof2[a] = vof2;
+                if (c.renorm_now) {
+                    double rho = P.rho[a] / P.vof[a];
+                    P.vof[a] = (double)vof2;
+                    P.rho[a] = rho * (double)vof2;
+                }
+            } else {
+                P.dvof[a] = dvf;
+            }
+            P.countiac[a] = chits;
+            if (u.update) update_one(P, a, c, u.first, u.with_vof, 0);   // last pass of the water phase
+        }
+        count_stats(cnt, 2, -1, chits, valid);
     }
 }
 
@@ -522,9 +607,14 @@ __global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_B : 1) k_
 // s, repulsive_force (two-phase only), gravity, av_vel; then per particle
 // plastic_or_not :3447, plastic_flow_rule3 :3700 and Jaumann_rate :3047,
 // whose spin sum wxy comes from the same pass.
-template <typename T, int SKF, bool SINGLE>
-__global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_SOIL : 1) k_soil_pass(PhaseDev<T> P, GridGeom g, SearchConst sc, SimConst c,
-                                                       DevCounters* cnt, int slot, StepCtl u) {
+//
+// Two-phase (SINGLE = false): the soil side of the cross pairs follows in the
+// same kernel (cross_soil_sums), then volume_fraction_soil :3970 and, as the
+// last pass of the soil phase, the leapfrog corrector.  FCH as in
+// cross_soil_sums.
+template <typename T, int SKF, bool SINGLE, bool FCH>
+__global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_SOIL : 1) k_soil_pass(PhaseDev<T> P, PhaseDev<T> W, GridGeom g, SearchConst sc,
+                                                       SearchConst scx, SimConst c, DevCounters* cnt, int slot, StepCtl u) {
     typedef typename V2<T>::t T2;
     SPHG_HITBUF(T);
     const int k = gtid();
@@ -621,18 +711,17 @@ __global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_SOIL : 1)
         }
     }, [&](int m) { prefetch_l1(P.recA + m); prefetch_l1(P.recB + m); });
     int fail = 0, fail3 = 0;
+    T dvx, dvy;
+    if (SINGLE) { dvx = -s1x + s2x + s3x; dvy = -s1y + s2y + s3y; }
+    else {
+        dvx = -(s1x * ra.rho) + s2x * ra.rho + s3x * ra.rho;
+        dvy = -(s1y * ra.rho) + s2y * ra.rho + s3y * ra.rho;
+    }
+    if (ra.rho > T(0)) { dvx = dvx / ra.rho; dvy = dvy / ra.rho; }
+    dvx = dvx + avx + rpx;
+    dvy = dvy + avy + rpy + (T)c.gravity;
     if (valid) {
-        T dvx, dvy;
-        if (SINGLE) { dvx = -s1x + s2x + s3x; dvy = -s1y + s2y + s3y; }
-        else {
-            dvx = -(s1x * ra.rho) + s2x * ra.rho + s3x * ra.rho;
-            dvy = -(s1y * ra.rho) + s2y * ra.rho + s3y * ra.rho;
-        }
-        if (ra.rho > T(0)) { dvx = dvx / ra.rho; dvy = dvy / ra.rho; }
-        dvx = dvx + avx + rpx;
-        dvy = dvy + avy + rpy + (T)c.gravity;
-        T2 o; o.x = dvx; o.y = dvy;
-        P.dv[a] = o;
+        if (SINGLE) { T2 o; o.x = dvx; o.y = dvy; P.dv[a] = o; }
         if (xsph) {
             const T eps = (T)c.epsilon;
             T2 av; av.x = real_a ? eps * xsx : xsx; av.y = real_a ? eps * xsy : xsy;
@@ -681,123 +770,22 @@ __global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_SOIL : 1)
         P.countiac[a] = hits;
         if (SINGLE && u.update) fail3 = update_one(P, a, c, u.first, 0, u.do_dp);   // last pass of the soil-only step
     }
+    if constexpr (!SINGLE) {
+        T cdx = 0, cdy = 0, cpx = 0, cpy = 0;
+        cross_soil_sums<T, SKF, FCH>(hb, W, g, scx, c, ka, xa, ha, ra, valid, cdx, cdy, cpx, cpy);
+        if (valid) {
+            const T phis = qa.vof;
+            const T irs = T(1) / ra.rho;
+            const T fd = phis * (T)(-c.numeric_gravity / c.s_perm) * irs, fp = irs * phis;
+            T2 o; o.x = dvx + (fd * cdx + fp * cpx); o.y = dvy + (fd * cdy + fp * cpy);
+            P.dv[a] = o;
+            if (c.volume_fraction) P.vof[a] = P.rho[a] / c.s_rho0;
+            if (u.update) fail3 = update_one(P, a, c, u.first, u.with_vof, u.do_dp);   // last pass of the soil phase
+        }
+    }
     count_stats(cnt, slot, slot, hits, valid);
     if (c.plasticity == 3) count_fail(cnt, 2, fail);
-    if (SINGLE && u.update && u.do_dp) count_fail(cnt, 3, fail3);
-}
-
-// ------------------------------------------------------------- cross phase
-// Soil side of the water x soil pairs (direct_find_2 m_particles.f90:1004):
-// darcy_law :3832 and pore_water_pressure :3877, then volume_fraction_soil
-// :3970.  Neighbour data comes from the water records of this step; the
-// gradient is taken, as the reference does, with dx = x_water - x_soil.
-// With m = vol*rho, Darcy's m_w*cf*(v_w - v_s)*W/(rho_w rho_s) becomes
-// vol_w*rho_w*vof_w*vof_s*(-g/k)*(v_w - v_s)*W/rho_s and the pore pressure
-// m_w p_w/(rho_w rho_s) becomes vol_w p_w / rho_s.  FCH: the Forchheimer
-// drag, each pair's Darcy term scaled by (1 + k b |v_w - v_s|).
-template <typename T, int SKF, bool FCH>
-__global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_CROSS : 1) k_cross_soil(PhaseDev<T> S, PhaseDev<T> W, GridGeom g, SearchConst sc, SimConst c,
-                                                        StepCtl u, DevCounters* cnt) {
-    typedef typename V2<T>::t T2;
-    SPHG_HITBUF(T);
-    const int k = gtid();
-    const bool valid = k < S.n;
-    const int kk = valid ? k : 0;
-    const double2 xa = S.xs[kk];
-    const double ha = S.hs[kk];
-    const RecA<T> ra = S.recA[kk];
-    const T phis = S.recB[kk].vof;
-    const T negg_ks = (T)(-c.numeric_gravity / c.s_perm);
-    const T irs = T(1) / ra.rho;
-    KernelConst<T, SKF> ka;
-    ka.init((T)ha);
-    T ddx = 0, ddy = 0, dpx = 0, dpy = 0;
-    visit_batched(hb, g, sc, W.cell_start, W.xs, W.xsf, W.hs, xa, ha, -1, valid, [&](int m, T dx, T dy) {
-        const RecA<T> rb = W.recA[m];
-        const RecB<T> qb = W.recB[m];
-        T w, sr, rr, mh;
-        pair_kernel<T, SKF>(ka, sc, ha, W.hs, m, dx, dy, w, sr, rr, mh);
-        // x_water - x_soil = -(x_a - x_b)
-        const T gx = -sr * dx, gy = -sr * dy;
-        T q = rb.vol * rb.rho * qb.vof * w;
-        const T ux = rb.vx - ra.vx, uy = rb.vy - ra.vy;
-        if constexpr (FCH) q *= T(1) + (T)c.s_kb * sqrt(ux * ux + uy * uy);
-        ddx += q * ux;
-        ddy += q * uy;
-        const T mp = rb.vol * qb.p;
-        dpx += mp * gx;
-        dpy += mp * gy;
-    }, [&](int m) { prefetch_l1(W.recA + m); prefetch_l1(W.recB + m); });
-    int fail3 = 0;
-    if (valid) {
-        const int a = S.perm[k];
-        const T fd = phis * negg_ks * irs, fp = irs * phis;
-        T2 d = S.dv[a];
-        d.x += fd * ddx + fp * dpx;
-        d.y += fd * ddy + fp * dpy;
-        S.dv[a] = d;
-        if (c.volume_fraction) S.vof[a] = S.rho[a] / c.s_rho0;
-        if (u.update) fail3 = update_one(S, a, c, u.first, u.with_vof, u.do_dp);   // last pass of the soil phase
-    }
     if (u.update && u.do_dp) count_fail(cnt, 3, fail3);
-}
-
-// Water side: darcy_law :3832, volume_fraction_water2 :3940 (dvof),
-// volume_fraction_water :3912 (vof2), and every renorm_interval steps the
-// renormalisation rho <- rho/vof*vof2, vof <- vof2 (declarations_sph.f90:1414-1421).
-// FCH as in k_cross_soil.
-template <typename T, int SKF, bool FCH>
-__global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_CROSS : 1) k_cross_water(PhaseDev<T> W, PhaseDev<T> S, GridGeom g, SearchConst sc, SimConst c,
-                                                         DevCounters* cnt, StepCtl u) {
-    typedef typename V2<T>::t T2;
-    SPHG_HITBUF(T);
-    const int k = gtid();
-    const bool valid = k < W.n;
-    const int kk = valid ? k : 0;
-    const double2 xa = W.xs[kk];
-    const double ha = W.hs[kk];
-    const RecA<T> ra = W.recA[kk];
-    const T phiw = W.recB[kk].vof;
-    const T negg_ks = (T)(-c.numeric_gravity / c.s_perm);
-    const T irho0 = (T)(1.0 / c.s_rho0);
-    KernelConst<T, SKF> ka;
-    ka.init((T)ha);
-    T ddx = 0, ddy = 0, dvof = 0, v2 = 0;
-    const int hits = visit_batched(hb, g, sc, S.cell_start, S.xs, S.xsf, S.hs, xa, ha, -1, valid, [&](int m, T dx, T dy) {
-        const RecA<T> rb = S.recA[m];
-        const T phis = S.recB[m].vof;
-        T w, sr, rr, mh;
-        pair_kernel<T, SKF>(ka, sc, ha, S.hs, m, dx, dy, w, sr, rr, mh);
-        const T mb = rb.vol * rb.rho;
-        const T ux = ra.vx - rb.vx, uy = ra.vy - rb.vy;
-        T q = rb.vol * phis * w;
-        if constexpr (FCH) q *= T(1) + (T)c.s_kb * sqrt(ux * ux + uy * uy);
-        ddx -= q * ux;
-        ddy -= q * uy;
-        dvof -= mb * (sr * (ux * dx + uy * dy));
-        v2 += mb * w;
-    }, [&](int m) { prefetch_l1(S.recA + m); prefetch_l1(S.recB + m); });
-    if (valid) {
-        const int a = W.perm[k];
-        const T fd = phiw * negg_ks;
-        T2 d = W.dv[a];
-        d.x += fd * ddx;
-        d.y += fd * ddy;
-        W.dv[a] = d;
-        if (c.volume_fraction) {
-            W.dvof[a] = W.dvof[a] + dvof * irho0;
-            const T vof2 = T(1) - v2 * irho0;
-            W.vof2[a] = vof2;
-            if (c.renorm_now) {
-                double rho = W.rho[a] / W.vof[a];
-                W.vof[a] = (double)vof2;
-                W.rho[a] = rho * (double)vof2;
-            }
-        }
-        W.countiac[a] = hits;
-        if (u.update) update_one(W, a, c, u.first, u.with_vof, 0);   // last pass of the water phase
-    }
-    count_stats(cnt, 2, -1, hits, valid);
 }
 
 // Sticky per-batch flags: a pair list above max_interaction (the reference

@@ -229,12 +229,15 @@ struct WsShape {
     static constexpr uint32_t B_KC = N * 16;            // ... of the resident B
     static constexpr uint32_t A_BYTES = (K / 8) * A_KC;
     static constexpr uint32_t B_BYTES = (K / 8) * B_KC;
-    static constexpr uint32_t SMEM = B_BYTES + 2 * A_BYTES + 32;
+    static constexpr uint32_t STAGE_OFF = B_BYTES + 2 * A_BYTES + 32;   // epilogue staging, 16-byte aligned
+    static constexpr uint32_t STAGE_BYTES = 8 * 32 * 64;                  // 8 warps x 32 rows x 16 fp32
+    static constexpr uint32_t SMEM = STAGE_OFF + STAGE_BYTES;
     static constexpr int TCOLS = 2 * N;                 // two accumulators
-    // at most 2 CTAs per SM (TMEM: 2 x 256 columns), 1 when N = 256
+    // at most 2 CTAs per SM (TMEM: 2 x 256 columns), 1 when N = 256; the SM
+    // holds 228 KB of shared memory, 1 KB of it reserved per CTA
     static constexpr uint32_t SMEM_REQ = N == 256 ? (SMEM > 120 * 1024 ? SMEM : 120 * 1024)
                                                   : (SMEM > 100 * 1024 ? SMEM : 100 * 1024);
-    static constexpr int PER_SM = N == 256 || SMEM > 110 * 1024 ? 1 : 2;
+    static constexpr int PER_SM = N == 256 || 2 * (SMEM_REQ + 1024) > 228 * 1024 ? 1 : 2;
 };
 
 constexpr int WS_THREADS = 256;   // 8 warps: warps w and w + 4 share TMEM lanes 32 (w % 4) ..
@@ -331,6 +334,96 @@ __device__ __forceinline__ void ws_epilogue(const SphgGemmEpi& ep, uint32_t tacc
     }
 }
 
+// The same epilogue through a per-warp staging tile in shared memory.  The
+// warp's 32 accumulator rows (one per lane, as TMEM delivers them) are
+// written to shared memory and read back so that 4 lanes cover the 64
+// contiguous bytes of one row's 16-column chunk: every global load and store
+// of the epilogue then touches 8 rows per instruction instead of 32.  In the
+// staging tile row r holds 4 16-byte units, unit u at slot u ^ ((r >> 1) & 3),
+// so that both the row-per-lane writes and the 4-lanes-per-row reads are free
+// of bank conflicts.  Sums are formed in the same order as ws_epilogue.
+template <int N, int K>
+__device__ __forceinline__ void ws_epilogue_staged(const SphgGemmEpi& ep, uint32_t tacc, long long row0, int c0,
+                                                   float4* __restrict__ stage, int lane) {
+    constexpr int CW = 16;
+    const int q = lane & 3, rs = lane >> 2;   // this lane's 16-byte unit, and its row within each group of 8
+    const bool readz = ep.mode == SPHG_EPI_ACC || ep.mode == SPHG_EPI_RESID;
+    const bool bias = ep.mode != SPHG_EPI_STORE && ep.mode != SPHG_EPI_ACC;
+    const bool hout = ep.mode != SPHG_EPI_STORE && ep.mode != SPHG_EPI_ACC && ep.h;
+    const bool act = ep.mode == SPHG_EPI_EDGE || (ep.mode == SPHG_EPI_BIAS_ACT && ep.relu);
+    bool edge[4];
+    const float4* ps[4];
+    const float4* pd[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const long long r = row0 + 8 * i + rs;
+        edge[i] = ep.mode == SPHG_EPI_EDGE && r < ep.nedge;
+        ps[i] = pd[i] = nullptr;
+        if (edge[i]) {
+            ps[i] = reinterpret_cast<const float4*>(ep.P + (long long)ep.src[r] * 2 * N);
+            pd[i] = reinterpret_cast<const float4*>(ep.P + (long long)ep.dst[r] * 2 * N + N);
+        }
+    }
+    const int wsw = (lane >> 1) & 3;   // swizzle of this lane's own staging row
+#pragma unroll 1
+    for (int c = c0; c < c0 + N / 2; c += CW) {
+        const int col = c + 4 * q;
+        float4 add[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            add[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (readz) add[i] = reinterpret_cast<const float4*>(ep.z + (row0 + 8 * i + rs) * N)[col / 4];
+            if (edge[i]) add[i] = add4f(add[i], add4f(ps[i][col / 4], pd[i][col / 4]));
+        }
+        if (bias) {
+            const float4 b4 = reinterpret_cast<const float4*>(ep.bias)[col / 4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) add[i] = add4f(add[i], b4);
+        }
+        float v[CW];
+        tmem_ld16(tacc + (uint32_t)c, v);
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            stage[lane * 4 + (u ^ wsw)] = make_float4(v[4 * u], v[4 * u + 1], v[4 * u + 2], v[4 * u + 3]);
+        __syncwarp();
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int r = 8 * i + rs;
+            const float4 a = stage[r * 4 + (q ^ ((r >> 1) & 3))];
+            float o[4] = {a.x + add[i].x, a.y + add[i].y, a.z + add[i].z, a.w + add[i].w};
+            const long long grow = row0 + r;
+            if (ep.z) reinterpret_cast<float4*>(ep.z + grow * N)[col / 4] = make_float4(o[0], o[1], o[2], o[3]);
+            if (hout) {
+                if (act) {
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) o[j] = fmaxf(o[j], 0.f);
+                }
+                __nv_bfloat162 t0 = __floats2bfloat162_rn(o[0], o[1]), t1 = __floats2bfloat162_rn(o[2], o[3]);
+                uint2 hv;
+                hv.x = *reinterpret_cast<uint32_t*>(&t0);
+                hv.y = *reinterpret_cast<uint32_t*>(&t1);
+                reinterpret_cast<uint2*>(static_cast<__nv_bfloat16*>(ep.h) + grow * N)[col / 4] = hv;
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// Staged epilogue (1) or the row-per-lane one (0).
+#ifndef SPHG_WS_STAGED
+#define SPHG_WS_STAGED 1
+#endif
+
+template <int N, int K>
+__device__ __forceinline__ void ws_epilogue_any(const SphgGemmEpi& ep, uint32_t tacc, long long row0, int c0,
+                                                float4* stage, int lane) {
+#if SPHG_WS_STAGED
+    ws_epilogue_staged<N, K>(ep, tacc, row0, c0, stage, lane);
+#else
+    ws_epilogue<N, K>(ep, tacc, row0 + lane, c0);
+#endif
+}
+
 template <int N, int K>
 __global__ void __launch_bounds__(WS_THREADS, 2) k_gemm_ws(const __nv_bfloat16* __restrict__ A,
                                                     const __nv_bfloat16* __restrict__ B, int M, SphgGemmEpi ep,
@@ -342,6 +435,7 @@ __global__ void __launch_bounds__(WS_THREADS, 2) k_gemm_ws(const __nv_bfloat16* 
     uint64_t* mbar = (uint64_t*)(smem + S::B_BYTES + 2 * S::A_BYTES);
     uint32_t* tslot = (uint32_t*)(mbar + 2);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    float4* stage = reinterpret_cast<float4*>(smem + S::STAGE_OFF) + warp * 128;
     const int ntiles = M / 128;
     const int my = blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
     auto tile_m0 = [&](int i) { return ((int)blockIdx.x + i * (int)gridDim.x) * 128; };
@@ -418,8 +512,8 @@ __global__ void __launch_bounds__(WS_THREADS, 2) k_gemm_ws(const __nv_bfloat16* 
         asm volatile("tcgen05.fence::after_thread_sync;" ::);
         if (i + 1 < my) ws_load_a<N, K>(sA0 + p * S::A_BYTES, A, tile_m0(i + 1), tid);
         cp_async_commit();
-        ws_epilogue<N, K>(ep, tmem + lane_off + (uint32_t)(p * N), (long long)tile_m0(i - 1) + (warp & 3) * 32 + lane,
-                          col0);
+        ws_epilogue_any<N, K>(ep, tmem + lane_off + (uint32_t)(p * N), (long long)tile_m0(i - 1) + (warp & 3) * 32,
+                              col0, stage, lane);
         asm volatile("tcgen05.fence::before_thread_sync;" ::);
         __syncthreads();
     }
@@ -431,8 +525,8 @@ __global__ void __launch_bounds__(WS_THREADS, 2) k_gemm_ws(const __nv_bfloat16* 
             ph ^= 1u << s;
             ++waited;
             asm volatile("tcgen05.fence::after_thread_sync;" ::);
-            ws_epilogue<N, K>(ep, tmem + lane_off + (uint32_t)(s * N),
-                              (long long)tile_m0(my - 1) + (warp & 3) * 32 + lane, col0);
+            ws_epilogue_any<N, K>(ep, tmem + lane_off + (uint32_t)(s * N), (long long)tile_m0(my - 1) + (warp & 3) * 32,
+                                  col0, stage, lane);
         }
     }
     if (!ok) {

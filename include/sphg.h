@@ -179,6 +179,19 @@ int sphg_single_step(sphg_ctx* ctx, int itimestep);
  * *itimestep and *time are advanced as the module globals are. */
 int sphg_time_integration(sphg_ctx* ctx, int maxtimestep, int* itimestep, double* time);
 
+/* A group of contexts stepped together (no counterpart in the reference; the
+ * batched ensemble uses it, one context per kind of scene).  Every step of the
+ * group after the first replays ONE CUDA graph that holds each context's step
+ * as a parallel branch, forked from and joined into the stream of ctxs[0], so
+ * the contexts' kernels overlap on the GPU.  The results are those of calling
+ * sphg_time_integration on each context in turn.  itimesteps and times hold
+ * one entry per context, as sphg_time_integration's arguments, and all
+ * itimesteps must be equal.  Destroy a group before its contexts. */
+typedef struct sphg_group sphg_group;
+int sphg_group_create(sphg_ctx* const* ctxs, int n, sphg_group** out);
+int sphg_group_time_integration(sphg_group* group, int maxtimestep, int* itimesteps, double* times);
+void sphg_group_destroy(sphg_group* group);
+
 /* Copy one phase back into the Fortran arrays (original particle order). */
 int sphg_download_phase(sphg_ctx* ctx, int phase, sphg_phase_host* v);
 

@@ -31,7 +31,8 @@ EXPORTS = ("sphg_default_params", "sphg_create", "sphg_upload_phase", "sphg_sing
            "sphg_set_stream", "sphg_kernel_profile", "sphg_kernel_report", "sphg_destroy",
            "sphg_strerror", "sphg_sum_density_noalloc", "sphg_set_scenes", "sphg_upload_scene_ids",
            "sphg_set_tuning", "sphg_read_case", "sphg_write_tecplot_phase", "sphg_write_tecplot",
-           "sphg_gemm_bf16_tn", "sphg_export_xv_device", "sphg_import_xv_device", *sorted(_GNN_SIGNATURES := {
+           "sphg_gemm_bf16_tn", "sphg_export_xv_device", "sphg_import_xv_device", "sphg_group_create",
+           "sphg_group_time_integration", "sphg_group_destroy", *sorted(_GNN_SIGNATURES := {
                # message-passing network kernels (include/sphg_learn.h); P pointer,
                # I int, L 64-bit count, F float, D double, S size_t pointer
                "sphg_gemm_bf16_ws": "PPIIIPPP",
@@ -102,6 +103,10 @@ def load(path: str = LIB_PATH):
                                      C.POINTER(C.c_int32)]
     L.sphg_sum_density_noalloc.argtypes = [C.POINTER(Params), C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
                                            C.c_void_p, C.c_void_p, C.c_void_p]
+    L.sphg_group_create.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.POINTER(P)]
+    L.sphg_group_time_integration.argtypes = [P, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double)]
+    L.sphg_group_destroy.argtypes = [P]
+    L.sphg_group_destroy.restype = None
     L.sphg_export_xv_device.argtypes = [P, C.c_int, P, P]
     L.sphg_import_xv_device.argtypes = [P, C.c_int, P, P]
     codes = {"P": C.c_void_p, "I": C.c_int, "L": C.c_longlong, "F": C.c_float, "D": C.c_double}
@@ -251,3 +256,38 @@ class Solver:
 
     def __exit__(self, *a):
         self.close()
+
+
+class SolverGroup:
+    """Several Solvers stepped together (sphg_group_*): after the first step,
+    one CUDA graph per step holds every context's step as a parallel branch.
+    Results equal stepping each Solver in turn.  All members must be at the
+    same itimestep; close the group before its Solvers."""
+
+    def __init__(self, solvers):
+        self.L = load()
+        self.solvers = list(solvers)
+        arr = (C.c_void_p * len(self.solvers))(*[sv.h.value for sv in self.solvers])
+        h = C.c_void_p()
+        _check(self.L.sphg_group_create(arr, len(self.solvers), C.byref(h)), "sphg_group_create")
+        self.h = h
+
+    def time_integration(self, maxtimestep: int):
+        n = len(self.solvers)
+        its = (C.c_int * n)(*[sv.itimestep for sv in self.solvers])
+        ts = (C.c_double * n)(*[sv.time for sv in self.solvers])
+        rc = self.L.sphg_group_time_integration(self.h, maxtimestep, its, ts)
+        for k, sv in enumerate(self.solvers):
+            sv.itimestep, sv.time = its[k], ts[k]
+        _check(rc, "sphg_group_time_integration")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.sphg_group_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -67,6 +67,14 @@ struct EngineBase {
     virtual int upload_scene_ids(int phase, const int32_t* ids) = 0;
     virtual int set_tuning(const sphg_tuning* t) = 0;
     virtual int xv_device(int phase, double* x, double* v, int to_caller) = 0;
+    // Joint graphs of several contexts (sphg_group_*): the kind of graph a
+    // regular step replays (-1: this step runs without a graph), the step's
+    // launches on ctx->stream for capture, and the bookkeeping of a replay.
+    virtual int graph_kind(int itimestep) = 0;
+    virtual int prepare_graph_step() = 0;
+    virtual int capture_step(int itimestep) = 0;
+    virtual void after_graph_step(long long launches) = 0;
+    virtual long long graph_epoch() const = 0;
 };
 
 struct sphg_ctx {
@@ -623,9 +631,28 @@ struct Engine : EngineBase {
     cudaGraphExec_t graphs[4] = {nullptr, nullptr, nullptr, nullptr};
     bool use_graphs = true;
 
+    long long epoch = 0;    // counts drop_graphs(): joint graphs of older epochs are stale
     void drop_graphs() {
         for (auto& g : graphs) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+        ++epoch;
     }
+
+    int graph_kind(int itimestep) override {
+        if (itimestep < 2 || !use_graphs || ctx->prof.on) return -1;
+        return step_kind(itimestep);
+    }
+    int prepare_graph_step() override { return prepare(); }
+    int capture_step(int itimestep) override {
+        StepCtl u{};
+        u.update = 1;
+        return run(itimestep, 1, u);
+    }
+    void after_graph_step(long long launches) override {
+        nfail_slot = 3;
+        if (!ctx->prm.single_phase) aliased = true;
+        ctx->prof.launches += launches;
+    }
+    long long graph_epoch() const override { return epoch; }
 
     int step_kind(int itimestep) const {
         const sphg_params& p = ctx->prm;
@@ -1029,6 +1056,206 @@ int sphg_time_integration(sphg_ctx* c, int maxtimestep, int* itimestep, double* 
     c->itimestep = *itimestep;
     c->time = *time;
     return rc ? rc : rc2;
+}
+
+// ------------------------------------------------------- context groups
+// One CUDA graph per step for several contexts: each context's step is a
+// branch of the graph, forked from and joined back into the stream of the
+// first context, so the contexts' kernels can overlap on the GPU.  A graph is
+// kept per combination of the contexts' step kinds and recaptured when any
+// context has dropped its own graphs (upload, tuning).
+struct sphg_group {
+    std::vector<sphg_ctx*> ctx;
+    struct Joint {
+        cudaGraphExec_t exec = nullptr;
+        std::vector<long long> launches, epochs;
+    };
+    std::map<unsigned long long, Joint> joint;
+    std::vector<cudaEvent_t> ev;   // 0: fork; 1..n-1: joins
+    bool use_graphs = true;
+    ~sphg_group() {
+        for (auto& kv : joint) if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+        for (auto e : ev) cudaEventDestroy(e);
+    }
+};
+
+namespace {
+
+// Capture the joint graph of step `ts`.  On entry every context's stream is
+// stream 0 (the stream of context 0); context i > 0 is captured on its
+// private stream, forked from and joined into stream 0.
+int group_capture(sphg_group* g, int ts, sphg_group::Joint& J) {
+    const int n = (int)g->ctx.size();
+    cudaStream_t origin = g->ctx[0]->stream;
+    std::vector<cudaStream_t> saved(n);
+    for (int i = 0; i < n; ++i) saved[i] = g->ctx[i]->stream;
+    J.launches.assign(n, 0);
+    J.epochs.assign(n, 0);
+    if (cudaStreamBeginCapture(origin, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        return -1;
+    }
+    int rc = 0;
+    cudaError_t e = cudaEventRecord(g->ev[0], origin);
+    for (int i = 1; i < n && e == cudaSuccess; ++i) {
+        g->ctx[i]->stream = g->ctx[i]->own_stream;
+        e = cudaStreamWaitEvent(g->ctx[i]->stream, g->ev[0], 0);
+    }
+    for (int i = 0; i < n && e == cudaSuccess && rc == 0; ++i) {
+        const long long before = g->ctx[i]->prof.launches;
+        rc = g->ctx[i]->eng->capture_step(ts);
+        J.launches[i] = g->ctx[i]->prof.launches - before;
+        g->ctx[i]->prof.launches = before;
+        J.epochs[i] = g->ctx[i]->eng->graph_epoch();
+    }
+    for (int i = 1; i < n && e == cudaSuccess; ++i) {
+        e = cudaEventRecord(g->ev[i], g->ctx[i]->stream);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(origin, g->ev[i], 0);
+    }
+    cudaGraph_t graph = nullptr;
+    cudaError_t ee = cudaStreamEndCapture(origin, &graph);
+    for (int i = 0; i < n; ++i) g->ctx[i]->stream = saved[i];
+    if (rc || e != cudaSuccess || ee != cudaSuccess || !graph) {
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        return rc ? rc : -1;
+    }
+    cudaError_t ei = cudaGraphInstantiate(&J.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ei != cudaSuccess) { J.exec = nullptr; cudaGetLastError(); return -1; }
+    return 0;
+}
+
+// One step of every context: a joint graph replay when every context can
+// replay one, else each context's own step in turn.
+int group_step(sphg_group* g, int ts) {
+    const int n = (int)g->ctx.size();
+    unsigned long long key = 0;
+    bool graphed = g->use_graphs;
+    for (int i = 0; i < n && graphed; ++i) {
+        const int k = g->ctx[i]->eng->graph_kind(ts);
+        if (k < 0) graphed = false;
+        key |= (unsigned long long)k << (2 * i);
+    }
+    if (graphed) {
+        for (int i = 0; i < n; ++i) {
+            int rc = g->ctx[i]->eng->prepare_graph_step();
+            if (rc) return rc;
+        }
+        auto it = g->joint.find(key);
+        if (it != g->joint.end()) {
+            bool stale = false;
+            for (int i = 0; i < n; ++i) stale |= it->second.epochs[i] != g->ctx[i]->eng->graph_epoch();
+            if (stale) {
+                if (it->second.exec) cudaGraphExecDestroy(it->second.exec);
+                g->joint.erase(it);
+                it = g->joint.end();
+            }
+        }
+        if (it == g->joint.end()) {
+            sphg_group::Joint J;
+            int rc = group_capture(g, ts, J);
+            if (rc > 0) return rc;
+            if (rc < 0) g->use_graphs = false;
+            else it = g->joint.emplace(key, J).first;
+        }
+        if (g->use_graphs) {
+            CUDA_TRY(cudaGraphLaunch(it->second.exec, g->ctx[0]->stream));
+            for (int i = 0; i < n; ++i) g->ctx[i]->eng->after_graph_step(it->second.launches[i]);
+            return 0;
+        }
+    }
+    for (int i = 0; i < n; ++i) {
+        int rc = g->ctx[i]->eng->step(ts);
+        if (rc) return rc;
+    }
+    return 0;
+}
+
+}  // namespace
+
+int sphg_group_create(sphg_ctx* const* ctxs, int n, sphg_group** out) {
+    if (!ctxs || !out || n < 1 || n > 32) return SPHG_ERR_BAD_ARG;
+    *out = nullptr;
+    for (int i = 0; i < n; ++i) {
+        if (!ctxs[i] || ctxs[i]->device != ctxs[0]->device) return SPHG_ERR_BAD_ARG;
+        for (int j = 0; j < i; ++j) if (ctxs[j] == ctxs[i]) return SPHG_ERR_BAD_ARG;
+    }
+    cudaSetDevice(ctxs[0]->device);
+    sphg_group* g = new sphg_group();
+    g->ctx.assign(ctxs, ctxs + n);
+    g->ev.assign(n, nullptr);
+    for (int i = 0; i < n; ++i) {
+        if (cudaEventCreateWithFlags(&g->ev[i], cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            delete g;
+            return SPHG_ERR_CUDA;
+        }
+    }
+    *out = g;
+    return SPHG_OK;
+}
+
+int sphg_group_time_integration(sphg_group* g, int maxtimestep, int* itimesteps, double* times) {
+    if (!g || !itimesteps || !times || maxtimestep < 0) return SPHG_ERR_BAD_ARG;
+    const int n = (int)g->ctx.size();
+    for (int i = 1; i < n; ++i) if (itimesteps[i] != itimesteps[0]) return SPHG_ERR_BAD_ARG;
+    cudaSetDevice(g->ctx[0]->device);
+    cudaStream_t origin = g->ctx[0]->stream;
+    std::vector<cudaStream_t> own(n);
+    for (int i = 0; i < n; ++i) own[i] = g->ctx[i]->stream;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a); cudaEventCreate(&b);
+    int rc = 0;
+    for (int i = 0; i < n && rc == 0; ++i) rc = g->ctx[i]->eng->begin_batch();
+    // Every step of the group runs on stream 0, graph replays and steps
+    // without a graph alike, so that they stay in order; only inside a joint
+    // graph do the contexts run as parallel branches.  Stream 0 first waits
+    // for the other contexts' earlier work.
+    for (int i = 1; i < n; ++i) {
+        if (own[i] == origin) continue;
+        cudaEventRecord(g->ev[i], own[i]);
+        cudaStreamWaitEvent(origin, g->ev[i], 0);
+    }
+    for (int i = 0; i < n; ++i) g->ctx[i]->stream = origin;
+    cudaEventRecord(a, origin);
+    for (int it = 0; it < maxtimestep && rc == 0; ++it) {
+        const int ts = itimesteps[0] + 1;
+        rc = group_step(g, ts);
+        if (rc) break;
+        for (int i = 0; i < n; ++i) {
+            itimesteps[i] = ts;
+            times[i] = times[i] + g->ctx[i]->prm.dt;
+        }
+    }
+    cudaEventRecord(b, origin);
+    for (int i = 0; i < n; ++i) g->ctx[i]->stream = own[i];
+    // the other contexts' later work (statistics, downloads) after stream 0
+    for (int i = 1; i < n; ++i) {
+        if (own[i] == origin) continue;
+        cudaStreamWaitEvent(own[i], b, 0);
+    }
+    int rc2 = 0;
+    for (int i = 0; i < n; ++i) {
+        int r = g->ctx[i]->eng->finish_batch();
+        if (!rc2) rc2 = r;
+    }
+    float ms = 0.f;
+    cudaEventSynchronize(b);
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a); cudaEventDestroy(b);
+    for (int i = 0; i < n; ++i) {
+        g->ctx[i]->last_step_ms = maxtimestep > 0 ? ms / maxtimestep : 0.0;
+        g->ctx[i]->itimestep = itimesteps[i];
+        g->ctx[i]->time = times[i];
+    }
+    return rc ? rc : rc2;
+}
+
+void sphg_group_destroy(sphg_group* g) {
+    if (!g) return;
+    cudaSetDevice(g->ctx[0]->device);
+    delete g;
 }
 
 int sphg_download_phase(sphg_ctx* c, int phase, sphg_phase_host* v) {

@@ -29,7 +29,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from . import Solver, scenes
+from . import Solver, SolverGroup, scenes
 from .abi import SPHG_FP32, SPHG_SOIL, SPHG_WATER, Params, PhaseArrays
 from .scenes import Scene, _copy_params
 
@@ -194,6 +194,7 @@ class Ensemble:
                 g.tuning, self.tuning_table[kind] = autotune(g)
             self.groups.append(g)
         self.solvers = [_solver(g, g.tuning) for g in self.groups]
+        self.group = None
 
     @property
     def n_particles(self) -> int:
@@ -204,8 +205,11 @@ class Ensemble:
             sv.set_stream(handle)
 
     def time_integration(self, nsteps: int):
-        for sv in self.solvers:
-            sv.time_integration(nsteps)
+        """Every group nsteps steps: one CUDA graph per step for all groups
+        (SolverGroup) once they are built."""
+        if self.group is None:
+            self.group = SolverGroup(self.solvers)
+        self.group.time_integration(nsteps)
 
     def scene(self, index: int):
         """Per-phase PhaseArrays of one scene, in its own coordinates."""
@@ -227,6 +231,9 @@ class Ensemble:
         raise IndexError(index)
 
     def close(self):
+        if self.group is not None:
+            self.group.close()
+            self.group = None
         for sv in self.solvers:
             sv.close()
         self.solvers = []

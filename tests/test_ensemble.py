@@ -96,3 +96,35 @@ def test_no_pair_crosses_scenes_and_autotuner_picks(cuda_ok):
         ens.time_integration(5)
     finally:
         ens.close()
+
+
+@pytest.mark.gpu
+def test_group_step_equals_contexts_stepped_in_turn(cuda_ok):
+    """One joint CUDA graph per step for all groups (sphg_group_*) gives
+    bit-identical states to stepping each context on its own, across reorder
+    steps and after a tuning change that makes the joint graphs stale."""
+    sp = small_specs()
+    a = ensemble.Ensemble(sp, tune=False)
+    b = ensemble.Ensemble(sp, tune=False)
+    try:
+        def check(steps):
+            for sa, sb in zip(a.solvers, b.solvers):
+                assert sa.itimestep == sb.itimestep == steps and sa.time == sb.time
+                for k in range(sa.nphase):
+                    pa, pb = sa.download(k + 1), sb.download(k + 1)
+                    for f in ("x", "vx", "rho", "p", "vof", "sxx", "sxy", "syy", "dvx", "drho"):
+                        assert np.array_equal(getattr(pa, f), getattr(pb, f)), (k, f)
+                assert list(sa.stats().niac) == list(sb.stats().niac)
+        a.time_integration(23)
+        for sv in b.solvers:
+            sv.time_integration(23)
+        check(23)
+        for sv in a.solvers + b.solvers:
+            sv.set_tuning(1.0, 7, 2)
+        a.time_integration(9)
+        for sv in b.solvers:
+            sv.time_integration(9)
+        check(32)
+    finally:
+        a.close()
+        b.close()

@@ -88,6 +88,7 @@ struct sphg_ctx {
     int itimestep = 0;
     double time = 0.0;
     double last_step_ms = 0.0;
+    cudaEvent_t ev_a = nullptr, ev_b = nullptr;   // timing of sphg_time_integration, made once
 };
 
 #define CUDA_TRY(x)                                        \
@@ -166,6 +167,7 @@ struct Engine : EngineBase {
         }
         kern<<<grid_, block, 0, ctx->stream>>>(args...);
         ctx->prof.launches++;
+        counters_fresh = false;
         cudaError_t e = cudaGetLastError();
         if (ctx->prof.on) {
             cudaEventRecord(b, ctx->stream);
@@ -744,6 +746,7 @@ struct Engine : EngineBase {
     }
 
     int begin_batch() override {
+        counters_fresh = false;
         if (!sticky) return 0;
         CUDA_TRY(cudaMemsetAsync(sticky, 0, 4 * sizeof(int), ctx->stream));
         return 0;
@@ -755,10 +758,14 @@ struct Engine : EngineBase {
         CUDA_TRY(cudaMemcpyAsync(&hcnt, cnt, sizeof(hcnt), cudaMemcpyDeviceToHost, ctx->stream));
         CUDA_TRY(cudaMemcpyAsync(hs, sticky, sizeof(hs), cudaMemcpyDeviceToHost, ctx->stream));
         CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-        if (hs[1]) return SPHG_ERR_NONFINITE;
-        if (hs[0]) return SPHG_ERR_PAIR_OVERFLOW;
-        return 0;
+        batch_rc = hs[1] ? SPHG_ERR_NONFINITE : hs[0] ? SPHG_ERR_PAIR_OVERFLOW : 0;
+        counters_fresh = true;
+        return batch_rc;
     }
+    // the host copy of the counters matches the device (no launch since the
+    // last finish_batch), so sphg_stats needs no second copy and sync
+    bool counters_fresh = false;
+    int batch_rc = 0;
 
     // ------------------------------------------------------------- download
     template <typename S>
@@ -922,7 +929,7 @@ struct Engine : EngineBase {
     }
 
     int stats(sphg_stats_t* out) override {
-        int rc = finish_batch();
+        int rc = counters_fresh ? batch_rc : finish_batch();
         memset(out, 0, sizeof(*out));
         out->niac[0] = (int64_t)(hcnt.pairs[0] / 2);
         out->niac[1] = (int64_t)(hcnt.pairs[1] / 2);
@@ -1035,8 +1042,11 @@ int sphg_single_step(sphg_ctx* c, int itimestep) {
 int sphg_time_integration(sphg_ctx* c, int maxtimestep, int* itimestep, double* time) {
     if (!c || !itimestep || !time || maxtimestep < 0) return SPHG_ERR_BAD_ARG;
     cudaSetDevice(c->device);
-    cudaEvent_t a, b;
-    cudaEventCreate(&a); cudaEventCreate(&b);
+    if (!c->ev_a && (cudaEventCreate(&c->ev_a) != cudaSuccess || cudaEventCreate(&c->ev_b) != cudaSuccess)) {
+        cudaGetLastError();
+        return SPHG_ERR_CUDA;
+    }
+    cudaEvent_t a = c->ev_a, b = c->ev_b;
     cudaEventRecord(a, c->stream);
     int rc = c->eng->begin_batch();
     for (int it = 0; it < maxtimestep && rc == 0; ++it) {
@@ -1051,7 +1061,6 @@ int sphg_time_integration(sphg_ctx* c, int maxtimestep, int* itimestep, double* 
     float ms = 0.f;
     cudaEventSynchronize(b);
     cudaEventElapsedTime(&ms, a, b);
-    cudaEventDestroy(a); cudaEventDestroy(b);
     c->last_step_ms = maxtimestep > 0 ? ms / maxtimestep : 0.0;
     c->itimestep = *itimestep;
     c->time = *time;
@@ -1365,6 +1374,8 @@ void sphg_destroy(sphg_ctx* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     c->prof.resolve();
     delete c->eng;
+    if (c->ev_a) cudaEventDestroy(c->ev_a);
+    if (c->ev_b) cudaEventDestroy(c->ev_b);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
 }

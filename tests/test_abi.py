@@ -127,6 +127,14 @@ def test_create_validates_before_touching_the_device(lib):
     p.abi_version = abi.SPHG_ABI_VERSION
     assert lib.sphg_create(None, 2, C.byref(h)) == abi.SPHG_ERR_BAD_ARG
     assert lib.sphg_single_step(None, 1) == abi.SPHG_ERR_BAD_ARG
+    # groups: no contexts, too many, a null member
+    g = C.c_void_p()
+    none = (C.c_void_p * 2)(None, None)
+    assert lib.sphg_group_create(none, 0, C.byref(g)) == abi.SPHG_ERR_BAD_ARG
+    assert lib.sphg_group_create(none, 33, C.byref(g)) == abi.SPHG_ERR_BAD_ARG
+    assert lib.sphg_group_create(none, 2, C.byref(g)) == abi.SPHG_ERR_BAD_ARG
+    assert lib.sphg_group_time_integration(None, 1, None, None) == abi.SPHG_ERR_BAD_ARG
+    lib.sphg_group_destroy(None)
     assert lib.sphg_stats(None, None) == abi.SPHG_ERR_BAD_ARG
 
 

@@ -89,6 +89,9 @@ struct sphg_ctx {
     double time = 0.0;
     double last_step_ms = 0.0;
     cudaEvent_t ev_a = nullptr, ev_b = nullptr;   // timing of sphg_time_integration, made once
+    // the soil pass runs beside water_pass_b on this stream, forked and joined by events
+    cudaStream_t side_stream = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 };
 
 #define CUDA_TRY(x)                                        \
@@ -608,18 +611,41 @@ struct Engine : EngineBase {
             if ((rc = launch("gather", k_gather<T>, blocks(W.n, 256), 256, W, sim, 0, 0, fh, 1, 0, cnt))) return rc;
             if ((rc = launch("gather", k_gather<T>, blocks(S.n, 256), 256, S, sim, 1, dp, fh, 1, dp, cnt))) return rc;
             if ((rc = launch("water_pass_a", k_water_pass_a<T, SKF, false>, blocks(W.n, tpb), tpb, W, grid, sc_same, sim, cnt))) return rc;
-            // the cross pairs run inside the last pass of each phase; the soil
-            // pass reads the water pressure that water_pass_a sets
-            if (p.forchheimer_b != 0.0) {
-                if ((rc = launch("water_pass_b", k_water_pass_b<T, SKF, false, true>, blocks(W.n, tpb), tpb, W, S, grid, sc_same,
-                                 sc_cross, sim, uw, cnt))) return rc;
-                if ((rc = launch("soil_pass", k_soil_pass<T, SKF, false, true>, blocks(S.n, tpb), tpb, S, W, grid, sc_same, sc_cross,
-                                 sim, cnt, 1, us))) return rc;
-            } else {
-                if ((rc = launch("water_pass_b", k_water_pass_b<T, SKF, false, false>, blocks(W.n, tpb), tpb, W, S, grid, sc_same,
-                                 sc_cross, sim, uw, cnt))) return rc;
-                if ((rc = launch("soil_pass", k_soil_pass<T, SKF, false, false>, blocks(S.n, tpb), tpb, S, W, grid, sc_same, sc_cross,
-                                 sim, cnt, 1, us))) return rc;
+            // The cross pairs run inside the last pass of each phase; the soil
+            // pass reads the water pressure that water_pass_a sets.  After
+            // water_pass_a the two last passes share no data: each reads the
+            // other phase's sorted records only, and writes its own phase's
+            // state (the counters by atomics).  So the soil pass runs on a
+            // side stream beside water_pass_b and fills the SMs its last
+            // partial wave leaves idle.  While kernels are timed one by one
+            // (sphg_kernel_profile) it runs on the main stream, so that each
+            // pass's time is its own.
+            const bool fch = p.forchheimer_b != 0.0;
+            cudaStream_t main_stream = ctx->stream;
+            cudaStream_t side = ctx->prof.on ? main_stream : ctx->side_stream;
+            if (side != main_stream) {
+                CUDA_TRY(cudaEventRecord(ctx->ev_fork, main_stream));
+                CUDA_TRY(cudaStreamWaitEvent(side, ctx->ev_fork, 0));
+            }
+            ctx->stream = side;
+            rc = fch ? launch("soil_pass", k_soil_pass<T, SKF, false, true>, blocks(S.n, tpb), tpb, S, W, grid, sc_same,
+                              sc_cross, sim, cnt, 1, us)
+                     : launch("soil_pass", k_soil_pass<T, SKF, false, false>, blocks(S.n, tpb), tpb, S, W, grid, sc_same,
+                              sc_cross, sim, cnt, 1, us);
+            cudaError_t ej = side != main_stream ? cudaEventRecord(ctx->ev_join, side) : cudaSuccess;
+            ctx->stream = main_stream;
+            if (rc == 0)
+                rc = fch ? launch("water_pass_b", k_water_pass_b<T, SKF, false, true>, blocks(W.n, tpb), tpb, W, S, grid,
+                                  sc_same, sc_cross, sim, uw, cnt)
+                         : launch("water_pass_b", k_water_pass_b<T, SKF, false, false>, blocks(W.n, tpb), tpb, W, S, grid,
+                                  sc_same, sc_cross, sim, uw, cnt);
+            // join in every case, so that a capture in progress ends joined
+            cudaError_t ew = ej != cudaSuccess ? ej
+                             : side != main_stream ? cudaStreamWaitEvent(main_stream, ctx->ev_join, 0) : cudaSuccess;
+            if (rc) return rc;
+            if (ew != cudaSuccess) {
+                fprintf(stderr, "libsphg: joining the soil pass failed: %s\n", cudaGetErrorString(ew));
+                return SPHG_ERR_CUDA;
             }
             aliased = true;
         }
@@ -1014,6 +1040,16 @@ int sphg_create(const sphg_params* p, int n_phase, sphg_ctx** out) {
     cudaGetDevice(&c->device);
     if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) { delete c; return SPHG_ERR_CUDA; }
     c->stream = c->own_stream;
+    if (cudaStreamCreateWithFlags(&c->side_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        if (c->side_stream) cudaStreamDestroy(c->side_stream);
+        if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+        cudaStreamDestroy(c->own_stream);
+        delete c;
+        return SPHG_ERR_CUDA;
+    }
     if (p->precision == SPHG_FP64) c->eng = new Engine<double>(c);
     else c->eng = new Engine<float>(c);
     *out = c;
@@ -1376,6 +1412,9 @@ void sphg_destroy(sphg_ctx* c) {
     delete c->eng;
     if (c->ev_a) cudaEventDestroy(c->ev_a);
     if (c->ev_b) cudaEventDestroy(c->ev_b);
+    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    if (c->ev_join) cudaEventDestroy(c->ev_join);
+    if (c->side_stream) { cudaStreamSynchronize(c->side_stream); cudaStreamDestroy(c->side_stream); }
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
 }

@@ -92,6 +92,8 @@ struct sphg_ctx {
     // the soil pass runs beside water_pass_b on this stream, forked and joined by events
     cudaStream_t side_stream = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    // the soil's cell list and gather run on the side stream beside the water's
+    cudaEvent_t ev_fork2 = nullptr, ev_join2 = nullptr;
 };
 
 #define CUDA_TRY(x)                                        \
@@ -117,6 +119,7 @@ struct Engine : EngineBase {
     int* counts[2] = {nullptr, nullptr};
     int* cell_start_buf[2] = {nullptr, nullptr};
     void* cub_tmp = nullptr;
+    void* cub_tmp1 = nullptr;        // the second phase's scan, which may run beside the first's
     size_t cub_bytes = 0;
     DevCounters* cnt = nullptr;     // device
     DevCounters hcnt{};             // host copy
@@ -496,6 +499,7 @@ struct Engine : EngineBase {
                 release(cell_start_buf[ph]); cell_start_buf[ph] = nullptr;
             }
             release(cub_tmp); cub_tmp = nullptr;
+            release(cub_tmp1); cub_tmp1 = nullptr;
             ncell = nc;
         }
         for (int ph = 0; ph < ctx->nphase; ++ph) {
@@ -511,6 +515,7 @@ struct Engine : EngineBase {
             cub_bytes = std::max(bytes, b2);
             if (alloc((char**)&cub_tmp, cub_bytes)) return SPHG_ERR_CUDA;
         }
+        if (ctx->nphase == 2 && !cub_tmp1 && alloc((char**)&cub_tmp1, cub_bytes)) return SPHG_ERR_CUDA;
         bool uniform = hmin == hmax;
         double K = sk * hmax;
         sc_same.scale_k = sk; sc_same.uniform = uniform; sc_same.r2_uniform = uniform ? exact_threshold(K) : 0.0;
@@ -533,7 +538,8 @@ struct Engine : EngineBase {
                         D.cell_fill, counts[ph], cnt);
         if (rc) return rc;
         size_t bytes = cub_bytes;
-        CUDA_TRY(cub::DeviceScan::ExclusiveSum(cub_tmp, bytes, counts[ph], D.cell_start, ncell + 1, ctx->stream));
+        CUDA_TRY(cub::DeviceScan::ExclusiveSum(ph == 1 && cub_tmp1 ? cub_tmp1 : cub_tmp, bytes, counts[ph], D.cell_start,
+                                               ncell + 1, ctx->stream));
         if ((rc = launch("cell_scatter", k_cell_scatter, blocks(D.n, 256), 256, D.n, (const int*)D.cell_id,
                          (const int*)D.cell_fill, (const int*)D.cell_start, D.perm)))
             return rc;
@@ -608,8 +614,8 @@ struct Engine : EngineBase {
             PhaseDev<T>& S = P[1];
             StepCtl uw = u; uw.with_vof = 1; uw.do_dp = 0;
             StepCtl us = u; us.with_vof = 1; us.do_dp = dp;
+            // the soil's gather was launched by run() on the side stream
             if ((rc = launch("gather", k_gather<T>, blocks(W.n, 256), 256, W, sim, 0, 0, fh, 1, 0, cnt))) return rc;
-            if ((rc = launch("gather", k_gather<T>, blocks(S.n, 256), 256, S, sim, 1, dp, fh, 1, dp, cnt))) return rc;
             if ((rc = launch("water_pass_a", k_water_pass_a<T, SKF, false>, blocks(W.n, tpb), tpb, W, grid, sc_same, sim, cnt))) return rc;
             // The cross pairs run inside the last pass of each phase; the soil
             // pass reads the water pressure that water_pass_a sets.  After
@@ -634,6 +640,11 @@ struct Engine : EngineBase {
                               sc_cross, sim, cnt, 1, us);
             cudaError_t ej = side != main_stream ? cudaEventRecord(ctx->ev_join, side) : cudaSuccess;
             ctx->stream = main_stream;
+            // water_pass_b reads the soil's records: wait for the soil's gather
+            if (side != main_stream) {
+                cudaError_t e2 = cudaStreamWaitEvent(main_stream, ctx->ev_join2, 0);
+                if (e2 != cudaSuccess && rc == 0) rc = SPHG_ERR_CUDA;
+            }
             if (rc == 0)
                 rc = fch ? launch("water_pass_b", k_water_pass_b<T, SKF, false, true>, blocks(W.n, tpb), tpb, W, S, grid,
                                   sc_same, sc_cross, sim, uw, cnt)
@@ -734,9 +745,35 @@ struct Engine : EngineBase {
         if ((rc = reset_counters())) return rc;
         const sphg_params& p = ctx->prm;
         bool reorder_now = p.reorder_interval > 0 && itimestep > 0 && itimestep % p.reorder_interval == 0;
-        for (int ph = 0; ph < ctx->nphase; ++ph) {
-            if ((rc = build_cells(ph))) return rc;
-            if (reorder_now && (rc = reorder(ph))) return rc;
+        if (ctx->nphase == 2 && !p.single_phase) {
+            // The soil's cell list, reorder and gather touch soil data only,
+            // so they run on the side stream beside the water's (serially
+            // while kernels are timed one by one); water_pass_b waits for
+            // them (passes).
+            cudaStream_t main_stream = ctx->stream;
+            cudaStream_t side = ctx->prof.on ? main_stream : ctx->side_stream;
+            if (side != main_stream) {
+                CUDA_TRY(cudaEventRecord(ctx->ev_fork2, main_stream));
+                CUDA_TRY(cudaStreamWaitEvent(side, ctx->ev_fork2, 0));
+            }
+            ctx->stream = side;
+            rc = build_cells(1);
+            if (!rc && reorder_now) rc = reorder(1);
+            if (!rc) rc = launch("gather", k_gather<T>, blocks(P[1].n, 256), 256, P[1], sim, 1, sim.yield_dp, fh, 1,
+                                 sim.yield_dp, cnt);
+            cudaError_t ej = side != main_stream ? cudaEventRecord(ctx->ev_join2, side) : cudaSuccess;
+            ctx->stream = main_stream;
+            if (rc || ej != cudaSuccess) {
+                if (side != main_stream && ej == cudaSuccess) cudaStreamWaitEvent(main_stream, ctx->ev_join2, 0);
+                return rc ? rc : SPHG_ERR_CUDA;
+            }
+            if ((rc = build_cells(0))) return rc;
+            if (reorder_now && (rc = reorder(0))) return rc;
+        } else {
+            for (int ph = 0; ph < ctx->nphase; ++ph) {
+                if ((rc = build_cells(ph))) return rc;
+                if (reorder_now && (rc = reorder(ph))) return rc;
+            }
         }
         switch (p.skf) {
             case 1: rc = passes<1>(fh, u); break;
@@ -1042,10 +1079,14 @@ int sphg_create(const sphg_params* p, int n_phase, sphg_ctx** out) {
     c->stream = c->own_stream;
     if (cudaStreamCreateWithFlags(&c->side_stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+        cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_fork2, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_join2, cudaEventDisableTiming) != cudaSuccess) {
         cudaGetLastError();
         if (c->side_stream) cudaStreamDestroy(c->side_stream);
         if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+        if (c->ev_join) cudaEventDestroy(c->ev_join);
+        if (c->ev_fork2) cudaEventDestroy(c->ev_fork2);
         cudaStreamDestroy(c->own_stream);
         delete c;
         return SPHG_ERR_CUDA;
@@ -1414,6 +1455,8 @@ void sphg_destroy(sphg_ctx* c) {
     if (c->ev_b) cudaEventDestroy(c->ev_b);
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);
     if (c->ev_join) cudaEventDestroy(c->ev_join);
+    if (c->ev_fork2) cudaEventDestroy(c->ev_fork2);
+    if (c->ev_join2) cudaEventDestroy(c->ev_join2);
     if (c->side_stream) { cudaStreamSynchronize(c->side_stream); cudaStreamDestroy(c->side_stream); }
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;

@@ -252,8 +252,8 @@ def learned_arm(solver, scene, torch, plain_value, strides):
     history of 5 strides (k = 10 steps) from the plain solver, then `strides`
     learned strides timed end to end (graph search, network, stride update and
     the fallback-gate sums, wall clock with a synchronisation per stride), and
-    the plain solver's own strides from the same state as the judge of the
-    position error."""
+    the plain solver's own strides from the same state as the yardstick of
+    the position error."""
     import numpy as np
     from sources_b200 import learn
     if not os.path.exists(learn.DEFAULT_WEIGHTS):

@@ -1,7 +1,7 @@
 """Learned particle stepper: a message-passing network over the particles
 that predicts each particle's mean acceleration over a stride of k solver
 steps, trained on rollouts of the batched SPH solver, with the plain SPH
-step as its fallback and as the judge of its error.  The reference has no
+step as its fallback and as the yardstick of its error.  The reference has no
 counterpart: its step is the SPH solver alone.
 
 Everything numeric runs in libsphg's own CUDA kernels (include/sphg_learn.h):

@@ -139,6 +139,26 @@ module sphg_iface
        integer(c_int), value :: phase
        type(c_ptr), value :: x_dev, v_dev
      end function
+     ! several contexts stepped together, one CUDA graph per step (destroy the
+     ! group before its contexts); itimesteps and times hold one entry per context
+     integer(c_int) function sphg_group_create(ctxs, n, group) bind(C, name="sphg_group_create")
+       import :: c_int, c_ptr
+       type(c_ptr), intent(in) :: ctxs(*)
+       integer(c_int), value :: n
+       type(c_ptr), intent(out) :: group
+     end function
+     integer(c_int) function sphg_group_time_integration(group, maxtimestep, itimesteps, times) &
+          bind(C, name="sphg_group_time_integration")
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: group
+       integer(c_int), value :: maxtimestep
+       integer(c_int), intent(inout) :: itimesteps(*)
+       real(c_double), intent(inout) :: times(*)
+     end function
+     subroutine sphg_group_destroy(group) bind(C, name="sphg_group_destroy")
+       import :: c_ptr
+       type(c_ptr), value :: group
+     end subroutine
      subroutine sphg_destroy(ctx) bind(C, name="sphg_destroy")
        import :: c_ptr
        type(c_ptr), value :: ctx

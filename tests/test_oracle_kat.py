@@ -212,3 +212,49 @@ def test_forchheimer_drag_is_linear_in_b_opposes_slip_and_conserves_momentum():
     ms = (dv[0.0][1].mass[:, None] * (dv[4e4][1].dvx - dv[0.0][1].dvx)).sum(axis=0)
     assert np.all(np.abs(mw + ms) <= 1e-9 * np.abs(mw).max())
     assert mw[0] < 0 < ms[0]                             # water slowed, soil dragged along
+
+
+def test_vof_renormalisation_is_overwritten_by_the_corrector():
+    """The every-renorm_interval-steps renormalisation (declarations_sph.f90:
+    1414-1421) rewrites water rho and vof inside single_step, but second_half
+    then rebuilds both from rho_min / vof_min and the rates, so a run with it
+    and one without end in the same state, bit for bit; single_step on its own
+    does show the renormalised fields."""
+    s = scenes.small("two_phase", precision=SPHG_FP64)
+    s.params.renorm_interval = 4
+    on, off = s.copy(), s.copy()
+    on.params.volume_fraction_renorm = 1
+    off.params.volume_fraction_renorm = 0
+    a, b = Oracle(on), Oracle(off)
+    assert a.time_integration(9) == 0 and b.time_integration(9) == 0   # passes steps 4 and 8
+    for k in (1, 2):
+        pa, pb = a.download(k), b.download(k)
+        for f in ("x", "vx", "rho", "vof", "p"):
+            assert np.array_equal(getattr(pa, f), getattr(pb, f)), (k, f)
+    # the right-hand side alone at a renormalisation step changes water rho and vof
+    c, d = Oracle(on), Oracle(off)
+    assert c.single_step(4) == 0 and d.single_step(4) == 0
+    wc, wd = c.download(1), d.download(1)
+    assert not np.array_equal(wc.vof, wd.vof) and not np.array_equal(wc.rho, wd.rho)
+
+
+def test_darcy_drag_uses_the_soil_volume_fraction_of_the_step_before():
+    """darcy_law and pore_water_pressure (m_particles.f90:3832,3877) run before
+    volume_fraction_soil (:3970) sets the soil fraction from rho, so the drag of
+    a step uses the fraction the step started with.  Two scenes that differ only
+    in that starting fraction give different water accelerations, and leave the
+    same soil fraction behind."""
+    base = scenes.jitter(scenes.small("two_phase", precision=SPHG_FP64), 0.0002, seed=17)
+    W, S = base.phases
+    W.vx[:W.ntotal] = np.random.default_rng(2).normal(0, 0.02, size=(W.ntotal, 2))
+    out = []
+    for f in (1.0, 0.8):
+        s = base.copy()
+        s.phases[1].vof[:] = s.phases[1].vof * f
+        o = Oracle(s)
+        assert o.single_step(1) == 0
+        out.append((o.download(1), o.download(2)))
+    (w0, s0), (w1, s1) = out
+    assert not np.array_equal(w0.dvx, w1.dvx)
+    assert np.array_equal(s0.vof, s1.vof)
+    assert np.allclose(s0.vof, s0.rho / base.params.soil.rho0, rtol=1e-15, atol=0)

@@ -258,3 +258,30 @@ def test_darcy_drag_uses_the_soil_volume_fraction_of_the_step_before():
     assert not np.array_equal(w0.dvx, w1.dvx)
     assert np.array_equal(s0.vof, s1.vof)
     assert np.allclose(s0.vof, s0.rho / base.params.soil.rho0, rtol=1e-15, atol=0)
+
+
+def test_wall_force_pushes_real_particles_away_from_the_wall():
+    """repulsive_force (m_particles.f90:1605-1642), part of the two-phase step,
+    acts on a real particle within dspp of a virtual one along x_real -
+    x_virtual: it pushes the particle away from the wall.  The difference of
+    the accelerations with and without the force (dd = 0) points from the
+    virtual particle to the real one."""
+    base = scenes.small("two_phase", precision=SPHG_FP64)
+    P = base.phases[0]
+    virt = np.arange(P.ntotal, P.n)
+    floor = virt[P.x[virt, 1] < P.x[:P.ntotal, 1].min()]
+    top = floor[np.isclose(P.x[floor, 1], P.x[floor, 1].max())]
+    v = int(top[np.argmin(np.abs(P.x[top, 0] - 0.15))])              # floor, right of the soil block
+    i = int(np.argmin(np.sum((P.x[:P.ntotal] - P.x[v]) ** 2, axis=1)))   # the nearest real particle
+    dirv = np.array([0.3, 1.0]) / np.hypot(0.3, 1.0)
+    acc = []
+    for dd in (0.0, base.params.dd):
+        s = base.copy()
+        s.phases[0].x[i] = s.phases[0].x[v] + 0.5 * P.dspp * dirv
+        s.params.dd = dd
+        o = Oracle(s)
+        assert o.single_step(1) == 0
+        acc.append(o.download(1).dvx[i].copy())
+    push = acc[1] - acc[0]
+    assert np.linalg.norm(push) > 0
+    assert np.dot(push, dirv) / np.linalg.norm(push) > 0.999

@@ -1152,6 +1152,7 @@ int sphg_time_integration(sphg_ctx* c, int maxtimestep, int* itimestep, double* 
 // context has dropped its own graphs (upload, tuning).
 struct sphg_group {
     std::vector<sphg_ctx*> ctx;
+    int device = 0;     // kept so that destroying the group touches no context
     struct Joint {
         cudaGraphExec_t exec = nullptr;
         std::vector<long long> launches, epochs;
@@ -1270,6 +1271,7 @@ int sphg_group_create(sphg_ctx* const* ctxs, int n, sphg_group** out) {
     cudaSetDevice(ctxs[0]->device);
     sphg_group* g = new sphg_group();
     g->ctx.assign(ctxs, ctxs + n);
+    g->device = ctxs[0]->device;
     g->ev.assign(n, nullptr);
     for (int i = 0; i < n; ++i) {
         if (cudaEventCreateWithFlags(&g->ev[i], cudaEventDisableTiming) != cudaSuccess) {
@@ -1340,7 +1342,7 @@ int sphg_group_time_integration(sphg_group* g, int maxtimestep, int* itimesteps,
 
 void sphg_group_destroy(sphg_group* g) {
     if (!g) return;
-    cudaSetDevice(g->ctx[0]->device);
+    cudaSetDevice(g->device);
     delete g;
 }
 

@@ -186,7 +186,9 @@ int sphg_time_integration(sphg_ctx* ctx, int maxtimestep, int* itimestep, double
  * the contexts' kernels overlap on the GPU.  The results are those of calling
  * sphg_time_integration on each context in turn.  itimesteps and times hold
  * one entry per context, as sphg_time_integration's arguments, and all
- * itimesteps must be equal.  Destroy a group before its contexts. */
+ * itimesteps must be equal.  A group must not be stepped once one of its
+ * contexts is destroyed; sphg_group_destroy touches no context, so it may come
+ * before or after them. */
 typedef struct sphg_group sphg_group;
 int sphg_group_create(sphg_ctx* const* ctxs, int n, sphg_group** out);
 int sphg_group_time_integration(sphg_group* group, int maxtimestep, int* itimesteps, double* times);

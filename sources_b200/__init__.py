@@ -262,7 +262,7 @@ class SolverGroup:
     """Several Solvers stepped together (sphg_group_*): after the first step,
     one CUDA graph per step holds every context's step as a parallel branch.
     Results equal stepping each Solver in turn.  All members must be at the
-    same itimestep; close the group before its Solvers."""
+    same itimestep; the group must not be stepped once a member is closed."""
 
     def __init__(self, solvers):
         self.L = load()

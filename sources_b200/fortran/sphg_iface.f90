@@ -139,8 +139,8 @@ module sphg_iface
        integer(c_int), value :: phase
        type(c_ptr), value :: x_dev, v_dev
      end function
-     ! several contexts stepped together, one CUDA graph per step (destroy the
-     ! group before its contexts); itimesteps and times hold one entry per context
+     ! several contexts stepped together, one CUDA graph per step (not to be
+     ! stepped once a context is destroyed); itimesteps and times hold one entry per context
      integer(c_int) function sphg_group_create(ctxs, n, group) bind(C, name="sphg_group_create")
        import :: c_int, c_ptr
        type(c_ptr), intent(in) :: ctxs(*)

@@ -1,5 +1,6 @@
-"""A second, independent restatement of the water-only right-hand side,
-written in numpy straight from the reference's Fortran, against the C oracle.
+"""A second, independent restatement of the water-only and soil-only
+right-hand sides, written in numpy straight from the reference's Fortran,
+against the C oracle.
 
 single_step_for_water (declarations_sph.f90:1439-1526) calls direct_find
 (m_particles.f90:938), kernel (:1469, cubic spline), sum_density (:2243), df2
@@ -149,5 +150,150 @@ def test_numpy_restatement_matches_the_c_oracle(seed):
     d = o.download(1)
     assert len(o.pairs(0)[0]) == ref["npairs"]
     for f in ("rho", "drho", "p", "dvx", "av", "txx", "tyy", "txy"):
+        a, b = np.asarray(getattr(d, f)), ref[f]
+        assert np.array_equal(a, b), (f, int((a != b).sum()), float(np.abs(a - b).max()))
+
+
+def soil_rhs(scene):
+    """single_step_for_soil (declarations_sph.f90:1530-1655) with continuity
+    density: con_density (m_particles.f90:2402), delta_sph (:2658),
+    shear_strain_rate (:2855), velocity_divergence (:1996), pressure (:2133,
+    c = soil c), drucker_prager_failure_criterion (:3323), df (:1711),
+    plastic_or_not (:3447), plastic_flow_rule3 (:3700), Jaumann_rate (:3047),
+    art_visc (:2504), delta_sph on p and the stresses, gravity, av_vel (:2761).
+    The soil's spin array wxy is its txy working array (allocate_sph)."""
+    prm = scene.params
+    P = scene.phases[0]
+    sm = prm.soil
+    n = P.n
+    x, vx, m, h = P.x, P.vx, P.mass, P.hsml
+    rho, c = P.rho.copy(), P.c.copy()
+    p, sxx, sxy, syy = P.p.copy(), P.sxx.copy(), P.sxy.copy(), P.syy.copy()
+    eps_p = P.epsilon_p.copy()
+    i, j = np.triu_indices(n, 1)
+    dx = x[i, 0] - x[j, 0]
+    dy = x[i, 1] - x[j, 1]
+    r2 = dx * dx + dy * dy
+    mh = (h[i] + h[j]) / 2.0
+    keep = np.sqrt(r2) < 2 * mh
+    i, j, dx, dy, r2, mh = i[keep], j[keep], dx[keep], dy[keep], r2[keep], mh[keep]
+    w, gx, gy = _cubic(np.sqrt(r2), dx, dy, mh)
+    u, v = vx[:, 0], vx[:, 1]
+    # con_density
+    vcc_k = (u[i] - u[j]) * gx + (v[i] - v[j]) * gy
+    drho = _scatter(n, i, j, m[j] * vcc_k, m[i] * vcc_k)
+
+    def delta(f, df):
+        rr = 0.0 + dx * dx + dy * dy
+        muv = 2.0 * (f[i] - f[j]) / rr
+        hh = 0.0 + dx * muv * gx + dy * muv * gy
+        d = prm.delta
+        return _scatter(n, i, j, d * h[i] * c[i] * m[j] * hh / rho[j], -(d * h[j] * c[j] * m[i] * hh / rho[i]), init=df)
+    if prm.artificial_density:
+        drho = delta(rho, drho)
+    # shear_strain_rate, dv = v_j - v_i
+    du, dv = u[j] - u[i], v[j] - v[i]
+    c23 = F32(2.0 / 3.0)
+    hxx = c23 * (2.0 * du * gx - dv * gy)
+    hxy = du * gy + dv * gx
+    hyy = c23 * (2.0 * dv * gy - du * gx)
+    txx = _scatter(n, i, j, m[j] * hxx / rho[j], m[i] * hxx / rho[i])
+    txy = _scatter(n, i, j, m[j] * hxy / rho[j], m[i] * hxy / rho[i])
+    tyy = _scatter(n, i, j, m[j] * hyy / rho[j], m[i] * hyy / rho[i])
+    # velocity_divergence
+    hv = du * gx + dv * gy
+    vcc = _scatter(n, i, j, m[j] * hv / rho[j], m[i] * hv / rho[i])
+    # pressure: c = soil c
+    c = np.full(n, sm.c)
+    # drucker_prager_failure_criterion
+    t = math.tan(sm.phi)
+    alpha1 = t / math.sqrt(9.0 + 12.0 * (t * t))
+    p = np.where(p < 0.0, 0.0, p)
+    I1 = 3.0 * p
+    J2 = np.sqrt((sxx * sxx + 2.0 * (sxy * sxy) + syy * syy + (sxx + syy) * (sxx + syy)) / 2.0) + 1.0e-6
+    fail = J2 > alpha1 * I1
+    skale = alpha1 * I1[fail] / J2[fail]
+    sxx[fail], sxy[fail], syy[fail] = skale * sxx[fail], skale * sxy[fail], skale * syy[fail]
+
+    def df(f, g):
+        fw = (f[i] + f[j]) * g
+        return _scatter(n, i, j, m[j] / rho[j] * fw, -(m[i] / rho[i] * fw))
+    ax = -df(p, gx) + df(sxx, gx) + df(sxy, gy)
+    ay = -df(p, gy) + df(sxy, gx) + df(syy, gy)
+    pos = rho > 0.0
+    ax[pos] = ax[pos] / rho[pos]
+    ay[pos] = ay[pos] / rho[pos]
+    dsxx, dsxy, dsyy, dp = np.zeros(n), np.zeros(n), np.zeros(n), np.zeros(n)
+    K, G = sm.k, sm.E / (2.0 * (1 + sm.niu))
+    # plastic_or_not, then plastic_flow_rule3 on the failed points
+    J2a = np.sqrt((sxx * sxx + 2.0 * (sxy * sxy) + syy * syy + (sxx + syy) * (sxx + syy)) / 2.0) + 1.0e-6
+    fail = np.abs(J2a - alpha1 * I1) < F32(1.0e-5)
+    for a in np.nonzero(fail)[0]:
+        exx = txx[a] / 2.0 + vcc[a] / 3.0
+        exy = txy[a] / 2.0
+        eyy = tyy[a] / 2.0 + vcc[a] / 3.0
+        sde = sxx[a] * exx + 2.0 * sxy[a] * exy + syy[a] * eyy
+        J2f = (sxx[a] * sxx[a] + 2.0 * (sxy[a] * sxy[a]) + syy[a] * syy[a] + (sxx[a] + syy[a]) * (sxx[a] + syy[a])) / 2.0
+        J2f = J2f + 1.0e-10
+        dl = (3.0 * alpha1 * K * vcc[a] + G / math.sqrt(J2f) * sde) / (9.0 * (alpha1 * alpha1) * K + G)
+        if dl < 0:
+            continue
+        dsxx[a] = dsxx[a] - dl * (G / math.sqrt(J2f) * sxx[a])
+        dsxy[a] = dsxy[a] - dl * (G / math.sqrt(J2f) * sxy[a])
+        dsyy[a] = dsyy[a] - dl * (G / math.sqrt(J2f) * syy[a])
+        dp[a] = dp[a] + 3.0 * K * alpha1 * dl
+        eps_p[a] = eps_p[a] + dl * sxy[a] / (2 * math.sqrt(J2f)) * F32(0.000005)
+    # Jaumann_rate: Hooke, pressure rate, spin (into the txy array)
+    dsxx, dsxy, dsyy = dsxx + G * txx, dsxy + G * txy, dsyy + G * tyy
+    dp = dp - K * vcc
+    hw = 0.5 * (du * gy - dv * gx)
+    wxy = _scatter(n, i, j, m[j] * hw / rho[j], m[i] * hw / rho[i])
+    dsxx = dsxx + 2.0 * sxy * wxy
+    dsxy = dsxy - (sxx - syy) * wxy
+    dsyy = dsyy - 2.0 * sxy * wxy
+    # art_visc
+    if prm.visc_artificial:
+        ddx, ddy = u[i] - u[j], v[i] - v[j]
+        vr = 0.0 + ddx * dx + ddy * dy
+        rr = 0.0 + dx * dx + dy * dy
+        a = vr < 0.0
+        etq = prm.etq
+        muv = mh[a] * vr[a] / (rr[a] + mh[a] * mh[a] * etq * etq)
+        mc = 0.5 * (c[i[a]] + c[j[a]])
+        mrho = 0.5 * (rho[i[a]] + rho[j[a]])
+        piv = (prm.beta * muv - prm.alpha * mc) * muv / mrho
+        ia, ja = i[a], j[a]
+        hx, hy = -piv * gx[a], -piv * gy[a]
+        ax = _scatter(n, ia, ja, m[ja] * hx, -(m[ia] * hx), init=ax)
+        ay = _scatter(n, ia, ja, m[ja] * hy, -(m[ia] * hy), init=ay)
+    if prm.soil_artificial_stress:
+        dp, dsxx, dsxy, dsyy = delta(p, dp), delta(sxx, dsxx), delta(sxy, dsxy), delta(syy, dsyy)
+    ay = ay + prm.gravity
+    av = np.zeros((n, 2))
+    if prm.average_velocity:
+        mrho = (rho[i] + rho[j]) / 2.0
+        for d, comp in enumerate((u, v)):
+            dvd = comp[i] - comp[j]
+            av[:, d] = _scatter(n, i, j, -(m[j] * dvd / mrho * w), m[i] * dvd / mrho * w)
+        av[:P.ntotal] = prm.epsilon * av[:P.ntotal]
+    return dict(drho=drho, p=p, sxx=sxx, sxy=sxy, syy=syy, dvx=np.stack([ax, ay], axis=1), av=av,
+                dsxx=dsxx, dsxy=dsxy, dsyy=dsyy, dp=dp, epsilon_p=eps_p, fail=fail.astype(np.int32),
+                txx=txx, tyy=tyy, txy=wxy, vcc=vcc, c=c, npairs=len(i))
+
+
+@pytest.mark.parametrize("seed", [5, 6])
+def test_numpy_soil_restatement_matches_the_c_oracle(seed):
+    s = scenes.jitter(scenes.small("granular_column", precision=SPHG_FP64), 0.0002, seed=seed)
+    P = s.phases[0]
+    P.vx[:P.ntotal] = np.random.default_rng(seed).normal(0, 0.05, size=(P.ntotal, 2))
+    ref = soil_rhs(s)
+    o = Oracle(s)
+    assert o.single_step(1) == 0
+    d = o.download(1)
+    assert len(o.pairs(0)[0]) == ref["npairs"]
+    assert ref["fail"].sum() > 0                         # the flow rule is exercised
+    assert np.array_equal(np.asarray(d.fail) != 0, ref["fail"] != 0)
+    for f in ("drho", "p", "sxx", "sxy", "syy", "dvx", "av", "dsxx", "dsxy", "dsyy", "dp", "epsilon_p",
+              "txx", "tyy", "txy", "vcc", "c"):
         a, b = np.asarray(getattr(d, f)), ref[f]
         assert np.array_equal(a, b), (f, int((a != b).sum()), float(np.abs(a - b).max()))

@@ -1,8 +1,8 @@
-"""A second, independent restatement of the water-only and soil-only
-right-hand sides, written in numpy straight from the reference's Fortran,
-against the C oracle.
+"""A second, independent restatement of the three right-hand sides (water
+only, soil only, two-phase), written in numpy straight from the reference's
+Fortran, against the C oracle.
 
-single_step_for_water (declarations_sph.f90:1439-1526) calls direct_find
+The water-only single_step_for_water (declarations_sph.f90:1439-1526) calls direct_find
 (m_particles.f90:938), kernel (:1469, cubic spline), sum_density (:2243), df2
 (:1802), delta_sph (:2658), the Tait pressure, df (:1711), art_visc (:2504)
 and av_vel (:2761).  Every pair loop here scatters to both ends in pair order
@@ -297,3 +297,222 @@ def test_numpy_soil_restatement_matches_the_c_oracle(seed):
               "txx", "tyy", "txy", "vcc", "c"):
         a, b = np.asarray(getattr(d, f)), ref[f]
         assert np.array_equal(a, b), (f, int((a != b).sum()), float(np.abs(a - b).max()))
+
+
+def _pairs(xa, ha, xb=None, hb=None):
+    """direct_find (same phase, i < j) or direct_find_2 (i of a, j of b), in
+    the reference's loop order, with the kernel of each pair."""
+    if xb is None:
+        i, j = np.triu_indices(len(xa), 1)
+        xb, hb = xa, ha
+    else:
+        i, j = np.divmod(np.arange(len(xa) * len(xb)), len(xb))
+    dx = xa[i, 0] - xb[j, 0]
+    dy = xa[i, 1] - xb[j, 1]
+    r2 = dx * dx + dy * dy
+    mh = (ha[i] + hb[j]) / 2.0
+    keep = np.sqrt(r2) < 2 * mh
+    i, j, dx, dy, r2, mh = i[keep], j[keep], dx[keep], dy[keep], r2[keep], mh[keep]
+    w, gx, gy = _cubic(np.sqrt(r2), dx, dy, mh)
+    return i, j, dx, dy, mh, w, gx, gy
+
+
+def two_phase_rhs(scene, itimestep=1):
+    """single_step (declarations_sph.f90:1131-1435), water then soil, then the
+    water x soil pairs: darcy_law, pore_water_pressure and the volume
+    fractions (m_particles.f90:3832-3988).  The shared working arrays (txx,
+    tyy, txy and the water stress that aliases them) are not returned."""
+    prm = scene.params
+    Wp, Sp = scene.phases
+    out = {}
+    state = {}
+    for ph, P in ((1, Wp), (2, Sp)):
+        water = ph == 1
+        mat = prm.water if water else prm.soil
+        n = P.n
+        x, vx, m, h = P.x, P.vx, P.mass, P.hsml
+        rho, c, vof = P.rho.copy(), P.c.copy(), P.vof.copy()
+        p = P.p.copy()
+        i, j, dx, dy, mh, w, gx, gy = _pairs(x, h)
+        u, v = vx[:, 0], vx[:, 1]
+        sc = lambda vi, vj, init=None: _scatter(n, i, j, vi, vj, init)
+
+        def delta(f, df):
+            rr = 0.0 + dx * dx + dy * dy
+            muv = 2.0 * (f[i] - f[j]) / rr
+            hh = 0.0 + dx * muv * gx + dy * muv * gy
+            d = prm.delta
+            return sc(d * h[i] * c[i] * m[j] * hh / rho[j], -(d * h[j] * c[j] * m[i] * hh / rho[i]), init=df)
+        vk = (u[i] - u[j]) * gx + (v[i] - v[j]) * gy
+        drho = sc(m[j] * vk, m[i] * vk)
+        if prm.artificial_density:
+            drho = delta(rho, drho)
+        du, dv = u[j] - u[i], v[j] - v[i]
+        c23 = F32(2.0 / 3.0)
+        hxx = c23 * (2.0 * du * gx - dv * gy)
+        hxy = du * gy + dv * gx
+        hyy = c23 * (2.0 * dv * gy - du * gx)
+        txx = sc(m[j] * hxx / rho[j], m[i] * hxx / rho[i])
+        txy = sc(m[j] * hxy / rho[j], m[i] * hxy / rho[i])
+        tyy = sc(m[j] * hyy / rho[j], m[i] * hyy / rho[i])
+        pos = rho > 0.0
+        if water:
+            ratio = rho / (mat.rho0 * vof)
+            p = mat.b * (np.array([math.pow(r, mat.gamma) for r in ratio]) - 1)
+            c = mat.c * np.array([math.pow(r, 3.0) for r in ratio])
+            sxx, syy, sxy = mat.viscosity * txx, mat.viscosity * tyy, mat.viscosity * txy
+
+            def df(f, g):
+                fw = (f[i] + f[j]) * g
+                return sc(m[j] / rho[j] * fw, -(m[i] / rho[i] * fw))
+            ax = -(vof * df(p, gx)) + df(vof * sxx, gx) + df(vof * sxy, gy)
+            ay = -(vof * df(p, gy)) + df(vof * sxy, gx) + df(vof * syy, gy)
+        else:
+            hv = du * gx + dv * gy
+            vcc = sc(m[j] * hv / rho[j], m[i] * hv / rho[i])
+            c = np.full(n, mat.c)
+            sxx, sxy, syy = P.sxx.copy(), P.sxy.copy(), P.syy.copy()
+            t = math.tan(mat.phi)
+            alpha1 = t / math.sqrt(9.0 + 12.0 * (t * t))
+            p = np.where(p < 0.0, 0.0, p)
+            I1 = 3.0 * p
+            J2 = np.sqrt((sxx * sxx + 2.0 * (sxy * sxy) + syy * syy + (sxx + syy) * (sxx + syy)) / 2.0) + 1.0e-6
+            f1 = J2 > alpha1 * I1
+            sk = alpha1 * I1[f1] / J2[f1]
+            sxx[f1], sxy[f1], syy[f1] = sk * sxx[f1], sk * sxy[f1], sk * syy[f1]
+
+            def df3(f, g):
+                fw = (f[i] / (rho[i] * rho[i]) + f[j] / (rho[j] * rho[j])) * g
+                return sc(m[j] * fw, -(m[i] * fw)) * rho
+            ax = -df3(vof * p, gx) + df3(vof * sxx, gx) + df3(vof * sxy, gy)
+            ay = -df3(vof * p, gy) + df3(vof * sxy, gx) + df3(vof * syy, gy)
+        ax[pos] = ax[pos] / rho[pos]
+        ay[pos] = ay[pos] / rho[pos]
+        if not water:
+            K, G = mat.k, mat.E / (2.0 * (1 + mat.niu))
+            dsxx, dsxy, dsyy, dp = np.zeros(n), np.zeros(n), np.zeros(n), np.zeros(n)
+            eps_p = P.epsilon_p.copy()
+            J2a = np.sqrt((sxx * sxx + 2.0 * (sxy * sxy) + syy * syy + (sxx + syy) * (sxx + syy)) / 2.0) + 1.0e-6
+            fail = np.abs(J2a - alpha1 * I1) < F32(1.0e-5)
+            for a in np.nonzero(fail)[0]:
+                exx = txx[a] / 2.0 + vcc[a] / 3.0
+                exy = txy[a] / 2.0
+                eyy = tyy[a] / 2.0 + vcc[a] / 3.0
+                sde = sxx[a] * exx + 2.0 * sxy[a] * exy + syy[a] * eyy
+                J2f = (sxx[a] * sxx[a] + 2.0 * (sxy[a] * sxy[a]) + syy[a] * syy[a]
+                       + (sxx[a] + syy[a]) * (sxx[a] + syy[a])) / 2.0 + 1.0e-10
+                dl = (3.0 * alpha1 * K * vcc[a] + G / math.sqrt(J2f) * sde) / (9.0 * (alpha1 * alpha1) * K + G)
+                if dl < 0:
+                    continue
+                dsxx[a] = dsxx[a] - dl * (G / math.sqrt(J2f) * sxx[a])
+                dsxy[a] = dsxy[a] - dl * (G / math.sqrt(J2f) * sxy[a])
+                dsyy[a] = dsyy[a] - dl * (G / math.sqrt(J2f) * syy[a])
+                dp[a] = dp[a] + 3.0 * K * alpha1 * dl
+                eps_p[a] = eps_p[a] + dl * sxy[a] / (2 * math.sqrt(J2f)) * F32(0.000005)
+            dsxx, dsxy, dsyy = dsxx + G * txx, dsxy + G * txy, dsyy + G * tyy
+            dp = dp - K * vcc
+            hw = 0.5 * (du * gy - dv * gx)
+            wxy = sc(m[j] * hw / rho[j], m[i] * hw / rho[i])
+            dsxx = dsxx + 2.0 * sxy * wxy
+            dsxy = dsxy - (sxx - syy) * wxy
+            dsyy = dsyy - 2.0 * sxy * wxy
+        if prm.visc_artificial:
+            ddx, ddy = u[i] - u[j], v[i] - v[j]
+            vr = 0.0 + ddx * dx + ddy * dy
+            rr = 0.0 + dx * dx + dy * dy
+            a = vr < 0.0
+            etq = prm.etq
+            muv = mh[a] * vr[a] / (rr[a] + mh[a] * mh[a] * etq * etq)
+            mc = 0.5 * (c[i[a]] + c[j[a]])
+            mrho = 0.5 * (rho[i[a]] + rho[j[a]])
+            piv = (prm.beta * muv - prm.alpha * mc) * muv / mrho
+            ia, ja = i[a], j[a]
+            hx, hy = -piv * gx[a], -piv * gy[a]
+            ax = _scatter(n, ia, ja, m[ja] * hx, -(m[ia] * hx), init=ax)
+            ay = _scatter(n, ia, ja, m[ja] * hy, -(m[ia] * hy), init=ay)
+        dvof = np.zeros(n)
+        if not water and prm.soil_artificial_stress:
+            dp, dsxx, dsxy, dsyy = delta(p, dp), delta(sxx, dsxx), delta(sxy, dsxy), delta(syy, dsyy)
+        if water and prm.water_artificial_volume:
+            dvof = delta(vof, dvof)
+        # repulsive_force: real-virtual pairs within dspp, on the real particle
+        it = P.itype
+        rep = it[i] * it[j] <= 0
+        rr = np.sqrt(0.0 + dx * dx + dy * dy)
+        rep &= ~(rr > P.dspp)
+        for k in np.nonzero(rep)[0]:
+            f = (math.pow(P.dspp / rr[k], prm.p1) - math.pow(P.dspp / rr[k], prm.p2)) / (rr[k] * rr[k])
+            ii = j[k] if it[i[k]] < 0 else i[k]
+            ax[ii] = ax[ii] + prm.dd * dx[k] * f
+            ay[ii] = ay[ii] + prm.dd * dy[k] * f
+        ay = ay + prm.gravity
+        av = np.zeros((n, 2))
+        if prm.average_velocity:
+            mrho = (rho[i] + rho[j]) / 2.0
+            for d, comp in enumerate((u, v)):
+                dvd = comp[i] - comp[j]
+                av[:, d] = sc(-(m[j] * dvd / mrho * w), m[i] * dvd / mrho * w)
+            av[:P.ntotal] = prm.epsilon * av[:P.ntotal]
+        res = dict(drho=drho, p=p, c=c, dvx=np.stack([ax, ay], axis=1), av=av, rho=rho, vof=vof)
+        if water:
+            res["dvof"] = dvof
+        else:
+            res.update(sxx=sxx, sxy=sxy, syy=syy, dsxx=dsxx, dsxy=dsxy, dsyy=dsyy, dp=dp, epsilon_p=eps_p,
+                       vcc=vcc, fail=fail.astype(np.int32))
+        out[ph] = res
+    # water x soil pairs
+    W, S = out[1], out[2]
+    i, j, dx, dy, mh, w, gx, gy = _pairs(Wp.x, Wp.hsml, Sp.x, Sp.hsml)
+    mw, ms = Wp.mass, Sp.mass
+    rw, rs = W["rho"], S["rho"]
+    vw, vs = Wp.vx, Sp.vx
+    dvw, dvs = W["dvx"].copy(), S["dvx"].copy()
+    vofw, vofs = W["vof"], S["vof"]
+    ks = prm.soil.permeability
+    for k in range(len(i)):           # darcy_law
+        a, b = i[k], j[k]
+        rrw = w[k] / (rw[a] * rs[b])
+        cf = vofw[a] * vofs[b] * rw[a] * (-prm.numeric_gravity) / ks
+        for d in range(2):
+            sp = cf * (vw[a, d] - vs[b, d]) * rrw
+            dvw[a, d] = dvw[a, d] - ms[b] * sp
+            dvs[b, d] = dvs[b, d] + mw[a] * sp
+    pw = W["p"]
+    for k in range(len(i)):           # pore_water_pressure
+        a, b = i[k], j[k]
+        mprr = mw[a] * pw[a] / (rw[a] * rs[b])
+        dvs[b, 0] = dvs[b, 0] + mprr * gx[k] * vofs[b]
+        dvs[b, 1] = dvs[b, 1] + mprr * gy[k] * vofs[b]
+    W["dvx"], S["dvx"] = dvw, dvs
+    if prm.volume_fraction:
+        S["vof"] = rs / prm.soil.rho0                                      # volume_fraction_soil
+        tmp = (vw[i, 0] - vs[j, 0]) * gx + (vw[i, 1] - vs[j, 1]) * gy      # volume_fraction_water2
+        dvof = W["dvof"].copy()
+        np.add.at(dvof, i, -(ms[j] * tmp / prm.soil.rho0))
+        W["dvof"] = dvof
+        vof2 = np.zeros(Wp.n)                                              # volume_fraction_water
+        np.add.at(vof2, i, ms[j] * w)
+        W["vof2"] = 1.0 - vof2 / prm.soil.rho0
+        assert itimestep % 40 != 0    # the renormalisation is not restated here
+    W["npairs_cross"] = len(i)
+    return out
+
+
+@pytest.mark.parametrize("seed", [7, 8])
+def test_numpy_two_phase_restatement_matches_the_c_oracle(seed):
+    s = scenes.jitter(scenes.small("two_phase", precision=SPHG_FP64), 0.0002, seed=seed)
+    rng = np.random.default_rng(seed)
+    for P in s.phases:
+        P.vx[:P.ntotal] = rng.normal(0, 0.03, size=(P.ntotal, 2))
+    ref = two_phase_rhs(s)
+    o = Oracle(s)
+    assert o.single_step(1) == 0
+    assert len(o.pairs(2)[0]) == ref[1]["npairs_cross"]
+    fields = {1: ("drho", "p", "c", "dvx", "av", "rho", "vof", "dvof", "vof2"),
+              2: ("drho", "p", "c", "dvx", "av", "rho", "vof", "sxx", "sxy", "syy", "dsxx", "dsxy", "dsyy", "dp",
+                  "epsilon_p", "vcc")}
+    for ph in (1, 2):
+        d = o.download(ph)
+        for f in fields[ph]:
+            a, b = np.asarray(getattr(d, f)), ref[ph][f]
+            assert np.array_equal(a, b), (ph, f, int((a != b).sum()), float(np.abs(a - b).max()))

@@ -516,3 +516,87 @@ def test_numpy_two_phase_restatement_matches_the_c_oracle(seed):
         for f in fields[ph]:
             a, b = np.asarray(getattr(d, f)), ref[ph][f]
             assert np.array_equal(a, b), (ph, f, int((a != b).sum()), float(np.abs(a - b).max()))
+
+
+def _dp_return(p, sxx, sxy, syy, phi):
+    """drucker_prager_failure_criterion (m_particles.f90:3323-3381) on arrays."""
+    t = math.tan(phi)
+    alpha1 = t / math.sqrt(9.0 + 12.0 * (t * t))
+    p = np.where(p < 0.0, 0.0, p)
+    I1 = 3.0 * p
+    J2 = np.sqrt((sxx * sxx + 2.0 * (sxy * sxy) + syy * syy + (sxx + syy) * (sxx + syy)) / 2.0) + 1.0e-6
+    f = J2 > alpha1 * I1
+    sk = alpha1 * I1[f] / J2[f]
+    sxx, sxy, syy = sxx.copy(), sxy.copy(), syy.copy()
+    sxx[f], sxy[f], syy[f] = sk * sxx[f], sk * sxy[f], sk * syy[f]
+    return p, sxx, sxy, syy
+
+
+def two_phase_run(scene, steps):
+    """time_integration (declarations_sph.f90:525-791) of the two-phase step
+    with stress_integration = 1: first_half and Drucker-Prager on the soil
+    before the right-hand side (from the second step on), then first_step or
+    second_half and Drucker-Prager again.  The right-hand side writes p, c,
+    the soil stress, vof and eps_p back into the state, as the reference's
+    routines do in place."""
+    s = scene.copy()
+    prm = s.params
+    dt = prm.dt
+    rates = {}
+    mins = {}
+    for it in range(1, steps + 1):
+        W, S = s.phases
+        if it != 1:
+            for ph, P in ((1, W), (2, S)):
+                r = rates[ph]
+                mins[ph] = dict(rho=P.rho.copy(), v=P.vx.copy())
+                P.rho[:] = P.rho + (dt / 2.0) * r["drho"]
+                if ph == 1 and prm.volume_fraction:
+                    mins[ph]["vof"] = P.vof.copy()
+                    P.vof[:] = P.vof + (dt / 2.0) * r["dvof"]
+                move = P.itype >= 0
+                P.vx[move] = P.vx[move] + (dt / 2.0) * r["dvx"][move]
+            S.p[:], S.sxx[:], S.sxy[:], S.syy[:] = _dp_return(S.p, S.sxx, S.sxy, S.syy, prm.soil.phi)
+        out = two_phase_rhs(s, it)
+        W.p[:], W.c[:] = out[1]["p"], out[1]["c"]
+        for f in ("p", "sxx", "sxy", "syy", "c", "vof", "epsilon_p"):
+            getattr(S, f)[:] = out[2][f]
+        rates = out
+        for ph, P in ((1, W), (2, S)):
+            r = out[ph]
+            if it == 1:
+                P.rho[:] = P.rho + (dt / 2.0) * r["drho"]
+                if ph == 1 and prm.volume_fraction:
+                    P.vof[:] = P.vof + (dt / 2.0) * r["dvof"]
+            else:
+                P.rho[:] = mins[ph]["rho"] + dt * r["drho"]
+                if ph == 1 and prm.volume_fraction:
+                    P.vof[:] = mins[ph]["vof"] + dt * r["dvof"]
+            if ph == 2:
+                P.sxx[:] = P.sxx + dt * r["dsxx"]
+                P.sxy[:] = P.sxy + dt * r["dsxy"]
+                P.syy[:] = P.syy + dt * r["dsyy"]
+                P.p[:] = P.p + dt * r["dp"]
+            move = P.itype >= 0
+            base = P.vx if it == 1 else mins[ph]["v"]
+            hdt = dt / 2.0 if it == 1 else dt
+            vnew = base[move] + hdt * r["dvx"][move] + r["av"][move]
+            P.vx[move] = vnew
+            P.x[move] = P.x[move] + dt * vnew
+        S.p[:], S.sxx[:], S.sxy[:], S.syy[:] = _dp_return(S.p, S.sxx, S.sxy, S.syy, prm.soil.phi)
+    return s
+
+
+def test_numpy_two_phase_time_integration_matches_the_c_oracle():
+    """Six leapfrog steps (the first step, then predictor / corrector) of the
+    two-phase scene, numpy against the C oracle, bit for bit."""
+    s = scenes.jitter(scenes.small("two_phase", precision=SPHG_FP64), 0.0002, seed=9)
+    ref = two_phase_run(s, 6)
+    o = Oracle(s)
+    assert o.time_integration(6) == 0
+    for ph, fields in ((1, ("x", "vx", "rho", "vof", "p", "c")),
+                       (2, ("x", "vx", "rho", "vof", "p", "sxx", "sxy", "syy", "epsilon_p"))):
+        d, r = o.download(ph), ref.phases[ph - 1]
+        for f in fields:
+            a, b = np.asarray(getattr(d, f)), np.asarray(getattr(r, f))
+            assert np.array_equal(a, b), (ph, f, int((a != b).sum()), float(np.abs(a - b).max()))

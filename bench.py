@@ -180,13 +180,16 @@ def oracle_throughput(steps: int, warmup: int, cores: int):
 
 def cpu_baseline(steps: int, cores: int | None = None):
     """The oracle port of the serial reference step, one instance per host
-    core on a sub-domain sample of the workload (same spacing and physics)."""
+    core on a sub-domain sample of the workload (same spacing and physics),
+    and the same sample on one core alone (the reference's serial path)."""
     cores = cores or host_cores()
     n, dt, v = oracle_throughput(steps, 1, cores)
+    _, dt1, v1 = oracle_throughput(steps, 1, 1)
     return {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
             "sample": f"serial C restatement of the Fortran step, one instance per core on {cores} cores, each "
                       f"{steps} leapfrog steps of its own {n}-particle sub-domain of the workload ({SUBDOMAIN_TEXT})",
-            "seconds": dt}
+            "seconds": dt,
+            "serial": {"value": v1, "unit": UNIT, "cores": 1, "seconds": dt1}}
 
 
 def run_reference(args, rank, world):

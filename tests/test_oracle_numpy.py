@@ -657,21 +657,28 @@ def test_numpy_two_phase_time_integration_matches_the_c_oracle():
 
 def single_phase_run(scene, steps):
     """time_integration_for_water (declarations_sph.f90:794-886) or
-    time_integration_for_soil (:978-1127), stress_integration = 1.  The
-    right-hand side writes back what the reference's routines change in
-    place: the summation density and p (water); p, the stresses, c and eps_p
-    (soil)."""
+    time_integration_for_soil (:978-1127), with the soil stress integrated by
+    full-step Euler (stress_integration = 1) or leapfrog (2).  The right-hand
+    side writes back what the reference's routines change in place: the
+    summation density and p (water); p, the stresses, c and eps_p (soil)."""
     s = scene.copy()
     prm = s.params
     dt = prm.dt
     P = s.phases[0]
     soil = P.material == 2
     r = None
+    leap = soil and prm.stress_integration == 2
+    stress = ("sxx", "sxy", "syy", "p")
+    rates = {"sxx": "dsxx", "sxy": "dsxy", "syy": "dsyy", "p": "dp"}
     for it in range(1, steps + 1):
         move = P.itype >= 0
         if it != 1:
             rho_min, v_min = P.rho.copy(), P.vx.copy()
             P.rho[:] = P.rho + (dt / 2.0) * r["drho"]
+            if leap:
+                smin = {f: getattr(P, f).copy() for f in stress}
+                for f in stress:
+                    getattr(P, f)[:] = getattr(P, f) + (dt / 2.0) * r[rates[f]]
             P.vx[move] = P.vx[move] + (dt / 2.0) * r["dvx"][move]
             if soil:
                 P.p[:], P.sxx[:], P.sxy[:], P.syy[:] = _dp_return(P.p, P.sxx, P.sxy, P.syy, prm.soil.phi)
@@ -687,10 +694,13 @@ def single_phase_run(scene, steps):
         else:
             P.rho[:] = rho_min + dt * r["drho"]
         if soil:
-            P.sxx[:] = P.sxx + dt * r["dsxx"]
-            P.sxy[:] = P.sxy + dt * r["dsxy"]
-            P.syy[:] = P.syy + dt * r["dsyy"]
-            P.p[:] = P.p + dt * r["dp"]
+            for f in stress:
+                if not leap:
+                    getattr(P, f)[:] = getattr(P, f) + dt * r[rates[f]]
+                elif it == 1:
+                    getattr(P, f)[:] = getattr(P, f) + (dt / 2.0) * r[rates[f]]
+                else:
+                    getattr(P, f)[:] = smin[f] + dt * r[rates[f]]
         base = P.vx if it == 1 else v_min
         hdt = dt / 2.0 if it == 1 else dt
         vnew = base[move] + hdt * r["dvx"][move] + r["av"][move]
@@ -701,11 +711,13 @@ def single_phase_run(scene, steps):
     return s
 
 
-@pytest.mark.parametrize("name", ["dam_break", "granular_column"])
-def test_numpy_single_phase_time_integration_matches_the_c_oracle(name):
-    """Six leapfrog steps of the water-only and the soil-only step, numpy
-    against the C oracle, bit for bit."""
+@pytest.mark.parametrize("name,stress_integration", [("dam_break", 1), ("granular_column", 1),
+                                                     ("granular_column", 2)])
+def test_numpy_single_phase_time_integration_matches_the_c_oracle(name, stress_integration):
+    """Six leapfrog steps of the water-only and the soil-only step (soil
+    stress by Euler or by leapfrog), numpy against the C oracle, bit for bit."""
     s = scenes.jitter(scenes.small(name, precision=SPHG_FP64), 0.0002, seed=10)
+    s.params.stress_integration = stress_integration
     ref = single_phase_run(s, 6)
     o = Oracle(s)
     assert o.time_integration(6) == 0

@@ -546,20 +546,26 @@ def two_phase_rhs(scene, itimestep=1):
         vof2 = np.zeros(Wp.n)                                              # volume_fraction_water
         np.add.at(vof2, i, ms[j] * w)
         W["vof2"] = 1.0 - vof2 / prm.soil.rho0
-        assert itimestep % 40 != 0    # the renormalisation is not restated here
+        # the renormalisation every renorm_interval steps (declarations_sph.f90:1414-1421)
+        if prm.volume_fraction_renorm and prm.renorm_interval > 0 and itimestep % prm.renorm_interval == 0:
+            r = W["rho"] / W["vof"]
+            W["vof"] = W["vof2"].copy()
+            W["rho"] = r * W["vof"]
     W["npairs_cross"] = len(i)
     return out
 
 
-@pytest.mark.parametrize("seed", [7, 8])
-def test_numpy_two_phase_restatement_matches_the_c_oracle(seed):
+@pytest.mark.parametrize("seed,itimestep", [(7, 1), (8, 1), (7, 40)])
+def test_numpy_two_phase_restatement_matches_the_c_oracle(seed, itimestep):
+    """The two-phase right-hand side, at an ordinary step and at a step that
+    renormalises the water volume fraction."""
     s = scenes.jitter(scenes.small("two_phase", precision=SPHG_FP64), 0.0002, seed=seed)
     rng = np.random.default_rng(seed)
     for P in s.phases:
         P.vx[:P.ntotal] = rng.normal(0, 0.03, size=(P.ntotal, 2))
-    ref = two_phase_rhs(s)
+    ref = two_phase_rhs(s, itimestep)
     o = Oracle(s)
-    assert o.single_step(1) == 0
+    assert o.single_step(itimestep) == 0
     assert len(o.pairs(2)[0]) == ref[1]["npairs_cross"]
     fields = {1: ("drho", "p", "c", "dvx", "av", "rho", "vof", "dvof", "vof2"),
               2: ("drho", "p", "c", "dvx", "av", "rho", "vof", "sxx", "sxy", "syy", "dsxx", "dsxy", "dsyy", "dp",

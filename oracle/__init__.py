@@ -4,7 +4,8 @@ ctypes front-end of sph_oracle.c, the serial FP64 restatement of the
 reference's step (cwang2015/sources; see the C file's header for the
 reference lines it follows).  PARITY UNPINNED: the reference ships no golden
 vectors for this path and cannot be compiled here; known-answer tests in
-tests/ pin the restatement instead.
+tests/ pin the restatement instead, and a separate numpy restatement of the
+same Fortran agrees with it bit for bit (tests/test_oracle_numpy.py).
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
 this package, as the checker; the product never does.

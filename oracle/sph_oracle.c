@@ -20,7 +20,9 @@
  * modules `constants`/`declarations`).  The restatement is pinned instead by
  * known-answer checks in tests/ (kernel normalisation, finite-difference
  * gradients, partition of unity, momentum conservation, DP return, pair set
- * against brute force).
+ * against brute force), and by a second restatement in numpy, written
+ * separately from the same Fortran, that agrees with this one bit for bit on
+ * the three right-hand sides and integrators (tests/test_oracle_numpy.py).
  *
  * Only tests/, __graft_entry__.smoke() and the CPU-baseline leg of bench.py
  * use this file, as the checker.  The product (libsphg) never links it.

@@ -276,30 +276,6 @@ struct Engine : EngineBase {
     }
 
     // smallest double t with sqrt(t) >= K: then sqrt(r2) < K  <=>  r2 < t
-    // FP32 prefilter bounds (SearchConst).  Positions within |c| <= B are
-    // rounded to float with error <= 2^-24 (B + r) each, so dx and dy carry
-    // e' <= 2^-23 (B + r) + 2^-24 * 1.5 r; near the threshold r2 = r^2 the
-    // float r2 is off by at most 3 r e' + 2 e'^2 + 4 * 2^-24 r^2.  The band
-    // is twice that, rounded outwards; B is twice the domain extent.
-    void set_prefilter(SearchConst& sc) {
-        sc.prefilter = 0;
-#if SPHG_F32_SCAN
-        if (!sc.uniform) return;
-        const sphg_params& p = ctx->prm;
-        const double B = 2.0 * std::max(std::max(std::fabs(p.x_min), std::fabs(p.x_max)),
-                                        std::max(std::fabs(p.y_min), std::fabs(p.y_max)));
-        const double r2 = sc.r2_uniform, r = std::sqrt(r2);
-        const double u = std::ldexp(1.0, -24);
-        const double e = 2.0 * u * (B + r) + u * 1.5 * r;
-        const double band = 2.0 * (3.0 * r * e + 2.0 * e * e + 4.0 * u * r2);
-        if (!(band < 0.25 * r2)) return;
-        sc.r2_in = std::nextafter((float)(r2 - band), 0.0f);
-        sc.r2_out = std::nextafter((float)(r2 + band), INFINITY);
-        sc.bound = B;
-        sc.prefilter = 1;
-#endif
-    }
-
     static double exact_threshold(double K) {
         double t = K * K;
         while (t > 0 && std::sqrt(t) >= K) t = std::nextafter(t, 0.0);
@@ -315,7 +291,7 @@ struct Engine : EngineBase {
         void* old[] = {D.x, D.v, D.v_min, D.rho, D.rho_min, D.vof, D.vof_min, D.p, D.c, D.mass, D.hsml, D.sxx, D.sxy,
                        D.syy, D.sxx_min, D.sxy_min, D.syy_min, D.p_min, D.eps_p, D.itype, D.orig, D.fail, D.sid, D.drho,
                        D.dvof, D.dsxx, D.dsxy, D.dsyy, D.dp, D.txx, D.txy, D.tyy, D.vcc, D.wxy, D.vof2, D.dv, D.av,
-                       D.countiac, D.cell_id, D.cell_fill, D.perm, D.xs, D.xsf, D.hs, D.recA, D.recA2, D.recB};
+                       D.countiac, D.cell_id, D.cell_fill, D.perm, D.xs, D.hs, D.recA, D.recA2, D.recB};
         for (void* p : old) release(p);
         for (void* p : shadow[ph]) release(p);
         shadow[ph].clear();
@@ -335,7 +311,7 @@ struct Engine : EngineBase {
         rc |= alloc(&D.tyy, N); rc |= alloc(&D.vcc, N); rc |= alloc(&D.wxy, N); rc |= alloc(&D.vof2, N);
         rc |= alloc(&D.dv, N); rc |= alloc(&D.av, N);
         rc |= alloc(&D.countiac, N); rc |= alloc(&D.cell_id, N); rc |= alloc(&D.cell_fill, N); rc |= alloc(&D.perm, N);
-        rc |= alloc(&D.xs, N); rc |= alloc(&D.xsf, N); rc |= alloc(&D.hs, N);
+        rc |= alloc(&D.xs, N); rc |= alloc(&D.hs, N);
         rc |= alloc(&D.recA, N); rc |= alloc(&D.recA2, N); rc |= alloc(&D.recB, N);
         if (rc) return SPHG_ERR_CUDA;
         for (auto& f : field_refs(ph)) {
@@ -519,7 +495,6 @@ struct Engine : EngineBase {
         bool uniform = hmin == hmax;
         double K = sk * hmax;
         sc_same.scale_k = sk; sc_same.uniform = uniform; sc_same.r2_uniform = uniform ? exact_threshold(K) : 0.0;
-        set_prefilter(sc_same);
         sc_cross = sc_same;
         prepared = true;
         // spatial order from the start

@@ -52,14 +52,6 @@ struct SearchConst {
     double scale_k;       // get_scale_k (m_particles.f90:916)
     double r2_uniform;    // exact squared-radius threshold when every h is equal
     int uniform;          // all particles of both lists share one h
-    // FP32 prefilter of the uniform-h test (float copies of the sorted
-    // positions): r2 computed in float below r2_in is certainly a hit, above
-    // r2_out certainly a miss (margins cover the float rounding of positions
-    // up to |coordinate| <= bound); in between, and for particles beyond the
-    // bound, the exact FP64 test decides, so the pair set is unchanged
-    int prefilter;
-    float r2_in, r2_out;
-    double bound;
 };
 
 // The parameters that differ between the scenes of a batched context
@@ -100,7 +92,6 @@ struct PhaseDev {
     // cell list and sorted copies
     int *cell_id, *cell_fill, *cell_start, *perm;
     double2 *xs;
-    float2 *xsf;          // float copy of xs for the FP32 prefilter
     double *hs;
     RecA<T> *recA, *recA2;
     RecB<T> *recB;
@@ -326,64 +317,29 @@ struct KernelConst {
 };
 
 // Per-thread hit buffer in shared memory: entry i of thread t at [i*TPB + t],
-// so a warp's accesses are conflict-free.
-// FP32 prefilter of the candidate test (SearchConst.prefilter).  Off: on a
-// B200 at 912,016 particles it made the step slower (0.595 -> 0.735 ms; the
-// FP64 test is not what bounds the scan, the extra registers are).
-#ifndef SPHG_F32_SCAN
-#define SPHG_F32_SCAN 0
-#endif
+// so a warp's accesses are conflict-free.  Only the neighbour index is kept;
+// dx, dy are recomputed from the sorted positions when the buffer drains,
+// which leaves more of the unified L1/shared memory to L1, where the
+// neighbour records live.  Measured on a B200 at 912,016 particles and
+// dropped: an FP32 prefilter of the candidate test (0.595 -> 0.735 ms per
+// step), two neighbours per drain iteration (within 1 %), dx and dy kept in
+// the buffer (slower) and an L1 prefetch of the buffered records (no gain).
 #ifndef SPHG_SCAN_U
 #define SPHG_SCAN_U 4
-#endif
-// Neighbours per iteration of the drain loop (1 or 2); 2 measured within 1 %
-// of 1 on the 912,016-particle step (water_pass_b -6 %, cross_soil +11 %).
-#ifndef SPHG_BODY_U
-#define SPHG_BODY_U 1
-#endif
-// Hit buffer holds only the neighbour index; dx, dy are recomputed from the
-// sorted positions when the buffer drains.  The smaller buffer leaves more of
-// the unified L1/shared memory to L1, where the neighbour records live
-// (measured faster on B200 than keeping dx, dy in shared memory).
-#ifndef SPHG_HB_MONLY
-#define SPHG_HB_MONLY 1
-#endif
-#ifndef SPHG_PREFETCH
-#define SPHG_PREFETCH 0
 #endif
 
 template <typename T, int TPB, int CH>
 struct HitBuf {
     int m[CH * TPB];
-#if !SPHG_HB_MONLY
-    T dx[CH * TPB];
-    T dy[CH * TPB];
-#endif
 };
 
-__device__ __forceinline__ void prefetch_l1(const void* p) {
-    asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
-}
-
-// Warp-synchronous neighbour visitor.  Each lane scans the candidates of its
-// particle (three row runs of the sorted list) with the exact FP64 pair
-// test and appends hits to its buffer; as soon as any lane's buffer is full,
-// or every lane has finished scanning, the whole warp drains the buffers
-// through body(m, dx, dy) together.  Scanning (cheap, divergent) and pair
-// physics (expensive) thus run with full lanes instead of the body executing
-// under the hit/miss divergence of the scan.  All 32 lanes must call it;
-// `active` marks lanes that own a particle.
-template <typename T, int TPB, int CH, class F, class PF>
+template <typename T, int TPB, int CH, class F>
 __device__ __forceinline__ int visit_batched(HitBuf<T, TPB, CH>& buf, const GridGeom& g, const SearchConst& sc,
                                              const int* __restrict__ cstart, const double2* __restrict__ xs,
-                                             const float2* __restrict__ xsf, const double* __restrict__ hs,
-                                             double2 xa, double ha, int self, bool active, F&& body, PF&& pre) {
+                                             const double* __restrict__ hs, double2 xa, double ha, int self,
+                                             bool active, F&& body) {
     const unsigned FULL = 0xffffffffu;
     const int tid = threadIdx.x;
-#if SPHG_F32_SCAN
-    const bool pf = sc.prefilter && fabs(xa.x) <= sc.bound && fabs(xa.y) <= sc.bound;
-    const float2 xaf = make_float2((float)xa.x, (float)xa.y);
-#endif
     int b0 = 0, b1 = 0, b2 = 0, L0 = 0, L1 = 0, L2 = 0;
     if (active) {
         int cx, cy; bool clamped;
@@ -408,98 +364,40 @@ __device__ __forceinline__ int visit_batched(HitBuf<T, TPB, CH>& buf, const Grid
                 const int tt = t + u;
                 mm[u] = tt < L0 ? b0 + tt : (tt < L0 + L1 ? b1 + (tt - L0) : b2 + (tt - L0 - L1));
             }
+            double2 xb[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (t + u < tot) xb[u] = xs[mm[u]];
             // exact FP64 test (the reference's operations, m_particles.f90:972-973)
-            auto exact = [&](int m) {
-                const double2 xb = xs[m];
-                const double dx = xa.x - xb.x;
-                const double dy = xa.y - xb.y;
-                const double r2 = __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));
-                return sc.uniform ? (r2 < sc.r2_uniform) : (__dsqrt_rn(r2) < sc.scale_k * ((ha + hs[m]) / 2.0));
-            };
             bool hitu[U];
-#if SPHG_F32_SCAN
-            if (pf) {
-                float2 xbf[U];
 #pragma unroll
-                for (int u = 0; u < U; ++u)
-                    if (t + u < tot) xbf[u] = xsf[mm[u]];
-#pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    hitu[u] = false;
-                    if (t + u < tot && mm[u] != self) {
-                        const float dx = xaf.x - xbf[u].x, dy = xaf.y - xbf[u].y;
-                        const float r2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
-                        hitu[u] = r2 < sc.r2_in ? true : (r2 > sc.r2_out ? false : exact(mm[u]));
-                    }
-                }
-            } else
-#endif
-            {
-                double2 xb[U];
-#pragma unroll
-                for (int u = 0; u < U; ++u)
-                    if (t + u < tot) xb[u] = xs[mm[u]];
-#pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    hitu[u] = false;
-                    if (t + u < tot && mm[u] != self) {
-                        const double dx = xa.x - xb[u].x;
-                        const double dy = xa.y - xb[u].y;
-                        const double r2 = __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));
-                        hitu[u] = sc.uniform ? (r2 < sc.r2_uniform)
-                                             : (__dsqrt_rn(r2) < sc.scale_k * ((ha + hs[mm[u]]) / 2.0));
-                    }
+            for (int u = 0; u < U; ++u) {
+                hitu[u] = false;
+                if (t + u < tot && mm[u] != self) {
+                    const double dx = xa.x - xb[u].x;
+                    const double dy = xa.y - xb[u].y;
+                    const double r2 = __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));
+                    hitu[u] = sc.uniform ? (r2 < sc.r2_uniform)
+                                         : (__dsqrt_rn(r2) < sc.scale_k * ((ha + hs[mm[u]]) / 2.0));
                 }
             }
 #pragma unroll
             for (int u = 0; u < U; ++u) {
-                {
-                    const bool hit = hitu[u];
-                    if (hit) {
-                        buf.m[cnt * TPB + tid] = mm[u];
-#if !SPHG_HB_MONLY
-                        const double2 xb = xs[mm[u]];
-                        buf.dx[cnt * TPB + tid] = (T)(xa.x - xb.x);
-                        buf.dy[cnt * TPB + tid] = (T)(xa.y - xb.y);
-#endif
-                        ++cnt;
-                        ++hits;
-                    }
+                if (hitu[u]) {
+                    buf.m[cnt * TPB + tid] = mm[u];
+                    ++cnt;
+                    ++hits;
                 }
             }
             t = t + U < tot ? t + U : tot;
         }
-#if SPHG_PREFETCH
-        for (int i = 0; i < cnt; ++i) pre(buf.m[i * TPB + tid]);
-#endif
-#if SPHG_BODY_U == 2 && SPHG_HB_MONLY
-        // two neighbours per iteration, in buffer order: independent record
-        // loads and arithmetic chains the scheduler can overlap
-        for (int i = 0; __any_sync(FULL, i < cnt); i += 2) {
-            if (i + 1 < cnt) {
-                const int m0 = buf.m[i * TPB + tid], m1 = buf.m[(i + 1) * TPB + tid];
-                const double2 x0 = xs[m0], x1 = xs[m1];
-                body(m0, (T)(xa.x - x0.x), (T)(xa.y - x0.y));
-                body(m1, (T)(xa.x - x1.x), (T)(xa.y - x1.y));
-            } else if (i < cnt) {
-                const int m = buf.m[i * TPB + tid];
-                const double2 xb = xs[m];
-                body(m, (T)(xa.x - xb.x), (T)(xa.y - xb.y));
-            }
-        }
-#else
         for (int i = 0; __any_sync(FULL, i < cnt); ++i) {
             if (i < cnt) {
                 const int m = buf.m[i * TPB + tid];
-#if SPHG_HB_MONLY
                 const double2 xb = xs[m];
                 body(m, (T)(xa.x - xb.x), (T)(xa.y - xb.y));
-#else
-                body(m, buf.dx[i * TPB + tid], buf.dy[i * TPB + tid]);
-#endif
             }
         }
-#endif
         cnt = 0;
     }
     return hits;

@@ -215,9 +215,6 @@ __global__ void __launch_bounds__(256) k_gather(PhaseDev<T> P, SimConst c, int s
         int a = P.perm[k];
         if (fh) fail0 = first_half_one(P, a, c, with_vof, fh_dp);
         P.xs[k] = P.x[a];
-#if SPHG_F32_SCAN
-        P.xsf[k] = make_float2((float)P.x[a].x, (float)P.x[a].y);
-#endif
         P.hs[k] = P.hsml[a];
         double2 v = P.v[a];
         RecA<T> ra;
@@ -310,7 +307,7 @@ __global__ void __launch_bounds__(SPHG_TPB) k_water_sum(PhaseDev<T> P, GridGeom 
     T num = w0 * ma;
     T sx = T(0), sy = T(0);
     const RecA<T>* __restrict__ rec = P.recA;
-    const int hits = visit_batched(hb, g, sc, P.cell_start, P.xs, P.xsf, P.hs, xa, ha, k, valid, [&](int m, T dx, T dy) {
+    const int hits = visit_batched(hb, g, sc, P.cell_start, P.xs, P.hs, xa, ha, k, valid, [&](int m, T dx, T dy) {
         const RecA<T> rb = rec[m];
         T w, sr, r2, mh;
         pair_kernel<T, SKF>(ka, sc, ha, P.hs, m, dx, dy, w, sr, r2, mh);
@@ -319,7 +316,7 @@ __global__ void __launch_bounds__(SPHG_TPB) k_water_sum(PhaseDev<T> P, GridGeom 
         num += mb * w;
         sx += mb * ((rb.vx - ra.vx) * (sr * dx));
         sy += mb * ((rb.vy - ra.vy) * (sr * dy));
-    }, [&](int m) { prefetch_l1(rec + m); });
+    });
     if (valid) {
         const int a = P.perm[k];
         const T rho = num / wi;
@@ -358,7 +355,7 @@ __global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_A : 1) k_
     KernelConst<T, SKF> ka;
     ka.init((T)ha);
     T con = 0, dl = 0, t0 = 0, t1 = 0, t2 = 0, t3 = 0;
-    const int hits = visit_batched(hb, g, sc, P.cell_start, P.xs, P.xsf, P.hs, xa, ha, k, valid, [&](int m, T dx, T dy) {
+    const int hits = visit_batched(hb, g, sc, P.cell_start, P.xs, P.hs, xa, ha, k, valid, [&](int m, T dx, T dy) {
         const RecA<T> rb = rec[m];
         T w, sr, r2, mh;
         pair_kernel<T, SKF>(ka, sc, ha, P.hs, m, dx, dy, w, sr, r2, mh);
@@ -377,7 +374,7 @@ __global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_A : 1) k_
             t1 += rb.vol * (du * gy + dv * gx);
             t2 += rb.vol * (c23 * (T(2) * dv * gy - du * gx));
         }
-    }, [&](int m) { prefetch_l1(rec + m); });
+    });
     if (valid) {
         T txx, txy, tyy, drho;
         double p, cnew, vof;
@@ -432,7 +429,7 @@ template <typename T, int SKF, bool FCH, class HB>
 __device__ __forceinline__ void cross_soil_sums(HB& hb, const PhaseDev<T>& W, const GridGeom& g, const SearchConst& sc,
                                                 const SimConst& c, const KernelConst<T, SKF>& ka, double2 xa, double ha,
                                                 const RecA<T>& ra, bool valid, T& ddx, T& ddy, T& dpx, T& dpy) {
-    visit_batched(hb, g, sc, W.cell_start, W.xs, W.xsf, W.hs, xa, ha, -1, valid, [&](int m, T dx, T dy) {
+    visit_batched(hb, g, sc, W.cell_start, W.xs, W.hs, xa, ha, -1, valid, [&](int m, T dx, T dy) {
         const RecA<T> rb = W.recA[m];
         const RecB<T> qb = W.recB[m];
         T w, sr, rr, mh;
@@ -447,7 +444,7 @@ __device__ __forceinline__ void cross_soil_sums(HB& hb, const PhaseDev<T>& W, co
         const T mp = rb.vol * qb.p;
         dpx += mp * gx;
         dpy += mp * gy;
-    }, [&](int m) { prefetch_l1(W.recA + m); prefetch_l1(W.recB + m); });
+    });
 }
 
 // Water side: darcy_law :3832, volume_fraction_water2 :3940 (dvof) and
@@ -456,7 +453,7 @@ template <typename T, int SKF, bool FCH, class HB>
 __device__ __forceinline__ int cross_water_sums(HB& hb, const PhaseDev<T>& S, const GridGeom& g, const SearchConst& sc,
                                                 const SimConst& c, const KernelConst<T, SKF>& ka, double2 xa, double ha,
                                                 const RecA<T>& ra, bool valid, T& ddx, T& ddy, T& dvof, T& v2) {
-    return visit_batched(hb, g, sc, S.cell_start, S.xs, S.xsf, S.hs, xa, ha, -1, valid, [&](int m, T dx, T dy) {
+    return visit_batched(hb, g, sc, S.cell_start, S.xs, S.hs, xa, ha, -1, valid, [&](int m, T dx, T dy) {
         const RecA<T> rb = S.recA[m];
         const T phis = S.recB[m].vof;
         T w, sr, rr, mh;
@@ -469,7 +466,7 @@ __device__ __forceinline__ int cross_water_sums(HB& hb, const PhaseDev<T>& S, co
         ddy -= q * uy;
         dvof -= mb * (sr * (ux * dx + uy * dy));
         v2 += mb * w;
-    }, [&](int m) { prefetch_l1(S.recA + m); prefetch_l1(S.recB + m); });
+    });
 }
 
 // ----------------------------------------------------------- water: pass B
@@ -513,7 +510,7 @@ __global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_B : 1) k_
     ka.init((T)ha);
     T d1x = 0, d1y = 0, d2x = 0, d3x = 0, d2y = 0, d3y = 0;
     T avx = 0, avy = 0, rpx = 0, rpy = 0, dvf = 0, xsx = 0, xsy = 0;
-    visit_batched(hb, g, sc, P.cell_start, P.xs, P.xsf, P.hs, xa, ha, k, valid, [&](int m, T dx, T dy) {
+    visit_batched(hb, g, sc, P.cell_start, P.xs, P.hs, xa, ha, k, valid, [&](int m, T dx, T dy) {
         const RecA<T> rb = rec[m];
         const RecB<T> qb = P.recB[m];
         T w, sr, rr, mh;
@@ -555,7 +552,7 @@ __global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_B : 1) k_
             xsx -= q * dvx;
             xsy -= q * dvy;
         }
-    }, [&](int m) { prefetch_l1(rec + m); prefetch_l1(P.recB + m); });
+    });
     T dvx = -(phia * d1x) + d2x + d3x;
     T dvy = -(phia * d1y) + d2y + d3y;
     if (ra.rho > T(0)) { dvx = dvx / ra.rho; dvy = dvy / ra.rho; }
@@ -643,7 +640,7 @@ __global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_SOIL : 1)
     T s1x = 0, s1y = 0, s2x = 0, s3x = 0, s2y = 0, s3y = 0;
     T avx = 0, avy = 0, rpx = 0, rpy = 0, xsx = 0, xsy = 0;
     T dpp = 0, dsx = 0, dsxy = 0, dsy = 0;
-    const int hits = visit_batched(hb, g, sc, P.cell_start, P.xs, P.xsf, P.hs, xa, ha, k, valid, [&](int m, T dx, T dy) {
+    const int hits = visit_batched(hb, g, sc, P.cell_start, P.xs, P.hs, xa, ha, k, valid, [&](int m, T dx, T dy) {
         const RecA<T> rb = P.recA[m];
         const RecB<T> qb = P.recB[m];
         T w, sr, rr, mh;
@@ -709,7 +706,7 @@ __global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_SOIL : 1)
             xsx += q * du;
             xsy += q * dv;
         }
-    }, [&](int m) { prefetch_l1(P.recA + m); prefetch_l1(P.recB + m); });
+    });
     int fail = 0, fail3 = 0;
     T dvx, dvy;
     if (SINGLE) { dvx = -s1x + s2x + s3x; dvy = -s1y + s2y + s3y; }

@@ -308,10 +308,14 @@ const char* sphg_strerror(int code);
  * SPHG_NOALLOC_MAX_PARTICLES, or a neighbour grid above
  * SPHG_NOALLOC_MAX_CELLS cells, returns SPHG_ERR_BAD_ARG.  All calls share
  * that array, so calls whose GPU work overlaps race and must be serialised.
- * The first call on a device looks up the array's address and should come
- * before any stream capture.  The call waits on `cuda_stream` once (for the
- * h range); the result is complete when the stream reaches the end of the
- * call's work. */
+ * Every call looks up the array's device address with the caller's device
+ * current; the first call on a device loads the library's device module and
+ * should come before any stream capture.  The call waits on `cuda_stream`
+ * once (for the h range and the position check); the result is complete when
+ * the stream reaches the end of the call's work.  NaN or infinite positions
+ * return SPHG_ERR_NONFINITE, non-positive h SPHG_ERR_BAD_ARG, before any
+ * density kernel runs; particles outside the grid extent are clamped into
+ * its edge cells, which keeps their pairs exact. */
 int sphg_sum_density_noalloc(const sphg_params* p, int32_t n, const double* x_dev, const double* hsml_dev,
                              const double* mass_dev, const double* rho_dev, double* rho_out_dev,
                              void* cuda_stream);

@@ -21,14 +21,22 @@
 // zero.  Calls whose GPU work overlaps (two streams, or two host threads)
 // race on the array and must be serialised by the caller.
 //
-// Set-up: the first call on a device looks up the array's device address
-// (cudaGetSymbolAddress) with that device current and caches it; that first
-// call should come before any stream capture.  Every call also waits once on
-// its stream for the smoothing-length range it needs to size the grid.
+// Set-up: every call looks up the array's device address
+// (cudaGetSymbolAddress) with the caller's device current, so the address is
+// right even after the caller has reset the device and the module was loaded
+// anew.  The first call on a device loads the library's device module, and
+// with it the array; that first call should come before any stream capture.
+// Every call also waits once on its stream, for the smoothing-length range
+// it needs to size the grid and for the finiteness check of the positions.
+//
+// Errors: NaN or infinite positions return SPHG_ERR_NONFINITE and
+// non-positive or non-finite h return SPHG_ERR_BAD_ARG, both before any
+// density kernel runs.  Particles outside [x_min, x_max] x [y_min, y_max]
+// are clamped into the edge cells of the grid; every x cell is at least one
+// support radius wide, so their pairs are still all found.
 #include <cuda_runtime.h>
 
 #include <cmath>
-#include <mutex>
 
 #include "../../include/sphg.h"
 #include "sphg_kernels.cuh"
@@ -64,48 +72,44 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kBytes];
 
 namespace {
 
-std::mutex g_mu;
-void* g_base[64] = {nullptr};
-
-// Device address of the scratch array on the current device, looked up once.
+// Device address of the scratch array on the current device.
 int scratch_base(void** out) {
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return SPHG_ERR_NO_DEVICE;
-    std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_base[dev]) {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p) return SPHG_ERR_CUDA;
-        g_base[dev] = p;
-    }
-    *out = g_base[dev];
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) return SPHG_ERR_CUDA;
+    *out = p;
     return SPHG_OK;
 }
 
-// smoothing-length range [min, max] and a flag for non-positive/non-finite h
-__global__ void __launch_bounds__(1024) k_na_hrange(int n, const double* __restrict__ h, double* __restrict__ out) {
+// smoothing-length range [min, max], a flag for non-positive/non-finite h
+// and a flag for non-finite positions: out = {hmin, hmax, bad h, bad x}
+__global__ void __launch_bounds__(1024) k_na_hrange(int n, const double* __restrict__ h, const double2* __restrict__ x,
+                                                    double* __restrict__ out) {
     __shared__ double smin[32], smax[32];
-    __shared__ int sbad[32];
+    __shared__ int sbad[32], sbadx[32];
     double lo = INFINITY, hi = 0.0;
-    int bad = 0;
+    int bad = 0, badx = 0;
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
         const double v = h[i];
         if (!(v > 0.0) || !isfinite(v)) bad = 1;
         lo = fmin(lo, v); hi = fmax(hi, v);
+        const double2 p = x[i];
+        if (!(isfinite(p.x) && isfinite(p.y))) badx = 1;
     }
     for (int o = 16; o > 0; o >>= 1) {
         lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
         hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
         bad |= __shfl_xor_sync(0xffffffffu, bad, o);
+        badx |= __shfl_xor_sync(0xffffffffu, badx, o);
     }
     const int w = threadIdx.x >> 5;
-    if ((threadIdx.x & 31) == 0) { smin[w] = lo; smax[w] = hi; sbad[w] = bad; }
+    if ((threadIdx.x & 31) == 0) { smin[w] = lo; smax[w] = hi; sbad[w] = bad; sbadx[w] = badx; }
     __syncthreads();
     if (threadIdx.x == 0) {
         for (int i = 1; i < (int)(blockDim.x >> 5); ++i) {
-            lo = fmin(lo, smin[i]); hi = fmax(hi, smax[i]); bad |= sbad[i];
+            lo = fmin(lo, smin[i]); hi = fmax(hi, smax[i]); bad |= sbad[i]; badx |= sbadx[i];
         }
-        out[0] = lo; out[1] = hi; out[2] = bad ? 1.0 : 0.0;
+        out[0] = lo; out[1] = hi; out[2] = bad ? 1.0 : 0.0; out[3] = badx ? 1.0 : 0.0;
     }
 }
 
@@ -173,12 +177,15 @@ extern "C" int sphg_sum_density_noalloc(const sphg_params* p, int32_t n, const d
     DevCounters* cnt = (DevCounters*)(B + kOffCnt);
     double* hr = (double*)(B + kOffH);
 
-    // smoothing-length range, to size the grid as the other entry points do
-    k_na_hrange<<<1, 1024, 0, s>>>(n, hsml, hr);
-    double hh[3] = {0, 0, 0};
+    // smoothing-length range, to size the grid as the other entry points do,
+    // and the finiteness of the positions (the step's own check,
+    // SPHG_ERR_NONFINITE), before any density kernel runs
+    k_na_hrange<<<1, 1024, 0, s>>>(n, hsml, (const double2*)x, hr);
+    double hh[4] = {0, 0, 0, 0};
     if (cudaMemcpyAsync(hh, hr, sizeof(hh), cudaMemcpyDeviceToHost, s) != cudaSuccess) return SPHG_ERR_CUDA;
     if (cudaStreamSynchronize(s) != cudaSuccess) return SPHG_ERR_CUDA;
     if (hh[2] != 0.0) return SPHG_ERR_BAD_ARG;
+    if (hh[3] != 0.0) return SPHG_ERR_NONFINITE;
     const int sk = (p->skf == 2 || p->skf == 3) ? 3 : 2;
     const double cell = sk * hh[1] * (1.0 + 1e-6);
     const double ncx = std::ceil((p->x_max - p->x_min) / cell) + 1, ncy = std::ceil((p->y_max - p->y_min) / cell) + 1;
@@ -187,7 +194,7 @@ extern "C" int sphg_sum_density_noalloc(const sphg_params* p, int32_t n, const d
     g.ncx = (int)ncx; g.ncy = (int)ncy; g.x0 = p->x_min; g.y0 = p->y_min; g.inv = 1.0 / cell;
     g.kx = 1; g.invx = g.inv;
     const int ncell = g.ncx * g.ncy;
-    SearchConst sc;
+    SearchConst sc{};
     sc.scale_k = sk;
     sc.uniform = hh[0] == hh[1];
     sc.r2_uniform = 0.0;

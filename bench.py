@@ -56,8 +56,14 @@ ALG_BYTES = {
     "soil_pass": 4 + 16 + 8 + 16 + 32 + 4 + 8 + 24 + 16 + 4 + 8 + 8 + 4 + 12 + 4 + 8 + 12 + 4 + 4 + 8 + 8 + CORRECTOR_SOIL,
 }
 # Whole-step algorithmic bytes per particle-step (FP32 pair data, FP64 state):
-# the compulsory state read + write once per step plus the cell key.
+# the compulsory state read + write once per step plus the cell key; water:
+# x 32, v 16, rho 8, drho 8, dv 16, mass 4, type 4, key 8, vof 8, dvof 8;
+# soil: the same without vof/dvof, plus vof 8, stress and p 32, their rates 32.
+# The roofline of the dominant kernel charges its phase's full per-step bytes
+# to it (neighbour re-reads and the per-pass record traffic are not counted).
 STEP_BYTES = {"water": 112, "soil": 168}
+# FP32 peak of the part (148 SMs x 128 FP32 lanes x 2 flops per FMA per clock)
+FP32_LANES_PER_SM = 128
 
 
 def clocks_sampler(stop, out):
@@ -126,8 +132,22 @@ def ncu_traffic():
         return {}
 
 
-SUBDOMAIN = dict(width=1.0, height=1.0, block_w=0.25, block_h=0.1, water_h=0.2)
-SUBDOMAIN_TEXT = "1.0 m x 0.2 m water, 0.25 m x 0.1 m soil block, dx 0.002 m"
+def ncu_flops():
+    """FP32 flops per pair-end of each pass (ncu's executed FADD + FMUL +
+    2 FFMA, over the neighbour pairs each pass evaluated), from
+    profiles/ncu_flops.json."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "ncu_flops.json")) as f:
+            return json.load(f)["fp32_flops_per_pair_end"]
+    except Exception:
+        return {}
+
+
+# A sample of the workload with the same spacing and physics and the same
+# water:soil particle ratio (88.4 : 11.6, virtual particles included):
+# 51,508 water and 6,758 soil particles.
+SUBDOMAIN = dict(width=1.0, height=0.25, block_w=0.21, block_h=0.1, water_h=0.2)
+SUBDOMAIN_TEXT = "1.0 m x 0.2 m water, 0.21 m x 0.1 m soil block, dx 0.002 m, water:soil 88.4:11.6 as the workload"
 
 
 def _oracle_worker(args):
@@ -297,6 +317,7 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=60)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-stepper arm")
+    ap.add_argument("--fp64-steps", type=int, default=20, help="steps of the FP64-mode timing (0: skip)")
     ap.add_argument("--learned-strides", type=int, default=5)
     ap.add_argument("--forchheimer-b", type=float, default=0.0,
                     help="Forchheimer coefficient of the water-soil drag [s^2/m^2] (0: the reference's Darcy law)")
@@ -377,9 +398,15 @@ def main():
     top = max(kern.items(), key=lambda kv: kv[1][1])
     top_name, (top_launches, top_ms) = top[0], top[1]
     avg_ms = top_ms / max(top_launches, 1)
-    units = scene.phases[0].n if top_name in ("water_pass_a", "water_pass_b", "water_sum") \
-        else scene.phases[1].n
-    alg = ALG_BYTES.get(top_name, 0) * units
+
+    def phase_n(name):
+        return scene.phases[1].n if name == "soil_pass" else scene.phases[0].n
+
+    def step_bytes_of(name):   # the per-step bytes of the particles the kernel covers
+        return STEP_BYTES["soil" if name == "soil_pass" else "water"] * phase_n(name)
+
+    units = phase_n(top_name)
+    alg = step_bytes_of(top_name)
     peak, peak_kind = measured_peak_hbm()
     achieved = alg / (avg_ms / 1000.0) / 1e9
     tr = ncu_traffic().get(top_name)
@@ -392,6 +419,11 @@ def main():
     sms = torch.cuda.get_device_properties(local).multi_processor_count
     mhz = (clocks or {}).get("sm_mhz") or 1965.0
     issue_peak = sms * 4 * mhz * 1e6
+    fp32_peak = sms * FP32_LANES_PER_SM * 2 * mhz * 1e6
+    st = solver.stats()
+    pair_ends = {"water_pass_a": 2 * st.niac[0], "water_pass_b": 2 * st.niac[0] + st.niac[2],
+                 "soil_pass": 2 * st.niac[1] + st.niac[2]}
+    fpp = ncu_flops()
 
     def issue(name, ms_launch, particles):
         if name not in ipp:
@@ -399,23 +431,37 @@ def main():
         inst = ipp[name] * particles
         return {"warp_inst_per_launch": inst, "achieved": inst / (ms_launch / 1000.0), "peak": issue_peak,
                 "unit": "warp-inst/s", "frac": inst / (ms_launch / 1000.0) / issue_peak}
+
+    def fp32(name, ms_launch):
+        if name not in fpp or name not in pair_ends:
+            return None
+        fl = fpp[name] * pair_ends[name]
+        return {"flops_per_pair_end": fpp[name], "pair_ends_per_launch": int(pair_ends[name]),
+                "achieved": fl / (ms_launch / 1000.0) / 1e12, "peak": fp32_peak / 1e12, "unit": "TFLOP/s",
+                "frac": fl / (ms_launch / 1000.0) / fp32_peak}
+
+    def launch_ms(k):
+        return kern[k][1] / max(kern[k][0], 1)
+
     roofline = {"bound": "hbm", "kernel": top_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": peak_kind, "traffic": tr,
-                "alg_bytes_per_launch": alg, "avg_launch_ms": avg_ms,
+                "alg_bytes_per_launch": alg,
+                "alg_bytes_basis": "per-step state bytes of the particles the kernel covers: 112 B per water "
+                                   "particle-step, 168 B per soil particle-step",
+                "avg_launch_ms": avg_ms,
                 "issue": issue(top_name, avg_ms, units),
+                "fp32": fp32(top_name, avg_ms),
                 "step": {"alg_bytes": step_bytes, "achieved_gbs": step_bytes / (step_ms / 1000.0) / 1e9,
                          "frac": step_bytes / (step_ms / 1000.0) / 1e9 / peak},
                 "kernels_ms_per_step": {k: v[1] / args.steps for k, v in kern.items()},
-                "passes": {k: {"alg_bytes": ALG_BYTES[k] * (scene.phases[1].n if k == "soil_pass"
-                                                            else scene.phases[0].n),
-                               "avg_ms": kern[k][1] / max(kern[k][0], 1),
-                               "achieved_gbs": ALG_BYTES[k] * (scene.phases[1].n if k == "soil_pass"
-                                                               else scene.phases[0].n)
-                               / (kern[k][1] / max(kern[k][0], 1) / 1000.0) / 1e9,
+                "passes": {k: {"alg_bytes": step_bytes_of(k), "avg_ms": launch_ms(k),
+                               "achieved_gbs": step_bytes_of(k) / (launch_ms(k) / 1000.0) / 1e9,
+                               "frac": step_bytes_of(k) / (launch_ms(k) / 1000.0) / 1e9 / peak,
+                               "per_pass_bytes": ALG_BYTES[k] * phase_n(k),
+                               "per_pass_frac": ALG_BYTES[k] * phase_n(k) / (launch_ms(k) / 1000.0) / 1e9 / peak,
                                "traffic": ncu_traffic().get(k),
-                               "issue": issue(k, kern[k][1] / max(kern[k][0], 1),
-                                              scene.phases[1].n if k == "soil_pass"
-                                              else scene.phases[0].n)}
+                               "issue": issue(k, launch_ms(k), phase_n(k)),
+                               "fp32": fp32(k, launch_ms(k))}
                            for k in ALG_BYTES if k in kern}}
 
     # ---- end to end through the C ABI with pinned host buffers
@@ -473,6 +519,26 @@ def main():
                                      "steps": args.full_state_steps,
                                      "mode": "every step: upload the full state, one step, download the full state"}}
 
+    # ---- the FP64 parity mode on the same scene (every field and sum in double)
+    fp64 = None
+    if args.fp64_steps > 0:
+        from sources_b200.abi import SPHG_FP64
+        s64 = scene.copy()
+        s64.params.precision = SPHG_FP64
+        with Solver(s64) as g64:
+            g64.set_stream(stream.cuda_stream)
+            g64.time_integration(3)
+            torch.cuda.synchronize()
+            f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            f0.record(stream)
+            g64.time_integration(args.fp64_steps)
+            f1.record(stream)
+            torch.cuda.synchronize()
+            ms64 = replicas.max_over_ranks(f0.elapsed_time(f1), dist if world > 1 else None, device="cuda")
+        fp64 = {"value": replicas.weak_scaling_value(world, n, args.fp64_steps, ms64), "unit": UNIT,
+                "ms_per_step": ms64 / args.fp64_steps, "steps": args.fp64_steps, "warmup": 3, "dtype": "f64",
+                "mode": "FP64 parity mode: pair arithmetic, rates and state all in double"}
+
     learned = None
     if not args.no_learned and args.workload == WORKLOAD:
         learned = learned_arm(solver, scene, torch, value / world, args.learned_strides)
@@ -493,11 +559,12 @@ def main():
                 "config": {"workload": args.workload, "particles": n, "water": scene.phases[0].n,
                            "soil": scene.phases[1].n, "dx": 0.002, "precision": "fp32 pairs / fp64 state",
                            "skf": int(scene.params.skf), "parallelism": f"replicas{world}",
+                           "pairs": {"water": int(st.niac[0]), "soil": int(st.niac[1]), "cross": int(st.niac[2])},
                            "drag": ("darcy (the reference's law)" if args.forchheimer_b == 0
                                     else "darcy-forchheimer b=%g s^2/m^2" % args.forchheimer_b),
                            "l2": "inputs larger than L2 (state ~%.0f MB)" % (n * 250 / 1e6)},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-                "clocks": clocks, "learned": learned}
+                "clocks": clocks, "learned": learned, "fp64_mode": fp64}
         print(json.dumps(line))
     return 0
 

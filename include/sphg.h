@@ -278,6 +278,42 @@ int sphg_write_tecplot_phase(const char* path, int append, const sphg_phase_host
 int sphg_write_tecplot(sphg_ctx* ctx, const char* path_first, const char* path_second, int append,
                        const int32_t* zone_first, const int32_t* zone_second);
 
+/* Scene generators: the role of the reference's input_tank.f90 (water
+ * column in a tank), input_soilfail.f90 (soil column in a box) and
+ * input_mix_Savage.f90 (soil block under water), so that a Fortran host
+ * builds its arrays without another layer.  Particles sit on the cell
+ * centres of a dx lattice (block%cell_center, m_particles.f90:460-479, x outer
+ * and y inner), real particles first, then two layers of virtual particles
+ * under the floor and outside both walls (take_real / take_virtual,
+ * m_particles.f90:808-893).  The case-file values the reference reads
+ * (material constants, initial pressure and stress, dt) follow the choices
+ * stated in sphg_scenes.cpp.  Host code only; no GPU needed.
+ *   box_w x box_h   tank, box or domain
+ *   col_w x col_h   water column, soil column, or soil block at the left wall
+ *   water_h         two-phase only: depth of the water layer
+ * sphg_scene_default fills the sizes of the three workloads this library is
+ * measured on.  sphg_scene_size gives each phase's real and virtual particle
+ * counts (n_phase entries each); the host allocates its arrays (x is (2,n))
+ * and calls sphg_make_scene, which zeroes every non-NULL array of the views
+ * and fills x, hsml, itype, p, c, vof, rho, mass (and sxx, sxy, syy for soil,
+ * which are then required), and *p from sphg_default_params plus the scene's
+ * values.  ntotal and nvirt of each view must be the counts of
+ * sphg_scene_size. */
+enum { SPHG_SCENE_DAM_BREAK = 1, SPHG_SCENE_GRANULAR_COLUMN = 2, SPHG_SCENE_TWO_PHASE = 3 };
+typedef struct sphg_scene_spec {
+    int32_t kind, skf, precision, _pad;
+    double dx;
+    double box_w, box_h;
+    double col_w, col_h;
+    double water_h;
+    double phi_deg;                  /* soil friction angle [degrees]               */
+    double porosity, permeability;   /* two-phase: soil porosity, Darcy k [m/s]     */
+    double forchheimer_b;            /* two-phase: sphg_params.forchheimer_b        */
+} sphg_scene_spec;
+void sphg_scene_default(int kind, sphg_scene_spec* s);
+int sphg_scene_size(const sphg_scene_spec* s, int32_t* n_phase, int32_t* ntotal, int32_t* nvirt);
+int sphg_make_scene(const sphg_scene_spec* s, sphg_params* p, sphg_phase_host* first, sphg_phase_host* second);
+
 /* Run the context's work on a caller-owned cudaStream_t (passed as void*);
  * NULL restores the context's own stream. */
 int sphg_set_stream(sphg_ctx* ctx, void* cuda_stream);

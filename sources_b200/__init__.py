@@ -31,8 +31,9 @@ EXPORTS = ("sphg_default_params", "sphg_create", "sphg_upload_phase", "sphg_sing
            "sphg_set_stream", "sphg_kernel_profile", "sphg_kernel_report", "sphg_destroy",
            "sphg_strerror", "sphg_sum_density_noalloc", "sphg_set_scenes", "sphg_upload_scene_ids",
            "sphg_set_tuning", "sphg_read_case", "sphg_write_tecplot_phase", "sphg_write_tecplot",
-           "sphg_gemm_bf16_tn", "sphg_export_xv_device", "sphg_import_xv_device", "sphg_group_create",
-           "sphg_group_time_integration", "sphg_group_destroy", *sorted(_GNN_SIGNATURES := {
+           "sphg_gemm_bf16_tn", "sphg_gemm_wait_probe", "sphg_export_xv_device", "sphg_import_xv_device", "sphg_group_create",
+           "sphg_group_time_integration", "sphg_group_destroy", "sphg_scene_default", "sphg_scene_size",
+           "sphg_make_scene", *sorted(_GNN_SIGNATURES := {
                # message-passing network kernels (include/sphg_learn.h); P pointer,
                # I int, L 64-bit count, F float, D double, S size_t pointer
                "sphg_gemm_bf16_ws": "PPIIIPPP",
@@ -97,6 +98,7 @@ def load(path: str = LIB_PATH):
     L.sphg_upload_scene_ids.argtypes = [P, C.c_int, C.POINTER(C.c_int32)]
     L.sphg_set_tuning.argtypes = [P, C.POINTER(abi.Tuning)]
     L.sphg_gemm_bf16_tn.argtypes = [P, P, P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, P, P]
+    L.sphg_gemm_wait_probe.argtypes = [P, P, C.c_int, C.c_int, C.c_int, C.c_longlong, P, P]
     L.sphg_read_case.argtypes = [C.c_char_p, C.POINTER(Params), C.POINTER(abi.Case)]
     L.sphg_write_tecplot_phase.argtypes = [C.c_char_p, C.c_int, C.POINTER(PhaseHost), C.POINTER(C.c_int32)]
     L.sphg_write_tecplot.argtypes = [P, C.c_char_p, C.c_char_p, C.c_int, C.POINTER(C.c_int32),
@@ -107,6 +109,12 @@ def load(path: str = LIB_PATH):
     L.sphg_group_time_integration.argtypes = [P, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double)]
     L.sphg_group_destroy.argtypes = [P]
     L.sphg_group_destroy.restype = None
+    L.sphg_scene_default.argtypes = [C.c_int, C.POINTER(abi.SceneSpec)]
+    L.sphg_scene_default.restype = None
+    L.sphg_scene_size.argtypes = [C.POINTER(abi.SceneSpec), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                  C.POINTER(C.c_int32)]
+    L.sphg_make_scene.argtypes = [C.POINTER(abi.SceneSpec), C.POINTER(Params), C.POINTER(PhaseHost),
+                                  C.POINTER(PhaseHost)]
     L.sphg_export_xv_device.argtypes = [P, C.c_int, P, P]
     L.sphg_import_xv_device.argtypes = [P, C.c_int, P, P]
     codes = {"P": C.c_void_p, "I": C.c_int, "L": C.c_longlong, "F": C.c_float, "D": C.c_double}
@@ -127,6 +135,34 @@ def read_case(path: str, params: Params | None = None):
     if rc:
         raise SPHError(rc, f"sphg_read_case({path}): {c.bad_values} bad value(s)")
     return p, c
+
+
+def scene_spec(kind: int, **sizes) -> "abi.SceneSpec":
+    """sphg_scene_default of a scene kind (abi.SPHG_SCENE_*), with any field
+    of sphg_scene_spec overridden by keyword."""
+    L = load()
+    s = abi.SceneSpec()
+    L.sphg_scene_default(kind, C.byref(s))
+    for k, v in sizes.items():
+        setattr(s, k, v)
+    return s
+
+
+def make_scene(spec: "abi.SceneSpec"):
+    """A scene built by the library's own generators (sphg_make_scene):
+    (params, [PhaseArrays per phase])."""
+    L = load()
+    nph = C.c_int32()
+    nt, nv = (C.c_int32 * 2)(), (C.c_int32 * 2)()
+    _check(L.sphg_scene_size(C.byref(spec), C.byref(nph), nt, nv), "sphg_scene_size")
+    mats = [SPHG_WATER, SPHG_SOIL] if nph.value == 2 else \
+        [SPHG_WATER if spec.kind == abi.SPHG_SCENE_DAM_BREAK else SPHG_SOIL]
+    phases = [PhaseArrays(nt[k] + nv[k], nt[k], mats[k], spec.dx) for k in range(nph.value)]
+    hosts = [P.host_struct() for P in phases]
+    p = Params()
+    _check(L.sphg_make_scene(C.byref(spec), C.byref(p), C.byref(hosts[0]),
+                             C.byref(hosts[1]) if len(hosts) > 1 else None), "sphg_make_scene")
+    return p, phases
 
 
 def write_tecplot_phase(path: str, P: PhaseArrays, zone=None, append: bool = False):

@@ -100,6 +100,15 @@ class Case(C.Structure):
         ("particle_size", C.c_char * 32), ("operating_mode", C.c_char * 32)]
 
 
+SPHG_SCENE_DAM_BREAK, SPHG_SCENE_GRANULAR_COLUMN, SPHG_SCENE_TWO_PHASE = 1, 2, 3
+
+
+class SceneSpec(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("skf", C.c_int32), ("precision", C.c_int32), ("_pad", C.c_int32)] + [
+        (n, C.c_double) for n in ("dx", "box_w", "box_h", "col_w", "col_h", "water_h", "phi_deg", "porosity",
+                                  "permeability", "forchheimer_b")]
+
+
 class Stats(C.Structure):
     _fields_ = [("niac", C.c_int64 * 3), ("maxiac", C.c_int32 * 2), ("miniac", C.c_int32 * 2),
                 ("noiac", C.c_int32 * 2), ("nfail", C.c_int32), ("n_out_of_domain", C.c_int32),

@@ -15,7 +15,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 SRC = [os.path.join(HERE, "csrc", "sphg_api.cu"), os.path.join(HERE, "csrc", "sphg_noalloc.cu"),
-       os.path.join(HERE, "csrc", "sphg_io.cpp"), os.path.join(HERE, "csrc", "sphg_umma.cu"),
+       os.path.join(HERE, "csrc", "sphg_io.cpp"), os.path.join(HERE, "csrc", "sphg_scenes.cpp"),
+       os.path.join(HERE, "csrc", "sphg_umma.cu"),
        os.path.join(HERE, "csrc", "sphg_gnn.cu")]
 OUT = os.path.join(HERE, "libsphg.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

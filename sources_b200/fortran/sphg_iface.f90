@@ -47,6 +47,14 @@ module sphg_iface
      type(c_ptr) :: itype = c_null_ptr, fail = c_null_ptr
   end type
 
+  ! scene generators (the input_*.f90 routines of the reference)
+  integer(c_int), parameter :: SPHG_SCENE_DAM_BREAK = 1, SPHG_SCENE_GRANULAR_COLUMN = 2, SPHG_SCENE_TWO_PHASE = 3
+  type, bind(C) :: sphg_scene_spec
+     integer(c_int32_t) :: kind, skf, precision, pad
+     real(c_double) :: dx, box_w, box_h, col_w, col_h, water_h, phi_deg
+     real(c_double) :: porosity, permeability, forchheimer_b
+  end type
+
   type, bind(C) :: sphg_stats_t
      integer(c_int64_t) :: niac(3)
      integer(c_int32_t) :: maxiac(2), miniac(2), noiac(2)
@@ -159,6 +167,24 @@ module sphg_iface
        import :: c_ptr
        type(c_ptr), value :: group
      end subroutine
+     ! scene generators: sizes first, then the host allocates its particles
+     ! arrays (x is (2,n)) and points the phase views at them
+     subroutine sphg_scene_default(kind, s) bind(C, name="sphg_scene_default")
+       import :: c_int, sphg_scene_spec
+       integer(c_int), value :: kind
+       type(sphg_scene_spec), intent(out) :: s
+     end subroutine
+     integer(c_int) function sphg_scene_size(s, n_phase, ntotal, nvirt) bind(C, name="sphg_scene_size")
+       import :: c_int, c_int32_t, sphg_scene_spec
+       type(sphg_scene_spec), intent(in) :: s
+       integer(c_int32_t), intent(out) :: n_phase, ntotal(2), nvirt(2)
+     end function
+     integer(c_int) function sphg_make_scene(s, p, first, second) bind(C, name="sphg_make_scene")
+       import :: c_int, sphg_scene_spec, sphg_params, sphg_phase_host
+       type(sphg_scene_spec), intent(in) :: s
+       type(sphg_params), intent(out) :: p
+       type(sphg_phase_host), intent(inout) :: first, second
+     end function
      subroutine sphg_destroy(ctx) bind(C, name="sphg_destroy")
        import :: c_ptr
        type(c_ptr), value :: ctx

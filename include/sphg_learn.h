@@ -49,6 +49,17 @@ typedef struct SphgGemmEpi {
 int sphg_gemm_bf16_ws(const void* A, const void* B, int M, int N, int K, const SphgGemmEpi* epilogue, int* err_dev,
                       void* cuda_stream);
 
+/* Test of the bounded device waits (no counterpart in the reference, whose
+ * only failure path is `stop`): launches sphg_gemm_bf16_tn's kernel on
+ * A (M x K) and B (N x K) so that its first K block issues no MMA and waits
+ * for it with `spins` polls of the mbarrier.  The wait runs out while no MMA
+ * or copy is in flight; the kernel sets *err_dev, frees its TMEM and returns
+ * without writing any output.  The call waits for the stream and returns
+ * SPHG_ERR_TIMEOUT when *err_dev was set.  M % 128 == 0, N % 128 == 0,
+ * K % 64 == 0, spins > 0. */
+int sphg_gemm_wait_probe(const void* A, const void* B, int M, int N, int K, long long spins, int* err_dev,
+                         void* cuda_stream);
+
 /* ---------------------------------------------------------------------
  * Message-passing network kernels.  Feature matrices are row-major bf16 or
  * fp32 with the row count padded to a multiple of 128; L is the latent

@@ -65,7 +65,8 @@ template <int BN>
 __global__ void __launch_bounds__(128, 1) k_gemm_bf16_tn(const __nv_bfloat16* __restrict__ A,
                                                          const __nv_bfloat16* __restrict__ B, float* __restrict__ C,
                                                          int M, int N, int K, int k_per_split, int accumulate,
-                                                         int atomic_out, int* __restrict__ err) {
+                                                         int atomic_out, int* __restrict__ err,
+                                                         long long probe_spins) {
     constexpr int TCOLS = BN < 32 ? 32 : BN;
     constexpr uint32_t A_KC = 128 * 16;     // bytes between K chunks of the A stage
     constexpr uint32_t B_KC = BN * 16;      // bytes between K chunks of the B stage
@@ -99,6 +100,10 @@ __global__ void __launch_bounds__(128, 1) k_gemm_bf16_tn(const __nv_bfloat16* __
     bool ok = true;
     uint32_t parity = 0;
     int issued = 0;
+    // probe_spins > 0 (sphg_gemm_wait_probe): the first K block issues no MMA
+    // and waits for it with that many polls, so the bounded wait runs out
+    // while nothing is in flight and the kernel takes its error exit
+    const bool probe = probe_spins > 0;
     for (int k0 = kbeg; k0 < kend && ok; k0 += 64) {
         // stage A and B in the canonical K-major layout
         for (int c = tid; c < 128 * 8; c += 128) {
@@ -113,7 +118,7 @@ __global__ void __launch_bounds__(128, 1) k_gemm_bf16_tn(const __nv_bfloat16* __
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
-        if (tid == 0) {
+        if (tid == 0 && !probe) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::);
 #pragma unroll
             for (int kk = 0; kk < 4; ++kk) {
@@ -129,8 +134,8 @@ __global__ void __launch_bounds__(128, 1) k_gemm_bf16_tn(const __nv_bfloat16* __
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
                          ::"r"(mbar_a) : "memory");
         }
-        ++issued;
-        const bool done = mbar_wait(mbar_a, parity, kWaitLimit);
+        if (!probe) ++issued;
+        const bool done = mbar_wait(mbar_a, parity, probe ? probe_spins : kWaitLimit);
         parity ^= 1u;
         ok = __syncthreads_and(done ? 1 : 0) != 0;   // block-uniform: every thread leaves the loop together
     }
@@ -160,7 +165,7 @@ __global__ void __launch_bounds__(128, 1) k_gemm_bf16_tn(const __nv_bfloat16* __
         if (tid == 0) atomicExch(err, 1);
         // a bounded second wait for MMAs that may still be in flight
         if (issued > 0) mbar_wait(mbar_a, parity ^ 1u, kWaitLimit);
-    } else if (!accumulate && !atomic_out) {
+    } else if (!accumulate && !atomic_out && !probe) {
         // empty K range: C = 0
         const int row = m0 + warp * 32 + lane;
         for (int c = 0; c < BN; ++c) C[(size_t)row * N + n0 + c] = 0.f;
@@ -173,7 +178,7 @@ __global__ void __launch_bounds__(128, 1) k_gemm_bf16_tn(const __nv_bfloat16* __
 
 template <int BN>
 int launch_gemm(const __nv_bfloat16* A, const __nv_bfloat16* B, float* C, int M, int N, int K, int accumulate,
-                int split, int* err, cudaStream_t s) {
+                int split, int* err, cudaStream_t s, long long probe_spins = 0) {
     const size_t smem = 8 * (128 * 16) + 8 * (BN * 16) + 16 + 16;
     static bool configured = false;
     if (!configured) {
@@ -185,7 +190,8 @@ int launch_gemm(const __nv_bfloat16* A, const __nv_bfloat16* B, float* C, int M,
     const int kblocks = K / 64;
     const int per = (kblocks + split - 1) / split;
     dim3 grid(M / 128, N / BN, split);
-    k_gemm_bf16_tn<BN><<<grid, 128, smem, s>>>(A, B, C, M, N, K, per * 64, accumulate, split > 1 ? 1 : 0, err);
+    k_gemm_bf16_tn<BN><<<grid, 128, smem, s>>>(A, B, C, M, N, K, per * 64, accumulate, split > 1 ? 1 : 0, err,
+                                               probe_spins);
     return cudaGetLastError() == cudaSuccess ? SPHG_OK : SPHG_ERR_CUDA;
 }
 
@@ -602,4 +608,19 @@ extern "C" int sphg_gemm_bf16_tn(const void* A, const void* B, float* C, int M, 
     if (N % 64 == 0) return launch_gemm<64>(a, b, C, M, N, K, accumulate, split_k, err_dev, s);
     if (N % 32 == 0) return launch_gemm<32>(a, b, C, M, N, K, accumulate, split_k, err_dev, s);
     return launch_gemm<16>(a, b, C, M, N, K, accumulate, split_k, err_dev, s);
+}
+
+extern "C" int sphg_gemm_wait_probe(const void* A, const void* B, int M, int N, int K, long long spins, int* err_dev,
+                                    void* stream) {
+    if (!A || !B || !err_dev || spins <= 0) return SPHG_ERR_BAD_ARG;
+    if (M <= 0 || N <= 0 || K <= 0 || M % 128 || N % 128 || K % 64) return SPHG_ERR_BAD_ARG;
+    if ((((uintptr_t)A) | ((uintptr_t)B)) & 15) return SPHG_ERR_BAD_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    int rc = launch_gemm<128>((const __nv_bfloat16*)A, (const __nv_bfloat16*)B, nullptr, M, N, K, 0, 1, err_dev, s,
+                              spins);
+    if (rc) return rc;
+    int h = 0;
+    if (cudaMemcpyAsync(&h, err_dev, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess) return SPHG_ERR_CUDA;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return SPHG_ERR_CUDA;
+    return h ? SPHG_ERR_TIMEOUT : SPHG_OK;
 }

@@ -131,3 +131,31 @@ def test_ws_gemm_rejects_bad_arguments(lib):
     assert lib.sphg_gemm_bf16_ws(one, one, 128, 128, 128, a, one, None) != 0     # STORE without z
     E.mode = 9
     assert lib.sphg_gemm_bf16_ws(one, one, 128, 128, 128, a, one, None) != 0     # unknown epilogue
+
+
+def test_bounded_wait_runs_out_and_frees_tmem(cuda_ok, lib):
+    """A device wait that gives up: sphg_gemm_wait_probe launches the GEMM
+    kernel so that its first mbarrier wait has nothing to wait for and runs
+    out after 2,000 polls, before any MMA or copy is in flight.  The call
+    returns SPHG_ERR_TIMEOUT with the error flag set; the kernel freed its
+    TMEM, so ordinary GEMMs on the same SMs afterwards allocate TMEM again and
+    give the right product (twice, around a second probe)."""
+    import torch
+    from sources_b200.abi import SPHG_ERR_TIMEOUT
+    M, N, K = 128 * 296, 128, 128      # two CTAs per SM on every SM
+    g = torch.Generator(device="cuda").manual_seed(7)
+    A = torch.randn(M, K, device="cuda", generator=g).to(torch.bfloat16)
+    B = torch.randn(N, K, device="cuda", generator=g).to(torch.bfloat16)
+    ref = A.float() @ B.float().T
+    stream = torch.cuda.current_stream().cuda_stream
+    for _ in range(2):
+        err = torch.zeros(1, dtype=torch.int32, device="cuda")
+        rc = lib.sphg_gemm_wait_probe(A.data_ptr(), B.data_ptr(), M, N, K, 2000, err.data_ptr(), stream)
+        assert rc == SPHG_ERR_TIMEOUT and int(err.item()) == 1
+        err.zero_()
+        C = torch.zeros(M, N, device="cuda")
+        assert lib.sphg_gemm_bf16_tn(A.data_ptr(), B.data_ptr(), C.data_ptr(), M, N, K, 0, 1, err.data_ptr(),
+                                     stream) == 0
+        torch.cuda.synchronize()
+        assert int(err.item()) == 0
+        assert float((C - ref).abs().max()) <= 1e-4 * float(ref.abs().max()) * (K / 64) ** 0.5

@@ -146,6 +146,19 @@ def ncu_flops():
 # A sample of the workload with the same spacing and physics and the same
 # water:soil particle ratio (88.4 : 11.6, virtual particles included):
 # 51,508 water and 6,758 soil particles.
+def workload_config(workload: str, forchheimer_b: float, world: int) -> dict:
+    """The `config` of both arms' JSON lines (the same dict for the same run)."""
+    sizes = {WORKLOAD: (912016, 806008, 106008), "two_phase_456k": (508016, 404008, 104008)}
+    if workload not in sizes:
+        return {"workload": workload, "parallelism": f"replicas{world}"}
+    n, nw, ns = sizes[workload]
+    return {"workload": workload, "particles": n, "water": nw, "soil": ns, "dx": 0.002, "skf": 1,
+            "parallelism": f"replicas{world}",
+            "drag": ("darcy (the reference's law)" if forchheimer_b == 0
+                     else "darcy-forchheimer b=%g s^2/m^2" % forchheimer_b),
+            "l2": "inputs larger than L2 (state ~%.0f MB)" % (n * 250 / 1e6)}
+
+
 SUBDOMAIN = dict(width=1.0, height=0.25, block_w=0.21, block_h=0.1, water_h=0.2)
 SUBDOMAIN_TEXT = "1.0 m x 0.2 m water, 0.21 m x 0.1 m soil block, dx 0.002 m, water:soil 88.4:11.6 as the workload"
 
@@ -228,8 +241,8 @@ def run_reference(args, rank, world):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * dt / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (deterministic lattice scene)",
-            "config": {"workload": WORKLOAD, "particles": 912016, "sample_particles": n, "instances": cores,
-                       "precision": "fp64 (reference)", "l2": "state larger than L2"},
+            "config": workload_config(args.workload, args.forchheimer_b, world),
+            "precision": "fp64 (the reference's arithmetic)",
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -556,13 +569,9 @@ def main():
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (deterministic lattice scene, no dataset)",
-                "config": {"workload": args.workload, "particles": n, "water": scene.phases[0].n,
-                           "soil": scene.phases[1].n, "dx": 0.002, "precision": "fp32 pairs / fp64 state",
-                           "skf": int(scene.params.skf), "parallelism": f"replicas{world}",
-                           "pairs": {"water": int(st.niac[0]), "soil": int(st.niac[1]), "cross": int(st.niac[2])},
-                           "drag": ("darcy (the reference's law)" if args.forchheimer_b == 0
-                                    else "darcy-forchheimer b=%g s^2/m^2" % args.forchheimer_b),
-                           "l2": "inputs larger than L2 (state ~%.0f MB)" % (n * 250 / 1e6)},
+                "config": workload_config(args.workload, args.forchheimer_b, world),
+                "precision": "fp32 pairs / fp64 state",
+                "pairs": {"water": int(st.niac[0]), "soil": int(st.niac[1]), "cross": int(st.niac[2])},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
                 "clocks": clocks, "learned": learned, "fp64_mode": fp64}
         print(json.dumps(line))

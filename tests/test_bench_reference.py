@@ -17,7 +17,9 @@ def test_reference_arm_prints_its_line():
     line = json.loads(out.stdout.strip().splitlines()[-1])
     assert line["impl"] == "reference" and line["value"] > 0 and line["steps"] == 2
     assert line["unit"] == "particle-steps/s" and line["higher_is_better"] is True
-    assert line["cpu_baseline"]["cores"] == 2 == line["config"]["instances"]
+    assert line["cpu_baseline"]["cores"] == 2
+    # the same config as the arm on the GPU
+    assert line["config"]["workload"] == "two_phase_912k" and line["config"]["particles"] == 912016
     assert line["cpu_baseline"]["kind"] == "port"
     assert line["e2e"] == {"value": line["value"], "unit": line["unit"], "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}

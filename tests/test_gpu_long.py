@@ -26,7 +26,7 @@ import pytest
 
 from oracle import Oracle
 from sources_b200 import Solver, scenes
-from sources_b200.abi import SPHG_FP32, SPHG_FP64
+from sources_b200.abi import SPHG_FP32, SPHG_FP64, SPHG_PAIRS_FIRST
 
 pytestmark = pytest.mark.gpu
 
@@ -116,28 +116,39 @@ def test_leapfrog_across_renormalisation_steps(cuda_ok, steps):
     compare(ga, [o.download(k + 1) for k in range(2)], {f: 1e-7 for f in STATE}, steps)
 
 
-# dam-break, 2,000 FP64 steps: field-scale error against the oracle
-DAM_BREAK_2000 = {"x": 1e-9, "vx": 1e-7, "rho": 1e-9, "p": 1e-7, "drho": 1e-5, "dvx": 1e-6}
+# dam-break, 2,000 steps: field-scale error against the FP64 oracle (a B200
+# gave x 7.7e-15, vx 2.1e-13, rho 2.9e-14, p 5.6e-13, drho 2.7e-12, dvx 3.4e-13
+# in FP64 mode; x 2.9e-7, vx 9.6e-6, rho 1.3e-6, p 6.1e-5, drho 3.2e-4,
+# dvx 3.5e-5 in FP32 mode)
+DAM_BREAK_2000 = {SPHG_FP64: {"x": 1e-13, "vx": 2e-12, "rho": 3e-13, "p": 5e-12, "drho": 3e-11, "dvx": 3e-12},
+                  SPHG_FP32: {"x": 2e-6, "vx": 1e-4, "rho": 1e-5, "p": 5e-4, "drho": 3e-3, "dvx": 3e-4}}
 
 
-def test_dam_break_full_run_fp64(cuda_ok):
-    """The dam-break workload (4,008 particles) for its full 2,000 steps in
-    FP64 against the oracle; the pair set at the end is bit-exact."""
-    s = scenes.dam_break(precision=SPHG_FP64)
-    o = Oracle(s)
+@pytest.fixture(scope="module")
+def dam_break_oracle_2000():
+    o = Oracle(scenes.dam_break(precision=SPHG_FP64))
     assert o.time_integration(2000) == 0
+    return o.download(1)
+
+
+@pytest.mark.parametrize("precision", [SPHG_FP64, SPHG_FP32])
+def test_dam_break_full_run(cuda_ok, dam_break_oracle_2000, precision):
+    """The dam-break workload (4,008 particles) for its full 2,000 steps,
+    FP64 and FP32 modes, against the FP64 oracle; the pair set of the final
+    positions is bit-exact."""
+    s = scenes.dam_break(precision=precision)
     with Solver(s) as g:
         g.time_integration(2000)
         assert g.itimestep == 2000
         a = g.download(1)
-        gi, gj = g.pairs(1)
-    compare([a], [o.download(1)], DAM_BREAK_2000, "dam_break 2000")
+        gi, gj = g.pairs(SPHG_PAIRS_FIRST)
+    compare([a], [dam_break_oracle_2000], DAM_BREAK_2000[precision], ("dam_break 2000", precision))
     # the pair set of the final positions, as the oracle finds it from the GPU's positions
     s2 = s.copy()
     s2.phases = [a]
     o2 = Oracle(s2)
     assert o2.single_step(1) == 0
-    oi, oj = o2.pairs(1)
+    oi, oj = o2.pairs(SPHG_PAIRS_FIRST)
     assert np.array_equal(gi, oi) and np.array_equal(gj, oj)
 
 
@@ -149,9 +160,45 @@ def granular_oracle_20000():
     return o.download(1), o.time
 
 
-# granular column, 20,000 steps: FP64 and FP32 modes against the FP64 oracle
-GRANULAR_20000_FP64 = {"x": 1e-7, "vx": 1e-4, "rho": 1e-7, "p": 1e-4, "sxx": 1e-4, "sxy": 1e-4, "syy": 1e-4}
-GRANULAR_20000_FP32 = {"x": 1e-5, "vx": 1e-2, "rho": 1e-5, "p": 1e-2, "sxx": 1e-2, "sxy": 1e-2, "syy": 1e-2}
+# granular column, 20,000 steps against the FP64 oracle.  FP64 mode: a B200
+# gave x 6.2e-12, vx 7.3e-10, rho 5.1e-11, p 5.1e-10, sxx 3.6e-9, sxy 5.7e-10,
+# syy 4.1e-9 and identical fail flags.
+GRANULAR_20000_FP64 = {"x": 1e-10, "vx": 1e-8, "rho": 1e-9, "p": 1e-8, "sxx": 5e-8, "sxy": 1e-8, "syy": 5e-8}
+# FP32 mode: the reference flags a soil point as plastic when |J - alpha1 I1| <
+# 1e-5 Pa (plastic_or_not, m_particles.f90:3447-3505), finer than the FP32
+# rounding of the stress rates (~1e-4 Pa at these stresses), so the set of
+# flagged points, and with it flow rule 3, departs from FP64 and the collapse
+# takes a slightly different path: a B200 gave field-scale max / RMS errors of
+# x 7.3e-3 / 2.8e-4 (a few particles up to 3.7 dx, 0.14 dx RMS), vx 0.20 /
+# 8.1e-3, rho 4.3e-2 / 1.3e-3, p 0.40 / 1.0e-2, with 1,021 fail flags of 5,000
+# different.  The test holds the RMS errors and the shape of the deposit: the
+# runout and the free surface within 1 dx of the oracle's.
+GRANULAR_20000_FP32_RMS = {"x": 1e-3, "vx": 3e-2, "rho": 5e-3, "p": 3e-2, "sxx": 1e-1, "sxy": 3e-2, "syy": 1e-1}
+
+
+def rms_err(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    return float(np.sqrt(np.mean((a - b) ** 2)) / np.abs(b).max())
+
+
+def deposit(P, dx):
+    """Runout (furthest real particle from the left wall) and the height of
+    the highest real particle in each 2 dx bin along x."""
+    x = P.x[:P.ntotal]
+    runout = float(x[:, 0].max())
+    bins = np.floor(x[:, 0] / (2 * dx)).astype(int)
+    top = np.full(bins.max() + 1, np.nan)
+    np.fmax.at(top, bins, x[:, 1])
+    return runout, top
+
+
+@pytest.fixture(scope="module")
+def granular_oracle_20000():
+    s = scenes.granular_column(precision=SPHG_FP64)
+    o = Oracle(s)
+    assert o.time_integration(20000) == 0
+    return o.download(1), o.time
 
 
 @pytest.mark.parametrize("precision", [SPHG_FP64, SPHG_FP32])
@@ -159,12 +206,25 @@ def test_granular_column_full_run(cuda_ok, granular_oracle_20000, precision):
     """The dry granular column (6,608 particles) for its full 20,000 steps,
     FP64 and FP32 modes, against the FP64 oracle."""
     ref, t = granular_oracle_20000
-    with Solver(scenes.granular_column(precision=precision)) as g:
+    s = scenes.granular_column(precision=precision)
+    with Solver(s) as g:
         g.time_integration(20000)
         assert g.itimestep == 20000 and abs(g.time - t) <= 1e-12 * t
         a = g.download(1)
-    budget = GRANULAR_20000_FP64 if precision == SPHG_FP64 else GRANULAR_20000_FP32
-    compare([a], [ref], budget, ("granular 20000", precision))
+    if precision == SPHG_FP64:
+        compare([a], [ref], GRANULAR_20000_FP64, ("granular 20000", precision))
+        assert np.array_equal(a.fail, ref.fail)
+        return
+    for f, tol in GRANULAR_20000_FP32_RMS.items():
+        assert np.all(np.isfinite(getattr(a, f))), f
+        e = rms_err(getattr(a, f), getattr(ref, f))
+        assert e <= tol, (f, e, tol)
+    dx = float(s.phases[0].dspp)
+    ra, ta = deposit(a, dx)
+    rb, tb = deposit(ref, dx)
+    assert abs(ra - rb) <= dx, (ra, rb)
+    both = np.isfinite(ta[:len(tb)]) & np.isfinite(tb[:len(ta)])
+    assert np.nanmean(np.abs(ta[:len(tb)][both] - tb[:len(ta)][both])) <= dx
 
 
 FULL_1_FP64 = {f: 1e-9 for f in STATE}
@@ -189,9 +249,14 @@ def test_full_size_two_phase_one_step_against_oracle(cuda_ok):
             assert np.array_equal(a[1].fail, ref[1].fail)
 
 
-FULL_500_FP64 = {"x": 1e-9, "vx": 1e-5, "rho": 1e-8, "p": 1e-6, "vof": 1e-8, "sxx": 1e-5, "sxy": 1e-5,
-                 "syy": 1e-5, "drho": 1e-4, "dvx": 1e-5}
-FULL_500_FP32 = {"x": 5e-9, "vx": 1e-4, "rho": 5e-7, "p": 5e-4, "vof": 5e-7, "sxx": 2e-3, "sxy": 2e-4,
+# 500 steps at 912,016 particles, every 128th particle.  FP64 mode: a B200
+# gave at most x 1.1e-16, vx 1.0e-12, rho 3.5e-15, p 2.4e-13, vof 3.3e-15,
+# stress 2.5e-13, drho 9.5e-13, dvx 1.3e-13.  FP32 mode (whole fields, from
+# the full oracle state): x 7.8e-10, vx 4.5e-5, rho 1.6e-7, p 9.8e-5,
+# vof 1.5e-7, sxx 4.3e-4, sxy 4.5e-5, syy 4.2e-4, drho 1.3e-4, dvx 2.0e-5.
+FULL_500_FP64 = {"x": 1e-14, "vx": 1e-11, "rho": 1e-13, "p": 3e-12, "vof": 1e-13, "sxx": 3e-12, "sxy": 3e-12,
+                 "syy": 3e-12, "drho": 1e-11, "dvx": 2e-12}
+FULL_500_FP32 = {"x": 5e-9, "vx": 2e-4, "rho": 1e-6, "p": 5e-4, "vof": 1e-6, "sxx": 2e-3, "sxy": 3e-4,
                  "syy": 2e-3, "drho": 1e-3, "dvx": 1e-4}
 
 

@@ -49,6 +49,23 @@ typedef struct SphgGemmEpi {
 int sphg_gemm_bf16_ws(const void* A, const void* B, int M, int N, int K, const SphgGemmEpi* epilogue, int* err_dev,
                       void* cuda_stream);
 
+/* One message-passing edge layer in one kernel (inference; no counterpart in
+ * the reference):
+ *   a    = bf16(relu(E We^T + be + P[src[r], :128] + P[dst[r], 128:256]))   (gather for rows r < nedge)
+ *   EF   = EF + a W2^T + b2         (fp32, in place)
+ *   Eout = bf16(EF)
+ * the same results, bit for bit, as sphg_gemm_bf16_ws with the EDGE epilogue
+ * (h = a) followed by the RESID epilogue on a, without writing a.  E and Eout
+ * are [M x 128] bf16 and may be the same array (each 128-row tile of E is
+ * read before the same tile of Eout is written), EF [M x 128] fp32,
+ * P [nodes x 256] fp32,
+ * We and W2 [128 x 128] bf16, be and b2 [128] fp32; M % 128 == 0, 0 <=
+ * nedge <= M, 16-byte aligned arrays.  A device wait that gives up sets
+ * *err_dev to 1. */
+int sphg_gnn_edge_layer(const void* E, float* EF, void* E_out, const float* P, const int* src, const int* dst,
+                        long long nedge, int M, const void* We, const float* be, const void* W2, const float* b2,
+                        int* err_dev, void* cuda_stream);
+
 /* Test of the bounded device waits (no counterpart in the reference, whose
  * only failure path is `stop`): launches sphg_gemm_bf16_tn's kernel on
  * A (M x K) and B (N x K) so that its first K block issues no MMA and waits

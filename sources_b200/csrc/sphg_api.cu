@@ -73,7 +73,7 @@ struct EngineBase {
     virtual int graph_kind(int itimestep) = 0;
     virtual int prepare_graph_step() = 0;
     virtual int capture_step(int itimestep) = 0;
-    virtual void after_graph_step(long long launches) = 0;
+    virtual void after_graph_step(long long launches, int kind) = 0;
     virtual long long graph_epoch() const = 0;
 };
 
@@ -123,11 +123,12 @@ struct Engine : EngineBase {
     size_t cub_bytes = 0;
     DevCounters* cnt = nullptr;     // device
     DevCounters hcnt{};             // host copy
-    int* sticky = nullptr;          // device: [overflow, nonfinite]
+    int* sticky = nullptr;          // device: [overflow, nonfinite, staging timeout]
     double* stage = nullptr;        // transfer staging, 2*nmax doubles
     int* stage_i = nullptr;
     long long* stage_l = nullptr;
-    std::vector<void*> shadow[2];   // one reorder target per persistent field
+    std::vector<void*> shadow[2];   // the second buffer of every persistent field
+    int par[2] = {0, 0};            // per phase: flipped whenever fields and shadows swap
     int nmax = 0;
     double hrange[2][2] = {{0, 0}, {0, 0}};
     // per-scene parameters (entry 0 = the context's own parameters)
@@ -165,13 +166,18 @@ struct Engine : EngineBase {
     // ---------------------------------------------------------------- launch
     template <typename K, typename... A>
     int launch(const char* name, K kern, int grid_, int block, A... args) {
+        return launch_smem(name, kern, grid_, block, 0, args...);
+    }
+    // with `smem` bytes of dynamic shared memory (the neighbour staging space)
+    template <typename K, typename... A>
+    int launch_smem(const char* name, K kern, int grid_, int block, size_t smem, A... args) {
         if (grid_ <= 0) return 0;
         cudaEvent_t a = nullptr, b = nullptr;
         if (ctx->prof.on) {
             a = ctx->prof.get(); b = ctx->prof.get();
             cudaEventRecord(a, ctx->stream);
         }
-        kern<<<grid_, block, 0, ctx->stream>>>(args...);
+        kern<<<grid_, block, smem, ctx->stream>>>(args...);
         ctx->prof.launches++;
         counters_fresh = false;
         cudaError_t e = cudaGetLastError();
@@ -291,10 +297,11 @@ struct Engine : EngineBase {
         void* old[] = {D.x, D.v, D.v_min, D.rho, D.rho_min, D.vof, D.vof_min, D.p, D.c, D.mass, D.hsml, D.sxx, D.sxy,
                        D.syy, D.sxx_min, D.sxy_min, D.syy_min, D.p_min, D.eps_p, D.itype, D.orig, D.fail, D.sid, D.drho,
                        D.dvof, D.dsxx, D.dsxy, D.dsyy, D.dp, D.txx, D.txy, D.tyy, D.vcc, D.wxy, D.vof2, D.dv, D.av,
-                       D.countiac, D.cell_id, D.cell_fill, D.perm, D.xs, D.hs, D.recA, D.recA2, D.recB};
+                       D.countiac, D.cell_id, D.cell_fill, D.perm, D.xs, D.hs, D.recA, D.recA2, D.recB, D.hmask};
         for (void* p : old) release(p);
         for (void* p : shadow[ph]) release(p);
         shadow[ph].clear();
+        par[ph] = 0;
         memset(&D, 0, sizeof(D));
         D.n = n;
         size_t N = (size_t)n;
@@ -312,7 +319,7 @@ struct Engine : EngineBase {
         rc |= alloc(&D.dv, N); rc |= alloc(&D.av, N);
         rc |= alloc(&D.countiac, N); rc |= alloc(&D.cell_id, N); rc |= alloc(&D.cell_fill, N); rc |= alloc(&D.perm, N);
         rc |= alloc(&D.xs, N); rc |= alloc(&D.hs, N);
-        rc |= alloc(&D.recA, N); rc |= alloc(&D.recA2, N); rc |= alloc(&D.recB, N);
+        rc |= alloc(&D.recA, N); rc |= alloc(&D.recA2, N); rc |= alloc(&D.recB, N); rc |= alloc(&D.hmask, N);
         if (rc) return SPHG_ERR_CUDA;
         for (auto& f : field_refs(ph)) {
             char* q = nullptr;
@@ -496,6 +503,13 @@ struct Engine : EngineBase {
         double K = sk * hmax;
         sc_same.scale_k = sk; sc_same.uniform = uniform; sc_same.r2_uniform = uniform ? exact_threshold(K) : 0.0;
         sc_cross = sc_same;
+        switch (p.skf) {
+            case 1: rc0 = stage_attrs<1>(); break;
+            case 2: rc0 = stage_attrs<2>(); break;
+            case 3: rc0 = stage_attrs<3>(); break;
+            default: rc0 = stage_attrs<4>(); break;
+        }
+        if (rc0) return rc0;
         prepared = true;
         // spatial order from the start
         for (int ph = 0; ph < ctx->nphase; ++ph) {
@@ -538,8 +552,18 @@ struct Engine : EngineBase {
         return f;
     }
 
+    // Swap every persistent field of a phase with its shadow buffer.
+    void swap_buffers(int ph) {
+        auto refs = field_refs(ph);
+        for (size_t i = 0; i < refs.size() && i < shadow[ph].size(); ++i) std::swap(*refs[i].first, shadow[ph][i]);
+        par[ph] ^= 1;
+    }
+
     // Permute every persistent field into the current cell order in one launch
-    // (each into its shadow buffer), then swap fields and shadows.
+    // (each into its shadow buffer), then swap fields and shadows: the later
+    // launches of the step read the new buffers.  Every field thus lives in
+    // one of two fixed buffers, and a captured step graph is kept per
+    // combination of the phases' buffer sets (graph_index).
     int reorder(int ph) {
         PhaseDev<T>& D = P[ph];
         auto refs = field_refs(ph);
@@ -554,8 +578,30 @@ struct Engine : EngineBase {
         }
         int rc = launch("reorder", k_permute_all, blocks(D.n, 256), 256, D.n, (const int*)D.perm, L);
         if (rc) return rc;
-        if ((rc = launch("reorder", k_copy_back_all, blocks(D.n, 256), 256, D.n, L))) return rc;
+        swap_buffers(ph);
         return launch("iota", k_iota, blocks(D.n, 256), 256, D.n, D.perm);
+    }
+
+    // Dynamic shared memory of the two-phase water_pass_b: its neighbour
+    // staging space, which afterwards holds the cross pairs' hit buffer.
+    static size_t stage_b_bytes() {
+        const size_t b = (size_t)SPHG_STAGE_B * (16 + sizeof(RecA<T>) + sizeof(RecB<T>));
+        const size_t hb = sizeof(HitBuf<T, SPHG_TPB, Chunk<T>::value>);
+        return b > hb ? b : hb;
+    }
+    // Launches above 48 KB of dynamic shared memory must be allowed per kernel
+    // (outside any stream capture: prepare() runs before every capture).
+    template <int SKF>
+    int stage_attrs() {
+        const int b = (int)stage_b_bytes();
+        if (b > 48 * 1024) {
+            CUDA_TRY(cudaFuncSetAttribute(k_water_pass_b<T, SKF, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+            CUDA_TRY(cudaFuncSetAttribute(k_water_pass_b<T, SKF, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+        }
+        const int a = (int)((size_t)SPHG_STAGE_A * (16 + sizeof(RecA<T>)));
+        if (a > 48 * 1024)
+            CUDA_TRY(cudaFuncSetAttribute(k_water_pass_a<T, SKF, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, a));
+        return 0;
     }
 
     // -------------------------------------------------------------- the step
@@ -591,7 +637,9 @@ struct Engine : EngineBase {
             StepCtl us = u; us.with_vof = 1; us.do_dp = dp;
             // the soil's gather was launched by run() on the side stream
             if ((rc = launch("gather", k_gather<T>, blocks(W.n, 256), 256, W, sim, 0, 0, fh, 1, 0, cnt))) return rc;
-            if ((rc = launch("water_pass_a", k_water_pass_a<T, SKF, false>, blocks(W.n, tpb), tpb, W, grid, sc_same, sim, cnt))) return rc;
+            if ((rc = launch_smem("water_pass_a", k_water_pass_a<T, SKF, false>, blocks(W.n, tpb), tpb,
+                                  (size_t)SPHG_STAGE_A * (16 + sizeof(RecA<T>)), W, grid, sc_same, sim, cnt)))
+                return rc;
             // The cross pairs run inside the last pass of each phase; the soil
             // pass reads the water pressure that water_pass_a sets.  After
             // water_pass_a the two last passes share no data: each reads the
@@ -621,10 +669,10 @@ struct Engine : EngineBase {
                 if (e2 != cudaSuccess && rc == 0) rc = SPHG_ERR_CUDA;
             }
             if (rc == 0)
-                rc = fch ? launch("water_pass_b", k_water_pass_b<T, SKF, false, true>, blocks(W.n, tpb), tpb, W, S, grid,
-                                  sc_same, sc_cross, sim, uw, cnt)
-                         : launch("water_pass_b", k_water_pass_b<T, SKF, false, false>, blocks(W.n, tpb), tpb, W, S, grid,
-                                  sc_same, sc_cross, sim, uw, cnt);
+                rc = fch ? launch_smem("water_pass_b", k_water_pass_b<T, SKF, false, true>, blocks(W.n, tpb), tpb,
+                                       stage_b_bytes(), W, S, grid, sc_same, sc_cross, sim, uw, cnt)
+                         : launch_smem("water_pass_b", k_water_pass_b<T, SKF, false, false>, blocks(W.n, tpb), tpb,
+                                       stage_b_bytes(), W, S, grid, sc_same, sc_cross, sim, uw, cnt);
             // join in every case, so that a capture in progress ends joined
             cudaError_t ew = ej != cudaSuccess ? ej
                              : side != main_stream ? cudaStreamWaitEvent(main_stream, ctx->ev_join, 0) : cudaSuccess;
@@ -638,11 +686,12 @@ struct Engine : EngineBase {
         return 0;
     }
 
-    // One captured CUDA graph per kind of regular step (itimestep >= 2):
-    // bit 0 = reorder step, bit 1 = renormalisation step.  Every buffer keeps
-    // its address for the life of a phase, so a graph stays valid until the
-    // next upload.
-    cudaGraphExec_t graphs[4] = {nullptr, nullptr, nullptr, nullptr};
+    // One captured CUDA graph per kind of regular step (itimestep >= 2) and
+    // buffer set: bit 0 = reorder step, bit 1 = renormalisation step, bits 2
+    // and 3 = each phase's buffer set (par).  Buffers are allocated once per
+    // phase, so a graph stays valid until the next upload of another size.
+    static constexpr int NGRAPH = 16;
+    cudaGraphExec_t graphs[NGRAPH] = {};
     bool use_graphs = true;
 
     long long epoch = 0;    // counts drop_graphs(): joint graphs of older epochs are stale
@@ -651,20 +700,35 @@ struct Engine : EngineBase {
         ++epoch;
     }
 
+    int graph_index(int itimestep) const { return step_kind(itimestep) | par[0] << 2 | par[1] << 3; }
     int graph_kind(int itimestep) override {
         if (itimestep < 2 || !use_graphs || ctx->prof.on) return -1;
-        return step_kind(itimestep);
+        return graph_index(itimestep);
     }
     int prepare_graph_step() override { return prepare(); }
+    // Record the step into the stream being captured.  The host's buffer
+    // sets are left as before the step: they change when the graph is
+    // launched (after_graph_step).
     int capture_step(int itimestep) override {
         StepCtl u{};
         u.update = 1;
-        return run(itimestep, 1, u);
+        const int p0 = par[0], p1 = par[1];
+        int rc = run(itimestep, 1, u);
+        if (par[0] != p0) swap_buffers(0);
+        if (par[1] != p1) swap_buffers(1);
+        return rc;
     }
-    void after_graph_step(long long launches) override {
+    // After a launch of the graph of `kind` (a graph_index): a reorder step
+    // has swapped every phase's buffers.
+    void launched_step(int kind) {
+        if (kind & 1)
+            for (int ph = 0; ph < ctx->nphase; ++ph) swap_buffers(ph);
+    }
+    void after_graph_step(long long launches, int kind) override {
         nfail_slot = 3;
         if (!ctx->prm.single_phase) aliased = true;
         ctx->prof.launches += launches;
+        launched_step(kind);
     }
     long long graph_epoch() const override { return epoch; }
 
@@ -678,9 +742,9 @@ struct Engine : EngineBase {
     // needed.  If capture is not possible, graphs are switched off and the
     // caller launches the step directly.
     int step_graphed(int itimestep) {
-        const int kind = step_kind(itimestep);
         int rc = prepare();
         if (rc) return rc;
+        const int kind = graph_index(itimestep);
         if (!graphs[kind]) {
             cudaGraph_t g = nullptr;
             const long long before = ctx->prof.launches;
@@ -689,9 +753,7 @@ struct Engine : EngineBase {
                 use_graphs = false;
                 return 0;
             }
-            StepCtl u{};
-            u.update = 1;
-            rc = run(itimestep, 1, u);
+            rc = capture_step(itimestep);
             cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
             if (rc || e != cudaSuccess || !g) {
                 if (g) cudaGraphDestroy(g);
@@ -709,9 +771,10 @@ struct Engine : EngineBase {
         if (!ctx->prm.single_phase) aliased = true;
         CUDA_TRY(cudaGraphLaunch(graphs[kind], ctx->stream));
         ctx->prof.launches += launches_per_graph[kind];
+        launched_step(kind);
         return 0;
     }
-    long long launches_per_graph[4] = {0, 0, 0, 0};
+    long long launches_per_graph[NGRAPH] = {};
 
     int run(int itimestep, int fh, StepCtl u) {
         int rc = prepare();
@@ -796,7 +859,7 @@ struct Engine : EngineBase {
         CUDA_TRY(cudaMemcpyAsync(&hcnt, cnt, sizeof(hcnt), cudaMemcpyDeviceToHost, ctx->stream));
         CUDA_TRY(cudaMemcpyAsync(hs, sticky, sizeof(hs), cudaMemcpyDeviceToHost, ctx->stream));
         CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-        batch_rc = hs[1] ? SPHG_ERR_NONFINITE : hs[0] ? SPHG_ERR_PAIR_OVERFLOW : 0;
+        batch_rc = hs[2] ? SPHG_ERR_TIMEOUT : hs[1] ? SPHG_ERR_NONFINITE : hs[0] ? SPHG_ERR_PAIR_OVERFLOW : 0;
         counters_fresh = true;
         return batch_rc;
     }
@@ -1132,7 +1195,7 @@ struct sphg_group {
         cudaGraphExec_t exec = nullptr;
         std::vector<long long> launches, epochs;
     };
-    std::map<unsigned long long, Joint> joint;
+    std::map<std::vector<int>, Joint> joint;   // by the contexts' graph kinds
     std::vector<cudaEvent_t> ev;   // 0: fork; 1..n-1: joins
     bool use_graphs = true;
     ~sphg_group() {
@@ -1192,12 +1255,11 @@ int group_capture(sphg_group* g, int ts, sphg_group::Joint& J) {
 // replay one, else each context's own step in turn.
 int group_step(sphg_group* g, int ts) {
     const int n = (int)g->ctx.size();
-    unsigned long long key = 0;
+    std::vector<int> key(n, -1);
     bool graphed = g->use_graphs;
     for (int i = 0; i < n && graphed; ++i) {
-        const int k = g->ctx[i]->eng->graph_kind(ts);
-        if (k < 0) graphed = false;
-        key |= (unsigned long long)k << (2 * i);
+        key[i] = g->ctx[i]->eng->graph_kind(ts);
+        if (key[i] < 0) graphed = false;
     }
     if (graphed) {
         for (int i = 0; i < n; ++i) {
@@ -1223,7 +1285,7 @@ int group_step(sphg_group* g, int ts) {
         }
         if (g->use_graphs) {
             CUDA_TRY(cudaGraphLaunch(it->second.exec, g->ctx[0]->stream));
-            for (int i = 0; i < n; ++i) g->ctx[i]->eng->after_graph_step(it->second.launches[i]);
+            for (int i = 0; i < n; ++i) g->ctx[i]->eng->after_graph_step(it->second.launches[i], key[i]);
             return 0;
         }
     }

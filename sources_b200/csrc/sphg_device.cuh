@@ -73,6 +73,7 @@ struct DevCounters {
     int n_out;                       // particles clamped into edge cells
     int nonfinite;                   // NaN/Inf positions met
     int overflow;                    // a pair list exceeded max_interaction
+    int timeout;                     // blocks whose bounded staging wait ran out
 };
 
 template <typename T>
@@ -95,6 +96,11 @@ struct PhaseDev {
     double *hs;
     RecA<T> *recA, *recA2;
     RecB<T> *recB;
+    // sorted order: which of the particle's candidates passed the pair test in
+    // the first same-phase pass of the step (bit t = candidate t of the three
+    // row runs; bit 127 alone = more than 127 candidates, not recorded).  The
+    // later same-phase passes of the step replay it instead of testing again.
+    uint4* hmask;
 };
 
 // ---------------------------------------------------------------------------
@@ -222,6 +228,24 @@ __device__ __forceinline__ int dp_return(double& p, double& sxx, double& sxy, do
     return 0;
 }
 
+// x/y pairs of the pair terms.  In FP32 they use Blackwell's packed pair
+// arithmetic (fma/mul/add.rn.f32x2: one instruction for both components,
+// each rounded as the scalar operation); in FP64 they are two scalar
+// operations.  fma2(a, b, c) = a*b + c with one rounding, as the compiler
+// contracts the scalar `c += a*b`.
+__device__ __forceinline__ float2 splat2(float v) { return make_float2(v, v); }
+__device__ __forceinline__ double2 splat2(double v) { return make_double2(v, v); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ double2 mul2(double2 a, double2 b) { return make_double2(a.x * b.x, a.y * b.y); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ double2 add2(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(make_float2(-1.0f, -1.0f), b, a); }
+__device__ __forceinline__ double2 sub2(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ double2 fma2(double2 a, double2 b, double2 c) {
+    return make_double2(fma(a.x, b.x, c.x), fma(a.y, b.y, c.y));
+}
+
 template <typename T>
 __device__ __forceinline__ T warp_sum(T v) {
 #pragma unroll
@@ -328,30 +352,62 @@ struct KernelConst {
 #define SPHG_SCAN_U 4
 #endif
 
-template <typename T, int TPB, int CH>
+template <typename T, int TPB, int CH, typename I = int>
 struct HitBuf {
-    int m[CH * TPB];
+    I m[CH * TPB];
 };
 
-template <typename T, int TPB, int CH, class F>
-__device__ __forceinline__ int visit_batched(HitBuf<T, TPB, CH>& buf, const GridGeom& g, const SearchConst& sc,
-                                             const int* __restrict__ cstart, const double2* __restrict__ xs,
-                                             const double* __restrict__ hs, double2 xa, double ha, int self,
-                                             bool active, F&& body) {
-    const unsigned FULL = 0xffffffffu;
-    const int tid = threadIdx.x;
-    int b0 = 0, b1 = 0, b2 = 0, L0 = 0, L1 = 0, L2 = 0;
+// A particle's candidates: the three row runs of the cell-sorted list around
+// its cell (rows cy-1, cy, cy+1; cells cx-kx .. cx+kx), numbered 0 .. tot-1
+// in that order.
+struct CandRuns {
+    int b0, b1, b2, L0, L1, L2;
+    __device__ __forceinline__ int total() const { return L0 + L1 + L2; }
+    // sorted index of candidate t
+    __device__ __forceinline__ int at(int t) const {
+        return t < L0 ? b0 + t : (t < L0 + L1 ? b1 + (t - L0) : b2 + (t - L0 - L1));
+    }
+};
+
+__device__ __forceinline__ CandRuns candidate_runs(const GridGeom& g, const int* __restrict__ cstart, double2 xa,
+                                                   bool active) {
+    CandRuns r{0, 0, 0, 0, 0, 0};
     if (active) {
         int cx, cy; bool clamped;
         cell_coords(g, xa.x, xa.y, cx, cy, clamped);
         const int x0 = cx > g.kx ? cx - g.kx : 0;
         const int x1 = cx < g.ncx - 1 - g.kx ? cx + g.kx : g.ncx - 1;
-        if (cy - 1 >= 0) { b0 = __ldg(cstart + (cy - 1) * g.ncx + x0); L0 = __ldg(cstart + (cy - 1) * g.ncx + x1 + 1) - b0; }
-        b1 = __ldg(cstart + cy * g.ncx + x0); L1 = __ldg(cstart + cy * g.ncx + x1 + 1) - b1;
-        if (cy + 1 < g.ncy) { b2 = __ldg(cstart + (cy + 1) * g.ncx + x0); L2 = __ldg(cstart + (cy + 1) * g.ncx + x1 + 1) - b2; }
+        if (cy - 1 >= 0) { r.b0 = __ldg(cstart + (cy - 1) * g.ncx + x0); r.L0 = __ldg(cstart + (cy - 1) * g.ncx + x1 + 1) - r.b0; }
+        r.b1 = __ldg(cstart + cy * g.ncx + x0); r.L1 = __ldg(cstart + cy * g.ncx + x1 + 1) - r.b1;
+        if (cy + 1 < g.ncy) { r.b2 = __ldg(cstart + (cy + 1) * g.ncx + x0); r.L2 = __ldg(cstart + (cy + 1) * g.ncx + x1 + 1) - r.b2; }
     }
-    const int tot = L0 + L1 + L2;
-    constexpr int U = SPHG_SCAN_U;   // candidates per lane per iteration: independent loads and FP64 chains in flight
+    return r;
+}
+
+// Hit mask of the candidates (CandRuns numbering) that passed the pair test;
+// bit 127 alone marks a particle with more than 127 candidates.
+constexpr int SPHG_MASK_BITS = 127;
+__device__ __forceinline__ bool mask_overflow(uint4 m) { return m.w == 0x80000000u && !(m.x | m.y | m.z); }
+
+// Every particle of a sorted list that passes the reference's pair test
+// against (xa, ha) (m_particles.f90:966-973, 1027-1034), evaluated
+// bit-exactly: unfused double products and sum, IEEE sqrt (or its exact
+// squared threshold when every h is equal).  `self` (a sorted index) is
+// skipped.  Each lane tests its own candidates, U at a time, and keeps the
+// hits in its column of `buf`; whenever a lane's column is full, or every
+// lane is done, the warp drains its columns through `body(m, dx, dy)` (dx =
+// xa - x_m) together, so the pair body runs at full SIMT width.  The visiting
+// order is candidate order.  With REC the hits are also returned as a mask.
+template <bool REC, int U = SPHG_SCAN_U, typename T, int TPB, int CH, typename I, class F>
+__device__ __forceinline__ int scan_runs(HitBuf<T, TPB, CH, I>& buf, const SearchConst& sc, const CandRuns& cr,
+                                         const double2* __restrict__ xs, const double* __restrict__ hs, double2 xa,
+                                         double ha, int self, uint4& mask, F&& body) {
+    const unsigned FULL = 0xffffffffu;
+    const int tid = threadIdx.x;
+    const int b0 = cr.b0, b1 = cr.b1, b2 = cr.b2, L0 = cr.L0, L1 = cr.L1;
+    const int tot = cr.total();
+    unsigned long long mlo = 0ull, mhi = 0ull;
+    // U: candidates per lane per iteration (independent loads and FP64 chains in flight)
     int t = 0, cnt = 0, hits = 0;
     bool more = true;
     while (more) {
@@ -384,9 +440,14 @@ __device__ __forceinline__ int visit_batched(HitBuf<T, TPB, CH>& buf, const Grid
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 if (hitu[u]) {
-                    buf.m[cnt * TPB + tid] = mm[u];
+                    buf.m[cnt * TPB + tid] = (I)mm[u];
                     ++cnt;
                     ++hits;
+                    if (REC) {
+                        const int tt = t + u;
+                        if (tt < 64) mlo |= 1ull << tt;
+                        else mhi |= 1ull << (tt & 63);
+                    }
                 }
             }
             t = t + U < tot ? t + U : tot;
@@ -400,5 +461,241 @@ __device__ __forceinline__ int visit_batched(HitBuf<T, TPB, CH>& buf, const Grid
         }
         cnt = 0;
     }
+    if (REC) {
+        if (tot > SPHG_MASK_BITS) { mlo = 0ull; mhi = 1ull << 63; }
+        mask = make_uint4((unsigned)mlo, (unsigned)(mlo >> 32), (unsigned)mhi, (unsigned)(mhi >> 32));
+    }
     return hits;
+}
+
+template <typename T, int TPB, int CH, class F>
+__device__ __forceinline__ int visit_batched(HitBuf<T, TPB, CH>& buf, const GridGeom& g, const SearchConst& sc,
+                                             const int* __restrict__ cstart, const double2* __restrict__ xs,
+                                             const double* __restrict__ hs, double2 xa, double ha, int self,
+                                             bool active, F&& body) {
+    uint4 unused;
+    return scan_runs<false>(buf, sc, candidate_runs(g, cstart, xa, active), xs, hs, xa, ha, self, unused, body);
+}
+
+// visit_batched that also returns the hit mask (CandRuns numbering).
+template <typename T, int TPB, int CH, class F>
+__device__ __forceinline__ int visit_batched_rec(HitBuf<T, TPB, CH>& buf, const GridGeom& g, const SearchConst& sc,
+                                                 const int* __restrict__ cstart, const double2* __restrict__ xs,
+                                                 const double* __restrict__ hs, double2 xa, double ha, int self,
+                                                 bool active, uint4& mask, F&& body) {
+    return scan_runs<true>(buf, sc, candidate_runs(g, cstart, xa, active), xs, hs, xa, ha, self, mask, body);
+}
+
+// The same visit without the hit buffer: each lane tests its candidates one
+// at a time and runs the body on each hit at once (lanes diverge).  For the
+// rare particles and blocks the batched forms do not cover.
+template <bool REC, typename T, class F>
+__device__ __forceinline__ int scan_direct(const SearchConst& sc, const CandRuns& cr, const double2* __restrict__ xs,
+                                           const double* __restrict__ hs, double2 xa, double ha, int self,
+                                           uint4& mask, F&& body) {
+    unsigned long long mlo = 0ull, mhi = 0ull;
+    int hits = 0;
+    const int tot = cr.total();
+    for (int t = 0; t < tot; ++t) {
+        const int m = cr.at(t);
+        if (m == self) continue;
+        const double2 xb = xs[m];
+        const double dx = xa.x - xb.x, dy = xa.y - xb.y;
+        const double r2 = __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));
+        const bool hit = sc.uniform ? (r2 < sc.r2_uniform) : (__dsqrt_rn(r2) < sc.scale_k * ((ha + hs[m]) / 2.0));
+        if (hit) {
+            ++hits;
+            if (REC) {
+                if (t < 64) mlo |= 1ull << t;
+                else mhi |= 1ull << (t & 63);
+            }
+            body(m, (T)dx, (T)dy);
+        }
+    }
+    if (REC) {
+        if (tot > SPHG_MASK_BITS) { mlo = 0ull; mhi = 1ull << 63; }
+        mask = make_uint4((unsigned)mlo, (unsigned)(mlo >> 32), (unsigned)mhi, (unsigned)(mhi >> 32));
+    }
+    return hits;
+}
+
+// The same visit replayed from the hit mask an earlier pass of this step
+// recorded over the same sorted positions: the same neighbours in the same
+// order, so every sum is bit-identical, without testing any candidate again.
+// Each lane walks its own set bits.  A lane whose candidates did not fit the
+// mask (more than 127, three times the count of an uncompressed lattice)
+// tests them again, one at a time, in the same order.
+template <typename T, class F>
+__device__ __forceinline__ int replay_runs(const SearchConst& sc, const CandRuns& cr, const double2* __restrict__ xs,
+                                           const double* __restrict__ hs, double2 xa, double ha, int self,
+                                           bool active, uint4 mask, F&& body) {
+    const unsigned FULL = 0xffffffffu;
+    if (active && mask_overflow(mask)) {
+        uint4 unused;
+        return scan_direct<false, T>(sc, cr, xs, hs, xa, ha, self, unused, body);
+    }
+    unsigned long long lo = active ? ((unsigned long long)mask.y << 32 | mask.x) : 0ull;
+    unsigned long long hi = active ? ((unsigned long long)mask.w << 32 | mask.z) : 0ull;
+    const int hits = __popcll(lo) + __popcll(hi);
+    while (__any_sync(FULL, (lo | hi) != 0ull)) {
+        if (lo | hi) {
+            int t;
+            if (lo) { t = __ffsll((long long)lo) - 1; lo &= lo - 1; }
+            else { t = 63 + __ffsll((long long)hi); hi &= hi - 1; }
+            const int m = cr.at(t);
+            const double2 xb = xs[m];
+            body(m, (T)(xa.x - xb.x), (T)(xa.y - xb.y));
+        }
+    }
+    return hits;
+}
+
+template <typename T, class F>
+__device__ __forceinline__ int visit_masked(const GridGeom& g, const SearchConst& sc,
+                                            const int* __restrict__ cstart, const double2* __restrict__ xs,
+                                            const double* __restrict__ hs, double2 xa, double ha, int self,
+                                            bool active, uint4 mask, F&& body) {
+    return replay_runs<T>(sc, candidate_runs(g, cstart, xa, active), xs, hs, xa, ha, self, active, mask, body);
+}
+
+// ---------------------------------------------------------------------------
+// Shared-memory staging of a block's neighbour candidates.
+//
+// A block's particles are consecutive in the cell-sorted list: they lie in
+// one row of cells, or at the end of one row and the start of a later one.
+// For each such row part p (row row[p], cells xlo[p] .. xhi[p]) the
+// candidates of all its particles lie in three runs of the sorted list: rows
+// row[p]-1 .. row[p]+1, cells xlo[p]-kx .. xhi[p]+kx.  Those (at most six)
+// runs of each per-neighbour array are copied into shared memory by the
+// bulk-copy engine (cp.async.bulk, every copy completing on one mbarrier),
+// and the pass reads its neighbours from there.  A block whose runs exceed
+// the staging space, whose particles span three non-empty rows, or whose h
+// are not all equal reads from global memory instead.
+struct StageHdr {
+    unsigned long long bar;
+    int staged, total, bad;
+    int row[2], xlo[2], xhi[2];
+    int gbeg[6], len[6], soff[6];
+};
+
+template <int NB>
+struct StageArrays {
+    const void* src[NB];   // global, sorted order
+    void* dst[NB];         // shared, room for `cap` elements each
+    int esize[NB];         // bytes per element, a multiple of 16
+};
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar)) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait_parity(unsigned long long* bar, unsigned parity) {
+    unsigned done;
+    asm volatile("{\n\t.reg .pred P1;\n\t"
+                 "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+                 "selp.b32 %0, 1, 0, P1;\n\t}"
+                 : "=r"(done) : "r"(smem_addr(bar)), "r"(parity) : "memory");
+    return done != 0;
+}
+
+// Bounded wait on the staging barrier: on running out the block sets the
+// timeout counter and waits once more (bounded) for its copies in flight.
+constexpr long long SPHG_STAGE_WAIT = 1LL << 22;
+__device__ __forceinline__ void stage_wait(StageHdr& H, int* timeout) {
+    long long i = 0;
+    while (!mbar_try_wait_parity(&H.bar, 0)) {
+        if (++i == SPHG_STAGE_WAIT) {
+            if (threadIdx.x == 0) atomicAdd(timeout, 1);
+            for (long long j = 0; j < SPHG_STAGE_WAIT && !mbar_try_wait_parity(&H.bar, 0); ++j) {}
+            return;
+        }
+    }
+}
+
+// Whole block.  (cx, cy): the thread's particle's cell (valid particles).
+// Returns true (block-uniform) when the candidates are in shared memory.
+template <int TPB, int NB>
+__device__ __forceinline__ bool stage_block(StageHdr& H, const StageArrays<NB>& A, const GridGeom& g,
+                                            const int* __restrict__ cstart, const double2* __restrict__ xs, int n,
+                                            int cap, bool uniform, int cx, int cy, bool valid, int* timeout) {
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        const int k0 = blockIdx.x * TPB;
+        const int k1 = (k0 + TPB < n ? k0 + TPB : n) - 1;
+        const double2 p0 = xs[k0], p1 = xs[k1];
+        int c0x, c0y, c1x, c1y;
+        bool cl;
+        cell_coords(g, p0.x, p0.y, c0x, c0y, cl);
+        cell_coords(g, p1.x, p1.y, c1x, c1y, cl);
+        H.row[0] = c0y; H.row[1] = c1y;
+        H.xlo[0] = c0x; H.xhi[0] = c0x; H.xlo[1] = c1x; H.xhi[1] = c1x;
+        H.bad = uniform ? 0 : 1;
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&H.bar)) : "memory");
+    }
+    __syncthreads();
+    if (valid) {
+        if (cy == H.row[0]) atomicMax(&H.xhi[0], cx);
+        else if (cy == H.row[1]) atomicMin(&H.xlo[1], cx);
+        else H.bad = 1;
+    }
+    __syncthreads();
+    if (tid < 6) {
+        const int p = tid / 3, y = H.row[p] + tid % 3 - 1;
+        int gb = 0, len = 0;
+        if ((p == 0 || H.row[1] != H.row[0]) && y >= 0 && y < g.ncy) {
+            const int xl = H.xlo[p] - g.kx > 0 ? H.xlo[p] - g.kx : 0;
+            const int xh = H.xhi[p] + g.kx < g.ncx - 1 ? H.xhi[p] + g.kx : g.ncx - 1;
+            gb = cstart[y * g.ncx + xl];
+            len = cstart[y * g.ncx + xh + 1] - gb;
+        }
+        H.gbeg[tid] = gb;
+        H.len[tid] = len;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        int off = 0;
+        for (int j = 0; j < 6; ++j) { H.soff[j] = off; off += H.len[j]; }
+        H.total = off;
+        const int st = !H.bad && off <= cap;
+        H.staged = st;
+        if (st) {
+            unsigned bytes = 0;
+            for (int i = 0; i < NB; ++i) bytes += (unsigned)off * (unsigned)A.esize[i];
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(&H.bar)), "r"(bytes)
+                         : "memory");
+            for (int j = 0; j < 6; ++j) {
+                if (H.len[j] <= 0) continue;
+                for (int i = 0; i < NB; ++i)
+                    bulk_copy_g2s((char*)A.dst[i] + (size_t)H.soff[j] * A.esize[i],
+                                  (const char*)A.src[i] + (size_t)H.gbeg[j] * A.esize[i],
+                                  (unsigned)H.len[j] * (unsigned)A.esize[i], &H.bar);
+            }
+        }
+    }
+    __syncthreads();
+    if (!H.staged) return false;
+    stage_wait(H, timeout);
+    return true;
+}
+
+// Room for staged records: the launch's dynamic shared memory over the bytes
+// one staged neighbour takes (0 when launched without dynamic shared memory).
+__device__ __forceinline__ int stage_capacity(int bytes_per_record) {
+    unsigned dyn;
+    asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
+    return (int)(dyn / (unsigned)bytes_per_record);
+}
+
+// A particle's candidate runs as indices into the staged arrays, and its own
+// staged index.  cy: the particle's row.
+__device__ __forceinline__ CandRuns staged_runs(const StageHdr& H, CandRuns r, int cy, int k, int& self_s) {
+    const int j = cy == H.row[0] ? 0 : 3;
+    r.b0 = H.soff[j] + (r.b0 - H.gbeg[j]);
+    r.b1 = H.soff[j + 1] + (r.b1 - H.gbeg[j + 1]);
+    r.b2 = H.soff[j + 2] + (r.b2 - H.gbeg[j + 2]);
+    self_s = H.soff[j + 1] + (k - H.gbeg[j + 1]);
+    return r;
 }

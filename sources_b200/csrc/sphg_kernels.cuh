@@ -57,6 +57,22 @@ struct SimConst {
 #ifndef SPHG_MINB_B
 #define SPHG_MINB_B 6
 #endif
+// neighbours of one block of the two-phase water_pass_a staged in shared
+// memory (records; the sizes of 128 consecutive particles' candidate runs at
+// dx = 0.002 m: mean 414, largest 544)
+#ifndef SPHG_STAGE_A
+#define SPHG_STAGE_A 576
+#endif
+// the same for the two-phase water_pass_b (positions and both records; 0:
+// no staging)
+#ifndef SPHG_STAGE_B
+#define SPHG_STAGE_B 560
+#endif
+// candidates per lane per scan iteration in the staged pass (shared-memory
+// loads need less latency hiding than global ones)
+#ifndef SPHG_SCAN_U_STAGED
+#define SPHG_SCAN_U_STAGED 2
+#endif
 #ifndef SPHG_MINB_SOIL
 #define SPHG_MINB_SOIL 1
 #endif
@@ -307,7 +323,8 @@ __global__ void __launch_bounds__(SPHG_TPB) k_water_sum(PhaseDev<T> P, GridGeom 
     T num = w0 * ma;
     T sx = T(0), sy = T(0);
     const RecA<T>* __restrict__ rec = P.recA;
-    const int hits = visit_batched(hb, g, sc, P.cell_start, P.xs, P.hs, xa, ha, k, valid, [&](int m, T dx, T dy) {
+    uint4 mask;
+    const int hits = visit_batched_rec(hb, g, sc, P.cell_start, P.xs, P.hs, xa, ha, k, valid, mask, [&](int m, T dx, T dy) {
         const RecA<T> rb = rec[m];
         T w, sr, r2, mh;
         pair_kernel<T, SKF>(ka, sc, ha, P.hs, m, dx, dy, w, sr, r2, mh);
@@ -326,6 +343,7 @@ __global__ void __launch_bounds__(SPHG_TPB) k_water_sum(PhaseDev<T> P, GridGeom 
         r2.vx = ra.vx; r2.vy = ra.vy; r2.vol = (T)(P.mass[a] / (double)rho); r2.rho = rho;
         P.recA2[k] = r2;
         P.countiac[a] = hits;
+        if (P.hmask) P.hmask[k] = mask;
     }
     count_stats(cnt, 0, 0, hits, valid);
 }
@@ -340,7 +358,6 @@ __global__ void __launch_bounds__(SPHG_TPB) k_water_sum(PhaseDev<T> P, GridGeom 
 // since grad W = s dx.
 template <typename T, int SKF, bool SINGLE>
 __global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_A : 1) k_water_pass_a(PhaseDev<T> P, GridGeom g, SearchConst sc, SimConst c, DevCounters* cnt) {
-    SPHG_HITBUF(T);
     const int k = gtid();
     const bool valid = k < P.n;
     const int kk = valid ? k : 0;
@@ -355,8 +372,10 @@ __global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_A : 1) k_
     KernelConst<T, SKF> ka;
     ka.init((T)ha);
     T con = 0, dl = 0, t0 = 0, t1 = 0, t2 = 0, t3 = 0;
-    const int hits = visit_batched(hb, g, sc, P.cell_start, P.xs, P.hs, xa, ha, k, valid, [&](int m, T dx, T dy) {
-        const RecA<T> rb = rec[m];
+    uint4 mask = make_uint4(0u, 0u, 0u, 0u);
+    if (SINGLE && valid) mask = P.hmask[k];   // recorded by k_water_sum
+    auto body = [&](const RecA<T>* R, int m, T dx, T dy) {
+        const RecA<T> rb = R[m];
         T w, sr, r2, mh;
         pair_kernel<T, SKF>(ka, sc, ha, P.hs, m, dx, dy, w, sr, r2, mh);
         const T gx = sr * dx, gy = sr * dy;
@@ -374,7 +393,37 @@ __global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_A : 1) k_
             t1 += rb.vol * (du * gy + dv * gx);
             t2 += rb.vol * (c23 * (T(2) * dv * gy - du * gx));
         }
-    });
+    };
+    int hits;
+    if constexpr (SINGLE) {
+        hits = visit_masked<T>(g, sc, P.cell_start, P.xs, P.hs, xa, ha, k, valid, mask,
+                               [&](int m, T dx, T dy) { body(rec, m, dx, dy); });
+    } else {
+        // neighbours staged in shared memory when they fit (positions and records)
+        extern __shared__ __align__(128) unsigned char stage_mem[];
+        __shared__ StageHdr H;
+        __shared__ HitBuf<T, SPHG_TPB, Chunk<T>::value, unsigned short> hb16;   // staged indices
+        const int cap = stage_capacity(16 + (int)sizeof(RecA<T>));
+        int cx, cy;
+        bool cl;
+        cell_coords(g, xa.x, xa.y, cx, cy, cl);
+        const CandRuns cr = candidate_runs(g, P.cell_start, xa, valid);
+        StageArrays<2> A;
+        A.src[0] = P.xs; A.dst[0] = stage_mem; A.esize[0] = 16;
+        A.src[1] = rec; A.dst[1] = stage_mem + (size_t)cap * 16; A.esize[1] = (int)sizeof(RecA<T>);
+        if (cap > 0 && stage_block<SPHG_TPB, 2>(H, A, g, P.cell_start, P.xs, P.n, cap, sc.uniform, cx, cy, valid,
+                                                 &cnt->timeout)) {
+            int self_s;
+            const CandRuns sr = staged_runs(H, cr, cy, k, self_s);
+            const double2* sxs = (const double2*)stage_mem;
+            const RecA<T>* sA = (const RecA<T>*)(stage_mem + (size_t)cap * 16);
+            hits = scan_runs<true, SPHG_SCAN_U_STAGED>(hb16, sc, sr, sxs, P.hs, xa, ha, self_s, mask,
+                                   [&](int m, T dx, T dy) { body(sA, m, dx, dy); });
+        } else {   // rare: the block's runs do not fit
+            hits = scan_direct<true, T>(sc, cr, P.xs, P.hs, xa, ha, k, mask,
+                                        [&](int m, T dx, T dy) { body(rec, m, dx, dy); });
+        }
+    }
     if (valid) {
         T txx, txy, tyy, drho;
         double p, cnew, vof;
@@ -409,6 +458,7 @@ __global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_A : 1) k_
         rb.itype = (T)P.itype[a]; rb.aux = T(0);
         P.recB[k] = rb;
         P.countiac[a] = hits;
+        if (!SINGLE) P.hmask[k] = mask;
     }
     if (!SINGLE) count_stats(cnt, 0, 0, hits, valid);
 }
@@ -487,7 +537,7 @@ template <typename T, int SKF, bool SINGLE, bool FCH>
 __global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_B : 1) k_water_pass_b(PhaseDev<T> P, PhaseDev<T> S, GridGeom g, SearchConst sc,
                                                           SearchConst scx, SimConst c, StepCtl u, DevCounters* cnt) {
     typedef typename V2<T>::t T2;
-    SPHG_HITBUF(T);
+    extern __shared__ __align__(128) unsigned char stage_mem[];
     const int k = gtid();
     const bool valid = k < P.n;
     const int kk = valid ? k : 0;
@@ -508,34 +558,42 @@ __global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_B : 1) k_
     const bool visc = c.visc_artificial, xsph = c.average_velocity;
     KernelConst<T, SKF> ka;
     ka.init((T)ha);
-    T d1x = 0, d1y = 0, d2x = 0, d3x = 0, d2y = 0, d3y = 0;
-    T avx = 0, avy = 0, rpx = 0, rpy = 0, dvf = 0, xsx = 0, xsy = 0;
-    visit_batched(hb, g, sc, P.cell_start, P.xs, P.hs, xa, ha, k, valid, [&](int m, T dx, T dy) {
-        const RecA<T> rb = rec[m];
-        const RecB<T> qb = P.recB[m];
+    // x/y pairs: d1 = sum vb (pa+pb) gradW; d2 = sum vb (sxx, sxy) dW/dx;
+    // d3 = sum vb (sxy, syy) dW/dy; av, rp, xv as art_visc, repulsive_force, av_vel
+    T2 d1 = splat2(T(0)), d2 = splat2(T(0)), d3 = splat2(T(0)), av = splat2(T(0)), rp = splat2(T(0)), xv = splat2(T(0));
+    T dvf = 0;
+    T2 fa_a, fa_b, va;
+    fa_a.x = fa_xx; fa_a.y = fa_xy; fa_b.x = fa_xy; fa_b.y = fa_yy;
+    va.x = ra.vx; va.y = ra.vy;
+    const uint4 mask = valid ? P.hmask[k] : make_uint4(0u, 0u, 0u, 0u);   // recorded by the step's first water pass
+    auto body = [&](const RecA<T>* RA, const RecB<T>* RB, int m, T dx, T dy) {
+        const RecA<T> rb = RA[m];
+        const RecB<T> qb = RB[m];
         T w, sr, rr, mh;
         pair_kernel<T, SKF>(ka, sc, ha, P.hs, m, dx, dy, w, sr, rr, mh);
-        const T gx = sr * dx, gy = sr * dy;
+        T2 d, vb2;
+        d.x = dx; d.y = dy;
+        vb2.x = rb.vx; vb2.y = rb.vy;
+        const T2 gr = mul2(splat2(sr), d);                       // (gx, gy)
         const T vb = rb.vol;
         const T pp = qa.p + qb.p;
-        d1x += vb * (pp * gx);
-        d1y += vb * (pp * gy);
-        const T sxx = fa_xx + qb.vof * qb.sxx, sxy = fa_xy + qb.vof * qb.sxy, syy = fa_yy + qb.vof * qb.syy;
-        d2x += vb * (sxx * gx);
-        d3x += vb * (sxy * gy);
-        d2y += vb * (sxy * gx);
-        d3y += vb * (syy * gy);
-        const T dvx = ra.vx - rb.vx, dvy = ra.vy - rb.vy;
+        d1 = fma2(splat2(vb), mul2(splat2(pp), gr), d1);
+        T2 sb_a, sb_b;                                           // (sxx, sxy), (sxy, syy) of the neighbour
+        sb_a.x = qb.sxx; sb_a.y = qb.sxy; sb_b.x = qb.sxy; sb_b.y = qb.syy;
+        const T2 s_a = fma2(splat2(qb.vof), sb_a, fa_a);          // phi_a s_a + phi_b s_b
+        const T2 s_b = fma2(splat2(qb.vof), sb_b, fa_b);
+        d2 = fma2(splat2(vb), mul2(s_a, splat2(gr.x)), d2);
+        d3 = fma2(splat2(vb), mul2(s_b, splat2(gr.y)), d3);
+        const T2 dv = sub2(va, vb2);                              // v_a - v_b
         const T mb = vb * rb.rho;
         if (visc) {
-            const T vr = dvx * dx + dvy * dy;
+            const T vr = dv.x * dx + dv.y * dy;
             if (vr < T(0)) {
                 const T muv = div_<T>(mh * vr, rr + mh * mh * etq2);
                 const T mc = T(0.5) * (qa.c + qb.c);
                 const T mrho = T(0.5) * (ra.rho + rb.rho);
                 const T piv = div_<T>((beta * muv - alpha * mc) * muv, mrho);
-                avx -= mb * (piv * gx);
-                avy -= mb * (piv * gy);
+                av = fma2(splat2(-mb), mul2(splat2(piv), gr), av);
             }
         }
         if (do_dvof) dvf += pref * vb * ((phia - qb.vof) * (T(2) * sr));
@@ -543,16 +601,46 @@ __global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_B : 1) k_
             const T r = sqrt(rr);
             if (!(r > r0)) {
                 const T f = (pow(r0 / r, p1) - pow(r0 / r, p2)) / (r * r);
-                rpx += dd * dx * f;
-                rpy += dd * dy * f;
+                rp = fma2(mul2(splat2(dd), d), splat2(f), rp);
             }
         }
         if (xsph) {
             const T q = div_<T>(mb * w, (ra.rho + rb.rho) / T(2));
-            xsx -= q * dvx;
-            xsy -= q * dvy;
+            xv = fma2(splat2(-q), dv, xv);
         }
-    });
+    };
+    if constexpr (SINGLE) {
+        visit_masked<T>(g, sc, P.cell_start, P.xs, P.hs, xa, ha, k, valid, mask,
+                        [&](int m, T dx, T dy) { body(rec, P.recB, m, dx, dy); });
+    } else {
+        // neighbours staged in shared memory when they fit (positions and both records)
+        __shared__ StageHdr H;
+        const int cap = SPHG_STAGE_B > 0 ? stage_capacity(16 + (int)sizeof(RecA<T>) + (int)sizeof(RecB<T>)) : 0;
+        int cx, cy;
+        bool cl;
+        cell_coords(g, xa.x, xa.y, cx, cy, cl);
+        const CandRuns cr = candidate_runs(g, P.cell_start, xa, valid);
+        StageArrays<3> A;
+        A.src[0] = P.xs; A.dst[0] = stage_mem; A.esize[0] = 16;
+        A.src[1] = rec; A.dst[1] = stage_mem + (size_t)cap * 16; A.esize[1] = (int)sizeof(RecA<T>);
+        A.src[2] = P.recB; A.dst[2] = stage_mem + (size_t)cap * (16 + sizeof(RecA<T>)); A.esize[2] = (int)sizeof(RecB<T>);
+        if (cap > 0 && stage_block<SPHG_TPB, 3>(H, A, g, P.cell_start, P.xs, P.n, cap, sc.uniform, cx, cy, valid,
+                                                 &cnt->timeout)) {
+            int self_s;
+            const CandRuns sr = staged_runs(H, cr, cy, k, self_s);
+            const double2* sxs = (const double2*)A.dst[0];
+            const RecA<T>* sA = (const RecA<T>*)A.dst[1];
+            const RecB<T>* sB = (const RecB<T>*)A.dst[2];
+            replay_runs<T>(sc, sr, sxs, P.hs, xa, ha, self_s, valid, mask,
+                           [&](int m, T dx, T dy) { body(sA, sB, m, dx, dy); });
+        } else {
+            replay_runs<T>(sc, cr, P.xs, P.hs, xa, ha, k, valid, mask,
+                           [&](int m, T dx, T dy) { body(rec, P.recB, m, dx, dy); });
+        }
+        __syncthreads();   // the staging space becomes the cross pairs' hit buffer
+    }
+    const T d1x = d1.x, d1y = d1.y, d2x = d2.x, d2y = d2.y, d3x = d3.x, d3y = d3.y;
+    const T avx = av.x, avy = av.y, rpx = rp.x, rpy = rp.y, xsx = xv.x, xsy = xv.y;
     T dvx = -(phia * d1x) + d2x + d3x;
     T dvy = -(phia * d1y) + d2y + d3y;
     if (ra.rho > T(0)) { dvx = dvx / ra.rho; dvy = dvy / ra.rho; }
@@ -570,6 +658,8 @@ __global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_B : 1) k_
             if (u.update) update_one(P, a, c, u.first, 0, 0);   // last pass of the water-only step
         }
     } else {
+        // the launch gives at least sizeof(HitBuf) of dynamic shared memory (SPHG_STAGE_B)
+        auto& hb = *reinterpret_cast<HitBuf<T, SPHG_TPB, Chunk<T>::value>*>(stage_mem);
         T cdx = 0, cdy = 0, cdvof = 0, cv2 = 0;
         const int chits = cross_water_sums<T, SKF, FCH>(hb, S, g, scx, c, ka, xa, ha, ra, valid, cdx, cdy, cdvof, cv2);
         if (valid) {
@@ -791,6 +881,7 @@ static __global__ void k_check(const DevCounters* __restrict__ c, int* __restric
     if (threadIdx.x == 0 && blockIdx.x == 0) {
         if (c->pairs[0] / 2 > cap || c->pairs[1] / 2 > cap || c->pairs[2] > cap) sticky[0] = 1;
         if (c->nonfinite) sticky[1] = 1;
+        if (c->timeout) sticky[2] = 1;
     }
 }
 
@@ -799,28 +890,13 @@ static __global__ void k_check(const DevCounters* __restrict__ c, int* __restric
 // one launch: dst_i[k] = src_i[perm[k]].
 struct PermField { const void* src; void* dst; int bytes; int pad; };
 struct PermList { int count; int pad; PermField f[44]; };
-// Copy every field of the list back (identity order): after k_permute_all
-// has written the cell-ordered fields into their shadows, the state returns
-// to the same buffers, so buffer addresses never change and a captured CUDA
-// graph stays valid across reorders.
-static __global__ void __launch_bounds__(256) k_copy_back_all(int n, PermList L) {
-    int k = gtid();
-    if (k >= n) return;
-    for (int i = 0; i < L.count; ++i) {
-        const PermField& f = L.f[i];
-        if (f.bytes == 4) ((int*)f.src)[k] = ((const int*)f.dst)[k];
-        else if (f.bytes == 8) ((long long*)f.src)[k] = ((const long long*)f.dst)[k];
-        else ((int4*)f.src)[k] = ((const int4*)f.dst)[k];
-    }
-}
-
 // Per-step counters to their initial values (a kernel, so that it can live in a graph).
 static __global__ void k_reset_counters(DevCounters* c) {
     int i = threadIdx.x;
     if (i < 3) c->pairs[i] = 0ull;
     if (i < 2) { c->maxiac[i] = 0; c->miniac[i] = 0x7fffffff; c->noiac[i] = 0; }
     if (i < 4) c->nfail[i] = 0;
-    if (i == 0) { c->n_out = 0; c->nonfinite = 0; c->overflow = 0; }
+    if (i == 0) { c->n_out = 0; c->nonfinite = 0; c->overflow = 0; c->timeout = 0; }
 }
 
 static __global__ void __launch_bounds__(256) k_permute_all(int n, const int* __restrict__ perm, PermList L) {

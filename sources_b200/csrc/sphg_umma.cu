@@ -350,12 +350,13 @@ __device__ __forceinline__ void ws_epilogue(const SphgGemmEpi& ep, uint32_t tacc
 // of bank conflicts.  Sums are formed in the same order as ws_epilogue.
 template <int N, int K>
 __device__ __forceinline__ void ws_epilogue_staged(const SphgGemmEpi& ep, uint32_t tacc, long long row0, int c0,
-                                                   float4* __restrict__ stage, int lane) {
+                                                   float4* __restrict__ stage, int lane, uint8_t* hs = nullptr,
+                                                   int r0s = 0) {
     constexpr int CW = 16;
     const int q = lane & 3, rs = lane >> 2;   // this lane's 16-byte unit, and its row within each group of 8
     const bool readz = ep.mode == SPHG_EPI_ACC || ep.mode == SPHG_EPI_RESID;
     const bool bias = ep.mode != SPHG_EPI_STORE && ep.mode != SPHG_EPI_ACC;
-    const bool hout = ep.mode != SPHG_EPI_STORE && ep.mode != SPHG_EPI_ACC && ep.h;
+    const bool hout = ep.mode != SPHG_EPI_STORE && ep.mode != SPHG_EPI_ACC && (ep.h || hs);
     const bool act = ep.mode == SPHG_EPI_EDGE || (ep.mode == SPHG_EPI_BIAS_ACT && ep.relu);
     bool edge[4];
     const float4* ps[4];
@@ -408,7 +409,13 @@ __device__ __forceinline__ void ws_epilogue_staged(const SphgGemmEpi& ep, uint32
                 uint2 hv;
                 hv.x = *reinterpret_cast<uint32_t*>(&t0);
                 hv.y = *reinterpret_cast<uint32_t*>(&t1);
-                reinterpret_cast<uint2*>(static_cast<__nv_bfloat16*>(ep.h) + grow * N)[col / 4] = hv;
+                if (hs) {   // into shared memory as the A operand of a following MMA (tile row r0s + r)
+                    const int tr = r0s + r;
+                    *reinterpret_cast<uint2*>(hs + (col >> 3) * (128 * 16) + (tr >> 3) * 128 + (tr & 7) * 16 +
+                                              (col & 7) * 2) = hv;
+                } else {
+                    reinterpret_cast<uint2*>(static_cast<__nv_bfloat16*>(ep.h) + grow * N)[col / 4] = hv;
+                }
             }
         }
         __syncwarp();
@@ -571,7 +578,170 @@ int launch_ws(const __nv_bfloat16* A, const __nv_bfloat16* B, int M, const SphgG
     return cudaGetLastError() == cudaSuccess ? SPHG_OK : SPHG_ERR_CUDA;
 }
 
+// ------------------------------------------------------------------------
+// One message-passing edge layer in one kernel (inference):
+//   a  = bf16(relu(E We^T + be + P[src, :128] + P[dst, 128:]))   (rows < nedge gather)
+//   EF = EF + a W2^T + b2,   Eout = bf16(EF)
+// which the network otherwise runs as two weight-stationary GEMMs (EDGE and
+// RESID epilogues) with the 128-wide hidden rows `a` written to and read
+// back from global memory.  Here a tile's hidden rows go from the first
+// accumulator (TMEM columns 0..127) through the EDGE epilogue straight into
+// shared memory, in the canonical K-major layout, as the A operand of the
+// second MMA (columns 128..255).  Both weight matrices stay in shared memory
+// for the whole launch.  Each CTA (one per SM) loops over 128-row tiles; the
+// next tile's E rows are copied (cp.async) while the current tile's MMAs and
+// epilogues run.  Sums are formed in the order of the two-GEMM path, so the
+// results are bit-identical to it.  Every MMA wait is bounded; on timeout
+// the kernel sets *err, waits (bounded) for its MMAs, frees TMEM and returns.
+struct EdgeShape {
+    static constexpr uint32_t T = 32 * 1024;                  // one 128 x 128 bf16 operand
+    static constexpr uint32_t B1 = 0, B2 = T, A0 = 2 * T, Z = 4 * T;
+    static constexpr uint32_t BAR = 5 * T;                    // 2 mbarriers + TMEM slot
+    static constexpr uint32_t STAGE = BAR + 32;               // 8 warps x 2 KB staging
+    static constexpr uint32_t SMEM = STAGE + 8 * 32 * 64;
+};
+
+__device__ __forceinline__ void load_b128(uint8_t* sB, const __nv_bfloat16* __restrict__ B, int tid) {
+    for (int c = tid; c < 128 * 16; c += WS_THREADS) {
+        const int r = c / 16, kc = c % 16;
+        *reinterpret_cast<uint4*>(sB + kc * (128 * 16) + (r >> 3) * 128 + (r & 7) * 16) =
+            *reinterpret_cast<const uint4*>(B + (size_t)r * 128 + kc * 8);
+    }
+}
+
+__device__ __forceinline__ void mma_128x128(uint32_t tacc, const uint8_t* sA, const uint8_t* sB, uint64_t* bar) {
+    const uint32_t idesc = make_idesc(128);
+#pragma unroll
+    for (int kk = 0; kk < 8; ++kk) {
+        const uint64_t da = make_desc(smem_u32(sA + kk * 2 * 2048), 2048, 128);
+        const uint64_t db = make_desc(smem_u32(sB + kk * 2 * 2048), 2048, 128);
+        const uint32_t en = kk > 0 ? 1u : 0u;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+            ::"r"(tacc), "l"(da), "l"(db), "r"(idesc), "r"(en), "r"(0), "r"(0), "r"(0), "r"(0));
+    }
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__global__ void __launch_bounds__(WS_THREADS, 1) k_edge_layer(const __nv_bfloat16* __restrict__ E, int M,
+                                                               const __nv_bfloat16* __restrict__ We,
+                                                               const __nv_bfloat16* __restrict__ W2,
+                                                               SphgGemmEpi e1, SphgGemmEpi e2, int* __restrict__ err) {
+    typedef EdgeShape S;
+    extern __shared__ __align__(128) uint8_t smem[];
+    uint64_t* mbar = (uint64_t*)(smem + S::BAR);
+    uint32_t* tslot = (uint32_t*)(mbar + 2);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    float4* stage = reinterpret_cast<float4*>(smem + S::STAGE) + warp * 128;
+    const int ntiles = M / 128;
+    const int my = blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+    auto tile_m0 = [&](int i) { return ((int)blockIdx.x + i * (int)gridDim.x) * 128; };
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                     "r"(256));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mbar)), "r"(1));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mbar + 1)), "r"(1));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::);
+    }
+    load_b128(smem + S::B1, We, tid);
+    load_b128(smem + S::B2, W2, tid);
+    if (my > 0) ws_load_a<128, 128>(smem + S::A0, E, tile_m0(0), tid);
+    cp_async_commit();
+    asm volatile("tcgen05.fence::before_thread_sync;" ::);
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::);
+    const uint32_t tmem = *tslot;
+    const uint32_t lane_off = (uint32_t)((warp & 3) * 32) << 16;
+    const int col0 = (warp >> 2) * 64;
+    uint32_t ph = 0u;        // bit b: parity of the next completion of mbar[b]
+    int wb = -1;             // the barrier of the MMA group being waited for
+    bool ok = true;
+    for (int i = 0; i < my && ok; ++i) {
+        const int s = i & 1;
+        const long long row0 = (long long)tile_m0(i) + (warp & 3) * 32;
+        cp_async_wait_all();
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::);
+            mma_128x128(tmem, smem + S::A0 + s * S::T, smem + S::B1, mbar);
+        }
+        wb = 0;
+        // the other E buffer was last read by the previous tile's first MMA, seen complete
+        if (i + 1 < my) ws_load_a<128, 128>(smem + S::A0 + (s ^ 1) * S::T, E, tile_m0(i + 1), tid);
+        cp_async_commit();
+        bool done = mbar_wait(smem_u32(mbar), ph & 1u, kWaitLimit);
+        ok = __syncthreads_and(done ? 1 : 0) != 0;
+        if (!ok) break;
+        ph ^= 1u;
+        wb = -1;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::);
+        ws_epilogue_staged<128, 128>(e1, tmem + lane_off, row0, col0, stage, lane, smem + S::Z, (warp & 3) * 32);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::);
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::);
+            mma_128x128(tmem + 128u, smem + S::Z, smem + S::B2, mbar + 1);
+        }
+        wb = 1;
+        done = mbar_wait(smem_u32(mbar + 1), (ph >> 1) & 1u, kWaitLimit);
+        ok = __syncthreads_and(done ? 1 : 0) != 0;
+        if (!ok) break;
+        ph ^= 2u;
+        wb = -1;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::);
+        ws_epilogue_staged<128, 128>(e2, tmem + lane_off + 128u, row0, col0, stage, lane);
+        asm volatile("tcgen05.fence::before_thread_sync;" ::);
+    }
+    if (!ok) {
+        if (tid == 0) atomicExch(err, 1);
+        // the MMA group whose wait ran out (bounded)
+        if (wb >= 0) mbar_wait(smem_u32(mbar + wb), (ph >> wb) & 1u, kWaitLimit);
+    }
+    cp_async_wait_all();
+    asm volatile("tcgen05.fence::before_thread_sync;" ::);
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256));
+}
+
 }  // namespace
+
+extern "C" int sphg_gnn_edge_layer(const void* E, float* EF, void* E_out, const float* P, const int* src,
+                                   const int* dst, long long nedge, int M, const void* We, const float* be,
+                                   const void* W2, const float* b2, int* err_dev, void* stream) {
+    if (!E || !EF || !E_out || !P || !src || !dst || !We || !be || !W2 || !b2 || !err_dev) return SPHG_ERR_BAD_ARG;
+    if (M <= 0 || M % 128 || nedge < 0 || nedge > M) return SPHG_ERR_BAD_ARG;
+    if ((((uintptr_t)E) | ((uintptr_t)EF) | ((uintptr_t)E_out) | ((uintptr_t)P) | ((uintptr_t)We) | ((uintptr_t)be) |
+         ((uintptr_t)W2) | ((uintptr_t)b2)) & 15)
+        return SPHG_ERR_BAD_ARG;
+    static bool configured = false;
+    if (!configured) {
+        if (cudaFuncSetAttribute(k_edge_layer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)EdgeShape::SMEM) !=
+            cudaSuccess)
+            return SPHG_ERR_CUDA;
+        configured = true;
+    }
+    SphgGemmEpi e1{};
+    e1.mode = SPHG_EPI_EDGE; e1.relu = 1; e1.bias = be; e1.P = P; e1.src = src; e1.dst = dst; e1.nedge = nedge;
+    SphgGemmEpi e2{};
+    e2.mode = SPHG_EPI_RESID; e2.bias = b2; e2.z = EF; e2.h = E_out;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int ntiles = M / 128;
+    const int grid = ntiles < sms ? ntiles : sms;
+    k_edge_layer<<<grid, WS_THREADS, EdgeShape::SMEM, (cudaStream_t)stream>>>(
+        (const __nv_bfloat16*)E, M, (const __nv_bfloat16*)We, (const __nv_bfloat16*)W2, e1, e2, err_dev);
+    return cudaGetLastError() == cudaSuccess ? SPHG_OK : SPHG_ERR_CUDA;
+}
 
 extern "C" int sphg_gemm_bf16_ws(const void* A, const void* B, int M, int N, int K, const SphgGemmEpi* epi,
                                  int* err_dev, void* stream) {

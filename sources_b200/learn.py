@@ -231,6 +231,8 @@ class MPNet:
         self.vscale = 1.0
         self.norm = t.tensor([0.0, 0.0, 1.0, 1.0], dtype=t.float32, device=self.device)
         self.launches = 0
+        # inference runs each layer's two edge GEMMs as one kernel (sphg_gnn_edge_layer)
+        self.fused_edges = True
 
     # ------------------------------------------------------------ plumbing
     @property
@@ -326,12 +328,19 @@ class MPNet:
         agg = G("agg", (Np, L), f32)
         for l in range(LAYERS):
             p = f"p{l}."
-            a = G("a" + tag(l), (Ep, L), bf)
             self._ws(hb, W[p + "wsd"]["wb"], Np, 2 * L, L, EPI_STORE, z=P)
-            self._ws(eb, W[p + "we"]["wb"], Ep, L, L, EPI_EDGE, 1, B[p + "be"]["w"], opt("z" + tag(l), (Ep, L)), a,
-                     P, b.src, b.dst, b.E)
-            eb = G("eb" + tag(l + 1), (Ep, L), bf)
-            self._ws(a, W[p + "w2"]["wb"], Ep, L, L, EPI_RESID, 0, B[p + "b2"]["w"], ef, eb)   # e += relu(z) W2^T + b2
+            if keep or not self.fused_edges:
+                a = G("a" + tag(l), (Ep, L), bf)
+                self._ws(eb, W[p + "we"]["wb"], Ep, L, L, EPI_EDGE, 1, B[p + "be"]["w"], opt("z" + tag(l), (Ep, L)), a,
+                         P, b.src, b.dst, b.E)
+                eb = G("eb" + tag(l + 1), (Ep, L), bf)
+                self._ws(a, W[p + "w2"]["wb"], Ep, L, L, EPI_RESID, 0, B[p + "b2"]["w"], ef, eb)   # e += relu(z) W2^T + b2
+            else:   # both edge GEMMs in one kernel, the hidden rows never leave the SM; eb updated in place
+                self.launches += 1
+                _call(self.L.sphg_gnn_edge_layer(_ptr(eb), _ptr(ef), _ptr(eb), _ptr(P), _ptr(b.src), _ptr(b.dst),
+                                                 b.E, Ep, _ptr(W[p + "we"]["wb"]), _ptr(B[p + "be"]["w"]),
+                                                 _ptr(W[p + "w2"]["wb"]), _ptr(B[p + "b2"]["w"]), _ptr(self.err), s),
+                      "sphg_gnn_edge_layer")
             self._k("sphg_gnn_segsum", _ptr(ef), _ptr(b.off), _ptr(agg), b.n, L, AGG_SCALE, s)
             cat = G("cat" + tag(l), (Np, 2 * L), bf)
             self._k("sphg_gnn_node_concat", _ptr(hb), _ptr(agg), _ptr(cat), Np, L, s)

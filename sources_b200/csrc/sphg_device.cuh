@@ -275,6 +275,11 @@ template <> __device__ __forceinline__ float rcp_<float>(float x) { return __frc
 template <typename T> __device__ __forceinline__ T div_(T a, T b) { return a / b; }
 template <> __device__ __forceinline__ float div_<float>(float a, float b) { return __fdividef(a, b); }
 
+// x^p of the wall force: pow in FP64; in FP32 the fast exp2(p log2 x) (a few
+// ulp at the exponents and ranges of the wall force, p = 12 and 4, x >= 1)
+template <typename T> __device__ __forceinline__ T powr_(T x, T p) { return pow(x, p); }
+template <> __device__ __forceinline__ float powr_<float>(float x, float p) { return __powf(x, p); }
+
 template <typename T> __device__ __forceinline__ T sqsum(T dx, T dy) { return dx * dx + dy * dy; }
 template <> __device__ __forceinline__ double sqsum<double>(double dx, double dy) {
     return __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));

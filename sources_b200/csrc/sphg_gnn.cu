@@ -283,6 +283,23 @@ __global__ void k_segsum(const float* __restrict__ e, const int64_t* __restrict_
     reinterpret_cast<float4*>(agg + n * LW)[lane] = make_float4(s.x * scale, s.y * scale, s.z * scale, s.w * scale);
 }
 
+// the same over bf16 edge rows: each lane sums 4 columns of every received row
+__global__ void k_segsum_bf16(const __nv_bfloat16* __restrict__ e, const int64_t* __restrict__ off,
+                              float* __restrict__ agg, int nnode, float scale) {
+    long long n;
+    int lane;
+    row_lane<LW / 4>(n, lane);
+    if (n >= nnode) return;
+    float4 s = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (long long k = off[n]; k < off[n + 1]; ++k) {
+        const uint2 u = reinterpret_cast<const uint2*>(e + k * LW)[lane];
+        const float2 lo = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u.x));
+        const float2 hi = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u.y));
+        s = add4(s, make_float4(lo.x, lo.y, hi.x, hi.y));
+    }
+    reinterpret_cast<float4*>(agg + n * LW)[lane] = make_float4(s.x * scale, s.y * scale, s.z * scale, s.w * scale);
+}
+
 // de[k] += scale * dagg[receiver of k]
 __global__ void k_segsum_bwd(const float* __restrict__ dagg, const int* __restrict__ dst, float* __restrict__ de,
                              long long nedge, float scale) {
@@ -599,6 +616,11 @@ int sphg_gnn_transpose(const void* in, int in_is_f32, void* out, long long rows,
 int sphg_gnn_segsum(const float* e, const int64_t* off, float* agg, int nnode, int L, float scale, void* stream) {
     if (L != LW) return SPHG_ERR_BAD_ARG;
     ROWS(k_segsum, (long long)nnode, LW / 4, e, off, agg, nnode, scale);
+}
+
+int sphg_gnn_segsum_bf16(const void* e, const int64_t* off, float* agg, int nnode, int L, float scale, void* stream) {
+    if (L != LW) return SPHG_ERR_BAD_ARG;
+    ROWS(k_segsum_bf16, (long long)nnode, LW / 4, (const __nv_bfloat16*)e, off, agg, nnode, scale);
 }
 
 int sphg_gnn_segsum_bwd(const float* dagg, const int* dst, float* de, long long nedge, int L, float scale,

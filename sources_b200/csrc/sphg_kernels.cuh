@@ -584,13 +584,13 @@ __global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_B : 1) k_
         d3 = fma2(splat2(vb), mul2(s_b, splat2(gr.y)), d3);
         const T2 dv = sub2(va, vb2);                              // v_a - v_b
         const T mb = vb * rb.rho;
+        const T irho = rcp_<T>(T(0.5) * (ra.rho + rb.rho));       // 1 / mean density (art_visc and av_vel)
         if (visc) {
             const T vr = dv.x * dx + dv.y * dy;
             if (vr < T(0)) {
                 const T muv = div_<T>(mh * vr, rr + mh * mh * etq2);
                 const T mc = T(0.5) * (qa.c + qb.c);
-                const T mrho = T(0.5) * (ra.rho + rb.rho);
-                const T piv = div_<T>((beta * muv - alpha * mc) * muv, mrho);
+                const T piv = ((beta * muv - alpha * mc) * muv) * irho;
                 av = fma2(splat2(-mb), mul2(splat2(piv), gr), av);
             }
         }
@@ -598,12 +598,12 @@ __global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_B : 1) k_
         if (do_rep && qb.itype < T(0)) {
             const T r = sqrt(rr);
             if (!(r > r0)) {
-                const T f = (pow(r0 / r, p1) - pow(r0 / r, p2)) / (r * r);
+                const T f = (powr_<T>(r0 / r, p1) - powr_<T>(r0 / r, p2)) / (r * r);
                 rp = fma2(mul2(splat2(dd), d), splat2(f), rp);
             }
         }
         if (xsph) {
-            const T q = div_<T>(mb * w, (ra.rho + rb.rho) / T(2));
+            const T q = (mb * w) * irho;
             xv = fma2(splat2(-q), dv, xv);
         }
     };
@@ -758,7 +758,7 @@ __global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_SOIL : 1)
         if (do_rep && qb.itype < T(0)) {
             const T r = sqrt(rr);
             if (!(r > r0)) {
-                const T f = (pow(r0 / r, p1) - pow(r0 / r, p2)) / (r * r);
+                const T f = (powr_<T>(r0 / r, p1) - powr_<T>(r0 / r, p2)) / (r * r);
                 rpx += dd * dx * f;
                 rpy += dd * dy * f;
             }

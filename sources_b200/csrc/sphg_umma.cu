@@ -248,11 +248,11 @@ struct WsShape {
 
 constexpr int WS_THREADS = 256;   // 8 warps: warps w and w + 4 share TMEM lanes 32 (w % 4) ..
 
-template <int N, int K>
+template <int N, int K, int NT = WS_THREADS>
 __device__ __forceinline__ void ws_load_a(uint8_t* sA, const __nv_bfloat16* __restrict__ A, int m0, int tid) {
     constexpr int KC = K / 8;
 #pragma unroll 4
-    for (int c = tid; c < 128 * KC; c += WS_THREADS) {
+    for (int c = tid; c < 128 * KC; c += NT) {
         const int r = c / KC, kc = c % KC;
         cp_async16(smem_u32(sA + kc * WsShape<N, K>::A_KC + (r >> 3) * 128 + (r & 7) * 16),
                    A + (size_t)(m0 + r) * K + kc * 8);
@@ -351,7 +351,7 @@ __device__ __forceinline__ void ws_epilogue(const SphgGemmEpi& ep, uint32_t tacc
 template <int N, int K>
 __device__ __forceinline__ void ws_epilogue_staged(const SphgGemmEpi& ep, uint32_t tacc, long long row0, int c0,
                                                    float4* __restrict__ stage, int lane, uint8_t* hs = nullptr,
-                                                   int r0s = 0) {
+                                                   int r0s = 0, int ncols = N / 2, const uint8_t* zs = nullptr) {
     constexpr int CW = 16;
     const int q = lane & 3, rs = lane >> 2;   // this lane's 16-byte unit, and its row within each group of 8
     const bool readz = ep.mode == SPHG_EPI_ACC || ep.mode == SPHG_EPI_RESID;
@@ -373,13 +373,24 @@ __device__ __forceinline__ void ws_epilogue_staged(const SphgGemmEpi& ep, uint32
     }
     const int wsw = (lane >> 1) & 3;   // swizzle of this lane's own staging row
 #pragma unroll 1
-    for (int c = c0; c < c0 + N / 2; c += CW) {
+    for (int c = c0; c < c0 + ncols; c += CW) {
         const int col = c + 4 * q;
         float4 add[4];
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
             add[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (readz) add[i] = reinterpret_cast<const float4*>(ep.z + (row0 + 8 * i + rs) * N)[col / 4];
+            if (readz) {
+                if (ep.z) {
+                    add[i] = reinterpret_cast<const float4*>(ep.z + (row0 + 8 * i + rs) * N)[col / 4];
+                } else {   // bf16 rows in shared memory, canonical K-major layout (tile row r0s + 8i + rs)
+                    const int tr = r0s + 8 * i + rs;
+                    const uint2 u = *reinterpret_cast<const uint2*>(zs + (col >> 3) * (128 * 16) + (tr >> 3) * 128 +
+                                                                    (tr & 7) * 16 + (col & 7) * 2);
+                    const float2 lo = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u.x));
+                    const float2 hi = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u.y));
+                    add[i] = make_float4(lo.x, lo.y, hi.x, hi.y);
+                }
+            }
             if (edge[i]) add[i] = add4f(add[i], add4f(ps[i][col / 4], pd[i][col / 4]));
         }
         if (bias) {
@@ -582,13 +593,17 @@ int launch_ws(const __nv_bfloat16* A, const __nv_bfloat16* B, int M, const SphgG
 // One message-passing edge layer in one kernel (inference):
 //   a  = bf16(relu(E We^T + be + P[src, :128] + P[dst, 128:]))   (rows < nedge gather)
 //   EF = EF + a W2^T + b2,   Eout = bf16(EF)
+// or, without EF (a bf16 residual stream), Eout = bf16(E + a W2^T + b2) with
+// E read back from the tile's copy in shared memory;
 // which the network otherwise runs as two weight-stationary GEMMs (EDGE and
 // RESID epilogues) with the 128-wide hidden rows `a` written to and read
 // back from global memory.  Here a tile's hidden rows go from the first
 // accumulator (TMEM columns 0..127) through the EDGE epilogue straight into
 // shared memory, in the canonical K-major layout, as the A operand of the
 // second MMA (columns 128..255).  Both weight matrices stay in shared memory
-// for the whole launch.  Each CTA (one per SM) loops over 128-row tiles; the
+// for the whole launch.  Each CTA (one per SM, 16 warps: each TMEM lane
+// quarter of the tile's rows is read by four warps of 32 columns each, so
+// that enough epilogue loads are in flight) loops over 128-row tiles; the
 // next tile's E rows are copied (cp.async) while the current tile's MMAs and
 // epilogues run.  Sums are formed in the order of the two-GEMM path, so the
 // results are bit-identical to it.  Every MMA wait is bounded; on timeout
@@ -597,12 +612,14 @@ struct EdgeShape {
     static constexpr uint32_t T = 32 * 1024;                  // one 128 x 128 bf16 operand
     static constexpr uint32_t B1 = 0, B2 = T, A0 = 2 * T, Z = 4 * T;
     static constexpr uint32_t BAR = 5 * T;                    // 2 mbarriers + TMEM slot
-    static constexpr uint32_t STAGE = BAR + 32;               // 8 warps x 2 KB staging
-    static constexpr uint32_t SMEM = STAGE + 8 * 32 * 64;
+    static constexpr int THREADS = 512;                       // 16 warps: 4 per TMEM lane quarter
+    static constexpr uint32_t STAGE = BAR + 32;               // 16 warps x 2 KB staging
+    static constexpr uint32_t SMEM = STAGE + (THREADS / 32) * 32 * 64;
 };
 
+template <int NT>
 __device__ __forceinline__ void load_b128(uint8_t* sB, const __nv_bfloat16* __restrict__ B, int tid) {
-    for (int c = tid; c < 128 * 16; c += WS_THREADS) {
+    for (int c = tid; c < 128 * 16; c += NT) {
         const int r = c / 16, kc = c % 16;
         *reinterpret_cast<uint4*>(sB + kc * (128 * 16) + (r >> 3) * 128 + (r & 7) * 16) =
             *reinterpret_cast<const uint4*>(B + (size_t)r * 128 + kc * 8);
@@ -626,7 +643,7 @@ __device__ __forceinline__ void mma_128x128(uint32_t tacc, const uint8_t* sA, co
                  : "memory");
 }
 
-__global__ void __launch_bounds__(WS_THREADS, 1) k_edge_layer(const __nv_bfloat16* __restrict__ E, int M,
+__global__ void __launch_bounds__(EdgeShape::THREADS, 1) k_edge_layer(const __nv_bfloat16* __restrict__ E, int M,
                                                                const __nv_bfloat16* __restrict__ We,
                                                                const __nv_bfloat16* __restrict__ W2,
                                                                SphgGemmEpi e1, SphgGemmEpi e2, int* __restrict__ err) {
@@ -650,16 +667,16 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_edge_layer(const __nv_bfloat1
         asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mbar + 1)), "r"(1));
         asm volatile("fence.mbarrier_init.release.cluster;" ::);
     }
-    load_b128(smem + S::B1, We, tid);
-    load_b128(smem + S::B2, W2, tid);
-    if (my > 0) ws_load_a<128, 128>(smem + S::A0, E, tile_m0(0), tid);
+    load_b128<S::THREADS>(smem + S::B1, We, tid);
+    load_b128<S::THREADS>(smem + S::B2, W2, tid);
+    if (my > 0) ws_load_a<128, 128, S::THREADS>(smem + S::A0, E, tile_m0(0), tid);
     cp_async_commit();
     asm volatile("tcgen05.fence::before_thread_sync;" ::);
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::);
     const uint32_t tmem = *tslot;
     const uint32_t lane_off = (uint32_t)((warp & 3) * 32) << 16;
-    const int col0 = (warp >> 2) * 64;
+    const int col0 = (warp >> 2) * 32;   // this warp's 32 of the 128 columns
     uint32_t ph = 0u;        // bit b: parity of the next completion of mbar[b]
     int wb = -1;             // the barrier of the MMA group being waited for
     bool ok = true;
@@ -675,7 +692,7 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_edge_layer(const __nv_bfloat1
         }
         wb = 0;
         // the other E buffer was last read by the previous tile's first MMA, seen complete
-        if (i + 1 < my) ws_load_a<128, 128>(smem + S::A0 + (s ^ 1) * S::T, E, tile_m0(i + 1), tid);
+        if (i + 1 < my) ws_load_a<128, 128, S::THREADS>(smem + S::A0 + (s ^ 1) * S::T, E, tile_m0(i + 1), tid);
         cp_async_commit();
         bool done = mbar_wait(smem_u32(mbar), ph & 1u, kWaitLimit);
         ok = __syncthreads_and(done ? 1 : 0) != 0;
@@ -683,7 +700,7 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_edge_layer(const __nv_bfloat1
         ph ^= 1u;
         wb = -1;
         asm volatile("tcgen05.fence::after_thread_sync;" ::);
-        ws_epilogue_staged<128, 128>(e1, tmem + lane_off, row0, col0, stage, lane, smem + S::Z, (warp & 3) * 32);
+        ws_epilogue_staged<128, 128>(e1, tmem + lane_off, row0, col0, stage, lane, smem + S::Z, (warp & 3) * 32, 32);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         asm volatile("tcgen05.fence::before_thread_sync;" ::);
         __syncthreads();
@@ -698,7 +715,9 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_edge_layer(const __nv_bfloat1
         ph ^= 2u;
         wb = -1;
         asm volatile("tcgen05.fence::after_thread_sync;" ::);
-        ws_epilogue_staged<128, 128>(e2, tmem + lane_off + 128u, row0, col0, stage, lane);
+        // without EF the residual is this tile's E rows, still in shared memory
+        ws_epilogue_staged<128, 128>(e2, tmem + lane_off + 128u, row0, col0, stage, lane, nullptr, (warp & 3) * 32, 32,
+                                     smem + S::A0 + s * S::T);
         asm volatile("tcgen05.fence::before_thread_sync;" ::);
     }
     if (!ok) {
@@ -717,7 +736,7 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_edge_layer(const __nv_bfloat1
 extern "C" int sphg_gnn_edge_layer(const void* E, float* EF, void* E_out, const float* P, const int* src,
                                    const int* dst, long long nedge, int M, const void* We, const float* be,
                                    const void* W2, const float* b2, int* err_dev, void* stream) {
-    if (!E || !EF || !E_out || !P || !src || !dst || !We || !be || !W2 || !b2 || !err_dev) return SPHG_ERR_BAD_ARG;
+    if (!E || !E_out || !P || !src || !dst || !We || !be || !W2 || !b2 || !err_dev) return SPHG_ERR_BAD_ARG;
     if (M <= 0 || M % 128 || nedge < 0 || nedge > M) return SPHG_ERR_BAD_ARG;
     if ((((uintptr_t)E) | ((uintptr_t)EF) | ((uintptr_t)E_out) | ((uintptr_t)P) | ((uintptr_t)We) | ((uintptr_t)be) |
          ((uintptr_t)W2) | ((uintptr_t)b2)) & 15)
@@ -738,7 +757,7 @@ extern "C" int sphg_gnn_edge_layer(const void* E, float* EF, void* E_out, const 
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int ntiles = M / 128;
     const int grid = ntiles < sms ? ntiles : sms;
-    k_edge_layer<<<grid, WS_THREADS, EdgeShape::SMEM, (cudaStream_t)stream>>>(
+    k_edge_layer<<<grid, EdgeShape::THREADS, EdgeShape::SMEM, (cudaStream_t)stream>>>(
         (const __nv_bfloat16*)E, M, (const __nv_bfloat16*)We, (const __nv_bfloat16*)W2, e1, e2, err_dev);
     return cudaGetLastError() == cudaSuccess ? SPHG_OK : SPHG_ERR_CUDA;
 }

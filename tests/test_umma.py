@@ -218,3 +218,60 @@ def test_fused_edge_layer_rejects_bad_arguments(lib):
     assert lib.sphg_gnn_edge_layer(one, one, one, one, one, one, 200, 128, one, one, one, one, one, None) != 0  # nedge > M
     assert lib.sphg_gnn_edge_layer(odd, one, one, one, one, one, 128, 128, one, one, one, one, one, None) != 0  # alignment
     assert lib.sphg_gnn_edge_layer(None, one, one, one, one, one, 128, 128, one, one, one, one, one, None) != 0
+
+
+@pytest.mark.parametrize("M", [128 * 3, 128 * 1201])
+def test_fused_edge_layer_bf16_residual(cuda_ok, lib, M):
+    """Without the fp32 residual rows the fused layer keeps the edge latent
+    in bf16 alone: Eout = bf16(E + a W2^T + b2), the same bits as the RESID
+    epilogue given z = fp32(E); in place, padding rows included."""
+    import torch
+    from sources_b200 import learn
+    L = 128
+    g = torch.Generator(device="cuda").manual_seed(M + 5)
+    E = torch.randn(M, L, device="cuda", generator=g).to(torch.bfloat16)
+    We = (torch.randn(L, L, device="cuda", generator=g) / L ** 0.5).to(torch.bfloat16)
+    W2 = (torch.randn(L, L, device="cuda", generator=g) / L ** 0.5).to(torch.bfloat16)
+    be = torch.randn(L, device="cuda", generator=g)
+    b2 = torch.randn(L, device="cuda", generator=g)
+    nodes = max(M // 20, 7)
+    P = torch.randn(nodes, 2 * L, device="cuda", generator=g)
+    nedge = M - 51
+    src = torch.randint(0, nodes, (M,), device="cuda", generator=g, dtype=torch.int32)
+    dst = torch.sort(torch.randint(0, nodes, (M,), device="cuda", generator=g, dtype=torch.int32)).values
+    a = torch.zeros(M, L, device="cuda", dtype=torch.bfloat16)
+    _ws(lib, E, We, M, L, L, learn.GemmEpi(mode=learn.EPI_EDGE, relu=1, bias=be.data_ptr(), z=None, h=a.data_ptr(),
+                                           P=P.data_ptr(), src=src.data_ptr(), dst=dst.data_ptr(), nedge=nedge))
+    z = E.float()
+    Eout_ref = torch.zeros(M, L, device="cuda", dtype=torch.bfloat16)
+    _ws(lib, a, W2, M, L, L, learn.GemmEpi(mode=learn.EPI_RESID, bias=b2.data_ptr(), z=z.data_ptr(),
+                                           h=Eout_ref.data_ptr()))
+    Ein = E.clone()
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    rc = lib.sphg_gnn_edge_layer(Ein.data_ptr(), None, Ein.data_ptr(), P.data_ptr(), src.data_ptr(), dst.data_ptr(),
+                                 nedge, M, We.data_ptr(), be.data_ptr(), W2.data_ptr(), b2.data_ptr(), err.data_ptr(),
+                                 torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    assert rc == 0 and int(err.item()) == 0
+    assert torch.equal(Ein, Eout_ref)
+
+
+def test_segsum_bf16_matches_fp32_rows(cuda_ok, lib):
+    """sphg_gnn_segsum_bf16 sums the same rows as sphg_gnn_segsum given their
+    fp32 values: identical results."""
+    import torch
+    L, n = 128, 1000
+    g = torch.Generator(device="cuda").manual_seed(3)
+    deg = torch.randint(0, 40, (n,), device="cuda", generator=g)
+    off = torch.zeros(n + 1, dtype=torch.int64, device="cuda")
+    off[1:] = torch.cumsum(deg, 0)
+    E = int(off[-1].item())
+    e = torch.randn(E, L, device="cuda", generator=g).to(torch.bfloat16)
+    a32 = torch.zeros(n, L, device="cuda")
+    a16 = torch.zeros(n, L, device="cuda")
+    s = torch.cuda.current_stream().cuda_stream
+    ef = e.float().contiguous()
+    assert lib.sphg_gnn_segsum(ef.data_ptr(), off.data_ptr(), a32.data_ptr(), n, L, 0.0625, s) == 0
+    assert lib.sphg_gnn_segsum_bf16(e.data_ptr(), off.data_ptr(), a16.data_ptr(), n, L, 0.0625, s) == 0
+    torch.cuda.synchronize()
+    assert torch.equal(a32, a16)

@@ -166,18 +166,45 @@ struct Engine : EngineBase {
     // ---------------------------------------------------------------- launch
     template <typename K, typename... A>
     int launch(const char* name, K kern, int grid_, int block, A... args) {
-        return launch_smem(name, kern, grid_, block, 0, args...);
+        return launch_ex(name, false, kern, grid_, block, 0, args...);
     }
     // with `smem` bytes of dynamic shared memory (the neighbour staging space)
     template <typename K, typename... A>
     int launch_smem(const char* name, K kern, int grid_, int block, size_t smem, A... args) {
+        return launch_ex(name, false, kern, grid_, block, smem, args...);
+    }
+    // A kernel of the step chain (it begins with pdl_enter): launched with
+    // programmatic stream serialization, so that it may launch while its
+    // predecessor on the stream finishes.  Not while kernels are timed one by
+    // one.
+    template <typename K, typename... A>
+    int launch_pdl(const char* name, K kern, int grid_, int block, size_t smem, A... args) {
+        return launch_ex(name, true, kern, grid_, block, smem, args...);
+    }
+    bool use_pdl = SPHG_PDL != 0;
+    template <typename K, typename... A>
+    int launch_ex(const char* name, bool pdl, K kern, int grid_, int block, size_t smem, A... args) {
         if (grid_ <= 0) return 0;
         cudaEvent_t a = nullptr, b = nullptr;
         if (ctx->prof.on) {
             a = ctx->prof.get(); b = ctx->prof.get();
             cudaEventRecord(a, ctx->stream);
         }
-        kern<<<grid_, block, smem, ctx->stream>>>(args...);
+        if (pdl && use_pdl && !ctx->prof.on) {
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3((unsigned)grid_);
+            cfg.blockDim = dim3((unsigned)block);
+            cfg.dynamicSmemBytes = smem;
+            cfg.stream = ctx->stream;
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+            at[0].val.programmaticStreamSerializationAllowed = 1;
+            cfg.attrs = at;
+            cfg.numAttrs = 1;
+            cudaLaunchKernelEx(&cfg, kern, args...);
+        } else {
+            kern<<<grid_, block, smem, ctx->stream>>>(args...);
+        }
         ctx->prof.launches++;
         counters_fresh = false;
         cudaError_t e = cudaGetLastError();
@@ -523,17 +550,17 @@ struct Engine : EngineBase {
     int build_cells(int ph) {
         PhaseDev<T>& D = P[ph];
         CUDA_TRY(cudaMemsetAsync(counts[ph], 0, sizeof(int) * ((size_t)ncell + 1), ctx->stream));
-        int rc = launch("cell_count", k_cell_count, blocks(D.n, 256), 256, (const double2*)D.x, D.n, grid, D.cell_id,
-                        D.cell_fill, counts[ph], cnt);
+        int rc = launch_pdl("cell_count", k_cell_count, blocks(D.n, 256), 256, 0, (const double2*)D.x, D.n, grid,
+                            D.cell_id, D.cell_fill, counts[ph], cnt);
         if (rc) return rc;
         size_t bytes = cub_bytes;
         CUDA_TRY(cub::DeviceScan::ExclusiveSum(ph == 1 && cub_tmp1 ? cub_tmp1 : cub_tmp, bytes, counts[ph], D.cell_start,
                                                ncell + 1, ctx->stream));
-        if ((rc = launch("cell_scatter", k_cell_scatter, blocks(D.n, 256), 256, D.n, (const int*)D.cell_id,
-                         (const int*)D.cell_fill, (const int*)D.cell_start, D.perm)))
+        if ((rc = launch_pdl("cell_scatter", k_cell_scatter, blocks(D.n, 256), 256, 0, D.n, (const int*)D.cell_id,
+                             (const int*)D.cell_fill, (const int*)D.cell_start, D.perm)))
             return rc;
-        return launch("cell_sort", k_cell_sort, blocks(ncell, 256), 256, ncell, (const int*)D.cell_start,
-                      (const int*)D.orig, D.perm);
+        return launch_pdl("cell_sort", k_cell_sort, blocks(ncell, 256), 256, 0, ncell, (const int*)D.cell_start,
+                          (const int*)D.orig, D.perm);
     }
 
     // The persistent per-particle fields of a phase and their element sizes.
@@ -576,10 +603,10 @@ struct Engine : EngineBase {
             L.f[i].dst = shadow[ph][i];
             L.f[i].bytes = refs[i].second;
         }
-        int rc = launch("reorder", k_permute_all, blocks(D.n, 256), 256, D.n, (const int*)D.perm, L);
+        int rc = launch_pdl("reorder", k_permute_all, blocks(D.n, 256), 256, 0, D.n, (const int*)D.perm, L);
         if (rc) return rc;
         swap_buffers(ph);
-        return launch("iota", k_iota, blocks(D.n, 256), 256, D.n, D.perm);
+        return launch_pdl("iota", k_iota, blocks(D.n, 256), 256, 0, D.n, D.perm);
     }
 
     // Launches above 48 KB of dynamic shared memory must be allowed per kernel
@@ -593,7 +620,7 @@ struct Engine : EngineBase {
     }
 
     // -------------------------------------------------------------- the step
-    int reset_counters() { return launch("reset", k_reset_counters, 1, 32, cnt); }
+    int reset_counters() { return launch_pdl("reset", k_reset_counters, 1, 32, 0, cnt); }
 
     // The pair passes of one step for kernel function SKF.  fh: run the
     // leapfrog predictor inside the gathers; u: what the last pass of each
@@ -607,15 +634,15 @@ struct Engine : EngineBase {
         if (p.single_phase) {
             PhaseDev<T>& D = P[0];
             if (D.material == SPHG_WATER) {
-                if ((rc = launch("gather", k_gather<T>, blocks(D.n, 256), 256, D, sim, 0, 0, fh, 0, 0, cnt))) return rc;
-                if ((rc = launch("water_sum", k_water_sum<T, SKF>, blocks(D.n, tpb), tpb, D, grid, sc_same, sim, cnt))) return rc;
-                if ((rc = launch("water_pass_a", k_water_pass_a<T, SKF, true>, blocks(D.n, tpb), tpb, D, grid, sc_same, sim, cnt))) return rc;
-                if ((rc = launch("water_pass_b", k_water_pass_b<T, SKF, true, false>, blocks(D.n, tpb), tpb, D, D, grid, sc_same,
+                if ((rc = launch_pdl("gather", k_gather<T>, blocks(D.n, 256), 256, 0, D, sim, 0, 0, fh, 0, 0, cnt))) return rc;
+                if ((rc = launch_pdl("water_sum", k_water_sum<T, SKF>, blocks(D.n, tpb), tpb, 0, D, grid, sc_same, sim, cnt))) return rc;
+                if ((rc = launch_pdl("water_pass_a", k_water_pass_a<T, SKF, true>, blocks(D.n, tpb), tpb, 0, D, grid, sc_same, sim, cnt))) return rc;
+                if ((rc = launch_pdl("water_pass_b", k_water_pass_b<T, SKF, true, false>, blocks(D.n, tpb), tpb, 0, D, D, grid, sc_same,
                                  sc_same, sim, u, cnt))) return rc;
             } else {
-                if ((rc = launch("gather", k_gather<T>, blocks(D.n, 256), 256, D, sim, 1, dp, fh, 0, dp, cnt))) return rc;
+                if ((rc = launch_pdl("gather", k_gather<T>, blocks(D.n, 256), 256, 0, D, sim, 1, dp, fh, 0, dp, cnt))) return rc;
                 StepCtl us = u; us.with_vof = 0; us.do_dp = dp;
-                if ((rc = launch("soil_pass", k_soil_pass<T, SKF, true, false>, blocks(D.n, tpb), tpb, D, D, grid, sc_same, sc_same,
+                if ((rc = launch_pdl("soil_pass", k_soil_pass<T, SKF, true, false>, blocks(D.n, tpb), tpb, 0, D, D, grid, sc_same, sc_same,
                                  sim, cnt, 0, us))) return rc;
             }
         } else {
@@ -624,8 +651,8 @@ struct Engine : EngineBase {
             StepCtl uw = u; uw.with_vof = 1; uw.do_dp = 0;
             StepCtl us = u; us.with_vof = 1; us.do_dp = dp;
             // the soil's gather was launched by run() on the side stream
-            if ((rc = launch("gather", k_gather<T>, blocks(W.n, 256), 256, W, sim, 0, 0, fh, 1, 0, cnt))) return rc;
-            if ((rc = launch_smem("water_pass_a", k_water_pass_a<T, SKF, false>, blocks(W.n, tpb), tpb,
+            if ((rc = launch_pdl("gather", k_gather<T>, blocks(W.n, 256), 256, 0, W, sim, 0, 0, fh, 1, 0, cnt))) return rc;
+            if ((rc = launch_pdl("water_pass_a", k_water_pass_a<T, SKF, false>, blocks(W.n, tpb), tpb,
                                   (size_t)SPHG_STAGE_A * (16 + sizeof(RecA<T>)), W, grid, sc_same, sim, cnt)))
                 return rc;
             // The cross pairs run inside the last pass of each phase; the soil
@@ -645,9 +672,9 @@ struct Engine : EngineBase {
                 CUDA_TRY(cudaStreamWaitEvent(side, ctx->ev_fork, 0));
             }
             ctx->stream = side;
-            rc = fch ? launch("soil_pass", k_soil_pass<T, SKF, false, true>, blocks(S.n, tpb), tpb, S, W, grid, sc_same,
+            rc = fch ? launch_pdl("soil_pass", k_soil_pass<T, SKF, false, true>, blocks(S.n, tpb), tpb, 0, S, W, grid, sc_same,
                               sc_cross, sim, cnt, 1, us)
-                     : launch("soil_pass", k_soil_pass<T, SKF, false, false>, blocks(S.n, tpb), tpb, S, W, grid, sc_same,
+                     : launch_pdl("soil_pass", k_soil_pass<T, SKF, false, false>, blocks(S.n, tpb), tpb, 0, S, W, grid, sc_same,
                               sc_cross, sim, cnt, 1, us);
             cudaError_t ej = side != main_stream ? cudaEventRecord(ctx->ev_join, side) : cudaSuccess;
             ctx->stream = main_stream;
@@ -657,9 +684,9 @@ struct Engine : EngineBase {
                 if (e2 != cudaSuccess && rc == 0) rc = SPHG_ERR_CUDA;
             }
             if (rc == 0)
-                rc = fch ? launch("water_pass_b", k_water_pass_b<T, SKF, false, true>, blocks(W.n, tpb), tpb, W, S, grid,
+                rc = fch ? launch_pdl("water_pass_b", k_water_pass_b<T, SKF, false, true>, blocks(W.n, tpb), tpb, 0, W, S, grid,
                                   sc_same, sc_cross, sim, uw, cnt)
-                         : launch("water_pass_b", k_water_pass_b<T, SKF, false, false>, blocks(W.n, tpb), tpb, W, S, grid,
+                         : launch_pdl("water_pass_b", k_water_pass_b<T, SKF, false, false>, blocks(W.n, tpb), tpb, 0, W, S, grid,
                                   sc_same, sc_cross, sim, uw, cnt);
             // join in every case, so that a capture in progress ends joined
             cudaError_t ew = ej != cudaSuccess ? ej
@@ -785,7 +812,7 @@ struct Engine : EngineBase {
             ctx->stream = side;
             rc = build_cells(1);
             if (!rc && reorder_now) rc = reorder(1);
-            if (!rc) rc = launch("gather", k_gather<T>, blocks(P[1].n, 256), 256, P[1], sim, 1, sim.yield_dp, fh, 1,
+            if (!rc) rc = launch_pdl("gather", k_gather<T>, blocks(P[1].n, 256), 256, 0, P[1], sim, 1, sim.yield_dp, fh, 1,
                                  sim.yield_dp, cnt);
             cudaError_t ej = side != main_stream ? cudaEventRecord(ctx->ev_join2, side) : cudaSuccess;
             ctx->stream = main_stream;
@@ -808,7 +835,7 @@ struct Engine : EngineBase {
             default: rc = passes<4>(fh, u); break;
         }
         if (rc) return rc;
-        return launch("check", k_check, 1, 32, (const DevCounters*)cnt, sticky, (unsigned long long)p.max_interaction);
+        return launch_pdl("check", k_check, 1, 32, 0, (const DevCounters*)cnt, sticky, (unsigned long long)p.max_interaction);
     }
 
     // single_step / single_step_for_water / single_step_for_soil

@@ -75,13 +75,29 @@ struct SimConst {
 #define SPHG_MINB_SOIL 1
 #endif
 
+// launch the step's kernels with programmatic stream serialization (0: plain launches)
+#ifndef SPHG_PDL
+#define SPHG_PDL 1
+#endif
+
 __device__ __forceinline__ int gtid() { return blockIdx.x * blockDim.x + threadIdx.x; }
+
+// Programmatic dependent launch: the step's kernels are launched so that the
+// next one may start while this one finishes (Engine::launch_pdl).  A kernel
+// lets its successor launch as soon as all of its own blocks have started,
+// and waits for its predecessor's results before touching any memory.
+// Launched without the attribute, both are no-ops.
+__device__ __forceinline__ void pdl_enter() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
 
 // ----------------------------------------------------------------- cell list
 // cell key (row-major) and the particle's rank inside its cell.
 static __global__ void __launch_bounds__(256) k_cell_count(const double2* __restrict__ x, int n, GridGeom g,
                                                     int* __restrict__ cell_id, int* __restrict__ rank,
                                                     int* __restrict__ counts, DevCounters* cnt) {
+    pdl_enter();
     int a = gtid();
     if (a >= n) return;
     double2 p = x[a];
@@ -96,6 +112,7 @@ static __global__ void __launch_bounds__(256) k_cell_count(const double2* __rest
 
 static __global__ void __launch_bounds__(256) k_cell_scatter(int n, const int* __restrict__ cell_id, const int* __restrict__ rank,
                                                       const int* __restrict__ cell_start, int* __restrict__ perm) {
+    pdl_enter();
     int a = gtid();
     if (a >= n) return;
     perm[cell_start[cell_id[a]] + rank[a]] = a;
@@ -106,6 +123,7 @@ static __global__ void __launch_bounds__(256) k_cell_scatter(int n, const int* _
 // nor on the current state order (a download/upload restart is bit-identical).
 static __global__ void __launch_bounds__(256) k_cell_sort(int ncell, const int* __restrict__ cell_start,
                                                    const int* __restrict__ orig, int* __restrict__ perm) {
+    pdl_enter();
     int c = gtid();
     if (c >= ncell) return;
     int b = cell_start[c], e = cell_start[c + 1];
@@ -223,6 +241,7 @@ __device__ __forceinline__ void count_fail(DevCounters* cnt, int slot, int fail)
 template <typename T>
 __global__ void __launch_bounds__(256) k_gather(PhaseDev<T> P, SimConst c, int soil, int do_dp, int fh, int with_vof,
                                                 int fh_dp, DevCounters* cnt) {
+    pdl_enter();
     int k = gtid();
     int fail0 = 0, fail = 0;
     if (k < P.n) {
@@ -305,6 +324,7 @@ __device__ __forceinline__ void pair_kernel(const KernelConst<T, SKF>& ka, const
 // (declarations_sph.f90:1465-1466, df2 m_particles.f90:1802-1831).
 template <typename T, int SKF>
 __global__ void __launch_bounds__(SPHG_TPB) k_water_sum(PhaseDev<T> P, GridGeom g, SearchConst sc, SimConst c, DevCounters* cnt) {
+    pdl_enter();
     SPHG_HITBUF(T);
     const int k = gtid();
     const bool valid = k < P.n;
@@ -356,6 +376,7 @@ __global__ void __launch_bounds__(SPHG_TPB) k_water_sum(PhaseDev<T> P, GridGeom 
 // since grad W = s dx.
 template <typename T, int SKF, bool SINGLE>
 __global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_A : 1) k_water_pass_a(PhaseDev<T> P, GridGeom g, SearchConst sc, SimConst c, DevCounters* cnt) {
+    pdl_enter();
     const int k = gtid();
     const bool valid = k < P.n;
     const int kk = valid ? k : 0;
@@ -534,6 +555,7 @@ __device__ __forceinline__ int cross_water_sums(HB& hb, const PhaseDev<T>& S, co
 template <typename T, int SKF, bool SINGLE, bool FCH>
 __global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_B : 1) k_water_pass_b(PhaseDev<T> P, PhaseDev<T> S, GridGeom g, SearchConst sc,
                                                           SearchConst scx, SimConst c, StepCtl u, DevCounters* cnt) {
+    pdl_enter();
     typedef typename V2<T>::t T2;
     SPHG_HITBUF(T);
     const int k = gtid();
@@ -674,6 +696,7 @@ __global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_B : 1) k_
 template <typename T, int SKF, bool SINGLE, bool FCH>
 __global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_SOIL : 1) k_soil_pass(PhaseDev<T> P, PhaseDev<T> W, GridGeom g, SearchConst sc,
                                                        SearchConst scx, SimConst c, DevCounters* cnt, int slot, StepCtl u) {
+    pdl_enter();
     typedef typename V2<T>::t T2;
     SPHG_HITBUF(T);
     const int k = gtid();
@@ -850,6 +873,7 @@ __global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_SOIL : 1)
 // Sticky per-batch flags: a pair list above max_interaction (the reference
 // stops there, m_particles.f90:992-993) and non-finite positions.
 static __global__ void k_check(const DevCounters* __restrict__ c, int* __restrict__ sticky, unsigned long long cap) {
+    pdl_enter();
     if (threadIdx.x == 0 && blockIdx.x == 0) {
         if (c->pairs[0] / 2 > cap || c->pairs[1] / 2 > cap || c->pairs[2] > cap) sticky[0] = 1;
         if (c->nonfinite) sticky[1] = 1;
@@ -864,6 +888,7 @@ struct PermField { const void* src; void* dst; int bytes; int pad; };
 struct PermList { int count; int pad; PermField f[44]; };
 // Per-step counters to their initial values (a kernel, so that it can live in a graph).
 static __global__ void k_reset_counters(DevCounters* c) {
+    pdl_enter();
     int i = threadIdx.x;
     if (i < 3) c->pairs[i] = 0ull;
     if (i < 2) { c->maxiac[i] = 0; c->miniac[i] = 0x7fffffff; c->noiac[i] = 0; }
@@ -872,6 +897,7 @@ static __global__ void k_reset_counters(DevCounters* c) {
 }
 
 static __global__ void __launch_bounds__(256) k_permute_all(int n, const int* __restrict__ perm, PermList L) {
+    pdl_enter();
     int k = gtid();
     if (k >= n) return;
     const int a = perm[k];
@@ -889,6 +915,7 @@ __global__ void __launch_bounds__(256) k_permute(int n, const int* __restrict__ 
     if (k < n) dst[k] = src[perm[k]];
 }
 static __global__ void __launch_bounds__(256) k_iota(int n, int* __restrict__ v) {
+    pdl_enter();
     int k = gtid();
     if (k < n) v[k] = k;
 }

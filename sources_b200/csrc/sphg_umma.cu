@@ -277,94 +277,35 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
     for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
 }
 
-// Epilogue of one row (this thread's TMEM lane) over columns [c0, c0 + N/2)
-// in chunks of 16: every global input of a chunk (residual row, gathered
-// projection rows, bias) is requested before the TMEM read, so a thread has
-// up to 12 16-byte loads in flight; each chunk writes 64 contiguous bytes of
-// the fp32 row and 32 of the bf16 row.
-template <int N, int K>
-__device__ __forceinline__ void ws_epilogue(const SphgGemmEpi& ep, uint32_t tacc, long long row, int c0) {
-    constexpr int CW = 16;
-    const bool edge = ep.mode == SPHG_EPI_EDGE && row < ep.nedge;
-    const float4* ps = nullptr;
-    const float4* pd = nullptr;
-    if (edge) {
-        ps = reinterpret_cast<const float4*>(ep.P + (long long)ep.src[row] * 2 * N);
-        pd = reinterpret_cast<const float4*>(ep.P + (long long)ep.dst[row] * 2 * N + N);
-    }
-    const bool readz = ep.mode == SPHG_EPI_ACC || ep.mode == SPHG_EPI_RESID;
-    const bool bias = ep.mode != SPHG_EPI_STORE && ep.mode != SPHG_EPI_ACC;
-    float4* zr = ep.z ? reinterpret_cast<float4*>(ep.z + row * N) : nullptr;
-#pragma unroll 1
-    for (int c = c0; c < c0 + N / 2; c += CW) {
-        float4 add[CW / 4];
-#pragma unroll
-        for (int j = 0; j < CW / 4; ++j) add[j] = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (readz) {
-#pragma unroll
-            for (int j = 0; j < CW / 4; ++j) add[j] = zr[c / 4 + j];
-        }
-        if (edge) {
-            float4 a[CW / 4], b[CW / 4];
-#pragma unroll
-            for (int j = 0; j < CW / 4; ++j) { a[j] = ps[c / 4 + j]; b[j] = pd[c / 4 + j]; }
-#pragma unroll
-            for (int j = 0; j < CW / 4; ++j) add[j] = add4f(add[j], add4f(a[j], b[j]));
-        }
-        if (bias) {
-            const float4* b4 = reinterpret_cast<const float4*>(ep.bias + c);
-#pragma unroll
-            for (int j = 0; j < CW / 4; ++j) add[j] = add4f(add[j], b4[j]);
-        }
-        float v[CW];
-        tmem_ld16(tacc + (uint32_t)c, v);
-#pragma unroll
-        for (int j = 0; j < CW / 4; ++j) {
-            v[4 * j] += add[j].x; v[4 * j + 1] += add[j].y; v[4 * j + 2] += add[j].z; v[4 * j + 3] += add[j].w;
-        }
-        if (zr) {
-#pragma unroll
-            for (int j = 0; j < CW / 4; ++j)
-                zr[c / 4 + j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
-        }
-        if (ep.mode != SPHG_EPI_STORE && ep.mode != SPHG_EPI_ACC && ep.h) {
-            const bool act = ep.mode == SPHG_EPI_EDGE || (ep.mode == SPHG_EPI_BIAS_ACT && ep.relu);
-            if (act) {
-#pragma unroll
-                for (int j = 0; j < CW; ++j) v[j] = fmaxf(v[j], 0.f);
-            }
-            uint4* hr = reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(ep.h) + row * N + c);
-#pragma unroll
-            for (int j = 0; j < CW / 8; ++j) hr[j] = bf16x8(v + 8 * j);
-        }
-    }
-}
-
-// The same epilogue through a per-warp staging tile in shared memory.  The
-// warp's 32 accumulator rows (one per lane, as TMEM delivers them) are
+// The epilogue of a warp's 32 accumulator rows (one per lane, as TMEM
+// delivers them) over its columns, through a per-warp staging tile in shared
+// memory.  The warp's 32 accumulator rows (one per lane, as TMEM delivers them) are
 // written to shared memory and read back so that 4 lanes cover the 64
 // contiguous bytes of one row's 16-column chunk: every global load and store
 // of the epilogue then touches 8 rows per instruction instead of 32.  In the
 // staging tile row r holds 4 16-byte units, unit u at slot u ^ ((r >> 1) & 3),
 // so that both the row-per-lane writes and the 4-lanes-per-row reads are free
-// of bank conflicts.  Sums are formed in the same order as ws_epilogue.
-template <int N, int K>
+// of bank conflicts.  Each chunk of 16 columns forms z = acc + (((residual) +
+// (P[src] + P[dst])) + bias), the parts that apply to the mode, in that order.
+template <int N, int K, int MODE = -1>   // MODE >= 0: the epilogue mode known at compile time
 __device__ __forceinline__ void ws_epilogue_staged(const SphgGemmEpi& ep, uint32_t tacc, long long row0, int c0,
                                                    float4* __restrict__ stage, int lane, uint8_t* hs = nullptr,
-                                                   int r0s = 0, int ncols = N / 2, const uint8_t* zs = nullptr) {
+                                                   int r0s = 0, int ncols = N / 2,
+                                                   const __nv_bfloat16* zb = nullptr) {
     constexpr int CW = 16;
     const int q = lane & 3, rs = lane >> 2;   // this lane's 16-byte unit, and its row within each group of 8
-    const bool readz = ep.mode == SPHG_EPI_ACC || ep.mode == SPHG_EPI_RESID;
-    const bool bias = ep.mode != SPHG_EPI_STORE && ep.mode != SPHG_EPI_ACC;
-    const bool hout = ep.mode != SPHG_EPI_STORE && ep.mode != SPHG_EPI_ACC && (ep.h || hs);
-    const bool act = ep.mode == SPHG_EPI_EDGE || (ep.mode == SPHG_EPI_BIAS_ACT && ep.relu);
+    const int mode = MODE >= 0 ? MODE : ep.mode;
+    const bool readz = mode == SPHG_EPI_ACC || mode == SPHG_EPI_RESID;
+    const bool bias = mode != SPHG_EPI_STORE && mode != SPHG_EPI_ACC;
+    const bool hout = mode != SPHG_EPI_STORE && mode != SPHG_EPI_ACC && (ep.h || hs);
+    const bool act = mode == SPHG_EPI_EDGE || (mode == SPHG_EPI_BIAS_ACT && ep.relu);
     bool edge[4];
     const float4* ps[4];
     const float4* pd[4];
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
         const long long r = row0 + 8 * i + rs;
-        edge[i] = ep.mode == SPHG_EPI_EDGE && r < ep.nedge;
+        edge[i] = mode == SPHG_EPI_EDGE && r < ep.nedge;
         ps[i] = pd[i] = nullptr;
         if (edge[i]) {
             ps[i] = reinterpret_cast<const float4*>(ep.P + (long long)ep.src[r] * 2 * N);
@@ -372,6 +313,23 @@ __device__ __forceinline__ void ws_epilogue_staged(const SphgGemmEpi& ep, uint32
         }
     }
     const int wsw = (lane >> 1) & 3;   // swizzle of this lane's own staging row
+    // A chunk's global inputs are loaded one chunk ahead: the loads of chunk
+    // c + CW are in flight while chunk c is read from TMEM, staged and stored.
+    float4 zf[4], pa[4], pb[4], bb = make_float4(0.f, 0.f, 0.f, 0.f);
+    uint2 zh[4];
+    auto load_chunk = [&](int cc) {
+        const int col = cc + 4 * q;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            if (readz) {
+                if (ep.z) zf[i] = reinterpret_cast<const float4*>(ep.z + (row0 + 8 * i + rs) * N)[col / 4];
+                else zh[i] = reinterpret_cast<const uint2*>(zb + (row0 + 8 * i + rs) * N)[col / 4];
+            }
+            if (edge[i]) { pa[i] = ps[i][col / 4]; pb[i] = pd[i][col / 4]; }
+        }
+        if (bias) bb = reinterpret_cast<const float4*>(ep.bias)[col / 4];
+    };
+    load_chunk(c0);
 #pragma unroll 1
     for (int c = c0; c < c0 + ncols; c += CW) {
         const int col = c + 4 * q;
@@ -381,23 +339,20 @@ __device__ __forceinline__ void ws_epilogue_staged(const SphgGemmEpi& ep, uint32
             add[i] = make_float4(0.f, 0.f, 0.f, 0.f);
             if (readz) {
                 if (ep.z) {
-                    add[i] = reinterpret_cast<const float4*>(ep.z + (row0 + 8 * i + rs) * N)[col / 4];
-                } else {   // bf16 rows in shared memory, canonical K-major layout (tile row r0s + 8i + rs)
-                    const int tr = r0s + 8 * i + rs;
-                    const uint2 u = *reinterpret_cast<const uint2*>(zs + (col >> 3) * (128 * 16) + (tr >> 3) * 128 +
-                                                                    (tr & 7) * 16 + (col & 7) * 2);
-                    const float2 lo = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u.x));
-                    const float2 hi = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u.y));
+                    add[i] = zf[i];
+                } else {   // the residual as bf16 rows (zb); may be the rows this epilogue writes to h
+                    const float2 lo = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&zh[i].x));
+                    const float2 hi = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&zh[i].y));
                     add[i] = make_float4(lo.x, lo.y, hi.x, hi.y);
                 }
             }
-            if (edge[i]) add[i] = add4f(add[i], add4f(ps[i][col / 4], pd[i][col / 4]));
+            if (edge[i]) add[i] = add4f(add[i], add4f(pa[i], pb[i]));
         }
         if (bias) {
-            const float4 b4 = reinterpret_cast<const float4*>(ep.bias)[col / 4];
 #pragma unroll
-            for (int i = 0; i < 4; ++i) add[i] = add4f(add[i], b4);
+            for (int i = 0; i < 4; ++i) add[i] = add4f(add[i], bb);
         }
+        if (c + CW < c0 + ncols) load_chunk(c + CW);
         float v[CW];
         tmem_ld16(tacc + (uint32_t)c, v);
 #pragma unroll
@@ -433,22 +388,7 @@ __device__ __forceinline__ void ws_epilogue_staged(const SphgGemmEpi& ep, uint32
     }
 }
 
-// Staged epilogue (1) or the row-per-lane one (0).
-#ifndef SPHG_WS_STAGED
-#define SPHG_WS_STAGED 1
-#endif
-
-template <int N, int K>
-__device__ __forceinline__ void ws_epilogue_any(const SphgGemmEpi& ep, uint32_t tacc, long long row0, int c0,
-                                                float4* stage, int lane) {
-#if SPHG_WS_STAGED
-    ws_epilogue_staged<N, K>(ep, tacc, row0, c0, stage, lane);
-#else
-    ws_epilogue<N, K>(ep, tacc, row0 + lane, c0);
-#endif
-}
-
-template <int N, int K>
+template <int N, int K, int MODE>
 __global__ void __launch_bounds__(WS_THREADS, 2) k_gemm_ws(const __nv_bfloat16* __restrict__ A,
                                                     const __nv_bfloat16* __restrict__ B, int M, SphgGemmEpi ep,
                                                     int* __restrict__ err) {
@@ -536,8 +476,8 @@ __global__ void __launch_bounds__(WS_THREADS, 2) k_gemm_ws(const __nv_bfloat16* 
         asm volatile("tcgen05.fence::after_thread_sync;" ::);
         if (i + 1 < my) ws_load_a<N, K>(sA0 + p * S::A_BYTES, A, tile_m0(i + 1), tid);
         cp_async_commit();
-        ws_epilogue_any<N, K>(ep, tmem + lane_off + (uint32_t)(p * N), (long long)tile_m0(i - 1) + (warp & 3) * 32,
-                              col0, stage, lane);
+        ws_epilogue_staged<N, K, MODE>(ep, tmem + lane_off + (uint32_t)(p * N),
+                                       (long long)tile_m0(i - 1) + (warp & 3) * 32, col0, stage, lane);
         asm volatile("tcgen05.fence::before_thread_sync;" ::);
         __syncthreads();
     }
@@ -549,8 +489,8 @@ __global__ void __launch_bounds__(WS_THREADS, 2) k_gemm_ws(const __nv_bfloat16* 
             ph ^= 1u << s;
             ++waited;
             asm volatile("tcgen05.fence::after_thread_sync;" ::);
-            ws_epilogue_any<N, K>(ep, tmem + lane_off + (uint32_t)(s * N), (long long)tile_m0(my - 1) + (warp & 3) * 32,
-                                  col0, stage, lane);
+            ws_epilogue_staged<N, K, MODE>(ep, tmem + lane_off + (uint32_t)(s * N),
+                                           (long long)tile_m0(my - 1) + (warp & 3) * 32, col0, stage, lane);
         }
     }
     if (!ok) {
@@ -569,14 +509,14 @@ __global__ void __launch_bounds__(WS_THREADS, 2) k_gemm_ws(const __nv_bfloat16* 
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(S::TCOLS));
 }
 
-template <int N, int K>
-int launch_ws(const __nv_bfloat16* A, const __nv_bfloat16* B, int M, const SphgGemmEpi& ep, int* err,
-              cudaStream_t s) {
+template <int N, int K, int MODE>
+int launch_ws_mode(const __nv_bfloat16* A, const __nv_bfloat16* B, int M, const SphgGemmEpi& ep, int* err,
+                   cudaStream_t s) {
     typedef WsShape<N, K> S;
     static bool configured = false;
     if (!configured) {
-        if (cudaFuncSetAttribute(k_gemm_ws<N, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM_REQ) !=
-            cudaSuccess)
+        if (cudaFuncSetAttribute(k_gemm_ws<N, K, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)S::SMEM_REQ) != cudaSuccess)
             return SPHG_ERR_CUDA;
         configured = true;
     }
@@ -585,8 +525,21 @@ int launch_ws(const __nv_bfloat16* A, const __nv_bfloat16* B, int M, const SphgG
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int ntiles = M / 128;
     const int grid = ntiles < sms * S::PER_SM ? ntiles : sms * S::PER_SM;
-    k_gemm_ws<N, K><<<grid, WS_THREADS, S::SMEM_REQ, s>>>(A, B, M, ep, err);
+    k_gemm_ws<N, K, MODE><<<grid, WS_THREADS, S::SMEM_REQ, s>>>(A, B, M, ep, err);
     return cudaGetLastError() == cudaSuccess ? SPHG_OK : SPHG_ERR_CUDA;
+}
+
+// one kernel per epilogue mode, so that each carries only its mode's registers
+template <int N, int K>
+int launch_ws(const __nv_bfloat16* A, const __nv_bfloat16* B, int M, const SphgGemmEpi& ep, int* err,
+              cudaStream_t s) {
+    switch (ep.mode) {
+        case SPHG_EPI_STORE: return launch_ws_mode<N, K, SPHG_EPI_STORE>(A, B, M, ep, err, s);
+        case SPHG_EPI_ACC: return launch_ws_mode<N, K, SPHG_EPI_ACC>(A, B, M, ep, err, s);
+        case SPHG_EPI_BIAS_ACT: return launch_ws_mode<N, K, SPHG_EPI_BIAS_ACT>(A, B, M, ep, err, s);
+        case SPHG_EPI_EDGE: return launch_ws_mode<N, K, SPHG_EPI_EDGE>(A, B, M, ep, err, s);
+        default: return launch_ws_mode<N, K, SPHG_EPI_RESID>(A, B, M, ep, err, s);
+    }
 }
 
 // ------------------------------------------------------------------------
@@ -610,10 +563,11 @@ int launch_ws(const __nv_bfloat16* A, const __nv_bfloat16* B, int M, const SphgG
 // the kernel sets *err, waits (bounded) for its MMAs, frees TMEM and returns.
 struct EdgeShape {
     static constexpr uint32_t T = 32 * 1024;                  // one 128 x 128 bf16 operand
-    static constexpr uint32_t B1 = 0, B2 = T, A0 = 2 * T, Z = 4 * T;
-    static constexpr uint32_t BAR = 5 * T;                    // 2 mbarriers + TMEM slot
-    static constexpr int THREADS = 512;                       // 16 warps: 4 per TMEM lane quarter
-    static constexpr uint32_t STAGE = BAR + 32;               // 16 warps x 2 KB staging
+    static constexpr int NBUF = 3;                            // tiles in flight: E rows, then the hidden rows
+    static constexpr uint32_t B1 = 0, B2 = T, BUF = 2 * T;
+    static constexpr uint32_t BAR = BUF + NBUF * T;           // mbarriers, TMEM slot, abort flag
+    static constexpr int THREADS = 512;                       // two groups of 8 warps
+    static constexpr uint32_t STAGE = BAR + 128;              // 16 warps x 2 KB staging
     static constexpr uint32_t SMEM = STAGE + (THREADS / 32) * 32 * 64;
 };
 
@@ -643,19 +597,50 @@ __device__ __forceinline__ void mma_128x128(uint32_t tacc, const uint8_t* sA, co
                  : "memory");
 }
 
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// barrier of one 256-thread group (named barrier id) that also ANDs `ok` over the group
+__device__ __forceinline__ bool group_and(int id, bool ok) {
+    uint32_t r;
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.u32 p, %1, 0;\n\tbar.red.and.pred p, %2, 256, p;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(r) : "r"(ok ? 1u : 0u), "r"(id) : "memory");
+    return r != 0;
+}
+
+// The layer as a two-stage pipeline over the CTA's tiles.  Warps 0-7 (group
+// 1) run the EDGE epilogue of tile i from the first accumulator into the
+// tile's buffer (its E rows are no longer needed once the first MMA has read
+// them), and thread 0 issues the MMAs: the second MMA of tile i, then the
+// first of tile i + 1.  Warps 8-15 (group 2) meanwhile run the RESID
+// epilogue of tile i - 1 from the second accumulator, and load the E rows of
+// tile i + 2 into the buffer that tile i - 1 has freed (NBUF = 3 buffers).
+// mbarriers: mma[0] / mma[1] each MMA group's completion (tcgen05.commit),
+// acc2 the second accumulator read out (group 2), buf[b] the E rows of the
+// next tile of buffer b in shared memory (the 256 threads of group 2).
+// Every wait is bounded; a group that gives up sets *err and the abort flag,
+// and both groups leave their loops at the next wait.
 __global__ void __launch_bounds__(EdgeShape::THREADS, 1) k_edge_layer(const __nv_bfloat16* __restrict__ E, int M,
                                                                const __nv_bfloat16* __restrict__ We,
                                                                const __nv_bfloat16* __restrict__ W2,
-                                                               SphgGemmEpi e1, SphgGemmEpi e2, int* __restrict__ err) {
+                                                               SphgGemmEpi e1, SphgGemmEpi e2,
+                                                               int* __restrict__ err) {
     typedef EdgeShape S;
     extern __shared__ __align__(128) uint8_t smem[];
-    uint64_t* mbar = (uint64_t*)(smem + S::BAR);
-    uint32_t* tslot = (uint32_t*)(mbar + 2);
+    uint64_t* bar_mma = (uint64_t*)(smem + S::BAR);      // [2]
+    uint64_t* bar_acc2 = bar_mma + 2;
+    uint64_t* bar_buf = bar_mma + 3;                     // [NBUF]
+    uint32_t* tslot = (uint32_t*)(bar_mma + 3 + S::NBUF);
+    volatile int* abort_flag = (volatile int*)(tslot + 1);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const bool g1 = warp < 8;
     float4* stage = reinterpret_cast<float4*>(smem + S::STAGE) + warp * 128;
     const int ntiles = M / 128;
     const int my = blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
     auto tile_m0 = [&](int i) { return ((int)blockIdx.x + i * (int)gridDim.x) * 128; };
+    auto buf = [&](int i) { return smem + S::BUF + (i % S::NBUF) * S::T; };
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
@@ -663,69 +648,105 @@ __global__ void __launch_bounds__(EdgeShape::THREADS, 1) k_edge_layer(const __nv
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
     }
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mbar)), "r"(1));
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mbar + 1)), "r"(1));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar_mma)), "r"(1));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar_mma + 1)), "r"(1));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar_acc2)), "r"(1));
+        for (int b = 0; b < S::NBUF; ++b)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar_buf + b)), "r"(256));
         asm volatile("fence.mbarrier_init.release.cluster;" ::);
+        *abort_flag = 0;
     }
     load_b128<S::THREADS>(smem + S::B1, We, tid);
     load_b128<S::THREADS>(smem + S::B2, W2, tid);
-    if (my > 0) ws_load_a<128, 128, S::THREADS>(smem + S::A0, E, tile_m0(0), tid);
-    cp_async_commit();
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;" ::);
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::);
     const uint32_t tmem = *tslot;
     const uint32_t lane_off = (uint32_t)((warp & 3) * 32) << 16;
-    const int col0 = (warp >> 2) * 32;   // this warp's 32 of the 128 columns
-    uint32_t ph = 0u;        // bit b: parity of the next completion of mbar[b]
-    int wb = -1;             // the barrier of the MMA group being waited for
-    bool ok = true;
-    for (int i = 0; i < my && ok; ++i) {
-        const int s = i & 1;
-        const long long row0 = (long long)tile_m0(i) + (warp & 3) * 32;
+    const int col0 = ((warp & 7) >> 2) * 64;    // this warp's half of the 128 columns
+    const int gt = tid & 255;                    // thread index within the group
+    int issued1 = 0, issued2 = 0;                // MMA groups issued by thread 0
+
+    if (g1) {
+        bool ok = true;
+        for (int i = 0; i < my && ok; ++i) {
+            if (tid == 0 && i == 0) {
+                if (mbar_wait(smem_u32(bar_buf), 0u, kWaitLimit)) {
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::);
+                    mma_128x128(tmem, buf(0), smem + S::B1, bar_mma);
+                    ++issued1;
+                } else {
+                    atomicExch(err, 1);
+                    *abort_flag = 1;
+                }
+            }
+            const bool done = !*abort_flag && mbar_wait(smem_u32(bar_mma), (uint32_t)(i & 1), kWaitLimit);
+            ok = group_and(1, done);
+            if (!ok) break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::);
+            ws_epilogue_staged<128, 128, SPHG_EPI_EDGE>(e1, tmem + lane_off, (long long)tile_m0(i) + (warp & 3) * 32, col0, stage,
+                                         lane, buf(i), (warp & 3) * 32);
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            asm volatile("tcgen05.fence::before_thread_sync;" ::);
+            group_and(1, true);
+            if (tid == 0) {
+                asm volatile("tcgen05.fence::after_thread_sync;" ::);
+                // the second accumulator is free once group 2 has read out tile i - 1
+                bool w = i == 0 || mbar_wait(smem_u32(bar_acc2), (uint32_t)((i - 1) & 1), kWaitLimit);
+                if (w) {
+                    mma_128x128(tmem + 128u, buf(i), smem + S::B2, bar_mma + 1);
+                    ++issued2;
+                }
+                if (w && i + 1 < my) {
+                    w = mbar_wait(smem_u32(bar_buf + (i + 1) % S::NBUF), (uint32_t)(((i + 1) / S::NBUF) & 1),
+                                  kWaitLimit);
+                    if (w) {
+                        asm volatile("tcgen05.fence::after_thread_sync;" ::);
+                        mma_128x128(tmem, buf(i + 1), smem + S::B1, bar_mma);
+                        ++issued1;
+                    }
+                }
+                if (!w) { atomicExch(err, 1); *abort_flag = 1; }   // the group leaves at its next wait
+            }
+        }
+        if (!ok && tid == 0) { atomicExch(err, 1); *abort_flag = 1; }
+    } else {
+        bool ok = true;
+        // the first tiles' E rows
+        for (int j = 0; j < S::NBUF && j < my; ++j) ws_load_a<128, 128, 256>(buf(j), E, tile_m0(j), gt);
+        cp_async_commit();
         cp_async_wait_all();
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
-        if (tid == 0) {
+        for (int j = 0; j < S::NBUF && j < my; ++j) mbar_arrive(bar_buf + j);
+        for (int i = 0; i < my && ok; ++i) {
+            const bool done = !*abort_flag && mbar_wait(smem_u32(bar_mma + 1), (uint32_t)(i & 1), kWaitLimit);
+            ok = group_and(2, done);
+            if (!ok) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::);
-            mma_128x128(tmem, smem + S::A0 + s * S::T, smem + S::B1, mbar);
+            // both MMAs of tile i are done: its buffer takes the E rows of tile i + NBUF
+            const bool more = i + S::NBUF < my;
+            if (more) ws_load_a<128, 128, 256>(buf(i), E, tile_m0(i + S::NBUF), gt);
+            cp_async_commit();
+            // the residual is EF (e2.z) or, without it, tile i's bf16 E rows
+            ws_epilogue_staged<128, 128, SPHG_EPI_RESID>(e2, tmem + lane_off + 128u, (long long)tile_m0(i) + (warp & 3) * 32, col0,
+                                         stage, lane, nullptr, 0, 64, E);
+            asm volatile("tcgen05.fence::before_thread_sync;" ::);
+            group_and(2, true);
+            if (gt == 0) mbar_arrive(bar_acc2);
+            if (more) {
+                cp_async_wait_all();
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                mbar_arrive(bar_buf + i % S::NBUF);
+            }
         }
-        wb = 0;
-        // the other E buffer was last read by the previous tile's first MMA, seen complete
-        if (i + 1 < my) ws_load_a<128, 128, S::THREADS>(smem + S::A0 + (s ^ 1) * S::T, E, tile_m0(i + 1), tid);
-        cp_async_commit();
-        bool done = mbar_wait(smem_u32(mbar), ph & 1u, kWaitLimit);
-        ok = __syncthreads_and(done ? 1 : 0) != 0;
-        if (!ok) break;
-        ph ^= 1u;
-        wb = -1;
-        asm volatile("tcgen05.fence::after_thread_sync;" ::);
-        ws_epilogue_staged<128, 128>(e1, tmem + lane_off, row0, col0, stage, lane, smem + S::Z, (warp & 3) * 32, 32);
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        asm volatile("tcgen05.fence::before_thread_sync;" ::);
-        __syncthreads();
-        if (tid == 0) {
-            asm volatile("tcgen05.fence::after_thread_sync;" ::);
-            mma_128x128(tmem + 128u, smem + S::Z, smem + S::B2, mbar + 1);
-        }
-        wb = 1;
-        done = mbar_wait(smem_u32(mbar + 1), (ph >> 1) & 1u, kWaitLimit);
-        ok = __syncthreads_and(done ? 1 : 0) != 0;
-        if (!ok) break;
-        ph ^= 2u;
-        wb = -1;
-        asm volatile("tcgen05.fence::after_thread_sync;" ::);
-        // without EF the residual is this tile's E rows, still in shared memory
-        ws_epilogue_staged<128, 128>(e2, tmem + lane_off + 128u, row0, col0, stage, lane, nullptr, (warp & 3) * 32, 32,
-                                     smem + S::A0 + s * S::T);
-        asm volatile("tcgen05.fence::before_thread_sync;" ::);
+        cp_async_wait_all();
+        if (!ok && gt == 0) { atomicExch(err, 1); *abort_flag = 1; }
     }
-    if (!ok) {
-        if (tid == 0) atomicExch(err, 1);
-        // the MMA group whose wait ran out (bounded)
-        if (wb >= 0) mbar_wait(smem_u32(mbar + wb), (ph >> wb) & 1u, kWaitLimit);
+    if (tid == 0 && *abort_flag) {   // bounded waits for the MMA groups issued and not seen complete
+        if (issued1 > 0) mbar_wait(smem_u32(bar_mma), (uint32_t)((issued1 - 1) & 1), kWaitLimit);
+        if (issued2 > 0) mbar_wait(smem_u32(bar_mma + 1), (uint32_t)((issued2 - 1) & 1), kWaitLimit);
     }
-    cp_async_wait_all();
     asm volatile("tcgen05.fence::before_thread_sync;" ::);
     __syncthreads();
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256));

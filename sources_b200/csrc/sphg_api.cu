@@ -293,6 +293,7 @@ struct Engine : EngineBase {
     }
 
     int set_tuning(const sphg_tuning* t) override {
+        cells_ready = false;
         if (!t || !(t->cell_factor >= 1.0) || t->cell_factor > 4.0 || t->reorder_interval < 0) return SPHG_ERR_BAD_ARG;
         if (t->x_split < 0 || t->x_split > 8) return SPHG_ERR_BAD_ARG;
         cell_factor = t->cell_factor;
@@ -366,6 +367,7 @@ struct Engine : EngineBase {
     }
 
     int upload(int phase, const sphg_phase_host* h) override {
+        cells_ready = false;
         if (phase < 1 || phase > ctx->nphase || !h) return SPHG_ERR_BAD_ARG;
         if (!h->x || !h->vx || !h->rho || !h->p || !h->c || !h->mass || !h->hsml || !h->itype) return SPHG_ERR_BAD_ARG;
         int n = h->ntotal + h->nvirt;
@@ -539,6 +541,7 @@ struct Engine : EngineBase {
         if (rc0) return rc0;
         prepared = true;
         // spatial order from the start
+        cells_ready = false;
         for (int ph = 0; ph < ctx->nphase; ++ph) {
             int rc = build_cells(ph);
             if (rc) return rc;
@@ -547,12 +550,30 @@ struct Engine : EngineBase {
         return 0;
     }
 
-    int build_cells(int ph) {
+    // The cell keys, ranks and per-cell counts of the current positions: made
+    // by the previous step's corrector (cells_ready), else counted here.
+    bool cells_ready = false;
+    int count_cells(int ph, int next) {
         PhaseDev<T>& D = P[ph];
         CUDA_TRY(cudaMemsetAsync(counts[ph], 0, sizeof(int) * ((size_t)ncell + 1), ctx->stream));
-        int rc = launch_pdl("cell_count", k_cell_count, blocks(D.n, 256), 256, 0, (const double2*)D.x, D.n, grid,
-                            D.cell_id, D.cell_fill, counts[ph], cnt);
-        if (rc) return rc;
+        return launch_pdl("cell_count", k_cell_count, blocks(D.n, 256), 256, 0, (const double2*)D.x, D.n, grid,
+                          D.cell_id, D.cell_fill, counts[ph], cnt, next);
+    }
+    // Count the current positions' cells as a corrector would have, so that a
+    // captured step (which expects them) can run.
+    int prime_cells() {
+        if (cells_ready) return 0;
+        for (int ph = 0; ph < ctx->nphase; ++ph) {
+            int rc = count_cells(ph, 1);
+            if (rc) return rc;
+        }
+        cells_ready = true;
+        return 0;
+    }
+    int build_cells(int ph) {
+        PhaseDev<T>& D = P[ph];
+        int rc = 0;
+        if (!cells_ready && (rc = count_cells(ph, 0))) return rc;
         size_t bytes = cub_bytes;
         CUDA_TRY(cub::DeviceScan::ExclusiveSum(ph == 1 && cub_tmp1 ? cub_tmp1 : cub_tmp, bytes, counts[ph], D.cell_start,
                                                ncell + 1, ctx->stream));
@@ -560,7 +581,7 @@ struct Engine : EngineBase {
                              (const int*)D.cell_fill, (const int*)D.cell_start, D.perm)))
             return rc;
         return launch_pdl("cell_sort", k_cell_sort, blocks(ncell, 256), 256, 0, ncell, (const int*)D.cell_start,
-                          (const int*)D.orig, D.perm);
+                          (const int*)D.orig, D.perm, counts[ph]);
     }
 
     // The persistent per-particle fields of a phase and their element sizes.
@@ -620,7 +641,7 @@ struct Engine : EngineBase {
     }
 
     // -------------------------------------------------------------- the step
-    int reset_counters() { return launch_pdl("reset", k_reset_counters, 1, 32, 0, cnt); }
+    int reset_counters() { return launch_pdl("reset", k_reset_counters, 1, 32, 0, cnt, cells_ready ? 1 : 0); }
 
     // The pair passes of one step for kernel function SKF.  fh: run the
     // leapfrog predictor inside the gathers; u: what the last pass of each
@@ -628,6 +649,7 @@ struct Engine : EngineBase {
     template <int SKF>
     int passes(int fh, StepCtl u) {
         const sphg_params& p = ctx->prm;
+        u.ncount = nullptr;   // set per phase: the corrector counts that phase's next cells
         const int tpb = SPHG_TPB;
         const int dp = sim.yield_dp;
         int rc;
@@ -637,11 +659,14 @@ struct Engine : EngineBase {
                 if ((rc = launch_pdl("gather", k_gather<T>, blocks(D.n, 256), 256, 0, D, sim, 0, 0, fh, 0, 0, cnt))) return rc;
                 if ((rc = launch_pdl("water_sum", k_water_sum<T, SKF>, blocks(D.n, tpb), tpb, 0, D, grid, sc_same, sim, cnt))) return rc;
                 if ((rc = launch_pdl("water_pass_a", k_water_pass_a<T, SKF, true>, blocks(D.n, tpb), tpb, 0, D, grid, sc_same, sim, cnt))) return rc;
+                StepCtl uw = u;
+                uw.ncount = u.update ? counts[0] : nullptr;
                 if ((rc = launch_pdl("water_pass_b", k_water_pass_b<T, SKF, true, false>, blocks(D.n, tpb), tpb, 0, D, D, grid, sc_same,
-                                 sc_same, sim, u, cnt))) return rc;
+                                 sc_same, sim, uw, cnt))) return rc;
             } else {
                 if ((rc = launch_pdl("gather", k_gather<T>, blocks(D.n, 256), 256, 0, D, sim, 1, dp, fh, 0, dp, cnt))) return rc;
                 StepCtl us = u; us.with_vof = 0; us.do_dp = dp;
+                us.ncount = u.update ? counts[0] : nullptr;
                 if ((rc = launch_pdl("soil_pass", k_soil_pass<T, SKF, true, false>, blocks(D.n, tpb), tpb, 0, D, D, grid, sc_same, sc_same,
                                  sim, cnt, 0, us))) return rc;
             }
@@ -650,6 +675,8 @@ struct Engine : EngineBase {
             PhaseDev<T>& S = P[1];
             StepCtl uw = u; uw.with_vof = 1; uw.do_dp = 0;
             StepCtl us = u; us.with_vof = 1; us.do_dp = dp;
+            uw.ncount = u.update ? counts[0] : nullptr;
+            us.ncount = u.update ? counts[1] : nullptr;
             // the soil's gather was launched by run() on the side stream
             if ((rc = launch_pdl("gather", k_gather<T>, blocks(W.n, 256), 256, 0, W, sim, 0, 0, fh, 1, 0, cnt))) return rc;
             if ((rc = launch_pdl("water_pass_a", k_water_pass_a<T, SKF, false>, blocks(W.n, tpb), tpb,
@@ -720,7 +747,10 @@ struct Engine : EngineBase {
         if (itimestep < 2 || !use_graphs || ctx->prof.on) return -1;
         return graph_index(itimestep);
     }
-    int prepare_graph_step() override { return prepare(); }
+    int prepare_graph_step() override {
+        int rc = prepare();
+        return rc ? rc : prime_cells();
+    }
     // Record the step into the stream being captured.  The host's buffer
     // sets are left as before the step: they change when the graph is
     // launched (after_graph_step).
@@ -759,6 +789,7 @@ struct Engine : EngineBase {
     int step_graphed(int itimestep) {
         int rc = prepare();
         if (rc) return rc;
+        if ((rc = prime_cells())) return rc;   // a captured step expects the cells counted
         const int kind = graph_index(itimestep);
         if (!graphs[kind]) {
             cudaGraph_t g = nullptr;
@@ -792,6 +823,11 @@ struct Engine : EngineBase {
     long long launches_per_graph[NGRAPH] = {};
 
     int run(int itimestep, int fh, StepCtl u) {
+        const int rc = run_step(itimestep, fh, u);
+        if (rc) cells_ready = false;
+        return rc;
+    }
+    int run_step(int itimestep, int fh, StepCtl u) {
         int rc = prepare();
         if (rc) return rc;
         make_sim(itimestep);
@@ -834,6 +870,8 @@ struct Engine : EngineBase {
             case 3: rc = passes<3>(fh, u); break;
             default: rc = passes<4>(fh, u); break;
         }
+        // a step with the corrector has counted the next step's cells
+        cells_ready = rc == 0 && u.update != 0;
         if (rc) return rc;
         return launch_pdl("check", k_check, 1, 32, 0, (const DevCounters*)cnt, sticky, (unsigned long long)p.max_interaction);
     }
@@ -904,6 +942,7 @@ struct Engine : EngineBase {
         double* state[2] = {(double*)D.x, (double*)D.v};
         double* user[2] = {x, v};
         int rc = 0;
+        if (!to_caller && x) cells_ready = false;   // new positions
         for (int f = 0; f < 2; ++f) {
             if (!user[f]) continue;
             if (to_caller)
@@ -1004,9 +1043,13 @@ struct Engine : EngineBase {
         // the lists of the current positions (the last step's pair search if no
         // step ran since): rebuild sorted positions for both phases
         for (int ph = 0; ph < ctx->nphase; ++ph) {
-            if ((rc = build_cells(ph))) return rc;
-            if ((rc = launch("gather", k_gather<T>, blocks(P[ph].n, 256), 256, P[ph], sim, 0, 0, 0, 0, 0, cnt))) return rc;
+            if ((rc = build_cells(ph))) { cells_ready = false; return rc; }
+            if ((rc = launch("gather", k_gather<T>, blocks(P[ph].n, 256), 256, P[ph], sim, 0, 0, 0, 0, 0, cnt))) {
+                cells_ready = false;
+                return rc;
+            }
         }
+        cells_ready = false;   // the counts were consumed
         int n = A.n;
         int* count = stage_i;
         long long* off = stage_l;

@@ -74,6 +74,7 @@ struct DevCounters {
     int nonfinite;                   // NaN/Inf positions met
     int overflow;                    // a pair list exceeded max_interaction
     int timeout;                     // blocks whose bounded staging wait ran out
+    int n_out_next, nonfinite_next;  // the same, of the positions the corrector wrote for the next step
 };
 
 template <typename T>

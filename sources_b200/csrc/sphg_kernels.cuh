@@ -93,21 +93,27 @@ __device__ __forceinline__ void pdl_enter() {
 }
 
 // ----------------------------------------------------------------- cell list
-// cell key (row-major) and the particle's rank inside its cell.
+// Cell key (row-major) of a particle at p and its rank inside its cell; the
+// clamped and non-finite positions are counted into the step's counters, or
+// into the next step's (next != 0).
+__device__ __forceinline__ void cell_key(const GridGeom& g, double2 p, int a, int* __restrict__ cell_id,
+                                         int* __restrict__ rank, int* __restrict__ counts, DevCounters* cnt, int next) {
+    int cx, cy; bool clamped;
+    cell_coords(g, p.x, p.y, cx, cy, clamped);
+    if (clamped) atomicAdd(next ? &cnt->n_out_next : &cnt->n_out, 1);
+    if (!(isfinite(p.x) && isfinite(p.y))) atomicAdd(next ? &cnt->nonfinite_next : &cnt->nonfinite, 1);
+    const int c = cy * g.ncx + cx;
+    cell_id[a] = c;
+    rank[a] = atomicAdd(counts + c, 1);
+}
+
 static __global__ void __launch_bounds__(256) k_cell_count(const double2* __restrict__ x, int n, GridGeom g,
                                                     int* __restrict__ cell_id, int* __restrict__ rank,
-                                                    int* __restrict__ counts, DevCounters* cnt) {
+                                                    int* __restrict__ counts, DevCounters* cnt, int next) {
     pdl_enter();
     int a = gtid();
     if (a >= n) return;
-    double2 p = x[a];
-    int cx, cy; bool clamped;
-    cell_coords(g, p.x, p.y, cx, cy, clamped);
-    if (clamped) atomicAdd(&cnt->n_out, 1);
-    if (!(isfinite(p.x) && isfinite(p.y))) atomicAdd(&cnt->nonfinite, 1);
-    int c = cy * g.ncx + cx;
-    cell_id[a] = c;
-    rank[a] = atomicAdd(counts + c, 1);
+    cell_key(g, x[a], a, cell_id, rank, counts, cnt, next);
 }
 
 static __global__ void __launch_bounds__(256) k_cell_scatter(int n, const int* __restrict__ cell_id, const int* __restrict__ rank,
@@ -121,11 +127,15 @@ static __global__ void __launch_bounds__(256) k_cell_scatter(int n, const int* _
 // Insertion sort of each cell's (few) entries by original particle index, so
 // the visiting order, and with it every sum, depends neither on atomic timing
 // nor on the current state order (a download/upload restart is bit-identical).
+// The cell's count, consumed by the scan, is reset to zero for the corrector,
+// which counts the next step's cells.
 static __global__ void __launch_bounds__(256) k_cell_sort(int ncell, const int* __restrict__ cell_start,
-                                                   const int* __restrict__ orig, int* __restrict__ perm) {
+                                                   const int* __restrict__ orig, int* __restrict__ perm,
+                                                   int* __restrict__ counts) {
     pdl_enter();
     int c = gtid();
     if (c >= ncell) return;
+    counts[c] = 0;
     int b = cell_start[c], e = cell_start[c + 1];
     for (int i = b + 1; i < e; ++i) {
         int v = perm[i], ov = orig[v], j = i - 1;
@@ -142,6 +152,8 @@ struct StepCtl {
     int first;       // itimestep == 1: first_step
     int with_vof;    // integrate the water volume fraction (two-phase)
     int do_dp;       // Drucker-Prager after the corrector (soil)
+    int* ncount;     // non-null: after the corrector, the cell key and rank of the new position, counted
+                     // into this phase's per-cell counts for the next step's cell list
 };
 
 // first_half, declarations_sph.f90:643-684 (and :812-825, :998-1025), plus the
@@ -652,6 +664,7 @@ __global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_B : 1) k_
             T2 o; o.x = dvx; o.y = dvy;
             P.dv[a] = o;
             if (u.update) update_one(P, a, c, u.first, 0, 0);   // last pass of the water-only step
+            if (u.ncount) cell_key(g, P.x[a], a, P.cell_id, P.cell_fill, u.ncount, cnt, 1);
         }
     } else {
         T cdx = 0, cdy = 0, cdvof = 0, cv2 = 0;
@@ -675,6 +688,7 @@ __global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_B : 1) k_
             }
             P.countiac[a] = chits;
             if (u.update) update_one(P, a, c, u.first, u.with_vof, 0);   // last pass of the water phase
+            if (u.ncount) cell_key(g, P.x[a], a, P.cell_id, P.cell_fill, u.ncount, cnt, 1);
         }
         count_stats(cnt, 2, -1, chits, valid);
     }
@@ -851,6 +865,7 @@ __global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_SOIL : 1)
         P.vcc[a] = vcc;
         P.countiac[a] = hits;
         if (SINGLE && u.update) fail3 = update_one(P, a, c, u.first, 0, u.do_dp);   // last pass of the soil-only step
+        if (SINGLE && u.ncount) cell_key(g, P.x[a], a, P.cell_id, P.cell_fill, u.ncount, cnt, 1);
     }
     if constexpr (!SINGLE) {
         T cdx = 0, cdy = 0, cpx = 0, cpy = 0;
@@ -863,6 +878,7 @@ __global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_SOIL : 1)
             P.dv[a] = o;
             if (c.volume_fraction) P.vof[a] = P.rho[a] / c.s_rho0;
             if (u.update) fail3 = update_one(P, a, c, u.first, u.with_vof, u.do_dp);   // last pass of the soil phase
+            if (u.ncount) cell_key(g, P.x[a], a, P.cell_id, P.cell_fill, u.ncount, cnt, 1);
         }
     }
     count_stats(cnt, slot, slot, hits, valid);
@@ -887,13 +903,20 @@ static __global__ void k_check(const DevCounters* __restrict__ c, int* __restric
 struct PermField { const void* src; void* dst; int bytes; int pad; };
 struct PermList { int count; int pad; PermField f[44]; };
 // Per-step counters to their initial values (a kernel, so that it can live in a graph).
-static __global__ void k_reset_counters(DevCounters* c) {
+// take_next: the step's cell keys were counted by the previous step's
+// corrector, with its clamped and non-finite positions.
+static __global__ void k_reset_counters(DevCounters* c, int take_next) {
     pdl_enter();
     int i = threadIdx.x;
     if (i < 3) c->pairs[i] = 0ull;
     if (i < 2) { c->maxiac[i] = 0; c->miniac[i] = 0x7fffffff; c->noiac[i] = 0; }
     if (i < 4) c->nfail[i] = 0;
-    if (i == 0) { c->n_out = 0; c->nonfinite = 0; c->overflow = 0; c->timeout = 0; }
+    if (i == 0) {
+        c->n_out = take_next ? c->n_out_next : 0;
+        c->nonfinite = take_next ? c->nonfinite_next : 0;
+        c->n_out_next = 0; c->nonfinite_next = 0;
+        c->overflow = 0; c->timeout = 0;
+    }
 }
 
 static __global__ void __launch_bounds__(256) k_permute_all(int n, const int* __restrict__ perm, PermList L) {

@@ -228,10 +228,10 @@ extern "C" int sphg_sum_density_noalloc(const sphg_params* p, int32_t n, const d
     k_na_zero<<<(ncell + 1 + 255) / 256, 256, 0, s>>>(counts, ncell + 1);
     k_na_zero<<<1, 256, 0, s>>>((int*)cnt, (int)(sizeof(DevCounters) / sizeof(int)));
     k_iota<<<(n + 255) / 256, 256, 0, s>>>(n, D.orig);
-    k_cell_count<<<(n + 255) / 256, 256, 0, s>>>((const double2*)x, n, g, D.cell_id, D.cell_fill, counts, cnt);
+    k_cell_count<<<(n + 255) / 256, 256, 0, s>>>((const double2*)x, n, g, D.cell_id, D.cell_fill, counts, cnt, 0);
     k_na_scan<<<1, 1024, 0, s>>>(counts, D.cell_start, ncell + 1);
     k_cell_scatter<<<(n + 255) / 256, 256, 0, s>>>(n, D.cell_id, D.cell_fill, D.cell_start, D.perm);
-    k_cell_sort<<<(ncell + 255) / 256, 256, 0, s>>>(ncell, D.cell_start, D.orig, D.perm);
+    k_cell_sort<<<(ncell + 255) / 256, 256, 0, s>>>(ncell, D.cell_start, D.orig, D.perm, counts);
     k_na_gather<<<(n + 255) / 256, 256, 0, s>>>(n, D.perm, (const double2*)x, hsml, mass, rho, D.xs, D.hs, D.recA);
     SimConst c;
     memset(&c, 0, sizeof(c));

@@ -613,15 +613,17 @@ __device__ __forceinline__ bool group_and(int id, bool ok) {
 // The layer as a two-stage pipeline over the CTA's tiles.  Warps 0-7 (group
 // 1) run the EDGE epilogue of tile i from the first accumulator into the
 // tile's buffer (its E rows are no longer needed once the first MMA has read
-// them), and thread 0 issues the MMAs: the second MMA of tile i, then the
-// first of tile i + 1.  Warps 8-15 (group 2) meanwhile run the RESID
-// epilogue of tile i - 1 from the second accumulator, and load the E rows of
-// tile i + 2 into the buffer that tile i - 1 has freed (NBUF = 3 buffers).
-// mbarriers: mma[0] / mma[1] each MMA group's completion (tcgen05.commit),
-// acc2 the second accumulator read out (group 2), buf[b] the E rows of the
-// next tile of buffer b in shared memory (the 256 threads of group 2).
-// Every wait is bounded; a group that gives up sets *err and the abort flag,
-// and both groups leave their loops at the next wait.
+// them); their thread 0 then issues the first MMA of tile i + 1.  Warps 8-15
+// (group 2) issue the second MMA of tile i once its hidden rows are in
+// place, run the RESID epilogue from the second accumulator, and load the E
+// rows of tile i + NBUF into the buffer that tile i has freed (NBUF = 3).  So
+// group 1 works on tile i + 1 while group 2 finishes tile i, and neither
+// waits for the other's epilogue.  mbarriers: mma[0] / mma[1] each MMA
+// group's completion (tcgen05.commit), z[b] the hidden rows of buffer b's
+// tile written (group 1), buf[b] the E rows of buffer b's next tile loaded
+// (the 256 threads of group 2); per buffer, so that no waiter can fall two
+// phases behind its barrier.  Every wait is bounded; a group that gives up sets
+// *err and the abort flag, and both groups leave their loops at the next wait.
 __global__ void __launch_bounds__(EdgeShape::THREADS, 1) k_edge_layer(const __nv_bfloat16* __restrict__ E, int M,
                                                                const __nv_bfloat16* __restrict__ We,
                                                                const __nv_bfloat16* __restrict__ W2,
@@ -630,9 +632,9 @@ __global__ void __launch_bounds__(EdgeShape::THREADS, 1) k_edge_layer(const __nv
     typedef EdgeShape S;
     extern __shared__ __align__(128) uint8_t smem[];
     uint64_t* bar_mma = (uint64_t*)(smem + S::BAR);      // [2]
-    uint64_t* bar_acc2 = bar_mma + 2;
-    uint64_t* bar_buf = bar_mma + 3;                     // [NBUF]
-    uint32_t* tslot = (uint32_t*)(bar_mma + 3 + S::NBUF);
+    uint64_t* bar_z = bar_mma + 2;                       // [NBUF]
+    uint64_t* bar_buf = bar_z + S::NBUF;                 // [NBUF]
+    uint32_t* tslot = (uint32_t*)(bar_buf + S::NBUF);
     volatile int* abort_flag = (volatile int*)(tslot + 1);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const bool g1 = warp < 8;
@@ -650,9 +652,10 @@ __global__ void __launch_bounds__(EdgeShape::THREADS, 1) k_edge_layer(const __nv
     if (tid == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar_mma)), "r"(1));
         asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar_mma + 1)), "r"(1));
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar_acc2)), "r"(1));
-        for (int b = 0; b < S::NBUF; ++b)
+        for (int b = 0; b < S::NBUF; ++b) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar_z + b)), "r"(1));
             asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar_buf + b)), "r"(256));
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::);
         *abort_flag = 0;
     }
@@ -666,7 +669,8 @@ __global__ void __launch_bounds__(EdgeShape::THREADS, 1) k_edge_layer(const __nv
     const uint32_t lane_off = (uint32_t)((warp & 3) * 32) << 16;
     const int col0 = ((warp & 7) >> 2) * 64;    // this warp's half of the 128 columns
     const int gt = tid & 255;                    // thread index within the group
-    int issued1 = 0, issued2 = 0;                // MMA groups issued by thread 0
+    int issued = 0;                              // MMA groups issued by this thread (thread 0 or 256)
+    auto fail = [&]() { atomicExch(err, 1); *abort_flag = 1; };
 
     if (g1) {
         bool ok = true;
@@ -675,42 +679,35 @@ __global__ void __launch_bounds__(EdgeShape::THREADS, 1) k_edge_layer(const __nv
                 if (mbar_wait(smem_u32(bar_buf), 0u, kWaitLimit)) {
                     asm volatile("tcgen05.fence::after_thread_sync;" ::);
                     mma_128x128(tmem, buf(0), smem + S::B1, bar_mma);
-                    ++issued1;
+                    ++issued;
                 } else {
-                    atomicExch(err, 1);
-                    *abort_flag = 1;
+                    fail();
                 }
             }
             const bool done = !*abort_flag && mbar_wait(smem_u32(bar_mma), (uint32_t)(i & 1), kWaitLimit);
             ok = group_and(1, done);
             if (!ok) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::);
-            ws_epilogue_staged<128, 128, SPHG_EPI_EDGE>(e1, tmem + lane_off, (long long)tile_m0(i) + (warp & 3) * 32, col0, stage,
-                                         lane, buf(i), (warp & 3) * 32);
+            ws_epilogue_staged<128, 128, SPHG_EPI_EDGE>(e1, tmem + lane_off, (long long)tile_m0(i) + (warp & 3) * 32,
+                                                        col0, stage, lane, buf(i), (warp & 3) * 32);
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             asm volatile("tcgen05.fence::before_thread_sync;" ::);
             group_and(1, true);
             if (tid == 0) {
-                asm volatile("tcgen05.fence::after_thread_sync;" ::);
-                // the second accumulator is free once group 2 has read out tile i - 1
-                bool w = i == 0 || mbar_wait(smem_u32(bar_acc2), (uint32_t)((i - 1) & 1), kWaitLimit);
-                if (w) {
-                    mma_128x128(tmem + 128u, buf(i), smem + S::B2, bar_mma + 1);
-                    ++issued2;
-                }
-                if (w && i + 1 < my) {
-                    w = mbar_wait(smem_u32(bar_buf + (i + 1) % S::NBUF), (uint32_t)(((i + 1) / S::NBUF) & 1),
-                                  kWaitLimit);
-                    if (w) {
+                mbar_arrive(bar_z + i % S::NBUF);   // tile i's hidden rows are in its buffer
+                if (i + 1 < my) {
+                    if (mbar_wait(smem_u32(bar_buf + (i + 1) % S::NBUF), (uint32_t)(((i + 1) / S::NBUF) & 1),
+                                  kWaitLimit)) {
                         asm volatile("tcgen05.fence::after_thread_sync;" ::);
                         mma_128x128(tmem, buf(i + 1), smem + S::B1, bar_mma);
-                        ++issued1;
+                        ++issued;
+                    } else {
+                        fail();   // the group leaves at its next wait
                     }
                 }
-                if (!w) { atomicExch(err, 1); *abort_flag = 1; }   // the group leaves at its next wait
             }
         }
-        if (!ok && tid == 0) { atomicExch(err, 1); *abort_flag = 1; }
+        if (!ok && tid == 0) fail();
     } else {
         bool ok = true;
         // the first tiles' E rows
@@ -720,6 +717,15 @@ __global__ void __launch_bounds__(EdgeShape::THREADS, 1) k_edge_layer(const __nv
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         for (int j = 0; j < S::NBUF && j < my; ++j) mbar_arrive(bar_buf + j);
         for (int i = 0; i < my && ok; ++i) {
+            if (gt == 0) {   // the second MMA of tile i, once its hidden rows are in place
+                if (!*abort_flag && mbar_wait(smem_u32(bar_z + i % S::NBUF), (uint32_t)((i / S::NBUF) & 1), kWaitLimit)) {
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::);
+                    mma_128x128(tmem + 128u, buf(i), smem + S::B2, bar_mma + 1);
+                    ++issued;
+                } else {
+                    fail();
+                }
+            }
             const bool done = !*abort_flag && mbar_wait(smem_u32(bar_mma + 1), (uint32_t)(i & 1), kWaitLimit);
             ok = group_and(2, done);
             if (!ok) break;
@@ -729,11 +735,11 @@ __global__ void __launch_bounds__(EdgeShape::THREADS, 1) k_edge_layer(const __nv
             if (more) ws_load_a<128, 128, 256>(buf(i), E, tile_m0(i + S::NBUF), gt);
             cp_async_commit();
             // the residual is EF (e2.z) or, without it, tile i's bf16 E rows
-            ws_epilogue_staged<128, 128, SPHG_EPI_RESID>(e2, tmem + lane_off + 128u, (long long)tile_m0(i) + (warp & 3) * 32, col0,
-                                         stage, lane, nullptr, 0, 64, E);
+            ws_epilogue_staged<128, 128, SPHG_EPI_RESID>(e2, tmem + lane_off + 128u,
+                                                         (long long)tile_m0(i) + (warp & 3) * 32, col0, stage, lane,
+                                                         nullptr, 0, 64, E);
             asm volatile("tcgen05.fence::before_thread_sync;" ::);
-            group_and(2, true);
-            if (gt == 0) mbar_arrive(bar_acc2);
+            group_and(2, true);   // the second accumulator is read out before the next MMA into it
             if (more) {
                 cp_async_wait_all();
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -741,12 +747,10 @@ __global__ void __launch_bounds__(EdgeShape::THREADS, 1) k_edge_layer(const __nv
             }
         }
         cp_async_wait_all();
-        if (!ok && gt == 0) { atomicExch(err, 1); *abort_flag = 1; }
+        if (!ok && gt == 0) fail();
     }
-    if (tid == 0 && *abort_flag) {   // bounded waits for the MMA groups issued and not seen complete
-        if (issued1 > 0) mbar_wait(smem_u32(bar_mma), (uint32_t)((issued1 - 1) & 1), kWaitLimit);
-        if (issued2 > 0) mbar_wait(smem_u32(bar_mma + 1), (uint32_t)((issued2 - 1) & 1), kWaitLimit);
-    }
+    if (*abort_flag && gt == 0 && issued > 0)   // bounded wait for this thread's last MMA group
+        mbar_wait(smem_u32(bar_mma + (g1 ? 0 : 1)), (uint32_t)((issued - 1) & 1), kWaitLimit);
     asm volatile("tcgen05.fence::before_thread_sync;" ::);
     __syncthreads();
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256));

@@ -240,11 +240,16 @@ int sphg_upload_scene_ids(sphg_ctx* ctx, int phase, const int32_t* scene_id);
  * scans 3 rows of 2*x_split+1 cells: finer cells along x test fewer
  * candidates while each row stays one contiguous run of the cell-sorted
  * list.  They change the order in which neighbours are summed, so results
- * agree to rounding, and the pair sets not at all. */
+ * agree to rounding, and the pair sets not at all.  state_order picks the
+ * order the device state is permuted into at each reorder: 0 = the cell
+ * list's own order (rows of cells), 1 = the Morton (Z-order) curve over the
+ * support-radius cells; the neighbour search and every sum are the same
+ * either way (results bit-identical), only the memory layout differs. */
 typedef struct sphg_tuning {
     double cell_factor;
     int32_t reorder_interval;
     int32_t x_split;
+    int32_t state_order;
 } sphg_tuning;
 int sphg_set_tuning(sphg_ctx* ctx, const sphg_tuning* t);
 

@@ -253,8 +253,9 @@ class Solver:
         _check(self.L.sphg_upload_scene_ids(self.h, phase, a.ctypes.data_as(C.POINTER(C.c_int32))),
                "sphg_upload_scene_ids")
 
-    def set_tuning(self, cell_factor: float = 1.0, reorder_interval: int = 10, x_split: int = 0):
-        t = abi.Tuning(cell_factor, reorder_interval, x_split)
+    def set_tuning(self, cell_factor: float = 1.0, reorder_interval: int = 10, x_split: int = 0,
+                   state_order: int = 0):
+        t = abi.Tuning(cell_factor, reorder_interval, x_split, state_order)
         _check(self.L.sphg_set_tuning(self.h, C.byref(t)), "sphg_set_tuning")
 
     def write_tecplot(self, path_first: str, path_second: str | None = None, append: bool = False,

@@ -89,7 +89,8 @@ class SceneRow(C.Structure):
 
 
 class Tuning(C.Structure):
-    _fields_ = [("cell_factor", C.c_double), ("reorder_interval", C.c_int32), ("x_split", C.c_int32)]
+    _fields_ = [("cell_factor", C.c_double), ("reorder_interval", C.c_int32), ("x_split", C.c_int32),
+                ("state_order", C.c_int32)]
 
 
 class Case(C.Structure):

@@ -4,6 +4,7 @@
 // The engine is templated on the pair arithmetic T (double for SPHG_FP64,
 // float for SPHG_FP32).  One context owns one CUDA stream; every launch and
 // copy goes to that stream (or to a stream the caller sets).
+#include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 #include <cuda_runtime.h>
 
@@ -138,6 +139,18 @@ struct Engine : EngineBase {
     bool tab_custom = false;
     double cell_factor = 1.0;       // neighbour cell = factor * support radius (autotuned)
     int x_split = 0;                // x cells per neighbour cell (0: SPHG_X_SPLIT)
+    int state_order = 0;            // order of the state after a reorder: 0 cell list, 1 Morton curve
+    // Morton reorder scratch (state_order 1), one set per phase, since the two
+    // phases' reorders run on two streams at once: keys and slots in and out,
+    // the inverse order, the sort's space
+    struct MortonScratch {
+        unsigned* key[2] = {nullptr, nullptr};
+        int* val[2] = {nullptr, nullptr};
+        int* inv = nullptr;
+        void* tmp = nullptr;
+        size_t tmp_bytes = 0;
+        int n = 0;
+    } morton[2];
     std::vector<void*> allocs;
     SimConst sim{};
     int nfail_slot = 3;             // which DP site the reported nfail comes from
@@ -296,8 +309,10 @@ struct Engine : EngineBase {
         cells_ready = false;
         if (!t || !(t->cell_factor >= 1.0) || t->cell_factor > 4.0 || t->reorder_interval < 0) return SPHG_ERR_BAD_ARG;
         if (t->x_split < 0 || t->x_split > 8) return SPHG_ERR_BAD_ARG;
+        if (t->state_order < 0 || t->state_order > 1) return SPHG_ERR_BAD_ARG;
         cell_factor = t->cell_factor;
         x_split = t->x_split;
+        state_order = t->state_order;
         ctx->prm.reorder_interval = t->reorder_interval;
         prepared = false;
         drop_graphs();
@@ -528,6 +543,22 @@ struct Engine : EngineBase {
             if (alloc((char**)&cub_tmp, cub_bytes)) return SPHG_ERR_CUDA;
         }
         if (ctx->nphase == 2 && !cub_tmp1 && alloc((char**)&cub_tmp1, cub_bytes)) return SPHG_ERR_CUDA;
+        for (int ph = 0; state_order == 1 && ph < ctx->nphase; ++ph) {   // outside any stream capture
+            MortonScratch& M = morton[ph];
+            const int n = P[ph].n;
+            if (M.n >= n) continue;
+            for (int i = 0; i < 2; ++i) { release(M.key[i]); release(M.val[i]); M.key[i] = nullptr; M.val[i] = nullptr; }
+            release(M.inv); release(M.tmp);
+            M.inv = nullptr; M.tmp = nullptr;
+            size_t b = 0;
+            cub::DeviceRadixSort::SortPairs(nullptr, b, (unsigned*)nullptr, (unsigned*)nullptr, (int*)nullptr,
+                                            (int*)nullptr, n, 0, 32, ctx->stream);
+            M.tmp_bytes = b;
+            for (int i = 0; i < 2; ++i)
+                if (alloc(&M.key[i], (size_t)n) || alloc(&M.val[i], (size_t)n)) return SPHG_ERR_CUDA;
+            if (alloc(&M.inv, (size_t)n) || alloc((char**)&M.tmp, M.tmp_bytes)) return SPHG_ERR_CUDA;
+            M.n = n;
+        }
         bool uniform = hmin == hmax;
         double K = sk * hmax;
         sc_same.scale_k = sk; sc_same.uniform = uniform; sc_same.r2_uniform = uniform ? exact_threshold(K) : 0.0;
@@ -624,10 +655,30 @@ struct Engine : EngineBase {
             L.f[i].dst = shadow[ph][i];
             L.f[i].bytes = refs[i].second;
         }
+        if (state_order == 1) return reorder_morton(ph, L);
         int rc = launch_pdl("reorder", k_permute_all, blocks(D.n, 256), 256, 0, D.n, (const int*)D.perm, L);
         if (rc) return rc;
         swap_buffers(ph);
         return launch_pdl("iota", k_iota, blocks(D.n, 256), 256, 0, D.n, D.perm);
+    }
+    // The same into the Morton order of the support-radius cells: the cell
+    // list's slots sorted (stably) by their cells' Morton keys give the new
+    // state order; the cell list is then renumbered to the new state indices.
+    int reorder_morton(int ph, const PermList& L) {
+        PhaseDev<T>& D = P[ph];
+        MortonScratch& M = morton[ph];
+        const int n = D.n;
+        if (M.n < n || !M.tmp) return SPHG_ERR_STATE;
+        int rc = launch_pdl("reorder", k_morton_keys, blocks(n, 256), 256, 0, n, (const int*)D.perm,
+                            (const int*)D.cell_id, grid, M.key[0], M.val[0]);
+        if (rc) return rc;
+        size_t b = M.tmp_bytes;
+        CUDA_TRY(cub::DeviceRadixSort::SortPairs(M.tmp, b, M.key[0], M.key[1], M.val[0], M.val[1], n, 0, 32,
+                                                 ctx->stream));
+        if ((rc = launch_pdl("reorder", k_permute_all, blocks(n, 256), 256, 0, n, (const int*)M.val[1], L))) return rc;
+        swap_buffers(ph);
+        if ((rc = launch_pdl("reorder", k_invert, blocks(n, 256), 256, 0, n, (const int*)M.val[1], M.inv))) return rc;
+        return launch_pdl("reorder", k_renumber, blocks(n, 256), 256, 0, n, (const int*)M.inv, D.perm);
     }
 
     // Launches above 48 KB of dynamic shared memory must be allowed per kernel

@@ -60,16 +60,13 @@ struct SimConst {
 #endif
 // neighbours of one block of the two-phase water_pass_a staged in shared
 // memory (records; the sizes of 128 consecutive particles' candidate runs at
-// dx = 0.002 m: mean 414, largest 544).  The staged pass took 131.0 us per
-// launch at 912,016 particles; reading the same candidates through L1
-// instead (the direct scan of the blocks that do not fit) took 130.4 us.
+// dx = 0.002 m: mean 414, largest 544).  Each lane tests its candidates
+// from there one at a time and runs the pair body on each hit at once
+// (scan_direct): 123.5 us per launch at 912,016 particles, against 130.7 us
+// with the hit buffer that batches the bodies across the warp, and 130.4 us
+// for the direct scan reading through L1.
 #ifndef SPHG_STAGE_A
 #define SPHG_STAGE_A 576
-#endif
-// candidates per lane per scan iteration in the staged pass (shared-memory
-// loads need less latency hiding than global ones)
-#ifndef SPHG_SCAN_U_STAGED
-#define SPHG_SCAN_U_STAGED 2
 #endif
 #ifndef SPHG_MINB_SOIL
 #define SPHG_MINB_SOIL 1
@@ -433,7 +430,6 @@ __global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_A : 1) k_
         // neighbours staged in shared memory when they fit (positions and records)
         extern __shared__ __align__(128) unsigned char stage_mem[];
         __shared__ StageHdr H;
-        __shared__ HitBuf<T, SPHG_TPB, Chunk<T>::value, unsigned short> hb16;   // staged indices
         const int cap = stage_capacity(16 + (int)sizeof(RecA<T>));
         int cx, cy;
         bool cl;
@@ -448,8 +444,8 @@ __global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_A : 1) k_
             const CandRuns sr = staged_runs(H, cr, cy, k, self_s);
             const double2* sxs = (const double2*)stage_mem;
             const RecA<T>* sA = (const RecA<T>*)(stage_mem + (size_t)cap * 16);
-            hits = scan_runs<true, SPHG_SCAN_U_STAGED>(hb16, sc, sr, sxs, P.hs, xa, ha, self_s, mask,
-                                   [&](int m, T dx, T dy) { body(sA, m, dx, dy); });
+            hits = scan_direct<true, T>(sc, sr, sxs, P.hs, xa, ha, self_s, mask,
+                                        [&](int m, T dx, T dy) { body(sA, m, dx, dy); });
         } else {   // rare: the block's runs do not fit
             hits = scan_direct<true, T>(sc, cr, P.xs, P.hs, xa, ha, k, mask,
                                         [&](int m, T dx, T dy) { body(rec, m, dx, dy); });
@@ -644,7 +640,9 @@ __global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_B : 1) k_
     // Neighbours read through L1, not staged in shared memory: staging them
     // (positions and both records, up to 560 per block) cut the resident
     // blocks to 6 per SM and measured 179 us per launch at 912,016 particles
-    // against 164 us for this form at 7 blocks.
+    // against 164 us for this form at 7 blocks.  Loading each lane's next
+    // hit's records during the current one (16 more registers) measured 210
+    // us at 6 blocks.
     visit_masked<T>(g, sc, P.cell_start, P.xs, P.hs, xa, ha, k, valid, mask,
                     [&](int m, T dx, T dy) { body(rec, P.recB, m, dx, dy); });
     const T d1x = d1.x, d1y = d1.y, d2x = d2.x, d2y = d2.y, d3x = d3.x, d3y = d3.y;
@@ -930,6 +928,41 @@ static __global__ void __launch_bounds__(256) k_permute_all(int n, const int* __
         else if (f.bytes == 8) ((long long*)f.dst)[k] = ((const long long*)f.src)[a];
         else ((int4*)f.dst)[k] = ((const int4*)f.src)[a];
     }
+}
+
+// Morton (Z-order) state order: the key of the particle in sorted slot k is
+// the interleaved bits of its support-radius cell (x cell / kx, row); the
+// stable sort of the slots by key keeps the cell list's order inside a cell.
+__device__ __forceinline__ unsigned spread_bits16(unsigned v) {
+    v &= 0xffffu;
+    v = (v | (v << 8)) & 0x00ff00ffu;
+    v = (v | (v << 4)) & 0x0f0f0f0fu;
+    v = (v | (v << 2)) & 0x33333333u;
+    v = (v | (v << 1)) & 0x55555555u;
+    return v;
+}
+static __global__ void __launch_bounds__(256) k_morton_keys(int n, const int* __restrict__ perm,
+                                                            const int* __restrict__ cell_id, GridGeom g,
+                                                            unsigned* __restrict__ key, int* __restrict__ val) {
+    pdl_enter();
+    const int k = gtid();
+    if (k >= n) return;
+    const int a = perm[k];
+    const int c = cell_id[a];
+    key[k] = spread_bits16((unsigned)((c % g.ncx) / g.kx)) | (spread_bits16((unsigned)(c / g.ncx)) << 1);
+    val[k] = a;
+}
+// new state index of each old one (inv[order[j]] = j), then the cell list's
+// slots renumbered to the new state indices
+static __global__ void __launch_bounds__(256) k_invert(int n, const int* __restrict__ order, int* __restrict__ inv) {
+    pdl_enter();
+    const int j = gtid();
+    if (j < n) inv[order[j]] = j;
+}
+static __global__ void __launch_bounds__(256) k_renumber(int n, const int* __restrict__ inv, int* __restrict__ perm) {
+    pdl_enter();
+    const int k = gtid();
+    if (k < n) perm[k] = inv[perm[k]];
 }
 
 template <typename S>

@@ -1112,12 +1112,15 @@ def main(argv=None):
     ens_f = ensemble.Ensemble(test_specs, tune=False)
     solvers = _fallback_solvers(ens_f, HIST)
     res_net = evaluate(net, held, HIST, mode="net", solvers=solvers)
+    res_free = evaluate(net, held, HIST, mode="net")   # the same rollout with the fallback gates off
     res_grav = evaluate(net, held, HIST, mode="gravity")
     ens_f.close()
     report["learned"] = summarise(res_net)
+    report["learned_gates_off"] = summarise(res_free)
     report["gravity_only"] = summarise(res_grav)
-    report["per_scene"] = [dict(r, gravity_runout_dx=g["runout_dx"], gravity_surface_dx=g["surface_dx"])
-                           for r, g in zip(res_net["scenes"], res_grav["scenes"])]
+    report["per_scene"] = [dict(r, gates_off_runout_dx=f["runout_dx"], gates_off_surface_dx=f["surface_dx"],
+                                gravity_runout_dx=g["runout_dx"], gravity_surface_dx=g["surface_dx"])
+                           for r, f, g in zip(res_net["scenes"], res_free["scenes"], res_grav["scenes"])]
     report["total_s"] = time.perf_counter() - t0
     txt = json.dumps(report, indent=1)
     if a.report:

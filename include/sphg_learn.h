@@ -68,6 +68,27 @@ int sphg_gnn_edge_layer(const void* E, float* EF, void* E_out, const float* P, c
                         long long nedge, int M, const void* We, const float* be, const void* W2, const float* b2,
                         int* err_dev, void* cuda_stream);
 
+/* The edge layer of the network in inference form with the sender term
+ * inside the first GEMM (one kernel, K = 256):
+ *   z    = [E | H[src]] . [We | Ws]^T + (Pd[dst] + be)
+ *   Eout = bf16(E + (relu(z) . W2^T + b2))
+ * where Ws is the sender half of the node projection (rows 0..127 of wsd) and
+ * Pd = H Wd^T its receiver half per node (fp32, rows 128..255 of wsd, e.g.
+ * from sphg_gemm_bf16_ws with the STORE epilogue).  This is the same layer as
+ * sphg_gnn_edge_layer with EF NULL and P = [H Ws^T | Pd], except that the
+ * sender term is summed in the accumulator with the edge term instead of
+ * being rounded to an fp32 P row first (the results differ from it in the
+ * last bits of the fp32 sums).  Rows of E and Eout beyond nedge use zero node
+ * terms.  H [nnode x 128] bf16, Pd [nnode x 128] fp32, E and Eout [M x 128]
+ * bf16 (may be the same array), src and dst per edge, We, Ws and W2
+ * [128 x 128] bf16, be and b2 [128] fp32; M % 128 == 0, 0 <= nedge <= M,
+ * E and Eout 32-byte aligned, the other arrays 16-byte aligned.  *err_dev:
+ * bit 0 set when a device wait gave up, bit 1 when an index lies outside
+ * [0, nnode) (that node term is taken as zero). */
+int sphg_gnn_edge_layer_nodes(const void* E, void* E_out, const void* H, const float* Pd, int nnode, const int* src,
+                              const int* dst, long long nedge, int M, const void* We, const void* Ws, const float* be,
+                              const void* W2, const float* b2, int* err_dev, void* cuda_stream);
+
 /* Test of the bounded device waits (no counterpart in the reference, whose
  * only failure path is `stop`): launches sphg_gemm_bf16_tn's kernel on
  * A (M x K) and B (N x K) so that its first K block issues no MMA and waits

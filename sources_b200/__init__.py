@@ -38,6 +38,7 @@ EXPORTS = ("sphg_default_params", "sphg_create", "sphg_upload_phase", "sphg_sing
                # I int, L 64-bit count, F float, D double, S size_t pointer
                "sphg_gemm_bf16_ws": "PPIIIPPP",
                "sphg_gnn_edge_layer": "PPPPPPLIPPPPPP",
+               "sphg_gnn_edge_layer_nodes": "PPPPIPPLIPPPPPPP",
                "sphg_gnn_scan_bytes": "IP",
                "sphg_gnn_graph_count": "PPIPPPPPPLP",
                "sphg_gnn_graph_fill": "PPIPPPPPP",

@@ -17,6 +17,7 @@
 //     into C (split-K over gridDim.z).
 // Shapes: M % 128 == 0, N % BN == 0 with BN in {16, 32, 64, 128, 256},
 // K % 64 == 0, 16-byte aligned rows.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -219,15 +220,6 @@ __device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
-__device__ __forceinline__ uint4 bf16x8(const float* v) {
-    uint4 u;
-    __nv_bfloat162 t;
-    t = __floats2bfloat162_rn(v[0], v[1]); u.x = *reinterpret_cast<uint32_t*>(&t);
-    t = __floats2bfloat162_rn(v[2], v[3]); u.y = *reinterpret_cast<uint32_t*>(&t);
-    t = __floats2bfloat162_rn(v[4], v[5]); u.z = *reinterpret_cast<uint32_t*>(&t);
-    t = __floats2bfloat162_rn(v[6], v[7]); u.w = *reinterpret_cast<uint32_t*>(&t);
-    return u;
-}
 
 template <int N, int K>
 struct WsShape {
@@ -756,7 +748,528 @@ __global__ void __launch_bounds__(EdgeShape::THREADS, 1) k_edge_layer(const __nv
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256));
 }
 
+
+// ------------------------------------------------------------------------
+// Edge layer with the sender term inside the first GEMM (inference):
+//   z  = [e | h[src]] . [We | Ws]^T + (Pd[dst] + be)      (K = 256)
+//   e' = bf16(e + (relu(z) . W2^T + b2))
+// h is the bf16 node latent, Ws the sender half of the node projection and
+// Pd = h Wd^T its receiver half, computed once per node (fp32).  The sender
+// rows are products of the same bf16 operands as the projection GEMM,
+// accumulated in the same fp32 accumulator as the edge term; they are TMA
+// gathers into shared memory that run ahead of the MMAs.  The receiver term
+// is added in the epilogue: edges are sorted by receiver, so a tile's rows
+// share a few Pd rows and their loads are L1 hits.  Warp roles:
+//   warps 0-3   hidden epilogue: acc1 -> + (Pd[dst] + be), relu, bf16 -> the
+//               hidden rows, written back into acc1's first 64 TMEM columns
+//   warps 4-7   output epilogue: acc2 -> + (e + b2) -> bf16 e' (global)
+//   warp 8      one thread issues GEMM1 of every tile (as its K blocks arrive)
+//   warp 9      one thread issues GEMM2 of every tile (as its hidden rows
+//               arrive), with A (the hidden rows) read from TMEM
+//   warp 10     loader: TMA copies of 16 KB K blocks into a ring of NSLOT
+//               slots, in the 128-byte swizzle layout: an E block is one 2-D
+//               tile, the first half of the sender rows 32 tile::gather4
+//               copies of 4 rows; the slot's full barrier completes on the
+//               copies' byte count
+//   warps 11-12 row loaders: the second half of the sender rows by cp.async,
+//               so that the TMA unit and the load/store path gather at once
+// TMEM: two GEMM1 accumulators (each also holding its tile's hidden rows
+// until GEMM2 has read them) and two GEMM2 accumulators, 512 columns; so
+// GEMM1 of tile i + 1 overlaps the epilogues and GEMM2 of tile i, and neither
+// GEMM's issue waits for the other's inputs.  Resident in shared memory:
+// [We | Ws] (64 KB), W2 (32 KB), the ring (128 KB: two tiles' K blocks), be
+// and b2.  Every wait is bounded; a role that gives up sets *err and the
+// abort flag, the others leave at their next wait, and each MMA thread drains
+// its MMAs before TMEM is freed.
+struct EdgeNodeShape {
+    static constexpr uint32_t KC = 128 * 16;             // one 16-byte column of a 128-row operand
+    static constexpr uint32_t B1 = 0;                    // [We | Ws]: 32 columns
+    static constexpr uint32_t B2 = B1 + 32 * KC;         // W2: 16 columns
+    static constexpr int NSLOT = 8;
+    static constexpr uint32_t SLOT = 8 * KC;             // one K block of 64 (128 rows x 128 swizzled bytes)
+    static constexpr uint32_t RING = B2 + 16 * KC;
+    static constexpr uint32_t BIAS = RING + NSLOT * SLOT;  // be, b2 (fp32)
+    static constexpr uint32_t BAR = BIAS + 2 * 128 * 4;
+    static constexpr uint32_t SMEM = BAR + 256 + 1024;   // + alignment of the ring to 1024 bytes
+    static constexpr int KBLK = 4;                       // K blocks of GEMM1 per tile: E, E, h[src], h[src]
+    static constexpr int CPB = 3;                        // the K block copied by cp.async (slots 3 and 7)
+    static constexpr int ROWLOADERS = 64;                // its copy threads (warps 11-12)
+    static constexpr int THREADS = 13 * 32;
+};
+static_assert(EdgeNodeShape::SMEM <= 227 * 1024, "edge layer shared memory");
+static_assert(EdgeNodeShape::NSLOT % EdgeNodeShape::KBLK == 0, "a slot always holds the same K block");
+
+
+// 32 accumulator columns of this thread's TMEM lane
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
+}
+
+// 32 contiguous bytes per thread (256-bit global accesses, sm_100); the load is
+// cached in L2 only
+__device__ __forceinline__ void ld_global_32B(const void* p, uint32_t* r) {
+    asm volatile("ld.global.cg.v8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                 : "l"(p));
+}
+__device__ __forceinline__ void st_global_32B(void* p, const uint32_t* r) {
+    asm volatile("st.global.v8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(p), "r"(r[0]), "r"(r[1]), "r"(r[2]),
+                 "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7])
+                 : "memory");
+}
+
+// shared-memory descriptor of a K-major operand in the 128-byte swizzle layout that
+// TMA writes with CU_TENSOR_MAP_SWIZZLE_128B: row r of an 8-row, 1024-byte atom at
+// r * 128 with its 16-byte chunks XOR-permuted by r; atoms SBO = 1024 bytes apart.
+// The start address moves 32 bytes per K = 16 step inside the 128-byte rows.
+__device__ __forceinline__ uint64_t make_desc_sw128(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+    d |= (uint64_t)1 << 16;              // leading byte offset: unused for swizzled K-major (16 bytes)
+    d |= (uint64_t)(1024 >> 4) << 32;    // stride byte offset: 8 rows x 128 bytes
+    d |= (uint64_t)1 << 46;              // version
+    d |= (uint64_t)2 << 61;              // SWIZZLE_128B
+    return d;
+}
+
+__device__ __forceinline__ void umma_f16(uint32_t tacc, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+        ::"r"(tacc), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+// A from TMEM (tcgen05.mma ... [d], [a], b_desc, ...): the A tile is 128 lanes (rows)
+// x 8 columns per K = 16 step, two bf16 of consecutive K in each 32-bit column
+__device__ __forceinline__ void umma_f16_ta(uint32_t tacc, uint32_t ta, uint64_t db, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+        ::"r"(tacc), "r"(ta), "l"(db), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+// 16 columns of this thread's TMEM lane
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t* r) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16};" ::"r"(taddr), "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]),
+        "r"(r[7]), "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15])
+        : "memory");
+}
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__global__ void __launch_bounds__(EdgeNodeShape::THREADS, 1)
+    k_edge_layer_nodes(const __grid_constant__ CUtensorMap tmE, const __grid_constant__ CUtensorMap tmH,
+                       const __nv_bfloat16* E, __nv_bfloat16* E_out, const __nv_bfloat16* __restrict__ H,
+                       const float* __restrict__ Pd, int nnode,
+                       const int* __restrict__ src, const int* __restrict__ dst, long long nedge, int M,
+                       const __nv_bfloat16* __restrict__ We, const __nv_bfloat16* __restrict__ Ws,
+                       const float* __restrict__ be,
+                       const __nv_bfloat16* __restrict__ W2, const float* __restrict__ b2, int* __restrict__ err) {
+    typedef EdgeNodeShape S;
+    extern __shared__ __align__(128) uint8_t smem[];
+    // the swizzled ring slots need 1024-byte alignment in the shared window
+    uint8_t* sm = smem + ((1024u - (smem_u32(smem) & 1023u)) & 1023u);
+    uint64_t* full = (uint64_t*)(sm + S::BAR);          // [NSLOT] loaders -> MMA
+    uint64_t* empty = full + S::NSLOT;                    // [NSLOT] MMA (commit) -> loaders
+    uint64_t* acc1_full = empty + S::NSLOT;               // [2]
+    uint64_t* acc1_empty = acc1_full + 2;                 // [2]
+    uint64_t* acc2_full = acc1_empty + 2;                 // [2]
+    uint64_t* acc2_empty = acc2_full + 2;                 // [2]
+    uint64_t* hid_full = acc2_empty + 2;                 // [2] per GEMM1 accumulator: no waiter can fall
+                                                         // two phases behind (ep1 may run a tile ahead)
+    uint64_t* drain = hid_full + 2;                      // [2] one per MMA thread
+    uint32_t* tslot = (uint32_t*)(drain + 2);
+    volatile int* abort_flag = (volatile int*)(tslot + 1);
+    const float* sbe = (const float*)(sm + S::BIAS);
+    const float* sb2 = sbe + 128;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int ntiles = M / 128;
+    const int my = blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+    auto tile_m0 = [&](int i) { return ((long long)blockIdx.x + (long long)i * gridDim.x) * 128; };
+    auto fail = [&]() { atomicOr(err, 1); *abort_flag = 1; };
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                     "r"(512));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+    }
+    if (tid == 0) {
+        for (int s = 0; s < S::NSLOT; ++s) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(full + s)),
+                         "r"(s % S::KBLK == S::CPB ? S::ROWLOADERS : 1));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(empty + s)), "r"(1));
+        }
+        for (int a = 0; a < 2; ++a) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(acc1_full + a)), "r"(1));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(acc1_empty + a)), "r"(1));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(acc2_full + a)), "r"(1));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(acc2_empty + a)), "r"(128));
+        }
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(hid_full)), "r"(128));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(hid_full + 1)), "r"(128));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(drain)), "r"(1));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(drain + 1)), "r"(1));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::);
+        *abort_flag = 0;
+    }
+    // resident operands: column kc of [We | Ws] holds K elements 8 kc .. 8 kc + 7
+    for (int c = tid; c < 128 * 32; c += S::THREADS) {
+        const int n = c / 32, kc = c % 32;
+        const __nv_bfloat16* from = kc < 16 ? We + (size_t)n * 128 + kc * 8 : Ws + (size_t)n * 128 + (kc - 16) * 8;
+        *reinterpret_cast<uint4*>(sm + S::B1 + kc * S::KC + (n >> 3) * 128 + (n & 7) * 16) =
+            *reinterpret_cast<const uint4*>(from);
+    }
+    load_b128<S::THREADS>(sm + S::B2, W2, tid);
+    for (int c = tid; c < 256; c += S::THREADS)
+        reinterpret_cast<float*>(sm + S::BIAS)[c] = c < 128 ? be[c] : b2[c - 128];
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::);
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::);
+    const uint32_t tmem = *tslot;
+
+    if (warp < 4) {
+        // ---- hidden epilogue: TMEM lanes 32 warp .. = tile rows.  The receiver's row of
+        // Pd is prefetched into L1 a tile ahead (its index loaded two tiles ahead);
+        // rows of a tile share few receivers, so most of these loads hit the same lines.
+        const uint32_t lane_off = (uint32_t)(warp * 32) << 16;
+        const int r = warp * 32 + lane;
+        auto receiver = [&](int i) { const long long e = tile_m0(i) + r; return e < nedge ? dst[e] : -1; };
+        auto checked = [&](int i, int d) {   // -1 for padding rows and (flagged) indices outside the node rows
+            if (tile_m0(i) + r < nedge && (d < 0 || d >= nnode)) { atomicOr(err, 2); return -1; }
+            return d;
+        };
+        auto prefetch_row = [&](int d) {
+            if (d >= 0)
+                for (int q = 0; q < 4; ++q)
+                    asm volatile("prefetch.global.L1 [%0];" ::"l"(Pd + (size_t)d * 128 + 32 * q));
+        };
+        int d_cur = my > 0 ? checked(0, receiver(0)) : -1;
+        int d_next = my > 1 ? receiver(1) : -1;
+        prefetch_row(d_cur);
+        for (int i = 0; i < my; ++i) {
+            const int a = i & 1;
+            if (i + 1 < my) { d_next = checked(i + 1, d_next); prefetch_row(d_next); }
+            const int d_after = i + 2 < my ? receiver(i + 2) : -1;
+            const float4* pd = d_cur >= 0 ? reinterpret_cast<const float4*>(Pd + (size_t)d_cur * 128) : nullptr;
+            float4 pa[8], pb[8];   // Pd chunks c and c + 1
+#pragma unroll
+            for (int q = 0; q < 8; ++q) pa[q] = pd ? pd[q] : make_float4(0.f, 0.f, 0.f, 0.f);
+            bool ok = !*abort_flag && mbar_wait(smem_u32(acc1_full + a), (uint32_t)((i >> 1) & 1), kWaitLimit);
+            ok = __all_sync(0xffffffffu, ok);   // the warp's tcgen05.ld / st are warp-collective
+            if (!ok) { fail(); break; }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::);
+            const uint32_t acc = tmem + lane_off + (uint32_t)(a * 128);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {   // 32 accumulator columns at a time
+                float4* p = (c & 1) ? pb : pa;
+                float4* pn = (c & 1) ? pa : pb;
+                if (c < 3) {
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) pn[q] = pd ? pd[8 * (c + 1) + q] : make_float4(0.f, 0.f, 0.f, 0.f);
+                }
+                float v[32];
+                tmem_ld32(acc + (uint32_t)(32 * c), v);
+                uint32_t h[16];
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    const int col = 32 * c + 2 * j;
+                    const float4 t4 = p[j >> 1];
+                    const float p0 = (j & 1) ? t4.z : t4.x, p1 = (j & 1) ? t4.w : t4.y;
+                    const __nv_bfloat162 t = __floats2bfloat162_rn(fmaxf(v[2 * j] + (p0 + sbe[col]), 0.f),
+                                                                   fmaxf(v[2 * j + 1] + (p1 + sbe[col + 1]), 0.f));
+                    h[j] = *reinterpret_cast<const uint32_t*>(&t);
+                }
+                // the hidden row over the accumulator columns already read: K 32c .. 32c + 31 at columns 16c ..
+                tmem_st16(acc + (uint32_t)(16 * c), h);
+            }
+            asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+            asm volatile("tcgen05.fence::before_thread_sync;" ::);
+            mbar_arrive(hid_full + a);
+            d_cur = d_next;
+            d_next = d_after;
+        }
+    } else if (warp < 8) {
+        // ---- output epilogue
+        const int w = warp & 3, r = w * 32 + lane;
+        const uint32_t lane_off = (uint32_t)(w * 32) << 16;
+        for (int i = 0; i < my; ++i) {
+            const int a = i & 1;
+            const long long grow = tile_m0(i) + r;
+            // the residual row, loaded while the tile's GEMMs run (one lane per row, 32-byte accesses)
+            uint32_t res[64];
+            const uint8_t* er = reinterpret_cast<const uint8_t*>(E + grow * 128);
+#pragma unroll
+            for (int u = 0; u < 8; ++u) ld_global_32B(er + 32 * u, res + 8 * u);
+            bool ok = !*abort_flag && mbar_wait(smem_u32(acc2_full + a), (uint32_t)((i >> 1) & 1), kWaitLimit);
+            ok = __all_sync(0xffffffffu, ok);
+            if (!ok) { fail(); break; }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::);
+            uint8_t* out = reinterpret_cast<uint8_t*>(E_out + grow * 128);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                float v[32];
+                tmem_ld32(tmem + lane_off + (uint32_t)(256 + a * 128 + 32 * c), v);
+                uint32_t o[16];
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    const float2 e2 = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&res[16 * c + j]));
+                    const int col = 32 * c + 2 * j;
+                    const __nv_bfloat162 t = __floats2bfloat162_rn(v[2 * j] + (e2.x + sb2[col]),
+                                                                   v[2 * j + 1] + (e2.y + sb2[col + 1]));
+                    o[j] = *reinterpret_cast<const uint32_t*>(&t);
+                }
+                st_global_32B(out + 64 * c, o);
+                st_global_32B(out + 64 * c + 32, o + 8);
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::);
+            mbar_arrive(acc2_empty + a);
+        }
+    } else if (warp < 10) {
+        // ---- MMA issue: lane 0 of warp 8 issues GEMM1 of every tile, lane 0 of warp 9 GEMM2
+        if (lane == 0) {
+            const uint32_t idesc = make_idesc(128);
+            bool ok = true;
+            if (warp == 8) {
+                for (int i = 0; i < my && ok; ++i) {
+                    const int a = i & 1;
+                    if (i >= 2 && !(ok = !*abort_flag && mbar_wait(smem_u32(acc1_empty + a),
+                                                                   (uint32_t)(((i >> 1) & 1) ^ 1), kWaitLimit)))
+                        break;
+                    for (int kb = 0; kb < S::KBLK && ok; ++kb) {
+                        const int j = i * S::KBLK + kb, s = j % S::NSLOT;
+                        if (!(ok = !*abort_flag &&
+                                   mbar_wait(smem_u32(full + s), (uint32_t)((j / S::NSLOT) & 1), kWaitLimit)))
+                            break;
+                        // the cp.async block was written through the generic proxy; the MMAs read the async proxy
+                        if (kb == S::CPB) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                        asm volatile("tcgen05.fence::after_thread_sync;" ::);
+#pragma unroll
+                        for (int kk = 0; kk < 4; ++kk) {   // K = 16 is 32 bytes into the swizzled 128-byte rows
+                            const uint64_t da = make_desc_sw128(smem_u32(sm + S::RING + s * S::SLOT + kk * 32));
+                            const uint64_t db = make_desc(smem_u32(sm + S::B1 + (kb * 8 + kk * 2) * S::KC), S::KC, 128);
+                            umma_f16(tmem + (uint32_t)(a * 128), da, db, idesc, (kb | kk) != 0 ? 1u : 0u);
+                        }
+                        umma_commit(empty + s);   // the slot is free once these MMAs have read it
+                    }
+                    if (ok) umma_commit(acc1_full + a);
+                }
+            } else {
+                for (int i = 0; i < my && ok; ++i) {
+                    const int a = i & 1;
+                    if (!(ok = !*abort_flag &&
+                               mbar_wait(smem_u32(hid_full + a), (uint32_t)((i >> 1) & 1), kWaitLimit)))
+                        break;
+                    if (i >= 2 && !(ok = !*abort_flag && mbar_wait(smem_u32(acc2_empty + a),
+                                                                   (uint32_t)(((i >> 1) & 1) ^ 1), kWaitLimit)))
+                        break;
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::);
+#pragma unroll
+                    for (int kk = 0; kk < 8; ++kk) {
+                        const uint64_t db = make_desc(smem_u32(sm + S::B2 + kk * 2 * S::KC), S::KC, 128);
+                        umma_f16_ta(tmem + (uint32_t)(256 + a * 128), tmem + (uint32_t)(a * 128 + 8 * kk), db, idesc,
+                                    kk != 0 ? 1u : 0u);
+                    }
+                    umma_commit(acc1_empty + a);   // the hidden rows (in GEMM1's accumulator) have been read
+                    umma_commit(acc2_full + a);
+                }
+            }
+            if (!ok) fail();
+            // every MMA issued by this thread has completed before TMEM is freed
+            umma_commit(drain + (warp - 8));
+            mbar_wait(smem_u32(drain + (warp - 8)), 0u, kWaitLimit);
+        }
+    } else if (warp == 10) {
+        // ---- loader warp: TMA copies into the ring.  An edge-row block is one 2-D tile
+        // (64 columns x 128 rows); a node-row block is 32 tile::gather4 copies, lane l
+        // bringing the rows of edges 4l .. 4l + 3.  An index outside [0, nnode) becomes
+        // row nnode, which lies outside the tensor map and is filled with zeros.
+        bool ok = true;
+        int sr[4], nsr[4];
+        auto fetch = [&](int i) {   // raw sender indices of the lane's 4 rows, loaded one tile ahead
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const long long e = tile_m0(i) + 4 * lane + q;
+                nsr[q] = e < nedge ? src[e] : 0;
+            }
+        };
+        if (my > 0) fetch(0);
+        for (int i = 0; i < my && ok; ++i) {
+            const long long m0 = tile_m0(i);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) sr[q] = nsr[q];
+            if (i + 1 < my) fetch(i + 1);
+            if (lane == 0) {   // the edge rows of the tile after next into L2 (32 KB, one bulk prefetch)
+                for (int t = i == 0 ? 1 : i + 2; t <= i + 2 && t < my; ++t)
+                    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(E + tile_m0(t) * 128), "r"(32768)
+                                 : "memory");
+            }
+            bool bad = false;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const bool real = m0 + 4 * lane + q < nedge;
+                const bool sv = sr[q] >= 0 && sr[q] < nnode;
+                bad |= real && !sv;
+                if (!real || !sv) sr[q] = nnode;
+            }
+            if (bad) atomicOr(err, 2);   // an index outside the node rows
+            for (int kb = 0; kb < S::KBLK; ++kb) {
+                if (kb == S::CPB) continue;   // the row loaders' block
+                const int j = i * S::KBLK + kb, s = j % S::NSLOT;
+                bool got = true;
+                if (lane == 0 && j >= S::NSLOT)
+                    got = !*abort_flag &&
+                          mbar_wait(smem_u32(empty + s), (uint32_t)(((j / S::NSLOT) & 1) ^ 1), kWaitLimit);
+                if (!(ok = __shfl_sync(0xffffffffu, got, 0))) break;
+                const uint32_t slot = smem_u32(sm + S::RING + s * S::SLOT);
+                const uint32_t fb = smem_u32(full + s);
+                const int x = (kb & 1) * 64;   // first column of the block (128 bytes: the swizzle span)
+                if (lane == 0)
+                    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(fb), "r"(S::SLOT)
+                                 : "memory");
+                __syncwarp();
+                if (kb < 2) {
+                    if (lane == 0)
+                        asm volatile(
+                            "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+                            " [%0], [%1, {%2, %3}], [%4];" ::"r"(slot), "l"(&tmE), "r"(x), "r"((int)m0), "r"(fb)
+                            : "memory");
+                } else {
+                    asm volatile(
+                        "cp.async.bulk.tensor.2d.shared::cluster.global.tile::gather4.mbarrier::complete_tx::bytes"
+                        " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(slot + 4 * lane * 128), "l"(&tmH), "r"(x),
+                        "r"(sr[0]), "r"(sr[1]), "r"(sr[2]), "r"(sr[3]), "r"(fb)
+                        : "memory");
+                }
+            }
+        }
+        if (!ok && lane == 0) fail();
+    } else {
+        // ---- row loaders (warps 11-12): the second half of the sender rows (K block CPB)
+        // by cp.async, 16 bytes per request, into the same 128-byte swizzle layout
+        // (16-byte chunk u of row r at r * 128 + (u ^ (r & 7)) * 16); each instruction
+        // covers 8 rows x 64 contiguous bytes, and the 8 rows' chunks fall in distinct
+        // banks.  The slot's full barrier counts each thread once its copies have landed.
+        const int lt = tid - 11 * 32, lw = lt >> 5;
+        const int rlo = lane & 7, uq = lane >> 3;
+        bool ok = true;
+        int sn[8], nsn[8];
+        auto fetch = [&](int i) {
+#pragma unroll
+            for (int g = 0; g < 8; ++g) {
+                const long long e = tile_m0(i) + 64 * lw + 8 * g + rlo;
+                nsn[g] = e < nedge ? src[e] : -1;
+            }
+        };
+        if (my > 0) fetch(0);
+        for (int i = 0; i < my && ok; ++i) {
+            const long long m0 = tile_m0(i);
+#pragma unroll
+            for (int g = 0; g < 8; ++g) sn[g] = nsn[g];
+            if (i + 1 < my) fetch(i + 1);
+            const int j = i * S::KBLK + S::CPB, s = j % S::NSLOT;
+            if (j >= S::NSLOT &&
+                !(ok = !*abort_flag &&
+                       mbar_wait(smem_u32(empty + s), (uint32_t)(((j / S::NSLOT) & 1) ^ 1), kWaitLimit)))
+                break;
+            const uint32_t slot = smem_u32(sm + S::RING + s * S::SLOT);
+#pragma unroll
+            for (int g = 0; g < 8; ++g) {
+                const int row = 64 * lw + 8 * g + rlo;
+                const bool v = sn[g] >= 0 && sn[g] < nnode;   // out-of-range indices are flagged by the TMA loader
+                const __nv_bfloat16* from = H + (size_t)(v ? sn[g] : 0) * 128 + 64;
+#pragma unroll
+                for (int t = 0; t < 2; ++t) {
+                    const int u = 4 * t + uq;
+                    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(slot + row * 128 +
+                                                                                       ((u ^ rlo) << 4)),
+                                 "l"(from + u * 8), "r"(v ? 16 : 0)
+                                 : "memory");
+                }
+            }
+            asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(full + s)) : "memory");
+        }
+        cp_async_wait_all();
+        if (!ok) fail();
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::);
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
+}
+
 }  // namespace
+
+// cuTensorMapEncodeTiled from the driver, through the runtime (no link to libcuda)
+static CUresult encode_tiled(CUtensorMap* map, const void* base, uint64_t rows, uint32_t box_rows) {
+    typedef CUresult (*Encode)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                               const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                               CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+    static Encode encode = nullptr;
+    if (!encode) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn)
+            return CUDA_ERROR_NOT_FOUND;
+        encode = (Encode)fn;
+    }
+    // rows of 128 bf16 (256 bytes); boxes of 64 columns (128 bytes, the swizzle span)
+    const cuuint64_t dims[2] = {128, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {256};
+    const cuuint32_t box[2] = {64, box_rows};
+    const cuuint32_t estr[2] = {1, 1};
+    return encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+}
+
+extern "C" int sphg_gnn_edge_layer_nodes(const void* E, void* E_out, const void* H, const float* Pd, int nnode,
+                                         const int* src, const int* dst, long long nedge, int M, const void* We,
+                                         const void* Ws, const float* be, const void* W2, const float* b2,
+                                         int* err_dev, void* stream) {
+    if (!E || !E_out || !H || !Pd || !src || !dst || !We || !Ws || !be || !W2 || !b2 || !err_dev)
+        return SPHG_ERR_BAD_ARG;
+    if (M <= 0 || M % 128 || nedge < 0 || nedge > M || nnode <= 0 || nnode >= (1 << 30)) return SPHG_ERR_BAD_ARG;
+    if (((((uintptr_t)E) | ((uintptr_t)E_out)) & 31) ||
+        ((((uintptr_t)H) | ((uintptr_t)Pd) | ((uintptr_t)We) | ((uintptr_t)Ws) | ((uintptr_t)be) | ((uintptr_t)W2) |
+          ((uintptr_t)b2)) &
+         15))
+        return SPHG_ERR_BAD_ARG;
+    static bool configured = false;
+    if (!configured) {
+        if (cudaFuncSetAttribute(k_edge_layer_nodes, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)EdgeNodeShape::SMEM) != cudaSuccess)
+            return SPHG_ERR_CUDA;
+        configured = true;
+    }
+    CUtensorMap tmE, tmH;   // E: 128-row tiles; H: one row per gather4 row (the box is one row high)
+    if (encode_tiled(&tmE, E, (uint64_t)M, 128) != CUDA_SUCCESS || encode_tiled(&tmH, H, (uint64_t)nnode, 1) != CUDA_SUCCESS)
+        return SPHG_ERR_CUDA;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int ntiles = M / 128;
+    const int grid = ntiles < sms ? ntiles : sms;
+    k_edge_layer_nodes<<<grid, EdgeNodeShape::THREADS, EdgeNodeShape::SMEM, (cudaStream_t)stream>>>(
+        tmE, tmH, (const __nv_bfloat16*)E, (__nv_bfloat16*)E_out, (const __nv_bfloat16*)H, Pd, nnode, src, dst, nedge, M,
+        (const __nv_bfloat16*)We, (const __nv_bfloat16*)Ws, be, (const __nv_bfloat16*)W2, b2, err_dev);
+    return cudaGetLastError() == cudaSuccess ? SPHG_OK : SPHG_ERR_CUDA;
+}
 
 extern "C" int sphg_gnn_edge_layer(const void* E, float* EF, void* E_out, const float* P, const int* src,
                                    const int* dst, long long nedge, int M, const void* We, const float* be,

@@ -237,6 +237,9 @@ class MPNet:
         # the 64 held-out scenes gave the same runout and free-surface errors
         # as with the fp32 stream (mean 0.20 / 0.14 dx, worst 0.85 / 0.39 dx)
         self.edge_bf16 = True
+        # ... and gathers the sender latents into the edge layer's first GEMM
+        # (sphg_gnn_edge_layer_nodes) instead of projecting them to P rows first
+        self.edge_nodes = True
 
     # ------------------------------------------------------------ plumbing
     @property
@@ -331,16 +334,28 @@ class MPNet:
         self._ws(ea, W["enc_e.w2"]["wb"], Ep, L, L, EPI_BIAS_ACT, 0, B["enc_e.b2"]["w"], ef, eb)
         P = G("P", (Np, 2 * L), f32)
         agg = G("agg", (Np, L), f32)
+        gather = bf_edges and self.edge_nodes
+        Pd = G("Pd", (Np, L), f32) if gather else None
         for l in range(LAYERS):
             p = f"p{l}."
-            self._ws(hb, W[p + "wsd"]["wb"], Np, 2 * L, L, EPI_STORE, z=P)
-            if keep or not self.fused_edges:
+            if gather:   # receiver rows per node, then one kernel with the sender rows gathered into its first GEMM
+                wsd = W[p + "wsd"]["wb"]
+                self._ws(hb, wsd[L:], Np, L, L, EPI_STORE, z=Pd)
+                self.launches += 1
+                _call(self.L.sphg_gnn_edge_layer_nodes(_ptr(eb), _ptr(eb), _ptr(hb), _ptr(Pd), Np, _ptr(b.src),
+                                                       _ptr(b.dst), b.E, Ep, _ptr(W[p + "we"]["wb"]), _ptr(wsd),
+                                                       _ptr(B[p + "be"]["w"]), _ptr(W[p + "w2"]["wb"]),
+                                                       _ptr(B[p + "b2"]["w"]), _ptr(self.err), s),
+                      "sphg_gnn_edge_layer_nodes")
+            elif keep or not self.fused_edges:
+                self._ws(hb, W[p + "wsd"]["wb"], Np, 2 * L, L, EPI_STORE, z=P)
                 a = G("a" + tag(l), (Ep, L), bf)
                 self._ws(eb, W[p + "we"]["wb"], Ep, L, L, EPI_EDGE, 1, B[p + "be"]["w"], opt("z" + tag(l), (Ep, L)), a,
                          P, b.src, b.dst, b.E)
                 eb = G("eb" + tag(l + 1), (Ep, L), bf)
                 self._ws(a, W[p + "w2"]["wb"], Ep, L, L, EPI_RESID, 0, B[p + "b2"]["w"], ef, eb)   # e += relu(z) W2^T + b2
             else:   # both edge GEMMs in one kernel, the hidden rows never leave the SM; eb updated in place
+                self._ws(hb, W[p + "wsd"]["wb"], Np, 2 * L, L, EPI_STORE, z=P)
                 self.launches += 1
                 _call(self.L.sphg_gnn_edge_layer(_ptr(eb), _ptr(ef), _ptr(eb), _ptr(P), _ptr(b.src), _ptr(b.dst),
                                                  b.E, Ep, _ptr(W[p + "we"]["wb"]), _ptr(B[p + "be"]["w"]),
@@ -1013,7 +1028,7 @@ def summarise(res: dict) -> dict:
                 fallbacks=res["fallbacks"])
 
 
-def stride_bench(n_scenes: int, strides: int, weights=None, edge_bf16: bool = True):
+def stride_bench(n_scenes: int, strides: int, weights=None, edge_bf16: bool = True, edge_nodes: bool = True):
     """Learned strides on the largest group of n_scenes held-out scenes (a
     history of HIST strides from the plain solver first): wall time per
     stride, forward time (CUDA events) and the graph size, as one JSON line."""
@@ -1027,6 +1042,7 @@ def stride_bench(n_scenes: int, strides: int, weights=None, edge_bf16: bool = Tr
     path = weights or (DEFAULT_WEIGHTS if os.path.exists(DEFAULT_WEIGHTS) else None)
     net = MPNet.from_state(dict(np.load(path))) if path else MPNet(seed=0)
     net.edge_bf16 = edge_bf16
+    net.edge_nodes = edge_nodes
     r = max(roll, key=lambda q: q.X.shape[1])
     LearnedStepper(net, r, HIST, "net").step()
     st = LearnedStepper(net, r, HIST, "net")
@@ -1045,7 +1061,8 @@ def stride_bench(n_scenes: int, strides: int, weights=None, edge_bf16: bool = Tr
     n = r.X.shape[1]
     print(json.dumps(dict(nodes=n, edges=int(st.batch.E), kind=r.kind, strides=strides, ms_per_stride=wall * 1e3,
                           forward_ms=e0.elapsed_time(e1) / strides,
-                          particle_steps_per_s=n * K_STRIDE / wall, weights=path or "random")))
+                          particle_steps_per_s=n * K_STRIDE / wall, weights=path or "random",
+                          edge_bf16=edge_bf16, edge_nodes=edge_nodes)))
 
 
 def main(argv=None):
@@ -1068,18 +1085,21 @@ def main(argv=None):
     ap.add_argument("--report", default=None, help="write the JSON report")
     ap.add_argument("--edge-fp32", action="store_true",
                     help="inference keeps the fp32 residual stream of the edge latent (default: bf16 only)")
+    ap.add_argument("--edge-proj", action="store_true",
+                    help="inference adds projected node rows (P) in the edge layer's epilogue instead of "
+                         "gathering the node latents into its first GEMM")
     ap.add_argument("--stride-bench", type=int, default=0, metavar="S",
                     help="only time S learned strides on the first --test held-out scenes (no training)")
     a = ap.parse_args(argv)
     torch = _torch()
     if a.stride_bench:
-        return stride_bench(a.test, a.stride_bench, a.load, not a.edge_fp32)
+        return stride_bench(a.test, a.stride_bench, a.load, not a.edge_fp32, not a.edge_proj)
     strides = a.steps // K_STRIDE
     train_specs, test_specs = split_specs(a.pool, a.test)
     report = dict(config=dict(pool=a.pool, train_scenes=len(train_specs), test_scenes=len(test_specs),
                               steps=a.steps, stride=K_STRIDE, iters=a.iters, batch_nodes=a.batch_nodes,
                               lr=list(a.lr), noise=a.noise, balance=a.balance, kind_weight=a.kind_weight,
-                              edge_bf16=not a.edge_fp32,
+                              edge_bf16=not a.edge_fp32, edge_nodes=not a.edge_proj,
                               width=L_WIDTH, layers=LAYERS))
     t0 = time.perf_counter()
     if a.load:
@@ -1104,6 +1124,7 @@ def main(argv=None):
         if a.weights:
             np.savez_compressed(a.weights, **net.state())
     net.edge_bf16 = not a.edge_fp32
+    net.edge_nodes = not a.edge_proj
     torch.cuda.empty_cache()
     ens_t = ensemble.Ensemble(test_specs, tune=False)
     report["test_particles"] = ens_t.n_particles

@@ -275,3 +275,108 @@ def test_segsum_bf16_matches_fp32_rows(cuda_ok, lib):
     assert lib.sphg_gnn_segsum_bf16(e.data_ptr(), off.data_ptr(), a16.data_ptr(), n, L, 0.0625, s) == 0
     torch.cuda.synchronize()
     assert torch.equal(a32, a16)
+
+
+@pytest.mark.parametrize("M,inplace", [(128 * 3, True), (128 * 1201, True), (128 * 1201, False)])
+def test_edge_layer_nodes_matches_fp32_reference(cuda_ok, lib, M, inplace):
+    """sphg_gnn_edge_layer_nodes (sender node rows gathered into the first
+    GEMM, K = 256; receiver rows Pd = H Wd^T added in the epilogue) against the
+    fp32 arithmetic of the same bf16 operands, and against the projected-row
+    kernel (sphg_gnn_edge_layer with P = [H Ws^T | Pd]): the two differ only
+    where the rounding of the fp32 sums moves a bf16 hidden or output value by
+    one unit; rows beyond nedge use zero node terms; E may be updated in
+    place."""
+    import torch
+    L = 128
+    g = torch.Generator(device="cuda").manual_seed(M + 11)
+    E = torch.randn(M, L, device="cuda", generator=g).to(torch.bfloat16)
+    We = (torch.randn(L, L, device="cuda", generator=g) / L ** 0.5).to(torch.bfloat16)
+    Wsd = (torch.randn(2 * L, L, device="cuda", generator=g) / L ** 0.5).to(torch.bfloat16)
+    W2 = (torch.randn(L, L, device="cuda", generator=g) / L ** 0.5).to(torch.bfloat16)
+    be = torch.randn(L, device="cuda", generator=g)
+    b2 = torch.randn(L, device="cuda", generator=g)
+    nodes = max(M // 20, 7)
+    H = torch.randn(nodes, L, device="cuda", generator=g).to(torch.bfloat16)
+    Pd = (H.float() @ Wsd[L:].float().T).contiguous()
+    nedge = M - 37
+    src = torch.randint(0, nodes, (M,), device="cuda", generator=g, dtype=torch.int32)
+    dst = torch.sort(torch.randint(0, nodes, (M,), device="cuda", generator=g, dtype=torch.int32)).values
+    s = torch.cuda.current_stream().cuda_stream
+    Ein = E.clone()
+    Eout = Ein if inplace else torch.zeros(M, L, device="cuda", dtype=torch.bfloat16)
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    rc = lib.sphg_gnn_edge_layer_nodes(Ein.data_ptr(), Eout.data_ptr(), H.data_ptr(), Pd.data_ptr(), nodes,
+                                       src.data_ptr(), dst.data_ptr(), nedge, M, We.data_ptr(), Wsd.data_ptr(),
+                                       be.data_ptr(), W2.data_ptr(), b2.data_ptr(), err.data_ptr(), s)
+    torch.cuda.synchronize()
+    assert rc == 0 and int(err.item()) == 0
+    if not inplace:
+        assert torch.equal(Ein, E)
+    # fp32 arithmetic of the same bf16 operands
+    z = E.float() @ We.float().T + be
+    sl, dl = src[:nedge].long(), dst[:nedge].long()
+    z[:nedge] += H[sl].float() @ Wsd[:L].float().T + Pd[dl]
+    hid = z.clamp_min(0).to(torch.bfloat16).float()
+    ref = E.float() + (hid @ W2.float().T + b2)
+    out = Eout.float()
+    scale = float(ref.abs().max())
+    assert float((out - ref).abs().max()) <= 2e-2 * scale
+    assert float((out - ref).abs().mean()) <= 2e-3 * float(ref.abs().mean())
+    # the projected-row kernel on the same inputs
+    P = torch.cat([H.float() @ Wsd[:L].float().T, Pd], dim=1).contiguous()
+    Ep = E.clone()
+    assert lib.sphg_gnn_edge_layer(Ep.data_ptr(), None, Ep.data_ptr(), P.data_ptr(), src.data_ptr(), dst.data_ptr(),
+                                   nedge, M, We.data_ptr(), be.data_ptr(), W2.data_ptr(), b2.data_ptr(),
+                                   err.data_ptr(), s) == 0
+    torch.cuda.synchronize()
+    d = (Ep.float() - out).abs()
+    assert float(d.max()) <= 2e-2 * scale
+    assert float((d > 0).float().mean()) <= 0.05   # most outputs carry the same bits
+
+
+def test_edge_layer_nodes_flags_bad_indices_and_arguments(cuda_ok, lib):
+    """A sender or receiver index outside [0, nnode) sets bit 1 of *err and
+    takes that node term as zero; bad shapes, null or misaligned pointers are
+    refused before any launch."""
+    import ctypes
+    import torch
+    L, M, nodes = 128, 256, 40
+    g = torch.Generator(device="cuda").manual_seed(3)
+    E = torch.randn(M, L, device="cuda", generator=g).to(torch.bfloat16)
+    We = (torch.randn(L, L, device="cuda", generator=g) / L ** 0.5).to(torch.bfloat16)
+    Ws = (torch.randn(L, L, device="cuda", generator=g) / L ** 0.5).to(torch.bfloat16)
+    W2 = (torch.randn(L, L, device="cuda", generator=g) / L ** 0.5).to(torch.bfloat16)
+    be = torch.randn(L, device="cuda", generator=g)
+    b2 = torch.randn(L, device="cuda", generator=g)
+    H = torch.randn(nodes, L, device="cuda", generator=g).to(torch.bfloat16)
+    Pd = torch.randn(nodes, L, device="cuda", generator=g)
+    src = torch.randint(0, nodes, (M,), device="cuda", generator=g, dtype=torch.int32)
+    dst = torch.sort(torch.randint(0, nodes, (M,), device="cuda", generator=g, dtype=torch.int32)).values
+    src[5] = nodes          # outside the node rows
+    dst[9] = -1
+    # the same graph over [zero row | H] and [zero row | Pd]: those terms come from the zero rows
+    H2 = torch.cat([torch.zeros(1, L, device="cuda", dtype=torch.bfloat16), H])
+    Pd2 = torch.cat([torch.zeros(1, L, device="cuda"), Pd])
+    src2, dst2 = src + 1, dst + 1
+    src2[5] = 0
+    dst2[9] = 0
+    s = torch.cuda.current_stream().cuda_stream
+    outs = []
+    for Hx, Px, sx, dx, n in ((H, Pd, src, dst, nodes), (H2, Pd2, src2, dst2, nodes + 1)):
+        Eo = torch.zeros_like(E)
+        err = torch.zeros(1, dtype=torch.int32, device="cuda")
+        assert lib.sphg_gnn_edge_layer_nodes(E.data_ptr(), Eo.data_ptr(), Hx.data_ptr(), Px.data_ptr(), n,
+                                             sx.data_ptr(), dx.data_ptr(), M, M, We.data_ptr(), Ws.data_ptr(),
+                                             be.data_ptr(), W2.data_ptr(), b2.data_ptr(), err.data_ptr(), s) == 0
+        torch.cuda.synchronize()
+        outs.append((Eo, int(err.item())))
+    assert outs[0][1] == 2 and outs[1][1] == 0
+    assert torch.equal(outs[0][0], outs[1][0])
+    one = ctypes.c_void_p(256)
+    odd = ctypes.c_void_p(260)
+    f = lib.sphg_gnn_edge_layer_nodes
+    assert f(one, one, one, one, 8, one, one, 100, 100, one, one, one, one, one, one, None) != 0   # M % 128
+    assert f(one, one, one, one, 8, one, one, 200, 128, one, one, one, one, one, one, None) != 0   # nedge > M
+    assert f(one, one, one, one, 0, one, one, 128, 128, one, one, one, one, one, one, None) != 0   # no nodes
+    assert f(odd, one, one, one, 8, one, one, 128, 128, one, one, one, one, one, one, None) != 0   # alignment
+    assert f(one, one, one, None, 8, one, one, 128, 128, one, one, one, one, one, one, None) != 0

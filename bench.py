@@ -306,12 +306,20 @@ def learned_arm(solver, scene, torch, plain_value, strides):
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0
     n = hist.X.shape[1]
+    # the plain solver's strides from the same state, timed the same way (wall clock, a
+    # synchronisation per stride, the positions kept after each stride)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
     ref = learn.scene_rollout(solver, scene, "submerged", strides, x0=x0)
+    torch.cuda.synchronize()
+    wall_plain = time.perf_counter() - t0
     real = hist.nodes["type"] != learn.GNN_BOUNDARY
     d = ((st.x - ref.X[-1]).norm(dim=1).cpu().numpy()[real]) / hist.dx
     value = n * strides * learn.K_STRIDE / wall
     return {"value": value, "unit": UNIT, "vs_plain": value / plain_value, "stride_steps": learn.K_STRIDE,
-            "strides": strides, "ms_per_stride": wall / strides * 1e3, "edges": int(st.batch.E),
+            "strides": strides, "ms_per_stride": wall / strides * 1e3,
+            "plain_ms_per_stride_same_timing": wall_plain / strides * 1e3, "vs_plain_same_timing": wall_plain / wall,
+            "edges": int(st.batch.E),
             "position_error_dx": {"mean": float(d.mean()), "p99": float(np.percentile(d, 99)),
                                   "max": float(d.max())},
             "weights": "sources_b200/data/learned_weights.npz (trained on the 4 mm ensemble)",

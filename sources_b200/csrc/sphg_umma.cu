@@ -777,7 +777,7 @@ __global__ void __launch_bounds__(EdgeShape::THREADS, 1) k_edge_layer(const __nv
 // until GEMM2 has read them) and two GEMM2 accumulators, 512 columns; so
 // GEMM1 of tile i + 1 overlaps the epilogues and GEMM2 of tile i, and neither
 // GEMM's issue waits for the other's inputs.  Resident in shared memory:
-// [We | Ws] (64 KB), W2 (32 KB), the ring (128 KB: two tiles' K blocks), be
+// [We | Ws] (64 KB), W2 (32 KB), the ring (64 KB: one tile's K blocks), be
 // and b2.  Every wait is bounded; a role that gives up sets *err and the
 // abort flag, the others leave at their next wait, and each MMA thread drains
 // its MMAs before TMEM is freed.
@@ -785,14 +785,16 @@ struct EdgeNodeShape {
     static constexpr uint32_t KC = 128 * 16;             // one 16-byte column of a 128-row operand
     static constexpr uint32_t B1 = 0;                    // [We | Ws]: 32 columns
     static constexpr uint32_t B2 = B1 + 32 * KC;         // W2: 16 columns
-    static constexpr int NSLOT = 8;
+    // four slots (one tile's K blocks) measured faster than eight (0.893 against 0.927 ms
+    // per 5.12M rows): the shared memory they leave to L1 holds the prefetched receiver rows
+    static constexpr int NSLOT = 4;
     static constexpr uint32_t SLOT = 8 * KC;             // one K block of 64 (128 rows x 128 swizzled bytes)
     static constexpr uint32_t RING = B2 + 16 * KC;
     static constexpr uint32_t BIAS = RING + NSLOT * SLOT;  // be, b2 (fp32)
     static constexpr uint32_t BAR = BIAS + 2 * 128 * 4;
     static constexpr uint32_t SMEM = BAR + 256 + 1024;   // + alignment of the ring to 1024 bytes
     static constexpr int KBLK = 4;                       // K blocks of GEMM1 per tile: E, E, h[src], h[src]
-    static constexpr int CPB = 3;                        // the K block copied by cp.async (slots 3 and 7)
+    static constexpr int CPB = 3;                        // the K block copied by cp.async (slot 3)
     static constexpr int ROWLOADERS = 64;                // its copy threads (warps 11-12)
     static constexpr int THREADS = 13 * 32;
 };

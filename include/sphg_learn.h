@@ -89,6 +89,16 @@ int sphg_gnn_edge_layer_nodes(const void* E, void* E_out, const void* H, const f
                               const int* dst, long long nedge, int M, const void* We, const void* Ws, const float* be,
                               const void* W2, const float* b2, int* err_dev, void* cuda_stream);
 
+/* The edge encoder in one kernel (inference):
+ *   E_out = bf16(bf16(relu(F W1^T + b1)) W2^T + b2)
+ * with F the [M x 64] bf16 edge features, W1 [128 x 64] and W2 [128 x 128]
+ * bf16, b1 and b2 [128] fp32; the hidden rows stay in TMEM.  The same bits
+ * as sphg_gemm_bf16_ws with the BIAS_ACT epilogue twice (ReLU, then none),
+ * without writing the hidden rows.  M % 128 == 0; E_out 32-byte aligned, the
+ * other arrays 16-byte aligned.  A device wait that gives up sets *err_dev. */
+int sphg_gnn_edge_encoder(const void* F, void* E_out, int M, const void* W1, const float* b1, const void* W2,
+                          const float* b2, int* err_dev, void* cuda_stream);
+
 /* Test of the bounded device waits (no counterpart in the reference, whose
  * only failure path is `stop`): launches sphg_gemm_bf16_tn's kernel on
  * A (M x K) and B (N x K) so that its first K block issues no MMA and waits

@@ -874,6 +874,11 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar) {
                  : "memory");
 }
 
+// ENC: the edge encoder in the same pipeline, E_out = bf16(relu(E We^T + be) W2^T + b2)
+// with E the [M x 64] bf16 edge features (one K block per tile, no node rows, no
+// receiver term, no residual); the same sums, in the same order, as the two
+// weight-stationary GEMMs with the BIAS_ACT epilogue.
+template <bool ENC>
 __global__ void __launch_bounds__(EdgeNodeShape::THREADS, 1)
     k_edge_layer_nodes(const __grid_constant__ CUtensorMap tmE, const __grid_constant__ CUtensorMap tmH,
                        const __nv_bfloat16* E, __nv_bfloat16* E_out, const __nv_bfloat16* __restrict__ H,
@@ -883,6 +888,8 @@ __global__ void __launch_bounds__(EdgeNodeShape::THREADS, 1)
                        const float* __restrict__ be,
                        const __nv_bfloat16* __restrict__ W2, const float* __restrict__ b2, int* __restrict__ err) {
     typedef EdgeNodeShape S;
+    constexpr int KBLK = ENC ? 1 : S::KBLK;              // K blocks of GEMM1 per tile
+    constexpr int CPB = ENC ? -1 : S::CPB;               // the block the row loaders copy
     extern __shared__ __align__(128) uint8_t smem[];
     // the swizzled ring slots need 1024-byte alignment in the shared window
     uint8_t* sm = smem + ((1024u - (smem_u32(smem) & 1023u)) & 1023u);
@@ -913,7 +920,7 @@ __global__ void __launch_bounds__(EdgeNodeShape::THREADS, 1)
     if (tid == 0) {
         for (int s = 0; s < S::NSLOT; ++s) {
             asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(full + s)),
-                         "r"(s % S::KBLK == S::CPB ? S::ROWLOADERS : 1));
+                         "r"(s % KBLK == CPB ? S::ROWLOADERS : 1));
             asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(empty + s)), "r"(1));
         }
         for (int a = 0; a < 2; ++a) {
@@ -929,10 +936,13 @@ __global__ void __launch_bounds__(EdgeNodeShape::THREADS, 1)
         asm volatile("fence.mbarrier_init.release.cluster;" ::);
         *abort_flag = 0;
     }
-    // resident operands: column kc of [We | Ws] holds K elements 8 kc .. 8 kc + 7
-    for (int c = tid; c < 128 * 32; c += S::THREADS) {
-        const int n = c / 32, kc = c % 32;
-        const __nv_bfloat16* from = kc < 16 ? We + (size_t)n * 128 + kc * 8 : Ws + (size_t)n * 128 + (kc - 16) * 8;
+    // resident operands: column kc of [We | Ws] (of We alone, K = 64, for ENC) holds K
+    // elements 8 kc .. 8 kc + 7
+    constexpr int B1COLS = ENC ? 8 : 32;
+    for (int c = tid; c < 128 * B1COLS; c += S::THREADS) {
+        const int n = c / B1COLS, kc = c % B1COLS;
+        const __nv_bfloat16* from = ENC ? We + (size_t)n * 64 + kc * 8
+                                  : kc < 16 ? We + (size_t)n * 128 + kc * 8 : Ws + (size_t)n * 128 + (kc - 16) * 8;
         *reinterpret_cast<uint4*>(sm + S::B1 + kc * S::KC + (n >> 3) * 128 + (n & 7) * 16) =
             *reinterpret_cast<const uint4*>(from);
     }
@@ -951,9 +961,12 @@ __global__ void __launch_bounds__(EdgeNodeShape::THREADS, 1)
         // rows of a tile share few receivers, so most of these loads hit the same lines.
         const uint32_t lane_off = (uint32_t)(warp * 32) << 16;
         const int r = warp * 32 + lane;
-        auto receiver = [&](int i) { const long long e = tile_m0(i) + r; return e < nedge ? dst[e] : -1; };
+        auto receiver = [&](int i) {
+            const long long e = tile_m0(i) + r;
+            return !ENC && e < nedge ? dst[e] : -1;
+        };
         auto checked = [&](int i, int d) {   // -1 for padding rows and (flagged) indices outside the node rows
-            if (tile_m0(i) + r < nedge && (d < 0 || d >= nnode)) { atomicOr(err, 2); return -1; }
+            if (!ENC && tile_m0(i) + r < nedge && (d < 0 || d >= nnode)) { atomicOr(err, 2); return -1; }
             return d;
         };
         auto prefetch_row = [&](int d) {
@@ -1015,9 +1028,11 @@ __global__ void __launch_bounds__(EdgeNodeShape::THREADS, 1)
             const long long grow = tile_m0(i) + r;
             // the residual row, loaded while the tile's GEMMs run (one lane per row, 32-byte accesses)
             uint32_t res[64];
-            const uint8_t* er = reinterpret_cast<const uint8_t*>(E + grow * 128);
+            if (!ENC) {
+                const uint8_t* er = reinterpret_cast<const uint8_t*>(E + grow * 128);
 #pragma unroll
-            for (int u = 0; u < 8; ++u) ld_global_32B(er + 32 * u, res + 8 * u);
+                for (int u = 0; u < 8; ++u) ld_global_32B(er + 32 * u, res + 8 * u);
+            }
             bool ok = !*abort_flag && mbar_wait(smem_u32(acc2_full + a), (uint32_t)((i >> 1) & 1), kWaitLimit);
             ok = __all_sync(0xffffffffu, ok);
             if (!ok) { fail(); break; }
@@ -1030,10 +1045,15 @@ __global__ void __launch_bounds__(EdgeNodeShape::THREADS, 1)
                 uint32_t o[16];
 #pragma unroll
                 for (int j = 0; j < 16; ++j) {
-                    const float2 e2 = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&res[16 * c + j]));
                     const int col = 32 * c + 2 * j;
-                    const __nv_bfloat162 t = __floats2bfloat162_rn(v[2 * j] + (e2.x + sb2[col]),
-                                                                   v[2 * j + 1] + (e2.y + sb2[col + 1]));
+                    __nv_bfloat162 t;
+                    if (ENC) {
+                        t = __floats2bfloat162_rn(v[2 * j] + sb2[col], v[2 * j + 1] + sb2[col + 1]);
+                    } else {
+                        const float2 e2 =
+                            __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&res[16 * c + j]));
+                        t = __floats2bfloat162_rn(v[2 * j] + (e2.x + sb2[col]), v[2 * j + 1] + (e2.y + sb2[col + 1]));
+                    }
                     o[j] = *reinterpret_cast<const uint32_t*>(&t);
                 }
                 st_global_32B(out + 64 * c, o);
@@ -1053,13 +1073,13 @@ __global__ void __launch_bounds__(EdgeNodeShape::THREADS, 1)
                     if (i >= 2 && !(ok = !*abort_flag && mbar_wait(smem_u32(acc1_empty + a),
                                                                    (uint32_t)(((i >> 1) & 1) ^ 1), kWaitLimit)))
                         break;
-                    for (int kb = 0; kb < S::KBLK && ok; ++kb) {
-                        const int j = i * S::KBLK + kb, s = j % S::NSLOT;
+                    for (int kb = 0; kb < KBLK && ok; ++kb) {
+                        const int j = i * KBLK + kb, s = j % S::NSLOT;
                         if (!(ok = !*abort_flag &&
                                    mbar_wait(smem_u32(full + s), (uint32_t)((j / S::NSLOT) & 1), kWaitLimit)))
                             break;
                         // the cp.async block was written through the generic proxy; the MMAs read the async proxy
-                        if (kb == S::CPB) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                        if (kb == CPB) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                         asm volatile("tcgen05.fence::after_thread_sync;" ::);
 #pragma unroll
                         for (int kk = 0; kk < 4; ++kk) {   // K = 16 is 32 bytes into the swizzled 128-byte rows
@@ -1107,7 +1127,7 @@ __global__ void __launch_bounds__(EdgeNodeShape::THREADS, 1)
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
                 const long long e = tile_m0(i) + 4 * lane + q;
-                nsr[q] = e < nedge ? src[e] : 0;
+                nsr[q] = !ENC && e < nedge ? src[e] : 0;
             }
         };
         if (my > 0) fetch(0);
@@ -1116,9 +1136,12 @@ __global__ void __launch_bounds__(EdgeNodeShape::THREADS, 1)
 #pragma unroll
             for (int q = 0; q < 4; ++q) sr[q] = nsr[q];
             if (i + 1 < my) fetch(i + 1);
-            if (lane == 0) {   // the edge rows of the tile after next into L2 (32 KB, one bulk prefetch)
+            if (lane == 0) {   // the edge rows of the tile after next into L2 (one bulk prefetch)
+                constexpr int ROWB = ENC ? 128 : 256;   // bytes per row of E
                 for (int t = i == 0 ? 1 : i + 2; t <= i + 2 && t < my; ++t)
-                    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(E + tile_m0(t) * 128), "r"(32768)
+                    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(
+                                     reinterpret_cast<const uint8_t*>(E) + tile_m0(t) * ROWB),
+                                 "r"(128 * ROWB)
                                  : "memory");
             }
             bool bad = false;
@@ -1129,10 +1152,10 @@ __global__ void __launch_bounds__(EdgeNodeShape::THREADS, 1)
                 bad |= real && !sv;
                 if (!real || !sv) sr[q] = nnode;
             }
-            if (bad) atomicOr(err, 2);   // an index outside the node rows
-            for (int kb = 0; kb < S::KBLK; ++kb) {
-                if (kb == S::CPB) continue;   // the row loaders' block
-                const int j = i * S::KBLK + kb, s = j % S::NSLOT;
+            if (!ENC && bad) atomicOr(err, 2);   // an index outside the node rows
+            for (int kb = 0; kb < KBLK; ++kb) {
+                if (kb == CPB) continue;   // the row loaders' block
+                const int j = i * KBLK + kb, s = j % S::NSLOT;
                 bool got = true;
                 if (lane == 0 && j >= S::NSLOT)
                     got = !*abort_flag &&
@@ -1161,7 +1184,7 @@ __global__ void __launch_bounds__(EdgeNodeShape::THREADS, 1)
             }
         }
         if (!ok && lane == 0) fail();
-    } else {
+    } else if (!ENC) {
         // ---- row loaders (warps 11-12): the second half of the sender rows (K block CPB)
         // by cp.async, 16 bytes per request, into the same 128-byte swizzle layout
         // (16-byte chunk u of row r at r * 128 + (u ^ (r & 7)) * 16); each instruction
@@ -1217,7 +1240,8 @@ __global__ void __launch_bounds__(EdgeNodeShape::THREADS, 1)
 }  // namespace
 
 // cuTensorMapEncodeTiled from the driver, through the runtime (no link to libcuda)
-static CUresult encode_tiled(CUtensorMap* map, const void* base, uint64_t rows, uint32_t box_rows) {
+static CUresult encode_tiled(CUtensorMap* map, const void* base, uint64_t rows, uint32_t box_rows,
+                             uint64_t cols = 128) {
     typedef CUresult (*Encode)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -1230,9 +1254,9 @@ static CUresult encode_tiled(CUtensorMap* map, const void* base, uint64_t rows, 
             return CUDA_ERROR_NOT_FOUND;
         encode = (Encode)fn;
     }
-    // rows of 128 bf16 (256 bytes); boxes of 64 columns (128 bytes, the swizzle span)
-    const cuuint64_t dims[2] = {128, (cuuint64_t)rows};
-    const cuuint64_t strides[1] = {256};
+    // rows of `cols` bf16; boxes of 64 columns (128 bytes, the swizzle span)
+    const cuuint64_t dims[2] = {cols, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {cols * 2};
     const cuuint32_t box[2] = {64, box_rows};
     const cuuint32_t estr[2] = {1, 1};
     return encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
@@ -1254,7 +1278,7 @@ extern "C" int sphg_gnn_edge_layer_nodes(const void* E, void* E_out, const void*
         return SPHG_ERR_BAD_ARG;
     static bool configured = false;
     if (!configured) {
-        if (cudaFuncSetAttribute(k_edge_layer_nodes, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        if (cudaFuncSetAttribute(k_edge_layer_nodes<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)EdgeNodeShape::SMEM) != cudaSuccess)
             return SPHG_ERR_CUDA;
         configured = true;
@@ -1267,9 +1291,37 @@ extern "C" int sphg_gnn_edge_layer_nodes(const void* E, void* E_out, const void*
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int ntiles = M / 128;
     const int grid = ntiles < sms ? ntiles : sms;
-    k_edge_layer_nodes<<<grid, EdgeNodeShape::THREADS, EdgeNodeShape::SMEM, (cudaStream_t)stream>>>(
+    k_edge_layer_nodes<false><<<grid, EdgeNodeShape::THREADS, EdgeNodeShape::SMEM, (cudaStream_t)stream>>>(
         tmE, tmH, (const __nv_bfloat16*)E, (__nv_bfloat16*)E_out, (const __nv_bfloat16*)H, Pd, nnode, src, dst, nedge, M,
         (const __nv_bfloat16*)We, (const __nv_bfloat16*)Ws, be, (const __nv_bfloat16*)W2, b2, err_dev);
+    return cudaGetLastError() == cudaSuccess ? SPHG_OK : SPHG_ERR_CUDA;
+}
+
+extern "C" int sphg_gnn_edge_encoder(const void* F, void* E_out, int M, const void* W1, const float* b1, const void* W2,
+                                     const float* b2, int* err_dev, void* stream) {
+    if (!F || !E_out || !W1 || !b1 || !W2 || !b2 || !err_dev) return SPHG_ERR_BAD_ARG;
+    if (M <= 0 || M % 128) return SPHG_ERR_BAD_ARG;
+    if ((((uintptr_t)E_out) & 31) ||
+        ((((uintptr_t)F) | ((uintptr_t)W1) | ((uintptr_t)b1) | ((uintptr_t)W2) | ((uintptr_t)b2)) & 15))
+        return SPHG_ERR_BAD_ARG;
+    static bool configured = false;
+    if (!configured) {
+        if (cudaFuncSetAttribute(k_edge_layer_nodes<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)EdgeNodeShape::SMEM) != cudaSuccess)
+            return SPHG_ERR_CUDA;
+        configured = true;
+    }
+    CUtensorMap tmF;   // 128-row tiles of the 64 feature columns
+    if (encode_tiled(&tmF, F, (uint64_t)M, 128, 64) != CUDA_SUCCESS) return SPHG_ERR_CUDA;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int ntiles = M / 128;
+    const int grid = ntiles < sms ? ntiles : sms;
+    // the node-row map is unused by the encoder form; pass the feature map in its place
+    k_edge_layer_nodes<true><<<grid, EdgeNodeShape::THREADS, EdgeNodeShape::SMEM, (cudaStream_t)stream>>>(
+        tmF, tmF, (const __nv_bfloat16*)F, (__nv_bfloat16*)E_out, nullptr, nullptr, 1, nullptr, nullptr, 0, M,
+        (const __nv_bfloat16*)W1, nullptr, b1, (const __nv_bfloat16*)W2, b2, err_dev);
     return cudaGetLastError() == cudaSuccess ? SPHG_OK : SPHG_ERR_CUDA;
 }
 

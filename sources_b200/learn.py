@@ -326,12 +326,20 @@ class MPNet:
         hf = G("hf", (Np, L), f32)
         hb = G("hb" + tag(0), (Np, L), bf)
         self._ws(na, W["enc_n.w2"]["wb"], Np, L, L, EPI_BIAS_ACT, 0, B["enc_n.b2"]["w"], hf, hb)
-        ea = G("ea", (Ep, L), bf)
-        self._ws(b.fe, W["enc_e.w1"]["wb"], Ep, L, F_IN, EPI_BIAS_ACT, 1, B["enc_e.b1"]["w"], opt("ez", (Ep, L)), ea)
         bf_edges = self.edge_bf16 and not keep and self.fused_edges   # edge latent kept in bf16 only
         ef = None if bf_edges else G("ef", (Ep, L), f32)
         eb = G("eb" + tag(0), (Ep, L), bf)
-        self._ws(ea, W["enc_e.w2"]["wb"], Ep, L, L, EPI_BIAS_ACT, 0, B["enc_e.b2"]["w"], ef, eb)
+        if bf_edges and self.edge_nodes:   # both encoder GEMMs in one kernel, the hidden rows kept on the SM
+            self.launches += 1
+            _call(self.L.sphg_gnn_edge_encoder(_ptr(b.fe), _ptr(eb), Ep, _ptr(W["enc_e.w1"]["wb"]),
+                                               _ptr(B["enc_e.b1"]["w"]), _ptr(W["enc_e.w2"]["wb"]),
+                                               _ptr(B["enc_e.b2"]["w"]), _ptr(self.err), s),
+                  "sphg_gnn_edge_encoder")
+        else:
+            ea = G("ea", (Ep, L), bf)
+            self._ws(b.fe, W["enc_e.w1"]["wb"], Ep, L, F_IN, EPI_BIAS_ACT, 1, B["enc_e.b1"]["w"], opt("ez", (Ep, L)),
+                     ea)
+            self._ws(ea, W["enc_e.w2"]["wb"], Ep, L, L, EPI_BIAS_ACT, 0, B["enc_e.b2"]["w"], ef, eb)
         P = G("P", (Np, 2 * L), f32)
         agg = G("agg", (Np, L), f32)
         gather = bf_edges and self.edge_nodes

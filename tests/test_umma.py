@@ -380,3 +380,36 @@ def test_edge_layer_nodes_flags_bad_indices_and_arguments(cuda_ok, lib):
     assert f(one, one, one, one, 0, one, one, 128, 128, one, one, one, one, one, one, None) != 0   # no nodes
     assert f(odd, one, one, one, 8, one, one, 128, 128, one, one, one, one, one, one, None) != 0   # alignment
     assert f(one, one, one, None, 8, one, one, 128, 128, one, one, one, one, one, one, None) != 0
+
+
+@pytest.mark.parametrize("M", [128 * 3, 128 * 1201])
+def test_edge_encoder_equals_two_gemms(cuda_ok, lib, M):
+    """sphg_gnn_edge_encoder (both encoder GEMMs in one kernel, the hidden
+    rows kept in TMEM) gives the same bits as two weight-stationary GEMMs with
+    the BIAS_ACT epilogue (ReLU, then none)."""
+    import ctypes
+    import torch
+    from sources_b200 import learn
+    L, F = 128, 64
+    g = torch.Generator(device="cuda").manual_seed(M + 17)
+    X = torch.randn(M, F, device="cuda", generator=g).to(torch.bfloat16)
+    W1 = (torch.randn(L, F, device="cuda", generator=g) / F ** 0.5).to(torch.bfloat16)
+    W2 = (torch.randn(L, L, device="cuda", generator=g) / L ** 0.5).to(torch.bfloat16)
+    b1 = torch.randn(L, device="cuda", generator=g)
+    b2 = torch.randn(L, device="cuda", generator=g)
+    a = torch.zeros(M, L, device="cuda", dtype=torch.bfloat16)
+    ref = torch.zeros(M, L, device="cuda", dtype=torch.bfloat16)
+    _ws(lib, X, W1, M, L, F, learn.GemmEpi(mode=learn.EPI_BIAS_ACT, relu=1, bias=b1.data_ptr(), h=a.data_ptr()))
+    _ws(lib, a, W2, M, L, L, learn.GemmEpi(mode=learn.EPI_BIAS_ACT, relu=0, bias=b2.data_ptr(), h=ref.data_ptr()))
+    out = torch.zeros(M, L, device="cuda", dtype=torch.bfloat16)
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    rc = lib.sphg_gnn_edge_encoder(X.data_ptr(), out.data_ptr(), M, W1.data_ptr(), b1.data_ptr(), W2.data_ptr(),
+                                   b2.data_ptr(), err.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    assert rc == 0 and int(err.item()) == 0
+    assert torch.equal(out, ref)
+    one, odd = ctypes.c_void_p(256), ctypes.c_void_p(272)
+    f = lib.sphg_gnn_edge_encoder
+    assert f(one, one, 100, one, one, one, one, one, None) != 0   # M % 128
+    assert f(one, odd, 128, one, one, one, one, one, None) != 0   # E_out alignment
+    assert f(None, one, 128, one, one, one, one, one, None) != 0

@@ -144,7 +144,10 @@ class _Buffers:
         numel = int(np.prod(shape))
         t = self.buf.get(name)
         if t is None or t.numel() < numel:
-            t = self.torch.zeros(max(numel, 1), dtype=dtype, device=self.device)
+            # a quarter of headroom when a buffer grows, so that graphs growing by a few
+            # edges from stride to stride do not reallocate (and zero) every time
+            grown = numel if t is None else numel + numel // 4
+            t = self.torch.zeros(max(grown, 1), dtype=dtype, device=self.device)
             self.buf[name] = t
         v = t[:numel].view(*shape)
         if zero:

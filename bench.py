@@ -193,7 +193,7 @@ def host_cores() -> int:
 def oracle_throughput(steps: int, warmup: int, cores: int):
     """The serial C restatement of the reference step (the reference's own
     path is serial) on every host core at once: one independent instance per
-    core, each on its own copy of a 62,266-particle sub-domain of the workload.
+    core, each on its own copy of a 58,266-particle sub-domain of the workload.
     Aggregate particle-steps/s = all instances' particle-steps / the slowest
     instance's time (all start together).  Spawned processes: no fork after
     the CUDA context exists."""

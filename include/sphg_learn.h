@@ -178,6 +178,14 @@ int sphg_gnn_segsum(const float* e, const int64_t* off, float* agg, int nnode, i
 /* the same over bf16 edge rows */
 int sphg_gnn_segsum_bf16(const void* e_bf16, const int64_t* off, float* agg, int nnode, int L, float scale,
                          void* cuda_stream);
+
+/* The receiver sums written straight into the node MLP's input rows
+ * (inference): out[n] = [h[n] | bf16(scale * sum of e over the edges n
+ * receives)], out [npad x 2L] bf16, h [npad x L] bf16, e bf16 edge rows; the
+ * same bits as sphg_gnn_segsum_bf16 followed by sphg_gnn_node_concat, without
+ * the fp32 sums.  Rows from nnode to npad get zero sums; L must be 128. */
+int sphg_gnn_segsum_cat(const void* e_bf16, const int64_t* off, const void* h_bf16, void* out_bf16, int nnode,
+                        long long npad, int L, float scale, void* cuda_stream);
 int sphg_gnn_segsum_bwd(const float* dagg, const int* dst, float* de, long long nedge, int L, float scale,
                         void* cuda_stream);
 /* dP [nnode x 2L] (sender half zero on entry) from dz of the fused layer */

@@ -51,6 +51,7 @@ EXPORTS = ("sphg_default_params", "sphg_create", "sphg_upload_phase", "sphg_sing
                "sphg_gnn_transpose": "PIPLIP",
                "sphg_gnn_segsum": "PPPIIFP",
                "sphg_gnn_segsum_bf16": "PPPIIFP",
+               "sphg_gnn_segsum_cat": "PPPPILIFP",
                "sphg_gnn_segsum_bwd": "PPPLIFP",
                "sphg_gnn_gather_bwd": "PPPPILIP",
                "sphg_gnn_node_concat": "PPPLIP",

@@ -323,6 +323,36 @@ __global__ void k_segsum_bf16(const __nv_bfloat16* __restrict__ e, const int64_t
     reinterpret_cast<float4*>(agg + n * LW)[lane] = make_float4(s.x * scale, s.y * scale, s.z * scale, s.w * scale);
 }
 
+// The receiver sums written straight into the node MLP's input rows (inference):
+// out[n] = [h[n] | bf16(scale * sum of e over the edges n receives)], the same bits
+// as k_segsum_bf16 followed by k_node_concat, without the fp32 agg rows; rows from
+// nnode to npad get zero sums.  One warp per node: lane l copies 8 bytes of h and
+// sums columns 4l .. 4l + 3 in edge order.
+__global__ void k_segsum_cat(const __nv_bfloat16* __restrict__ e, const int64_t* __restrict__ off,
+                             const bf16* __restrict__ h, bf16* __restrict__ out, int nnode, long long npad,
+                             float scale) {
+    long long n;
+    int lane;
+    row_lane<LW / 4>(n, lane);
+    if (n >= npad) return;
+    float4 s = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (n < nnode) {
+        for (long long k = off[n]; k < off[n + 1]; ++k) {
+            const uint2 u = reinterpret_cast<const uint2*>(e + k * LW)[lane];
+            const float2 lo = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u.x));
+            const float2 hi = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u.y));
+            s = add4(s, make_float4(lo.x, lo.y, hi.x, hi.y));
+        }
+    }
+    uint2* row = reinterpret_cast<uint2*>(out + n * 2 * LW);
+    row[lane] = reinterpret_cast<const uint2*>(h + n * LW)[lane];
+    __nv_bfloat162 t0 = __floats2bfloat162_rn(s.x * scale, s.y * scale), t1 = __floats2bfloat162_rn(s.z * scale, s.w * scale);
+    uint2 a;
+    a.x = *reinterpret_cast<uint32_t*>(&t0);
+    a.y = *reinterpret_cast<uint32_t*>(&t1);
+    row[LW / 4 + lane] = a;
+}
+
 // de[k] += scale * dagg[receiver of k]
 __global__ void k_segsum_bwd(const float* __restrict__ dagg, const int* __restrict__ dst, float* __restrict__ de,
                              long long nedge, float scale) {
@@ -644,6 +674,12 @@ int sphg_gnn_segsum(const float* e, const int64_t* off, float* agg, int nnode, i
 int sphg_gnn_segsum_bf16(const void* e, const int64_t* off, float* agg, int nnode, int L, float scale, void* stream) {
     if (L != LW) return SPHG_ERR_BAD_ARG;
     ROWS(k_segsum_bf16, (long long)nnode, LW / 4, (const __nv_bfloat16*)e, off, agg, nnode, scale);
+}
+
+int sphg_gnn_segsum_cat(const void* e, const int64_t* off, const void* h, void* out, int nnode, long long npad, int L,
+                        float scale, void* stream) {
+    if (L != LW || npad < nnode) return SPHG_ERR_BAD_ARG;
+    ROWS(k_segsum_cat, npad, LW / 4, (const __nv_bfloat16*)e, off, (const bf16*)h, (bf16*)out, nnode, npad, scale);
 }
 
 int sphg_gnn_segsum_bwd(const float* dagg, const int* dst, float* de, long long nedge, int L, float scale,

@@ -372,12 +372,12 @@ class MPNet:
                                                  b.E, Ep, _ptr(W[p + "we"]["wb"]), _ptr(B[p + "be"]["w"]),
                                                  _ptr(W[p + "w2"]["wb"]), _ptr(B[p + "b2"]["w"]), _ptr(self.err), s),
                       "sphg_gnn_edge_layer")
-            if bf_edges:
-                self._k("sphg_gnn_segsum_bf16", _ptr(eb), _ptr(b.off), _ptr(agg), b.n, L, AGG_SCALE, s)
+            cat = G("cat" + tag(l), (Np, 2 * L), bf)
+            if bf_edges:   # the receiver sums straight into the node MLP's input rows
+                self._k("sphg_gnn_segsum_cat", _ptr(eb), _ptr(b.off), _ptr(hb), _ptr(cat), b.n, Np, L, AGG_SCALE, s)
             else:
                 self._k("sphg_gnn_segsum", _ptr(ef), _ptr(b.off), _ptr(agg), b.n, L, AGG_SCALE, s)
-            cat = G("cat" + tag(l), (Np, 2 * L), bf)
-            self._k("sphg_gnn_node_concat", _ptr(hb), _ptr(agg), _ptr(cat), Np, L, s)
+                self._k("sphg_gnn_node_concat", _ptr(hb), _ptr(agg), _ptr(cat), Np, L, s)
             ya = G("ya" + tag(l), (Np, L), bf)
             self._ws(cat, W[p + "v1"]["wb"], Np, L, 2 * L, EPI_BIAS_ACT, 1, B[p + "c1"]["w"], opt("y" + tag(l), (Np, L)),
                      ya)

@@ -413,3 +413,28 @@ def test_edge_encoder_equals_two_gemms(cuda_ok, lib, M):
     assert f(one, one, 100, one, one, one, one, one, None) != 0   # M % 128
     assert f(one, odd, 128, one, one, one, one, one, None) != 0   # E_out alignment
     assert f(None, one, 128, one, one, one, one, one, None) != 0
+
+
+def test_segsum_cat_equals_segsum_and_concat(cuda_ok, lib):
+    """sphg_gnn_segsum_cat gives the same bits as sphg_gnn_segsum_bf16 followed
+    by sphg_gnn_node_concat, padding rows (zero sums) and nodes without edges
+    included."""
+    import torch
+    L, n, npad = 128, 1000, 1024
+    g = torch.Generator(device="cuda").manual_seed(7)
+    deg = torch.randint(0, 40, (n,), device="cuda", generator=g)
+    deg[::9] = 0
+    off = torch.zeros(n + 1, dtype=torch.int64, device="cuda")
+    off[1:] = torch.cumsum(deg, 0)
+    E = int(deg.sum())
+    e = torch.randn(E, L, device="cuda", generator=g).to(torch.bfloat16)
+    h = torch.randn(npad, L, device="cuda", generator=g).to(torch.bfloat16)
+    s = torch.cuda.current_stream().cuda_stream
+    agg = torch.zeros(npad, L, device="cuda")
+    ref = torch.empty(npad, 2 * L, device="cuda", dtype=torch.bfloat16)
+    assert lib.sphg_gnn_segsum_bf16(e.data_ptr(), off.data_ptr(), agg.data_ptr(), n, L, 0.0625, s) == 0
+    assert lib.sphg_gnn_node_concat(h.data_ptr(), agg.data_ptr(), ref.data_ptr(), npad, L, s) == 0
+    out = torch.full((npad, 2 * L), float("nan"), device="cuda").to(torch.bfloat16)
+    assert lib.sphg_gnn_segsum_cat(e.data_ptr(), off.data_ptr(), h.data_ptr(), out.data_ptr(), n, npad, L, 0.0625, s) == 0
+    torch.cuda.synchronize()
+    assert torch.equal(out, ref)

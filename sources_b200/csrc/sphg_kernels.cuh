@@ -49,9 +49,9 @@ struct SimConst {
 // the compiler: 65,536 / (SPHG_TPB * min blocks) registers per thread); the
 // FP64 passes are left uncapped.  Timed on a B200 at 912,016 particles:
 // water_pass_a (staged, recording the hit masks) 131 us at 8 blocks, 134 at
-// 7.  water_pass_b (replaying the masks, with the cross pairs) 176 us at 6
-// blocks, 164 at 7.  soil_pass with the cross pairs: 86 us uncapped (128
-// registers), 91 at 5, 86 at 6.
+// 7, 138 at 10 (48 registers).  water_pass_b (replaying the masks, with the
+// cross pairs) 176 us at 6 blocks, 164 at 7, 181 at 8 (spills).  soil_pass
+// with the cross pairs: 86 us uncapped (128 registers), 91 at 5, 86 at 6.
 #ifndef SPHG_MINB_A
 #define SPHG_MINB_A 8
 #endif

@@ -760,8 +760,9 @@ __global__ void __launch_bounds__(EdgeShape::THREADS, 1) k_edge_layer(const __nv
 // gathers into shared memory that run ahead of the MMAs.  The receiver term
 // is added in the epilogue: edges are sorted by receiver, so a tile's rows
 // share a few Pd rows and their loads are L1 hits.  Warp roles:
-//   warps 0-3   hidden epilogue: acc1 -> + (Pd[dst] + be), relu, bf16 -> the
-//               hidden rows, written back into acc1's first 64 TMEM columns
+//   warps 0-3, 13-16  hidden epilogue, two warps per TMEM lane quarter (64
+//               columns each): acc1 -> + (Pd[dst] + be), relu, bf16 -> the
+//               hidden rows, written back into acc1's columns 0-31 and 64-95
 //   warps 4-7   output epilogue: acc2 -> + (e + b2) -> bf16 e' (global)
 //   warp 8      one thread issues GEMM1 of every tile (as its K blocks arrive)
 //   warp 9      one thread issues GEMM2 of every tile (as its hidden rows
@@ -773,6 +774,8 @@ __global__ void __launch_bounds__(EdgeShape::THREADS, 1) k_edge_layer(const __nv
 //               copies' byte count
 //   warps 11-12 row loaders: the second half of the sender rows by cp.async,
 //               so that the TMA unit and the load/store path gather at once
+// The encoder form (ENC) uses the same roles with one TMA feature block per
+// tile and no row loaders.
 // TMEM: two GEMM1 accumulators (each also holding its tile's hidden rows
 // until GEMM2 has read them) and two GEMM2 accumulators, 512 columns; so
 // GEMM1 of tile i + 1 overlaps the epilogues and GEMM2 of tile i, and neither
@@ -796,7 +799,7 @@ struct EdgeNodeShape {
     static constexpr int KBLK = 4;                       // K blocks of GEMM1 per tile: E, E, h[src], h[src]
     static constexpr int CPB = 3;                        // the K block copied by cp.async (slot 3)
     static constexpr int ROWLOADERS = 64;                // its copy threads (warps 11-12)
-    static constexpr int THREADS = 13 * 32;
+    static constexpr int THREADS = 17 * 32;              // + warps 13-16: the second half of the hidden epilogue
 };
 static_assert(EdgeNodeShape::SMEM <= 227 * 1024, "edge layer shared memory");
 static_assert(EdgeNodeShape::NSLOT % EdgeNodeShape::KBLK == 0, "a slot always holds the same K block");
@@ -861,13 +864,11 @@ __device__ __forceinline__ void umma_f16_ta(uint32_t tacc, uint32_t ta, uint64_t
         "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
         ::"r"(tacc), "r"(ta), "l"(db), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
 }
-// 16 columns of this thread's TMEM lane
-__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t* r) {
-    asm volatile(
-        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-        "%15, %16};" ::"r"(taddr), "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]),
-        "r"(r[7]), "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15])
-        : "memory");
+// 8 columns of this thread's TMEM lane
+__device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t* r) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(taddr),
+                 "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7])
+                 : "memory");
 }
 __device__ __forceinline__ void umma_commit(uint64_t* bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
@@ -929,8 +930,8 @@ __global__ void __launch_bounds__(EdgeNodeShape::THREADS, 1)
             asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(acc2_full + a)), "r"(1));
             asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(acc2_empty + a)), "r"(128));
         }
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(hid_full)), "r"(128));
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(hid_full + 1)), "r"(128));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(hid_full)), "r"(256));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(hid_full + 1)), "r"(256));
         asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(drain)), "r"(1));
         asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(drain + 1)), "r"(1));
         asm volatile("fence.mbarrier_init.release.cluster;" ::);
@@ -955,24 +956,31 @@ __global__ void __launch_bounds__(EdgeNodeShape::THREADS, 1)
     asm volatile("tcgen05.fence::after_thread_sync;" ::);
     const uint32_t tmem = *tslot;
 
-    if (warp < 4) {
-        // ---- hidden epilogue: TMEM lanes 32 warp .. = tile rows.  The receiver's row of
-        // Pd is prefetched into L1 a tile ahead (its index loaded two tiles ahead);
-        // rows of a tile share few receivers, so most of these loads hit the same lines.
-        const uint32_t lane_off = (uint32_t)(warp * 32) << 16;
-        const int r = warp * 32 + lane;
+    if (warp < 4 || warp >= 13) {
+        // ---- hidden epilogue, two warps per TMEM lane quarter (warp % 4): warps 0-3 take
+        // accumulator columns 0-63, warps 13-16 columns 64-127, 16 at a time.  The hidden
+        // rows go back into columns the warp has itself read: K 0-63 to columns 0-31, K
+        // 64-127 to columns 64-95 (two bf16 per column).  The receiver's row of Pd is
+        // prefetched into L1 a tile ahead (its index loaded two tiles ahead); rows of a
+        // tile share few receivers, so most of these loads hit the same lines.
+        const int q4 = warp & 3, half = warp >= 13 ? 1 : 0;
+        const uint32_t lane_off = (uint32_t)(q4 * 32) << 16;
+        const int r = q4 * 32 + lane;
         auto receiver = [&](int i) {
             const long long e = tile_m0(i) + r;
             return !ENC && e < nedge ? dst[e] : -1;
         };
         auto checked = [&](int i, int d) {   // -1 for padding rows and (flagged) indices outside the node rows
-            if (!ENC && tile_m0(i) + r < nedge && (d < 0 || d >= nnode)) { atomicOr(err, 2); return -1; }
+            if (!ENC && tile_m0(i) + r < nedge && (d < 0 || d >= nnode)) {
+                if (half == 0) atomicOr(err, 2);
+                return -1;
+            }
             return d;
         };
         auto prefetch_row = [&](int d) {
             if (d >= 0)
-                for (int q = 0; q < 4; ++q)
-                    asm volatile("prefetch.global.L1 [%0];" ::"l"(Pd + (size_t)d * 128 + 32 * q));
+                for (int q = 0; q < 2; ++q)
+                    asm volatile("prefetch.global.L1 [%0];" ::"l"(Pd + (size_t)d * 128 + 64 * half + 32 * q));
         };
         int d_cur = my > 0 ? checked(0, receiver(0)) : -1;
         int d_next = my > 1 ? receiver(1) : -1;
@@ -981,37 +989,38 @@ __global__ void __launch_bounds__(EdgeNodeShape::THREADS, 1)
             const int a = i & 1;
             if (i + 1 < my) { d_next = checked(i + 1, d_next); prefetch_row(d_next); }
             const int d_after = i + 2 < my ? receiver(i + 2) : -1;
-            const float4* pd = d_cur >= 0 ? reinterpret_cast<const float4*>(Pd + (size_t)d_cur * 128) : nullptr;
-            float4 pa[8], pb[8];   // Pd chunks c and c + 1
+            const float4* pd =
+                d_cur >= 0 ? reinterpret_cast<const float4*>(Pd + (size_t)d_cur * 128 + 64 * half) : nullptr;
+            float4 pa[4], pb[4];   // Pd chunks c and c + 1 (16 columns each)
 #pragma unroll
-            for (int q = 0; q < 8; ++q) pa[q] = pd ? pd[q] : make_float4(0.f, 0.f, 0.f, 0.f);
+            for (int q = 0; q < 4; ++q) pa[q] = pd ? pd[q] : make_float4(0.f, 0.f, 0.f, 0.f);
             bool ok = !*abort_flag && mbar_wait(smem_u32(acc1_full + a), (uint32_t)((i >> 1) & 1), kWaitLimit);
             ok = __all_sync(0xffffffffu, ok);   // the warp's tcgen05.ld / st are warp-collective
             if (!ok) { fail(); break; }
             asm volatile("tcgen05.fence::after_thread_sync;" ::);
             const uint32_t acc = tmem + lane_off + (uint32_t)(a * 128);
 #pragma unroll
-            for (int c = 0; c < 4; ++c) {   // 32 accumulator columns at a time
+            for (int c = 0; c < 4; ++c) {   // 16 accumulator columns at a time
                 float4* p = (c & 1) ? pb : pa;
                 float4* pn = (c & 1) ? pa : pb;
                 if (c < 3) {
 #pragma unroll
-                    for (int q = 0; q < 8; ++q) pn[q] = pd ? pd[8 * (c + 1) + q] : make_float4(0.f, 0.f, 0.f, 0.f);
+                    for (int q = 0; q < 4; ++q) pn[q] = pd ? pd[4 * (c + 1) + q] : make_float4(0.f, 0.f, 0.f, 0.f);
                 }
-                float v[32];
-                tmem_ld32(acc + (uint32_t)(32 * c), v);
-                uint32_t h[16];
+                const int cg = 64 * half + 16 * c;   // the chunk's first accumulator column
+                float v[16];
+                tmem_ld16(acc + (uint32_t)cg, v);
+                uint32_t h[8];
 #pragma unroll
-                for (int j = 0; j < 16; ++j) {
-                    const int col = 32 * c + 2 * j;
+                for (int j = 0; j < 8; ++j) {
+                    const int col = cg + 2 * j;
                     const float4 t4 = p[j >> 1];
                     const float p0 = (j & 1) ? t4.z : t4.x, p1 = (j & 1) ? t4.w : t4.y;
                     const __nv_bfloat162 t = __floats2bfloat162_rn(fmaxf(v[2 * j] + (p0 + sbe[col]), 0.f),
                                                                    fmaxf(v[2 * j + 1] + (p1 + sbe[col + 1]), 0.f));
                     h[j] = *reinterpret_cast<const uint32_t*>(&t);
                 }
-                // the hidden row over the accumulator columns already read: K 32c .. 32c + 31 at columns 16c ..
-                tmem_st16(acc + (uint32_t)(16 * c), h);
+                tmem_st8(acc + (uint32_t)(64 * half + 8 * c), h);
             }
             asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
             asm volatile("tcgen05.fence::before_thread_sync;" ::);
@@ -1026,13 +1035,11 @@ __global__ void __launch_bounds__(EdgeNodeShape::THREADS, 1)
         for (int i = 0; i < my; ++i) {
             const int a = i & 1;
             const long long grow = tile_m0(i) + r;
-            // the residual row, loaded while the tile's GEMMs run (one lane per row, 32-byte accesses)
-            uint32_t res[64];
-            if (!ENC) {
-                const uint8_t* er = reinterpret_cast<const uint8_t*>(E + grow * 128);
-#pragma unroll
-                for (int u = 0; u < 8; ++u) ld_global_32B(er + 32 * u, res + 8 * u);
-            }
+            // the residual row, 32 columns (64 bytes) at a time, each chunk loaded one chunk
+            // ahead; the first while the tile's GEMMs run (one lane per row, 32-byte accesses)
+            const uint8_t* er = reinterpret_cast<const uint8_t*>(E + grow * 128);
+            uint32_t ra_[16], rb_[16];
+            if (!ENC) { ld_global_32B(er, ra_); ld_global_32B(er + 32, ra_ + 8); }
             bool ok = !*abort_flag && mbar_wait(smem_u32(acc2_full + a), (uint32_t)((i >> 1) & 1), kWaitLimit);
             ok = __all_sync(0xffffffffu, ok);
             if (!ok) { fail(); break; }
@@ -1040,6 +1047,9 @@ __global__ void __launch_bounds__(EdgeNodeShape::THREADS, 1)
             uint8_t* out = reinterpret_cast<uint8_t*>(E_out + grow * 128);
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
+                uint32_t* res = (c & 1) ? rb_ : ra_;
+                uint32_t* rn = (c & 1) ? ra_ : rb_;
+                if (!ENC && c < 3) { ld_global_32B(er + 64 * (c + 1), rn); ld_global_32B(er + 64 * (c + 1) + 32, rn + 8); }
                 float v[32];
                 tmem_ld32(tmem + lane_off + (uint32_t)(256 + a * 128 + 32 * c), v);
                 uint32_t o[16];
@@ -1050,8 +1060,7 @@ __global__ void __launch_bounds__(EdgeNodeShape::THREADS, 1)
                     if (ENC) {
                         t = __floats2bfloat162_rn(v[2 * j] + sb2[col], v[2 * j + 1] + sb2[col + 1]);
                     } else {
-                        const float2 e2 =
-                            __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&res[16 * c + j]));
+                        const float2 e2 = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&res[j]));
                         t = __floats2bfloat162_rn(v[2 * j] + (e2.x + sb2[col]), v[2 * j + 1] + (e2.y + sb2[col + 1]));
                     }
                     o[j] = *reinterpret_cast<const uint32_t*>(&t);
@@ -1104,7 +1113,7 @@ __global__ void __launch_bounds__(EdgeNodeShape::THREADS, 1)
 #pragma unroll
                     for (int kk = 0; kk < 8; ++kk) {
                         const uint64_t db = make_desc(smem_u32(sm + S::B2 + kk * 2 * S::KC), S::KC, 128);
-                        umma_f16_ta(tmem + (uint32_t)(256 + a * 128), tmem + (uint32_t)(a * 128 + 8 * kk), db, idesc,
+                        umma_f16_ta(tmem + (uint32_t)(256 + a * 128), tmem + (uint32_t)(a * 128 + (kk < 4 ? 8 * kk : 64 + 8 * (kk - 4))), db, idesc,
                                     kk != 0 ? 1u : 0u);
                     }
                     umma_commit(acc1_empty + a);   // the hidden rows (in GEMM1's accumulator) have been read

@@ -99,6 +99,18 @@ int sphg_gnn_edge_layer_nodes(const void* E, void* E_out, const void* H, const f
 int sphg_gnn_edge_encoder(const void* F, void* E_out, int M, const void* W1, const float* b1, const void* W2,
                           const float* b2, int* err_dev, void* cuda_stream);
 
+/* A node MLP of the message-passing layer in one kernel (inference):
+ *   Z     = Z + (bf16(relu(X V1^T + c1)) V2^T + c2)      (fp32, in place)
+ *   H_out = bf16(Z)
+ * with X the [M x 256] bf16 rows [h | agg], V1 [128 x 256] and V2 [128 x 128]
+ * bf16, c1 and c2 [128] fp32; the hidden rows stay in TMEM.  The same bits as
+ * sphg_gemm_bf16_ws with the BIAS_ACT epilogue (ReLU) followed by the RESID
+ * epilogue on Z, without writing the hidden rows.  M % 128 == 0; H_out
+ * 32-byte aligned, the other arrays 16-byte aligned.  A device wait that gives
+ * up sets *err_dev. */
+int sphg_gnn_node_mlp(const void* X, int M, const void* V1, const float* c1, const void* V2, const float* c2,
+                      float* Z, void* H_out, int* err_dev, void* cuda_stream);
+
 /* Test of the bounded device waits (no counterpart in the reference, whose
  * only failure path is `stop`): launches sphg_gemm_bf16_tn's kernel on
  * A (M x K) and B (N x K) so that its first K block issues no MMA and waits

@@ -40,6 +40,7 @@ EXPORTS = ("sphg_default_params", "sphg_create", "sphg_upload_phase", "sphg_sing
                "sphg_gnn_edge_layer": "PPPPPPLIPPPPPP",
                "sphg_gnn_edge_layer_nodes": "PPPPIPPLIPPPPPPP",
                "sphg_gnn_edge_encoder": "PPIPPPPPP",
+               "sphg_gnn_node_mlp": "PIPPPPPPPP",
                "sphg_gnn_scan_bytes": "IP",
                "sphg_gnn_graph_count": "PPIPPPPPPLP",
                "sphg_gnn_graph_fill": "PPIPPPPPP",

@@ -774,8 +774,9 @@ __global__ void __launch_bounds__(EdgeShape::THREADS, 1) k_edge_layer(const __nv
 //               copies' byte count
 //   warps 11-12 row loaders: the second half of the sender rows by cp.async,
 //               so that the TMA unit and the load/store path gather at once
-// The encoder form (ENC) uses the same roles with one TMA feature block per
-// tile and no row loaders.
+// The encoder form (MODE 1) uses the same roles with one TMA feature block per
+// tile and no row loaders; the node-MLP form (MODE 2) four TMA blocks of the
+// [h | agg] rows and an output epilogue onto the fp32 residual stream.
 // TMEM: two GEMM1 accumulators (each also holding its tile's hidden rows
 // until GEMM2 has read them) and two GEMM2 accumulators, 512 columns; so
 // GEMM1 of tile i + 1 overlaps the epilogues and GEMM2 of tile i, and neither
@@ -875,11 +876,14 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar) {
                  : "memory");
 }
 
-// ENC: the edge encoder in the same pipeline, E_out = bf16(relu(E We^T + be) W2^T + b2)
-// with E the [M x 64] bf16 edge features (one K block per tile, no node rows, no
-// receiver term, no residual); the same sums, in the same order, as the two
-// weight-stationary GEMMs with the BIAS_ACT epilogue.
-template <bool ENC>
+// MODE 0: the edge layer.  MODE 1 (ENC): the edge encoder in the same pipeline,
+// E_out = bf16(relu(E We^T + be) W2^T + b2) with E the [M x 64] bf16 edge features
+// (one K block per tile, no node rows, no receiver term, no residual).  MODE 2
+// (NODE): a node MLP, z = z + (relu(E We^T + be) W2^T + b2) with E the [M x 256]
+// bf16 rows [h | agg] (four TMA K blocks per tile) and z the fp32 residual stream
+// (Z, in place), E_out = bf16(z).  The encoder and node forms form the same sums, in
+// the same order, as two weight-stationary GEMMs (BIAS_ACT, then BIAS_ACT or RESID).
+template <int MODE>
 __global__ void __launch_bounds__(EdgeNodeShape::THREADS, 1)
     k_edge_layer_nodes(const __grid_constant__ CUtensorMap tmE, const __grid_constant__ CUtensorMap tmH,
                        const __nv_bfloat16* E, __nv_bfloat16* E_out, const __nv_bfloat16* __restrict__ H,
@@ -887,10 +891,12 @@ __global__ void __launch_bounds__(EdgeNodeShape::THREADS, 1)
                        const int* __restrict__ src, const int* __restrict__ dst, long long nedge, int M,
                        const __nv_bfloat16* __restrict__ We, const __nv_bfloat16* __restrict__ Ws,
                        const float* __restrict__ be,
-                       const __nv_bfloat16* __restrict__ W2, const float* __restrict__ b2, int* __restrict__ err) {
+                       const __nv_bfloat16* __restrict__ W2, const float* __restrict__ b2, float* Z,
+                       int* __restrict__ err) {
     typedef EdgeNodeShape S;
+    constexpr bool ENC = MODE == 1, NODE = MODE == 2, GATHER = MODE == 0;
     constexpr int KBLK = ENC ? 1 : S::KBLK;              // K blocks of GEMM1 per tile
-    constexpr int CPB = ENC ? -1 : S::CPB;               // the block the row loaders copy
+    constexpr int CPB = GATHER ? S::CPB : -1;            // the block the row loaders copy
     extern __shared__ __align__(128) uint8_t smem[];
     // the swizzled ring slots need 1024-byte alignment in the shared window
     uint8_t* sm = smem + ((1024u - (smem_u32(smem) & 1023u)) & 1023u);
@@ -943,6 +949,7 @@ __global__ void __launch_bounds__(EdgeNodeShape::THREADS, 1)
     for (int c = tid; c < 128 * B1COLS; c += S::THREADS) {
         const int n = c / B1COLS, kc = c % B1COLS;
         const __nv_bfloat16* from = ENC ? We + (size_t)n * 64 + kc * 8
+                                  : NODE ? We + (size_t)n * 256 + kc * 8
                                   : kc < 16 ? We + (size_t)n * 128 + kc * 8 : Ws + (size_t)n * 128 + (kc - 16) * 8;
         *reinterpret_cast<uint4*>(sm + S::B1 + kc * S::KC + (n >> 3) * 128 + (n & 7) * 16) =
             *reinterpret_cast<const uint4*>(from);
@@ -968,10 +975,10 @@ __global__ void __launch_bounds__(EdgeNodeShape::THREADS, 1)
         const int r = q4 * 32 + lane;
         auto receiver = [&](int i) {
             const long long e = tile_m0(i) + r;
-            return !ENC && e < nedge ? dst[e] : -1;
+            return GATHER && e < nedge ? dst[e] : -1;
         };
         auto checked = [&](int i, int d) {   // -1 for padding rows and (flagged) indices outside the node rows
-            if (!ENC && tile_m0(i) + r < nedge && (d < 0 || d >= nnode)) {
+            if (GATHER && tile_m0(i) + r < nedge && (d < 0 || d >= nnode)) {
                 if (half == 0) atomicOr(err, 2);
                 return -1;
             }
@@ -1039,17 +1046,43 @@ __global__ void __launch_bounds__(EdgeNodeShape::THREADS, 1)
             // ahead; the first while the tile's GEMMs run (one lane per row, 32-byte accesses)
             const uint8_t* er = reinterpret_cast<const uint8_t*>(E + grow * 128);
             uint32_t ra_[16], rb_[16];
-            if (!ENC) { ld_global_32B(er, ra_); ld_global_32B(er + 32, ra_ + 8); }
+            if (GATHER) { ld_global_32B(er, ra_); ld_global_32B(er + 32, ra_ + 8); }
             bool ok = !*abort_flag && mbar_wait(smem_u32(acc2_full + a), (uint32_t)((i >> 1) & 1), kWaitLimit);
             ok = __all_sync(0xffffffffu, ok);
             if (!ok) { fail(); break; }
             asm volatile("tcgen05.fence::after_thread_sync;" ::);
             uint8_t* out = reinterpret_cast<uint8_t*>(E_out + grow * 128);
+            if (NODE) {   // z = acc + (z + b2), in place; E_out = bf16(z)
+                float4* zr = reinterpret_cast<float4*>(Z + grow * 128);
 #pragma unroll
-            for (int c = 0; c < 4; ++c) {
+                for (int c = 0; c < 4; ++c) {
+                    float4 zc[8];
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) zc[q] = zr[8 * c + q];
+                    float v[32];
+                    tmem_ld32(tmem + lane_off + (uint32_t)(256 + a * 128 + 32 * c), v);
+                    uint32_t o[16];
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        const int col = 32 * c + 4 * q;
+                        const float4 zq = zc[q];
+                        const float4 nz = make_float4(v[4 * q] + (zq.x + sb2[col]), v[4 * q + 1] + (zq.y + sb2[col + 1]),
+                                                      v[4 * q + 2] + (zq.z + sb2[col + 2]),
+                                                      v[4 * q + 3] + (zq.w + sb2[col + 3]));
+                        zr[8 * c + q] = nz;
+                        const __nv_bfloat162 t0 = __floats2bfloat162_rn(nz.x, nz.y), t1 = __floats2bfloat162_rn(nz.z, nz.w);
+                        o[2 * q] = *reinterpret_cast<const uint32_t*>(&t0);
+                        o[2 * q + 1] = *reinterpret_cast<const uint32_t*>(&t1);
+                    }
+                    st_global_32B(out + 64 * c, o);
+                    st_global_32B(out + 64 * c + 32, o + 8);
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < (NODE ? 0 : 4); ++c) {
                 uint32_t* res = (c & 1) ? rb_ : ra_;
                 uint32_t* rn = (c & 1) ? ra_ : rb_;
-                if (!ENC && c < 3) { ld_global_32B(er + 64 * (c + 1), rn); ld_global_32B(er + 64 * (c + 1) + 32, rn + 8); }
+                if (GATHER && c < 3) { ld_global_32B(er + 64 * (c + 1), rn); ld_global_32B(er + 64 * (c + 1) + 32, rn + 8); }
                 float v[32];
                 tmem_ld32(tmem + lane_off + (uint32_t)(256 + a * 128 + 32 * c), v);
                 uint32_t o[16];
@@ -1136,7 +1169,7 @@ __global__ void __launch_bounds__(EdgeNodeShape::THREADS, 1)
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
                 const long long e = tile_m0(i) + 4 * lane + q;
-                nsr[q] = !ENC && e < nedge ? src[e] : 0;
+                nsr[q] = GATHER && e < nedge ? src[e] : 0;
             }
         };
         if (my > 0) fetch(0);
@@ -1146,7 +1179,7 @@ __global__ void __launch_bounds__(EdgeNodeShape::THREADS, 1)
             for (int q = 0; q < 4; ++q) sr[q] = nsr[q];
             if (i + 1 < my) fetch(i + 1);
             if (lane == 0) {   // the edge rows of the tile after next into L2 (one bulk prefetch)
-                constexpr int ROWB = ENC ? 128 : 256;   // bytes per row of E
+                constexpr int ROWB = ENC ? 128 : NODE ? 512 : 256;   // bytes per row of E
                 for (int t = i == 0 ? 1 : i + 2; t <= i + 2 && t < my; ++t)
                     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(
                                      reinterpret_cast<const uint8_t*>(E) + tile_m0(t) * ROWB),
@@ -1161,7 +1194,7 @@ __global__ void __launch_bounds__(EdgeNodeShape::THREADS, 1)
                 bad |= real && !sv;
                 if (!real || !sv) sr[q] = nnode;
             }
-            if (!ENC && bad) atomicOr(err, 2);   // an index outside the node rows
+            if (GATHER && bad) atomicOr(err, 2);   // an index outside the node rows
             for (int kb = 0; kb < KBLK; ++kb) {
                 if (kb == CPB) continue;   // the row loaders' block
                 const int j = i * KBLK + kb, s = j % S::NSLOT;
@@ -1172,12 +1205,12 @@ __global__ void __launch_bounds__(EdgeNodeShape::THREADS, 1)
                 if (!(ok = __shfl_sync(0xffffffffu, got, 0))) break;
                 const uint32_t slot = smem_u32(sm + S::RING + s * S::SLOT);
                 const uint32_t fb = smem_u32(full + s);
-                const int x = (kb & 1) * 64;   // first column of the block (128 bytes: the swizzle span)
+                const int x = NODE ? kb * 64 : (kb & 1) * 64;   // first column of the block (128 bytes: the swizzle span)
                 if (lane == 0)
                     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(fb), "r"(S::SLOT)
                                  : "memory");
                 __syncwarp();
-                if (kb < 2) {
+                if (kb < 2 || !GATHER) {
                     if (lane == 0)
                         asm volatile(
                             "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
@@ -1193,7 +1226,7 @@ __global__ void __launch_bounds__(EdgeNodeShape::THREADS, 1)
             }
         }
         if (!ok && lane == 0) fail();
-    } else if (!ENC) {
+    } else if (GATHER) {
         // ---- row loaders (warps 11-12): the second half of the sender rows (K block CPB)
         // by cp.async, 16 bytes per request, into the same 128-byte swizzle layout
         // (16-byte chunk u of row r at r * 128 + (u ^ (r & 7)) * 16); each instruction
@@ -1287,7 +1320,7 @@ extern "C" int sphg_gnn_edge_layer_nodes(const void* E, void* E_out, const void*
         return SPHG_ERR_BAD_ARG;
     static bool configured = false;
     if (!configured) {
-        if (cudaFuncSetAttribute(k_edge_layer_nodes<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        if (cudaFuncSetAttribute(k_edge_layer_nodes<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)EdgeNodeShape::SMEM) != cudaSuccess)
             return SPHG_ERR_CUDA;
         configured = true;
@@ -1300,9 +1333,9 @@ extern "C" int sphg_gnn_edge_layer_nodes(const void* E, void* E_out, const void*
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int ntiles = M / 128;
     const int grid = ntiles < sms ? ntiles : sms;
-    k_edge_layer_nodes<false><<<grid, EdgeNodeShape::THREADS, EdgeNodeShape::SMEM, (cudaStream_t)stream>>>(
+    k_edge_layer_nodes<0><<<grid, EdgeNodeShape::THREADS, EdgeNodeShape::SMEM, (cudaStream_t)stream>>>(
         tmE, tmH, (const __nv_bfloat16*)E, (__nv_bfloat16*)E_out, (const __nv_bfloat16*)H, Pd, nnode, src, dst, nedge, M,
-        (const __nv_bfloat16*)We, (const __nv_bfloat16*)Ws, be, (const __nv_bfloat16*)W2, b2, err_dev);
+        (const __nv_bfloat16*)We, (const __nv_bfloat16*)Ws, be, (const __nv_bfloat16*)W2, b2, nullptr, err_dev);
     return cudaGetLastError() == cudaSuccess ? SPHG_OK : SPHG_ERR_CUDA;
 }
 
@@ -1315,7 +1348,7 @@ extern "C" int sphg_gnn_edge_encoder(const void* F, void* E_out, int M, const vo
         return SPHG_ERR_BAD_ARG;
     static bool configured = false;
     if (!configured) {
-        if (cudaFuncSetAttribute(k_edge_layer_nodes<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        if (cudaFuncSetAttribute(k_edge_layer_nodes<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)EdgeNodeShape::SMEM) != cudaSuccess)
             return SPHG_ERR_CUDA;
         configured = true;
@@ -1328,9 +1361,36 @@ extern "C" int sphg_gnn_edge_encoder(const void* F, void* E_out, int M, const vo
     const int ntiles = M / 128;
     const int grid = ntiles < sms ? ntiles : sms;
     // the node-row map is unused by the encoder form; pass the feature map in its place
-    k_edge_layer_nodes<true><<<grid, EdgeNodeShape::THREADS, EdgeNodeShape::SMEM, (cudaStream_t)stream>>>(
+    k_edge_layer_nodes<1><<<grid, EdgeNodeShape::THREADS, EdgeNodeShape::SMEM, (cudaStream_t)stream>>>(
         tmF, tmF, (const __nv_bfloat16*)F, (__nv_bfloat16*)E_out, nullptr, nullptr, 1, nullptr, nullptr, 0, M,
-        (const __nv_bfloat16*)W1, nullptr, b1, (const __nv_bfloat16*)W2, b2, err_dev);
+        (const __nv_bfloat16*)W1, nullptr, b1, (const __nv_bfloat16*)W2, b2, nullptr, err_dev);
+    return cudaGetLastError() == cudaSuccess ? SPHG_OK : SPHG_ERR_CUDA;
+}
+
+extern "C" int sphg_gnn_node_mlp(const void* X, int M, const void* V1, const float* c1, const void* V2,
+                                 const float* c2, float* Z, void* H_out, int* err_dev, void* stream) {
+    if (!X || !V1 || !c1 || !V2 || !c2 || !Z || !H_out || !err_dev) return SPHG_ERR_BAD_ARG;
+    if (M <= 0 || M % 128) return SPHG_ERR_BAD_ARG;
+    if ((((uintptr_t)H_out) & 31) || ((((uintptr_t)X) | ((uintptr_t)V1) | ((uintptr_t)c1) | ((uintptr_t)V2) |
+                                        ((uintptr_t)c2) | ((uintptr_t)Z)) & 15))
+        return SPHG_ERR_BAD_ARG;
+    static bool configured = false;
+    if (!configured) {
+        if (cudaFuncSetAttribute(k_edge_layer_nodes<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)EdgeNodeShape::SMEM) != cudaSuccess)
+            return SPHG_ERR_CUDA;
+        configured = true;
+    }
+    CUtensorMap tmX;   // 128-row tiles of the 256 columns [h | agg]
+    if (encode_tiled(&tmX, X, (uint64_t)M, 128, 256) != CUDA_SUCCESS) return SPHG_ERR_CUDA;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int ntiles = M / 128;
+    const int grid = ntiles < sms ? ntiles : sms;
+    k_edge_layer_nodes<2><<<grid, EdgeNodeShape::THREADS, EdgeNodeShape::SMEM, (cudaStream_t)stream>>>(
+        tmX, tmX, (const __nv_bfloat16*)X, (__nv_bfloat16*)H_out, nullptr, nullptr, 1, nullptr, nullptr, 0, M,
+        (const __nv_bfloat16*)V1, nullptr, c1, (const __nv_bfloat16*)V2, c2, Z, err_dev);
     return cudaGetLastError() == cudaSuccess ? SPHG_OK : SPHG_ERR_CUDA;
 }
 

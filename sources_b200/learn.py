@@ -378,11 +378,18 @@ class MPNet:
             else:
                 self._k("sphg_gnn_segsum", _ptr(ef), _ptr(b.off), _ptr(agg), b.n, L, AGG_SCALE, s)
                 self._k("sphg_gnn_node_concat", _ptr(hb), _ptr(agg), _ptr(cat), Np, L, s)
-            ya = G("ya" + tag(l), (Np, L), bf)
-            self._ws(cat, W[p + "v1"]["wb"], Np, L, 2 * L, EPI_BIAS_ACT, 1, B[p + "c1"]["w"], opt("y" + tag(l), (Np, L)),
-                     ya)
             hb = G("hb" + tag(l + 1), (Np, L), bf)
-            self._ws(ya, W[p + "v2"]["wb"], Np, L, L, EPI_RESID, 0, B[p + "c2"]["w"], hf, hb)  # h += relu(y) V2^T + c2
+            if gather:   # both node GEMMs in one kernel, the hidden rows kept on the SM; h += relu(y) V2^T + c2
+                self.launches += 1
+                _call(self.L.sphg_gnn_node_mlp(_ptr(cat), Np, _ptr(W[p + "v1"]["wb"]), _ptr(B[p + "c1"]["w"]),
+                                               _ptr(W[p + "v2"]["wb"]), _ptr(B[p + "c2"]["w"]), _ptr(hf), _ptr(hb),
+                                               _ptr(self.err), s),
+                      "sphg_gnn_node_mlp")
+            else:
+                ya = G("ya" + tag(l), (Np, L), bf)
+                self._ws(cat, W[p + "v1"]["wb"], Np, L, 2 * L, EPI_BIAS_ACT, 1, B[p + "c1"]["w"],
+                         opt("y" + tag(l), (Np, L)), ya)
+                self._ws(ya, W[p + "v2"]["wb"], Np, L, L, EPI_RESID, 0, B[p + "c2"]["w"], hf, hb)  # h += relu(y) V2^T + c2
         dua = G("dua", (Np, L), bf)
         self._ws(hb, W["dec.w1"]["wb"], Np, L, L, EPI_BIAS_ACT, 1, B["dec.b1"]["w"], opt("du", (Np, L)), dua)
         out = G("out", (Np, L), f32)

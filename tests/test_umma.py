@@ -438,3 +438,33 @@ def test_segsum_cat_equals_segsum_and_concat(cuda_ok, lib):
     assert lib.sphg_gnn_segsum_cat(e.data_ptr(), off.data_ptr(), h.data_ptr(), out.data_ptr(), n, npad, L, 0.0625, s) == 0
     torch.cuda.synchronize()
     assert torch.equal(out, ref)
+
+
+@pytest.mark.parametrize("M", [128 * 2, 128 * 900])
+def test_node_mlp_equals_two_gemms(cuda_ok, lib, M):
+    """sphg_gnn_node_mlp (both node-MLP GEMMs in one kernel, the hidden rows
+    kept in TMEM, the fp32 residual stream updated in place) gives the same bits
+    as the weight-stationary GEMMs with the BIAS_ACT (ReLU) and RESID epilogues."""
+    import torch
+    from sources_b200 import learn
+    L = 128
+    g = torch.Generator(device="cuda").manual_seed(M + 29)
+    X = torch.randn(M, 2 * L, device="cuda", generator=g).to(torch.bfloat16)
+    V1 = (torch.randn(L, 2 * L, device="cuda", generator=g) / 16).to(torch.bfloat16)
+    V2 = (torch.randn(L, L, device="cuda", generator=g) / L ** 0.5).to(torch.bfloat16)
+    c1 = torch.randn(L, device="cuda", generator=g)
+    c2 = torch.randn(L, device="cuda", generator=g)
+    Z0 = torch.randn(M, L, device="cuda", generator=g)
+    ya = torch.zeros(M, L, device="cuda", dtype=torch.bfloat16)
+    Zr, hr = Z0.clone(), torch.zeros(M, L, device="cuda", dtype=torch.bfloat16)
+    _ws(lib, X, V1, M, L, 2 * L, learn.GemmEpi(mode=learn.EPI_BIAS_ACT, relu=1, bias=c1.data_ptr(), h=ya.data_ptr()))
+    _ws(lib, ya, V2, M, L, L, learn.GemmEpi(mode=learn.EPI_RESID, bias=c2.data_ptr(), z=Zr.data_ptr(),
+                                            h=hr.data_ptr()))
+    Z, h = Z0.clone(), torch.zeros(M, L, device="cuda", dtype=torch.bfloat16)
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    rc = lib.sphg_gnn_node_mlp(X.data_ptr(), M, V1.data_ptr(), c1.data_ptr(), V2.data_ptr(), c2.data_ptr(),
+                               Z.data_ptr(), h.data_ptr(), err.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    assert rc == 0 and int(err.item()) == 0
+    assert torch.equal(Z, Zr)
+    assert torch.equal(h, hr)

@@ -122,10 +122,18 @@ struct Engine : EngineBase {
     void* cub_tmp = nullptr;
     void* cub_tmp1 = nullptr;        // the second phase's scan, which may run beside the first's
     size_t cub_bytes = 0;
-    DevCounters* cnt = nullptr;     // device
+    // The step's counters and the sticky flags side by side on the device, so
+    // that one copy into pinned host memory reads both after a batch.
+    struct CounterBlock { DevCounters c; int sticky[4]; };
+    CounterBlock* cblk = nullptr;   // device
+    CounterBlock* hblk = nullptr;   // pinned host copy (nullptr if cudaHostAlloc failed: hblk_heap)
+    CounterBlock hblk_heap{};
+    DevCounters* cnt = nullptr;     // device, &cblk->c
     DevCounters hcnt{};             // host copy
-    int* sticky = nullptr;          // device: [overflow, nonfinite, staging timeout]
+    int* sticky = nullptr;          // device, cblk->sticky: [overflow, nonfinite, staging timeout]
     double* stage = nullptr;        // transfer staging, 2*nmax doubles
+    double* xstage = nullptr;       // staging of a group of fields (bulk transfers), xstage_cap doubles
+    size_t xstage_cap = 0;
     int* stage_i = nullptr;
     long long* stage_l = nullptr;
     std::vector<void*> shadow[2];   // the second buffer of every persistent field
@@ -159,6 +167,7 @@ struct Engine : EngineBase {
     ~Engine() override {
         drop_graphs();
         for (void* p : allocs) cudaFree(p);
+        if (hblk) cudaFreeHost(hblk);
     }
 
     template <typename S>
@@ -376,10 +385,22 @@ struct Engine : EngineBase {
                 return SPHG_ERR_CUDA;
         }
         if (!cnt) {
-            if (alloc(&cnt, 1) || alloc(&sticky, 4)) return SPHG_ERR_CUDA;
+            if (alloc(&cblk, 1)) return SPHG_ERR_CUDA;
+            cnt = &cblk->c;
+            sticky = cblk->sticky;
+            void* hp = nullptr;
+            if (cudaHostAlloc(&hp, sizeof(CounterBlock), cudaHostAllocDefault) == cudaSuccess) hblk = (CounterBlock*)hp;
+            else cudaGetLastError();
         }
         return 0;
     }
+
+    // A host array in original order and its device field in state order
+    // (wide: FP64 on the device, else the precision's type T).
+    struct HostField { const double* h; void* d; int comps; int wide; };
+    // A device field and the host arrays it is copied to (h1: a second copy,
+    // for the water's shared stress/strain-rate working arrays).
+    struct DevField { const void* d; int comps; int wide; double* h0; double* h1; };
 
     int upload(int phase, const sphg_phase_host* h) override {
         cells_ready = false;
@@ -388,22 +409,51 @@ struct Engine : EngineBase {
         int n = h->ntotal + h->nvirt;
         if (n <= 0 || h->ntotal < 0 || h->nvirt < 0) return SPHG_ERR_BAD_ARG;
         int ph = phase - 1;
-        int rc = alloc_phase(ph, n);
+        // Same particles again (size, material; the h range is checked below):
+        // start the copies into the staging area now, so that the scan of h
+        // below runs while they are in flight.
+        const bool same = have[ph] && prepared && P[ph].n == n && P[ph].ntotal == h->ntotal &&
+                          P[ph].material == h->material;
+        int rc = alloc_phase(ph, n);   // keeps every buffer when the size is the same
         if (rc) return rc;
         PhaseDev<T>& D = P[ph];
-        D.ntotal = h->ntotal; D.material = h->material; D.dspp = h->dspp;
-        double lo = INFINITY, hi = 0.0;
-        for (int i = 0; i < n; ++i) {
-            double v = h->hsml[i];
-            if (!(v > 0.0) || !std::isfinite(v)) return SPHG_ERR_BAD_ARG;
-            lo = std::min(lo, v); hi = std::max(hi, v);
+        std::vector<HostField> f;
+        XferList L;
+        bool staged = false;
+        if (same) {
+            f = host_fields(h, D);
+            if ((rc = stage_fields(n, f, L, staged))) return rc;
         }
-        // same particles again (size, material, h range): refill the arrays in
-        // the current state order and keep the grid, the cell order and the
-        // captured graphs
-        if (have[ph] && prepared && P[ph].n == n && P[ph].ntotal == h->ntotal && P[ph].material == h->material &&
-            hrange[ph][0] == lo && hrange[ph][1] == hi)
-            return refill(ph, h);
+        D.ntotal = h->ntotal; D.material = h->material; D.dspp = h->dspp;
+        // every h positive and finite; their range (four independent lanes, no
+        // branch per element: this scan is part of every upload)
+        double lo4[4] = {INFINITY, INFINITY, INFINITY, INFINITY}, hi4[4] = {0.0, 0.0, 0.0, 0.0};
+        int ok = 1;
+        int i = 0;
+        for (; i + 4 <= n; i += 4) {
+            for (int j = 0; j < 4; ++j) {
+                const double v = h->hsml[i + j];
+                ok &= (v > 0.0) & (v < INFINITY);
+                lo4[j] = v < lo4[j] ? v : lo4[j];
+                hi4[j] = v > hi4[j] ? v : hi4[j];
+            }
+        }
+        for (; i < n; ++i) {
+            const double v = h->hsml[i];
+            ok &= (v > 0.0) & (v < INFINITY);
+            lo4[0] = v < lo4[0] ? v : lo4[0];
+            hi4[0] = v > hi4[0] ? v : hi4[0];
+        }
+        const double lo = std::min(std::min(lo4[0], lo4[1]), std::min(lo4[2], lo4[3]));
+        const double hi = std::max(std::max(hi4[0], hi4[1]), std::max(hi4[2], hi4[3]));
+        // same particles and h range: refill the arrays in the current state
+        // order and keep the grid, the cell order and the captured graphs
+        if (ok && same && hrange[ph][0] == lo && hrange[ph][1] == hi)
+            return refill(ph, h, staged ? &f : nullptr, staged ? &L : nullptr);
+        // otherwise the staged copies go unused: let them finish before the
+        // caller's arrays can be released
+        if (staged) CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        if (!ok) return SPHG_ERR_BAD_ARG;
         hrange[ph][0] = lo; hrange[ph][1] = hi;
         // original order == state order until the first reorder
         if ((rc = launch("iota", k_iota, blocks(n, 256), 256, n, D.orig))) return rc;
@@ -434,40 +484,157 @@ struct Engine : EngineBase {
     }
 
     // host (original order) -> state order through the current permutation
-    template <typename S>
-    int fill(int n, const int* orig, const double* src, S* dst, int comps) {
-        if (!src) { CUDA_TRY(cudaMemsetAsync(dst, 0, sizeof(S) * (size_t)n * comps, ctx->stream)); return 0; }
-        CUDA_TRY(cudaMemcpyAsync(stage, src, sizeof(double) * (size_t)n * comps, cudaMemcpyHostToDevice, ctx->stream));
-        return launch("refill", k_from_original<S>, blocks(n, 256), 256, n, orig, (const double*)stage, dst, comps);
-    }
-    int refill(int ph, const sphg_phase_host* h) {
+    int refill(int ph, const sphg_phase_host* h, const std::vector<HostField>* staged = nullptr,
+               const XferList* L = nullptr) {
         PhaseDev<T>& D = P[ph];
         const int n = D.n;
-        const int* o = D.orig;
         D.dspp = h->dspp;
-        int rc = 0;
-        rc |= fill(n, o, h->x, (double*)D.x, 2); rc |= fill(n, o, h->vx, (double*)D.v, 2);
-        rc |= fill(n, o, h->v_min, (double*)D.v_min, 2);
-        rc |= fill(n, o, h->rho, D.rho, 1); rc |= fill(n, o, h->rho_min, D.rho_min, 1);
-        rc |= fill(n, o, h->vof, D.vof, 1); rc |= fill(n, o, h->vof_min, D.vof_min, 1);
-        rc |= fill(n, o, h->p, D.p, 1); rc |= fill(n, o, h->c, D.c, 1); rc |= fill(n, o, h->mass, D.mass, 1);
-        rc |= fill(n, o, h->hsml, D.hsml, 1);
-        rc |= fill(n, o, h->sxx, D.sxx, 1); rc |= fill(n, o, h->sxy, D.sxy, 1); rc |= fill(n, o, h->syy, D.syy, 1);
-        rc |= fill(n, o, h->sxx_min, D.sxx_min, 1); rc |= fill(n, o, h->sxy_min, D.sxy_min, 1);
-        rc |= fill(n, o, h->syy_min, D.syy_min, 1); rc |= fill(n, o, h->p_min, D.p_min, 1);
-        rc |= fill(n, o, h->epsilon_p, D.eps_p, 1);
-        rc |= fill(n, o, h->drho, D.drho, 1); rc |= fill(n, o, h->dvof, D.dvof, 1);
-        rc |= fill(n, o, h->dsxx, D.dsxx, 1); rc |= fill(n, o, h->dsxy, D.dsxy, 1); rc |= fill(n, o, h->dsyy, D.dsyy, 1);
-        rc |= fill(n, o, h->dp, D.dp, 1); rc |= fill(n, o, h->dvx, (T*)D.dv, 2); rc |= fill(n, o, h->av, (T*)D.av, 2);
-        rc |= fill(n, o, h->vof2, D.vof2, 1); rc |= fill(n, o, h->vcc, D.vcc, 1);
-        rc |= fill(n, o, h->txx, D.txx, 1); rc |= fill(n, o, h->tyy, D.tyy, 1); rc |= fill(n, o, h->txy, D.txy, 1);
-        if (rc) return SPHG_ERR_CUDA;
+        int rc = staged ? finish_fields(n, D.orig, *staged, *L) : put_fields(n, D.orig, host_fields(h, D));
+        if (rc) return rc;
         CUDA_TRY(cudaMemcpyAsync(stage_i, h->itype, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, ctx->stream));
-        if (launch("refill", k_from_original_i, blocks(n, 256), 256, n, o, (const int*)stage_i, D.itype))
+        if (launch("refill", k_from_original_i, blocks(n, 256), 256, n, D.orig, (const int*)stage_i, D.itype))
             return SPHG_ERR_CUDA;
         aliased = false;
         CUDA_TRY(cudaStreamSynchronize(ctx->stream));
         return 0;
+    }
+
+    // ------------------------------------------------------- bulk transfers
+    // Staging for every transferred field of an n-particle phase (37 doubles
+    // a particle), up to 2^26 doubles (512 MB) and at least one
+    // two-component field.  Sized for all fields, whatever one call moves, so
+    // that an upload after a download (or the reverse) never reallocates: a
+    // cudaFree would synchronise the device.
+    static constexpr size_t kXferDoubles = 37;
+    int xstage_reserve(int n) {
+        const size_t want = std::max<size_t>(2 * (size_t)n, std::min<size_t>(kXferDoubles * n, (size_t)1 << 26));
+        if (xstage_cap >= want) return 0;
+        release(xstage);
+        xstage = nullptr;
+        xstage_cap = 0;
+        if (alloc(&xstage, want)) return SPHG_ERR_CUDA;
+        xstage_cap = want;
+        return 0;
+    }
+
+    // Every host array of a phase and its device field.
+    std::vector<HostField> host_fields(const sphg_phase_host* h, PhaseDev<T>& D) {
+        return {{h->x, D.x, 2, 1}, {h->vx, D.v, 2, 1}, {h->v_min, D.v_min, 2, 1},
+                {h->rho, D.rho, 1, 1}, {h->rho_min, D.rho_min, 1, 1}, {h->vof, D.vof, 1, 1}, {h->vof_min, D.vof_min, 1, 1},
+                {h->p, D.p, 1, 1}, {h->c, D.c, 1, 1}, {h->mass, D.mass, 1, 1}, {h->hsml, D.hsml, 1, 1},
+                {h->sxx, D.sxx, 1, 1}, {h->sxy, D.sxy, 1, 1}, {h->syy, D.syy, 1, 1},
+                {h->sxx_min, D.sxx_min, 1, 1}, {h->sxy_min, D.sxy_min, 1, 1}, {h->syy_min, D.syy_min, 1, 1},
+                {h->p_min, D.p_min, 1, 1}, {h->epsilon_p, D.eps_p, 1, 1},
+                {h->drho, D.drho, 1, 0}, {h->dvof, D.dvof, 1, 0}, {h->dsxx, D.dsxx, 1, 0}, {h->dsxy, D.dsxy, 1, 0},
+                {h->dsyy, D.dsyy, 1, 0}, {h->dp, D.dp, 1, 0}, {h->dvx, D.dv, 2, 0}, {h->av, D.av, 2, 0},
+                {h->vof2, D.vof2, 1, 0}, {h->vcc, D.vcc, 1, 0}, {h->txx, D.txx, 1, 0}, {h->tyy, D.tyy, 1, 0},
+                {h->txy, D.txy, 1, 0}};
+    }
+
+    // The copies of every non-null host array into the staging area, when
+    // they fit one group (staged; L the group).  The state is not touched, so
+    // the caller may still decline the transfer (after a synchronisation).
+    int stage_fields(int n, const std::vector<HostField>& f, XferList& L, bool& staged) {
+        staged = false;
+        int rc = xstage_reserve(n);
+        if (rc) return rc;
+        size_t need = 0;
+        int nf = 0;
+        for (const HostField& e : f)
+            if (e.h) { need += (size_t)n * e.comps; ++nf; }
+        if (need > xstage_cap || nf > (int)(sizeof(L.f) / sizeof(L.f[0]))) return 0;
+        memset(&L, 0, sizeof(L));
+        size_t off = 0;
+        for (const HostField& e : f) {
+            if (!e.h) continue;
+            const size_t cnt_d = (size_t)n * e.comps;
+            CUDA_TRY(cudaMemcpyAsync(xstage + off, e.h, cnt_d * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+            L.f[L.count++] = XferField{e.d, (long long)off, e.comps, e.wide};
+            off += cnt_d;
+        }
+        staged = true;
+        return 0;
+    }
+    // The rest of a staged transfer: zero the fields without a host array,
+    // then permute and narrow the group into the state.
+    int finish_fields(int n, const int* orig, const std::vector<HostField>& f, const XferList& L) {
+        for (const HostField& e : f)
+            if (!e.h)
+                CUDA_TRY(cudaMemsetAsync(e.d, 0, (size_t)n * e.comps * (e.wide ? sizeof(double) : sizeof(T)), ctx->stream));
+        return L.count ? launch("refill", k_from_original_all<T>, blocks(n, 256), 256, n, orig, L, (const double*)xstage) : 0;
+    }
+
+    // Host -> state order for a list of fields: the copies of a group of
+    // fields go back to back into the staging area, then one launch permutes
+    // and narrows the whole group.  A null host array zeroes its field.
+    int put_fields(int n, const int* orig, const std::vector<HostField>& f) {
+        XferList L;
+        bool staged = false;
+        int rc = stage_fields(n, f, L, staged);
+        if (rc) return rc;
+        if (staged) return finish_fields(n, orig, f, L);
+        memset(&L, 0, sizeof(L));
+        size_t off = 0;
+        auto flush = [&]() -> int {
+            if (L.count == 0) return 0;
+            const int r = launch("refill", k_from_original_all<T>, blocks(n, 256), 256, n, orig, L, (const double*)xstage);
+            L.count = 0;
+            off = 0;
+            return r;
+        };
+        const int cap = (int)(sizeof(L.f) / sizeof(L.f[0]));
+        for (const HostField& e : f) {
+            const size_t cnt_d = (size_t)n * e.comps;
+            if (!e.h) {
+                CUDA_TRY(cudaMemsetAsync(e.d, 0, cnt_d * (e.wide ? sizeof(double) : sizeof(T)), ctx->stream));
+                continue;
+            }
+            if (L.count == cap || off + cnt_d > xstage_cap)
+                if ((rc = flush())) return rc;
+            CUDA_TRY(cudaMemcpyAsync(xstage + off, e.h, cnt_d * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+            L.f[L.count++] = XferField{e.d, (long long)off, e.comps, e.wide};
+            off += cnt_d;
+        }
+        return flush();
+    }
+
+    // State order -> host for a list of fields: one launch permutes and
+    // widens a group of fields into the staging area, then their copies to
+    // the host go back to back.
+    int get_fields(int n, const int* orig, const std::vector<DevField>& f) {
+        int rc = xstage_reserve(n);
+        if (rc) return rc;
+        XferList L;
+        memset(&L, 0, sizeof(L));
+        const DevField* grp[sizeof(L.f) / sizeof(L.f[0])];
+        size_t off = 0;
+        auto flush = [&]() -> int {
+            if (L.count == 0) return 0;
+            int r = launch("download", k_to_original_all<T>, blocks(n, 256), 256, n, orig, L, xstage);
+            if (r) return r;
+            for (int i = 0; i < L.count; ++i) {
+                const size_t bytes = (size_t)n * grp[i]->comps * sizeof(double);
+                double* const hd[2] = {grp[i]->h0, grp[i]->h1};
+                for (int k = 0; k < 2; ++k) {
+                    if (!hd[k]) continue;
+                    CUDA_TRY(cudaMemcpyAsync(hd[k], xstage + L.f[i].off, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+                }
+            }
+            L.count = 0;
+            off = 0;
+            return 0;
+        };
+        const int cap = (int)(sizeof(L.f) / sizeof(L.f[0]));
+        for (const DevField& e : f) {
+            if (!e.h0 && !e.h1) continue;
+            const size_t cnt_d = (size_t)n * e.comps;
+            if (L.count == cap || off + cnt_d > xstage_cap)
+                if ((rc = flush())) return rc;
+            grp[L.count] = &e;
+            L.f[L.count++] = XferField{const_cast<void*>(e.d), (long long)off, e.comps, e.wide};
+            off += cnt_d;
+        }
+        return flush();
     }
 
     int put_state(int n, const double* src, double* dst, int comps) {
@@ -959,10 +1126,12 @@ struct Engine : EngineBase {
 
     // read counters and the sticky flags after a batch
     int finish_batch() override {
-        int hs[4];
-        CUDA_TRY(cudaMemcpyAsync(&hcnt, cnt, sizeof(hcnt), cudaMemcpyDeviceToHost, ctx->stream));
-        CUDA_TRY(cudaMemcpyAsync(hs, sticky, sizeof(hs), cudaMemcpyDeviceToHost, ctx->stream));
+        if (!cblk) return 0;   // nothing uploaded yet: no counters
+        CounterBlock* hb = hblk ? hblk : &hblk_heap;
+        CUDA_TRY(cudaMemcpyAsync(hb, cblk, sizeof(CounterBlock), cudaMemcpyDeviceToHost, ctx->stream));
         CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        hcnt = hb->c;
+        const int* hs = hb->sticky;
         batch_rc = hs[2] ? SPHG_ERR_TIMEOUT : hs[1] ? SPHG_ERR_NONFINITE : hs[0] ? SPHG_ERR_PAIR_OVERFLOW : 0;
         counters_fresh = true;
         return batch_rc;
@@ -1014,36 +1183,29 @@ struct Engine : EngineBase {
         int n = D.n, rc = 0;
         const int* o = D.orig;
         h->ntotal = D.ntotal; h->nvirt = n - D.ntotal; h->material = D.material; h->dspp = D.dspp;
-        rc |= get(n, o, (const double*)D.x, h->x, 2); rc |= get(n, o, (const double*)D.v, h->vx, 2);
-        rc |= get(n, o, (const double*)D.v_min, h->v_min, 2);
-        rc |= get(n, o, (const T*)D.dv, h->dvx, 2); rc |= get(n, o, (const T*)D.av, h->av, 2);
-        rc |= get(n, o, (const double*)D.rho, h->rho, 1); rc |= get(n, o, (const double*)D.rho_min, h->rho_min, 1);
-        rc |= get(n, o, (const T*)D.drho, h->drho, 1); rc |= get(n, o, (const double*)D.p, h->p, 1);
-        rc |= get(n, o, (const double*)D.c, h->c, 1); rc |= get(n, o, (const double*)D.mass, h->mass, 1);
-        rc |= get(n, o, (const double*)D.hsml, h->hsml, 1);
-        rc |= get(n, o, (const double*)D.vof, h->vof, 1); rc |= get(n, o, (const double*)D.vof_min, h->vof_min, 1);
-        rc |= get(n, o, (const T*)D.dvof, h->dvof, 1); rc |= get(n, o, (const T*)D.vof2, h->vof2, 1);
-        rc |= get(n, o, (const T*)D.dsxx, h->dsxx, 1); rc |= get(n, o, (const T*)D.dsxy, h->dsxy, 1);
-        rc |= get(n, o, (const T*)D.dsyy, h->dsyy, 1); rc |= get(n, o, (const T*)D.dp, h->dp, 1);
-        rc |= get(n, o, (const double*)D.sxx_min, h->sxx_min, 1); rc |= get(n, o, (const double*)D.sxy_min, h->sxy_min, 1);
-        rc |= get(n, o, (const double*)D.syy_min, h->syy_min, 1); rc |= get(n, o, (const double*)D.p_min, h->p_min, 1);
-        rc |= get(n, o, (const double*)D.eps_p, h->epsilon_p, 1); rc |= get(n, o, (const T*)D.vcc, h->vcc, 1);
+        std::vector<DevField> f = {
+            {D.x, 2, 1, h->x, nullptr}, {D.v, 2, 1, h->vx, nullptr}, {D.v_min, 2, 1, h->v_min, nullptr},
+            {D.dv, 2, 0, h->dvx, nullptr}, {D.av, 2, 0, h->av, nullptr},
+            {D.rho, 1, 1, h->rho, nullptr}, {D.rho_min, 1, 1, h->rho_min, nullptr}, {D.drho, 1, 0, h->drho, nullptr},
+            {D.p, 1, 1, h->p, nullptr}, {D.c, 1, 1, h->c, nullptr}, {D.mass, 1, 1, h->mass, nullptr},
+            {D.hsml, 1, 1, h->hsml, nullptr}, {D.vof, 1, 1, h->vof, nullptr}, {D.vof_min, 1, 1, h->vof_min, nullptr},
+            {D.dvof, 1, 0, h->dvof, nullptr}, {D.vof2, 1, 0, h->vof2, nullptr},
+            {D.dsxx, 1, 0, h->dsxx, nullptr}, {D.dsxy, 1, 0, h->dsxy, nullptr}, {D.dsyy, 1, 0, h->dsyy, nullptr},
+            {D.dp, 1, 0, h->dp, nullptr},
+            {D.sxx_min, 1, 1, h->sxx_min, nullptr}, {D.sxy_min, 1, 1, h->sxy_min, nullptr},
+            {D.syy_min, 1, 1, h->syy_min, nullptr}, {D.p_min, 1, 1, h->p_min, nullptr},
+            {D.eps_p, 1, 1, h->epsilon_p, nullptr}, {D.vcc, 1, 0, h->vcc, nullptr}};
         if (D.material == SPHG_SOIL) {
-            rc |= get(n, o, (const double*)D.sxx, h->sxx, 1); rc |= get(n, o, (const double*)D.sxy, h->sxy, 1);
-            rc |= get(n, o, (const double*)D.syy, h->syy, 1);
-            rc |= get(n, o, (const T*)D.txx, h->txx, 1); rc |= get(n, o, (const T*)D.tyy, h->tyy, 1);
-            rc |= get(n, o, (const T*)D.txy, h->txy, 1);
+            f.push_back({D.sxx, 1, 1, h->sxx, nullptr}); f.push_back({D.sxy, 1, 1, h->sxy, nullptr});
+            f.push_back({D.syy, 1, 1, h->syy, nullptr});
+            f.push_back({D.txx, 1, 0, h->txx, nullptr}); f.push_back({D.tyy, 1, 0, h->tyy, nullptr});
+            f.push_back({D.txy, 1, 0, h->txy, nullptr});
         } else {
             // water stress lives in the shared working arrays (sxx => txx, ...)
-            double* xx[2] = {h->sxx, h->txx};
-            double* yy[2] = {h->syy, h->tyy};
-            double* xy[2] = {h->sxy, h->txy};
-            for (int t = 0; t < 2; ++t) {
-                rc |= get(n, o, (const double*)D.sxx, xx[t], 1);
-                rc |= get(n, o, (const double*)D.syy, yy[t], 1);
-                rc |= get(n, o, (const double*)D.sxy, xy[t], 1);
-            }
+            f.push_back({D.sxx, 1, 1, h->sxx, h->txx}); f.push_back({D.syy, 1, 1, h->syy, h->tyy});
+            f.push_back({D.sxy, 1, 1, h->sxy, h->txy});
         }
+        rc = get_fields(n, o, f);
         if (h->itype) {
             rc |= launch("download", k_to_original_i, blocks(n, 256), 256, n, o, (const int*)D.itype, stage_i);
             CUDA_TRY(cudaMemcpyAsync(h->itype, stage_i, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));

@@ -122,11 +122,14 @@ struct Engine : EngineBase {
     void* cub_tmp = nullptr;
     void* cub_tmp1 = nullptr;        // the second phase's scan, which may run beside the first's
     size_t cub_bytes = 0;
-    // The step's counters and the sticky flags side by side on the device, so
-    // that one copy into pinned host memory reads both after a batch.
-    struct CounterBlock { DevCounters c; int sticky[4]; };
+    // The step's counters and the sticky flags side by side on the device.
+    // Each step's check also writes them into mapped pinned host memory
+    // (hblk), which the host reads after a batch with no copy; without it
+    // (cudaHostAlloc failed) one copy into hblk_heap reads both.
+    typedef CounterMirror CounterBlock;
     CounterBlock* cblk = nullptr;   // device
-    CounterBlock* hblk = nullptr;   // pinned host copy (nullptr if cudaHostAlloc failed: hblk_heap)
+    CounterBlock* hblk = nullptr;   // mapped pinned host memory, or nullptr
+    CounterBlock* hblk_dev = nullptr;   // its device address
     CounterBlock hblk_heap{};
     DevCounters* cnt = nullptr;     // device, &cblk->c
     DevCounters hcnt{};             // host copy
@@ -389,8 +392,19 @@ struct Engine : EngineBase {
             cnt = &cblk->c;
             sticky = cblk->sticky;
             void* hp = nullptr;
-            if (cudaHostAlloc(&hp, sizeof(CounterBlock), cudaHostAllocDefault) == cudaSuccess) hblk = (CounterBlock*)hp;
-            else cudaGetLastError();
+            void* dp = nullptr;
+            if (cudaHostAlloc(&hp, sizeof(CounterBlock), cudaHostAllocMapped) == cudaSuccess) {
+                if (cudaHostGetDevicePointer(&dp, hp, 0) == cudaSuccess) {
+                    hblk = (CounterBlock*)hp;
+                    hblk_dev = (CounterBlock*)dp;
+                    memset(hblk, 0, sizeof(CounterBlock));
+                } else {
+                    cudaGetLastError();
+                    cudaFreeHost(hp);
+                }
+            } else {
+                cudaGetLastError();
+            }
         }
         return 0;
     }
@@ -401,6 +415,9 @@ struct Engine : EngineBase {
     // A device field and the host arrays it is copied to (h1: a second copy,
     // for the water's shared stress/strain-rate working arrays).
     struct DevField { const void* d; int comps; int wide; double* h0; double* h1; };
+    // A staged water field whose first entries the soil's values replace
+    // (k_alias_soil) before it is copied out.
+    struct SoilAlias { const void* d; const T* src; int zero_tail; };
 
     int upload(int phase, const sphg_phase_host* h) override {
         cells_ready = false;
@@ -601,7 +618,7 @@ struct Engine : EngineBase {
     // State order -> host for a list of fields: one launch permutes and
     // widens a group of fields into the staging area, then their copies to
     // the host go back to back.
-    int get_fields(int n, const int* orig, const std::vector<DevField>& f) {
+    int get_fields(int n, const int* orig, const std::vector<DevField>& f, const std::vector<SoilAlias>& alias = {}) {
         int rc = xstage_reserve(n);
         if (rc) return rc;
         XferList L;
@@ -612,6 +629,15 @@ struct Engine : EngineBase {
             if (L.count == 0) return 0;
             int r = launch("download", k_to_original_all<T>, blocks(n, 256), 256, n, orig, L, xstage);
             if (r) return r;
+            for (const SoilAlias& al : alias) {
+                for (int i = 0; i < L.count; ++i) {
+                    if (L.f[i].dev != al.d) continue;
+                    const int ns = P[1].n;
+                    if ((r = launch("download", k_alias_soil<T>, blocks(std::max(ns, n), 256), 256, ns, n,
+                                    (const int*)P[1].orig, al.src, xstage + L.f[i].off, al.zero_tail)))
+                        return r;
+                }
+            }
             for (int i = 0; i < L.count; ++i) {
                 const size_t bytes = (size_t)n * grp[i]->comps * sizeof(double);
                 double* const hd[2] = {grp[i]->h0, grp[i]->h1};
@@ -1091,7 +1117,8 @@ struct Engine : EngineBase {
         // a step with the corrector has counted the next step's cells
         cells_ready = rc == 0 && u.update != 0;
         if (rc) return rc;
-        return launch_pdl("check", k_check, 1, 32, 0, (const DevCounters*)cnt, sticky, (unsigned long long)p.max_interaction);
+        return launch_pdl("check", k_check, 1, 32, 0, (const DevCounters*)cnt, sticky, (unsigned long long)p.max_interaction,
+                          hblk_dev);
     }
 
     // single_step / single_step_for_water / single_step_for_soil
@@ -1120,6 +1147,12 @@ struct Engine : EngineBase {
     int begin_batch() override {
         counters_fresh = false;
         if (!sticky) return 0;
+        // the last batch ended in a synchronisation, so no kernel writes the
+        // mirror now: the host clears its flags itself
+        if (hblk) {
+            memset(hblk->sticky, 0, sizeof(hblk->sticky));
+            return 0;
+        }
         CUDA_TRY(cudaMemsetAsync(sticky, 0, 4 * sizeof(int), ctx->stream));
         return 0;
     }
@@ -1128,7 +1161,7 @@ struct Engine : EngineBase {
     int finish_batch() override {
         if (!cblk) return 0;   // nothing uploaded yet: no counters
         CounterBlock* hb = hblk ? hblk : &hblk_heap;
-        CUDA_TRY(cudaMemcpyAsync(hb, cblk, sizeof(CounterBlock), cudaMemcpyDeviceToHost, ctx->stream));
+        if (!hblk) CUDA_TRY(cudaMemcpyAsync(hb, cblk, sizeof(CounterBlock), cudaMemcpyDeviceToHost, ctx->stream));
         CUDA_TRY(cudaStreamSynchronize(ctx->stream));
         hcnt = hb->c;
         const int* hs = hb->sticky;
@@ -1142,14 +1175,6 @@ struct Engine : EngineBase {
     int batch_rc = 0;
 
     // ------------------------------------------------------------- download
-    template <typename S>
-    int get(int n, const int* orig, const S* src, double* dst, int comps) {
-        if (!dst) return 0;
-        int rc = launch("download", k_to_original<S>, blocks(n, 256), 256, n, orig, src, stage, comps);
-        if (rc) return rc;
-        CUDA_TRY(cudaMemcpyAsync(dst, stage, sizeof(double) * (size_t)n * comps, cudaMemcpyDeviceToHost, ctx->stream));
-        return 0;
-    }
 
     // positions and velocities between the state and caller device arrays in
     // original order, on the context's stream (no host copy, no sync)
@@ -1205,7 +1230,12 @@ struct Engine : EngineBase {
             f.push_back({D.sxx, 1, 1, h->sxx, h->txx}); f.push_back({D.syy, 1, 1, h->syy, h->tyy});
             f.push_back({D.sxy, 1, 1, h->sxy, h->txy});
         }
-        rc = get_fields(n, o, f);
+        // after a two-phase step the soil pass has overwritten the water's
+        // shared working arrays in part (k_alias_soil)
+        std::vector<SoilAlias> alias;
+        if (D.material == SPHG_WATER && ctx->nphase == 2 && aliased)
+            alias = {{D.sxx, P[1].txx, 0}, {D.syy, P[1].tyy, 0}, {D.sxy, P[1].txy, 1}};
+        rc = get_fields(n, o, f, alias);
         if (h->itype) {
             rc |= launch("download", k_to_original_i, blocks(n, 256), 256, n, o, (const int*)D.itype, stage_i);
             CUDA_TRY(cudaMemcpyAsync(h->itype, stage_i, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
@@ -1216,28 +1246,6 @@ struct Engine : EngineBase {
         }
         CUDA_TRY(cudaStreamSynchronize(ctx->stream));
         if (rc) return SPHG_ERR_CUDA;
-        // Cross-phase aliasing of the working arrays (declarations_sph.f90:371-377,
-        // 414-415): after a two-phase step the soil pass has overwritten the first
-        // n_soil entries of txx/tyy with soil strain rates and all of txy with
-        // the soil spin (zero beyond n_soil, Jaumann_rate m_particles.f90:3077).
-        if (D.material == SPHG_WATER && ctx->nphase == 2 && aliased) {
-            PhaseDev<T>& S = P[1];
-            int ns = S.n;
-            std::vector<double> t((size_t)ns);
-            const T* src[3] = {S.txx, S.tyy, S.txy};
-            double* dxx[3][2] = {{h->sxx, h->txx}, {h->syy, h->tyy}, {h->sxy, h->txy}};
-            for (int f = 0; f < 3; ++f) {
-                bool want = dxx[f][0] || dxx[f][1];
-                if (!want) continue;
-                if (get(ns, S.orig, src[f], t.data(), 1)) return SPHG_ERR_CUDA;
-                CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-                for (int s = 0; s < 2; ++s) {
-                    double* d = dxx[f][s];
-                    if (!d) continue;
-                    for (int i = 0; i < n; ++i) d[i] = i < ns ? t[(size_t)i] : (f == 2 ? 0.0 : d[i]);
-                }
-            }
-        }
         h->nfail = hcnt.nfail[nfail_slot];
         return 0;
     }

@@ -884,14 +884,28 @@ __global__ void __launch_bounds__(SPHG_TPB, sizeof(T) == 4 ? SPHG_MINB_SOIL : 1)
     if (u.update && u.do_dp) count_fail(cnt, 3, fail3);
 }
 
+// The step's counters and the batch's sticky flags as the host reads them.
+struct CounterMirror { DevCounters c; int sticky[4]; };
+
 // Sticky per-batch flags: a pair list above max_interaction (the reference
-// stops there, m_particles.f90:992-993) and non-finite positions.
-static __global__ void k_check(const DevCounters* __restrict__ c, int* __restrict__ sticky, unsigned long long cap) {
+// stops there, m_particles.f90:992-993) and non-finite positions.  With a
+// mirror (mapped pinned host memory) the step's counters and the flags are
+// also written there, so the host reads them after its synchronisation with
+// no copy of its own.
+static __global__ void k_check(const DevCounters* __restrict__ c, int* __restrict__ sticky, unsigned long long cap,
+                               CounterMirror* __restrict__ mirror) {
     pdl_enter();
     if (threadIdx.x == 0 && blockIdx.x == 0) {
-        if (c->pairs[0] / 2 > cap || c->pairs[1] / 2 > cap || c->pairs[2] > cap) sticky[0] = 1;
-        if (c->nonfinite) sticky[1] = 1;
-        if (c->timeout) sticky[2] = 1;
+        const int f[3] = {c->pairs[0] / 2 > cap || c->pairs[1] / 2 > cap || c->pairs[2] > cap, c->nonfinite != 0,
+                          c->timeout != 0};
+        for (int i = 0; i < 3; ++i)
+            if (f[i]) sticky[i] = 1;
+        if (mirror) {
+            mirror->c = *c;
+            for (int i = 0; i < 3; ++i)
+                if (f[i]) mirror->sticky[i] = 1;
+            __threadfence_system();
+        }
     }
 }
 
@@ -1029,6 +1043,23 @@ __global__ void __launch_bounds__(256) k_to_original_all(int n, const int* __res
             const S* s = (const S*)f.dev + (size_t)a * f.comps;
             for (int t = 0; t < f.comps; ++t) d[t] = (double)s[t];
         }
+    }
+}
+// The water's shared working arrays after a two-phase step (sxx => txx,
+// syy => tyy, sxy => txy; declarations_sph.f90:371-377, 414-415): the soil
+// pass has written the first n_soil entries with soil values, indexed by the
+// soil's original order, and txy holds zero beyond them (Jaumann_rate,
+// m_particles.f90:3077).  stage: the water field staged in the water's
+// original order (nw entries).
+template <typename S>
+__global__ void __launch_bounds__(256) k_alias_soil(int ns, int nw, const int* __restrict__ sorig, const S* __restrict__ src,
+                                                    double* __restrict__ stage, int zero_tail) {
+    const int i = gtid();
+    if (i < ns) {
+        const int o = sorig[i];
+        if (o < nw) stage[o] = (double)src[i];
+    } else if (zero_tail && i < nw) {
+        stage[i] = 0.0;
     }
 }
 template <typename S>

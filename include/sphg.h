@@ -166,7 +166,10 @@ void sphg_default_params(sphg_params* p);
  * current CUDA device.  Replaces allocate_sph (declarations_sph.f90:338). */
 int sphg_create(const sphg_params* p, int n_phase, sphg_ctx** out);
 
-/* Copy one phase (1-based: 1 = `parts`, 2 = `soil`) to the device. */
+/* Copy one phase (1-based: 1 = `parts`, 2 = `soil`) to the device.  Uploads
+ * and downloads go through one device staging area of up to 37 doubles a
+ * particle (at most 512 MB), made at the first transfer of the largest phase
+ * and kept until sphg_destroy; pinned host arrays move at the link's speed. */
 int sphg_upload_phase(sphg_ctx* ctx, int phase, const sphg_phase_host* v);
 
 /* Right-hand side only: single_step (declarations_sph.f90:1131), or

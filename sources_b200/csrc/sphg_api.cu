@@ -193,6 +193,12 @@ struct Engine : EngineBase {
     int launch(const char* name, K kern, int grid_, int block, A... args) {
         return launch_ex(name, false, kern, grid_, block, 0, args...);
     }
+    // gx blocks for each of gy fields (blockIdx.y)
+    template <typename K, typename... A>
+    int launch_fields(const char* name, K kern, int gx, int gy, int block, A... args) {
+        if (gx <= 0 || gy <= 0) return 0;
+        return launch_dim(name, false, kern, dim3((unsigned)gx, (unsigned)gy), block, 0, args...);
+    }
     // with `smem` bytes of dynamic shared memory (the neighbour staging space)
     template <typename K, typename... A>
     int launch_smem(const char* name, K kern, int grid_, int block, size_t smem, A... args) {
@@ -210,6 +216,10 @@ struct Engine : EngineBase {
     template <typename K, typename... A>
     int launch_ex(const char* name, bool pdl, K kern, int grid_, int block, size_t smem, A... args) {
         if (grid_ <= 0) return 0;
+        return launch_dim(name, pdl, kern, dim3((unsigned)grid_), block, smem, args...);
+    }
+    template <typename K, typename... A>
+    int launch_dim(const char* name, bool pdl, K kern, dim3 grid_, int block, size_t smem, A... args) {
         cudaEvent_t a = nullptr, b = nullptr;
         if (ctx->prof.on) {
             a = ctx->prof.get(); b = ctx->prof.get();
@@ -217,7 +227,7 @@ struct Engine : EngineBase {
         }
         if (pdl && use_pdl && !ctx->prof.on) {
             cudaLaunchConfig_t cfg = {};
-            cfg.gridDim = dim3((unsigned)grid_);
+            cfg.gridDim = grid_;
             cfg.blockDim = dim3((unsigned)block);
             cfg.dynamicSmemBytes = smem;
             cfg.stream = ctx->stream;
@@ -578,7 +588,7 @@ struct Engine : EngineBase {
         for (const HostField& e : f)
             if (!e.h)
                 CUDA_TRY(cudaMemsetAsync(e.d, 0, (size_t)n * e.comps * (e.wide ? sizeof(double) : sizeof(T)), ctx->stream));
-        return L.count ? launch("refill", k_from_original_all<T>, blocks(n, 256), 256, n, orig, L, (const double*)xstage) : 0;
+        return launch_fields("refill", k_from_original_all<T>, blocks(n, 256), L.count, 256, n, orig, L, (const double*)xstage);
     }
 
     // Host -> state order for a list of fields: the copies of a group of
@@ -594,7 +604,8 @@ struct Engine : EngineBase {
         size_t off = 0;
         auto flush = [&]() -> int {
             if (L.count == 0) return 0;
-            const int r = launch("refill", k_from_original_all<T>, blocks(n, 256), 256, n, orig, L, (const double*)xstage);
+            const int r = launch_fields("refill", k_from_original_all<T>, blocks(n, 256), L.count, 256, n, orig, L,
+                                        (const double*)xstage);
             L.count = 0;
             off = 0;
             return r;
@@ -627,7 +638,7 @@ struct Engine : EngineBase {
         size_t off = 0;
         auto flush = [&]() -> int {
             if (L.count == 0) return 0;
-            int r = launch("download", k_to_original_all<T>, blocks(n, 256), 256, n, orig, L, xstage);
+            int r = launch_fields("download", k_to_original_all<T>, blocks(n, 256), L.count, 256, n, orig, L, xstage);
             if (r) return r;
             for (const SoilAlias& al : alias) {
                 for (int i = 0; i < L.count; ++i) {

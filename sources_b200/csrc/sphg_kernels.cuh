@@ -1024,25 +1024,24 @@ static __global__ void __launch_bounds__(256) k_from_original_i(int n, const int
 // original order, through one staging area in which field i occupies
 // stage[off, off + n*comps) in original order.  wide: the device field is
 // FP64, else of the precision's type S.  One launch per group of fields lets
-// the host copies of the group run back to back on the copy engine.
+// the host copies of the group run back to back on the copy engine; each
+// field has its own row of blocks (blockIdx.y), so that the fields' loads do
+// not wait on one another.
 struct XferField { void* dev; long long off; int comps; int wide; };
 struct XferList { int count; int pad; XferField f[40]; };
 template <typename S>
 __global__ void __launch_bounds__(256) k_to_original_all(int n, const int* __restrict__ orig, const __grid_constant__ XferList L,
                                                          double* __restrict__ stage) {
     const int a = gtid();
-    if (a >= n) return;
-    const size_t o = (size_t)orig[a];
-    for (int i = 0; i < L.count; ++i) {
-        const XferField& f = L.f[i];
-        double* d = stage + f.off + o * f.comps;
-        if (f.wide) {
-            const double* s = (const double*)f.dev + (size_t)a * f.comps;
-            for (int t = 0; t < f.comps; ++t) d[t] = s[t];
-        } else {
-            const S* s = (const S*)f.dev + (size_t)a * f.comps;
-            for (int t = 0; t < f.comps; ++t) d[t] = (double)s[t];
-        }
+    if (a >= n || (int)blockIdx.y >= L.count) return;
+    const XferField& f = L.f[blockIdx.y];
+    double* d = stage + f.off + (size_t)orig[a] * f.comps;
+    if (f.wide) {
+        const double* s = (const double*)f.dev + (size_t)a * f.comps;
+        for (int t = 0; t < f.comps; ++t) d[t] = s[t];
+    } else {
+        const S* s = (const S*)f.dev + (size_t)a * f.comps;
+        for (int t = 0; t < f.comps; ++t) d[t] = (double)s[t];
     }
 }
 // The water's shared working arrays after a two-phase step (sxx => txx,
@@ -1066,18 +1065,15 @@ template <typename S>
 __global__ void __launch_bounds__(256) k_from_original_all(int n, const int* __restrict__ orig, const __grid_constant__ XferList L,
                                                            const double* __restrict__ stage) {
     const int a = gtid();
-    if (a >= n) return;
-    const size_t o = (size_t)orig[a];
-    for (int i = 0; i < L.count; ++i) {
-        const XferField& f = L.f[i];
-        const double* s = stage + f.off + o * f.comps;
-        if (f.wide) {
-            double* d = (double*)f.dev + (size_t)a * f.comps;
-            for (int t = 0; t < f.comps; ++t) d[t] = s[t];
-        } else {
-            S* d = (S*)f.dev + (size_t)a * f.comps;
-            for (int t = 0; t < f.comps; ++t) d[t] = (S)s[t];
-        }
+    if (a >= n || (int)blockIdx.y >= L.count) return;
+    const XferField& f = L.f[blockIdx.y];
+    const double* s = stage + f.off + (size_t)orig[a] * f.comps;
+    if (f.wide) {
+        double* d = (double*)f.dev + (size_t)a * f.comps;
+        for (int t = 0; t < f.comps; ++t) d[t] = s[t];
+    } else {
+        S* d = (S*)f.dev + (size_t)a * f.comps;
+        for (int t = 0; t < f.comps; ++t) d[t] = (S)s[t];
     }
 }
 

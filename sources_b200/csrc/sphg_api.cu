@@ -429,7 +429,20 @@ struct Engine : EngineBase {
     // (k_alias_soil) before it is copied out.
     struct SoilAlias { const void* d; const T* src; int zero_tail; };
 
+    // On an error after copies were queued, let them finish before returning:
+    // the caller may release its host arrays once the call has returned.
     int upload(int phase, const sphg_phase_host* h) override {
+        const int rc = upload_work(phase, h);
+        if (rc && ctx) cudaStreamSynchronize(ctx->stream);
+        return rc;
+    }
+    int download(int phase, sphg_phase_host* h) override {
+        const int rc = download_work(phase, h);
+        if (rc && ctx) cudaStreamSynchronize(ctx->stream);
+        return rc;
+    }
+
+    int upload_work(int phase, const sphg_phase_host* h) {
         cells_ready = false;
         if (phase < 1 || phase > ctx->nphase || !h) return SPHG_ERR_BAD_ARG;
         if (!h->x || !h->vx || !h->rho || !h->p || !h->c || !h->mass || !h->hsml || !h->itype) return SPHG_ERR_BAD_ARG;
@@ -1211,7 +1224,7 @@ struct Engine : EngineBase {
         return rc ? SPHG_ERR_CUDA : SPHG_OK;
     }
 
-    int download(int phase, sphg_phase_host* h) override {
+    int download_work(int phase, sphg_phase_host* h) {
         if (phase < 1 || phase > ctx->nphase || !h) return SPHG_ERR_BAD_ARG;
         int ph = phase - 1;
         if (!have[ph]) return SPHG_ERR_STATE;

@@ -1453,8 +1453,10 @@ int sphg_single_step(sphg_ctx* c, int itimestep) {
     int rc = c->eng->begin_batch();
     if (rc) return rc;
     rc = c->eng->rhs(itimestep);
-    if (rc) return rc;
-    return c->eng->finish_batch();
+    // close the batch in every case: it ends in the synchronisation after
+    // which the next batch may clear the status flags on the host
+    const int rc2 = c->eng->finish_batch();
+    return rc ? rc : rc2;
 }
 
 int sphg_time_integration(sphg_ctx* c, int maxtimestep, int* itimestep, double* time) {

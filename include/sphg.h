@@ -200,21 +200,6 @@ void sphg_group_destroy(sphg_group* group);
 /* Copy one phase back into the Fortran arrays (original particle order). */
 int sphg_download_phase(sphg_ctx* ctx, int phase, sphg_phase_host* v);
 
-/* Page-lock every non-NULL array of nview phase views (ntotal + nvirt
- * entries each), so that sphg_upload_phase and sphg_download_phase copy them
- * at the host link's speed rather than through the driver's staging of
- * pageable memory.  No counterpart in the reference: it serves hosts whose
- * arrays come from their own allocator (Fortran ALLOCATE, malloc) and that
- * have no CUDA runtime binding of their own.  Pass every phase in one call:
- * the whole pages under all the arrays are locked, ranges that touch merged,
- * so arrays of two phases that share a page are covered too.  A second call
- * with the same views is accepted; views that overlap memory the caller
- * locked only in part are refused with SPHG_ERR_BAD_ARG and left as they
- * were.  sphg_unregister_phases with the same views undoes it; call it after
- * the last transfer, before the arrays are freed.  Neither needs a context. */
-int sphg_register_phases(const sphg_phase_host* views, int nview);
-int sphg_unregister_phases(const sphg_phase_host* views, int nview);
-
 /* Positions and velocities of one phase (2n doubles each, original particle
  * order) copied to (export) or from (import) caller DEVICE arrays on the
  * context's stream, without a host copy or a synchronisation; either

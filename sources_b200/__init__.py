@@ -33,7 +33,7 @@ EXPORTS = ("sphg_default_params", "sphg_create", "sphg_upload_phase", "sphg_sing
            "sphg_set_tuning", "sphg_read_case", "sphg_write_tecplot_phase", "sphg_write_tecplot",
            "sphg_gemm_bf16_tn", "sphg_gemm_wait_probe", "sphg_export_xv_device", "sphg_import_xv_device", "sphg_group_create",
            "sphg_group_time_integration", "sphg_group_destroy", "sphg_scene_default", "sphg_scene_size",
-           "sphg_make_scene", "sphg_register_phases", "sphg_unregister_phases", *sorted(_GNN_SIGNATURES := {
+           "sphg_make_scene", *sorted(_GNN_SIGNATURES := {
                # message-passing network kernels (include/sphg_learn.h); P pointer,
                # I int, L 64-bit count, F float, D double, S size_t pointer
                "sphg_gemm_bf16_ws": "PPIIIPPP",
@@ -121,8 +121,6 @@ def load(path: str = LIB_PATH):
                                   C.POINTER(C.c_int32)]
     L.sphg_make_scene.argtypes = [C.POINTER(abi.SceneSpec), C.POINTER(Params), C.POINTER(PhaseHost),
                                   C.POINTER(PhaseHost)]
-    L.sphg_register_phases.argtypes = [C.POINTER(PhaseHost), C.c_int]
-    L.sphg_unregister_phases.argtypes = [C.POINTER(PhaseHost), C.c_int]
     L.sphg_export_xv_device.argtypes = [P, C.c_int, P, P]
     L.sphg_import_xv_device.argtypes = [P, C.c_int, P, P]
     codes = {"P": C.c_void_p, "I": C.c_int, "L": C.c_longlong, "F": C.c_float, "D": C.c_double}

@@ -1696,105 +1696,6 @@ int sphg_download_phase(sphg_ctx* c, int phase, sphg_phase_host* v) {
     return c->eng->download(phase, v);
 }
 
-// Every array of the phase views with its size in bytes (n = ntotal + nvirt).
-static std::vector<std::pair<void*, size_t>> phase_arrays(const sphg_phase_host* views, int nview) {
-    std::vector<std::pair<void*, size_t>> a;
-    for (int k = 0; k < nview; ++k) {
-        const sphg_phase_host* v = views + k;
-        const size_t n = (size_t)v->ntotal + (size_t)v->nvirt;
-        for (double* p : {v->x, v->vx, v->dvx, v->av, v->v_min}) a.push_back({p, 2 * n * sizeof(double)});
-        for (double* p : {v->rho, v->rho_min, v->drho, v->p, v->c, v->mass, v->hsml, v->vof, v->vof_min, v->dvof,
-                          v->vof2, v->sxx, v->sxy, v->syy, v->dsxx, v->dsxy, v->dsyy, v->dp, v->sxx_min, v->sxy_min,
-                          v->syy_min, v->p_min, v->epsilon_p, v->vcc, v->txx, v->tyy, v->txy})
-            a.push_back({p, n * sizeof(double)});
-        for (int32_t* p : {v->itype, v->fail}) a.push_back({p, n * sizeof(int32_t)});
-    }
-    std::vector<std::pair<void*, size_t>> out;
-    for (const auto& x : a)
-        if (x.first && x.second) out.push_back(x);
-    return out;
-}
-
-// The whole pages under those arrays, overlapping or touching ranges merged,
-// so that every array lies inside one registration.
-static std::vector<std::pair<uintptr_t, size_t>> phase_pages(const std::vector<std::pair<void*, size_t>>& arrays) {
-    const uintptr_t page = 4096;
-    std::vector<std::pair<uintptr_t, uintptr_t>> r;
-    for (const auto& a : arrays) {
-        const uintptr_t b = (uintptr_t)a.first;
-        r.push_back({b & ~(page - 1), (b + a.second + page - 1) & ~(page - 1)});
-    }
-    std::sort(r.begin(), r.end());
-    std::vector<std::pair<uintptr_t, size_t>> out;
-    for (const auto& x : r) {
-        if (!out.empty() && x.first <= out.back().first + out.back().second) {
-            const uintptr_t end = std::max(out.back().first + out.back().second, x.second);
-            out.back().second = end - out.back().first;
-        } else {
-            out.push_back({x.first, x.second - x.first});
-        }
-    }
-    return out;
-}
-
-static bool page_locked(const void* p) {
-    cudaPointerAttributes at{};
-    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
-        cudaGetLastError();
-        return false;
-    }
-    return at.type == cudaMemoryTypeHost;
-}
-
-static bool views_ok(const sphg_phase_host* views, int nview) {
-    if (!views || nview < 1) return false;
-    for (int k = 0; k < nview; ++k)
-        if (views[k].ntotal < 0 || views[k].nvirt < 0) return false;
-    return true;
-}
-
-int sphg_unregister_phases(const sphg_phase_host* views, int nview) {
-    if (!views_ok(views, nview)) return SPHG_ERR_BAD_ARG;
-    for (const auto& r : phase_pages(phase_arrays(views, nview)))
-        if (cudaHostUnregister((void*)r.first) != cudaSuccess) cudaGetLastError();   // not registered here
-    return SPHG_OK;
-}
-
-int sphg_register_phases(const sphg_phase_host* views, int nview) {
-    if (!views_ok(views, nview)) return SPHG_ERR_BAD_ARG;
-    const auto arrays = phase_arrays(views, nview);
-    std::vector<void*> mine;
-    auto undo = [&]() {
-        for (void* p : mine) cudaHostUnregister(p);
-        cudaGetLastError();
-    };
-    for (const auto& r : phase_pages(arrays)) {
-        const cudaError_t e = cudaHostRegister((void*)r.first, r.second, cudaHostRegisterDefault);
-        if (e == cudaSuccess) {
-            mine.push_back((void*)r.first);
-            continue;
-        }
-        cudaGetLastError();
-        if (e != cudaErrorHostMemoryAlreadyRegistered) {
-            fprintf(stderr, "libsphg: cudaHostRegister failed: %s\n", cudaGetErrorString(e));
-            undo();
-            return e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver ? SPHG_ERR_NO_DEVICE : SPHG_ERR_CUDA;
-        }
-        // locked before (an earlier call on the same views, or the caller):
-        // accepted only if every array in the range is page-locked from its
-        // first byte to its last
-        for (const auto& a : arrays) {
-            const uintptr_t b = (uintptr_t)a.first;
-            if (b < r.first || b >= r.first + r.second) continue;
-            if (!page_locked(a.first) || !page_locked((const char*)a.first + a.second - 1)) {
-                undo();
-                return SPHG_ERR_BAD_ARG;
-            }
-        }
-    }
-    return SPHG_OK;
-}
-
 int sphg_export_xv_device(sphg_ctx* c, int phase, double* x_dev, double* v_dev) {
     if (!c) return SPHG_ERR_BAD_ARG;
     cudaSetDevice(c->device);

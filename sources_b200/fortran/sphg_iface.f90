@@ -98,17 +98,6 @@ module sphg_iface
        integer(c_int), value :: phase
        type(sphg_phase_host), intent(inout) :: v
      end function
-     ! page-lock / release the arrays of all phase views (no counterpart in the reference)
-     integer(c_int) function sphg_register_phases(views, nview) bind(C, name="sphg_register_phases")
-       import :: sphg_phase_host, c_int
-       type(sphg_phase_host), intent(in) :: views(*)
-       integer(c_int), value :: nview
-     end function
-     integer(c_int) function sphg_unregister_phases(views, nview) bind(C, name="sphg_unregister_phases")
-       import :: sphg_phase_host, c_int
-       type(sphg_phase_host), intent(in) :: views(*)
-       integer(c_int), value :: nview
-     end function
      integer(c_int) function sphg_export_pairs(ctx, which, pair_i, pair_j, cap, n) &
           bind(C, name="sphg_export_pairs")
        import :: c_int, c_ptr, c_int32_t, c_int64_t

@@ -43,31 +43,3 @@ def test_grouped_transfers_round_trip_and_keep_the_trajectory(cuda_ok):
             a, b = full.download(k + 1), trip.download(k + 1)
             for f in ("x", "vx", "rho", "p", "vof", "drho", "dvx"):
                 assert np.array_equal(getattr(a, f), getattr(b, f)), (k, f)
-
-
-def test_registered_host_arrays_round_trip(cuda_ok):
-    """Arrays page-locked by sphg_register_phases (as a Fortran host would do
-    after ALLOCATE: plain host memory, small arrays of both phases side by
-    side) move bit for bit; registering twice and unregistering twice are
-    both accepted, and the arrays stay ordinary memory after."""
-    import ctypes as C
-    from sources_b200 import load
-    from sources_b200.abi import PhaseHost
-    L = load()
-    s = scenes.small("two_phase", precision=SPHG_FP32)
-    with Solver(s) as g:
-        g.time_integration(12)
-        host = [g.download(k + 1) for k in range(2)]          # plain numpy (pageable) arrays
-        views = (PhaseHost * 2)(*[P.host_struct() for P in host])
-        assert L.sphg_register_phases(views, 2) == 0
-        assert L.sphg_register_phases(views, 2) == 0
-        for k, P in enumerate(host):
-            g.download(k + 1, into=P)
-            g.upload(k + 1, P)
-        again = [g.download(k + 1) for k in range(2)]
-        assert L.sphg_unregister_phases(views, 2) == 0
-        assert L.sphg_unregister_phases(views, 2) == 0
-        for A, B in zip(host, again):
-            for f in VEC_FIELDS + SCALAR_FIELDS + INT_FIELDS:
-                assert np.array_equal(getattr(A, f), getattr(B, f)), f
-        host[0].x[0, 0] += 1.0                                  # still ordinary memory
